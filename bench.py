@@ -1,0 +1,374 @@
+"""Benchmark of the per-patch explicit FV step on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--n 256]
+
+Workload (one periodic Cartesian patch of n^3 cells per GPU, default 256^3 =
+16.8 M cells): uniform Mach 0.3 flow with an isentropic vortex (strength 5,
+radius 0.1) and a Gaussian density pulse (1e-2, width 0.05); AUSM+ flux with
+Upwind2 / van Albada reconstruction; 3-stage low-storage RK (alpha 1/4, 1/2,
+1) at CFL 0.5.  A step is one RK time step (three stage launches).
+
+Metric: Mcell-updates/s per RK stage = cells * 3 * K / time / 1e6, for the
+FP32 bulk path (`value`) and the plain FP64 path (`fp64_plain`), with the
+FP32 error against the FP64 run after the same steps and the FP32
+conservation drift.  Prints one JSON line on rank 0.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "Mcell-updates/s per RK stage, FP32-batched vs FP64 plain at stated L2 error"
+UNIT = "Mcell-updates/s"
+STAGES = 3
+
+
+def workload_name(n):
+    return (f"single periodic patch {n}^3, Mach 0.3 flow + isentropic vortex (beta 5, R 0.1) + Gaussian "
+            f"density pulse (1e-2, w 0.05), AUSM+ / Upwind2-VanAlbada / RK3 (1/4, 1/2, 1), CFL 0.5")
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """Samples nvidia-smi clocks and throttle reasons while running."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index):
+        self.device_index = device_index
+        self.proc = None
+        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_bench_rank{device_index}.csv")
+
+    def start(self):
+        try:
+            os.makedirs(os.path.dirname(self.path), exist_ok=True)
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.device_index}", f"--query-gpu={self.QUERY}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=self.f, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.f.close()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+            except ValueError:
+                continue
+            for nm, val in zip(names, parts[5:9]):
+                if val.lower().startswith("active"):
+                    reasons.add(nm)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": float(max(smax)), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def cpu_baseline(U0, h, dt, budget_s=20.0):
+    """The reference CPU iterator (compiled from its own sources) on the host
+    cores, on a bounded sample of the same workload."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pyoracle
+    cells = U0[0].size
+    if pyoracle.ref_available():
+        threads = os.cpu_count() or 1
+        s = pyoracle.RefSession(U0, h, threads=threads)
+        sec = s.step(1, dt)
+        steps = 1
+        extra = int(max(0, min(3, budget_s / max(sec, 1e-3) - 1)))
+        if extra:
+            sec += s.step(extra, dt)
+            steps += extra
+        s.close()
+        return {"value": cells * STAGES * steps / sec / 1e6, "unit": UNIT, "cores": s.threads,
+                "kind": "reference",
+                "sample": f"{steps} RK step(s) of the same {U0.shape[1]}^3 patch, reference CartesianIterator "
+                          f"(FP64, OpenMP {s.threads} threads), RungeKutta::operator() timed"}
+    # the restatement (single thread) on a smaller sample of the same physics
+    from drnum_b200 import cases
+    n = 64
+    U, hh, dts = cases.periodic_box(n)
+    t0 = time.perf_counter()
+    pyoracle.oracle_run(U, hh, dts, 2)
+    sec = time.perf_counter() - t0
+    return {"value": n ** 3 * STAGES * 2 / sec / 1e6, "unit": UNIT, "cores": 1, "kind": "port",
+            "sample": f"2 RK steps of a {n}^3 box of the same physics, oracle restatement (1 thread)"}
+
+
+def run_reference(args, rank, world):
+    """The reference's own CPU implementation of the path (compiled reference
+    library, all host threads), same config and metric as our arm."""
+    if rank != 0:
+        return 0
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pyoracle
+    from drnum_b200 import cases
+    if not pyoracle.ref_available():
+        print(json.dumps({"impl": "reference", "unavailable": "compiled reference library oracle/_ref is missing"}))
+        return 0
+    n = args.n
+    U0, h, dt = cases.periodic_box(n)
+    threads = os.cpu_count() or 1
+    s = pyoracle.RefSession(U0, h, threads=threads)
+    sample_n = n
+    # calibrate with the first warm-up step; shrink the per-step sample if the
+    # whole run would exceed about three minutes
+    t_first = s.step(1, dt)
+    if (args.warmup + args.steps) * t_first > 180.0 and n > 128:
+        s.close()
+        sample_n = 128
+        U0, h, dt = cases.periodic_box(sample_n)
+        s = pyoracle.RefSession(U0, h, threads=threads)
+        s.step(1, dt)
+    for _ in range(max(0, args.warmup - 1)):
+        s.step(1, dt)
+    sec = s.step(args.steps, dt)
+    cells = sample_n ** 3
+    value = cells * STAGES * args.steps / sec / 1e6
+    sample = (f"each step one RK step (3 stages) of a periodic {sample_n}^3 patch of the workload, reference "
+              f"CartesianIterator + RungeKutta compiled FP64 from its own sources, OpenMP {s.threads} threads")
+    s.close()
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": sec / args.steps * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic", "config": {"workload": workload_name(n), "cells": n ** 3},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "reference", "sample": sample},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+    return 0
+
+
+def run_ours(args, rank, world, local_rank):
+    import torch
+    import torch.distributed as dist
+    from drnum_b200 import _lib, cases
+    from drnum_b200.api import AusmPlus, B200CartesianIterator, CartesianPatch
+
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    n = args.n
+    U0, h, dt = cases.periodic_box(n)
+    cells = n ** 3
+    stream = torch.cuda.current_stream(dev)
+
+    def make(precision):
+        patch = CartesianPatch(n, n, n, spacing=(h, h, h))
+        patch.setField(0, U0)
+        it = B200CartesianIterator(AusmPlus(), local_rank, precision)
+        it.addPatch(patch)
+        it.updateDevice(fields=(0,))
+        it.sync()
+        _lib.check(it.ctx, it.lib.dn_set_stream(it.ctx, ctypes_void(stream.cuda_stream)))
+        return patch, it
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    def max_over_ranks(x):
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def timed_steps(it, k):
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        barrier()
+        torch.cuda.synchronize(dev)
+        l0 = it.launchCount()
+        e0.record(stream)
+        for _ in range(k):
+            it.rkStep(dt, cases.RK3_ALPHA)
+        e1.record(stream)
+        torch.cuda.synchronize(dev)
+        barrier()
+        return e0.elapsed_time(e1) / 1e3, it.launchCount() - l0
+
+    # ---- FP32 bulk (headline)
+    p32, it32 = make(_lib.DN_FP32)
+    s0 = it32.conservationSums()
+    for _ in range(args.warmup):
+        it32.rkStep(dt, cases.RK3_ALPHA)
+    it32.sync()
+    clocks = ClockSampler(local_rank)
+    clocks.start()
+    t32, launches = timed_steps(it32, args.steps)
+    clock_info = clocks.stop()
+    it32.sync()
+    s1 = it32.conservationSums()
+    t32 = max_over_ranks(t32)
+    value = world * cells * STAGES * args.steps / t32 / 1e6
+
+    # ---- plain FP64, same steps from the same initial state
+    p64, it64 = make(_lib.DN_FP64)
+    for _ in range(args.warmup):
+        it64.rkStep(dt, cases.RK3_ALPHA)
+    it64.sync()
+    t64, _ = timed_steps(it64, args.steps)
+    t64 = max_over_ranks(t64)
+    value64 = world * cells * STAGES * args.steps / t64 / 1e6
+
+    # ---- error of the FP32 run against the FP64 run after warmup + steps
+    it32.updateHost(fields=(0,))
+    it64.updateHost(fields=(0,))
+    a, b = p32.getField(0), p64.getField(0)
+    drho = (a[0] - b[0]) / cases.RHO_INF
+    pa = cases.cons_to_prim(a)[0]
+    pb = cases.cons_to_prim(b)[0]
+    dp = (pa - pb) / cases.P_INF
+    err = {"l2_rho_rel": float(np.sqrt(np.mean(drho ** 2))), "linf_rho_rel": float(np.abs(drho).max()),
+           "l2_p_rel": float(np.sqrt(np.mean(dp ** 2))), "linf_p_rel": float(np.abs(dp).max()),
+           "steps": args.warmup + args.steps, "against": "FP64 plain GPU path (bit-identical to the reference CPU iterator)"}
+    drift = [float((s1[v] - s0[v]) / abs(s0[v])) if s0[v] != 0 else float(s1[v] - s0[v]) for v in range(5)]
+    it64.close()
+    del p64, a, b
+
+    # ---- e2e through the C ABI with pinned host buffers (float, the reference's default `real`)
+    host = torch.empty((5, n, n, n), dtype=torch.float32, pin_memory=True).numpy()
+    host[...] = p32.getField(0).astype(np.float32)
+    ctx, lib = it32.ctx, it32.lib
+    fptr = _lib.fptr(host)
+    alpha = np.ascontiguousarray(cases.RK3_ALPHA, dtype=np.float64)
+
+    def e2e_step():
+        _lib.check(ctx, lib.dn_patch_upload_f32(ctx, 0, 0, fptr))
+        _lib.check(ctx, lib.dn_rk_step(ctx, dt, _lib.dptr(alpha), 3))
+        _lib.check(ctx, lib.dn_patch_download_f32(ctx, 0, 0, fptr))
+
+    for _ in range(min(args.warmup, 3)):
+        e2e_step()
+    barrier()
+    torch.cuda.synchronize(dev)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        e2e_step()
+    e1.record(stream)
+    torch.cuda.synchronize(dev)
+    te = max_over_ranks(e0.elapsed_time(e1) / 1e3)
+    e2e_value = world * cells * STAGES * args.steps / te / 1e6
+    it32.close()
+
+    # ---- roofline of the dominant kernel (the FP32 stage kernel)
+    peak, peak_kind = measured_peaks()
+    bytes_per_launch = 60.0 * cells      # read f(k-1) + read f(n) + write f(k), 5 x FP32 each
+    launch_s = t32 / (STAGES * args.steps)
+    achieved = bytes_per_launch / launch_s / 1e9
+    traffic = None
+    tp = os.path.join(ROOT, "profiles", "traffic_fv_stage_f32.json")
+    if os.path.exists(tp):
+        with open(tp) as f:
+            tj = json.load(f)
+        traffic = tj.get("dram_bytes_per_launch_scaled", {}).get(str(n))
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(U0, h, dt)
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": t32 / args.steps * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": workload_name(n), "cells_per_gpu": cells, "stages_per_step": STAGES,
+                       "dt": dt, "l2": "inputs larger than L2 (each field 5 x 4 B x cells = "
+                                         f"{20 * cells / 1e6:.0f} MB per GPU)",
+                       "parallelism": f"one independent patch per GPU (x{world}), no collective on the data path"},
+            "fp64_plain": {"value": value64, "unit": UNIT, "ms_per_step": t64 / args.steps * 1e3,
+                           "fp32_over_fp64": value / value64},
+            "error_vs_fp64": err,
+            "conservation_drift_rel": {"mass": drift[0], "mom_x": drift[1], "mom_y": drift[2], "mom_z": drift[3],
+                                       "energy": drift[4], "steps": args.warmup + args.steps},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
+                         "kernel": "fv_stage_kernel<PolicyF32Q,8,32>",
+                         "algorithmic_bytes_per_launch": bytes_per_launch,
+                         "avg_launch_ms": launch_s * 1e3},
+            "cpu_baseline": cpu,
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 20 * cells,
+                    "d2h_bytes_per_step": 20 * cells,
+                    "path": "dn_patch_upload_f32 (pinned host) + dn_rk_step + dn_patch_download_f32 per step"},
+            "gpu_launches": int(launches),
+            "clocks": clock_info,
+        }
+        print(json.dumps(line), flush=True)
+    return 0
+
+
+def ctypes_void(x):
+    import ctypes
+    return ctypes.c_void_p(x)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--n", type=int, default=256)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3 and args.impl == "ours":
+        args.warmup = 3
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        return run_reference(args, rank, world)
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local_rank))
+    try:
+        return run_ours(args, rank, world, local_rank)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,111 @@
+"""ctypes binding of the drnum_b200 C ABI (include/drnum_b200.h).
+
+The shared library is built in-tree by ``python -m drnum_b200.build``.  There
+is no fallback: if the library is missing or cannot be loaded, every call
+raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from ctypes import POINTER, c_double, c_float, c_int, c_int32, c_int64, c_size_t, c_uint8, c_void_p
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libdrnum_b200.so")
+
+DN_OK = 0
+DN_ERR_ARG = -1
+DN_ERR_CUDA = -2
+DN_ERR_STATE = -3
+DN_ERR_NOMEM = -4
+DN_ERR_RANGE = -5
+DN_ERR_DEVICE = -6
+
+DN_FP64 = 0
+DN_FP32 = 1
+
+DN_FACE_PERIODIC = 0
+DN_FACE_CLOSED = 1
+
+
+class dn_patch_desc(ctypes.Structure):
+    _fields_ = [
+        ("ni", c_int32), ("nj", c_int32), ("nk", c_int32),
+        ("face", c_int32 * 3),
+        ("dx", c_double), ("dy", c_double), ("dz", c_double),
+        ("origin", c_double * 3),
+    ]
+
+
+# name -> (restype, argtypes); every declaration of include/drnum_b200.h
+SIGNATURES = {
+    "dn_ctx_create": (c_int, [c_int, c_int, POINTER(c_void_p)]),
+    "dn_ctx_destroy": (c_int, [c_void_p]),
+    "dn_last_error": (c_int, [c_void_p, ctypes.c_char_p, c_size_t]),
+    "dn_set_stream": (c_int, [c_void_p, c_void_p]),
+    "dn_patch_add": (c_int, [c_void_p, POINTER(dn_patch_desc), POINTER(c_int)]),
+    "dn_patch_set_base": (c_int, [c_void_p, c_int, POINTER(c_double), POINTER(c_double)]),
+    "dn_patch_upload": (c_int, [c_void_p, c_int, c_int, POINTER(c_double)]),
+    "dn_patch_upload_f32": (c_int, [c_void_p, c_int, c_int, POINTER(c_float)]),
+    "dn_patch_download": (c_int, [c_void_p, c_int, c_int, POINTER(c_double)]),
+    "dn_patch_download_f32": (c_int, [c_void_p, c_int, c_int, POINTER(c_float)]),
+    "dn_patch_set_active": (c_int, [c_void_p, c_int, POINTER(c_uint8)]),
+    "dn_copy_field": (c_int, [c_void_p, c_int, c_int]),
+    "dn_compute": (c_int, [c_void_p, c_double]),
+    "dn_rk_step": (c_int, [c_void_p, c_double, POINTER(c_double), c_int]),
+    "dn_sync": (c_int, [c_void_p]),
+    "dn_conservation_sums": (c_int, [c_void_p, POINTER(c_double)]),
+    "dn_field_difference": (c_int, [c_void_p, c_int, c_int, c_int, c_int, c_int,
+                                    POINTER(c_double), POINTER(c_double)]),
+    "dn_launch_count": (c_int, [c_void_p, POINTER(c_int64)]),
+}
+
+_lib = None
+
+
+def load(path: str | None = None) -> ctypes.CDLL:
+    """Loads the library (once) and declares every C ABI signature."""
+    global _lib
+    if _lib is not None and path is None:
+        return _lib
+    p = path or LIB_PATH
+    if not os.path.exists(p):
+        raise RuntimeError(f"drnum_b200 native library not built: {p} "
+                           "(run `python -m drnum_b200.build`)")
+    lib = ctypes.CDLL(p)
+    for name, (res, args) in SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    if path is None:
+        _lib = lib
+    return lib
+
+
+class DnError(RuntimeError):
+    def __init__(self, code: int, message: str):
+        super().__init__(f"drnum_b200 error {code}: {message}")
+        self.code = code
+
+
+def check(ctx, code: int) -> None:
+    if code == DN_OK:
+        return
+    msg = ""
+    if ctx:
+        buf = ctypes.create_string_buffer(512)
+        load().dn_last_error(ctx, buf, 512)
+        msg = buf.value.decode(errors="replace")
+    raise DnError(code, msg)
+
+
+def dptr(a):
+    return a.ctypes.data_as(POINTER(c_double))
+
+
+def fptr(a):
+    return a.ctypes.data_as(POINTER(c_float))
+
+
+def u8ptr(a):
+    return a.ctypes.data_as(POINTER(c_uint8))

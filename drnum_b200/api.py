@@ -1,0 +1,286 @@
+"""Host-side mirror of the reference operator API for the patch step.
+
+Names, argument meaning and error behaviour follow DrNUM's host classes so a
+driver written against the reference reads the same:
+
+    reference (file:line)                              here
+    -------------------------------------------------  ---------------------------
+    CartesianPatch (cartesianpatch.h, patch_common.h)  CartesianPatch
+    AusmPlus<5, Upwind2<5, VanAlbada>, PerfectGas>     AusmPlus(Upwind2(VanAlbada()), PerfectGas())
+      (fluxes/ausmplus.h:29-106)
+    GPU_CartesianIterator<5, OP>(op, cuda_device)      B200CartesianIterator(op, cuda_device, precision)
+      (iterators/gpu_cartesianiterator.h:29-40)
+    PatchIterator::addPatch/compute/computeAll/        same method names
+      copyField/updateHost/updateDevice
+      (iterators/patchiterator.h:28-72)
+    RungeKutta::addAlpha/addIterator/operator()(dt)    RungeKutta.addAlpha/addIterator/__call__(dt)
+      (rungekutta.h:28-40, timeintegration.h:33-50)
+
+Errors: the reference prints and exits (BUG/ERROR, drnum.h:109-128); here a
+failing call raises DnError with the library's message.  All numerical work
+goes through the native library (libdrnum_b200.so); there is no host
+fallback.
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+from . import _lib
+from ._lib import DN_FACE_CLOSED, DN_FACE_PERIODIC, DN_FP32, DN_FP64, check
+
+
+# ----------------------------------------------------------- flux functor concept
+
+class VanAlbada:
+    """reconstruction/vanalbada.h:26-34"""
+
+
+class Upwind2:
+    """reconstruction/upwind2.h:26-53 (MUSCL on conservative variables)."""
+
+    def __init__(self, limiter=None):
+        self.limiter = limiter if limiter is not None else VanAlbada()
+
+
+class PerfectGas:
+    """perfectgas.h:26-45: R = 287.2, gamma = 1.4, cp = 1004.5, cv = 717.5."""
+    R = 287.2
+    gamma = 1.4
+    cp = 1004.5
+    cv = 717.5
+
+
+class AusmPlus:
+    """The AUSM+ face-flux functor (fluxes/ausmplus.h:29-106) with its
+    reconstruction and gas model; the device kernels implement exactly this
+    combination."""
+
+    def __init__(self, reconstruction=None, gas=None):
+        self.reconstruction = reconstruction if reconstruction is not None else Upwind2(VanAlbada())
+        self.gas = gas if gas is not None else PerfectGas()
+        if not isinstance(self.reconstruction, Upwind2) or not isinstance(self.reconstruction.limiter, VanAlbada):
+            raise ValueError("the device path implements Upwind2<VanAlbada> reconstruction only")
+        if not isinstance(self.gas, PerfectGas):
+            raise ValueError("the device path implements PerfectGas only")
+
+
+# ----------------------------------------------------------------------- patches
+
+class CartesianPatch:
+    """A Cartesian patch with host-side fields [field][var][i][j][k].
+
+    Mirrors CartesianPatch's geometry accessors (sizeI/J/K, dx/dy/dz, dV),
+    its field accessors (getField, f) and the active mask
+    (activate/deactivate/isActive, cartesianpatch_common.h:332-334).
+    Faces are periodic or closed per axis.
+    """
+
+    def __init__(self, ni, nj, nk, lengths=None, spacing=None, origin=(0.0, 0.0, 0.0),
+                 periodic=(True, True, True), num_fields=3):
+        self.m_NumI, self.m_NumJ, self.m_NumK = int(ni), int(nj), int(nk)
+        if spacing is None:
+            if lengths is None:
+                raise ValueError("give lengths or spacing")
+            # CartesianPatch::computeDeltas (cartesianpatch.cpp:160-162)
+            spacing = (lengths[0] / ni, lengths[1] / nj, lengths[2] / nk)
+        self.m_Dx, self.m_Dy, self.m_Dz = (float(s) for s in spacing)
+        self.origin = tuple(float(o) for o in origin)
+        self.periodic = tuple(bool(p) for p in periodic)
+        self.m_NumFields = num_fields
+        self.data = np.zeros((num_fields, 5, ni, nj, nk))
+        self.active = np.ones((ni, nj, nk), dtype=np.uint8)
+
+    def sizeI(self): return self.m_NumI
+    def sizeJ(self): return self.m_NumJ
+    def sizeK(self): return self.m_NumK
+    def sizeL(self): return self.m_NumI * self.m_NumJ * self.m_NumK
+    def dx(self): return self.m_Dx
+    def dy(self): return self.m_Dy
+    def dz(self): return self.m_Dz
+    def dV(self): return self.m_Dx * self.m_Dy * self.m_Dz
+    def numVariables(self): return 5
+    def numFields(self): return self.m_NumFields
+
+    def getField(self, i_field):
+        return self.data[i_field]
+
+    def f(self, i_field, i_var, i, j, k):
+        return self.data[i_field, i_var, i, j, k]
+
+    def setField(self, i_field, values):
+        self.data[i_field][...] = values
+
+    def deactivate(self, i, j, k): self.active[i, j, k] = 0
+    def activate(self, i, j, k): self.active[i, j, k] = 1
+    def isActive(self, i, j, k): return bool(self.active[i, j, k])
+
+    def desc(self) -> _lib.dn_patch_desc:
+        d = _lib.dn_patch_desc()
+        d.ni, d.nj, d.nk = self.m_NumI, self.m_NumJ, self.m_NumK
+        for a in range(3):
+            d.face[a] = DN_FACE_PERIODIC if self.periodic[a] else DN_FACE_CLOSED
+        d.dx, d.dy, d.dz = self.m_Dx, self.m_Dy, self.m_Dz
+        for a in range(3):
+            d.origin[a] = self.origin[a]
+        return d
+
+
+# --------------------------------------------------------------------- iterator
+
+class B200CartesianIterator:
+    """Counterpart of GPU_CartesianIterator<5, OP>(op, cuda_device) for the
+    B200 kernels.  `precision` selects the plain FP64 path (DN_FP64) or the
+    FP32 bulk path (DN_FP32)."""
+
+    def __init__(self, op=None, cuda_device=0, precision=DN_FP64):
+        self.m_Op = op if op is not None else AusmPlus()
+        if not isinstance(self.m_Op, AusmPlus):
+            raise ValueError("flux functor must be AusmPlus(Upwind2(VanAlbada()), PerfectGas())")
+        self.lib = _lib.load()
+        self.precision = precision
+        self.ctx = ctypes.c_void_p()
+        check(None, self.lib.dn_ctx_create(int(cuda_device), int(precision), ctypes.byref(self.ctx)))
+        self.m_Patches: list[CartesianPatch] = []
+        self.m_PatchActive: list[bool] = []
+
+    def __del__(self):
+        ctx = getattr(self, "ctx", None)
+        if ctx:
+            self.lib.dn_ctx_destroy(ctx)
+            self.ctx = None
+
+    def close(self):
+        self.__del__()
+
+    # PatchIterator interface (patchiterator.h:43-54)
+    def addPatch(self, patch: CartesianPatch) -> int:
+        pid = ctypes.c_int()
+        d = patch.desc()
+        check(self.ctx, self.lib.dn_patch_add(self.ctx, ctypes.byref(d), ctypes.byref(pid)))
+        self.m_Patches.append(patch)
+        self.m_PatchActive.append(True)
+        return pid.value
+
+    def numPatches(self):
+        return len(self.m_Patches)
+
+    def getPatch(self, i):
+        return self.m_Patches[i]
+
+    def activatePatch(self, i):
+        self.m_PatchActive[i] = True
+
+    def deactivatePatch(self, i):
+        if not 0 <= i < len(self.m_Patches):
+            raise IndexError(i)
+        self.m_PatchActive[i] = False
+        if not all(self.m_PatchActive):
+            raise NotImplementedError("per-patch deactivation is not supported by the fused path")
+
+    def setBase(self, i_patch, base, scale):
+        b = np.ascontiguousarray(base, dtype=np.float64)
+        s = np.ascontiguousarray(scale, dtype=np.float64)
+        check(self.ctx, self.lib.dn_patch_set_base(self.ctx, i_patch, _lib.dptr(b), _lib.dptr(s)))
+
+    def updateDevice(self, fields=(0, 1)):
+        for pid, p in enumerate(self.m_Patches):
+            for f in fields:
+                a = np.ascontiguousarray(p.data[f], dtype=np.float64)
+                check(self.ctx, self.lib.dn_patch_upload(self.ctx, pid, f, _lib.dptr(a)))
+            if p.active.all():
+                check(self.ctx, self.lib.dn_patch_set_active(self.ctx, pid, None))
+            else:
+                m = np.ascontiguousarray(p.active, dtype=np.uint8)
+                check(self.ctx, self.lib.dn_patch_set_active(self.ctx, pid, _lib.u8ptr(m)))
+
+    def updateHost(self, fields=(0, 1)):
+        for pid, p in enumerate(self.m_Patches):
+            for f in fields:
+                a = np.empty(p.data[f].shape, dtype=np.float64)
+                check(self.ctx, self.lib.dn_patch_download(self.ctx, pid, f, _lib.dptr(a)))
+                p.data[f][...] = a
+
+    def copyField(self, i_src, i_dst):
+        check(self.ctx, self.lib.dn_copy_field(self.ctx, i_src, i_dst))
+
+    def compute(self, factor, patches=None):
+        if patches is not None and list(patches) != list(range(len(self.m_Patches))):
+            raise NotImplementedError("the fused path computes all patches of the iterator")
+        check(self.ctx, self.lib.dn_compute(self.ctx, float(factor)))
+
+    def computeAll(self, factor):
+        self.compute(factor)
+
+    def copyDonorData(self, i_field):
+        # no overlap coupling registered: nothing to transfer
+        return None
+
+    def rkStep(self, dt, alphas):
+        a = np.ascontiguousarray(alphas, dtype=np.float64)
+        check(self.ctx, self.lib.dn_rk_step(self.ctx, float(dt), _lib.dptr(a), len(a)))
+
+    def sync(self):
+        check(self.ctx, self.lib.dn_sync(self.ctx))
+
+    def conservationSums(self):
+        out = np.zeros(5)
+        check(self.ctx, self.lib.dn_conservation_sums(self.ctx, _lib.dptr(out)))
+        return out
+
+    def computeVariableDifference(self, i_patch, i_field1, i_var1, i_field2, i_var2):
+        mx, l2 = ctypes.c_double(), ctypes.c_double()
+        check(self.ctx, self.lib.dn_field_difference(self.ctx, i_patch, i_field1, i_var1, i_field2, i_var2,
+                                                     ctypes.byref(mx), ctypes.byref(l2)))
+        return mx.value, l2.value
+
+    def launchCount(self):
+        n = ctypes.c_int64()
+        check(self.ctx, self.lib.dn_launch_count(self.ctx, ctypes.byref(n)))
+        return n.value
+
+
+# ------------------------------------------------------------- time integration
+
+class RungeKutta:
+    """RungeKutta (rungekutta.h:28-40, rungekutta.cpp:27-42) over
+    B200CartesianIterator objects: one fused dn_rk_step per iterator when no
+    post-operation is registered, else the reference's stage sequence."""
+
+    def __init__(self):
+        self.m_Alpha: list[float] = []
+        self.m_Iterators: list[B200CartesianIterator] = []
+        self.m_PostOperations = []
+
+    def addAlpha(self, a):
+        self.m_Alpha.append(float(a))
+
+    def addIterator(self, it):
+        self.m_Iterators.append(it)
+
+    def addPostOperation(self, op):
+        self.m_PostOperations.append(op)
+
+    def copyDonorData(self, i_field):
+        for it in self.m_Iterators:
+            it.copyDonorData(i_field)
+
+    def __call__(self, dt):
+        if not self.m_PostOperations:
+            for it in self.m_Iterators:
+                it.rkStep(dt, self.m_Alpha)
+            return
+        self.copyDonorData(0)
+        for it in self.m_Iterators:
+            it.copyField(0, 1)
+        first = True
+        for a in self.m_Alpha:
+            if not first:
+                self.copyDonorData(0)
+            first = False
+            for it in self.m_Iterators:
+                it.computeAll(a * dt)
+            self.copyDonorData(0)
+            for op in self.m_PostOperations:
+                op()

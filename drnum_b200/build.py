@@ -1,0 +1,91 @@
+"""Builds the drnum_b200 shared library (CUDA, sm_100a) in-tree.
+
+    python -m drnum_b200.build            # -> drnum_b200/libdrnum_b200.so
+
+Every CUDA translation unit is compiled for sm_100a only; the FP64 stage
+kernel gets -fmad=false (bitwise parity with the reference CPU iterator), the
+FP32 kernel gets fast-math intrinsics.
+"""
+from __future__ import annotations
+
+import os
+import shutil
+import subprocess
+import sys
+from concurrent.futures import ThreadPoolExecutor
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(HERE)
+CSRC = os.path.join(HERE, "csrc")
+INCLUDE = os.path.join(ROOT, "include")
+OBJDIR = os.path.join(HERE, "_build")
+LIB = os.path.join(HERE, "libdrnum_b200.so")
+
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-I", INCLUDE, "-I", CSRC,
+          "--expt-relaxed-constexpr"]
+
+# translation unit -> extra flags
+UNITS = {
+    "dn_api.cu": [],
+    "fv_fp64.cu": ["-fmad=false"],
+    "fv_fp32.cu": ["-use_fast_math"],
+}
+
+
+def nvcc() -> str:
+    cand = shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc"
+    if not os.path.exists(cand):
+        raise RuntimeError("nvcc not found")
+    return cand
+
+
+def _sources_newer(target: str, deps: list[str]) -> bool:
+    if not os.path.exists(target):
+        return True
+    t = os.path.getmtime(target)
+    return any(os.path.getmtime(d) > t for d in deps)
+
+
+def _headers() -> list[str]:
+    hs = [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".cuh", ".h"))]
+    hs.append(os.path.join(INCLUDE, "drnum_b200.h"))
+    return hs
+
+
+def build(verbose: bool = False, ptxas_info: bool = False) -> str:
+    os.makedirs(OBJDIR, exist_ok=True)
+    cc = nvcc()
+    headers = _headers()
+
+    def compile_one(unit: str) -> str:
+        src = os.path.join(CSRC, unit)
+        obj = os.path.join(OBJDIR, unit.replace(".cu", ".o"))
+        if _sources_newer(obj, [src, *headers]) or ptxas_info:
+            cmd = [cc, *ARCH, *COMMON, *UNITS[unit], "-c", src, "-o", obj]
+            if ptxas_info:
+                cmd.insert(1, "-Xptxas=-v")
+            if verbose:
+                print(" ".join(cmd), flush=True)
+            res = subprocess.run(cmd, capture_output=True, text=True)
+            if res.returncode != 0:
+                raise RuntimeError(f"nvcc failed for {unit}:\n{res.stdout}\n{res.stderr}")
+            if ptxas_info:
+                print(res.stderr)
+        return obj
+
+    with ThreadPoolExecutor(max_workers=len(UNITS)) as ex:
+        objs = list(ex.map(compile_one, UNITS))
+    if _sources_newer(LIB, objs):
+        cmd = [cc, *ARCH, "-shared", "-o", LIB, *objs]
+        if verbose:
+            print(" ".join(cmd), flush=True)
+        res = subprocess.run(cmd, capture_output=True, text=True)
+        if res.returncode != 0:
+            raise RuntimeError(f"link failed:\n{res.stdout}\n{res.stderr}")
+    return LIB
+
+
+if __name__ == "__main__":
+    build(verbose=True, ptxas_info="-v" in sys.argv)
+    print(LIB)

@@ -1,0 +1,118 @@
+"""Seeded synthetic initial states of the benchmark workloads (FP64, host).
+
+All states are conservative variables [rho, rho u, rho v, rho w, rho E] laid
+out [5][ni][nj][nk] (k fastest), built with the reference's gas model:
+PerfectGas::primitiveToConservative (perfectgas.h:58-66), R = 287.2,
+gamma = 1.4, cv = 717.5.  The reference ships no cases, so these are the
+stand-ins for its workloads; every generator is deterministic.
+"""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+
+GAS_R = 287.2
+GAS_GAMMA = 1.4
+GAS_CV = 717.5
+
+P_INF = 1.0e5
+T_INF = 300.0
+RHO_INF = P_INF / (GAS_R * T_INF)
+A_INF = math.sqrt(GAS_GAMMA * GAS_R * T_INF)
+
+RK3_ALPHA = (0.25, 0.5, 1.0)   # drnumJetDemo/main.h:131-133
+
+
+def prim_to_cons(p, T, u, v, w):
+    """PerfectGas::primitiveToConservative(p, T, u, v, w) (perfectgas.h:58-66)."""
+    r = p / (GAS_R * T)
+    out = np.empty((5,) + np.shape(r))
+    out[0] = r
+    out[1] = r * u
+    out[2] = r * v
+    out[3] = r * w
+    out[4] = r * (GAS_CV * T + 0.5 * (u * u + v * v + w * w))
+    return out
+
+
+def cons_to_prim(U):
+    """PerfectGas::conservativeToPrimitive (perfectgas.h:84-93): p, T, u, v, w."""
+    r = U[0]
+    u, v, w = U[1] / r, U[2] / r, U[3] / r
+    T = (U[4] / r - 0.5 * (u * u + v * v + w * w)) / GAS_CV
+    p = r * GAS_R * T
+    return p, T, u, v, w
+
+
+def cell_centres(n, h, origin=0.0):
+    return origin + (np.arange(n) + 0.5) * h
+
+
+def vortex_pulse(ni, nj, nk, lengths=(1.0, 1.0, 1.0), mach=0.3, beta=5.0, radius=0.1,
+                 pulse_amp=1e-2, pulse_width=0.05, centre=None):
+    """Uniform flow along x at `mach`, an isentropic vortex (axis along z,
+    strength beta, radius `radius`, centred) and a Gaussian density pulse
+    at constant pressure, on a periodic box of `lengths`.
+
+    Vortex (Yee-type, velocities in units of a_inf, radius-normalised r):
+        du = -beta/(2 pi) * y' * exp((1 - r^2)/2),  dv = +beta/(2 pi) * x' * exp((1 - r^2)/2)
+        T/T_inf = 1 - (gamma-1) beta^2 / (8 gamma pi^2) * exp(1 - r^2),  rho ~ T^(1/(gamma-1))
+    Pulse: rho *= 1 + pulse_amp * exp(-|x - c|^2 / pulse_width^2) at fixed p.
+    """
+    Lx, Ly, Lz = lengths
+    hx, hy, hz = Lx / ni, Ly / nj, Lz / nk
+    if centre is None:
+        centre = (0.5 * Lx, 0.5 * Ly, 0.5 * Lz)
+    x = cell_centres(ni, hx)[:, None, None]
+    y = cell_centres(nj, hy)[None, :, None]
+    z = cell_centres(nk, hz)[None, None, :]
+    xr = (x - centre[0]) / radius
+    yr = (y - centre[1]) / radius
+    r2 = xr * xr + yr * yr
+    e = np.exp(0.5 * (1.0 - r2))
+    k = beta / (2.0 * math.pi)
+    u = mach * A_INF - k * yr * e * A_INF
+    v = k * xr * e * A_INF
+    w = np.zeros_like(u)
+    Tn = 1.0 - (GAS_GAMMA - 1.0) * beta * beta / (8.0 * GAS_GAMMA * math.pi ** 2) * e * e
+    T = T_INF * Tn
+    rho = RHO_INF * Tn ** (1.0 / (GAS_GAMMA - 1.0))
+    p = rho * GAS_R * T
+    d2 = (x - centre[0]) ** 2 + (y - centre[1]) ** 2 + (z - centre[2]) ** 2
+    rho = rho * (1.0 + pulse_amp * np.exp(-d2 / pulse_width ** 2))
+    T = p / (rho * GAS_R)
+    shape = (ni, nj, nk)
+    return prim_to_cons(np.broadcast_to(p, shape), np.broadcast_to(T, shape),
+                        np.broadcast_to(u, shape), np.broadcast_to(v, shape), np.broadcast_to(w, shape))
+
+
+def random_state(ni, nj, nk, seed=0, amp=0.05, mach=0.4):
+    """A rough seeded state (white-noise perturbations of every primitive) that
+    drives the limiter and the sub/supersonic AUSM+ branches everywhere."""
+    rng = np.random.default_rng(seed)
+    shape = (ni, nj, nk)
+    p = P_INF * (1.0 + amp * rng.standard_normal(shape))
+    T = T_INF * (1.0 + amp * rng.standard_normal(shape))
+    u = A_INF * (mach + 10 * amp * rng.standard_normal(shape))
+    v = A_INF * (10 * amp * rng.standard_normal(shape))
+    w = A_INF * (10 * amp * rng.standard_normal(shape))
+    return prim_to_cons(p, T, u, v, w)
+
+
+def cfl_dt(U, dx, cfl=0.5):
+    """dt = cfl * dx / max(|u| + a) over the state (drnumJetDemo/main.h:108-111
+    style characteristic speed with the cell-wise velocity magnitude)."""
+    p, T, u, v, w = cons_to_prim(U)
+    a = np.sqrt(GAS_GAMMA * GAS_R * T)
+    s = np.sqrt(u * u + v * v + w * w) + a
+    return cfl * dx / float(s.max())
+
+
+def periodic_box(n, steps_hint=None):
+    """The single periodic patch workload of n^3 cells on the unit cube:
+    returns (U0, h, dt)."""
+    h = 1.0 / n
+    U = vortex_pulse(n, n, n)
+    dt = cfl_dt(U, h, 0.5)
+    return U, h, dt

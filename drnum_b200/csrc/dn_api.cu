@@ -1,0 +1,675 @@
+// C ABI of drnum_b200 (declared in include/drnum_b200.h): contexts, patches,
+// host <-> device transfers, RK stepping and FP64 reductions.
+//
+// A context owns, per patch, three physical field buffers and an optional
+// active mask.  Logical fields 0/1/2 (current state / step-start state /
+// scratch, as in the reference applications) map onto the physical buffers
+// through a permutation, so an RK step never copies a field: stage s reads
+// the previous stage's output (or the step-start state) and writes the other
+// buffer, and the step-start state stays untouched as field 1
+// (rungekutta.cpp:27-42 copies field 0 into field 1 instead).
+#include "drnum_b200.h"
+#include "fv_launch.h"
+
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+namespace {
+
+struct DnPatch {
+  dn_patch_desc d;
+  size_t nc = 0;
+  void* buf[3] = {nullptr, nullptr, nullptr};
+  uint8_t* active = nullptr;
+  double base[5] = {0, 0, 0, 0, 0};
+  double quantum[5] = {1, 1, 1, 1, 1};
+  bool base_set = false;
+};
+
+} // namespace
+
+struct dn_ctx {
+  int device = 0;
+  int precision = DN_FP64;
+  int num_sms = 148;
+  cudaStream_t own = nullptr;
+  cudaStream_t stream = nullptr;
+  std::vector<DnPatch> patches;
+  int fmap[3] = {0, 1, 2};
+  std::string err;
+  int* d_err = nullptr;
+  void* staging = nullptr;
+  size_t staging_bytes = 0;
+  double* d_partials = nullptr;
+  size_t partials_cap = 0;
+  int64_t launches = 0;
+};
+
+namespace {
+
+constexpr int kSumThreads = 256;
+constexpr int kSumBlocks = 1184;   // 8 per SM on 148 SMs; fixed => deterministic order
+
+int fail(dn_ctx* c, int code, const char* fmt, ...)
+{
+  if (c) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    c->err = buf;
+  }
+  return code;
+}
+
+int cuda_fail(dn_ctx* c, cudaError_t e, const char* what)
+{
+  return fail(c, DN_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e));
+}
+
+size_t elem_size(const dn_ctx* c) { return c->precision == DN_FP64 ? sizeof(double) : sizeof(float); }
+
+int set_device(dn_ctx* c)
+{
+  cudaError_t e = cudaSetDevice(c->device);
+  return e == cudaSuccess ? DN_OK : cuda_fail(c, e, "cudaSetDevice");
+}
+
+int ensure_staging(dn_ctx* c, size_t bytes)
+{
+  if (c->staging_bytes >= bytes) return DN_OK;
+  if (c->staging) cudaFree(c->staging);
+  c->staging = nullptr;
+  c->staging_bytes = 0;
+  cudaError_t e = cudaMalloc(&c->staging, bytes);
+  if (e != cudaSuccess) return cuda_fail(c, e, "cudaMalloc(staging)");
+  c->staging_bytes = bytes;
+  return DN_OK;
+}
+
+int check_patch(dn_ctx* c, int id)
+{
+  if (!c) return DN_ERR_ARG;
+  if (id < 0 || id >= (int)c->patches.size()) return fail(c, DN_ERR_ARG, "invalid patch id %d", id);
+  return DN_OK;
+}
+
+int check_field(dn_ctx* c, int f)
+{
+  if (f < 0 || f > 2) return fail(c, DN_ERR_ARG, "invalid field %d (0..2)", f);
+  return DN_OK;
+}
+
+// ---------------------------------------------------------------- kernels
+
+struct QParams {
+  double base[5];
+  double inv_q[5];
+  double q[5];
+};
+
+template <typename Src>
+__global__ void k_quantize(const Src* __restrict__ src, float* __restrict__ dst, size_t nc, QParams qp, int* err)
+{
+  const size_t n = 5 * nc;
+  for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < n; e += (size_t)gridDim.x * blockDim.x) {
+    const int v = (int)(e / nc);
+    const double o = rint(((double)src[e] - qp.base[v]) * qp.inv_q[v]);
+    if (!(fabs(o) < 16777216.0)) atomicOr(err, 2);
+    dst[e] = (float)o;
+  }
+}
+
+template <typename Dst>
+__global__ void k_dequantize(const float* __restrict__ src, Dst* __restrict__ dst, size_t nc, QParams qp)
+{
+  const size_t n = 5 * nc;
+  for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < n; e += (size_t)gridDim.x * blockDim.x) {
+    const int v = (int)(e / nc);
+    dst[e] = (Dst)(qp.base[v] + qp.q[v] * (double)src[e]);
+  }
+}
+
+template <typename Src, typename Dst>
+__global__ void k_convert(const Src* __restrict__ src, Dst* __restrict__ dst, size_t n)
+{
+  for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < n; e += (size_t)gridDim.x * blockDim.x)
+    dst[e] = (Dst)src[e];
+}
+
+// Per-block FP64 partial sums of the five variables over one field; each
+// block covers a fixed contiguous range and reduces it in a fixed tree order,
+// so the result does not depend on scheduling.
+template <typename T>
+__global__ void __launch_bounds__(kSumThreads)
+k_partial_sums(const T* __restrict__ f, size_t nc, double* __restrict__ partials)
+{
+  __shared__ double red[5][kSumThreads];
+  const size_t per = (nc + gridDim.x - 1) / gridDim.x;
+  const size_t c0 = blockIdx.x * per;
+  const size_t c1 = c0 + per < nc ? c0 + per : nc;
+  double acc[5] = {0, 0, 0, 0, 0};
+  for (size_t c = c0 + threadIdx.x; c < c1; c += blockDim.x) {
+    #pragma unroll
+    for (int v = 0; v < 5; ++v) acc[v] += (double)f[v * nc + c];
+  }
+  #pragma unroll
+  for (int v = 0; v < 5; ++v) red[v][threadIdx.x] = acc[v];
+  __syncthreads();
+  for (int s = kSumThreads / 2; s > 0; s >>= 1) {
+    if ((int)threadIdx.x < s) {
+      #pragma unroll
+      for (int v = 0; v < 5; ++v) red[v][threadIdx.x] += red[v][threadIdx.x + s];
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x < 5) partials[blockIdx.x * 5 + threadIdx.x] = red[threadIdx.x][0];
+}
+
+// max and sum of squared differences of two variables (Patch::computeVariableDifference)
+template <typename T>
+__global__ void __launch_bounds__(kSumThreads)
+k_diff(const T* __restrict__ a, const T* __restrict__ b, size_t nc, QParams qa, int va, QParams qb, int vb,
+       int quantized, double* __restrict__ partials)
+{
+  __shared__ double smax[kSumThreads];
+  __shared__ double ssum[kSumThreads];
+  const size_t per = (nc + gridDim.x - 1) / gridDim.x;
+  const size_t c0 = blockIdx.x * per;
+  const size_t c1 = c0 + per < nc ? c0 + per : nc;
+  double mx = 0, sm = 0;
+  for (size_t c = c0 + threadIdx.x; c < c1; c += blockDim.x) {
+    double x = (double)a[c], y = (double)b[c];
+    if (quantized) {
+      x = qa.base[va] + qa.q[va] * x;
+      y = qb.base[vb] + qb.q[vb] * y;
+    }
+    const double d = (y - x) * (y - x);
+    mx = d > mx ? d : mx;
+    sm += d;
+  }
+  smax[threadIdx.x] = mx;
+  ssum[threadIdx.x] = sm;
+  __syncthreads();
+  for (int s = kSumThreads / 2; s > 0; s >>= 1) {
+    if ((int)threadIdx.x < s) {
+      smax[threadIdx.x] = smax[threadIdx.x] > smax[threadIdx.x + s] ? smax[threadIdx.x] : smax[threadIdx.x + s];
+      ssum[threadIdx.x] += ssum[threadIdx.x + s];
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    partials[blockIdx.x * 2] = smax[0];
+    partials[blockIdx.x * 2 + 1] = ssum[0];
+  }
+}
+
+int grid_for(size_t n)
+{
+  size_t g = (n + 255) / 256;
+  if (g > 148 * 16) g = 148 * 16;
+  if (g < 1) g = 1;
+  return (int)g;
+}
+
+QParams qparams(const DnPatch& p)
+{
+  QParams q;
+  for (int v = 0; v < 5; ++v) {
+    q.base[v] = p.base[v];
+    q.q[v] = p.quantum[v];
+    q.inv_q[v] = 1.0 / p.quantum[v];
+  }
+  return q;
+}
+
+int ensure_partials(dn_ctx* c, size_t n)
+{
+  if (c->partials_cap >= n) return DN_OK;
+  if (c->d_partials) cudaFree(c->d_partials);
+  c->d_partials = nullptr;
+  c->partials_cap = 0;
+  cudaError_t e = cudaMalloc(&c->d_partials, n * sizeof(double));
+  if (e != cudaSuccess) return cuda_fail(c, e, "cudaMalloc(partials)");
+  c->partials_cap = n;
+  return DN_OK;
+}
+
+int read_device_error(dn_ctx* c)
+{
+  int h = 0;
+  cudaError_t e = cudaMemcpyAsync(&h, c->d_err, sizeof(int), cudaMemcpyDeviceToHost, c->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+  if (e != cudaSuccess) return cuda_fail(c, e, "device error word");
+  if (h != 0) {
+    cudaMemsetAsync(c->d_err, 0, sizeof(int), c->stream);
+    if (h & 1) return fail(c, DN_ERR_RANGE, "FP32 offset left its exact range (|o| >= 2^24) during a stage");
+    if (h & 2) return fail(c, DN_ERR_RANGE, "uploaded state outside the FP32 offset range of the patch base/quantum");
+    return fail(c, DN_ERR_DEVICE, "device error word 0x%x", h);
+  }
+  return DN_OK;
+}
+
+// Derives base and quantum from a host state: base = mean per variable;
+// quantum = 2^ceil(log2(M_v / 2^24)) with M_v the magnitude scale of the
+// variable (max |rho|, max rho*(|u|+a) for all three momenta, max |rho E|),
+// so that offsets of up to M_v stay exact and the resolution equals the FP32
+// spacing at M_v.
+template <typename T>
+void derive_base(DnPatch& p, const T* h)
+{
+  const size_t nc = p.nc;
+  double sum[5] = {0, 0, 0, 0, 0};
+  double mr = 0, mm = 0, me = 0;
+  for (size_t c = 0; c < nc; ++c) {
+    const double r = h[c], ru = h[nc + c], rv = h[2 * nc + c], rw = h[3 * nc + c], rE = h[4 * nc + c];
+    sum[0] += r; sum[1] += ru; sum[2] += rv; sum[3] += rw; sum[4] += rE;
+    const double ar = std::fabs(r);
+    mr = ar > mr ? ar : mr;
+    me = std::fabs(rE) > me ? std::fabs(rE) : me;
+    if (r > 0) {
+      const double u = ru / r, v = rv / r, w = rw / r;
+      const double q2 = u * u + v * v + w * w;
+      const double T_ = (rE / r - 0.5 * q2) / 717.5;
+      const double a = T_ > 0 ? std::sqrt(1.4 * 287.2 * T_) : 0.0;
+      const double m = r * (std::sqrt(q2) + a);
+      mm = m > mm ? m : mm;
+    }
+  }
+  const double M[5] = {mr, mm, mm, mm, me};
+  for (int v = 0; v < 5; ++v) {
+    p.base[v] = sum[v] / (double)nc;
+    double Mv = M[v] > 0 ? M[v] : 1.0;
+    p.quantum[v] = std::ldexp(1.0, (int)std::ceil(std::log2(Mv / 16777216.0)));
+  }
+  p.base_set = true;
+}
+
+int stage_patch(dn_ctx* c, DnPatch& p, int in_b, int un_b, int out_b, double factor)
+{
+  const double dx = p.d.dx, dy = p.d.dy, dz = p.d.dz;
+  const double dV = dx * dy * dz;
+  const double pf = factor / dV;
+  dn::StageGeom g;
+  g.ni = p.d.ni; g.nj = p.d.nj; g.nk = p.d.nk;
+  g.per_x = p.d.face[0] == DN_FACE_PERIODIC;
+  g.per_y = p.d.face[1] == DN_FACE_PERIODIC;
+  g.per_z = p.d.face[2] == DN_FACE_PERIODIC;
+  cudaError_t e;
+  dn::StageShape shape{0, 0, 0};
+  if (c->precision == DN_FP64) {
+    dn::StageArgs<dn::PolicyF64> a;
+    a.in = (const double*)p.buf[in_b];
+    a.un = (const double*)p.buf[un_b];
+    a.out = (double*)p.buf[out_b];
+    a.active = p.active;
+    a.err = c->d_err;
+    g.i_chunk = dn::default_i_chunk(g.ni, g.nj, g.nk, 4, 32, c->num_sms, 3);
+    a.g = g;
+    a.p.Ax = dy * dz; a.p.Ay = dx * dz; a.p.Az = dx * dy; a.p.pf = pf;
+    e = dn::launch_stage_f64(a, shape, c->stream);
+  } else {
+    dn::StageArgs<dn::PolicyF32Q> a;
+    a.in = (const float*)p.buf[in_b];
+    a.un = (const float*)p.buf[un_b];
+    a.out = (float*)p.buf[out_b];
+    a.active = p.active;
+    a.err = c->d_err;
+    g.i_chunk = dn::default_i_chunk(g.ni, g.nj, g.nk, 8, 32, c->num_sms, 4);
+    a.g = g;
+    a.p.Ax = (float)(dy * dz); a.p.Ay = (float)(dx * dz); a.p.Az = (float)(dx * dy);
+    for (int v = 0; v < 5; ++v) {
+      a.p.base[v] = (float)p.base[v];
+      a.p.quantum[v] = (float)p.quantum[v];
+      a.p.face_scale[v] = (float)(pf / p.quantum[v]);
+    }
+    e = dn::launch_stage_f32q(a, shape, c->stream);
+  }
+  c->launches++;
+  if (e != cudaSuccess) return cuda_fail(c, e, "stage kernel launch");
+  return DN_OK;
+}
+
+template <typename H>
+int upload_impl(dn_ctx* c, int id, int field, const H* host)
+{
+  int s = check_patch(c, id);
+  if (s) return s;
+  if ((s = check_field(c, field))) return s;
+  if (!host) return fail(c, DN_ERR_ARG, "host pointer is NULL");
+  if (set_device(c) != DN_OK) return DN_ERR_CUDA;
+  DnPatch& p = c->patches[id];
+  void* dst = p.buf[c->fmap[field]];
+  const size_t n = 5 * p.nc;
+  cudaError_t e;
+  if (c->precision == DN_FP64 && sizeof(H) == sizeof(double)) {
+    e = cudaMemcpyAsync(dst, host, n * sizeof(double), cudaMemcpyHostToDevice, c->stream);
+    if (e != cudaSuccess) return cuda_fail(c, e, "upload copy");
+    return DN_OK;
+  }
+  if (c->precision == DN_FP32 && !p.base_set) derive_base(p, host);
+  if ((s = ensure_staging(c, n * sizeof(H)))) return s;
+  e = cudaMemcpyAsync(c->staging, host, n * sizeof(H), cudaMemcpyHostToDevice, c->stream);
+  if (e != cudaSuccess) return cuda_fail(c, e, "upload copy");
+  if (c->precision == DN_FP64) {
+    k_convert<H, double><<<grid_for(n), 256, 0, c->stream>>>((const H*)c->staging, (double*)dst, n);
+  } else {
+    k_quantize<H><<<grid_for(n), 256, 0, c->stream>>>((const H*)c->staging, (float*)dst, p.nc, qparams(p), c->d_err);
+  }
+  c->launches++;
+  e = cudaGetLastError();
+  if (e != cudaSuccess) return cuda_fail(c, e, "upload conversion");
+  if (c->precision == DN_FP32) return read_device_error(c);
+  return DN_OK;
+}
+
+template <typename H>
+int download_impl(dn_ctx* c, int id, int field, H* host)
+{
+  int s = check_patch(c, id);
+  if (s) return s;
+  if ((s = check_field(c, field))) return s;
+  if (!host) return fail(c, DN_ERR_ARG, "host pointer is NULL");
+  if (set_device(c) != DN_OK) return DN_ERR_CUDA;
+  DnPatch& p = c->patches[id];
+  const void* src = p.buf[c->fmap[field]];
+  const size_t n = 5 * p.nc;
+  cudaError_t e;
+  if (c->precision == DN_FP64 && sizeof(H) == sizeof(double)) {
+    e = cudaMemcpyAsync(host, src, n * sizeof(double), cudaMemcpyDeviceToHost, c->stream);
+  } else {
+    if ((s = ensure_staging(c, n * sizeof(H)))) return s;
+    if (c->precision == DN_FP64) {
+      k_convert<double, H><<<grid_for(n), 256, 0, c->stream>>>((const double*)src, (H*)c->staging, n);
+    } else {
+      k_dequantize<H><<<grid_for(n), 256, 0, c->stream>>>((const float*)src, (H*)c->staging, p.nc, qparams(p));
+    }
+    c->launches++;
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return cuda_fail(c, e, "download conversion");
+    e = cudaMemcpyAsync(host, c->staging, n * sizeof(H), cudaMemcpyDeviceToHost, c->stream);
+  }
+  if (e != cudaSuccess) return cuda_fail(c, e, "download copy");
+  e = cudaStreamSynchronize(c->stream);
+  if (e != cudaSuccess) return cuda_fail(c, e, "download sync");
+  return read_device_error(c);
+}
+
+} // namespace
+
+extern "C" {
+
+int dn_ctx_create(int device, int precision, dn_ctx** out)
+{
+  if (!out) return DN_ERR_ARG;
+  *out = nullptr;
+  if (precision != DN_FP64 && precision != DN_FP32) return DN_ERR_ARG;
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess || device < 0 || device >= n) return DN_ERR_CUDA;
+  dn_ctx* c = new dn_ctx();
+  c->device = device;
+  c->precision = precision;
+  if (set_device(c) != DN_OK) { delete c; return DN_ERR_CUDA; }
+  cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, device);
+  if (cudaStreamCreateWithFlags(&c->own, cudaStreamNonBlocking) != cudaSuccess) { delete c; return DN_ERR_CUDA; }
+  c->stream = c->own;
+  if (cudaMalloc(&c->d_err, sizeof(int)) != cudaSuccess) { cudaStreamDestroy(c->own); delete c; return DN_ERR_NOMEM; }
+  cudaMemsetAsync(c->d_err, 0, sizeof(int), c->stream);
+  *out = c;
+  return DN_OK;
+}
+
+int dn_ctx_destroy(dn_ctx* c)
+{
+  if (!c) return DN_OK;
+  cudaSetDevice(c->device);
+  cudaStreamSynchronize(c->stream);
+  for (auto& p : c->patches) {
+    for (int b = 0; b < 3; ++b) if (p.buf[b]) cudaFree(p.buf[b]);
+    if (p.active) cudaFree(p.active);
+  }
+  if (c->staging) cudaFree(c->staging);
+  if (c->d_partials) cudaFree(c->d_partials);
+  if (c->d_err) cudaFree(c->d_err);
+  if (c->own) cudaStreamDestroy(c->own);
+  delete c;
+  return DN_OK;
+}
+
+int dn_last_error(const dn_ctx* c, char* buf, size_t n)
+{
+  if (!c || !buf || n == 0) return DN_ERR_ARG;
+  std::strncpy(buf, c->err.c_str(), n - 1);
+  buf[n - 1] = 0;
+  return DN_OK;
+}
+
+int dn_set_stream(dn_ctx* c, void* stream)
+{
+  if (!c) return DN_ERR_ARG;
+  c->stream = stream ? (cudaStream_t)stream : c->own;
+  return DN_OK;
+}
+
+int dn_patch_add(dn_ctx* c, const dn_patch_desc* d, int* id)
+{
+  if (!c || !d || !id) return DN_ERR_ARG;
+  if (d->ni < 1 || d->nj < 1 || d->nk < 1) return fail(c, DN_ERR_ARG, "patch size must be positive");
+  for (int a = 0; a < 3; ++a) {
+    if (d->face[a] != DN_FACE_PERIODIC && d->face[a] != DN_FACE_CLOSED)
+      return fail(c, DN_ERR_ARG, "face kind of axis %d is not DN_FACE_PERIODIC or DN_FACE_CLOSED", a);
+    const int n = a == 0 ? d->ni : (a == 1 ? d->nj : d->nk);
+    if (d->face[a] == DN_FACE_PERIODIC && n < 3)
+      return fail(c, DN_ERR_ARG, "periodic axis %d needs at least 3 cells", a);
+  }
+  if (!(d->dx > 0) || !(d->dy > 0) || !(d->dz > 0)) return fail(c, DN_ERR_ARG, "cell spacing must be positive");
+  const size_t nc = (size_t)d->ni * d->nj * d->nk;
+  if (nc > ((size_t)1 << 40)) return fail(c, DN_ERR_ARG, "patch too large");
+  if (set_device(c) != DN_OK) return DN_ERR_CUDA;
+  DnPatch p;
+  p.d = *d;
+  p.nc = nc;
+  const size_t bytes = 5 * nc * elem_size(c);
+  for (int b = 0; b < 3; ++b) {
+    cudaError_t e = cudaMalloc(&p.buf[b], bytes);
+    if (e != cudaSuccess) {
+      for (int q = 0; q < b; ++q) cudaFree(p.buf[q]);
+      return fail(c, DN_ERR_NOMEM, "cudaMalloc of %zu bytes for a patch field failed", bytes);
+    }
+    cudaMemsetAsync(p.buf[b], 0, bytes, c->stream);
+  }
+  c->patches.push_back(p);
+  *id = (int)c->patches.size() - 1;
+  return DN_OK;
+}
+
+int dn_patch_set_base(dn_ctx* c, int id, const double base[5], const double range[5])
+{
+  int s = check_patch(c, id);
+  if (s) return s;
+  if (!base || !range) return fail(c, DN_ERR_ARG, "base and range are required");
+  DnPatch& p = c->patches[id];
+  for (int v = 0; v < 5; ++v) {
+    if (!std::isfinite(base[v]) || !(range[v] > 0) || !std::isfinite(range[v]))
+      return fail(c, DN_ERR_ARG, "base/range of variable %d invalid", v);
+  }
+  for (int v = 0; v < 5; ++v) {
+    p.base[v] = base[v];
+    p.quantum[v] = std::ldexp(1.0, (int)std::ceil(std::log2(range[v] / 16777216.0)));
+  }
+  p.base_set = true;
+  return DN_OK;
+}
+
+int dn_patch_upload(dn_ctx* c, int id, int field, const double* host) { return upload_impl(c, id, field, host); }
+int dn_patch_upload_f32(dn_ctx* c, int id, int field, const float* host) { return upload_impl(c, id, field, host); }
+int dn_patch_download(dn_ctx* c, int id, int field, double* host) { return download_impl(c, id, field, host); }
+int dn_patch_download_f32(dn_ctx* c, int id, int field, float* host) { return download_impl(c, id, field, host); }
+
+int dn_patch_set_active(dn_ctx* c, int id, const uint8_t* mask)
+{
+  int s = check_patch(c, id);
+  if (s) return s;
+  if (set_device(c) != DN_OK) return DN_ERR_CUDA;
+  DnPatch& p = c->patches[id];
+  if (!mask) {
+    if (p.active) {
+      cudaStreamSynchronize(c->stream);
+      cudaFree(p.active);
+    }
+    p.active = nullptr;
+    return DN_OK;
+  }
+  cudaError_t e;
+  if (!p.active) {
+    e = cudaMalloc(&p.active, p.nc);
+    if (e != cudaSuccess) return fail(c, DN_ERR_NOMEM, "cudaMalloc(active mask)");
+  }
+  e = cudaMemcpyAsync(p.active, mask, p.nc, cudaMemcpyHostToDevice, c->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+  if (e != cudaSuccess) return cuda_fail(c, e, "active mask upload");
+  return DN_OK;
+}
+
+int dn_copy_field(dn_ctx* c, int i_src, int i_dst)
+{
+  if (!c) return DN_ERR_ARG;
+  int s;
+  if ((s = check_field(c, i_src)) || (s = check_field(c, i_dst))) return s;
+  if (i_src == i_dst) return DN_OK;
+  if (set_device(c) != DN_OK) return DN_ERR_CUDA;
+  for (auto& p : c->patches) {
+    cudaError_t e = cudaMemcpyAsync(p.buf[c->fmap[i_dst]], p.buf[c->fmap[i_src]], 5 * p.nc * elem_size(c),
+                                    cudaMemcpyDeviceToDevice, c->stream);
+    if (e != cudaSuccess) return cuda_fail(c, e, "copyField");
+  }
+  return DN_OK;
+}
+
+int dn_compute(dn_ctx* c, double factor)
+{
+  if (!c) return DN_ERR_ARG;
+  if (!std::isfinite(factor)) return fail(c, DN_ERR_ARG, "factor is not finite");
+  if (set_device(c) != DN_OK) return DN_ERR_CUDA;
+  for (auto& p : c->patches) {
+    int s = stage_patch(c, p, c->fmap[0], c->fmap[1], c->fmap[2], factor);
+    if (s) return s;
+  }
+  std::swap(c->fmap[0], c->fmap[2]);
+  return DN_OK;
+}
+
+int dn_rk_step(dn_ctx* c, double dt, const double* alpha, int n_alpha)
+{
+  if (!c) return DN_ERR_ARG;
+  if (!alpha || n_alpha < 1 || n_alpha > 16) return fail(c, DN_ERR_ARG, "need 1..16 RK stage coefficients");
+  if (!std::isfinite(dt)) return fail(c, DN_ERR_ARG, "dt is not finite");
+  if (set_device(c) != DN_OK) return DN_ERR_CUDA;
+  // A = step-start state, X/Y = the two other buffers
+  const int A = c->fmap[0], X = c->fmap[2], Y = c->fmap[1];
+  int in = A;
+  for (int s = 0; s < n_alpha; ++s) {
+    const int out = (s & 1) ? Y : X;
+    const double factor = alpha[s] * dt;   // (*i)*dt, rungekutta.cpp:37
+    for (auto& p : c->patches) {
+      int st = stage_patch(c, p, in, A, out, factor);
+      if (st) return st;
+    }
+    in = out;
+  }
+  c->fmap[0] = in;
+  c->fmap[1] = A;
+  c->fmap[2] = (in == X) ? Y : X;
+  return DN_OK;
+}
+
+int dn_sync(dn_ctx* c)
+{
+  if (!c) return DN_ERR_ARG;
+  if (set_device(c) != DN_OK) return DN_ERR_CUDA;
+  cudaError_t e = cudaStreamSynchronize(c->stream);
+  if (e != cudaSuccess) return cuda_fail(c, e, "stream synchronize");
+  return read_device_error(c);
+}
+
+int dn_conservation_sums(dn_ctx* c, double out[5])
+{
+  if (!c || !out) return DN_ERR_ARG;
+  if (set_device(c) != DN_OK) return DN_ERR_CUDA;
+  int s;
+  if ((s = ensure_partials(c, (size_t)kSumBlocks * 5))) return s;
+  std::vector<double> h((size_t)kSumBlocks * 5);
+  double tot[5] = {0, 0, 0, 0, 0};
+  for (auto& p : c->patches) {
+    const void* f = p.buf[c->fmap[0]];
+    if (c->precision == DN_FP64)
+      k_partial_sums<double><<<kSumBlocks, kSumThreads, 0, c->stream>>>((const double*)f, p.nc, c->d_partials);
+    else
+      k_partial_sums<float><<<kSumBlocks, kSumThreads, 0, c->stream>>>((const float*)f, p.nc, c->d_partials);
+    c->launches++;
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaMemcpyAsync(h.data(), c->d_partials, h.size() * sizeof(double), cudaMemcpyDeviceToHost, c->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    if (e != cudaSuccess) return cuda_fail(c, e, "conservation sums");
+    double ps[5] = {0, 0, 0, 0, 0};
+    for (int b = 0; b < kSumBlocks; ++b)
+      for (int v = 0; v < 5; ++v) ps[v] += h[(size_t)b * 5 + v];
+    const double dV = p.d.dx * p.d.dy * p.d.dz;
+    for (int v = 0; v < 5; ++v) {
+      double pv = c->precision == DN_FP64 ? ps[v] : ((double)p.nc * p.base[v] + p.quantum[v] * ps[v]);
+      tot[v] += pv * dV;
+    }
+  }
+  for (int v = 0; v < 5; ++v) out[v] = tot[v];
+  return read_device_error(c);
+}
+
+int dn_field_difference(dn_ctx* c, int id, int f1, int v1, int f2, int v2, double* max_norm, double* l2_norm)
+{
+  int s = check_patch(c, id);
+  if (s) return s;
+  if ((s = check_field(c, f1)) || (s = check_field(c, f2))) return s;
+  if (v1 < 0 || v1 > 4 || v2 < 0 || v2 > 4) return fail(c, DN_ERR_ARG, "variable index out of range");
+  if (!max_norm || !l2_norm) return DN_ERR_ARG;
+  if (set_device(c) != DN_OK) return DN_ERR_CUDA;
+  if ((s = ensure_partials(c, (size_t)kSumBlocks * 2))) return s;
+  DnPatch& p = c->patches[id];
+  QParams q = qparams(p);
+  if (c->precision == DN_FP64) {
+    const double* a = (const double*)p.buf[c->fmap[f1]] + (size_t)v1 * p.nc;
+    const double* b = (const double*)p.buf[c->fmap[f2]] + (size_t)v2 * p.nc;
+    k_diff<double><<<kSumBlocks, kSumThreads, 0, c->stream>>>(a, b, p.nc, q, v1, q, v2, 0, c->d_partials);
+  } else {
+    const float* a = (const float*)p.buf[c->fmap[f1]] + (size_t)v1 * p.nc;
+    const float* b = (const float*)p.buf[c->fmap[f2]] + (size_t)v2 * p.nc;
+    k_diff<float><<<kSumBlocks, kSumThreads, 0, c->stream>>>(a, b, p.nc, q, v1, q, v2, 1, c->d_partials);
+  }
+  c->launches++;
+  std::vector<double> h((size_t)kSumBlocks * 2);
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess) e = cudaMemcpyAsync(h.data(), c->d_partials, h.size() * sizeof(double), cudaMemcpyDeviceToHost, c->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+  if (e != cudaSuccess) return cuda_fail(c, e, "field difference");
+  double mx = 0, sm = 0;
+  for (int b = 0; b < kSumBlocks; ++b) {
+    mx = h[(size_t)b * 2] > mx ? h[(size_t)b * 2] : mx;
+    sm += h[(size_t)b * 2 + 1];
+  }
+  *max_norm = std::sqrt(mx);
+  *l2_norm = std::sqrt(sm);
+  return DN_OK;
+}
+
+int dn_launch_count(const dn_ctx* c, int64_t* count)
+{
+  if (!c || !count) return DN_ERR_ARG;
+  *count = c->launches;
+  return DN_OK;
+}
+
+} // extern "C"

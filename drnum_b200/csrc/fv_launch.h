@@ -1,0 +1,23 @@
+// Host-side launchers of the fused stage kernels (one translation unit per
+// arithmetic form so each gets its own floating-point compile flags).
+#pragma once
+
+#include <cuda_runtime.h>
+#include "fv_policies.cuh"
+#include "fv_stage.cuh"
+
+namespace dn {
+
+// Tile and chunk shape of one launch.
+struct StageShape {
+  int tj, tk;      // CTA tile in j and k (threads = tj*tk)
+  int i_chunk;     // planes per CTA along i
+};
+
+cudaError_t launch_stage_f64(const StageArgs<PolicyF64>& a, const StageShape& s, cudaStream_t st);
+cudaError_t launch_stage_f32q(const StageArgs<PolicyF32Q>& a, const StageShape& s, cudaStream_t st);
+
+// Chooses the i-chunk so that the grid holds enough CTAs to fill the GPU.
+int default_i_chunk(int ni, int nj, int nk, int tj, int tk, int num_sms, int ctas_per_sm);
+
+} // namespace dn

@@ -1,0 +1,283 @@
+// Fused RK-stage kernel for one Cartesian patch: residual (all x, y and z
+// face fluxes) and update f_out = f_n + factor/dV * Res(f_in) in one launch.
+//
+// Replaces the reference's per-stage sequence of a residual memset plus ten
+// launches (six colour-split flux kernels, three boundary kernels, advance;
+// iterators/gpu_cartesianiterator.h:54-304) that read-modify-write a residual
+// field in HBM.  Here:
+//   - a CTA owns a TJ x TK tile of (j, k) columns (k fastest, coalesced) and
+//     marches along i through a chunk of planes;
+//   - each plane of the stencil state is staged once in shared memory with a
+//     two-cell halo in j and k (a ring of four planes covers i-1 .. i+2);
+//   - every face flux is evaluated exactly once: x faces per thread along its
+//     own column (the upper face of cell i is kept in registers as the lower
+//     face of cell i+1), y and z faces of the current plane into shared
+//     memory;
+//   - the residual is summed per cell in registers in the reference's order
+//     (+Fx_lo +Fy_lo +Fz_lo -Fz_hi -Fy_hi -Fx_hi, the order the single-thread
+//     CPU iterator produces, cartesianiterator.h:115-188), no atomics;
+//   - the update is written once; inactive cells copy their input
+//     (cartesianiterator.h:315, gpu_cartesianiterator.h:199-201).
+//
+// The storage/arithmetic form is a policy:
+//   Policy::Store   element type in HBM
+//   Policy::Real    arithmetic type
+//   Policy::load(v, x)           stored value -> arithmetic value
+//   Policy::face(v, F)           face flux -> value summed into the residual
+//   Policy::update(v, un, r)     new stored value from stored f_n and residual
+#pragma once
+
+#include <cstdint>
+#include "fv_numerics.cuh"
+
+namespace dn {
+
+struct StageGeom {
+  int ni, nj, nk;
+  int per_x, per_y, per_z;   // 1 = periodic wrap, 0 = closed
+  int i_chunk;               // planes per CTA along i
+};
+
+template <class Policy>
+struct StageArgs {
+  const typename Policy::Store* in;   // stencil state f(k-1), [5][ni][nj][nk]
+  const typename Policy::Store* un;   // step-start state f(n), own cell only
+  typename Policy::Store* out;        // f(k)
+  const uint8_t* active;              // per cell, NULL = all active
+  int* err;                           // device error word (bit flags)
+  StageGeom g;
+  typename Policy::Params p;
+};
+
+// index along an axis with periodic wrap; returns -1 if outside a closed axis
+__device__ __forceinline__ int axis_idx(int x, int n, int per)
+{
+  if (per) {
+    x %= n;
+    return x < 0 ? x + n : x;
+  }
+  return (x < 0 || x >= n) ? -1 : x;
+}
+
+// does the face below cell index x (between x-1 and x) exist?
+__device__ __forceinline__ bool face_exists(int x, int n, int per)
+{
+  if (n <= 2) return false;               // cartesianiterator.h:149,160,171
+  return per ? true : (x >= 1 && x <= n - 1);
+}
+
+// is cell index x inside the axis (or wrapped)?
+__device__ __forceinline__ bool cell_ok(int x, int n, int per)
+{
+  return per ? true : (x >= 0 && x < n);
+}
+
+template <class Policy, int TJ, int TK>
+struct StageSmem {
+  using Real = typename Policy::Real;
+  using FaceT = typename Policy::FaceT;
+  static constexpr int PJ = TJ + 4;
+  static constexpr int PK = TK + 4;
+  Real plane[4][5][PJ][PK];
+  FaceT fy[5][TJ + 1][TK];
+  FaceT fz[5][TJ][TK + 1];
+};
+
+template <class Policy, int TJ, int TK>
+__device__ __forceinline__ void load_plane(StageSmem<Policy, TJ, TK>& sm, int slot,
+                                           const typename Policy::Store* __restrict__ in,
+                                           const typename Policy::Params& pp,
+                                           const StageGeom& g, int ip, int j0, int k0)
+{
+  using Real = typename Policy::Real;
+  constexpr int PJ = TJ + 4, PK = TK + 4;
+  const int i = axis_idx(ip, g.ni, g.per_x);
+  if (i < 0) return;                      // plane outside a closed patch: never read
+  const size_t nc = (size_t)g.ni * g.nj * g.nk;
+  const int tid = threadIdx.y * TK + threadIdx.x;
+  for (int e = tid; e < 5 * PJ * PK; e += TJ * TK) {
+    const int v = e / (PJ * PK);
+    const int rem = e - v * (PJ * PK);
+    const int jj = rem / PK;
+    const int kk = rem - jj * PK;
+    const int j = axis_idx(j0 - 2 + jj, g.nj, g.per_y);
+    const int k = axis_idx(k0 - 2 + kk, g.nk, g.per_z);
+    Real val = Real(0);
+    if (j >= 0 && k >= 0) {
+      val = Policy::load(pp, v, in[v * nc + ((size_t)i * g.nj + j) * g.nk + k]);
+    }
+    sm.plane[slot][v][jj][kk] = val;
+  }
+}
+
+template <class Policy, int TJ, int TK>
+__global__ void __launch_bounds__(TJ * TK)
+fv_stage_kernel(const StageArgs<Policy> a)
+{
+  using Real = typename Policy::Real;
+  using FaceT = typename Policy::FaceT;
+  using Smem = StageSmem<Policy, TJ, TK>;
+  extern __shared__ __align__(16) unsigned char dn_smem_raw[];
+  Smem& sm = *reinterpret_cast<Smem*>(dn_smem_raw);
+
+  const StageGeom& g = a.g;
+  const int tx = threadIdx.x, ty = threadIdx.y;
+  const int k0 = blockIdx.x * TK, j0 = blockIdx.y * TJ;
+  const int i0 = blockIdx.z * g.i_chunk;
+  const int i1 = min(g.ni, i0 + g.i_chunk);
+  const int j = j0 + ty, k = k0 + tx;
+  const bool own = (j < g.nj) && (k < g.nk);
+  const size_t nc = (size_t)g.ni * g.nj * g.nk;
+  const Real Ax = a.p.Ax, Ay = a.p.Ay, Az = a.p.Az;
+
+  // prologue: planes i0-2 .. i0+1 and the x face below cell i0
+  for (int q = -2; q <= 1; ++q) load_plane<Policy, TJ, TK>(sm, (i0 + q + 8) & 3, a.in, a.p, g, i0 + q, j0, k0);
+  __syncthreads();
+
+  FaceT fx_lo[5];
+  {
+    const bool ex = face_exists(i0, g.ni, g.per_x);
+    if (ex && own) {
+      Real vl[5], vr[5], F[5];
+      const bool sl = cell_ok(i0 - 2, g.ni, g.per_x);
+      const bool sr = cell_ok(i0 + 1, g.ni, g.per_x);
+      #pragma unroll
+      for (int v = 0; v < 5; ++v) {
+        const Real um2 = sm.plane[(i0 + 6) & 3][v][ty + 2][tx + 2];
+        const Real um1 = sm.plane[(i0 + 7) & 3][v][ty + 2][tx + 2];
+        const Real up0 = sm.plane[(i0 + 8) & 3][v][ty + 2][tx + 2];
+        const Real up1 = sm.plane[(i0 + 9) & 3][v][ty + 2][tx + 2];
+        vl[v] = upwind2_left(um2, um1, up0, sl);
+        vr[v] = upwind2_right(um1, up0, up1, sr);
+      }
+      ausm_plus<0>(face_side(vl), face_side(vr), Ax, F);
+      #pragma unroll
+      for (int v = 0; v < 5; ++v) fx_lo[v] = Policy::face(a.p, v, F[v]);
+    } else {
+      #pragma unroll
+      for (int v = 0; v < 5; ++v) fx_lo[v] = FaceT(0);
+    }
+  }
+
+  for (int i = i0; i < i1; ++i) {
+    // plane i+2 replaces plane i-2 in the ring
+    __syncthreads();
+    load_plane<Policy, TJ, TK>(sm, (i + 2) & 3, a.in, a.p, g, i + 2, j0, k0);
+    __syncthreads();
+    const int sm1 = (i + 3) & 3, s0 = i & 3, sp1 = (i + 1) & 3, sp2 = (i + 2) & 3;
+
+    // x face above cell i (between i and i+1), own column
+    FaceT fx_hi[5];
+    {
+      const bool ex = face_exists(i + 1, g.ni, g.per_x);
+      if (ex && own) {
+        Real vl[5], vr[5], F[5];
+        const bool sl = cell_ok(i - 1, g.ni, g.per_x);
+        const bool sr = cell_ok(i + 2, g.ni, g.per_x);
+        #pragma unroll
+        for (int v = 0; v < 5; ++v) {
+          const Real um2 = sm.plane[sm1][v][ty + 2][tx + 2];
+          const Real um1 = sm.plane[s0][v][ty + 2][tx + 2];
+          const Real up0 = sm.plane[sp1][v][ty + 2][tx + 2];
+          const Real up1 = sm.plane[sp2][v][ty + 2][tx + 2];
+          vl[v] = upwind2_left(um2, um1, up0, sl);
+          vr[v] = upwind2_right(um1, up0, up1, sr);
+        }
+        ausm_plus<0>(face_side(vl), face_side(vr), Ax, F);
+        #pragma unroll
+        for (int v = 0; v < 5; ++v) fx_hi[v] = Policy::face(a.p, v, F[v]);
+      } else {
+        #pragma unroll
+        for (int v = 0; v < 5; ++v) fx_hi[v] = FaceT(0);
+      }
+    }
+
+    // y faces of plane i: face at row jj (0..TJ) lies below cell j0+jj
+    for (int f = ty * TK + tx; f < (TJ + 1) * TK; f += TJ * TK) {
+      const int jj = f / TK, kk = f - jj * TK;
+      const int jf = j0 + jj, kf = k0 + kk;
+      FaceT out[5];
+      const bool ex = face_exists(jf, g.nj, g.per_y) && kf < g.nk && (g.per_y || jf < g.nj);
+      if (ex) {
+        Real vl[5], vr[5], F[5];
+        const bool sl = cell_ok(jf - 2, g.nj, g.per_y);
+        const bool sr = cell_ok(jf + 1, g.nj, g.per_y);
+        #pragma unroll
+        for (int v = 0; v < 5; ++v) {
+          const Real um2 = sm.plane[s0][v][jj][kk + 2];
+          const Real um1 = sm.plane[s0][v][jj + 1][kk + 2];
+          const Real up0 = sm.plane[s0][v][jj + 2][kk + 2];
+          const Real up1 = sm.plane[s0][v][jj + 3][kk + 2];
+          vl[v] = upwind2_left(um2, um1, up0, sl);
+          vr[v] = upwind2_right(um1, up0, up1, sr);
+        }
+        ausm_plus<1>(face_side(vl), face_side(vr), Ay, F);
+        #pragma unroll
+        for (int v = 0; v < 5; ++v) out[v] = Policy::face(a.p, v, F[v]);
+      } else {
+        #pragma unroll
+        for (int v = 0; v < 5; ++v) out[v] = FaceT(0);
+      }
+      #pragma unroll
+      for (int v = 0; v < 5; ++v) sm.fy[v][jj][kk] = out[v];
+    }
+
+    // z faces of plane i: face at column kk (0..TK) lies below cell k0+kk
+    for (int f = ty * TK + tx; f < TJ * (TK + 1); f += TJ * TK) {
+      const int jj = f / (TK + 1), kk = f - jj * (TK + 1);
+      const int jf = j0 + jj, kf = k0 + kk;
+      FaceT out[5];
+      const bool ex = face_exists(kf, g.nk, g.per_z) && jf < g.nj && (g.per_z || kf < g.nk);
+      if (ex) {
+        Real vl[5], vr[5], F[5];
+        const bool sl = cell_ok(kf - 2, g.nk, g.per_z);
+        const bool sr = cell_ok(kf + 1, g.nk, g.per_z);
+        #pragma unroll
+        for (int v = 0; v < 5; ++v) {
+          const Real um2 = sm.plane[s0][v][jj + 2][kk];
+          const Real um1 = sm.plane[s0][v][jj + 2][kk + 1];
+          const Real up0 = sm.plane[s0][v][jj + 2][kk + 2];
+          const Real up1 = sm.plane[s0][v][jj + 2][kk + 3];
+          vl[v] = upwind2_left(um2, um1, up0, sl);
+          vr[v] = upwind2_right(um1, up0, up1, sr);
+        }
+        ausm_plus<2>(face_side(vl), face_side(vr), Az, F);
+        #pragma unroll
+        for (int v = 0; v < 5; ++v) out[v] = Policy::face(a.p, v, F[v]);
+      } else {
+        #pragma unroll
+        for (int v = 0; v < 5; ++v) out[v] = FaceT(0);
+      }
+      #pragma unroll
+      for (int v = 0; v < 5; ++v) sm.fz[v][jj][kk] = out[v];
+    }
+    __syncthreads();
+
+    if (own) {
+      const size_t c = ((size_t)i * g.nj + j) * g.nk + k;
+      const bool act = a.active ? (a.active[c] != 0) : true;
+      int bad = 0;
+      #pragma unroll
+      for (int v = 0; v < 5; ++v) {
+        FaceT r = fx_lo[v];
+        r += sm.fy[v][ty][tx];
+        r += sm.fz[v][ty][tx];
+        r -= sm.fz[v][ty][tx + 1];
+        r -= sm.fy[v][ty + 1][tx];
+        r -= fx_hi[v];
+        typename Policy::Store o;
+        if (act) {
+          o = Policy::update(a.p, v, a.un[v * nc + c], r, bad);
+        } else {
+          o = a.in[v * nc + c];
+        }
+        a.out[v * nc + c] = o;
+      }
+      if (bad && a.err) atomicOr(a.err, bad);
+    }
+    #pragma unroll
+    for (int v = 0; v < 5; ++v) fx_lo[v] = fx_hi[v];
+  }
+}
+
+} // namespace dn

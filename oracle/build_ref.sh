@@ -1,0 +1,43 @@
+#!/usr/bin/env bash
+# Builds the reference DrNUM library's CPU path (FP64) from its sources where
+# they lie, as the checker for this repository's oracle restatement.
+# Outputs go only to oracle/_ref/ (git-ignored).  Nothing is copied from the
+# reference into the repository; one generated header (drnum.h with the
+# single-precision switch at drnum.h:43 commented out) is written to
+# oracle/_ref/gen/ and found first through gcc's -I- include split.
+#
+# usage: oracle/build_ref.sh [reference-root]      (default /root/reference)
+set -euo pipefail
+HERE="$(cd "$(dirname "${BASH_SOURCE[0]}")" && pwd)"
+REFROOT="${1:-${DRNUM_REFERENCE:-/root/reference}}"
+LIB="$REFROOT/src/drnumlib"
+OUT="$HERE/_ref"
+if [ ! -f "$LIB/drnum.h" ]; then
+  echo "build_ref.sh: reference sources not found under $REFROOT" >&2
+  exit 2
+fi
+mkdir -p "$OUT/gen" "$OUT/obj"
+sed -e 's|^#define DRNUM_SINGLE_PRECISION|/* FP64 oracle build */|' "$LIB/drnum.h" > "$OUT/gen/drnum.h"
+
+SRCS="patch.cpp cartesianpatch.cpp patchgrid.cpp patchgroups.cpp geometrytools.cpp
+      codestring.cpp transformation.cpp math/coordtransform.cpp math/coordtransformvv.cpp
+      rungekutta.cpp timeintegration.cpp debug.cpp blockcfd.cpp cartesianraster.cpp
+      raster.cpp structuredhexraster.cpp levelsetobject.cpp levelsetdefinition.cpp
+      spherelevelset.cpp levelsetobjectbc.cpp"
+CXX="${CXX:-g++}"
+FLAGS="-O2 -std=c++14 -fPIC -fpermissive -w -fopenmp -DOPEN_MP -ffp-contract=off
+       -include $HERE/ref_fp64_shim.h
+       -I$OUT/gen -I$HERE/ref_stubs -I- -I$OUT/gen -I$HERE/ref_stubs -I$LIB -I$LIB/math -I$LIB/iterators
+       -I$LIB/fluxes -I$LIB/reconstruction"
+OBJS=""
+pids=""
+for s in $SRCS; do
+  o="$OUT/obj/$(echo "$s" | tr '/' '_' | sed 's/\.cpp$/.o/')"
+  OBJS="$OBJS $o"
+  $CXX $FLAGS -c "$LIB/$s" -o "$o" &
+  pids="$pids $!"
+done
+for p in $pids; do wait $p; done
+$CXX $FLAGS -c "$HERE/ref_driver.cpp" -o "$OUT/obj/ref_driver.o"
+$CXX -shared -o "$OUT/libdrnum_ref.so" $OBJS "$OUT/obj/ref_driver.o" -L/usr/lib/gcc/x86_64-linux-gnu/13 -lgomp -lpthread
+echo "built $OUT/libdrnum_ref.so"

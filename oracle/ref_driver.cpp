@@ -1,0 +1,261 @@
+// Driver for the compiled reference DrNUM library (FP64), used as the checker
+// that pins this repository's oracle restatement and as the CPU baseline.
+// Test infrastructure only: it links the reference's own sources (built by
+// oracle/build_ref.sh into oracle/_ref/) and exposes a few extern "C" entry
+// points that run the reference code paths on caller-provided inputs.
+//
+// Everything numerical below is done by the reference's own classes:
+//   CartesianPatch / PatchGrid           (cartesianpatch.cpp, patchgrid.cpp, patch.cpp)
+//   CartesianIterator<5, OP>             (iterators/cartesianiterator.h:87-325)
+//   AusmPlus<5, Upwind2<5, VanAlbada>, PerfectGas>  (fluxes/ausmplus.h:39-106)
+//   RungeKutta                           (rungekutta.cpp:27-42)
+// The only pieces written here are harness glue: a periodic ghost-layer copy
+// post-operation (the reference has only a k-axis GPU version,
+// cartesiancycliccopy.h:51-69) and zero patch-face fluxes, because the
+// periodic ghosts overwrite every outer cell anyway.
+
+#include "patchgrid.h"
+#include "cartesianpatch.h"
+#include "rungekutta.h"
+#include "genericoperation.h"
+#include "perfectgas.h"
+#include "fluxes/ausmplus.h"
+#include "reconstruction/upwind2.h"
+#include "reconstruction/vanalbada.h"
+#include "iterators/cartesianiterator.h"
+
+#include <chrono>
+#include <sstream>
+#include <string>
+#include <vector>
+#include <cstring>
+#include <unistd.h>
+
+// utilities.cpp is not compiled (it needs Qt's file classes); this restates
+// the one function the compiled sources use (utilities.cpp:95-106).
+bool checkVector(vec3_t V)
+{
+  for (int i = 0; i < 3; i++) {
+    if (std::isnan(V[i])) return false;
+    if (std::isinf(V[i])) return false;
+  }
+  return true;
+}
+
+namespace {
+
+typedef AusmPlus<5, Upwind2<5, VanAlbada>, PerfectGas> RefAusm;
+
+// Flux functor with the reference's AUSM+ field fluxes and zero patch-face
+// fluxes (the ghost layers of periodic axes overwrite the outer cells; closed
+// axes are walls with no flux).
+struct PeriodicFlux
+{
+  RefAusm m_Ausm;
+  template <typename P> void xField(P* p, size_t i, size_t j, size_t k, real x, real y, real z, real A, real* f) { m_Ausm.xField(p, i, j, k, x, y, z, A, f); }
+  template <typename P> void yField(P* p, size_t i, size_t j, size_t k, real x, real y, real z, real A, real* f) { m_Ausm.yField(p, i, j, k, x, y, z, A, f); }
+  template <typename P> void zField(P* p, size_t i, size_t j, size_t k, real x, real y, real z, real A, real* f) { m_Ausm.zField(p, i, j, k, x, y, z, A, f); }
+  template <typename P> void xWallM(P*, size_t, size_t, size_t, real, real, real, real, real*) {}
+  template <typename P> void xWallP(P*, size_t, size_t, size_t, real, real, real, real, real*) {}
+  template <typename P> void yWallM(P*, size_t, size_t, size_t, real, real, real, real, real*) {}
+  template <typename P> void yWallP(P*, size_t, size_t, size_t, real, real, real, real, real*) {}
+  template <typename P> void zWallM(P*, size_t, size_t, size_t, real, real, real, real, real*) {}
+  template <typename P> void zWallP(P*, size_t, size_t, size_t, real, real, real, real, real*) {}
+};
+
+// Periodic ghost copy, field 0, for the axes flagged periodic; each such axis
+// carries G ghost layers per side (ghosted size N = n + 2G).
+struct PeriodicGhostCopy : public GenericOperation
+{
+  CartesianPatch* m_P;
+  size_t m_G[3];
+  PeriodicGhostCopy(CartesianPatch* p, const size_t g[3]) : m_P(p) { for (int a = 0; a < 3; ++a) m_G[a] = g[a]; }
+  virtual void operator()()
+  {
+    CartesianPatch* p = m_P;
+    const size_t NI = p->sizeI(), NJ = p->sizeJ(), NK = p->sizeK();
+    const size_t ni = NI - 2*m_G[0], nj = NJ - 2*m_G[1], nk = NK - 2*m_G[2];
+    for (size_t v = 0; v < 5; ++v) {
+      for (size_t g = 0; g < m_G[0]; ++g) {
+        for (size_t j = 0; j < NJ; ++j) for (size_t k = 0; k < NK; ++k) {
+          p->f(0, v, g, j, k)                = p->f(0, v, g + ni, j, k);
+          p->f(0, v, NI - m_G[0] + g, j, k)  = p->f(0, v, m_G[0] + g, j, k);
+        }
+      }
+      for (size_t g = 0; g < m_G[1]; ++g) {
+        for (size_t i = 0; i < NI; ++i) for (size_t k = 0; k < NK; ++k) {
+          p->f(0, v, i, g, k)                = p->f(0, v, i, g + nj, k);
+          p->f(0, v, i, NJ - m_G[1] + g, k)  = p->f(0, v, i, m_G[1] + g, k);
+        }
+      }
+      for (size_t g = 0; g < m_G[2]; ++g) {
+        for (size_t i = 0; i < NI; ++i) for (size_t j = 0; j < NJ; ++j) {
+          p->f(0, v, i, j, g)                = p->f(0, v, i, j, g + nk);
+          p->f(0, v, i, j, NK - m_G[2] + g)  = p->f(0, v, i, j, m_G[2] + g);
+        }
+      }
+    }
+  }
+};
+
+std::string patchText(double x0, double y0, double z0, size_t ni, size_t nj, size_t nk,
+                      const size_t seek[6], double lx, double ly, double lz)
+{
+  std::ostringstream s;
+  s.precision(17);
+  s << x0 << " " << y0 << " " << z0 << "  1 0 0  0 1 0  1  "
+    << ni << " " << nj << " " << nk << "  "
+    << seek[0] << " " << seek[1] << " " << seek[2] << " " << seek[3] << " " << seek[4] << " " << seek[5] << "  "
+    << lx << " " << ly << " " << lz << "  0 0 0 0 0 0 0";
+  return s.str();
+}
+
+CartesianPatch* addPatch(PatchGrid& grid, const std::string& text)
+{
+  CartesianPatch* p = new CartesianPatch(&grid);
+  size_t index = grid.insertPatch(p);
+  p->setIndex(index);
+  std::istringstream iss(text);
+  p->readFromFile(iss, 1.0);
+  return p;
+}
+
+} // namespace
+
+extern "C" {
+
+// Runs `steps` RK steps (alpha[0..n_alpha-1]) of the reference CPU iterator
+// on one patch of ni x nj x nk cells of spacing (hx, hy, hz).  Axes flagged in
+// periodic[3] are periodic (two ghost layers refreshed after every stage, as a
+// post-operation); the other axes are closed (the reference's own first-order
+// edge reconstruction, zero patch-face flux).  active may be NULL.
+// init/out: [5][ni][nj][nk] conservative variables (k fastest).
+// Returns 0 on success; *seconds = steady_clock time of the RK loop only.
+int dnref_run(int ni, int nj, int nk, const int* periodic, double hx, double hy, double hz,
+              const double* init, const unsigned char* active, int steps, double dt,
+              const double* alpha, int n_alpha, int threads, double* out, double* seconds)
+{
+  if (sizeof(real) != 8) return -1;
+  if (ni < 1 || nj < 1 || nk < 1 || n_alpha < 1) return -2;
+  size_t G[3];
+  for (int a = 0; a < 3; ++a) G[a] = (periodic && periodic[a]) ? 2 : 0;
+  const size_t NI = ni + 2*G[0], NJ = nj + 2*G[1], NK = nk + 2*G[2];
+#ifdef OPEN_MP
+  if (threads > 0) omp_set_num_threads(threads);
+#endif
+  PatchGrid grid;
+  grid.setNumberOfFields(3);
+  grid.setNumberOfVariables(5);
+  grid.defineVectorVar(1);
+  size_t seek[6] = {0, 0, 0, 0, 0, 0};
+  CartesianPatch* p = addPatch(grid, patchText(0, 0, 0, NI, NJ, NK, seek, NI*hx, NJ*hy, NK*hz));
+  const size_t n = size_t(ni)*nj*nk;
+  for (size_t v = 0; v < 5; ++v)
+    for (size_t i = 0; i < size_t(ni); ++i)
+      for (size_t j = 0; j < size_t(nj); ++j)
+        for (size_t k = 0; k < size_t(nk); ++k)
+          p->f(0, v, i + G[0], j + G[1], k + G[2]) = init[v*n + (i*nj + j)*nk + k];
+  if (active) {
+    for (size_t i = 0; i < size_t(ni); ++i)
+      for (size_t j = 0; j < size_t(nj); ++j)
+        for (size_t k = 0; k < size_t(nk); ++k)
+          if (!active[(i*nj + j)*nk + k]) p->deactivate(i + G[0], j + G[1], k + G[2]);
+  }
+  PeriodicGhostCopy ghosts(p, G);
+  ghosts();
+
+  PeriodicFlux flux;
+  CartesianIterator<5, PeriodicFlux> iterator(flux);
+  iterator.addPatch(p);
+  RungeKutta rk;
+  for (int a = 0; a < n_alpha; ++a) rk.addAlpha(alpha[a]);
+  rk.addIterator(&iterator);
+  rk.addPostOperation(&ghosts);
+
+  auto t0 = std::chrono::steady_clock::now();
+  for (int s = 0; s < steps; ++s) rk(dt);
+  auto t1 = std::chrono::steady_clock::now();
+  if (seconds) *seconds = std::chrono::duration<double>(t1 - t0).count();
+
+  for (size_t v = 0; v < 5; ++v)
+    for (size_t i = 0; i < size_t(ni); ++i)
+      for (size_t j = 0; j < size_t(nj); ++j)
+        for (size_t k = 0; k < size_t(nk); ++k)
+          out[v*n + (i*nj + j)*nk + k] = p->f(0, v, i + G[0], j + G[1], k + G[2]);
+  return 0;
+}
+
+int dnref_real_size() { return int(sizeof(real)); }
+
+// A persistent single-patch run for timing: set up once, step repeatedly.
+struct DnRefSession
+{
+  PatchGrid grid;
+  CartesianPatch* patch = nullptr;
+  PeriodicGhostCopy* ghosts = nullptr;
+  CartesianIterator<5, PeriodicFlux>* iterator = nullptr;
+  RungeKutta rk;
+  size_t G[3];
+};
+
+void* dnref_session_create(int ni, int nj, int nk, const int* periodic, double hx, double hy, double hz,
+                           const double* init, const double* alpha, int n_alpha, int threads)
+{
+  if (sizeof(real) != 8 || ni < 1 || nj < 1 || nk < 1 || n_alpha < 1) return nullptr;
+#ifdef OPEN_MP
+  if (threads > 0) omp_set_num_threads(threads);
+#endif
+  DnRefSession* s = new DnRefSession();
+  for (int a = 0; a < 3; ++a) s->G[a] = (periodic && periodic[a]) ? 2 : 0;
+  const size_t NI = ni + 2*s->G[0], NJ = nj + 2*s->G[1], NK = nk + 2*s->G[2];
+  s->grid.setNumberOfFields(3);
+  s->grid.setNumberOfVariables(5);
+  s->grid.defineVectorVar(1);
+  size_t seek[6] = {0, 0, 0, 0, 0, 0};
+  s->patch = addPatch(s->grid, patchText(0, 0, 0, NI, NJ, NK, seek, NI*hx, NJ*hy, NK*hz));
+  const size_t n = size_t(ni)*nj*nk;
+  for (size_t v = 0; v < 5; ++v)
+    for (size_t i = 0; i < size_t(ni); ++i)
+      for (size_t j = 0; j < size_t(nj); ++j)
+        for (size_t k = 0; k < size_t(nk); ++k)
+          s->patch->f(0, v, i + s->G[0], j + s->G[1], k + s->G[2]) = init[v*n + (i*nj + j)*nk + k];
+  s->ghosts = new PeriodicGhostCopy(s->patch, s->G);
+  (*s->ghosts)();
+  PeriodicFlux flux;
+  s->iterator = new CartesianIterator<5, PeriodicFlux>(flux);
+  s->iterator->addPatch(s->patch);
+  for (int a = 0; a < n_alpha; ++a) s->rk.addAlpha(alpha[a]);
+  s->rk.addIterator(s->iterator);
+  s->rk.addPostOperation(s->ghosts);
+  return s;
+}
+
+// Runs `steps` RK steps; returns the steady_clock seconds of RungeKutta::operator() only.
+double dnref_session_step(void* session, int steps, double dt)
+{
+  DnRefSession* s = (DnRefSession*)session;
+  auto t0 = std::chrono::steady_clock::now();
+  for (int i = 0; i < steps; ++i) s->rk(dt);
+  auto t1 = std::chrono::steady_clock::now();
+  return std::chrono::duration<double>(t1 - t0).count();
+}
+
+void dnref_session_destroy(void* session)
+{
+  DnRefSession* s = (DnRefSession*)session;
+  if (!s) return;
+  delete s->iterator;
+  delete s->ghosts;
+  delete s;
+}
+
+int dnref_max_threads()
+{
+#ifdef OPEN_MP
+  return omp_get_max_threads();
+#else
+  return 1;
+#endif
+}
+
+} // extern "C"

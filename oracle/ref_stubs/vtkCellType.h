@@ -1,0 +1,1 @@
+#include "stub_vtk.h"

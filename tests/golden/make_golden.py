@@ -1,0 +1,61 @@
+"""Generates the golden fixtures of tests/golden/ from the reference itself.
+
+    python tests/golden/make_golden.py
+
+Needs oracle/_ref/libdrnum_ref.so, i.e. the reference DrNUM library compiled
+(FP64) from its own sources by oracle/build_ref.sh.  Each fixture stores the
+input state, the case parameters and the reference's output after the given
+number of RK steps (one OpenMP thread: the reference's canonical accumulation
+order).  The 64^3 x 100-step case stores SHA-256 digests and sums instead of
+the 10 MB field.
+"""
+from __future__ import annotations
+
+import hashlib
+import json
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+sys.path.insert(0, os.path.join(ROOT, "oracle"))
+sys.path.insert(0, HERE)
+
+import pyoracle  # noqa: E402
+import cases_def  # noqa: E402
+
+
+def digest(a: np.ndarray) -> str:
+    return hashlib.sha256(np.ascontiguousarray(a, dtype=np.float64).tobytes()).hexdigest()
+
+
+def main():
+    assert pyoracle.ref_lib().dnref_real_size() == 8
+    for name in cases_def.FULL:
+        c = cases_def.build(name)
+        out, sec = pyoracle.ref_run(c["U0"], c["h"], c["dt"], c["steps"], cases_def.ALPHA,
+                                    c["periodic"], c["active"], threads=1)
+        np.savez_compressed(os.path.join(HERE, f"{name}.npz"), U0=c["U0"], out=out, h=c["h"], dt=c["dt"],
+                            steps=c["steps"], periodic=np.array(c["periodic"], dtype=np.int8),
+                            active=c["active"] if c["active"] is not None else np.ones(0, np.uint8),
+                            alpha=np.array(cases_def.ALPHA))
+        print(f"{name}: {sec:.3f} s")
+    meta = {}
+    for name in cases_def.DIGEST:
+        c = cases_def.build(name)
+        out, sec = pyoracle.ref_run(c["U0"], c["h"], c["dt"], c["steps"], cases_def.ALPHA,
+                                    c["periodic"], c["active"], threads=1)
+        meta[name] = dict(input_sha256=digest(c["U0"]), output_sha256=digest(out),
+                          sums=[float(x) for x in out.reshape(5, -1).sum(axis=1)],
+                          rho_sample=[float(x) for x in out[0].reshape(-1)[::4099]],
+                          h=c["h"], dt=c["dt"], steps=c["steps"], seconds=sec)
+        print(f"{name}: {sec:.3f} s")
+    with open(os.path.join(HERE, "digests.json"), "w") as f:
+        json.dump(meta, f, indent=1)
+
+
+if __name__ == "__main__":
+    main()
