@@ -17,7 +17,6 @@ from __future__ import annotations
 
 import argparse
 import json
-import math
 import os
 import subprocess
 import sys
@@ -184,7 +183,9 @@ def run_ours(args, rank, world, local_rank):
     n = args.n
     U0, h, dt = cases.periodic_box(n)
     cells = n ** 3
-    stream = torch.cuda.current_stream(dev)
+    # a dedicated (non-default) stream: the library's kernels and the timing
+    # events are issued on it
+    stream = torch.cuda.Stream(dev)
 
     def make(precision):
         patch = CartesianPatch(n, n, n, spacing=(h, h, h))

@@ -42,6 +42,7 @@ struct dn_ctx {
   int fmap[3] = {0, 1, 2};
   std::string err;
   int* d_err = nullptr;
+  unsigned long long* d_err_info = nullptr;   // [cell, var, bits(f_n), bits(residual)] of the first failure
   void* staging = nullptr;
   size_t staging_bytes = 0;
   double* d_partials = nullptr;
@@ -247,8 +248,17 @@ int read_device_error(dn_ctx* c)
   if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
   if (e != cudaSuccess) return cuda_fail(c, e, "device error word");
   if (h != 0) {
+    unsigned long long info[4] = {0, 0, 0, 0};
+    cudaMemcpyAsync(info, c->d_err_info, sizeof(info), cudaMemcpyDeviceToHost, c->stream);
     cudaMemsetAsync(c->d_err, 0, sizeof(int), c->stream);
-    if (h & 1) return fail(c, DN_ERR_RANGE, "FP32 offset left its exact range (|o| >= 2^24) during a stage");
+    cudaMemsetAsync(c->d_err_info, 0xff, 4 * sizeof(unsigned long long), c->stream);
+    cudaStreamSynchronize(c->stream);
+    double un, r;
+    std::memcpy(&un, &info[2], sizeof(double));
+    std::memcpy(&r, &info[3], sizeof(double));
+    if (h & 1)
+      return fail(c, DN_ERR_RANGE, "FP32 offset left its exact range (|o| >= 2^24) during a stage "
+                  "(first at cell %llu var %llu: f_n offset %.9g, residual %.9g quanta)", info[0], info[1], un, r);
     if (h & 2) return fail(c, DN_ERR_RANGE, "uploaded state outside the FP32 offset range of the patch base/quantum");
     return fail(c, DN_ERR_DEVICE, "device error word 0x%x", h);
   }
@@ -309,6 +319,7 @@ int stage_patch(dn_ctx* c, DnPatch& p, int in_b, int un_b, int out_b, double fac
     a.out = (double*)p.buf[out_b];
     a.active = p.active;
     a.err = c->d_err;
+    a.err_info = c->d_err_info;
     g.i_chunk = dn::default_i_chunk(g.ni, g.nj, g.nk, 4, 32, c->num_sms, 3);
     a.g = g;
     a.p.Ax = dy * dz; a.p.Ay = dx * dz; a.p.Az = dx * dy; a.p.pf = pf;
@@ -320,6 +331,7 @@ int stage_patch(dn_ctx* c, DnPatch& p, int in_b, int un_b, int out_b, double fac
     a.out = (float*)p.buf[out_b];
     a.active = p.active;
     a.err = c->d_err;
+    a.err_info = c->d_err_info;
     g.i_chunk = dn::default_i_chunk(g.ni, g.nj, g.nk, 8, 32, c->num_sms, 4);
     a.g = g;
     a.p.Ax = (float)(dy * dz); a.p.Ay = (float)(dx * dz); a.p.Az = (float)(dx * dy);
@@ -419,7 +431,11 @@ int dn_ctx_create(int device, int precision, dn_ctx** out)
   if (cudaStreamCreateWithFlags(&c->own, cudaStreamNonBlocking) != cudaSuccess) { delete c; return DN_ERR_CUDA; }
   c->stream = c->own;
   if (cudaMalloc(&c->d_err, sizeof(int)) != cudaSuccess) { cudaStreamDestroy(c->own); delete c; return DN_ERR_NOMEM; }
+  if (cudaMalloc(&c->d_err_info, 4 * sizeof(unsigned long long)) != cudaSuccess) {
+    cudaFree(c->d_err); cudaStreamDestroy(c->own); delete c; return DN_ERR_NOMEM;
+  }
   cudaMemsetAsync(c->d_err, 0, sizeof(int), c->stream);
+  cudaMemsetAsync(c->d_err_info, 0xff, 4 * sizeof(unsigned long long), c->stream);
   *out = c;
   return DN_OK;
 }
@@ -436,6 +452,7 @@ int dn_ctx_destroy(dn_ctx* c)
   if (c->staging) cudaFree(c->staging);
   if (c->d_partials) cudaFree(c->d_partials);
   if (c->d_err) cudaFree(c->d_err);
+  if (c->d_err_info) cudaFree(c->d_err_info);
   if (c->own) cudaStreamDestroy(c->own);
   delete c;
   return DN_OK;

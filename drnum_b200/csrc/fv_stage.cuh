@@ -45,6 +45,7 @@ struct StageArgs {
   typename Policy::Store* out;        // f(k)
   const uint8_t* active;              // per cell, NULL = all active
   int* err;                           // device error word (bit flags)
+  unsigned long long* err_info;       // first failing cell: [cell, var, bits(un), bits(r)]
   StageGeom g;
   typename Policy::Params p;
 };
@@ -259,6 +260,7 @@ fv_stage_kernel(const StageArgs<Policy> a)
       int bad = 0;
       #pragma unroll
       for (int v = 0; v < 5; ++v) {
+        const int bad_before = bad;
         FaceT r = fx_lo[v];
         r += sm.fy[v][ty][tx];
         r += sm.fz[v][ty][tx];
@@ -272,6 +274,12 @@ fv_stage_kernel(const StageArgs<Policy> a)
           o = a.in[v * nc + c];
         }
         a.out[v * nc + c] = o;
+        if (bad != bad_before && a.err_info &&
+            atomicCAS(&a.err_info[0], ~0ull, (unsigned long long)c) == ~0ull) {
+          a.err_info[1] = (unsigned long long)v;
+          a.err_info[2] = (unsigned long long)__double_as_longlong((double)a.un[v * nc + c]);
+          a.err_info[3] = (unsigned long long)__double_as_longlong((double)r);
+        }
       }
       if (bad && a.err) atomicOr(a.err, bad);
     }
