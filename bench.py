@@ -308,7 +308,7 @@ def run_ours(args, rank, world, local_rank):
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": t32 / args.steps * 1e3, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32 (int32 fixed-point storage)", "data": "synthetic",
             "config": {"workload": workload_name(n), "cells_per_gpu": cells, "stages_per_step": STAGES,
                        "dt": dt, "l2": "inputs larger than L2 (each field 5 x 4 B x cells = "
                                          f"{20 * cells / 1e6:.0f} MB per GPU)",
@@ -320,7 +320,7 @@ def run_ours(args, rank, world, local_rank):
                                        "energy": drift[4], "steps": args.warmup + args.steps},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
-                         "kernel": "fv_stage_kernel<PolicyF32Q,8,32>",
+                         "kernel": "fx_stage_kernel<8,32> (FP32 arithmetic, int32 fixed-point storage)",
                          "algorithmic_bytes_per_launch": bytes_per_launch,
                          "avg_launch_ms": launch_s * 1e3},
             "cpu_baseline": cpu,

@@ -10,6 +10,7 @@
 // (rungekutta.cpp:27-42 copies field 0 into field 1 instead).
 #include "drnum_b200.h"
 #include "fv_launch.h"
+#include "fv_fx32.cuh"
 
 #include <cmath>
 #include <cstdarg>
@@ -115,19 +116,22 @@ struct QParams {
 };
 
 template <typename Src>
-__global__ void k_quantize(const Src* __restrict__ src, float* __restrict__ dst, size_t nc, QParams qp, int* err)
+__global__ void k_quantize(const Src* __restrict__ src, int32_t* __restrict__ dst, size_t nc, QParams qp, int* err)
 {
   const size_t n = 5 * nc;
   for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < n; e += (size_t)gridDim.x * blockDim.x) {
     const int v = (int)(e / nc);
-    const double o = rint(((double)src[e] - qp.base[v]) * qp.inv_q[v]);
-    if (!(fabs(o) < 16777216.0)) atomicOr(err, 2);
-    dst[e] = (float)o;
+    double o = rint(((double)src[e] - qp.base[v]) * qp.inv_q[v]);
+    if (!(fabs(o) < (double)dn::kFxLimit)) {
+      atomicOr(err, 2);
+      o = 0.0;
+    }
+    dst[e] = (int32_t)o;
   }
 }
 
 template <typename Dst>
-__global__ void k_dequantize(const float* __restrict__ src, Dst* __restrict__ dst, size_t nc, QParams qp)
+__global__ void k_dequantize(const int32_t* __restrict__ src, Dst* __restrict__ dst, size_t nc, QParams qp)
 {
   const size_t n = 5 * nc;
   for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < n; e += (size_t)gridDim.x * blockDim.x) {
@@ -158,6 +162,32 @@ k_partial_sums(const T* __restrict__ f, size_t nc, double* __restrict__ partials
   for (size_t c = c0 + threadIdx.x; c < c1; c += blockDim.x) {
     #pragma unroll
     for (int v = 0; v < 5; ++v) acc[v] += (double)f[v * nc + c];
+  }
+  #pragma unroll
+  for (int v = 0; v < 5; ++v) red[v][threadIdx.x] = acc[v];
+  __syncthreads();
+  for (int s = kSumThreads / 2; s > 0; s >>= 1) {
+    if ((int)threadIdx.x < s) {
+      #pragma unroll
+      for (int v = 0; v < 5; ++v) red[v][threadIdx.x] += red[v][threadIdx.x + s];
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x < 5) partials[blockIdx.x * 5 + threadIdx.x] = red[threadIdx.x][0];
+}
+
+// Exact per-block sums of int32 offsets (int64 accumulation, fixed order).
+__global__ void __launch_bounds__(kSumThreads)
+k_partial_sums_i32(const int32_t* __restrict__ f, size_t nc, long long* __restrict__ partials)
+{
+  __shared__ long long red[5][kSumThreads];
+  const size_t per = (nc + gridDim.x - 1) / gridDim.x;
+  const size_t c0 = blockIdx.x * per;
+  const size_t c1 = c0 + per < nc ? c0 + per : nc;
+  long long acc[5] = {0, 0, 0, 0, 0};
+  for (size_t c = c0 + threadIdx.x; c < c1; c += blockDim.x) {
+    #pragma unroll
+    for (int v = 0; v < 5; ++v) acc[v] += f[v * nc + c];
   }
   #pragma unroll
   for (int v = 0; v < 5; ++v) red[v][threadIdx.x] = acc[v];
@@ -257,7 +287,7 @@ int read_device_error(dn_ctx* c)
     std::memcpy(&un, &info[2], sizeof(double));
     std::memcpy(&r, &info[3], sizeof(double));
     if (h & 1)
-      return fail(c, DN_ERR_RANGE, "FP32 offset left its exact range (|o| >= 2^24) during a stage "
+      return fail(c, DN_ERR_RANGE, "fixed-point offset left its range (|o| >= 2^30) during a stage "
                   "(first at cell %llu var %llu: f_n offset %.9g, residual %.9g quanta)", info[0], info[1], un, r);
     if (h & 2) return fail(c, DN_ERR_RANGE, "uploaded state outside the FP32 offset range of the patch base/quantum");
     return fail(c, DN_ERR_DEVICE, "device error word 0x%x", h);
@@ -266,10 +296,10 @@ int read_device_error(dn_ctx* c)
 }
 
 // Derives base and quantum from a host state: base = mean per variable;
-// quantum = 2^ceil(log2(M_v / 2^24)) with M_v the magnitude scale of the
-// variable (max |rho|, max rho*(|u|+a) for all three momenta, max |rho E|),
-// so that offsets of up to M_v stay exact and the resolution equals the FP32
-// spacing at M_v.
+// quantum = 2^ceil(log2(4 M_v / 2^30)) with M_v the magnitude scale of the
+// variable (max |rho|, max rho*(|u|+a) for all three momenta, max |rho E|):
+// offsets up to 4 M_v stay inside the int32 range used (|o| < 2^30) and the
+// resolution, about 4e-9 M_v, is far below the FP32 spacing of U.
 template <typename T>
 void derive_base(DnPatch& p, const T* h)
 {
@@ -295,7 +325,7 @@ void derive_base(DnPatch& p, const T* h)
   for (int v = 0; v < 5; ++v) {
     p.base[v] = sum[v] / (double)nc;
     double Mv = M[v] > 0 ? M[v] : 1.0;
-    p.quantum[v] = std::ldexp(1.0, (int)std::ceil(std::log2(Mv / 16777216.0)));
+    p.quantum[v] = std::ldexp(1.0, (int)std::ceil(std::log2(4.0 * Mv / (double)dn::kFxLimit)));
   }
   p.base_set = true;
 }
@@ -311,7 +341,6 @@ int stage_patch(dn_ctx* c, DnPatch& p, int in_b, int un_b, int out_b, double fac
   g.per_y = p.d.face[1] == DN_FACE_PERIODIC;
   g.per_z = p.d.face[2] == DN_FACE_PERIODIC;
   cudaError_t e;
-  dn::StageShape shape{0, 0, 0};
   if (c->precision == DN_FP64) {
     dn::StageArgs<dn::PolicyF64> a;
     a.in = (const double*)p.buf[in_b];
@@ -323,24 +352,27 @@ int stage_patch(dn_ctx* c, DnPatch& p, int in_b, int un_b, int out_b, double fac
     g.i_chunk = dn::default_i_chunk(g.ni, g.nj, g.nk, 4, 32, c->num_sms, 3);
     a.g = g;
     a.p.Ax = dy * dz; a.p.Ay = dx * dz; a.p.Az = dx * dy; a.p.pf = pf;
-    e = dn::launch_stage_f64(a, shape, c->stream);
+    e = dn::launch_stage_f64(a, dn::StageShape{4, 32, g.i_chunk}, c->stream);
   } else {
-    dn::StageArgs<dn::PolicyF32Q> a;
-    a.in = (const float*)p.buf[in_b];
-    a.un = (const float*)p.buf[un_b];
-    a.out = (float*)p.buf[out_b];
+    dn::FxArgs a;
+    a.in = (const int32_t*)p.buf[in_b];
+    a.un = (const int32_t*)p.buf[un_b];
+    a.out = (int32_t*)p.buf[out_b];
     a.active = p.active;
     a.err = c->d_err;
     a.err_info = c->d_err_info;
-    g.i_chunk = dn::default_i_chunk(g.ni, g.nj, g.nk, 8, 32, c->num_sms, 4);
-    a.g = g;
+    int tj, tk;
+    dn::fx32_tile(&tj, &tk);
+    a.g.ni = g.ni; a.g.nj = g.nj; a.g.nk = g.nk;
+    a.g.per_x = g.per_x; a.g.per_y = g.per_y; a.g.per_z = g.per_z;
+    a.g.i_chunk = dn::default_i_chunk(g.ni, g.nj, g.nk, tj, tk, c->num_sms, 2);
     a.p.Ax = (float)(dy * dz); a.p.Ay = (float)(dx * dz); a.p.Az = (float)(dx * dy);
     for (int v = 0; v < 5; ++v) {
       a.p.base[v] = (float)p.base[v];
       a.p.quantum[v] = (float)p.quantum[v];
       a.p.face_scale[v] = (float)(pf / p.quantum[v]);
     }
-    e = dn::launch_stage_f32q(a, shape, c->stream);
+    e = dn::launch_stage_fx32(a, c->stream);
   }
   c->launches++;
   if (e != cudaSuccess) return cuda_fail(c, e, "stage kernel launch");
@@ -371,7 +403,7 @@ int upload_impl(dn_ctx* c, int id, int field, const H* host)
   if (c->precision == DN_FP64) {
     k_convert<H, double><<<grid_for(n), 256, 0, c->stream>>>((const H*)c->staging, (double*)dst, n);
   } else {
-    k_quantize<H><<<grid_for(n), 256, 0, c->stream>>>((const H*)c->staging, (float*)dst, p.nc, qparams(p), c->d_err);
+    k_quantize<H><<<grid_for(n), 256, 0, c->stream>>>((const H*)c->staging, (int32_t*)dst, p.nc, qparams(p), c->d_err);
   }
   c->launches++;
   e = cudaGetLastError();
@@ -399,7 +431,7 @@ int download_impl(dn_ctx* c, int id, int field, H* host)
     if (c->precision == DN_FP64) {
       k_convert<double, H><<<grid_for(n), 256, 0, c->stream>>>((const double*)src, (H*)c->staging, n);
     } else {
-      k_dequantize<H><<<grid_for(n), 256, 0, c->stream>>>((const float*)src, (H*)c->staging, p.nc, qparams(p));
+      k_dequantize<H><<<grid_for(n), 256, 0, c->stream>>>((const int32_t*)src, (H*)c->staging, p.nc, qparams(p));
     }
     c->launches++;
     e = cudaGetLastError();
@@ -487,6 +519,8 @@ int dn_patch_add(dn_ctx* c, const dn_patch_desc* d, int* id)
   if (!(d->dx > 0) || !(d->dy > 0) || !(d->dz > 0)) return fail(c, DN_ERR_ARG, "cell spacing must be positive");
   const size_t nc = (size_t)d->ni * d->nj * d->nk;
   if (nc > ((size_t)1 << 40)) return fail(c, DN_ERR_ARG, "patch too large");
+  if (c->precision == DN_FP32 && 5 * nc >= ((size_t)1 << 31))
+    return fail(c, DN_ERR_ARG, "FP32 patch limited to 5*cells < 2^31 (32-bit element offsets)");
   if (set_device(c) != DN_OK) return DN_ERR_CUDA;
   DnPatch p;
   p.d = *d;
@@ -517,7 +551,7 @@ int dn_patch_set_base(dn_ctx* c, int id, const double base[5], const double rang
   }
   for (int v = 0; v < 5; ++v) {
     p.base[v] = base[v];
-    p.quantum[v] = std::ldexp(1.0, (int)std::ceil(std::log2(range[v] / 16777216.0)));
+    p.quantum[v] = std::ldexp(1.0, (int)std::ceil(std::log2(range[v] / (double)dn::kFxLimit)));
   }
   p.base_set = true;
   return DN_OK;
@@ -621,24 +655,35 @@ int dn_conservation_sums(dn_ctx* c, double out[5])
   int s;
   if ((s = ensure_partials(c, (size_t)kSumBlocks * 5))) return s;
   std::vector<double> h((size_t)kSumBlocks * 5);
+  std::vector<long long> hi((size_t)kSumBlocks * 5);
   double tot[5] = {0, 0, 0, 0, 0};
   for (auto& p : c->patches) {
     const void* f = p.buf[c->fmap[0]];
-    if (c->precision == DN_FP64)
+    cudaError_t e;
+    const double dV = p.d.dx * p.d.dy * p.d.dz;
+    if (c->precision == DN_FP64) {
       k_partial_sums<double><<<kSumBlocks, kSumThreads, 0, c->stream>>>((const double*)f, p.nc, c->d_partials);
-    else
-      k_partial_sums<float><<<kSumBlocks, kSumThreads, 0, c->stream>>>((const float*)f, p.nc, c->d_partials);
+      e = cudaGetLastError();
+      if (e == cudaSuccess) e = cudaMemcpyAsync(h.data(), c->d_partials, h.size() * sizeof(double), cudaMemcpyDeviceToHost, c->stream);
+    } else {
+      k_partial_sums_i32<<<kSumBlocks, kSumThreads, 0, c->stream>>>((const int32_t*)f, p.nc, (long long*)c->d_partials);
+      e = cudaGetLastError();
+      if (e == cudaSuccess) e = cudaMemcpyAsync(hi.data(), c->d_partials, hi.size() * sizeof(long long), cudaMemcpyDeviceToHost, c->stream);
+    }
     c->launches++;
-    cudaError_t e = cudaGetLastError();
-    if (e == cudaSuccess) e = cudaMemcpyAsync(h.data(), c->d_partials, h.size() * sizeof(double), cudaMemcpyDeviceToHost, c->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
     if (e != cudaSuccess) return cuda_fail(c, e, "conservation sums");
-    double ps[5] = {0, 0, 0, 0, 0};
-    for (int b = 0; b < kSumBlocks; ++b)
-      for (int v = 0; v < 5; ++v) ps[v] += h[(size_t)b * 5 + v];
-    const double dV = p.d.dx * p.d.dy * p.d.dz;
     for (int v = 0; v < 5; ++v) {
-      double pv = c->precision == DN_FP64 ? ps[v] : ((double)p.nc * p.base[v] + p.quantum[v] * ps[v]);
+      double pv;
+      if (c->precision == DN_FP64) {
+        double ps = 0;
+        for (int b = 0; b < kSumBlocks; ++b) ps += h[(size_t)b * 5 + v];
+        pv = ps;
+      } else {
+        long long ps = 0;   // exact
+        for (int b = 0; b < kSumBlocks; ++b) ps += hi[(size_t)b * 5 + v];
+        pv = (double)p.nc * p.base[v] + p.quantum[v] * (double)ps;
+      }
       tot[v] += pv * dV;
     }
   }
@@ -662,9 +707,9 @@ int dn_field_difference(dn_ctx* c, int id, int f1, int v1, int f2, int v2, doubl
     const double* b = (const double*)p.buf[c->fmap[f2]] + (size_t)v2 * p.nc;
     k_diff<double><<<kSumBlocks, kSumThreads, 0, c->stream>>>(a, b, p.nc, q, v1, q, v2, 0, c->d_partials);
   } else {
-    const float* a = (const float*)p.buf[c->fmap[f1]] + (size_t)v1 * p.nc;
-    const float* b = (const float*)p.buf[c->fmap[f2]] + (size_t)v2 * p.nc;
-    k_diff<float><<<kSumBlocks, kSumThreads, 0, c->stream>>>(a, b, p.nc, q, v1, q, v2, 1, c->d_partials);
+    const int32_t* a = (const int32_t*)p.buf[c->fmap[f1]] + (size_t)v1 * p.nc;
+    const int32_t* b = (const int32_t*)p.buf[c->fmap[f2]] + (size_t)v2 * p.nc;
+    k_diff<int32_t><<<kSumBlocks, kSumThreads, 0, c->stream>>>(a, b, p.nc, q, v1, q, v2, 1, c->d_partials);
   }
   c->launches++;
   std::vector<double> h((size_t)kSumBlocks * 2);

@@ -1,26 +1,28 @@
-// FP32 bulk stage kernel instantiation (grid-quantised offset storage).
+// FX32 (FP32 bulk, fixed-point storage) stage kernel instantiation.
 #include "fv_launch.h"
+#include "fv_fx32.cuh"
 
 namespace dn {
 
 namespace {
-constexpr int F32_TJ = 8;
-constexpr int F32_TK = 32;
+constexpr int FX_TJ = 8;
+constexpr int FX_TK = 32;
 }
 
-cudaError_t launch_stage_f32q(const StageArgs<PolicyF32Q>& a, const StageShape& s, cudaStream_t st)
+cudaError_t launch_stage_fx32(const FxArgs& a, cudaStream_t st)
 {
-  using Smem = StageSmem<PolicyF32Q, F32_TJ, F32_TK>;
-  auto kern = fv_stage_kernel<PolicyF32Q, F32_TJ, F32_TK>;
+  using Smem = FxSmem<FX_TJ, FX_TK>;
+  auto kern = fx_stage_kernel<FX_TJ, FX_TK>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(Smem));
   if (e != cudaSuccess) return e;
-  (void)s;
-  dim3 block(F32_TK, F32_TJ, 1);
-  dim3 grid((a.g.nk + F32_TK - 1) / F32_TK, (a.g.nj + F32_TJ - 1) / F32_TJ,
+  dim3 block(FX_TK, FX_TJ, 1);
+  dim3 grid((a.g.nk + FX_TK - 1) / FX_TK, (a.g.nj + FX_TJ - 1) / FX_TJ,
             (a.g.ni + a.g.i_chunk - 1) / a.g.i_chunk);
   kern<<<grid, block, sizeof(Smem), st>>>(a);
   return cudaGetLastError();
 }
+
+void fx32_tile(int* tj, int* tk) { *tj = FX_TJ; *tk = FX_TK; }
 
 int default_i_chunk(int ni, int nj, int nk, int tj, int tk, int num_sms, int ctas_per_sm)
 {
@@ -33,5 +35,6 @@ int default_i_chunk(int ni, int nj, int nk, int tj, int tk, int num_sms, int cta
   if (ic > ni) ic = ni;
   return (int)ic;
 }
+
 
 } // namespace dn

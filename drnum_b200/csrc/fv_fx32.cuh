@@ -1,0 +1,465 @@
+// FP32 bulk stage kernel with fixed-point storage ("FX32").
+//
+// Same scheme as the reference (Upwind2 MUSCL on conservative variables with
+// the van Albada limiter, AUSM+ flux, low-storage RK update; see
+// fv_numerics.cuh for the reference citations) evaluated in FP32, with
+// storage and accumulation arranged for bandwidth and exact conservation:
+//
+// Storage.  A patch holds per variable v an FP64 base B_v and a power-of-two
+// quantum q_v; a cell stores the int32 offset o with U = B_v + q_v * o.  The
+// quantum is 2^-30 of four times the variable's magnitude scale, far below
+// the FP32 spacing of U, so storage adds no visible rounding.
+//
+// Update.  Each face flux F (FP32) is scaled by (factor/dV)/q_v and rounded
+// once to an integer number of quanta; the two cells of the face add the
+// same integer with opposite signs and the cell update o_new = o_n + sum of
+// its six face integers is exact.  The per-variable totals over a periodic
+// patch are therefore conserved exactly and their FP64 sums are exact.
+//
+// Reconstruction.  For the van Albada limiter the reference's two face-side
+// states of a cell (upwind2.h:29-52 with vanalbada.h:28-33, evaluated once
+// per face side, i.e. two limiter calls and four divisions per cell and
+// direction) are U_c + s and U_c - s with the same slope
+//     s = 1/2 * a*b*(a+b) / (a^2 + b^2),  a = U_c - U_{c-1},  b = U_{c+1} - U_c
+// (phi(r) a / 2 with r = b/a, phi = (r^2+r)/(r^2+1), and phi(1/r) = phi(r)/r for
+// the opposite side), so one division per cell, direction and variable gives
+// both states.  s = 0 where c-1 or c+1 lies outside a closed patch (the
+// reference's first-order fallback, upwind2.h:39-42).
+//
+// Element offsets are 32-bit: the host limits an FX32 patch to 5*cells < 2^31.
+//
+// Data flow per CTA: a TJ x TK tile of (j, k) columns marches along i.  Each
+// plane of the stencil state (int32) is prefetched into registers one step
+// ahead, dequantised once, and stored as FP32 in a four-plane shared-memory
+// ring with a two-cell halo in j and k.  x faces are evaluated per thread
+// along its own column (the left state of the next face stays in registers);
+// y and z face states and face integers are exchanged through shared memory.
+#pragma once
+
+#include <cstdint>
+#include "fv_numerics.cuh"
+
+namespace dn {
+
+struct FxParams {
+  float Ax, Ay, Az;
+  float base[5];        // B_v rounded to FP32
+  float quantum[5];     // q_v
+  float face_scale[5];  // (factor/dV)/q_v
+};
+
+struct FxGeom {
+  int ni, nj, nk;
+  int per_x, per_y, per_z;
+  int i_chunk;
+};
+
+struct FxArgs {
+  const int32_t* in;     // f(k-1) offsets, [5][ni][nj][nk]
+  const int32_t* un;     // f(n) offsets (own cell)
+  int32_t* out;          // f(k) offsets
+  const uint8_t* active; // NULL = all active
+  int* err;
+  unsigned long long* err_info;
+  FxGeom g;
+  FxParams p;
+};
+
+constexpr int kFxLimit = 1 << 30;   // |o| must stay below this
+
+// Primitive face-side state (COMPRESSIBLE_*_VARS): density, velocity,
+// pressure, speed of sound and total enthalpy.  p = rho R T with
+// T = (rE/rho - |u|^2/2)/cv, written as p = (R/cv) (rE - rho|u|^2/2).
+struct Prim {
+  float r, u, v, w, p, a, H;
+};
+
+__device__ __forceinline__ Prim fx_prim(float r, float ru, float rv, float rw, float rE)
+{
+  constexpr float R_over_cv = (float)(Gas::R / Gas::cv);
+  constexpr float gam = (float)Gas::gamma;
+  Prim s;
+  const float ir = __fdividef(1.0f, r);
+  s.r = r;
+  s.u = ru * ir;
+  s.v = rv * ir;
+  s.w = rw * ir;
+  const float ke2 = ru * s.u + rv * s.v + rw * s.w;       // rho |u|^2
+  s.p = R_over_cv * (rE - 0.5f * ke2);
+  s.a = sqrtf(gam * s.p * ir);
+  s.H = (rE + s.p) * ir;
+  return s;
+}
+
+// AUSM+ flux (ausmplus.h:39-106) between face sides L and R, normal DIR.
+template <int DIR>
+__device__ __forceinline__ void fx_ausm(const Prim& L, const Prim& R, float A, float F[5])
+{
+  const float unl = DIR == 0 ? L.u : (DIR == 1 ? L.v : L.w);
+  const float unr = DIR == 0 ? R.u : (DIR == 1 ? R.v : R.w);
+  const float a = 0.5f * (L.a + R.a);
+  const float ia = __fdividef(1.0f, a);
+  const float Ml = unl * ia, Mr = unr * ia;
+  const float M = ausm_m4(Ml, 1.0f) + ausm_m4(Mr, -1.0f);
+  const float Mp = 0.5f * (M + fabsf(M));
+  const float Mm = 0.5f * (M - fabsf(M));
+  const float p = ausm_p5(Ml, 1.0f) * L.p + ausm_p5(Mr, -1.0f) * R.p;
+  const float f0 = a * A * (L.r * Mp + R.r * Mm);
+  const float h0 = 0.5f * f0;
+  const float g0 = 0.5f * fabsf(f0);
+  F[0] = f0;
+  F[1] = h0 * (L.u + R.u) - g0 * (R.u - L.u) + (DIR == 0 ? A * p : 0.0f);
+  F[2] = h0 * (L.v + R.v) - g0 * (R.v - L.v) + (DIR == 1 ? A * p : 0.0f);
+  F[3] = h0 * (L.w + R.w) - g0 * (R.w - L.w) + (DIR == 2 ? A * p : 0.0f);
+  F[4] = h0 * (L.H + R.H) - g0 * (R.H - L.H);
+}
+
+// van Albada slope shared by both face-side states of a cell
+__device__ __forceinline__ float fx_slope(float a, float b)
+{
+  const float den = fmaf(a, a, b * b);
+  const float num = 0.5f * a * b * (a + b);
+  return den > 1e-30f ? __fdividef(num, den) : 0.0f;
+}
+
+__device__ __forceinline__ int fx_wrap(int x, int n, int per)
+{
+  if (per) {
+    if (x < 0) x += n;
+    else if (x >= n) x -= n;
+    return (x >= 0 && x < n) ? x : -1;   // n >= 3 and |shift| <= 2 keep one fold enough
+  }
+  return (x < 0 || x >= n) ? -1 : x;
+}
+
+__device__ __forceinline__ bool fx_face_exists(int x, int n, int per)
+{
+  if (n <= 2) return false;
+  return per ? true : (x >= 1 && x <= n - 1);
+}
+
+__device__ __forceinline__ bool fx_cell_ok(int x, int n, int per)
+{
+  return per ? true : (x >= 0 && x < n);
+}
+
+template <int TJ, int TK>
+struct FxSmem {
+  static constexpr int PJ = TJ + 4;
+  static constexpr int PK = TK + 4;
+  float plane[4][5][PJ][PK];          // dequantised state, ring over planes i-1 .. i+2
+  float sy[5][TJ + 1][TK];            // y: left state of the face above row jj-1 (row -1 .. TJ-1)
+  float sy_top[5][TK];                // y: right state of the face below row TJ (halo)
+  float sz[5][TJ][TK + 1];            // z: left state of the face above col kk-1 (col -1 .. TK-1)
+  float sz_top[5][TJ];                // z: right state of the face below col TK (halo)
+  int qy[5][TJ + 1][TK];              // y face integers, face below row jj
+  int qz[5][TJ][TK + 1];              // z face integers, face below col kk
+};
+
+template <int TJ, int TK>
+__global__ void __launch_bounds__(TJ * TK)
+fx_stage_kernel(const FxArgs a)
+{
+  constexpr int NT = TJ * TK;
+  constexpr int PJ = TJ + 4, PK = TK + 4;
+  constexpr int NE = 5 * PJ * PK;                 // elements per plane tile
+  constexpr int EPT = (NE + NT - 1) / NT;         // elements per thread
+  using Smem = FxSmem<TJ, TK>;
+  extern __shared__ __align__(16) unsigned char fx_smem_raw[];
+  Smem& sm = *reinterpret_cast<Smem*>(fx_smem_raw);
+
+  const FxGeom& g = a.g;
+  const FxParams& P = a.p;
+  const int tx = threadIdx.x, ty = threadIdx.y;
+  const int tid = ty * TK + tx;
+  const int k0 = blockIdx.x * TK, j0 = blockIdx.y * TJ;
+  const int i0 = blockIdx.z * g.i_chunk;
+  const int i1 = min(g.ni, i0 + g.i_chunk);
+  const int j = j0 + ty, k = k0 + tx;
+  const bool own = (j < g.nj) && (k < g.nk);
+  const int njk = g.nj * g.nk;
+  const size_t nc = (size_t)g.ni * njk;
+
+  // per-thread plane elements: in-plane offset (v*nc + j*nk + k) or -1, and
+  // the destination index inside a plane slot
+  int32_t eoff[EPT];
+  #pragma unroll
+  for (int m = 0; m < EPT; ++m) {
+    const int e = tid + m * NT;
+    eoff[m] = -1;
+    if (e < NE) {
+      const int v = e / (PJ * PK);
+      const int rem = e - v * (PJ * PK);
+      const int jj = rem / PK;
+      const int kk = rem - jj * PK;
+      const int jw = fx_wrap(j0 - 2 + jj, g.nj, g.per_y);
+      const int kw = fx_wrap(k0 - 2 + kk, g.nk, g.per_z);
+      if (jw >= 0 && kw >= 0) eoff[m] = (int32_t)(v * (int32_t)nc + jw * g.nk + kw);
+    }
+  }
+
+  int32_t pre[EPT];
+  auto fetch = [&](int ip) {
+    const int iw = fx_wrap(ip, g.ni, g.per_x);
+    #pragma unroll
+    for (int m = 0; m < EPT; ++m) {
+      pre[m] = 0;
+      if (iw >= 0 && eoff[m] >= 0) pre[m] = __ldg(a.in + (eoff[m] + iw * njk));
+    }
+  };
+  auto commit = [&](int ip) {
+    float* dst = &sm.plane[ip & 3][0][0][0];
+    #pragma unroll
+    for (int m = 0; m < EPT; ++m) {
+      const int e = tid + m * NT;
+      if (e < NE) {
+        const int v = e / (PJ * PK);
+        dst[e] = fmaf(P.quantum[v], (float)pre[m], P.base[v]);
+      }
+    }
+  };
+
+  // prologue: planes i0-1 .. i0+2 in the ring
+  for (int q = -1; q <= 2; ++q) {
+    fetch(i0 + q);
+    commit(i0 + q + 4);     // +4 keeps the slot index non-negative
+  }
+  fetch(i0 + 3);
+  __syncthreads();
+
+  // x direction registers: left state of the face above the current cell,
+  // the downwind difference of the current cell, and the lower face integers
+  Prim xleft;
+  float xb[5];           // U_{i+1} - U_i of the own column (becomes a of cell i+1)
+  int qx_lo[5];
+  {
+    // slope of cell i0 (needs i0-1, i0, i0+1) and the face below i0
+    const int s_m1 = (i0 + 3) & 3, s_0 = i0 & 3, s_p1 = (i0 + 1) & 3;
+    float Ul[5], Sp[5], Sm[5];
+    const bool sx = own && fx_cell_ok(i0 - 1, g.ni, g.per_x) && fx_cell_ok(i0 + 1, g.ni, g.per_x);
+    float U0[5];
+    #pragma unroll
+    for (int v = 0; v < 5; ++v) {
+      const float um = sm.plane[s_m1][v][ty + 2][tx + 2];
+      const float uc = sm.plane[s_0][v][ty + 2][tx + 2];
+      const float up = sm.plane[s_p1][v][ty + 2][tx + 2];
+      const float s = sx ? fx_slope(uc - um, up - uc) : 0.0f;
+      U0[v] = uc;
+      Sp[v] = uc + s;
+      Sm[v] = uc - s;
+      xb[v] = up - uc;
+      Ul[v] = um;
+    }
+    xleft = fx_prim(Sp[0], Sp[1], Sp[2], Sp[3], Sp[4]);
+    // face below i0: left state from cell i0-1 (slope needs i0-2)
+    const bool ex = own && fx_face_exists(i0, g.ni, g.per_x);
+    if (ex) {
+      const int iw2 = fx_wrap(i0 - 2, g.ni, g.per_x);
+      const bool sl = fx_cell_ok(i0 - 2, g.ni, g.per_x);
+      float Lm[5];
+      #pragma unroll
+      for (int v = 0; v < 5; ++v) {
+        float umm = Ul[v];
+        if (sl) umm = fmaf(P.quantum[v], (float)__ldg(a.in + (int64_t)v * nc + (int64_t)iw2 * njk + (int64_t)j * g.nk + k), P.base[v]);
+        const float s = sl ? fx_slope(Ul[v] - umm, U0[v] - Ul[v]) : 0.0f;
+        Lm[v] = Ul[v] + s;
+      }
+      float F[5];
+      fx_ausm<0>(fx_prim(Lm[0], Lm[1], Lm[2], Lm[3], Lm[4]), fx_prim(Sm[0], Sm[1], Sm[2], Sm[3], Sm[4]), P.Ax, F);
+      #pragma unroll
+      for (int v = 0; v < 5; ++v) qx_lo[v] = __float2int_rn(F[v] * P.face_scale[v]);
+    } else {
+      #pragma unroll
+      for (int v = 0; v < 5; ++v) qx_lo[v] = 0;
+    }
+  }
+
+  for (int i = i0; i < i1; ++i) {
+    const int s0 = i & 3, sp1 = (i + 1) & 3, sp2 = (i + 2) & 3;
+
+    // ---------------- x: face above cell i (between i and i+1)
+    int qx_hi[5];
+    {
+      const bool ex = own && fx_face_exists(i + 1, g.ni, g.per_x);
+      const bool sx = fx_cell_ok(i + 2, g.ni, g.per_x);   // slope of cell i+1 needs i+2 (i is in range)
+      float Sm[5], Sp[5];
+      #pragma unroll
+      for (int v = 0; v < 5; ++v) {
+        const float uc = sm.plane[sp1][v][ty + 2][tx + 2];
+        const float up = sm.plane[sp2][v][ty + 2][tx + 2];
+        const float b = up - uc;
+        const float s = sx ? fx_slope(xb[v], b) : 0.0f;
+        Sm[v] = uc - s;
+        Sp[v] = uc + s;
+        xb[v] = b;
+      }
+      if (ex) {
+        float F[5];
+        fx_ausm<0>(xleft, fx_prim(Sm[0], Sm[1], Sm[2], Sm[3], Sm[4]), P.Ax, F);
+        #pragma unroll
+        for (int v = 0; v < 5; ++v) qx_hi[v] = __float2int_rn(F[v] * P.face_scale[v]);
+      } else {
+        #pragma unroll
+        for (int v = 0; v < 5; ++v) qx_hi[v] = 0;
+      }
+      xleft = fx_prim(Sp[0], Sp[1], Sp[2], Sp[3], Sp[4]);
+    }
+
+    // ---------------- y and z face states of plane i
+    float ym[5], zm[5];   // right states of the faces below the own cell
+    {
+      const bool sy = fx_cell_ok(j - 1, g.nj, g.per_y) && fx_cell_ok(j + 1, g.nj, g.per_y);
+      const bool sz = fx_cell_ok(k - 1, g.nk, g.per_z) && fx_cell_ok(k + 1, g.nk, g.per_z);
+      #pragma unroll
+      for (int v = 0; v < 5; ++v) {
+        const float uc = sm.plane[s0][v][ty + 2][tx + 2];
+        const float uyl = sm.plane[s0][v][ty + 1][tx + 2];
+        const float uyh = sm.plane[s0][v][ty + 3][tx + 2];
+        const float uzl = sm.plane[s0][v][ty + 2][tx + 1];
+        const float uzh = sm.plane[s0][v][ty + 2][tx + 3];
+        const float s_y = sy ? fx_slope(uc - uyl, uyh - uc) : 0.0f;
+        const float s_z = sz ? fx_slope(uc - uzl, uzh - uc) : 0.0f;
+        sm.sy[v][ty + 1][tx] = uc + s_y;
+        sm.sz[v][ty][tx + 1] = uc + s_z;
+        ym[v] = uc - s_y;
+        zm[v] = uc - s_z;
+      }
+    }
+    // halo cells: y rows -1 (left state) and TJ (right state); z cols -1 and TK
+    for (int h = tid; h < 2 * TK + 2 * TJ; h += NT) {
+      if (h < 2 * TK) {
+        const int kk = h % TK;
+        const bool top = h >= TK;
+        const int jj = top ? TJ : -1;               // tile-relative row
+        const int jc = j0 + jj, kc = k0 + kk;
+        const bool sy = fx_cell_ok(jc - 1, g.nj, g.per_y) && fx_cell_ok(jc + 1, g.nj, g.per_y) &&
+                        fx_cell_ok(jc, g.nj, g.per_y);
+        #pragma unroll
+        for (int v = 0; v < 5; ++v) {
+          const float uc = sm.plane[s0][v][jj + 2][kk + 2];
+          const float ul = sm.plane[s0][v][jj + 1][kk + 2];
+          const float uh = sm.plane[s0][v][jj + 3][kk + 2];
+          const float s = (sy && kc < g.nk) ? fx_slope(uc - ul, uh - uc) : 0.0f;
+          if (top) sm.sy_top[v][kk] = uc - s;
+          else sm.sy[v][0][kk] = uc + s;
+        }
+      } else {
+        const int hh = h - 2 * TK;
+        const int jj = hh % TJ;
+        const bool top = hh >= TJ;
+        const int kk = top ? TK : -1;
+        const int jc = j0 + jj, kc = k0 + kk;
+        const bool sz = fx_cell_ok(kc - 1, g.nk, g.per_z) && fx_cell_ok(kc + 1, g.nk, g.per_z) &&
+                        fx_cell_ok(kc, g.nk, g.per_z);
+        #pragma unroll
+        for (int v = 0; v < 5; ++v) {
+          const float uc = sm.plane[s0][v][jj + 2][kk + 2];
+          const float ul = sm.plane[s0][v][jj + 2][kk + 1];
+          const float uh = sm.plane[s0][v][jj + 2][kk + 3];
+          const float s = (sz && jc < g.nj) ? fx_slope(uc - ul, uh - uc) : 0.0f;
+          if (top) sm.sz_top[v][jj] = uc - s;
+          else sm.sz[v][jj][0] = uc + s;
+        }
+      }
+    }
+    __syncthreads();
+
+    // ---------------- y and z faces below the own cell (+ the top halo faces)
+    {
+      // the face below row j is needed even when row j itself lies beyond a
+      // periodic patch (it is the wrapped face above the last row)
+      const bool exy = k < g.nk && fx_face_exists(j, g.nj, g.per_y) && (g.per_y || j < g.nj);
+      const bool exz = j < g.nj && fx_face_exists(k, g.nk, g.per_z) && (g.per_z || k < g.nk);
+      float F[5];
+      if (exy) {
+        fx_ausm<1>(fx_prim(sm.sy[0][ty][tx], sm.sy[1][ty][tx], sm.sy[2][ty][tx], sm.sy[3][ty][tx], sm.sy[4][ty][tx]),
+                   fx_prim(ym[0], ym[1], ym[2], ym[3], ym[4]), P.Ay, F);
+        #pragma unroll
+        for (int v = 0; v < 5; ++v) sm.qy[v][ty][tx] = __float2int_rn(F[v] * P.face_scale[v]);
+      } else {
+        #pragma unroll
+        for (int v = 0; v < 5; ++v) sm.qy[v][ty][tx] = 0;
+      }
+      if (exz) {
+        fx_ausm<2>(fx_prim(sm.sz[0][ty][tx], sm.sz[1][ty][tx], sm.sz[2][ty][tx], sm.sz[3][ty][tx], sm.sz[4][ty][tx]),
+                   fx_prim(zm[0], zm[1], zm[2], zm[3], zm[4]), P.Az, F);
+        #pragma unroll
+        for (int v = 0; v < 5; ++v) sm.qz[v][ty][tx] = __float2int_rn(F[v] * P.face_scale[v]);
+      } else {
+        #pragma unroll
+        for (int v = 0; v < 5; ++v) sm.qz[v][ty][tx] = 0;
+      }
+    }
+    for (int h = tid; h < TK + TJ; h += NT) {
+      float F[5];
+      if (h < TK) {
+        const int kk = h;
+        const int jf = j0 + TJ, kf = k0 + kk;   // face below halo row TJ
+        const bool ex = kf < g.nk && fx_face_exists(jf, g.nj, g.per_y) && (g.per_y || jf < g.nj);
+        if (ex) {
+          fx_ausm<1>(fx_prim(sm.sy[0][TJ][kk], sm.sy[1][TJ][kk], sm.sy[2][TJ][kk], sm.sy[3][TJ][kk], sm.sy[4][TJ][kk]),
+                     fx_prim(sm.sy_top[0][kk], sm.sy_top[1][kk], sm.sy_top[2][kk], sm.sy_top[3][kk], sm.sy_top[4][kk]),
+                     P.Ay, F);
+          #pragma unroll
+          for (int v = 0; v < 5; ++v) sm.qy[v][TJ][kk] = __float2int_rn(F[v] * P.face_scale[v]);
+        } else {
+          #pragma unroll
+          for (int v = 0; v < 5; ++v) sm.qy[v][TJ][kk] = 0;
+        }
+      } else {
+        const int jj = h - TK;
+        const int jf = j0 + jj, kf = k0 + TK;   // face below halo col TK
+        const bool ex = jf < g.nj && fx_face_exists(kf, g.nk, g.per_z) && (g.per_z || kf < g.nk);
+        if (ex) {
+          fx_ausm<2>(fx_prim(sm.sz[0][jj][TK], sm.sz[1][jj][TK], sm.sz[2][jj][TK], sm.sz[3][jj][TK], sm.sz[4][jj][TK]),
+                     fx_prim(sm.sz_top[0][jj], sm.sz_top[1][jj], sm.sz_top[2][jj], sm.sz_top[3][jj], sm.sz_top[4][jj]),
+                     P.Az, F);
+          #pragma unroll
+          for (int v = 0; v < 5; ++v) sm.qz[v][jj][TK] = __float2int_rn(F[v] * P.face_scale[v]);
+        } else {
+          #pragma unroll
+          for (int v = 0; v < 5; ++v) sm.qz[v][jj][TK] = 0;
+        }
+      }
+    }
+    __syncthreads();
+
+    // ---------------- residual and update of the own cell
+    if (own) {
+      const size_t c = (size_t)i * njk + (size_t)j * g.nk + k;
+      const bool act = a.active ? (a.active[c] != 0) : true;
+      int bad = 0;
+      #pragma unroll
+      for (int v = 0; v < 5; ++v) {
+        int32_t o;
+        if (act) {
+          const int r = qx_lo[v] + sm.qy[v][ty][tx] + sm.qz[v][ty][tx]
+                      - sm.qz[v][ty][tx + 1] - sm.qy[v][ty + 1][tx] - qx_hi[v];
+          const long long on = (long long)a.un[v * nc + c] + r;
+          if (on >= kFxLimit || on <= -kFxLimit) {
+            bad |= 1;
+            if (a.err_info && atomicCAS(&a.err_info[0], ~0ull, (unsigned long long)c) == ~0ull) {
+              a.err_info[1] = (unsigned long long)v;
+              a.err_info[2] = (unsigned long long)__double_as_longlong((double)a.un[v * nc + c]);
+              a.err_info[3] = (unsigned long long)__double_as_longlong((double)r);
+            }
+          }
+          o = (int32_t)on;
+        } else {
+          o = a.in[v * nc + c];
+        }
+        a.out[v * nc + c] = o;
+      }
+      if (bad && a.err) atomicOr(a.err, bad);
+    }
+    #pragma unroll
+    for (int v = 0; v < 5; ++v) qx_lo[v] = qx_hi[v];
+
+    // ---------------- ring: plane i+3 (prefetched) replaces plane i-1
+    commit(i + 3 + 4);
+    fetch(i + 4);
+    __syncthreads();
+  }
+}
+
+} // namespace dn

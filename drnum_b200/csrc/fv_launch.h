@@ -15,7 +15,10 @@ struct StageShape {
 };
 
 cudaError_t launch_stage_f64(const StageArgs<PolicyF64>& a, const StageShape& s, cudaStream_t st);
-cudaError_t launch_stage_f32q(const StageArgs<PolicyF32Q>& a, const StageShape& s, cudaStream_t st);
+
+struct FxArgs;
+cudaError_t launch_stage_fx32(const FxArgs& a, cudaStream_t st);
+void fx32_tile(int* tj, int* tk);
 
 // Chooses the i-chunk so that the grid holds enough CTAs to fill the GPU.
 int default_i_chunk(int ni, int nj, int nk, int tj, int tk, int num_sms, int ctas_per_sm);
