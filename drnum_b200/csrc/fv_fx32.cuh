@@ -91,6 +91,34 @@ __device__ __forceinline__ Prim fx_prim(float r, float ru, float rv, float rw, f
   return s;
 }
 
+// AUSM+ split Mach number and pressure polynomials of one face side
+// (compressibleflux.h:46-75) in closed form:
+//   s = +1:  M4 = 1/4 (M+1)^2 (1 + 1/2 (M-1)^2),  P5 = 1/4 (M+1)^2 ((2-M) + 3/4 M (M-1)^2)
+//   s = -1:  M4 = -1/4 (M-1)^2 (1 + 1/2 (M+1)^2), P5 = 1/4 (M-1)^2 ((2+M) - 3/4 M (M+1)^2)
+// for |M| < 1; for |M| >= 1, M4 = M1 = (M + s|M|)/2 and P5 = M1/M, which is
+// exactly 1 when s*M > 0 and 0 otherwise (no division needed).
+template <int S>
+__device__ __forceinline__ void fx_split(float M, float& m4, float& p5)
+{
+  const float ap = M + 1.0f, am = M - 1.0f;
+  const float ap2 = ap * ap, am2 = am * am;
+  float sub_m4, sub_p5, sup_m4, sup_p5;
+  if (S > 0) {
+    sub_m4 = 0.25f * ap2 * fmaf(0.5f, am2, 1.0f);
+    sub_p5 = 0.25f * ap2 * fmaf(0.75f * M, am2, 2.0f - M);
+    sup_m4 = fmaxf(M, 0.0f);
+    sup_p5 = M > 0.0f ? 1.0f : 0.0f;
+  } else {
+    sub_m4 = -0.25f * am2 * fmaf(0.5f, ap2, 1.0f);
+    sub_p5 = 0.25f * am2 * fmaf(-0.75f * M, ap2, 2.0f + M);
+    sup_m4 = fminf(M, 0.0f);
+    sup_p5 = M < 0.0f ? 1.0f : 0.0f;
+  }
+  const bool sup = fabsf(M) >= 1.0f;
+  m4 = sup ? sup_m4 : sub_m4;
+  p5 = sup ? sup_p5 : sub_p5;
+}
+
 // AUSM+ flux (ausmplus.h:39-106) between face sides L and R, normal DIR.
 template <int DIR>
 __device__ __forceinline__ void fx_ausm(const Prim& L, const Prim& R, float A, float F[5])
@@ -100,10 +128,13 @@ __device__ __forceinline__ void fx_ausm(const Prim& L, const Prim& R, float A, f
   const float a = 0.5f * (L.a + R.a);
   const float ia = __fdividef(1.0f, a);
   const float Ml = unl * ia, Mr = unr * ia;
-  const float M = ausm_m4(Ml, 1.0f) + ausm_m4(Mr, -1.0f);
-  const float Mp = 0.5f * (M + fabsf(M));
-  const float Mm = 0.5f * (M - fabsf(M));
-  const float p = ausm_p5(Ml, 1.0f) * L.p + ausm_p5(Mr, -1.0f) * R.p;
+  float m4l, p5l, m4r, p5r;
+  fx_split<1>(Ml, m4l, p5l);
+  fx_split<-1>(Mr, m4r, p5r);
+  const float M = m4l + m4r;
+  const float Mp = fmaxf(M, 0.0f);
+  const float Mm = fminf(M, 0.0f);
+  const float p = p5l * L.p + p5r * R.p;
   const float f0 = a * A * (L.r * Mp + R.r * Mm);
   const float h0 = 0.5f * f0;
   const float g0 = 0.5f * fabsf(f0);
@@ -231,6 +262,7 @@ fx_stage_kernel(const FxArgs a)
   // the downwind difference of the current cell, and the lower face integers
   Prim xleft;
   float xb[5];           // U_{i+1} - U_i of the own column (becomes a of cell i+1)
+  float xu0[5], xu1[5];  // own-column state at planes i and i+1
   int qx_lo[5];
   {
     // slope of cell i0 (needs i0-1, i0, i0+1) and the face below i0
@@ -245,6 +277,8 @@ fx_stage_kernel(const FxArgs a)
       const float up = sm.plane[s_p1][v][ty + 2][tx + 2];
       const float s = sx ? fx_slope(uc - um, up - uc) : 0.0f;
       U0[v] = uc;
+      xu0[v] = uc;
+      xu1[v] = up;
       Sp[v] = uc + s;
       Sm[v] = uc - s;
       xb[v] = up - uc;
@@ -279,14 +313,16 @@ fx_stage_kernel(const FxArgs a)
 
     // ---------------- x: face above cell i (between i and i+1)
     int qx_hi[5];
+    float xu2[5];
     {
       const bool ex = own && fx_face_exists(i + 1, g.ni, g.per_x);
       const bool sx = fx_cell_ok(i + 2, g.ni, g.per_x);   // slope of cell i+1 needs i+2 (i is in range)
       float Sm[5], Sp[5];
       #pragma unroll
       for (int v = 0; v < 5; ++v) {
-        const float uc = sm.plane[sp1][v][ty + 2][tx + 2];
+        const float uc = xu1[v];
         const float up = sm.plane[sp2][v][ty + 2][tx + 2];
+        xu2[v] = up;
         const float b = up - uc;
         const float s = sx ? fx_slope(xb[v], b) : 0.0f;
         Sm[v] = uc - s;
@@ -312,7 +348,7 @@ fx_stage_kernel(const FxArgs a)
       const bool sz = fx_cell_ok(k - 1, g.nk, g.per_z) && fx_cell_ok(k + 1, g.nk, g.per_z);
       #pragma unroll
       for (int v = 0; v < 5; ++v) {
-        const float uc = sm.plane[s0][v][ty + 2][tx + 2];
+        const float uc = xu0[v];
         const float uyl = sm.plane[s0][v][ty + 1][tx + 2];
         const float uyh = sm.plane[s0][v][ty + 3][tx + 2];
         const float uzl = sm.plane[s0][v][ty + 2][tx + 1];
@@ -426,7 +462,8 @@ fx_stage_kernel(const FxArgs a)
 
     // ---------------- residual and update of the own cell
     if (own) {
-      const size_t c = (size_t)i * njk + (size_t)j * g.nk + k;
+      const int c = i * njk + j * g.nk + k;       // 5*cells < 2^31 (host check)
+      const int ncv = (int)nc;
       const bool act = a.active ? (a.active[c] != 0) : true;
       int bad = 0;
       #pragma unroll
@@ -435,25 +472,31 @@ fx_stage_kernel(const FxArgs a)
         if (act) {
           const int r = qx_lo[v] + sm.qy[v][ty][tx] + sm.qz[v][ty][tx]
                       - sm.qz[v][ty][tx + 1] - sm.qy[v][ty + 1][tx] - qx_hi[v];
-          const long long on = (long long)a.un[v * nc + c] + r;
+          // |un| < 2^30 and |r| < 2^30 (face integers are bounded by the
+          // exact range of the update), so the int32 sum cannot overflow
+          const int on = a.un[v * ncv + c] + r;
           if (on >= kFxLimit || on <= -kFxLimit) {
             bad |= 1;
             if (a.err_info && atomicCAS(&a.err_info[0], ~0ull, (unsigned long long)c) == ~0ull) {
               a.err_info[1] = (unsigned long long)v;
-              a.err_info[2] = (unsigned long long)__double_as_longlong((double)a.un[v * nc + c]);
+              a.err_info[2] = (unsigned long long)__double_as_longlong((double)a.un[v * ncv + c]);
               a.err_info[3] = (unsigned long long)__double_as_longlong((double)r);
             }
           }
-          o = (int32_t)on;
+          o = on;
         } else {
-          o = a.in[v * nc + c];
+          o = a.in[v * ncv + c];
         }
-        a.out[v * nc + c] = o;
+        a.out[v * ncv + c] = o;
       }
       if (bad && a.err) atomicOr(a.err, bad);
     }
     #pragma unroll
-    for (int v = 0; v < 5; ++v) qx_lo[v] = qx_hi[v];
+    for (int v = 0; v < 5; ++v) {
+      qx_lo[v] = qx_hi[v];
+      xu0[v] = xu1[v];
+      xu1[v] = xu2[v];
+    }
 
     // ---------------- ring: plane i+3 (prefetched) replaces plane i-1
     commit(i + 3 + 4);
