@@ -4,7 +4,8 @@
 
 Every CUDA translation unit is compiled for sm_100a only; the FP64 stage
 kernel gets -fmad=false (bitwise parity with the reference CPU iterator), the
-FP32 (fixed-point storage) kernel gets fast-math intrinsics.
+FP32 (fixed-point storage) kernel gets fast-math intrinsics without implicit
+FMA contraction (duplicated border faces must round identically).
 """
 from __future__ import annotations
 
@@ -29,7 +30,7 @@ COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-I", INCLUDE
 UNITS = {
     "dn_api.cu": [],
     "fv_fp64.cu": ["-fmad=false"],
-    "fv_fx32.cu": ["-use_fast_math"],
+    "fv_fx32.cu": ["-use_fast_math", "-fmad=false"],
 }
 
 

@@ -28,6 +28,12 @@
 //
 // Element offsets are 32-bit: the host limits an FX32 patch to 5*cells < 2^31.
 //
+// Faces on tile and chunk borders are evaluated by both neighbouring CTAs;
+// conservation needs both evaluations to give the same integer, so the
+// translation unit is compiled without implicit multiply-add contraction
+// (every FMA is written out with fmaf) and identical inputs always produce
+// identical bits.
+//
 // Data flow per CTA: a TJ x TK tile of (j, k) columns marches along i.  Each
 // plane of the stencil state (int32) is prefetched into registers one step
 // ahead, dequantised once, and stored as FP32 in a four-plane shared-memory
@@ -84,8 +90,8 @@ __device__ __forceinline__ Prim fx_prim(float r, float ru, float rv, float rw, f
   s.u = ru * ir;
   s.v = rv * ir;
   s.w = rw * ir;
-  const float ke2 = ru * s.u + rv * s.v + rw * s.w;       // rho |u|^2
-  s.p = R_over_cv * (rE - 0.5f * ke2);
+  const float ke2 = fmaf(rw, s.w, fmaf(rv, s.v, ru * s.u));   // rho |u|^2
+  s.p = R_over_cv * fmaf(-0.5f, ke2, rE);
   s.a = sqrtf(gam * s.p * ir);
   s.H = (rE + s.p) * ir;
   return s;
@@ -134,15 +140,16 @@ __device__ __forceinline__ void fx_ausm(const Prim& L, const Prim& R, float A, f
   const float M = m4l + m4r;
   const float Mp = fmaxf(M, 0.0f);
   const float Mm = fminf(M, 0.0f);
-  const float p = p5l * L.p + p5r * R.p;
-  const float f0 = a * A * (L.r * Mp + R.r * Mm);
+  const float p = fmaf(p5l, L.p, p5r * R.p);
+  const float f0 = a * A * fmaf(L.r, Mp, R.r * Mm);
   const float h0 = 0.5f * f0;
   const float g0 = 0.5f * fabsf(f0);
+  const float Ap = A * p;
   F[0] = f0;
-  F[1] = h0 * (L.u + R.u) - g0 * (R.u - L.u) + (DIR == 0 ? A * p : 0.0f);
-  F[2] = h0 * (L.v + R.v) - g0 * (R.v - L.v) + (DIR == 1 ? A * p : 0.0f);
-  F[3] = h0 * (L.w + R.w) - g0 * (R.w - L.w) + (DIR == 2 ? A * p : 0.0f);
-  F[4] = h0 * (L.H + R.H) - g0 * (R.H - L.H);
+  F[1] = fmaf(h0, L.u + R.u, fmaf(-g0, R.u - L.u, DIR == 0 ? Ap : 0.0f));
+  F[2] = fmaf(h0, L.v + R.v, fmaf(-g0, R.v - L.v, DIR == 1 ? Ap : 0.0f));
+  F[3] = fmaf(h0, L.w + R.w, fmaf(-g0, R.w - L.w, DIR == 2 ? Ap : 0.0f));
+  F[4] = fmaf(h0, L.H + R.H, -g0 * (R.H - L.H));
 }
 
 // van Albada slope shared by both face-side states of a cell
