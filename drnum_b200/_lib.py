@@ -58,6 +58,7 @@ SIGNATURES = {
     "dn_field_difference": (c_int, [c_void_p, c_int, c_int, c_int, c_int, c_int,
                                     POINTER(c_double), POINTER(c_double)]),
     "dn_launch_count": (c_int, [c_void_p, POINTER(c_int64)]),
+    "dn_field_sums_noalloc": (c_int, [c_void_p, c_int64, c_double, POINTER(c_double), c_void_p]),
 }
 
 _lib = None

@@ -31,6 +31,7 @@ UNITS = {
     "dn_api.cu": [],
     "fv_fp64.cu": ["-fmad=false"],
     "fv_fx32.cu": ["-use_fast_math", "-fmad=false"],
+    "dn_noalloc.cu": [],
 }
 
 

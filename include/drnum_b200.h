@@ -136,6 +136,19 @@ int dn_field_difference(dn_ctx* ctx, int patch_id, int i_field1, int i_var1,
 /* Number of device kernel launches the context has issued so far. */
 int dn_launch_count(const dn_ctx* ctx, int64_t* count);
 
+/* No counterpart in the reference.  The FP64 sums of dn_conservation_sums
+ * (sum of U * dV per variable) over a caller-owned device field
+ * [5][ncells] (FP64), for callers that cannot allocate device memory, such as
+ * a solver that reserves all device memory at start-up or a host framework
+ * that owns the device memory pool.  Allocates nothing: the per-block partial
+ * sums live in a fixed 320 KiB device array inside the library, which limits
+ * the field to 2^27 cells (larger fields return DN_ERR_RANGE).  `out` is a
+ * host array; the call synchronises `stream` (a cudaStream_t, NULL = legacy
+ * default stream).  All calls on a device share that array: calls that
+ * overlap on the GPU race.  The first call on a device (with it current)
+ * resolves the array's device address; make it before any stream capture. */
+int dn_field_sums_noalloc(const double* field, int64_t ncells, double dV, double out[5], void* stream);
+
 #ifdef __cplusplus
 }
 #endif
