@@ -8,7 +8,7 @@ from __future__ import annotations
 
 import ctypes
 import os
-from ctypes import POINTER, c_double, c_float, c_int, c_int32, c_int64, c_size_t, c_uint8, c_void_p
+from ctypes import POINTER, c_double, c_float, c_int, c_int32, c_int64, c_size_t, c_uint8, c_uint64, c_void_p
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libdrnum_b200.so")
@@ -34,6 +34,9 @@ class dn_patch_desc(ctypes.Structure):
         ("face", c_int32 * 3),
         ("dx", c_double), ("dy", c_double), ("dz", c_double),
         ("origin", c_double * 3),
+        ("length", c_double * 3),
+        ("seek", c_int32 * 6),
+        ("add_protect", c_int32),
     ]
 
 
@@ -59,6 +62,19 @@ SIGNATURES = {
                                     POINTER(c_double), POINTER(c_double)]),
     "dn_launch_count": (c_int, [c_void_p, POINTER(c_int64)]),
     "dn_field_sums_noalloc": (c_int, [c_void_p, c_int64, c_double, POINTER(c_double), c_void_p]),
+    "dn_grid_compute_dependencies": (c_int, [c_void_p, POINTER(c_int64)]),
+    "dn_patch_donor_counts": (c_int, [c_void_p, c_int, POINTER(c_int64)]),
+    "dn_patch_get_donors": (c_int, [c_void_p, c_int, POINTER(c_uint64), POINTER(c_int32), POINTER(c_int64),
+                                    POINTER(c_int32), POINTER(c_uint64), POINTER(c_uint64), POINTER(c_double)]),
+    "dn_patch_set_donors": (c_int, [c_void_p, c_int, POINTER(c_int64), POINTER(c_uint64), POINTER(c_int32),
+                                    POINTER(c_int64), POINTER(c_int32), POINTER(c_uint64), POINTER(c_uint64),
+                                    POINTER(c_double)]),
+    "dn_overlap_build": (c_int, [POINTER(dn_patch_desc), c_int, POINTER(c_void_p), POINTER(c_int64)]),
+    "dn_overlap_counts": (c_int, [c_void_p, c_int, POINTER(c_int64)]),
+    "dn_overlap_get": (c_int, [c_void_p, c_int, POINTER(c_uint64), POINTER(c_int32), POINTER(c_int64),
+                               POINTER(c_int32), POINTER(c_uint64), POINTER(c_uint64), POINTER(c_double)]),
+    "dn_overlap_destroy": (c_int, [c_void_p]),
+    "dn_copy_donor_data": (c_int, [c_void_p, c_int]),
 }
 
 _lib = None
@@ -110,3 +126,40 @@ def fptr(a):
 
 def u8ptr(a):
     return a.ctypes.data_as(POINTER(c_uint8))
+
+
+def ptr(a, ctype):
+    """ctypes pointer to the data of a contiguous numpy array (NULL for None)."""
+    if a is None:
+        return None
+    return a.ctypes.data_as(POINTER(ctype))
+
+
+# donor-table arrays in the order of dn_patch_get_donors / dn_overlap_get:
+# (name, numpy dtype, ctypes type, counts index)
+DONOR_FIELDS = (
+    ("rec_unique", "uint64", c_uint64, 0),
+    ("donor_patch", "int32", c_int32, 1),
+    ("num_receivers", "int64", c_int64, 1),
+    ("stride", "int32", c_int32, 1),
+    ("rec_concat", "uint64", c_uint64, 2),
+    ("donor_idx", "uint64", c_uint64, 3),
+    ("weight", "float64", c_double, 3),
+)
+
+
+def read_donor_tables(counts_fn, get_fn, handle, patch_id):
+    """Reads one patch's donor tables through a counts/get function pair
+    (dn_patch_donor_counts/dn_patch_get_donors or dn_overlap_counts/
+    dn_overlap_get) into a dict of numpy arrays."""
+    import numpy as np
+    counts = np.zeros(4, dtype=np.int64)
+    rc = counts_fn(handle, patch_id, ptr(counts, c_int64))
+    if rc != DN_OK:
+        raise DnError(rc, f"donor counts of patch {patch_id}")
+    arrs = {name: np.zeros(int(counts[ci]), dtype=dt) for name, dt, _, ci in DONOR_FIELDS}
+    rc = get_fn(handle, patch_id, *[ptr(arrs[name], ct) for name, _, ct, _ in DONOR_FIELDS])
+    if rc != DN_OK:
+        raise DnError(rc, f"donor tables of patch {patch_id}")
+    arrs["counts"] = counts
+    return arrs

@@ -6,6 +6,7 @@ driver written against the reference reads the same:
     reference (file:line)                              here
     -------------------------------------------------  ---------------------------
     CartesianPatch (cartesianpatch.h, patch_common.h)  CartesianPatch
+    PatchGrid (patchgrid.h:45-200)                     PatchGrid.insertPatch/computeDependencies
     AusmPlus<5, Upwind2<5, VanAlbada>, PerfectGas>     AusmPlus(Upwind2(VanAlbada()), PerfectGas())
       (fluxes/ausmplus.h:29-106)
     GPU_CartesianIterator<5, OP>(op, cuda_device)      B200CartesianIterator(op, cuda_device, precision)
@@ -78,8 +79,9 @@ class CartesianPatch:
     """
 
     def __init__(self, ni, nj, nk, lengths=None, spacing=None, origin=(0.0, 0.0, 0.0),
-                 periodic=(True, True, True), num_fields=3):
+                 periodic=(True, True, True), num_fields=3, seek=(0, 0, 0, 0, 0, 0), add_protect=0):
         self.m_NumI, self.m_NumJ, self.m_NumK = int(ni), int(nj), int(nk)
+        self.lengths = (0.0, 0.0, 0.0) if lengths is None else tuple(float(x) for x in lengths)
         if spacing is None:
             if lengths is None:
                 raise ValueError("give lengths or spacing")
@@ -88,6 +90,12 @@ class CartesianPatch:
         self.m_Dx, self.m_Dy, self.m_Dz = (float(s) for s in spacing)
         self.origin = tuple(float(o) for o in origin)
         self.periodic = tuple(bool(p) for p in periodic)
+        # seek layers imin..kmax and additional protected layers
+        # (CartesianPatch::setSeekExceptions, cartesianpatch.cpp:146-157)
+        self.seek = tuple(int(x) for x in seek)
+        self.add_protect = int(add_protect)
+        self.grid = None
+        self.grid_index = None
         self.m_NumFields = num_fields
         self.data = np.zeros((num_fields, 5, ni, nj, nk))
         self.active = np.ones((ni, nj, nk), dtype=np.uint8)
@@ -124,7 +132,58 @@ class CartesianPatch:
         d.dx, d.dy, d.dz = self.m_Dx, self.m_Dy, self.m_Dz
         for a in range(3):
             d.origin[a] = self.origin[a]
+            d.length[a] = self.lengths[a]
+        for a in range(6):
+            d.seek[a] = self.seek[a]
+        d.add_protect = self.add_protect
         return d
+
+
+# -------------------------------------------------------------------- patch grid
+
+class PatchGrid:
+    """PatchGrid (patchgrid.h:45-200): the patches of a case and their
+    overlap dependencies.  computeDependencies() builds every patch's donor
+    tables on the host (dn_overlap_build: receiving cells, 8-point trilinear
+    donor stencils, multi-donor averaging), equal to the reference's
+    PatchGrid::computeDependencies (patchgrid.cpp:119-268)."""
+
+    def __init__(self, num_seeklayers=2, num_addprotectlayers=0):
+        self.m_NumSeekLayers = int(num_seeklayers)
+        self.m_NumAddProtectLayers = int(num_addprotectlayers)
+        self.m_Patches: list[CartesianPatch] = []
+        self.tables = None
+        self.no_donor = 0
+
+    def insertPatch(self, patch: CartesianPatch) -> int:
+        patch.add_protect = self.m_NumAddProtectLayers
+        patch.grid = self
+        patch.grid_index = len(self.m_Patches)
+        self.m_Patches.append(patch)
+        self.tables = None
+        return patch.grid_index
+
+    def getNumPatches(self):
+        return len(self.m_Patches)
+
+    def getPatch(self, i):
+        return self.m_Patches[i]
+
+    def computeDependencies(self, with_intercoeff=True):
+        if not with_intercoeff:
+            raise ValueError("only with_intercoeff=True is supported (patchgrid.cpp:150-153)")
+        lib = _lib.load()
+        arr = (_lib.dn_patch_desc * len(self.m_Patches))(*[p.desc() for p in self.m_Patches])
+        h = ctypes.c_void_p()
+        nd = ctypes.c_int64()
+        check(None, lib.dn_overlap_build(arr, len(self.m_Patches), ctypes.byref(h), ctypes.byref(nd)))
+        try:
+            self.tables = [_lib.read_donor_tables(lib.dn_overlap_counts, lib.dn_overlap_get, h, p)
+                           for p in range(len(self.m_Patches))]
+        finally:
+            lib.dn_overlap_destroy(h)
+        self.no_donor = int(nd.value)
+        return self.tables
 
 
 # --------------------------------------------------------------------- iterator
@@ -184,7 +243,35 @@ class B200CartesianIterator:
         s = np.ascontiguousarray(scale, dtype=np.float64)
         check(self.ctx, self.lib.dn_patch_set_base(self.ctx, i_patch, _lib.dptr(b), _lib.dptr(s)))
 
+    def setDonorTables(self):
+        """Hands the donor tables of the patches' PatchGrid to the device
+        (dn_patch_set_donors); donor patch ids map through the grid."""
+        for pid, p in enumerate(self.m_Patches):
+            if p.grid is None or p.grid.tables is None:
+                continue
+            to_it = {q.grid_index: i for i, q in enumerate(self.m_Patches) if q.grid is p.grid}
+            t = p.grid.tables[p.grid_index]
+            dp = np.ascontiguousarray([to_it[int(d)] for d in t["donor_patch"]], dtype=np.int32)
+            counts = np.ascontiguousarray(t["counts"], dtype=np.int64)
+            args = [np.ascontiguousarray(t[k]) for k in ("rec_unique",)] + [dp] + \
+                   [np.ascontiguousarray(t[k]) for k in ("num_receivers", "stride", "rec_concat", "donor_idx", "weight")]
+            types = [c for _, _, c, _ in _lib.DONOR_FIELDS]
+            check(self.ctx, self.lib.dn_patch_set_donors(self.ctx, pid, _lib.ptr(counts, ctypes.c_int64),
+                                                         *[_lib.ptr(a, ct) for a, ct in zip(args, types)]))
+
+    def computeDependencies(self):
+        """Builds the donor tables of the iterator's patches on the context
+        (dn_grid_compute_dependencies); returns the number of seek cells
+        without a donor."""
+        nd = ctypes.c_int64()
+        check(self.ctx, self.lib.dn_grid_compute_dependencies(self.ctx, ctypes.byref(nd)))
+        return nd.value
+
+    def donorTables(self, i_patch):
+        return _lib.read_donor_tables(self.lib.dn_patch_donor_counts, self.lib.dn_patch_get_donors, self.ctx, i_patch)
+
     def updateDevice(self, fields=(0, 1)):
+        self.setDonorTables()
         for pid, p in enumerate(self.m_Patches):
             for f in fields:
                 a = np.ascontiguousarray(p.data[f], dtype=np.float64)
@@ -214,8 +301,8 @@ class B200CartesianIterator:
         self.compute(factor)
 
     def copyDonorData(self, i_field):
-        # no overlap coupling registered: nothing to transfer
-        return None
+        """PatchIterator::copyDonorData (patchiterator.h:106-111)."""
+        check(self.ctx, self.lib.dn_copy_donor_data(self.ctx, int(i_field)))
 
     def rkStep(self, dt, alphas):
         a = np.ascontiguousarray(alphas, dtype=np.float64)

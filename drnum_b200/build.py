@@ -5,7 +5,9 @@
 Every CUDA translation unit is compiled for sm_100a only; the FP64 stage
 kernel gets -fmad=false (bitwise parity with the reference CPU iterator), the
 FP32 (fixed-point storage) kernel gets fast-math intrinsics without implicit
-FMA contraction (duplicated border faces must round identically).
+FMA contraction (duplicated border faces must round identically); the donor
+copy and the host overlap set-up are built without contraction too (weights
+and interpolated values round like the reference's).
 """
 from __future__ import annotations
 
@@ -32,6 +34,8 @@ UNITS = {
     "fv_fp64.cu": ["-fmad=false"],
     "fv_fx32.cu": ["-use_fast_math", "-fmad=false"],
     "dn_noalloc.cu": [],
+    "dn_donor.cu": ["-fmad=false"],
+    "dn_overlap.cpp": ["-Xcompiler", "-ffp-contract=off"],
 }
 
 
@@ -62,7 +66,7 @@ def build(verbose: bool = False, ptxas_info: bool = False) -> str:
 
     def compile_one(unit: str) -> str:
         src = os.path.join(CSRC, unit)
-        obj = os.path.join(OBJDIR, unit.replace(".cu", ".o"))
+        obj = os.path.join(OBJDIR, os.path.splitext(unit)[0] + ".o")
         if _sources_newer(obj, [src, *headers]) or ptxas_info:
             cmd = [cc, *ARCH, *COMMON, *UNITS[unit], "-c", src, "-o", obj]
             if ptxas_info:

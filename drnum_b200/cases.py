@@ -116,3 +116,74 @@ def periodic_box(n, steps_hint=None):
     U = vortex_pulse(n, n, n)
     dt = cfl_dt(U, h, 0.5)
     return U, h, dt
+
+
+# ------------------------------------------------------------------ patch grids
+#
+# A grid is a list of axis-aligned patches, each a dict with
+#   n (cells per axis), origin, length (extent per axis), seek (6 layers:
+#   imin imax jmin jmax kmin kmax; 0 on a side without a neighbour).
+
+def patch_centres(p):
+    """Cell-centre coordinates (x, y, z) of a patch, inertial frame, as
+    broadcastable arrays (CartesianPatch::xyzCell, cartesianpatch.h:267-273)."""
+    h = [p["length"][a] / p["n"][a] for a in range(3)]
+    xs = [p["origin"][a] + (0.5 * h[a] + np.arange(p["n"][a]) * h[a]) for a in range(3)]
+    return xs[0][:, None, None], xs[1][None, :, None], xs[2][None, None, :]
+
+
+def octant_grid(nf=(8, 8, 8), h=1.0 / 16, overlap=3, seek=2):
+    """Dual-resolution 2x2x2 box: the octant at the origin is one patch at
+    spacing h with nf cells per axis, the seven other octants are patches at
+    spacing 2h.  Every patch reaches `overlap` of its own cells across each
+    interior interface and receives data in `seek` layers there; the box
+    faces carry no seek layers."""
+    X = [nf[a] * h for a in range(3)]
+    patches = []
+    for oc in range(8):
+        bits = ((oc >> 2) & 1, (oc >> 1) & 1, oc & 1)
+        fine = oc == 0
+        hh = h if fine else 2.0 * h
+        n, origin, sk = [], [], []
+        for a in range(3):
+            cells = nf[a] if fine else nf[a] // 2
+            n.append(cells + overlap)
+            if bits[a] == 0:      # lower octant: interior side is the upper one
+                origin.append(0.0)
+                sk += [0, seek]
+            else:
+                origin.append(X[a] - overlap * hh)
+                sk += [seek, 0]
+        patches.append(dict(n=tuple(n), origin=tuple(origin), length=tuple(n[a] * hh for a in range(3)),
+                            seek=tuple(sk)))
+    return patches
+
+
+def grid_state(patches, mach=0.3, beta=5.0, radius=0.1, centre=(0.25, 0.25, 0.25), pulse_amp=1e-2,
+               pulse_width=0.05):
+    """The vortex-and-pulse field of vortex_pulse evaluated at every patch's
+    own cell centres (overlapping patches agree where they overlap)."""
+    out = []
+    for p in patches:
+        x, y, z = patch_centres(p)
+        xr = (x - centre[0]) / radius
+        yr = (y - centre[1]) / radius
+        e = np.exp(0.5 * (1.0 - (xr * xr + yr * yr)))
+        k = beta / (2.0 * math.pi)
+        shape = tuple(p["n"])
+        u = np.broadcast_to(mach * A_INF - k * yr * e * A_INF, shape)
+        v = np.broadcast_to(k * xr * e * A_INF, shape)
+        w = np.zeros(shape)
+        Tn = np.broadcast_to(1.0 - (GAS_GAMMA - 1.0) * beta * beta / (8.0 * GAS_GAMMA * math.pi ** 2) * e * e, shape)
+        rho = RHO_INF * Tn ** (1.0 / (GAS_GAMMA - 1.0))
+        pr = rho * GAS_R * T_INF * Tn
+        d2 = (x - centre[0]) ** 2 + (y - centre[1]) ** 2 + (z - centre[2]) ** 2
+        rho = rho * (1.0 + pulse_amp * np.exp(-d2 / pulse_width ** 2))
+        T = pr / (rho * GAS_R)
+        out.append(np.ascontiguousarray(prim_to_cons(pr, T, u, v, w)))
+    return out
+
+
+def grid_dt(patches, states, cfl=0.5):
+    """One global time step: cfl * min over patches of h / max(|u| + a)."""
+    return min(cfl_dt(U, min(p["length"][a] / p["n"][a] for a in range(3)), cfl) for p, U in zip(patches, states))

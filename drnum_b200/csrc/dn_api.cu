@@ -11,10 +11,13 @@
 #include "drnum_b200.h"
 #include "fv_launch.h"
 #include "fv_fx32.cuh"
+#include "dn_donor.cuh"
+#include "dn_overlap.h"
 
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
+#include <algorithm>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -49,6 +52,11 @@ struct dn_ctx {
   double* d_partials = nullptr;
   size_t partials_cap = 0;
   int64_t launches = 0;
+  // donor tables (host) and their device form
+  std::vector<dn::DonorTables> tables;
+  bool plan_dirty = true;
+  std::vector<void*> plan_mem;
+  dn::DonorPlan plan{};
 };
 
 namespace {
@@ -330,6 +338,118 @@ void derive_base(DnPatch& p, const T* h)
   p.base_set = true;
 }
 
+// ------------------------------------------------------------ donor plan
+
+void free_plan(dn_ctx* c)
+{
+  for (void* m : c->plan_mem) cudaFree(m);
+  c->plan_mem.clear();
+  c->plan = dn::DonorPlan{};
+}
+
+template <typename T>
+int plan_upload(dn_ctx* c, const std::vector<T>& h, const T** out)
+{
+  *out = nullptr;
+  if (h.empty()) return DN_OK;
+  void* d = nullptr;
+  cudaError_t e = cudaMalloc(&d, h.size() * sizeof(T));
+  if (e != cudaSuccess) return fail(c, DN_ERR_NOMEM, "cudaMalloc(donor plan)");
+  c->plan_mem.push_back(d);
+  e = cudaMemcpyAsync(d, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice, c->stream);
+  if (e != cudaSuccess) return cuda_fail(c, e, "donor plan upload");
+  *out = static_cast<const T*>(d);
+  return DN_OK;
+}
+
+bool has_donors(const dn_ctx* c)
+{
+  for (const auto& t : c->tables) if (!t.rec_unique.empty()) return true;
+  return false;
+}
+
+// Regroups the per-patch tables by receiving cell (groups in donor order)
+// and uploads them with the per-patch buffer table.
+int build_plan(dn_ctx* c)
+{
+  free_plan(c);
+  const size_t np = c->patches.size();
+  std::vector<int32_t> rv_patch, rv_grp(1, 0), gp_donor, gp_stride;
+  std::vector<int64_t> rv_cell, gp_wi, idx, nc(np);
+  std::vector<double> w, base(np * 5), quantum(np * 5);
+  std::vector<void*> bufs(np * 3);
+  for (size_t r = 0; r < np; ++r) {
+    const DnPatch& P = c->patches[r];
+    nc[r] = (int64_t)P.nc;
+    for (int b = 0; b < 3; ++b) bufs[r * 3 + b] = P.buf[b];
+    for (int v = 0; v < 5; ++v) { base[r * 5 + v] = P.base[v]; quantum[r * 5 + v] = P.quantum[v]; }
+    if (r >= c->tables.size()) continue;
+    const dn::DonorTables& T = c->tables[r];
+    const size_t nu = T.rec_unique.size();
+    if (nu == 0) continue;
+    // groups of this patch in (donor, receiver) order, then listed per receiving cell
+    std::vector<int32_t> ld, ls;
+    std::vector<int64_t> lw;
+    std::vector<std::vector<size_t>> groups(nu);
+    const int64_t wi_base = (int64_t)idx.size();
+    size_t rc_off = 0;
+    int64_t wi_off = 0;
+    for (size_t q = 0; q < T.donor_patch.size(); ++q) {
+      for (int64_t ll = 0; ll < T.num_receivers[q]; ++ll) {
+        const uint64_t cell = T.rec_concat[rc_off + (size_t)ll];
+        const size_t u = (size_t)(std::lower_bound(T.rec_unique.begin(), T.rec_unique.end(), cell) - T.rec_unique.begin());
+        groups[u].push_back(ld.size());
+        ld.push_back(T.donor_patch[q]);
+        ls.push_back(T.stride[q]);
+        lw.push_back(wi_base + wi_off + ll * T.stride[q]);
+      }
+      rc_off += (size_t)T.num_receivers[q];
+      wi_off += T.num_receivers[q] * T.stride[q];
+    }
+    idx.insert(idx.end(), T.donor_idx.begin(), T.donor_idx.end());
+    w.insert(w.end(), T.weight.begin(), T.weight.end());
+    for (size_t u = 0; u < nu; ++u) {
+      rv_patch.push_back((int32_t)r);
+      rv_cell.push_back((int64_t)T.rec_unique[u]);
+      for (size_t g : groups[u]) {
+        gp_donor.push_back(ld[g]);
+        gp_stride.push_back(ls[g]);
+        gp_wi.push_back(lw[g]);
+      }
+      rv_grp.push_back((int32_t)gp_donor.size());
+    }
+  }
+  if (rv_patch.size() >= (size_t)INT32_MAX || gp_donor.size() >= (size_t)INT32_MAX)
+    return fail(c, DN_ERR_RANGE, "too many receiving cells or donor groups for one donor plan");
+  int s;
+  dn::DonorPlan& P = c->plan;
+  P.n_recv = (int32_t)rv_patch.size();
+  if ((s = plan_upload(c, rv_patch, &P.rv_patch)) || (s = plan_upload(c, rv_cell, &P.rv_cell)) ||
+      (s = plan_upload(c, rv_grp, &P.rv_grp)) || (s = plan_upload(c, gp_donor, &P.gp_donor)) ||
+      (s = plan_upload(c, gp_stride, &P.gp_stride)) || (s = plan_upload(c, gp_wi, &P.gp_wi)) ||
+      (s = plan_upload(c, idx, &P.idx)) || (s = plan_upload(c, w, &P.w)) || (s = plan_upload(c, nc, &P.nc)) ||
+      (s = plan_upload(c, base, &P.base)) || (s = plan_upload(c, quantum, &P.quantum))) {
+    free_plan(c);
+    return s;
+  }
+  if ((s = plan_upload(c, bufs, &P.bufs))) { free_plan(c); return s; }
+  c->plan_dirty = false;
+  return DN_OK;
+}
+
+// Donor copy into physical buffer `b` of every patch.
+int donor_copy(dn_ctx* c, int b)
+{
+  if (!has_donors(c)) return DN_OK;
+  int s;
+  if (c->plan_dirty && (s = build_plan(c))) return s;
+  cudaError_t e = c->precision == DN_FP64 ? dn::launch_donor_copy_f64(c->plan, b, c->stream)
+                                          : dn::launch_donor_copy_fx32(c->plan, b, c->d_err, c->stream);
+  c->launches++;
+  if (e != cudaSuccess) return cuda_fail(c, e, "donor copy launch");
+  return DN_OK;
+}
+
 int stage_patch(dn_ctx* c, DnPatch& p, int in_b, int un_b, int out_b, double factor)
 {
   const double dx = p.d.dx, dy = p.d.dy, dz = p.d.dz;
@@ -396,7 +516,10 @@ int upload_impl(dn_ctx* c, int id, int field, const H* host)
     if (e != cudaSuccess) return cuda_fail(c, e, "upload copy");
     return DN_OK;
   }
-  if (c->precision == DN_FP32 && !p.base_set) derive_base(p, host);
+  if (c->precision == DN_FP32 && !p.base_set) {
+    derive_base(p, host);
+    c->plan_dirty = true;
+  }
   if ((s = ensure_staging(c, n * sizeof(H)))) return s;
   e = cudaMemcpyAsync(c->staging, host, n * sizeof(H), cudaMemcpyHostToDevice, c->stream);
   if (e != cudaSuccess) return cuda_fail(c, e, "upload copy");
@@ -481,6 +604,7 @@ int dn_ctx_destroy(dn_ctx* c)
     for (int b = 0; b < 3; ++b) if (p.buf[b]) cudaFree(p.buf[b]);
     if (p.active) cudaFree(p.active);
   }
+  free_plan(c);
   if (c->staging) cudaFree(c->staging);
   if (c->d_partials) cudaFree(c->d_partials);
   if (c->d_err) cudaFree(c->d_err);
@@ -516,14 +640,26 @@ int dn_patch_add(dn_ctx* c, const dn_patch_desc* d, int* id)
     if (d->face[a] == DN_FACE_PERIODIC && n < 3)
       return fail(c, DN_ERR_ARG, "periodic axis %d needs at least 3 cells", a);
   }
-  if (!(d->dx > 0) || !(d->dy > 0) || !(d->dz > 0)) return fail(c, DN_ERR_ARG, "cell spacing must be positive");
+  dn_patch_desc dd = *d;
+  const int nn[3] = {d->ni, d->nj, d->nk};
+  double* sp[3] = {&dd.dx, &dd.dy, &dd.dz};
+  for (int a = 0; a < 3; ++a) {
+    if (d->length[a] > 0) *sp[a] = d->length[a] / nn[a];   // CartesianPatch::computeDeltas
+    if (!(*sp[a] > 0) || !std::isfinite(*sp[a])) return fail(c, DN_ERR_ARG, "cell spacing of axis %d must be positive", a);
+    if (!std::isfinite(d->origin[a])) return fail(c, DN_ERR_ARG, "origin must be finite");
+    if (d->seek[2 * a] < 0 || d->seek[2 * a + 1] < 0 || d->add_protect < 0 ||
+        d->seek[2 * a] + d->seek[2 * a + 1] + 2 * d->add_protect > nn[a])
+      return fail(c, DN_ERR_ARG, "seek/protect layers of axis %d exceed the patch", a);
+    if (d->face[a] == DN_FACE_PERIODIC && (d->seek[2 * a] || d->seek[2 * a + 1]))
+      return fail(c, DN_ERR_ARG, "a periodic axis (%d) cannot have seek layers", a);
+  }
   const size_t nc = (size_t)d->ni * d->nj * d->nk;
   if (nc > ((size_t)1 << 40)) return fail(c, DN_ERR_ARG, "patch too large");
   if (c->precision == DN_FP32 && 5 * nc >= ((size_t)1 << 31))
     return fail(c, DN_ERR_ARG, "FP32 patch limited to 5*cells < 2^31 (32-bit element offsets)");
   if (set_device(c) != DN_OK) return DN_ERR_CUDA;
   DnPatch p;
-  p.d = *d;
+  p.d = dd;
   p.nc = nc;
   const size_t bytes = 5 * nc * elem_size(c);
   for (int b = 0; b < 3; ++b) {
@@ -535,6 +671,8 @@ int dn_patch_add(dn_ctx* c, const dn_patch_desc* d, int* id)
     cudaMemsetAsync(p.buf[b], 0, bytes, c->stream);
   }
   c->patches.push_back(p);
+  c->tables.resize(c->patches.size());
+  c->plan_dirty = true;
   *id = (int)c->patches.size() - 1;
   return DN_OK;
 }
@@ -554,6 +692,7 @@ int dn_patch_set_base(dn_ctx* c, int id, const double base[5], const double rang
     p.quantum[v] = std::ldexp(1.0, (int)std::ceil(std::log2(range[v] / (double)dn::kFxLimit)));
   }
   p.base_set = true;
+  c->plan_dirty = true;
   return DN_OK;
 }
 
@@ -624,13 +763,18 @@ int dn_rk_step(dn_ctx* c, double dt, const double* alpha, int n_alpha)
   // A = step-start state, X/Y = the two other buffers
   const int A = c->fmap[0], X = c->fmap[2], Y = c->fmap[1];
   int in = A;
+  int st;
+  // copyDonorData(0) before the step-start copy (rungekutta.cpp:30); the
+  // copy before each later stage (:34-36) repeats the previous stage's and
+  // is skipped
+  if ((st = donor_copy(c, A))) return st;
   for (int s = 0; s < n_alpha; ++s) {
     const int out = (s & 1) ? Y : X;
     const double factor = alpha[s] * dt;   // (*i)*dt, rungekutta.cpp:37
     for (auto& p : c->patches) {
-      int st = stage_patch(c, p, in, A, out, factor);
-      if (st) return st;
+      if ((st = stage_patch(c, p, in, A, out, factor))) return st;
     }
+    if ((st = donor_copy(c, out))) return st;   // copyDonorData(0) after the stage (:38)
     in = out;
   }
   c->fmap[0] = in;
@@ -725,6 +869,115 @@ int dn_field_difference(dn_ctx* c, int id, int f1, int v1, int f2, int v2, doubl
   *max_norm = std::sqrt(mx);
   *l2_norm = std::sqrt(sm);
   return DN_OK;
+}
+
+int dn_grid_compute_dependencies(dn_ctx* c, int64_t* no_donor)
+{
+  if (!c) return DN_ERR_ARG;
+  std::vector<dn::OverlapPatch> ops;
+  for (const DnPatch& p : c->patches) ops.push_back(dn::overlap_patch(p.d));
+  std::vector<dn::DonorTables> t;
+  std::string err;
+  if (!dn::build_overlap(ops, t, err)) return fail(c, DN_ERR_ARG, "%s", err.c_str());
+  int64_t nd = 0;
+  for (const auto& x : t) nd += x.no_donor;
+  c->tables.swap(t);
+  c->plan_dirty = true;
+  if (no_donor) *no_donor = nd;
+  return DN_OK;
+}
+
+int dn_patch_donor_counts(dn_ctx* c, int id, int64_t counts[4])
+{
+  int s = check_patch(c, id);
+  if (s) return s;
+  if (!counts) return fail(c, DN_ERR_ARG, "counts is NULL");
+  const dn::DonorTables& t = c->tables[id];
+  counts[0] = (int64_t)t.rec_unique.size();
+  counts[1] = (int64_t)t.donor_patch.size();
+  counts[2] = (int64_t)t.rec_concat.size();
+  counts[3] = (int64_t)t.donor_idx.size();
+  return DN_OK;
+}
+
+int dn_patch_get_donors(dn_ctx* c, int id, uint64_t* rec_unique, int32_t* donor_patch, int64_t* num_receivers,
+                        int32_t* stride, uint64_t* rec_concat, uint64_t* donor_idx, double* weight)
+{
+  int s = check_patch(c, id);
+  if (s) return s;
+  const dn::DonorTables& t = c->tables[id];
+  if ((!rec_unique && !t.rec_unique.empty()) || (!rec_concat && !t.rec_concat.empty()) ||
+      (!donor_idx && !t.donor_idx.empty()) || (!weight && !t.weight.empty()) ||
+      (!t.donor_patch.empty() && (!donor_patch || !num_receivers || !stride)))
+    return fail(c, DN_ERR_ARG, "an output array is NULL");
+  std::copy(t.rec_unique.begin(), t.rec_unique.end(), rec_unique);
+  std::copy(t.donor_patch.begin(), t.donor_patch.end(), donor_patch);
+  std::copy(t.num_receivers.begin(), t.num_receivers.end(), num_receivers);
+  std::copy(t.stride.begin(), t.stride.end(), stride);
+  std::copy(t.rec_concat.begin(), t.rec_concat.end(), rec_concat);
+  std::copy(t.donor_idx.begin(), t.donor_idx.end(), donor_idx);
+  std::copy(t.weight.begin(), t.weight.end(), weight);
+  return DN_OK;
+}
+
+int dn_patch_set_donors(dn_ctx* c, int id, const int64_t counts[4], const uint64_t* rec_unique,
+                        const int32_t* donor_patch, const int64_t* num_receivers, const int32_t* stride,
+                        const uint64_t* rec_concat, const uint64_t* donor_idx, const double* weight)
+{
+  int s = check_patch(c, id);
+  if (s) return s;
+  if (!counts) return fail(c, DN_ERR_ARG, "counts is NULL");
+  for (int q = 0; q < 4; ++q) if (counts[q] < 0) return fail(c, DN_ERR_ARG, "negative table size");
+  if ((counts[0] && !rec_unique) || (counts[1] && (!donor_patch || !num_receivers || !stride)) ||
+      (counts[2] && !rec_concat) || (counts[3] && (!donor_idx || !weight)))
+    return fail(c, DN_ERR_ARG, "a table array is NULL");
+  const size_t nc = c->patches[id].nc;
+  dn::DonorTables t;
+  t.rec_unique.assign(rec_unique, rec_unique + counts[0]);
+  for (size_t u = 0; u < t.rec_unique.size(); ++u) {
+    if (t.rec_unique[u] >= nc || (u > 0 && t.rec_unique[u] <= t.rec_unique[u - 1]))
+      return fail(c, DN_ERR_ARG, "receiving cells must be ascending cell indices of the patch");
+  }
+  int64_t nrec = 0, nwi = 0;
+  for (int64_t q = 0; q < counts[1]; ++q) {
+    if (donor_patch[q] < 0 || donor_patch[q] >= (int)c->patches.size() || donor_patch[q] == id)
+      return fail(c, DN_ERR_ARG, "donor %lld: invalid donor patch %d", (long long)q, donor_patch[q]);
+    if (num_receivers[q] < 0 || stride[q] < 1) return fail(c, DN_ERR_ARG, "donor %lld: invalid size", (long long)q);
+    nrec += num_receivers[q];
+    nwi += num_receivers[q] * stride[q];
+  }
+  if (nrec != counts[2] || nwi != counts[3]) return fail(c, DN_ERR_ARG, "table sizes do not add up");
+  t.donor_patch.assign(donor_patch, donor_patch + counts[1]);
+  t.num_receivers.assign(num_receivers, num_receivers + counts[1]);
+  t.stride.assign(stride, stride + counts[1]);
+  t.rec_concat.assign(rec_concat, rec_concat + counts[2]);
+  for (uint64_t cell : t.rec_concat) {
+    if (!std::binary_search(t.rec_unique.begin(), t.rec_unique.end(), cell))
+      return fail(c, DN_ERR_ARG, "concatenated receiving cell %llu is not a receiving cell", (unsigned long long)cell);
+  }
+  t.donor_idx.assign(donor_idx, donor_idx + counts[3]);
+  t.weight.assign(weight, weight + counts[3]);
+  int64_t off = 0;
+  for (int64_t q = 0; q < counts[1]; ++q) {
+    const size_t ncd = c->patches[donor_patch[q]].nc;
+    for (int64_t e = 0; e < num_receivers[q] * stride[q]; ++e) {
+      if (t.donor_idx[(size_t)(off + e)] >= ncd) return fail(c, DN_ERR_ARG, "donor cell index out of range");
+      if (!std::isfinite(t.weight[(size_t)(off + e)])) return fail(c, DN_ERR_ARG, "donor weight not finite");
+    }
+    off += num_receivers[q] * stride[q];
+  }
+  c->tables[id] = std::move(t);
+  c->plan_dirty = true;
+  return DN_OK;
+}
+
+int dn_copy_donor_data(dn_ctx* c, int field)
+{
+  if (!c) return DN_ERR_ARG;
+  int s;
+  if ((s = check_field(c, field))) return s;
+  if (set_device(c) != DN_OK) return DN_ERR_CUDA;
+  return donor_copy(c, c->fmap[field]);
 }
 
 int dn_launch_count(const dn_ctx* c, int64_t* count)

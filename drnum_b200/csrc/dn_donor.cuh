@@ -1,0 +1,36 @@
+// Device form of the donor tables of all patches of a context, and the
+// launchers of the donor copy (receiving cell <- weighted donor cells).
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace dn {
+
+// All receiving cells of all patches, each with its contributions grouped
+// by donor patch in table order (device pointers).
+struct DonorPlan {
+  int32_t n_recv;             // unique receiving cells over all patches
+  const int32_t* rv_patch;    // receiving patch per receiving cell
+  const int64_t* rv_cell;     // cell index in the receiving patch
+  const int32_t* rv_grp;      // [n_recv + 1] CSR offsets into the groups
+  const int32_t* gp_donor;    // donor patch per group
+  const int32_t* gp_stride;   // contributions per group
+  const int64_t* gp_wi;       // first contribution of the group in idx/w
+  const int64_t* idx;         // donor cell per contribution
+  const double* w;            // weight per contribution
+  void* const* bufs;          // [num_patches * 3] physical field buffers
+  const int64_t* nc;          // [num_patches] cells per patch
+  const double* base;         // [num_patches * 5] FP32-bulk base state
+  const double* quantum;      // [num_patches * 5] FP32-bulk quantum
+};
+
+// FP64 fields: recv = sum over donor patches of (sum over contributions of
+// donor * weight), with the reference's rounding order.
+cudaError_t launch_donor_copy_f64(const DonorPlan& p, int buf, cudaStream_t st);
+
+// int32 fixed-point fields (FP32 bulk): donors dequantised and summed in
+// FP64 with the FP64 weights, result quantised to the receiving patch.
+cudaError_t launch_donor_copy_fx32(const DonorPlan& p, int buf, int* err, cudaStream_t st);
+
+} // namespace dn

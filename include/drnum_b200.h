@@ -20,6 +20,8 @@
  *     (patchiterator.h:80-87, gpu_cartesianiterator.h:218-304)
  *   RungeKutta::operator()(dt) (rungekutta.cpp:27-42)        dn_rk_step
  *   Patch::computeVariableDifference (patch.cpp:733-746)     dn_field_difference
+ *   PatchGrid::computeDependencies (patchgrid.cpp:119-268)   dn_grid_compute_dependencies
+ *   PatchIterator::copyDonorData (patchiterator.h:106-111)   dn_copy_donor_data
  *
  * Conventions
  *   - Every call returns an int status: DN_OK (0) or a negative DN_ERR_*.
@@ -59,12 +61,19 @@ extern "C" {
 
 typedef struct dn_ctx dn_ctx;
 
-/* Geometry of one Cartesian patch (CartesianPatch: sizeI/J/K, dx/dy/dz, origin). */
+/* Geometry of one axis-aligned Cartesian patch (CartesianPatch::readFromFile,
+ * cartesianpatch.cpp:98-133: origin, NI NJ NK, seek layers per side, lengths). */
 typedef struct dn_patch_desc {
   int32_t ni, nj, nk;      /* cells per axis */
   int32_t face[3];         /* DN_FACE_* for the x, y and z axis */
-  double  dx, dy, dz;      /* cell spacing, as CartesianPatch::computeDeltas (cartesianpatch.cpp:160-165) */
+  double  dx, dy, dz;      /* cell spacing; ignored on an axis whose length[] is > 0 */
   double  origin[3];       /* lower corner in inertial coordinates */
+  double  length[3];       /* patch extent per axis; if > 0 the spacing is length/n, exactly
+                              as CartesianPatch::computeDeltas (cartesianpatch.cpp:160-165) */
+  int32_t seek[6];         /* receiving (seek) layers at imin, imax, jmin, jmax, kmin, kmax;
+                              0 = none (CartesianPatch::setSeekExceptions, cartesianpatch.cpp:146-157) */
+  int32_t add_protect;     /* additional protected layers next to the seek layers
+                              (PatchGrid::setNumAddProtectLayers, patchgrid.cpp:87-90) */
 } dn_patch_desc;
 
 /* Creates a context on CUDA device `device` with precision DN_FP64 or DN_FP32.
@@ -117,7 +126,8 @@ int dn_compute(dn_ctx* ctx, double factor);
 
 /* One full low-storage RK time step with stage factors alpha[0..n-1]*dt,
  * without the field 0 -> 1 copy (field 1 holds the step-start state after
- * the call, as after the reference's step).
+ * the call, as after the reference's step).  With donor tables it runs the
+ * reference's sequence: donor copy, then per stage compute + donor copy.
  * Replaces: RungeKutta::operator()(dt) (rungekutta.cpp:27-42). */
 int dn_rk_step(dn_ctx* ctx, double dt, const double* alpha, int n_alpha);
 
@@ -132,6 +142,61 @@ int dn_conservation_sums(dn_ctx* ctx, double out[5]);
  * Replaces: Patch::computeVariableDifference (patch.cpp:733-746). */
 int dn_field_difference(dn_ctx* ctx, int patch_id, int i_field1, int i_var1,
                         int i_field2, int i_var2, double* max_norm, double* l2_norm);
+
+/* Builds the donor tables of every patch from the patches' geometry and seek
+ * and protection layers: receiving cells, donor patches, 8-point trilinear
+ * donor stencils and weights, multi-donor averaging and padding.  Indices and
+ * FP64 weights equal the reference's.  *no_donor (may be NULL) receives the
+ * number of seek cells that found no donor; they are dropped, as the
+ * reference does after its warning (patch.cpp:370-395).
+ * Replaces: PatchGrid::computeDependencies(true) (patchgrid.cpp:119-268),
+ * Patch::finalizeDependencies / buildDonorTransferData (patch.cpp:319-465,128-218). */
+int dn_grid_compute_dependencies(dn_ctx* ctx, int64_t* no_donor);
+
+/* Sizes of a patch's donor tables: counts[0] unique receiving cells,
+ * counts[1] donor patches, counts[2] concatenated receiving cells,
+ * counts[3] concatenated contributions (Patch::getNumReceivingCellsUnique,
+ * getNumDonorPatches, getNumReceivingCellsConcat, getNumDonorWIConcat,
+ * patch_common.h:132-150). */
+int dn_patch_donor_counts(dn_ctx* ctx, int patch_id, int64_t counts[4]);
+
+/* Copies a patch's donor tables out, in the reference's direct-transfer
+ * layout (patch.cpp:128-218): rec_unique[counts[0]]; per donor
+ * donor_patch/num_receivers/stride[counts[1]]; rec_concat[counts[2]];
+ * donor_idx/weight[counts[3]]. */
+int dn_patch_get_donors(dn_ctx* ctx, int patch_id, uint64_t* rec_unique, int32_t* donor_patch,
+                        int64_t* num_receivers, int32_t* stride, uint64_t* rec_concat,
+                        uint64_t* donor_idx, double* weight);
+
+/* Sets a patch's donor tables built elsewhere (for example by the
+ * reference's PatchGrid), same layout as dn_patch_get_donors.  Donor patches
+ * are context patch ids.  Replaces: GPU_Patch's donor-table upload and
+ * updateDonorPointers (gpu_patch.h:43-129,142-173). */
+int dn_patch_set_donors(dn_ctx* ctx, int patch_id, const int64_t counts[4], const uint64_t* rec_unique,
+                        const int32_t* donor_patch, const int64_t* num_receivers, const int32_t* stride,
+                        const uint64_t* rec_concat, const uint64_t* donor_idx, const double* weight);
+
+/* Host-only form of dn_grid_compute_dependencies: builds the donor tables of
+ * np patch descriptions without a context or a GPU (patch ids are positions
+ * in `patches`).  Read them with dn_overlap_counts / dn_overlap_get (same
+ * layout as dn_patch_get_donors), hand them to a context with
+ * dn_patch_set_donors, free them with dn_overlap_destroy.
+ * Replaces: PatchGrid::computeDependencies(true) (patchgrid.cpp:119-268). */
+typedef struct dn_overlap dn_overlap;
+int dn_overlap_build(const dn_patch_desc* patches, int np, dn_overlap** out, int64_t* no_donor);
+int dn_overlap_counts(const dn_overlap* ov, int patch_id, int64_t counts[4]);
+int dn_overlap_get(const dn_overlap* ov, int patch_id, uint64_t* rec_unique, int32_t* donor_patch,
+                   int64_t* num_receivers, int32_t* stride, uint64_t* rec_concat,
+                   uint64_t* donor_idx, double* weight);
+int dn_overlap_destroy(dn_overlap* ov);
+
+/* Donor copy into field `field` of every patch: each receiving cell gets
+ * the weighted sum of its donor cells (per donor patch in table order, then
+ * summed over donor patches).  Patches are axis-aligned, so no vector
+ * rotation applies.  Replaces: PatchIterator::copyDonorData
+ * (patchiterator.h:106-111) -> Patch::accessDonorDataDirect (patch.cpp:573-653),
+ * GPU_PatchIterator::copyDonorData (gpu_patchiterator.h:190-233). */
+int dn_copy_donor_data(dn_ctx* ctx, int field);
 
 /* Number of device kernel launches the context has issued so far. */
 int dn_launch_count(const dn_ctx* ctx, int64_t* count);

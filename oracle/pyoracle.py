@@ -152,3 +152,144 @@ class RefSession:
 
     def __del__(self):
         self.close()
+
+
+# ------------------------------------------------------------------ patch grids
+
+def _grid_arrays(patches):
+    """patches: list of dicts with n (3), origin (3), length (3), seek (6)."""
+    n = np.ascontiguousarray([p["n"] for p in patches], dtype=np.int32).ravel()
+    o = np.ascontiguousarray([p["origin"] for p in patches], dtype=np.float64).ravel()
+    L = np.ascontiguousarray([p["length"] for p in patches], dtype=np.float64).ravel()
+    s = np.ascontiguousarray([p["seek"] for p in patches], dtype=np.int32).ravel()
+    return n, o, L, s
+
+
+class RefGrid:
+    """The reference's PatchGrid over axis-aligned Cartesian patches (compiled
+    reference library): donor tables from PatchGrid::computeDependencies and
+    RK steps with Patch::accessDonorDataDirect after every stage."""
+
+    def __init__(self, patches, add_protect=0, threads=1):
+        lib = ref_lib()
+        lib.dnref_grid_create.restype = c_void_p
+        lib.dnref_grid_create.argtypes = [c_int, POINTER(c_int), _P, _P, POINTER(c_int), c_int, c_int]
+        lib.dnref_grid_tables.restype = c_int
+        lib.dnref_grid_tables.argtypes = [c_void_p, c_int] + [c_void_p] * 8
+        for nm in ("dnref_grid_set_state", "dnref_grid_get_state"):
+            getattr(lib, nm).restype = c_int
+            getattr(lib, nm).argtypes = [c_void_p, c_int, _P]
+        lib.dnref_grid_copy_donor_data.restype = c_int
+        lib.dnref_grid_copy_donor_data.argtypes = [c_void_p, c_int]
+        lib.dnref_grid_run.restype = c_int
+        lib.dnref_grid_run.argtypes = [c_void_p, c_int, c_double, _P, c_int, _P]
+        lib.dnref_grid_destroy.restype = None
+        lib.dnref_grid_destroy.argtypes = [c_void_p]
+        self.lib = lib
+        self.patches = patches
+        n, o, L, s = _grid_arrays(patches)
+        self.h = lib.dnref_grid_create(len(patches), n.ctypes.data_as(POINTER(c_int)), o.ctypes.data_as(_P),
+                                       L.ctypes.data_as(_P), s.ctypes.data_as(POINTER(c_int)),
+                                       int(add_protect), int(threads))
+        if not self.h:
+            raise RuntimeError("reference grid creation failed")
+
+    def tables(self, p):
+        counts = np.zeros(4, dtype=np.int64)
+        rc = self.lib.dnref_grid_tables(self.h, p, counts.ctypes.data, None, None, None, None, None, None, None)
+        if rc != 0:
+            raise RuntimeError(f"reference tables failed: {rc}")
+        t = {"rec_unique": np.zeros(counts[0], np.uint64), "donor_patch": np.zeros(counts[1], np.int32),
+             "num_receivers": np.zeros(counts[1], np.int64), "stride": np.zeros(counts[1], np.int32),
+             "rec_concat": np.zeros(counts[2], np.uint64), "donor_idx": np.zeros(counts[3], np.uint64),
+             "weight": np.zeros(counts[3], np.float64)}
+        rc = self.lib.dnref_grid_tables(self.h, p, counts.ctypes.data, t["rec_unique"].ctypes.data,
+                                        t["donor_patch"].ctypes.data, t["num_receivers"].ctypes.data,
+                                        t["stride"].ctypes.data, t["rec_concat"].ctypes.data,
+                                        t["donor_idx"].ctypes.data, t["weight"].ctypes.data)
+        if rc != 0:
+            raise RuntimeError(f"reference tables failed: {rc}")
+        t["counts"] = counts
+        return t
+
+    def set_state(self, p, U):
+        U = np.ascontiguousarray(U, dtype=np.float64)
+        if self.lib.dnref_grid_set_state(self.h, p, U.ctypes.data_as(_P)) != 0:
+            raise RuntimeError("set_state failed")
+
+    def get_state(self, p):
+        n = self.patches[p]["n"]
+        U = np.empty((5, n[0], n[1], n[2]))
+        if self.lib.dnref_grid_get_state(self.h, p, U.ctypes.data_as(_P)) != 0:
+            raise RuntimeError("get_state failed")
+        return U
+
+    def copy_donor_data(self, field=0):
+        if self.lib.dnref_grid_copy_donor_data(self.h, field) != 0:
+            raise RuntimeError("copy_donor_data failed")
+
+    def run(self, steps, dt, alpha=(0.25, 0.5, 1.0)):
+        al = np.ascontiguousarray(alpha, dtype=np.float64)
+        sec = c_double()
+        rc = self.lib.dnref_grid_run(self.h, int(steps), float(dt), al.ctypes.data_as(_P), len(al), ctypes.byref(sec))
+        if rc != 0:
+            raise RuntimeError(f"reference grid run failed: {rc}")
+        return sec.value
+
+    def close(self):
+        if self.h:
+            self.lib.dnref_grid_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+
+def oracle_donor_copy(states, tables):
+    """Donor copy (Patch::accessDonorDataDirect, patch.cpp:573-653) over the
+    state list, in place: each receiving cell = sum over donor patches (table
+    order) of the donor's sum over contributions of U_donor * w."""
+    for r, t in enumerate(tables):
+        nu = len(t["rec_unique"])
+        if nu == 0:
+            continue
+        Ur = states[r].reshape(5, -1)
+        acc = {}
+        rc = 0
+        wi = 0
+        for q, d in enumerate(t["donor_patch"]):
+            m, s = int(t["num_receivers"][q]), int(t["stride"][q])
+            cells = t["rec_concat"][rc:rc + m].astype(np.int64)
+            idx = t["donor_idx"][wi:wi + m * s].astype(np.int64).reshape(m, s)
+            w = t["weight"][wi:wi + m * s].reshape(m, s)
+            Ud = states[int(d)].reshape(5, -1)
+            inter = np.zeros((5, m))
+            for k in range(s):
+                inter = inter + Ud[:, idx[:, k]] * w[:, k]
+            for j, c in enumerate(cells):
+                acc.setdefault(int(c), []).append(inter[:, j])
+            rc += m
+            wi += m * s
+        for c, parts in acc.items():
+            a = np.zeros(5)
+            for x in parts:
+                a = a + x
+            Ur[:, c] = a
+
+
+def oracle_grid_run(states, spacings, tables, dt, steps, alpha=(0.25, 0.5, 1.0)):
+    """RK steps of a patch grid with the C restatement of the residual
+    (closed patch faces) and the numpy donor copy, in the order of
+    RungeKutta::operator() (rungekutta.cpp:27-42).  Returns new states."""
+    U = [np.ascontiguousarray(s, dtype=np.float64).copy() for s in states]
+    for _ in range(steps):
+        oracle_donor_copy(U, tables)
+        Un = [u.copy() for u in U]
+        for a in alpha:
+            for p, u in enumerate(U):
+                hx, hy, hz = spacings[p]
+                res = oracle_residual(u, (hx, hy, hz), periodic=(False, False, False))
+                pf = (a * dt) / (hx * hy * hz)
+                U[p] = Un[p] + pf * res
+            oracle_donor_copy(U, tables)
+    return U

@@ -258,4 +258,135 @@ int dnref_max_threads()
 #endif
 }
 
+// ---------------------------------------------------------------- patch grids
+// A grid of axis-aligned Cartesian patches with overlap interpolation: the
+// reference's PatchGrid::computeDependencies builds the donor tables, and
+// RungeKutta + CartesianIterator + Patch::accessDonorDataDirect step it.
+// Patch faces carry zero flux (closed); receiving cells are overwritten by
+// the donor copy after every stage.
+struct DnRefGrid
+{
+  PatchGrid grid;
+  std::vector<CartesianPatch*> patches;
+  CartesianIterator<5, PeriodicFlux>* iterator = nullptr;
+};
+
+// n[3*np], origin[3*np], length[3*np], seek[6*np] (imin imax jmin jmax kmin kmax)
+void* dnref_grid_create(int np, const int* n, const double* origin, const double* length, const int* seek,
+                        int add_protect, int threads)
+{
+  if (sizeof(real) != 8 || np < 1) return nullptr;
+#ifdef OPEN_MP
+  if (threads > 0) omp_set_num_threads(threads);
+#endif
+  DnRefGrid* g = new DnRefGrid();
+  g->grid.setNumberOfFields(3);
+  g->grid.setNumberOfVariables(5);
+  g->grid.defineVectorVar(1);
+  g->grid.setInterpolateData();
+  g->grid.setNumSeekLayers(2);
+  g->grid.setNumAddProtectLayers(size_t(add_protect));
+  g->grid.setTransferType("padded_direct");
+  for (int p = 0; p < np; ++p) {
+    size_t sk[6];
+    for (int a = 0; a < 6; ++a) sk[a] = size_t(seek[6*p + a]);
+    g->patches.push_back(addPatch(g->grid, patchText(origin[3*p], origin[3*p+1], origin[3*p+2],
+                                                     n[3*p], n[3*p+1], n[3*p+2], sk,
+                                                     length[3*p], length[3*p+1], length[3*p+2])));
+  }
+  g->grid.computeDependencies(true);
+  return g;
+}
+
+// Donor tables of patch p.  counts[4] = {unique receiving cells, donor
+// patches, concatenated receiving cells, concatenated contributions}; the
+// arrays may be NULL (counts only).  donor_patch/num_receivers/stride have
+// one entry per donor patch.
+int dnref_grid_tables(void* handle, int p, long long* counts, unsigned long long* rec_unique,
+                      int* donor_patch, long long* num_receivers, int* stride, unsigned long long* rec_concat,
+                      unsigned long long* donor_idx, double* weight)
+{
+  DnRefGrid* g = (DnRefGrid*)handle;
+  if (!g || p < 0 || p >= int(g->patches.size())) return -1;
+  CartesianPatch* P = g->patches[p];
+  counts[0] = (long long)P->getNumReceivingCellsUnique();
+  counts[1] = (long long)P->getNumDonorPatches();
+  counts[2] = (long long)P->getNumReceivingCellsConcat();
+  counts[3] = (long long)P->getNumDonorWIConcat();
+  if (!rec_unique) return 0;
+  for (size_t i = 0; i < P->getNumReceivingCellsUnique(); ++i) rec_unique[i] = P->getReceivingCellIndicesUnique()[i];
+  for (size_t i = 0; i < P->getNumReceivingCellsConcat(); ++i) rec_concat[i] = P->getReceivingCellIndicesConcat()[i];
+  for (size_t i = 0; i < P->getNumDonorWIConcat(); ++i) {
+    donor_idx[i] = P->getDonorIndexConcat()[i];
+    weight[i] = P->getDonorWeightConcat()[i];
+  }
+  for (size_t d = 0; d < P->getNumDonorPatches(); ++d) {
+    const donor_t& dn = P->getDonors()[d];
+    int idx = -1;
+    for (size_t q = 0; q < g->patches.size(); ++q) if (g->patches[q]->getField(0) == dn.data) idx = int(q);
+    donor_patch[d] = idx;
+    num_receivers[d] = (long long)dn.num_receiver_cells;
+    stride[d] = int(dn.stride);
+    const bool identity = dn.axx == 1 && dn.ayy == 1 && dn.azz == 1 && dn.axy == 0 && dn.axz == 0 &&
+                          dn.ayx == 0 && dn.ayz == 0 && dn.azx == 0 && dn.azy == 0;
+    if (!identity) return -2;   // axis-aligned patches only
+  }
+  return 0;
+}
+
+// Field 0 of patch p, [5][ni][nj][nk].
+int dnref_grid_set_state(void* handle, int p, const double* U)
+{
+  DnRefGrid* g = (DnRefGrid*)handle;
+  if (!g || p < 0 || p >= int(g->patches.size())) return -1;
+  CartesianPatch* P = g->patches[p];
+  const size_t n = P->sizeI()*P->sizeJ()*P->sizeK();
+  for (size_t v = 0; v < 5; ++v)
+    for (size_t c = 0; c < n; ++c) P->getVariable(0, v)[c] = U[v*n + c];
+  return 0;
+}
+
+int dnref_grid_get_state(void* handle, int p, double* U)
+{
+  DnRefGrid* g = (DnRefGrid*)handle;
+  if (!g || p < 0 || p >= int(g->patches.size())) return -1;
+  CartesianPatch* P = g->patches[p];
+  const size_t n = P->sizeI()*P->sizeJ()*P->sizeK();
+  for (size_t v = 0; v < 5; ++v)
+    for (size_t c = 0; c < n; ++c) U[v*n + c] = P->getVariable(0, v)[c];
+  return 0;
+}
+
+// Donor copy into field `field` of every patch (PatchIterator::copyDonorData).
+int dnref_grid_copy_donor_data(void* handle, int field)
+{
+  DnRefGrid* g = (DnRefGrid*)handle;
+  if (!g) return -1;
+  for (size_t p = 0; p < g->patches.size(); ++p) g->patches[p]->accessDonorDataDirect(size_t(field));
+  return 0;
+}
+
+// `steps` RK steps of all patches; *seconds = time of RungeKutta::operator() only.
+int dnref_grid_run(void* handle, int steps, double dt, const double* alpha, int n_alpha, double* seconds)
+{
+  DnRefGrid* g = (DnRefGrid*)handle;
+  if (!g || n_alpha < 1) return -1;
+  PeriodicFlux flux;
+  CartesianIterator<5, PeriodicFlux> iterator(flux);
+  for (size_t p = 0; p < g->patches.size(); ++p) iterator.addPatch(g->patches[p]);
+  RungeKutta rk;
+  for (int a = 0; a < n_alpha; ++a) rk.addAlpha(alpha[a]);
+  rk.addIterator(&iterator);
+  auto t0 = std::chrono::steady_clock::now();
+  for (int s = 0; s < steps; ++s) rk(dt);
+  auto t1 = std::chrono::steady_clock::now();
+  if (seconds) *seconds = std::chrono::duration<double>(t1 - t0).count();
+  return 0;
+}
+
+void dnref_grid_destroy(void* handle)
+{
+  delete (DnRefGrid*)handle;
+}
+
 } // extern "C"

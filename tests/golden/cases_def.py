@@ -49,3 +49,46 @@ def build(name):
 # full-field fixtures (small); the 64^3 x 100 case stores a digest
 FULL = ["rough_8", "ragged_12x10x9", "vortex_16", "closed_10x7x12", "masked_9", "thin_3x5x4"]
 DIGEST = ["cfg1_64_100"]
+
+
+# ------------------------------------------------------------------ patch grids
+
+def grid_layout(name):
+    """Patch layouts of the donor-table fixtures (list of patch dicts)."""
+    if name == "pair_x":
+        return [dict(n=(12, 8, 8), origin=(0.0, 0.0, 0.0), length=(1.2, 0.8, 0.8), seek=(0, 2, 0, 0, 0, 0)),
+                dict(n=(12, 8, 8), origin=(0.8, 0.0, 0.0), length=(1.2, 0.8, 0.8), seek=(2, 0, 0, 0, 0, 0))]
+    if name == "embedded":
+        return [dict(n=(10, 10, 10), origin=(0.0, 0.0, 0.0), length=(1.0, 1.0, 1.0), seek=(2, 2, 2, 2, 2, 2)),
+                dict(n=(16, 16, 16), origin=(0.3, 0.27, 0.31), length=(0.4, 0.4, 0.4), seek=(2, 2, 2, 2, 2, 2))]
+    if name in ("random6", "random6_prot1"):
+        rng = np.random.default_rng(3)
+        out = []
+        for p in range(6):
+            n = tuple(int(x) for x in rng.integers(6, 14, 3))
+            if name == "random6_prot1":
+                n = tuple(max(x, 9) for x in n)
+            h = [0.1, 0.05][p % 2]
+            out.append(dict(n=n, origin=tuple(float(x) for x in rng.uniform(0, 0.6, 3)),
+                            length=tuple(h * x for x in n), seek=(2, 2, 2, 2, 2, 2)))
+        return out
+    if name == "octants_8":
+        return cases.octant_grid(nf=(8, 8, 8), h=1.0 / 16, overlap=3, seek=2)
+    if name == "octants_ragged":
+        return cases.octant_grid(nf=(12, 8, 10), h=1.0 / 24, overlap=4, seek=2)
+    raise KeyError(name)
+
+
+GRID_ADD_PROTECT = {"random6_prot1": 1}
+# layouts whose donor tables are fixtures; the octant grids also store RK steps
+GRID_TABLES = ["pair_x", "embedded", "random6", "random6_prot1", "octants_8", "octants_ragged"]
+GRID_STEPS = {"octants_8": 3, "octants_ragged": 2}
+
+
+def grid_case(name):
+    """Layout, initial states, spacings and time step of a stepped grid case."""
+    patches = grid_layout(name)
+    states = cases.grid_state(patches)
+    dt = cases.grid_dt(patches, states)
+    spacings = [tuple(p["length"][a] / p["n"][a] for a in range(3)) for p in patches]
+    return patches, states, spacings, dt, GRID_STEPS[name]

@@ -55,7 +55,38 @@ def main():
         print(f"{name}: {sec:.3f} s")
     with open(os.path.join(HERE, "digests.json"), "w") as f:
         json.dump(meta, f, indent=1)
+    make_grids()
+
+
+def make_grids():
+    """Donor tables of the reference's PatchGrid::computeDependencies for the
+    grid layouts, and the reference's multi-patch RK steps (RungeKutta +
+    CartesianIterator + Patch::accessDonorDataDirect) for the octant grids."""
+    for name in cases_def.GRID_TABLES:
+        patches = cases_def.grid_layout(name)
+        g = pyoracle.RefGrid(patches, cases_def.GRID_ADD_PROTECT.get(name, 0), threads=1)
+        arrays = {}
+        for p in range(len(patches)):
+            t = g.tables(p)
+            for k, v in t.items():
+                arrays[f"p{p}_{k}"] = v
+        if name in cases_def.GRID_STEPS:
+            _, states, _, dt, steps = cases_def.grid_case(name)
+            for p, U in enumerate(states):
+                g.set_state(p, U)
+            g.run(steps, dt, cases_def.ALPHA)
+            for p in range(len(patches)):
+                arrays[f"p{p}_out"] = g.get_state(p)
+            arrays["dt"] = np.array(dt)
+            arrays["steps"] = np.array(steps)
+        g.close()
+        arrays["num_patches"] = np.array(len(patches))
+        np.savez_compressed(os.path.join(HERE, f"grid_{name}.npz"), **arrays)
+        print(f"grid_{name}: {len(patches)} patches")
 
 
 if __name__ == "__main__":
-    main()
+    if "--grids" in sys.argv:
+        make_grids()
+    else:
+        main()

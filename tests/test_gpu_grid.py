@@ -1,0 +1,152 @@
+"""Multi-patch (overlap) path on the GPU through the C ABI: donor tables on
+the context, the donor copy kernel and RK steps of a dual-resolution grid,
+against the reference's own outputs (tests/golden/grid_*.npz) and the oracle."""
+import ctypes
+import os
+
+import numpy as np
+import pytest
+
+import cases_def
+import pyoracle
+from drnum_b200 import _lib, cases
+from drnum_b200._lib import DN_FP32, DN_FP64
+from drnum_b200.api import AusmPlus, B200CartesianIterator, CartesianPatch, PatchGrid, RungeKutta
+
+pytestmark = pytest.mark.gpu
+
+TABLE_KEYS = ("rec_unique", "donor_patch", "num_receivers", "stride", "rec_concat", "donor_idx", "weight")
+# FP32 bulk against FP64 on the grid: relative to the free-stream scale
+F32_GRID_L2_TOL = 1e-5
+F32_GRID_LINF_TOL = 1e-4
+
+
+def _fixture(golden_dir, name):
+    return np.load(os.path.join(golden_dir, f"grid_{name}.npz"))
+
+
+def make_grid(name, precision, states=None):
+    patches, st0, spacings, dt, steps = cases_def.grid_case(name)
+    states = st0 if states is None else states
+    grid = PatchGrid()
+    objs = []
+    for p, U in zip(patches, states):
+        cp = CartesianPatch(*p["n"], lengths=p["length"], origin=p["origin"], periodic=(False, False, False),
+                            seek=p["seek"])
+        cp.setField(0, U)
+        grid.insertPatch(cp)
+        objs.append(cp)
+    grid.computeDependencies()
+    it = B200CartesianIterator(AusmPlus(), 0, precision)
+    for cp in objs:
+        it.addPatch(cp)
+    it.updateDevice(fields=(0,))
+    return it, objs, grid, dt, steps
+
+
+@pytest.mark.parametrize("name", sorted(cases_def.GRID_STEPS))
+def test_grid_fp64_bitwise_vs_reference(golden_dir, name):
+    z = _fixture(golden_dir, name)
+    it, objs, _, dt, steps = make_grid(name, DN_FP64)
+    for _ in range(steps):
+        it.rkStep(dt, cases.RK3_ALPHA)
+    it.updateHost(fields=(0,))
+    it.close()
+    for p, cp in enumerate(objs):
+        ref = z[f"p{p}_out"]
+        assert np.array_equal(cp.getField(0), ref), (name, p, np.abs(cp.getField(0) - ref).max())
+
+
+def test_context_tables_equal_reference(golden_dir):
+    z = _fixture(golden_dir, "octants_ragged")
+    it, objs, _, _, _ = make_grid("octants_ragged", DN_FP64)
+    assert it.computeDependencies() == 0          # rebuilt on the context from the patch descriptions
+    for p in range(len(objs)):
+        t = it.donorTables(p)
+        for k in TABLE_KEYS:
+            a, b = t[k], z[f"p{p}_{k}"]
+            if a.dtype == np.float64:
+                a, b = a.view(np.uint64), b.view(np.uint64)
+            assert np.array_equal(a, b), (p, k)
+    it.close()
+
+
+def test_donor_copy_matches_oracle():
+    patches, _, _, _, _ = cases_def.grid_case("octants_8")
+    rng = np.random.default_rng(7)
+    states = [cases.random_state(*p["n"], seed=int(rng.integers(1 << 30)), amp=0.02) for p in patches]
+    it, objs, grid, _, _ = make_grid("octants_8", DN_FP64, states)
+    it.copyDonorData(0)
+    it.updateHost(fields=(0,))
+    it.close()
+    expect = [s.copy() for s in states]
+    pyoracle.oracle_donor_copy(expect, grid.tables)
+    for p, cp in enumerate(objs):
+        assert np.array_equal(cp.getField(0), expect[p]), p
+
+
+def test_grid_stagewise_api_equals_fused_step(golden_dir):
+    name = "octants_8"
+    z = _fixture(golden_dir, name)
+    it, objs, _, dt, steps = make_grid(name, DN_FP64)
+    rk = RungeKutta()
+    for a in cases.RK3_ALPHA:
+        rk.addAlpha(a)
+    rk.addIterator(it)
+    rk.addPostOperation(lambda: None)    # forces the reference's stage-by-stage sequence
+    for _ in range(steps):
+        rk(dt)
+    it.updateHost(fields=(0,))
+    it.close()
+    for p, cp in enumerate(objs):
+        assert np.array_equal(cp.getField(0), z[f"p{p}_out"]), p
+
+
+def test_grid_fp32_against_fp64():
+    name = "octants_ragged"
+    steps = 6
+    out = {}
+    for prec in (DN_FP64, DN_FP32):
+        it, objs, _, dt, _ = make_grid(name, prec)
+        for _ in range(steps):
+            it.rkStep(dt, cases.RK3_ALPHA)
+        it.updateHost(fields=(0,))
+        it.close()
+        out[prec] = [cp.getField(0).copy() for cp in objs]
+    scale = np.array([cases.RHO_INF, cases.RHO_INF * cases.A_INF, cases.RHO_INF * cases.A_INF,
+                      cases.RHO_INF * cases.A_INF, cases.RHO_INF * cases.A_INF ** 2])[:, None, None, None]
+    for a, b in zip(out[DN_FP32], out[DN_FP64]):
+        d = (a - b) / scale
+        l2 = np.sqrt((d ** 2).reshape(5, -1).mean(1))
+        assert l2.max() < F32_GRID_L2_TOL, l2
+        assert np.abs(d).max() < F32_GRID_LINF_TOL
+
+
+def test_set_donors_rejects_invalid_tables(golden_dir):
+    z = _fixture(golden_dir, "pair_x")
+    patches = cases_def.grid_layout("pair_x")
+    it = B200CartesianIterator(AusmPlus(), 0, DN_FP64)
+    for p in patches:
+        it.addPatch(CartesianPatch(*p["n"], lengths=p["length"], origin=p["origin"],
+                                   periodic=(False, False, False), seek=p["seek"]))
+    lib, ctx = it.lib, it.ctx
+
+    def call(t):
+        counts = np.ascontiguousarray(t["counts"], dtype=np.int64)
+        arrs = [np.ascontiguousarray(t[k]) for k in TABLE_KEYS]
+        types = [c for _, _, c, _ in _lib.DONOR_FIELDS]
+        return lib.dn_patch_set_donors(ctx, 0, _lib.ptr(counts, ctypes.c_int64),
+                                       *[_lib.ptr(a, ct) for a, ct in zip(arrs, types)])
+
+    good = {k: z[f"p0_{k}"].copy() for k in TABLE_KEYS + ("counts",)}
+    assert call(good) == _lib.DN_OK
+    bad = {k: v.copy() for k, v in good.items()}
+    bad["donor_patch"][0] = 0                      # a patch cannot be its own donor
+    assert call(bad) == _lib.DN_ERR_ARG
+    bad = {k: v.copy() for k, v in good.items()}
+    bad["donor_idx"][0] = 10 ** 9                  # donor cell outside the donor patch
+    assert call(bad) == _lib.DN_ERR_ARG
+    bad = {k: v.copy() for k, v in good.items()}
+    bad["rec_unique"] = bad["rec_unique"][::-1].copy()   # not ascending
+    assert call(bad) == _lib.DN_ERR_ARG
+    it.close()

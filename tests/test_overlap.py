@@ -1,0 +1,139 @@
+"""Overlap set-up (donor tables) and the oracle's multi-patch step against the
+reference (CPU only).
+
+The fixtures tests/golden/grid_*.npz hold the reference's own donor tables
+(PatchGrid::computeDependencies, patchgrid.cpp:119-268) and, for the octant
+grids, its multi-patch RK steps; they are generated from the compiled
+reference by tests/golden/make_golden.py --grids.
+"""
+import ctypes
+import os
+
+import numpy as np
+import pytest
+
+import cases_def
+import pyoracle
+from drnum_b200 import _lib
+
+TABLE_KEYS = ("rec_unique", "donor_patch", "num_receivers", "stride", "rec_concat", "donor_idx", "weight")
+
+
+def _descs(patches, add_protect=0):
+    arr = (_lib.dn_patch_desc * len(patches))()
+    for d, p in zip(arr, patches):
+        d.ni, d.nj, d.nk = p["n"]
+        for a in range(3):
+            d.face[a] = _lib.DN_FACE_CLOSED
+            d.origin[a] = p["origin"][a]
+            d.length[a] = p["length"][a]
+        for a in range(6):
+            d.seek[a] = p["seek"][a]
+        d.add_protect = add_protect
+    return arr
+
+
+def build_tables(patches, add_protect=0):
+    lib = _lib.load()
+    h = ctypes.c_void_p()
+    nd = ctypes.c_int64()
+    rc = lib.dn_overlap_build(_descs(patches, add_protect), len(patches), ctypes.byref(h), ctypes.byref(nd))
+    assert rc == _lib.DN_OK
+    try:
+        return [_lib.read_donor_tables(lib.dn_overlap_counts, lib.dn_overlap_get, h, p)
+                for p in range(len(patches))], nd.value
+    finally:
+        lib.dn_overlap_destroy(h)
+
+
+def _same(a, b):
+    a, b = np.asarray(a), np.asarray(b)
+    if a.shape != b.shape:
+        return False
+    if a.dtype == np.float64:
+        return np.array_equal(a.view(np.uint64), b.view(np.uint64))   # bit for bit
+    return np.array_equal(a, b)
+
+
+def _fixture(golden_dir, name):
+    return np.load(os.path.join(golden_dir, f"grid_{name}.npz"))
+
+
+@pytest.mark.parametrize("name", cases_def.GRID_TABLES)
+def test_donor_tables_equal_reference_fixtures(golden_dir, name):
+    z = _fixture(golden_dir, name)
+    patches = cases_def.grid_layout(name)
+    mine, _ = build_tables(patches, cases_def.GRID_ADD_PROTECT.get(name, 0))
+    for p in range(len(patches)):
+        for k in TABLE_KEYS + ("counts",):
+            assert _same(mine[p][k], z[f"p{p}_{k}"]), (name, p, k)
+
+
+@pytest.mark.skipif(not pyoracle.ref_available(), reason="compiled reference (oracle/_ref) not built")
+@pytest.mark.parametrize("seed", [11, 12, 13])
+def test_donor_tables_equal_live_reference(seed):
+    rng = np.random.default_rng(seed)
+    patches = []
+    for p in range(5):
+        n = tuple(int(x) for x in rng.integers(8, 16, 3))
+        h = float(rng.choice([0.1, 0.05, 0.025]))
+        seek = tuple(int(x) for x in rng.integers(0, 3, 6))
+        patches.append(dict(n=n, origin=tuple(float(x) for x in rng.uniform(0, 0.5, 3)),
+                            length=tuple(h * x for x in n), seek=seek))
+    ref = pyoracle.RefGrid(patches, 0)
+    mine, _ = build_tables(patches)
+    for p in range(len(patches)):
+        t = ref.tables(p)
+        for k in TABLE_KEYS:
+            assert _same(mine[p][k], t[k]), (seed, p, k)
+
+
+@pytest.mark.parametrize("name", ["octants_8", "octants_ragged"])
+def test_octant_grids_leave_no_seek_cell_without_donor(name):
+    _, nd = build_tables(cases_def.grid_layout(name))
+    assert nd == 0
+
+
+@pytest.mark.parametrize("name", sorted(cases_def.GRID_STEPS))
+def test_oracle_grid_steps_equal_reference(golden_dir, name):
+    z = _fixture(golden_dir, name)
+    patches, states, spacings, dt, steps = cases_def.grid_case(name)
+    assert float(z["dt"]) == dt and int(z["steps"]) == steps
+    tables = [{k: z[f"p{p}_{k}"] for k in TABLE_KEYS} for p in range(len(patches))]
+    out = pyoracle.oracle_grid_run(states, spacings, tables, dt, steps, cases_def.ALPHA)
+    for p in range(len(patches)):
+        assert np.array_equal(out[p], z[f"p{p}_out"]), (name, p, np.abs(out[p] - z[f"p{p}_out"]).max())
+
+
+def test_oracle_donor_copy_detects_planted_weight_error(golden_dir):
+    # a weight changed in the oracle's tables changes the interpolated cells
+    z = _fixture(golden_dir, "octants_8")
+    patches, states, _, _, _ = cases_def.grid_case("octants_8")
+    tables = [{k: z[f"p{p}_{k}"].copy() for k in TABLE_KEYS} for p in range(len(patches))]
+    a = [s.copy() for s in states]
+    pyoracle.oracle_donor_copy(a, tables)
+    tables[0]["weight"][0] *= 1.0 + 1e-9
+    b = [s.copy() for s in states]
+    pyoracle.oracle_donor_copy(b, tables)
+    assert not np.array_equal(a[0], b[0])
+
+
+def test_degenerate_donor_zone_is_reported():
+    # a donor zone one cell wide: the reference stops with a BUG
+    # (cartesianpatch.cpp:1146-1151); the set-up returns an error instead
+    patches = [dict(n=(6, 6, 6), origin=(0.0, 0.0, 0.0), length=(0.6, 0.6, 0.6), seek=(2, 2, 2, 2, 2, 2)),
+               dict(n=(6, 6, 6), origin=(0.15, 0.15, 0.15), length=(0.6, 0.6, 0.6), seek=(2, 2, 2, 2, 2, 2))]
+    lib = _lib.load()
+    h = ctypes.c_void_p()
+    rc = lib.dn_overlap_build(_descs(patches, 1), 2, ctypes.byref(h), None)
+    assert rc == _lib.DN_ERR_ARG and not h.value
+
+
+def test_overlap_build_rejects_invalid_layouts():
+    lib = _lib.load()
+    h = ctypes.c_void_p()
+    bad = [dict(n=(4, 4, 4), origin=(0.0, 0.0, 0.0), length=(0.4, 0.4, 0.4), seek=(3, 3, 0, 0, 0, 0))]
+    assert lib.dn_overlap_build(_descs(bad), 1, ctypes.byref(h), None) == _lib.DN_ERR_ARG
+    assert lib.dn_overlap_build(None, 1, ctypes.byref(h), None) == _lib.DN_ERR_ARG
+    assert lib.dn_overlap_build(_descs(bad), 0, ctypes.byref(h), None) == _lib.DN_ERR_ARG
+    assert lib.dn_overlap_counts(None, 0, None) == _lib.DN_ERR_ARG
