@@ -27,6 +27,11 @@ DN_FP32 = 1
 DN_FACE_PERIODIC = 0
 DN_FACE_CLOSED = 1
 
+DN_BC_ZERO_FLUX = 0
+DN_BC_FARFIELD = 1
+DN_BC_SLIP = 2
+DN_BC_INFLOW = 3
+
 
 class dn_patch_desc(ctypes.Structure):
     _fields_ = [
@@ -75,6 +80,7 @@ SIGNATURES = {
                                POINTER(c_int32), POINTER(c_uint64), POINTER(c_uint64), POINTER(c_double)]),
     "dn_overlap_destroy": (c_int, [c_void_p]),
     "dn_copy_donor_data": (c_int, [c_void_p, c_int]),
+    "dn_patch_set_bc": (c_int, [c_void_p, c_int, c_int, c_int, POINTER(c_double), POINTER(c_double)]),
 }
 
 _lib = None

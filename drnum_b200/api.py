@@ -96,6 +96,8 @@ class CartesianPatch:
         self.add_protect = int(add_protect)
         self.grid = None
         self.grid_index = None
+        # patch-face fluxes per side: (kind, params, table), see setBoundary
+        self.bcs = {}
         self.m_NumFields = num_fields
         self.data = np.zeros((num_fields, 5, ni, nj, nk))
         self.active = np.ones((ni, nj, nk), dtype=np.uint8)
@@ -119,6 +121,17 @@ class CartesianPatch:
 
     def setField(self, i_field, values):
         self.data[i_field][...] = values
+
+    def setBoundary(self, side, kind, params=None, table=None):
+        """Flux functor wall method of side 0..5 (x-min, x-max, y-min, y-max,
+        z-min, z-max): DN_BC_ZERO_FLUX, DN_BC_FARFIELD (params p, T, u, v, w:
+        CompressibleFarfieldFlux::setFarfield, compressiblefarfieldflux.h:87-90),
+        DN_BC_SLIP (CompressibleSlipFlux) or DN_BC_INFLOW (a per-face table
+        {p or NaN, T, u, v, w}, the JetFlux::xWallM form)."""
+        if self.periodic[side // 2]:
+            raise ValueError(f"axis {side // 2} is periodic")
+        self.bcs[int(side)] = (int(kind), None if params is None else tuple(float(x) for x in params),
+                               None if table is None else np.ascontiguousarray(table, dtype=np.float64))
 
     def deactivate(self, i, j, k): self.active[i, j, k] = 0
     def activate(self, i, j, k): self.active[i, j, k] = 1
@@ -270,8 +283,18 @@ class B200CartesianIterator:
     def donorTables(self, i_patch):
         return _lib.read_donor_tables(self.lib.dn_patch_donor_counts, self.lib.dn_patch_get_donors, self.ctx, i_patch)
 
+    def setBoundaries(self):
+        """Hands every patch's side fluxes to the device (dn_patch_set_bc)."""
+        for pid, p in enumerate(self.m_Patches):
+            for side, (kind, params, table) in sorted(p.bcs.items()):
+                pa = None if params is None else np.ascontiguousarray(params, dtype=np.float64)
+                check(self.ctx, self.lib.dn_patch_set_bc(self.ctx, pid, side, kind,
+                                                         None if pa is None else _lib.dptr(pa),
+                                                         None if table is None else _lib.dptr(table)))
+
     def updateDevice(self, fields=(0, 1)):
         self.setDonorTables()
+        self.setBoundaries()
         for pid, p in enumerate(self.m_Patches):
             for f in fields:
                 a = np.ascontiguousarray(p.data[f], dtype=np.float64)

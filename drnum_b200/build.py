@@ -30,7 +30,7 @@ COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-I", INCLUDE
 
 # translation unit -> extra flags
 UNITS = {
-    "dn_api.cu": [],
+    "dn_api.cu": ["-Xcompiler", "-ffp-contract=off"],
     "fv_fp64.cu": ["-fmad=false"],
     "fv_fx32.cu": ["-use_fast_math", "-fmad=false"],
     "dn_noalloc.cu": [],

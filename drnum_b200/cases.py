@@ -187,3 +187,68 @@ def grid_state(patches, mach=0.3, beta=5.0, radius=0.1, centre=(0.25, 0.25, 0.25
 def grid_dt(patches, states, cfl=0.5):
     """One global time step: cfl * min over patches of h / max(|u| + a)."""
     return min(cfl_dt(U, min(p["length"][a] / p["n"][a] for a in range(3)), cfl) for p, U in zip(patches, states))
+
+
+# ------------------------------------------------------------ patch-face fluxes
+#
+# Boundary conditions of a grid: {patch: {side: (kind, params, table)}} with
+# side 0..5 = x-min, x-max, y-min, y-max, z-min, z-max and kind as DN_BC_*
+# (0 zero flux, 1 far field with params p, T, u, v, w, 2 slip wall, 3 face
+# table [faces][5] = p (NaN: boundary cell), T, u, v, w).
+
+BC_ZERO, BC_FARFIELD, BC_SLIP, BC_INFLOW = 0, 1, 2, 3
+
+
+def iterator_face_coords(n, h):
+    """Face-centre coordinates along one axis of a patch side as the
+    reference's wall loops produce them: start at h/2 and add h per face
+    (cartesianiterator.h:193-207)."""
+    out = np.empty(n)
+    c = 0.5 * h
+    for q in range(n):
+        out[q] = c
+        c += h
+    return out
+
+
+def jet_table(patch, u_jet, T_jet, radius, u_far=0.0, T_far=T_INF, p_jet=None, noise=0.0, seed=1234):
+    """Face table of a top-hat jet on the x-min side of `patch`, the state
+    JetFlux::xWallM prescribes (applications/drnumJetDemo/jetflux.h:165-191):
+    inside radius (around the side's centre, patch coordinates) u = u_jet,
+    T = T_jet and p = p_jet or the boundary cell's; outside u = u_far,
+    T = T_far, p from the boundary cell.  `noise` adds seeded white noise of
+    that relative amplitude (times u_jet) to the jet's u, v, w."""
+    ni, nj, nk = patch["n"]
+    dy, dz = patch["length"][1] / nj, patch["length"][2] / nk
+    y, z = iterator_face_coords(nj, dy), iterator_face_coords(nk, dz)
+    y0, z0 = 0.5 * nj * dy, 0.5 * nk * dz
+    rr = (y[:, None] - y0) ** 2 + (z[None, :] - z0) ** 2
+    inside = rr < radius * radius
+    rng = np.random.default_rng(seed)
+    t = np.empty((nj, nk, 5))
+    t[..., 0] = np.nan
+    t[..., 1] = np.where(inside, T_jet, T_far)
+    t[..., 2] = np.where(inside, u_jet, u_far)
+    t[..., 3] = 0.0
+    t[..., 4] = 0.0
+    if p_jet is not None:
+        t[..., 0] = np.where(inside, p_jet, np.nan)
+    if noise:
+        pert = noise * u_jet * rng.uniform(-1.0, 1.0, (nj, nk, 3))
+        t[..., 2:5] += np.where(inside[..., None], pert, 0.0)
+    return t.reshape(-1, 5)
+
+
+def outer_farfield_bcs(patches, state=(P_INF, T_INF, 0.0, 0.0, 0.0)):
+    """Far field on every side of every patch that has no seek layers."""
+    return {p: {side: (BC_FARFIELD, tuple(state), None) for side in range(6) if patch["seek"][side] == 0}
+            for p, patch in enumerate(patches)}
+
+
+def jet_bcs(patches, core=0, mach_jet=0.8, radius=0.05, noise=1e-3, seed=1234):
+    """Far field at rest on the outer sides and a top-hat jet of Mach
+    `mach_jet` on the x-min side of patch `core`."""
+    bcs = outer_farfield_bcs(patches)
+    bcs[core][0] = (BC_INFLOW, None, jet_table(patches[core], mach_jet * A_INF, T_INF, radius, noise=noise,
+                                               seed=seed))
+    return bcs

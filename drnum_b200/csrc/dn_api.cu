@@ -32,6 +32,7 @@ struct DnPatch {
   double base[5] = {0, 0, 0, 0, 0};
   double quantum[5] = {1, 1, 1, 1, 1};
   bool base_set = false;
+  dn::WallBC wall{};                        // device view (table pointers are device memory)
 };
 
 } // namespace
@@ -472,6 +473,7 @@ int stage_patch(dn_ctx* c, DnPatch& p, int in_b, int un_b, int out_b, double fac
     g.i_chunk = dn::default_i_chunk(g.ni, g.nj, g.nk, 4, 32, c->num_sms, 3);
     a.g = g;
     a.p.Ax = dy * dz; a.p.Ay = dx * dz; a.p.Az = dx * dy; a.p.pf = pf;
+    a.wall = p.wall;
     e = dn::launch_stage_f64(a, dn::StageShape{4, 32, g.i_chunk}, c->stream);
   } else {
     dn::FxArgs a;
@@ -492,6 +494,7 @@ int stage_patch(dn_ctx* c, DnPatch& p, int in_b, int un_b, int out_b, double fac
       a.p.quantum[v] = (float)p.quantum[v];
       a.p.face_scale[v] = (float)(pf / p.quantum[v]);
     }
+    a.wall = p.wall;
     e = dn::launch_stage_fx32(a, c->stream);
   }
   c->launches++;
@@ -603,6 +606,7 @@ int dn_ctx_destroy(dn_ctx* c)
   for (auto& p : c->patches) {
     for (int b = 0; b < 3; ++b) if (p.buf[b]) cudaFree(p.buf[b]);
     if (p.active) cudaFree(p.active);
+    for (int sd = 0; sd < 6; ++sd) if (p.wall.table[sd]) cudaFree((void*)p.wall.table[sd]);
   }
   free_plan(c);
   if (c->staging) cudaFree(c->staging);
@@ -868,6 +872,67 @@ int dn_field_difference(dn_ctx* c, int id, int f1, int v1, int f2, int v2, doubl
   }
   *max_norm = std::sqrt(mx);
   *l2_norm = std::sqrt(sm);
+  return DN_OK;
+}
+
+int dn_patch_set_bc(dn_ctx* c, int id, int side, int kind, const double* params, const double* table)
+{
+  int s = check_patch(c, id);
+  if (s) return s;
+  if (side < 0 || side > 5) return fail(c, DN_ERR_ARG, "side %d is not 0..5", side);
+  DnPatch& P = c->patches[id];
+  const int axis = side / 2;
+  if (P.d.face[axis] == DN_FACE_PERIODIC) return fail(c, DN_ERR_ARG, "axis %d of patch %d is periodic", axis, id);
+  if (kind != DN_BC_ZERO_FLUX && kind != DN_BC_FARFIELD && kind != DN_BC_SLIP && kind != DN_BC_INFLOW)
+    return fail(c, DN_ERR_ARG, "unknown boundary kind %d", kind);
+  if (set_device(c) != DN_OK) return DN_ERR_CUDA;
+  if (kind == DN_BC_FARFIELD) {
+    if (!params) return fail(c, DN_ERR_ARG, "far field needs p, T, u, v, w");
+    for (int q = 0; q < 5; ++q) if (!std::isfinite(params[q])) return fail(c, DN_ERR_ARG, "far-field value not finite");
+    if (!(params[0] > 0) || !(params[1] > 0)) return fail(c, DN_ERR_ARG, "far-field p and T must be positive");
+    // CompressibleFarfieldFlux::setFarfield stores the conservative state
+    // (perfectgas.h:58-66); its wall methods convert it back (perfectgas.h:84-93)
+    const double pp = params[0], T = params[1], u = params[2], v = params[3], w = params[4];
+    const double R = 287.2, cv = 717.5, gamma = 1.4;
+    double var[5];
+    var[0] = pp / (R * T);
+    var[1] = var[0] * u;
+    var[2] = var[0] * v;
+    var[3] = var[0] * w;
+    var[4] = var[0] * (cv * T + 0.5 * (u * u + v * v + w * w));
+    const double ir = 1.0 / var[0];
+    const double u0 = var[1] * ir, v0 = var[2] * ir, w0 = var[3] * ir;
+    const double T0 = (var[4] * ir - 0.5 * (u0 * u0 + v0 * v0 + w0 * w0)) / cv;
+    const double p0 = var[0] * R * T0;
+    double* f = P.wall.ff[side];
+    f[0] = p0; f[1] = T0; f[2] = u0; f[3] = v0; f[4] = w0;
+    f[5] = std::sqrt(gamma * R * T0);
+  }
+  if (P.wall.table[side]) {
+    cudaStreamSynchronize(c->stream);
+    cudaFree((void*)P.wall.table[side]);
+    P.wall.table[side] = nullptr;
+  }
+  if (kind == DN_BC_INFLOW) {
+    if (!table) return fail(c, DN_ERR_ARG, "inflow needs a face table");
+    const size_t na = axis == 0 ? (size_t)P.d.nj * P.d.nk : (axis == 1 ? (size_t)P.d.ni * P.d.nk : (size_t)P.d.ni * P.d.nj);
+    for (size_t q = 0; q < na; ++q) {
+      const double* e = table + 5 * q;
+      if (!(e[1] > 0) || !std::isfinite(e[1]) || !std::isfinite(e[2]) || !std::isfinite(e[3]) ||
+          !std::isfinite(e[4]) || (e[0] == e[0] && !(e[0] > 0)))
+        return fail(c, DN_ERR_ARG, "inflow face %zu: invalid state", q);
+    }
+    void* d = nullptr;
+    cudaError_t e = cudaMalloc(&d, na * 5 * sizeof(double));
+    if (e != cudaSuccess) return fail(c, DN_ERR_NOMEM, "cudaMalloc(inflow table)");
+    e = cudaMemcpyAsync(d, table, na * 5 * sizeof(double), cudaMemcpyHostToDevice, c->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    if (e != cudaSuccess) { cudaFree(d); return cuda_fail(c, e, "inflow table upload"); }
+    P.wall.table[side] = static_cast<const double*>(d);
+  }
+  P.wall.kind[side] = kind;
+  P.wall.any = 0;
+  for (int q = 0; q < 6; ++q) if (P.wall.kind[q] != DN_BC_ZERO_FLUX) P.wall.any = 1;
   return DN_OK;
 }
 

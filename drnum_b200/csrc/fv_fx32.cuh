@@ -44,6 +44,7 @@
 
 #include <cstdint>
 #include "fv_numerics.cuh"
+#include "fv_wall.cuh"
 
 namespace dn {
 
@@ -69,6 +70,7 @@ struct FxArgs {
   unsigned long long* err_info;
   FxGeom g;
   FxParams p;
+  WallBC wall;           // patch-face fluxes of the non-periodic axes
 };
 
 constexpr int kFxLimit = 1 << 30;   // |o| must stay below this
@@ -473,12 +475,19 @@ fx_stage_kernel(const FxArgs a)
       const int ncv = (int)nc;
       const bool act = a.active ? (a.active[c] != 0) : true;
       int bad = 0;
+      int res[5];
+      #pragma unroll
+      for (int v = 0; v < 5; ++v)
+        res[v] = qx_lo[v] + sm.qy[v][ty][tx] + sm.qz[v][ty][tx]
+               - sm.qz[v][ty][tx + 1] - sm.qy[v][ty + 1][tx] - qx_hi[v];
+      if (a.wall.any && (i == 0 || i == g.ni - 1 || j == 0 || j == g.nj - 1 || k == 0 || k == g.nk - 1))
+        add_wall_fluxes(a.wall, g.ni, g.nj, g.nk, g.per_x, g.per_y, g.per_z, i, j, k, xu0, P.Ax, P.Ay, P.Az, res,
+                        [&](int v, float F) { return __float2int_rn(F * P.face_scale[v]); });
       #pragma unroll
       for (int v = 0; v < 5; ++v) {
         int32_t o;
         if (act) {
-          const int r = qx_lo[v] + sm.qy[v][ty][tx] + sm.qz[v][ty][tx]
-                      - sm.qz[v][ty][tx + 1] - sm.qy[v][ty + 1][tx] - qx_hi[v];
+          const int r = res[v];
           // |un| < 2^30 and |r| < 2^30 (face integers are bounded by the
           // exact range of the update), so the int32 sum cannot overflow
           const int on = a.un[v * ncv + c] + r;

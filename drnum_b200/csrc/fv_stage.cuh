@@ -29,6 +29,7 @@
 
 #include <cstdint>
 #include "fv_numerics.cuh"
+#include "fv_wall.cuh"
 
 namespace dn {
 
@@ -48,6 +49,7 @@ struct StageArgs {
   unsigned long long* err_info;       // first failing cell: [cell, var, bits(un), bits(r)]
   StageGeom g;
   typename Policy::Params p;
+  WallBC wall;                        // patch-face fluxes of the non-periodic axes
 };
 
 // index along an axis with periodic wrap; returns -1 if outside a closed axis
@@ -258,15 +260,28 @@ fv_stage_kernel(const StageArgs<Policy> a)
       const size_t c = ((size_t)i * g.nj + j) * g.nk + k;
       const bool act = a.active ? (a.active[c] != 0) : true;
       int bad = 0;
+      FaceT res[5];
       #pragma unroll
       for (int v = 0; v < 5; ++v) {
-        const int bad_before = bad;
         FaceT r = fx_lo[v];
         r += sm.fy[v][ty][tx];
         r += sm.fz[v][ty][tx];
         r -= sm.fz[v][ty][tx + 1];
         r -= sm.fy[v][ty + 1][tx];
         r -= fx_hi[v];
+        res[v] = r;
+      }
+      if (a.wall.any && (i == 0 || i == g.ni - 1 || j == 0 || j == g.nj - 1 || k == 0 || k == g.nk - 1)) {
+        Real U[5];
+        #pragma unroll
+        for (int v = 0; v < 5; ++v) U[v] = sm.plane[s0][v][ty + 2][tx + 2];
+        add_wall_fluxes(a.wall, g.ni, g.nj, g.nk, g.per_x, g.per_y, g.per_z, i, j, k, U, Ax, Ay, Az, res,
+                        [&](int v, Real F) { return Policy::face(a.p, v, F); });
+      }
+      #pragma unroll
+      for (int v = 0; v < 5; ++v) {
+        const int bad_before = bad;
+        const FaceT r = res[v];
         typename Policy::Store o;
         if (act) {
           o = Policy::update(a.p, v, a.un[v * nc + c], r, bad);

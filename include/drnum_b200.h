@@ -59,6 +59,14 @@ extern "C" {
 #define DN_FACE_PERIODIC  0   /* index wrap (periodic patch) */
 #define DN_FACE_CLOSED    1   /* first-order reconstruction at the edge, zero face flux */
 
+/* Flux through an outer face of a non-periodic patch axis (the flux
+ * functor's x/y/zWall{M,P}, iterators/cartesianiterator.h:190-308). */
+#define DN_BC_ZERO_FLUX   0   /* wall methods that add nothing */
+#define DN_BC_FARFIELD    1   /* CompressibleFarfieldFlux (fluxes/compressiblefarfieldflux.h:26-181) */
+#define DN_BC_SLIP        2   /* CompressibleSlipFlux (fluxes/compressibleslipflux.h:34-98) */
+#define DN_BC_INFLOW      3   /* prescribed face state per face, the JetFlux::xWallM form
+                                 (applications/drnumJetDemo/jetflux.h:158-192) */
+
 typedef struct dn_ctx dn_ctx;
 
 /* Geometry of one axis-aligned Cartesian patch (CartesianPatch::readFromFile,
@@ -94,6 +102,17 @@ int dn_set_stream(dn_ctx* ctx, void* stream);
  * Replaces: GPU_PatchIterator::addPatch + GPU_Patch ctor
  * (iterators/gpu_patchiterator.h:86-95, gpu_patch.h:43-129). */
 int dn_patch_add(dn_ctx* ctx, const dn_patch_desc* desc, int* patch_id);
+
+/* Boundary flux of side `side` (0 x-min, 1 x-max, 2 y-min, 3 y-max, 4 z-min,
+ * 5 z-max) of a non-periodic axis; every side starts as DN_BC_ZERO_FLUX.
+ *   DN_BC_FARFIELD: params = far-field p, T, u, v, w
+ *                   (CompressibleFarfieldFlux::setFarfield, compressiblefarfieldflux.h:87-90)
+ *   DN_BC_INFLOW:   table = per face {p, T, u, v, w}; p = NaN takes the boundary
+ *                   cell's pressure.  Faces ordered j*nk+k (x sides), i*nk+k (y sides),
+ *                   i*nj+j (z sides).  The table is copied.
+ * The face flux uses the boundary cell's own state and is added to its
+ * residual after the interior faces, as the reference's iterator does. */
+int dn_patch_set_bc(dn_ctx* ctx, int patch_id, int side, int kind, const double* params, const double* table);
 
 /* DN_FP32 only: FP64 base state the FP32 offsets are stored against, and the
  * per-variable offset quantum is derived from `range` (the largest expected

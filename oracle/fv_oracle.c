@@ -74,6 +74,11 @@ typedef struct {
   int ni, nj, nk;
   int periodic[3];          /* per axis: 1 = periodic wrap, 0 = closed */
   double dx, dy, dz;
+  /* patch-face fluxes of closed axes, per side x-min, x-max, y-min, y-max,
+   * z-min, z-max: 0 zero flux, 1 far field, 2 slip wall, 3 inflow table */
+  int bc[6];
+  double ff[6][5];          /* far field p, T, u, v, w */
+  const double* table[6];   /* inflow: per face p (NaN: boundary cell), T, u, v, w */
 } dno_patch;
 
 static size_t cell(const dno_patch* p, long i, long j, long k)
@@ -214,6 +219,111 @@ static int face_flux(const dno_patch* p, const double* f, int dir,
  * holds for the wrapped faces of a periodic patch (the reference runs those
  * on a ghosted patch whose ghosts are refreshed after every stage).
  */
+#define GAS_CP 1004.5     /* perfectgas.h:33 */
+
+/* PerfectGas::conservativeToPrimitive, perfectgas.h:84-93 (also COMPR_VARS,
+ * compressibleflux.h:26-38) */
+static void cons_to_prim(const double* var, double* p, double* T, double* u, double* v, double* w)
+{
+  double ir = 1.0/var[0];
+  *u = var[1]*ir;
+  *v = var[2]*ir;
+  *w = var[3]*ir;
+  *T = (var[4]*ir - 0.5*(*u * *u + *v * *v + *w * *w))/GAS_CV;
+  *p = var[0]*GAS_R * *T;
+}
+
+/* face-state flux, compressiblefarfieldflux.h:100-105 and jetflux.h:186-190 */
+static void state_flux(int dir, double A, double p, double T, double u, double v, double w, double* flux)
+{
+  double un = dir == 0 ? u : (dir == 1 ? v : w);
+  flux[0] = A*p/(GAS_R*T)*un;
+  flux[1] = flux[0]*u + (dir == 0 ? A*p : 0.0);
+  flux[2] = flux[0]*v + (dir == 1 ? A*p : 0.0);
+  flux[3] = flux[0]*w + (dir == 2 ? A*p : 0.0);
+  if (dir != 0) flux[1] = flux[0]*u;
+  if (dir != 1) flux[2] = flux[0]*v;
+  if (dir != 2) flux[3] = flux[0]*w;
+  flux[4] = flux[0]*(GAS_CP*T + 0.5*(u*u + v*v + w*w));
+}
+
+/* Wall flux of one side for boundary-cell state var (first order: the
+ * Upwind2 projection at the patch edge, upwind2.h:39-42).  Returns 0 for a
+ * zero-flux side.
+ *   far field: CompressibleFarfieldFlux::x/y/zWall{M,P}, compressiblefarfieldflux.h:26-181
+ *   slip:      CompressibleSlipFlux, compressibleslipflux.h:34-98
+ *   inflow:    JetFlux::xWallM, jetflux.h:158-192 (state from a face table) */
+static int wall_flux(const dno_patch* p, int side, size_t face, const double* var, double A, double* flux)
+{
+  int kind = p->bc[side];
+  int dir = side/2, plus = side & 1;
+  double p1, T1, u1, v1, w1;
+  if (kind == 0) return 0;
+  cons_to_prim(var, &p1, &T1, &u1, &v1, &w1);
+  if (kind == 2) {
+    for (int v = 0; v < 5; ++v) flux[v] = 0;
+    flux[1 + dir] += A*p1;
+    return 1;
+  }
+  if (kind == 3) {
+    const double* e = p->table[side] + 5*face;
+    double pp = (e[0] == e[0]) ? e[0] : p1;
+    state_flux(dir, A, pp, e[1], e[2], e[3], e[4], flux);
+    return 1;
+  }
+  /* far field: setFarfield stores the conservative state (perfectgas.h:58-66) */
+  double m[5], p0, T0, u0, v0, w0;
+  const double* q = p->ff[side];
+  m[0] = q[0]/(GAS_R*q[1]);
+  m[1] = m[0]*q[2];
+  m[2] = m[0]*q[3];
+  m[3] = m[0]*q[4];
+  m[4] = m[0]*(GAS_CV*q[1] + 0.5*(q[2]*q[2] + q[3]*q[3] + q[4]*q[4]));
+  cons_to_prim(m, &p0, &T0, &u0, &v0, &w0);
+  double a0 = sqrt(GAS_GAMMA*GAS_R*T0);
+  double a1 = sqrt(GAS_GAMMA*GAS_R*T1);
+  double un0 = dir == 0 ? u0 : (dir == 1 ? v0 : w0);
+  double un1 = dir == 0 ? u1 : (dir == 1 ? v1 : w1);
+  double M0 = plus ? -(un0/a0) : un0/a0;
+  double M1 = plus ? -(un1/a1) : un1/a1;
+  double M = 0.5*(M0 + M1);
+  if (M >= 0) {
+    state_flux(dir, A, M >= 1 ? p0 : p1, T0, u0, v0, w0, flux);
+  } else {
+    state_flux(dir, A, p1, T1, u1, v1, w1, flux);   /* `M <= 1` always holds here */
+  }
+  return 1;
+}
+
+/* Wall loops of cartesianiterator.h:190-308: x-min (+), x-max (-), y-min,
+ * y-max, z-min, z-max, each over its whole side, after the interior faces. */
+static void add_walls(const dno_patch* p, const double* f, double* res)
+{
+  const size_t nc = (size_t)p->ni*p->nj*p->nk;
+  const int n[3] = {p->ni, p->nj, p->nk};
+  const double A[3] = {p->dy*p->dz, p->dx*p->dz, p->dx*p->dy};
+  for (int side = 0; side < 6; ++side) {
+    int dir = side/2, plus = side & 1;
+    if (p->periodic[dir] || n[dir] <= 2 || p->bc[side] == 0) continue;
+    int a = dir == 0 ? 1 : 0, b = dir == 2 ? 1 : 2;     /* the two axes spanning the side */
+    for (long ia = 0; ia < n[a]; ++ia)
+      for (long ib = 0; ib < n[b]; ++ib) {
+        long c[3];
+        c[dir] = plus ? n[dir] - 1 : 0;
+        c[a] = ia;
+        c[b] = ib;
+        size_t cc = cell(p, c[0], c[1], c[2]);
+        double var[5], flux[5];
+        for (int v = 0; v < 5; ++v) var[v] = f[v*nc + cc];
+        if (!wall_flux(p, side, (size_t)ia*n[b] + ib, var, A[dir], flux)) continue;
+        for (int v = 0; v < 5; ++v) {
+          if (plus) res[v*nc + cc] -= flux[v];
+          else res[v*nc + cc] += flux[v];
+        }
+      }
+  }
+}
+
 static void residual_canonical(const dno_patch* p, const double* f, double* res,
                                double* fx, double* fy, double* fz)
 {
@@ -256,6 +366,7 @@ static void residual_canonical(const dno_patch* p, const double* f, double* res,
           res[v*nc + cc] = r;
         }
       }
+  add_walls(p, f, res);
 }
 
 /*
@@ -290,6 +401,7 @@ int dno_run(int ni, int nj, int nk, const int* periodic,
 {
   if (ni < 1 || nj < 1 || nk < 1 || n_alpha < 1 || !state || !alpha) return -1;
   dno_patch p;
+  memset(&p, 0, sizeof p);
   p.ni = ni; p.nj = nj; p.nk = nk;
   p.periodic[0] = periodic ? periodic[0] : 1;
   p.periodic[1] = periodic ? periodic[1] : 1;
@@ -316,11 +428,39 @@ int dno_residual(int ni, int nj, int nk, const int* periodic,
                  const double* state, double* res)
 {
   dno_patch p;
+  memset(&p, 0, sizeof p);
   p.ni = ni; p.nj = nj; p.nk = nk;
   p.periodic[0] = periodic ? periodic[0] : 1;
   p.periodic[1] = periodic ? periodic[1] : 1;
   p.periodic[2] = periodic ? periodic[2] : 1;
   p.dx = dx; p.dy = dy; p.dz = dz;
+  const size_t nc = (size_t)ni*nj*nk;
+  double* work = (double*)malloc(15*nc*sizeof(double));
+  if (!work) return -2;
+  residual_canonical(&p, state, res, work, work + 5*nc, work + 10*nc);
+  free(work);
+  return 0;
+}
+
+/* One residual evaluation with patch-face fluxes on the closed axes:
+ * bc[6] kinds (0 zero flux, 1 far field, 2 slip, 3 inflow), ff[6*5] far-field
+ * p, T, u, v, w per side, tables[6] inflow face tables (or NULL). */
+int dno_residual_bc(int ni, int nj, int nk, const int* periodic,
+                    double dx, double dy, double dz,
+                    const int* bc, const double* ff, const double* const* tables,
+                    const double* state, double* res)
+{
+  dno_patch p;
+  memset(&p, 0, sizeof p);
+  p.ni = ni; p.nj = nj; p.nk = nk;
+  for (int a = 0; a < 3; ++a) p.periodic[a] = periodic ? periodic[a] : 1;
+  p.dx = dx; p.dy = dy; p.dz = dz;
+  for (int sd = 0; sd < 6; ++sd) {
+    p.bc[sd] = bc ? bc[sd] : 0;
+    for (int q = 0; q < 5; ++q) p.ff[sd][q] = ff ? ff[5*sd + q] : 0.0;
+    p.table[sd] = tables ? tables[sd] : NULL;
+    if (p.bc[sd] == 3 && !p.table[sd]) return -3;
+  }
   const size_t nc = (size_t)ni*nj*nk;
   double* work = (double*)malloc(15*nc*sizeof(double));
   if (!work) return -2;

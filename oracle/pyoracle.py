@@ -87,6 +87,36 @@ def oracle_run(U0, h, dt, steps, alpha=(0.25, 0.5, 1.0), periodic=(True, True, T
     return U
 
 
+def oracle_residual_bc(U0, h, bcs, periodic=(False, False, False)):
+    """Residual with patch-face fluxes: bcs = {side: (kind, params, table)}
+    for sides 0..5 (x-min, x-max, y-min, y-max, z-min, z-max)."""
+    lib = oracle_lib()
+    lib.dno_residual_bc.restype = c_int
+    lib.dno_residual_bc.argtypes = [c_int, c_int, c_int, POINTER(c_int), c_double, c_double, c_double,
+                                    POINTER(c_int), _P, POINTER(_P), _P, _P]
+    U = np.ascontiguousarray(U0, dtype=np.float64)
+    _, ni, nj, nk = U.shape
+    hx, hy, hz = (h, h, h) if np.isscalar(h) else h
+    kinds = (c_int * 6)()
+    ff = np.zeros(30)
+    tabs = (_P * 6)()
+    keep = []
+    for side, (kind, params, table) in (bcs or {}).items():
+        kinds[side] = int(kind)
+        if params is not None:
+            ff[5 * side:5 * side + 5] = params
+        if table is not None:
+            t = np.ascontiguousarray(table, dtype=np.float64)
+            keep.append(t)
+            tabs[side] = t.ctypes.data_as(_P)
+    res = np.empty_like(U)
+    rc = lib.dno_residual_bc(ni, nj, nk, _per(periodic), hx, hy, hz, kinds, ff.ctypes.data_as(_P), tabs,
+                             U.ctypes.data_as(_P), res.ctypes.data_as(_P))
+    if rc != 0:
+        raise RuntimeError(f"oracle failed: {rc}")
+    return res
+
+
 def oracle_residual(U0, h, periodic=(True, True, True)):
     U = np.ascontiguousarray(U0, dtype=np.float64)
     _, ni, nj, nk = U.shape
@@ -212,6 +242,16 @@ class RefGrid:
         t["counts"] = counts
         return t
 
+    def set_bc(self, p, side, kind, params=None, table=None):
+        self.lib.dnref_grid_set_bc.restype = c_int
+        self.lib.dnref_grid_set_bc.argtypes = [c_void_p, c_int, c_int, c_int, _P, _P]
+        pa = None if params is None else np.ascontiguousarray(params, dtype=np.float64)
+        ta = None if table is None else np.ascontiguousarray(table, dtype=np.float64)
+        rc = self.lib.dnref_grid_set_bc(self.h, p, side, kind, None if pa is None else pa.ctypes.data_as(_P),
+                                        None if ta is None else ta.ctypes.data_as(_P))
+        if rc != 0:
+            raise RuntimeError(f"reference set_bc failed: {rc}")
+
     def set_state(self, p, U):
         U = np.ascontiguousarray(U, dtype=np.float64)
         if self.lib.dnref_grid_set_state(self.h, p, U.ctypes.data_as(_P)) != 0:
@@ -277,9 +317,10 @@ def oracle_donor_copy(states, tables):
             Ur[:, c] = a
 
 
-def oracle_grid_run(states, spacings, tables, dt, steps, alpha=(0.25, 0.5, 1.0)):
+def oracle_grid_run(states, spacings, tables, dt, steps, alpha=(0.25, 0.5, 1.0), bcs=None):
     """RK steps of a patch grid with the C restatement of the residual
-    (closed patch faces) and the numpy donor copy, in the order of
+    (closed patch faces, with the patch-face fluxes of bcs[p] = {side: (kind,
+    params, table)}) and the numpy donor copy, in the order of
     RungeKutta::operator() (rungekutta.cpp:27-42).  Returns new states."""
     U = [np.ascontiguousarray(s, dtype=np.float64).copy() for s in states]
     for _ in range(steps):
@@ -288,7 +329,7 @@ def oracle_grid_run(states, spacings, tables, dt, steps, alpha=(0.25, 0.5, 1.0))
         for a in alpha:
             for p, u in enumerate(U):
                 hx, hy, hz = spacings[p]
-                res = oracle_residual(u, (hx, hy, hz), periodic=(False, False, False))
+                res = oracle_residual_bc(u, (hx, hy, hz), (bcs or {}).get(p, {}))
                 pf = (a * dt) / (hx * hy * hz)
                 U[p] = Un[p] + pf * res
             oracle_donor_copy(U, tables)

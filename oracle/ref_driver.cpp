@@ -20,6 +20,9 @@
 #include "genericoperation.h"
 #include "perfectgas.h"
 #include "fluxes/ausmplus.h"
+#include "fluxes/compressiblefarfieldflux.h"
+#include "fluxes/compressibleslipflux.h"
+#include "reconstruction/upwind1.h"
 #include "reconstruction/upwind2.h"
 #include "reconstruction/vanalbada.h"
 #include "iterators/cartesianiterator.h"
@@ -61,6 +64,84 @@ struct PeriodicFlux
   template <typename P> void yWallP(P*, size_t, size_t, size_t, real, real, real, real, real*) {}
   template <typename P> void zWallM(P*, size_t, size_t, size_t, real, real, real, real, real*) {}
   template <typename P> void zWallP(P*, size_t, size_t, size_t, real, real, real, real, real*) {}
+};
+
+// Patch-face fluxes per patch and side (x-min, x-max, y-min, y-max, z-min,
+// z-max): 0 none, 1 the reference's CompressibleFarfieldFlux, 2 its
+// CompressibleSlipFlux, 3 a prescribed face state per face (the flux of the
+// jet application's JetFlux::xWallM, applications/drnumJetDemo/jetflux.h:
+// 165-191, restated here because that class lives in an application).
+typedef CompressibleFarfieldFlux<5, Upwind1<5>, PerfectGas> RefFarfield;
+typedef CompressibleSlipFlux<5, Upwind1<5>, PerfectGas> RefSlip;
+
+struct SideConfig
+{
+  int kind[6] = {0, 0, 0, 0, 0, 0};
+  RefFarfield farfield[6];
+  std::vector<double> table[6];
+};
+
+struct GridBC
+{
+  std::vector<SideConfig> patches;
+};
+
+struct SideFlux
+{
+  RefAusm m_Ausm;
+  RefSlip m_Slip;
+  GridBC* m_BC = nullptr;
+
+  template <typename P> void xField(P* p, size_t i, size_t j, size_t k, real x, real y, real z, real A, real* f) { m_Ausm.xField(p, i, j, k, x, y, z, A, f); }
+  template <typename P> void yField(P* p, size_t i, size_t j, size_t k, real x, real y, real z, real A, real* f) { m_Ausm.yField(p, i, j, k, x, y, z, A, f); }
+  template <typename P> void zField(P* p, size_t i, size_t j, size_t k, real x, real y, real z, real A, real* f) { m_Ausm.zField(p, i, j, k, x, y, z, A, f); }
+
+  template <typename P> SideConfig* cfg(P* p)
+  {
+    if (!m_BC || p->getIndex() >= m_BC->patches.size()) return nullptr;
+    return &m_BC->patches[p->getIndex()];
+  }
+
+  // prescribed face state: boundary cell (ic, jc, kc), face entry e
+  template <typename P> void inflow(P* p, int dir, size_t ic, size_t jc, size_t kc, const double* e, real A, real* flux)
+  {
+    dim_t<5> dim;
+    real var[5];
+    real pp, T, u, v, w;
+    p->getVar(dim, 0, ic, jc, kc, var);
+    PerfectGas::conservativeToPrimitive(var, pp, T, u, v, w);
+    if (e[0] == e[0]) pp = e[0];
+    T = e[1]; u = e[2]; v = e[3]; w = e[4];
+    real un = dir == 0 ? u : (dir == 1 ? v : w);
+    flux[0] = A*pp/(PerfectGas::R()*T)*un;
+    flux[1] = flux[0]*u;
+    flux[2] = flux[0]*v;
+    flux[3] = flux[0]*w;
+    if (dir == 0) flux[1] = flux[0]*u + A*pp;
+    if (dir == 1) flux[2] = flux[0]*v + A*pp;
+    if (dir == 2) flux[3] = flux[0]*w + A*pp;
+    flux[4] = flux[0]*(PerfectGas::cp()*T + 0.5*(u*u + v*v + w*w));
+  }
+
+#define DN_SIDE(NAME, SIDE, DIR, IC, JC, KC, FACE)                                                     \
+  template <typename P> void NAME(P* p, size_t i, size_t j, size_t k, real x, real y, real z, real A, real* f) \
+  {                                                                                                  \
+    SideConfig* c = cfg(p);                                                                          \
+    if (!c) return;                                                                                  \
+    switch (c->kind[SIDE]) {                                                                         \
+      case 1: c->farfield[SIDE].NAME(p, i, j, k, x, y, z, A, f); break;                              \
+      case 2: m_Slip.NAME(p, i, j, k, x, y, z, A, f); break;                                         \
+      case 3: inflow(p, DIR, IC, JC, KC, &c->table[SIDE][5*(FACE)], A, f); break;                    \
+      default: break;                                                                                \
+    }                                                                                                \
+  }
+  DN_SIDE(xWallM, 0, 0, i, j, k, j*p->sizeK() + k)
+  DN_SIDE(xWallP, 1, 0, i - 1, j, k, j*p->sizeK() + k)
+  DN_SIDE(yWallM, 2, 1, i, j, k, i*p->sizeK() + k)
+  DN_SIDE(yWallP, 3, 1, i, j - 1, k, i*p->sizeK() + k)
+  DN_SIDE(zWallM, 4, 2, i, j, k, i*p->sizeJ() + j)
+  DN_SIDE(zWallP, 5, 2, i, j, k - 1, i*p->sizeJ() + j)
+#undef DN_SIDE
 };
 
 // Periodic ghost copy, field 0, for the axes flagged periodic; each such axis
@@ -268,7 +349,7 @@ struct DnRefGrid
 {
   PatchGrid grid;
   std::vector<CartesianPatch*> patches;
-  CartesianIterator<5, PeriodicFlux>* iterator = nullptr;
+  GridBC bc;
 };
 
 // n[3*np], origin[3*np], length[3*np], seek[6*np] (imin imax jmin jmax kmin kmax)
@@ -295,7 +376,27 @@ void* dnref_grid_create(int np, const int* n, const double* origin, const double
                                                      length[3*p], length[3*p+1], length[3*p+2])));
   }
   g->grid.computeDependencies(true);
+  g->bc.patches.resize(g->patches.size());
   return g;
+}
+
+// Patch-face flux of side `side` of patch p: kind 0 none, 1 far field
+// (params p, T, u, v, w), 2 slip wall, 3 face table ([faces][5] p or NaN, T,
+// u, v, w; x sides j*nk+k, y sides i*nk+k, z sides i*nj+j).
+int dnref_grid_set_bc(void* handle, int p, int side, int kind, const double* params, const double* table)
+{
+  DnRefGrid* g = (DnRefGrid*)handle;
+  if (!g || p < 0 || p >= int(g->patches.size()) || side < 0 || side > 5 || kind < 0 || kind > 3) return -1;
+  SideConfig& c = g->bc.patches[p];
+  c.kind[side] = kind;
+  if (kind == 1) c.farfield[side].setFarfield(params[0], params[1], params[2], params[3], params[4]);
+  if (kind == 3) {
+    CartesianPatch* P = g->patches[p];
+    const int axis = side / 2;
+    const size_t n = axis == 0 ? P->sizeJ()*P->sizeK() : (axis == 1 ? P->sizeI()*P->sizeK() : P->sizeI()*P->sizeJ());
+    c.table[side].assign(table, table + 5*n);
+  }
+  return 0;
 }
 
 // Donor tables of patch p.  counts[4] = {unique receiving cells, donor
@@ -371,8 +472,9 @@ int dnref_grid_run(void* handle, int steps, double dt, const double* alpha, int 
 {
   DnRefGrid* g = (DnRefGrid*)handle;
   if (!g || n_alpha < 1) return -1;
-  PeriodicFlux flux;
-  CartesianIterator<5, PeriodicFlux> iterator(flux);
+  SideFlux flux;
+  flux.m_BC = &g->bc;
+  CartesianIterator<5, SideFlux> iterator(flux);
   for (size_t p = 0; p < g->patches.size(); ++p) iterator.addPatch(g->patches[p]);
   RungeKutta rk;
   for (int a = 0; a < n_alpha; ++a) rk.addAlpha(alpha[a]);

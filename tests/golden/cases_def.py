@@ -76,19 +76,40 @@ def grid_layout(name):
         return cases.octant_grid(nf=(8, 8, 8), h=1.0 / 16, overlap=3, seek=2)
     if name == "octants_ragged":
         return cases.octant_grid(nf=(12, 8, 10), h=1.0 / 24, overlap=4, seek=2)
+    if name == "octants_jet":
+        return grid_layout("octants_8")
+    if name == "bc_box":
+        return [dict(n=(10, 8, 9), origin=(0.0, 0.0, 0.0), length=(1.0, 0.8, 0.9), seek=(0, 0, 0, 0, 0, 0))]
     raise KeyError(name)
 
 
 GRID_ADD_PROTECT = {"random6_prot1": 1}
 # layouts whose donor tables are fixtures; the octant grids also store RK steps
-GRID_TABLES = ["pair_x", "embedded", "random6", "random6_prot1", "octants_8", "octants_ragged"]
-GRID_STEPS = {"octants_8": 3, "octants_ragged": 2}
+GRID_TABLES = ["pair_x", "embedded", "random6", "random6_prot1", "octants_8", "octants_ragged", "octants_jet",
+               "bc_box"]
+GRID_STEPS = {"octants_8": 3, "octants_ragged": 2, "octants_jet": 3, "bc_box": 3}
 
 
 def grid_case(name):
     """Layout, initial states, spacings and time step of a stepped grid case."""
     patches = grid_layout(name)
-    states = cases.grid_state(patches)
+    states = cases.grid_state(patches, centre=(0.45, 0.4, 0.45)) if name == "bc_box" else cases.grid_state(patches)
     dt = cases.grid_dt(patches, states)
     spacings = [tuple(p["length"][a] / p["n"][a] for a in range(3)) for p in patches]
     return patches, states, spacings, dt, GRID_STEPS[name]
+
+
+# grids with patch-face fluxes: layout name -> boundary conditions
+def grid_bcs(name):
+    if name == "octants_jet":
+        return cases.jet_bcs(grid_layout("octants_8"), radius=0.12, noise=1e-3)
+    if name == "bc_box":
+        patch = grid_layout("bc_box")[0]
+        t = cases.jet_table(patch, 0.6 * cases.A_INF, 0.9 * cases.T_INF, radius=0.2, u_far=0.1 * cases.A_INF,
+                            p_jet=1.05 * cases.P_INF, noise=1e-2)
+        far_a = (cases.P_INF, cases.T_INF, 0.3 * cases.A_INF, 0.05 * cases.A_INF, 0.0)
+        far_b = (0.95 * cases.P_INF, 1.1 * cases.T_INF, 0.0, -1.2 * cases.A_INF, 0.1 * cases.A_INF)
+        return {0: {0: (cases.BC_INFLOW, None, t), 1: (cases.BC_FARFIELD, far_a, None),
+                    2: (cases.BC_SLIP, None, None), 3: (cases.BC_FARFIELD, far_b, None),
+                    4: (cases.BC_SLIP, None, None), 5: (cases.BC_ZERO, None, None)}}
+    return None

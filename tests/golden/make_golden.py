@@ -70,6 +70,10 @@ def make_grids():
             t = g.tables(p)
             for k, v in t.items():
                 arrays[f"p{p}_{k}"] = v
+        bcs = cases_def.grid_bcs(name) or {}
+        for p, sides in bcs.items():
+            for side, (kind, params, table) in sides.items():
+                g.set_bc(p, side, kind, params, table)
         if name in cases_def.GRID_STEPS:
             _, states, _, dt, steps = cases_def.grid_case(name)
             for p, U in enumerate(states):

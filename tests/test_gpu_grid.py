@@ -30,10 +30,13 @@ def make_grid(name, precision, states=None):
     states = st0 if states is None else states
     grid = PatchGrid()
     objs = []
-    for p, U in zip(patches, states):
+    bcs = cases_def.grid_bcs(name) or {}
+    for q, (p, U) in enumerate(zip(patches, states)):
         cp = CartesianPatch(*p["n"], lengths=p["length"], origin=p["origin"], periodic=(False, False, False),
                             seek=p["seek"])
         cp.setField(0, U)
+        for side, (kind, params, table) in bcs.get(q, {}).items():
+            cp.setBoundary(side, kind, params, table)
         grid.insertPatch(cp)
         objs.append(cp)
     grid.computeDependencies()
@@ -102,9 +105,8 @@ def test_grid_stagewise_api_equals_fused_step(golden_dir):
         assert np.array_equal(cp.getField(0), z[f"p{p}_out"]), p
 
 
-def test_grid_fp32_against_fp64():
-    name = "octants_ragged"
-    steps = 6
+@pytest.mark.parametrize("name,steps", [("octants_ragged", 6), ("octants_jet", 30)])
+def test_grid_fp32_against_fp64(name, steps):
     out = {}
     for prec in (DN_FP64, DN_FP32):
         it, objs, _, dt, _ = make_grid(name, prec)
@@ -149,4 +151,20 @@ def test_set_donors_rejects_invalid_tables(golden_dir):
     bad = {k: v.copy() for k, v in good.items()}
     bad["rec_unique"] = bad["rec_unique"][::-1].copy()   # not ascending
     assert call(bad) == _lib.DN_ERR_ARG
+    it.close()
+
+
+def test_boundary_kinds_rejected_where_invalid():
+    it = B200CartesianIterator(AusmPlus(), 0, DN_FP64)
+    pid = it.addPatch(CartesianPatch(6, 6, 6, lengths=(1.0, 1.0, 1.0), periodic=(True, False, False)))
+    lib, ctx = it.lib, it.ctx
+    ff = np.array([1e5, 300.0, 10.0, 0.0, 0.0])
+    assert lib.dn_patch_set_bc(ctx, pid, 0, _lib.DN_BC_FARFIELD, _lib.dptr(ff), None) == _lib.DN_ERR_ARG  # periodic axis
+    assert lib.dn_patch_set_bc(ctx, pid, 2, 7, None, None) == _lib.DN_ERR_ARG                        # unknown kind
+    assert lib.dn_patch_set_bc(ctx, pid, 6, _lib.DN_BC_SLIP, None, None) == _lib.DN_ERR_ARG           # no side 6
+    assert lib.dn_patch_set_bc(ctx, pid, 2, _lib.DN_BC_INFLOW, None, None) == _lib.DN_ERR_ARG         # table missing
+    bad = ff.copy()
+    bad[1] = -1.0
+    assert lib.dn_patch_set_bc(ctx, pid, 2, _lib.DN_BC_FARFIELD, _lib.dptr(bad), None) == _lib.DN_ERR_ARG
+    assert lib.dn_patch_set_bc(ctx, pid, 3, _lib.DN_BC_FARFIELD, _lib.dptr(ff), None) == _lib.DN_OK
     it.close()

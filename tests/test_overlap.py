@@ -100,7 +100,7 @@ def test_oracle_grid_steps_equal_reference(golden_dir, name):
     patches, states, spacings, dt, steps = cases_def.grid_case(name)
     assert float(z["dt"]) == dt and int(z["steps"]) == steps
     tables = [{k: z[f"p{p}_{k}"] for k in TABLE_KEYS} for p in range(len(patches))]
-    out = pyoracle.oracle_grid_run(states, spacings, tables, dt, steps, cases_def.ALPHA)
+    out = pyoracle.oracle_grid_run(states, spacings, tables, dt, steps, cases_def.ALPHA, cases_def.grid_bcs(name))
     for p in range(len(patches)):
         assert np.array_equal(out[p], z[f"p{p}_out"]), (name, p, np.abs(out[p] - z[f"p{p}_out"]).max())
 
