@@ -81,6 +81,17 @@ SIGNATURES = {
     "dn_overlap_destroy": (c_int, [c_void_p]),
     "dn_copy_donor_data": (c_int, [c_void_p, c_int]),
     "dn_patch_set_bc": (c_int, [c_void_p, c_int, c_int, c_int, POINTER(c_double), POINTER(c_double)]),
+    "dn_patch_set_levelset": (c_int, [c_void_p, c_int, POINTER(c_double), c_int, c_int, c_double]),
+    "dn_patch_levelset_count": (c_int, [c_void_p, c_int, c_int, c_int, POINTER(c_int64)]),
+    "dn_patch_levelset_get": (c_int, [c_void_p, c_int, c_int, c_int, POINTER(c_uint64), POINTER(c_double),
+                                      POINTER(c_double), POINTER(c_uint64), POINTER(c_double)]),
+    "dn_apply_levelset_bc": (c_int, [c_void_p, c_int]),
+    "dn_levelset_classify": (c_int, [POINTER(dn_patch_desc), POINTER(c_double), c_int, c_int, c_double,
+                                     POINTER(c_void_p)]),
+    "dn_lslayers_count": (c_int, [c_void_p, c_int, c_int, POINTER(c_int64)]),
+    "dn_lslayers_get": (c_int, [c_void_p, c_int, c_int, POINTER(c_uint64), POINTER(c_double), POINTER(c_double),
+                                POINTER(c_uint64), POINTER(c_double)]),
+    "dn_lslayers_destroy": (c_int, [c_void_p]),
 }
 
 _lib = None
@@ -169,3 +180,29 @@ def read_donor_tables(counts_fn, get_fn, handle, patch_id):
         raise DnError(rc, f"donor tables of patch {patch_id}")
     arrs["counts"] = counts
     return arrs
+
+
+def read_levelset_layers(count_fn, get_fn, handle, args, num_inner, num_outer):
+    """Reads a level-set classification through a count/get pair
+    (dn_patch_levelset_count/get with args = (patch_id,), or
+    dn_lslayers_count/get with args = ()).  Returns
+    {"inner": [layer dicts], "outer": [...]} with cells, g, grad, donors, weights."""
+    import numpy as np
+    out = {}
+    for inner, num in ((1, num_inner), (0, num_outer)):
+        layers = []
+        for layer in range(num):
+            n = c_int64()
+            rc = count_fn(handle, *args, inner, layer, ctypes.byref(n))
+            if rc != DN_OK:
+                raise DnError(rc, "level-set layer count")
+            m = n.value
+            d = {"cells": np.zeros(m, np.uint64), "g": np.zeros(m), "grad": np.zeros((m, 3)),
+                 "donors": np.zeros((m, 8), np.uint64), "weights": np.zeros((m, 8))}
+            rc = get_fn(handle, *args, inner, layer, ptr(d["cells"], c_uint64), ptr(d["g"], c_double),
+                        ptr(d["grad"], c_double), ptr(d["donors"], c_uint64), ptr(d["weights"], c_double))
+            if rc != DN_OK:
+                raise DnError(rc, "level-set layer")
+            layers.append(d)
+        out["inner" if inner else "outer"] = layers
+    return out

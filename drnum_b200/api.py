@@ -98,6 +98,8 @@ class CartesianPatch:
         self.grid_index = None
         # patch-face fluxes per side: (kind, params, table), see setBoundary
         self.bcs = {}
+        # level-set wall: (G, num_inner, num_outer, min_inner_rel_dist), see setLevelSet
+        self.levelset = None
         self.m_NumFields = num_fields
         self.data = np.zeros((num_fields, 5, ni, nj, nk))
         self.active = np.ones((ni, nj, nk), dtype=np.uint8)
@@ -132,6 +134,20 @@ class CartesianPatch:
             raise ValueError(f"axis {side // 2} is periodic")
         self.bcs[int(side)] = (int(kind), None if params is None else tuple(float(x) for x in params),
                                None if table is None else np.ascontiguousarray(table, dtype=np.float64))
+
+    def setLevelSet(self, G, num_inner_layers=3, num_outer_layers=0, min_inner_rel_dist=0.1):
+        """Slip wall on the zero level of the signed-distance field G
+        ([ni][nj][nk]): LevelSetObject(levelset, grid, field, var, num_inner,
+        num_outer, min_inner_rel_dist) + CPU_LevelSetObjectBC<LSOBCCompressibleEulerOp>
+        (levelsetobject.cpp:24-41, cpu_levelsetobjectbc.h:58-90).  G = None
+        removes the wall."""
+        if G is None:
+            self.levelset = None
+            return
+        G = np.ascontiguousarray(G, dtype=np.float64)
+        if G.shape != (self.m_NumI, self.m_NumJ, self.m_NumK):
+            raise ValueError("level-set field must have the patch's shape")
+        self.levelset = (G, int(num_inner_layers), int(num_outer_layers), float(min_inner_rel_dist))
 
     def deactivate(self, i, j, k): self.active[i, j, k] = 0
     def activate(self, i, j, k): self.active[i, j, k] = 1
@@ -292,9 +308,26 @@ class B200CartesianIterator:
                                                          None if pa is None else _lib.dptr(pa),
                                                          None if table is None else _lib.dptr(table)))
 
+    def setLevelSets(self):
+        """Hands every patch's level-set wall to the device (dn_patch_set_levelset)."""
+        for pid, p in enumerate(self.m_Patches):
+            if p.levelset is None:
+                check(self.ctx, self.lib.dn_patch_set_levelset(self.ctx, pid, None, 0, 0, 0.0))
+            else:
+                G, ni, no, mr = p.levelset
+                check(self.ctx, self.lib.dn_patch_set_levelset(self.ctx, pid, _lib.dptr(G), ni, no, mr))
+
+    def levelSetLayers(self, i_patch):
+        p = self.m_Patches[i_patch]
+        if p.levelset is None:
+            return None
+        return _lib.read_levelset_layers(self.lib.dn_patch_levelset_count, self.lib.dn_patch_levelset_get, self.ctx,
+                                         (i_patch,), p.levelset[1], p.levelset[2])
+
     def updateDevice(self, fields=(0, 1)):
         self.setDonorTables()
         self.setBoundaries()
+        self.setLevelSets()
         for pid, p in enumerate(self.m_Patches):
             for f in fields:
                 a = np.ascontiguousarray(p.data[f], dtype=np.float64)
@@ -349,6 +382,19 @@ class B200CartesianIterator:
         n = ctypes.c_int64()
         check(self.ctx, self.lib.dn_launch_count(self.ctx, ctypes.byref(n)))
         return n.value
+
+
+class B200LevelSetObjectBC:
+    """Post-operation form of the level-set wall (CPU_LevelSetObjectBC::operator(),
+    cpu_levelsetobjectbc.h:58-90) for the stage-by-stage RungeKutta sequence;
+    dn_rk_step applies it by itself."""
+
+    def __init__(self, iterator, field=0):
+        self.it = iterator
+        self.field = int(field)
+
+    def __call__(self):
+        check(self.it.ctx, self.it.lib.dn_apply_levelset_bc(self.it.ctx, self.field))
 
 
 # ------------------------------------------------------------- time integration

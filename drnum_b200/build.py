@@ -36,6 +36,8 @@ UNITS = {
     "dn_noalloc.cu": [],
     "dn_donor.cu": ["-fmad=false"],
     "dn_overlap.cpp": ["-Xcompiler", "-ffp-contract=off"],
+    "dn_levelset.cpp": ["-Xcompiler", "-ffp-contract=off"],
+    "dn_lsbc.cu": ["-fmad=false"],
 }
 
 

@@ -252,3 +252,27 @@ def jet_bcs(patches, core=0, mach_jet=0.8, radius=0.05, noise=1e-3, seed=1234):
     bcs[core][0] = (BC_INFLOW, None, jet_table(patches[core], mach_jet * A_INF, T_INF, radius, noise=noise,
                                                seed=seed))
     return bcs
+
+
+# ------------------------------------------------------------------ level sets
+
+def sphere_sdf(patch, centre, radius, fp32=True):
+    """Signed distance |x - c| - R of a sphere at every cell centre of a
+    patch (SphereLevelSet::calcDistance, spherelevelset.cpp:21-32), optionally
+    rounded to FP32 (the FP32 signed-distance field of the wall workload)."""
+    x, y, z = patch_centres(patch)
+    dx, dy, dz = x - centre[0], y - centre[1], z - centre[2]
+    g = np.sqrt(dx * dx + dy * dy + dz * dz) - radius
+    g = np.broadcast_to(g, tuple(patch["n"]))
+    return np.ascontiguousarray(g.astype(np.float32).astype(np.float64) if fp32 else g)
+
+
+def uniform_state(patches, mach=0.5, p=P_INF, T=T_INF):
+    """Free stream at `mach` along x on every patch."""
+    out = []
+    for q in patches:
+        shape = tuple(q["n"])
+        out.append(np.ascontiguousarray(prim_to_cons(np.full(shape, p), np.full(shape, T),
+                                                     np.full(shape, mach * A_INF), np.zeros(shape),
+                                                     np.zeros(shape))))
+    return out

@@ -13,6 +13,8 @@
 #include "fv_fx32.cuh"
 #include "dn_donor.cuh"
 #include "dn_overlap.h"
+#include "dn_levelset.h"
+#include "dn_lsbc.cuh"
 
 #include <cmath>
 #include <cstdarg>
@@ -58,6 +60,12 @@ struct dn_ctx {
   bool plan_dirty = true;
   std::vector<void*> plan_mem;
   dn::DonorPlan plan{};
+  // level-set layers per patch and their device form
+  std::vector<dn::LevelSetLayers> ls;
+  std::vector<char> ls_on;
+  bool ls_dirty = true;
+  std::vector<void*> ls_mem;
+  dn::LsPlan ls_plan{};
 };
 
 namespace {
@@ -299,6 +307,8 @@ int read_device_error(dn_ctx* c)
       return fail(c, DN_ERR_RANGE, "fixed-point offset left its range (|o| >= 2^30) during a stage "
                   "(first at cell %llu var %llu: f_n offset %.9g, residual %.9g quanta)", info[0], info[1], un, r);
     if (h & 2) return fail(c, DN_ERR_RANGE, "uploaded state outside the FP32 offset range of the patch base/quantum");
+    if (h & 4) return fail(c, DN_ERR_RANGE, "an interpolated receiving cell left the offset range of its patch");
+    if (h & 8) return fail(c, DN_ERR_RANGE, "a level-set wall cell left the offset range of its patch");
     return fail(c, DN_ERR_DEVICE, "device error word 0x%x", h);
   }
   return DN_OK;
@@ -438,6 +448,92 @@ int build_plan(dn_ctx* c)
   return DN_OK;
 }
 
+// ------------------------------------------------------- level-set plan
+
+void free_ls_plan(dn_ctx* c)
+{
+  for (void* m : c->ls_mem) cudaFree(m);
+  c->ls_mem.clear();
+  c->ls_plan = dn::LsPlan{};
+}
+
+template <typename T>
+int ls_upload(dn_ctx* c, const std::vector<T>& h, const T** out)
+{
+  *out = nullptr;
+  if (h.empty()) return DN_OK;
+  void* d = nullptr;
+  cudaError_t e = cudaMalloc(&d, h.size() * sizeof(T));
+  if (e != cudaSuccess) return fail(c, DN_ERR_NOMEM, "cudaMalloc(level-set plan)");
+  c->ls_mem.push_back(d);
+  e = cudaMemcpyAsync(d, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice, c->stream);
+  if (e != cudaSuccess) return cuda_fail(c, e, "level-set plan upload");
+  *out = static_cast<const T*>(d);
+  return DN_OK;
+}
+
+// Flattens the inner layer cells of all patches with a level set (patch,
+// layer, cell order, as LevelSetObjectBC::transferCellLayerData,
+// levelsetobjectbc.cpp:38-134) and uploads them.
+int build_ls_plan(dn_ctx* c)
+{
+  free_ls_plan(c);
+  const size_t np = c->patches.size();
+  std::vector<int32_t> patch;
+  std::vector<int64_t> cell, donor, nc(np);
+  std::vector<double> grad, w, base(np * 5), quantum(np * 5);
+  std::vector<void*> bufs(np * 3);
+  for (size_t r = 0; r < np; ++r) {
+    const DnPatch& P = c->patches[r];
+    nc[r] = (int64_t)P.nc;
+    for (int b = 0; b < 3; ++b) bufs[r * 3 + b] = P.buf[b];
+    for (int v = 0; v < 5; ++v) { base[r * 5 + v] = P.base[v]; quantum[r * 5 + v] = P.quantum[v]; }
+    if (r >= c->ls.size() || !c->ls_on[r]) continue;
+    for (const auto& layer : c->ls[r].inner) {
+      for (const dn::LayerCell& lc : layer) {
+        patch.push_back((int32_t)r);
+        cell.push_back((int64_t)lc.cell);
+        for (int a = 0; a < 3; ++a) grad.push_back(lc.grad[a]);
+        for (int q = 0; q < 8; ++q) { donor.push_back((int64_t)lc.donor[q]); w.push_back(lc.weight[q]); }
+      }
+    }
+  }
+  if (patch.size() >= (size_t)INT32_MAX) return fail(c, DN_ERR_RANGE, "too many level-set layer cells");
+  dn::LsPlan& L = c->ls_plan;
+  L.n = (int32_t)patch.size();
+  int s;
+  if ((s = ls_upload(c, patch, &L.patch)) || (s = ls_upload(c, cell, &L.cell)) || (s = ls_upload(c, grad, &L.grad)) ||
+      (s = ls_upload(c, donor, &L.donor)) || (s = ls_upload(c, w, &L.w)) || (s = ls_upload(c, nc, &L.nc)) ||
+      (s = ls_upload(c, base, &L.base)) || (s = ls_upload(c, quantum, &L.quantum)) ||
+      (s = ls_upload(c, bufs, &L.bufs))) {
+    free_ls_plan(c);
+    return s;
+  }
+  if (L.n > 0) {
+    void* d = nullptr;
+    cudaError_t e = cudaMalloc(&d, (size_t)L.n * 5 * sizeof(double));
+    if (e != cudaSuccess) { free_ls_plan(c); return fail(c, DN_ERR_NOMEM, "cudaMalloc(level-set scratch)"); }
+    c->ls_mem.push_back(d);
+    L.acc = static_cast<double*>(d);
+  }
+  c->ls_dirty = false;
+  return DN_OK;
+}
+
+// Level-set slip-wall condition on physical buffer `b` of every patch.
+int levelset_bc(dn_ctx* c, int b)
+{
+  bool any = false;
+  for (char on : c->ls_on) any = any || on;
+  if (!any) return DN_OK;
+  int s;
+  if (c->ls_dirty && (s = build_ls_plan(c))) return s;
+  cudaError_t e = dn::launch_levelset_bc(c->ls_plan, b, c->precision != DN_FP64, c->d_err, c->stream);
+  c->launches += 2;
+  if (e != cudaSuccess) return cuda_fail(c, e, "level-set boundary launch");
+  return DN_OK;
+}
+
 // Donor copy into physical buffer `b` of every patch.
 int donor_copy(dn_ctx* c, int b)
 {
@@ -522,6 +618,7 @@ int upload_impl(dn_ctx* c, int id, int field, const H* host)
   if (c->precision == DN_FP32 && !p.base_set) {
     derive_base(p, host);
     c->plan_dirty = true;
+  c->ls_dirty = true;
   }
   if ((s = ensure_staging(c, n * sizeof(H)))) return s;
   e = cudaMemcpyAsync(c->staging, host, n * sizeof(H), cudaMemcpyHostToDevice, c->stream);
@@ -609,6 +706,7 @@ int dn_ctx_destroy(dn_ctx* c)
     for (int sd = 0; sd < 6; ++sd) if (p.wall.table[sd]) cudaFree((void*)p.wall.table[sd]);
   }
   free_plan(c);
+  free_ls_plan(c);
   if (c->staging) cudaFree(c->staging);
   if (c->d_partials) cudaFree(c->d_partials);
   if (c->d_err) cudaFree(c->d_err);
@@ -676,7 +774,10 @@ int dn_patch_add(dn_ctx* c, const dn_patch_desc* d, int* id)
   }
   c->patches.push_back(p);
   c->tables.resize(c->patches.size());
+  c->ls.resize(c->patches.size());
+  c->ls_on.resize(c->patches.size(), 0);
   c->plan_dirty = true;
+  c->ls_dirty = true;
   *id = (int)c->patches.size() - 1;
   return DN_OK;
 }
@@ -697,6 +798,7 @@ int dn_patch_set_base(dn_ctx* c, int id, const double base[5], const double rang
   }
   p.base_set = true;
   c->plan_dirty = true;
+  c->ls_dirty = true;
   return DN_OK;
 }
 
@@ -769,16 +871,21 @@ int dn_rk_step(dn_ctx* c, double dt, const double* alpha, int n_alpha)
   int in = A;
   int st;
   // copyDonorData(0) before the step-start copy (rungekutta.cpp:30); the
-  // copy before each later stage (:34-36) repeats the previous stage's and
-  // is skipped
+  // copy before each later stage (:34-36) repeats the previous stage's, so
+  // it is skipped unless a post-operation (the level-set wall) may have
+  // changed donor cells since
+  bool post_op = false;
+  for (char on : c->ls_on) post_op = post_op || on;
   if ((st = donor_copy(c, A))) return st;
   for (int s = 0; s < n_alpha; ++s) {
     const int out = (s & 1) ? Y : X;
     const double factor = alpha[s] * dt;   // (*i)*dt, rungekutta.cpp:37
+    if (s > 0 && post_op && (st = donor_copy(c, in))) return st;
     for (auto& p : c->patches) {
       if ((st = stage_patch(c, p, in, A, out, factor))) return st;
     }
     if ((st = donor_copy(c, out))) return st;   // copyDonorData(0) after the stage (:38)
+    if ((st = levelset_bc(c, out))) return st;   // runPostOperations() (:39)
     in = out;
   }
   c->fmap[0] = in;
@@ -948,6 +1055,7 @@ int dn_grid_compute_dependencies(dn_ctx* c, int64_t* no_donor)
   for (const auto& x : t) nd += x.no_donor;
   c->tables.swap(t);
   c->plan_dirty = true;
+  c->ls_dirty = true;
   if (no_donor) *no_donor = nd;
   return DN_OK;
 }
@@ -1033,7 +1141,75 @@ int dn_patch_set_donors(dn_ctx* c, int id, const int64_t counts[4], const uint64
   }
   c->tables[id] = std::move(t);
   c->plan_dirty = true;
+  c->ls_dirty = true;
   return DN_OK;
+}
+
+int dn_patch_set_levelset(dn_ctx* c, int id, const double* G, int num_inner_layers, int num_outer_layers,
+                          double min_inner_rel_dist)
+{
+  int s = check_patch(c, id);
+  if (s) return s;
+  if (!G) {
+    c->ls_on[id] = 0;
+    c->ls[id] = dn::LevelSetLayers();
+    c->ls_dirty = true;
+    return DN_OK;
+  }
+  if (!(min_inner_rel_dist <= 0) && !std::isfinite(min_inner_rel_dist))
+    return fail(c, DN_ERR_ARG, "min_inner_rel_dist must be finite");
+  for (size_t l = 0; l < c->patches[id].nc; ++l)
+    if (!std::isfinite(G[l])) return fail(c, DN_ERR_ARG, "level-set value of cell %zu is not finite", l);
+  dn::LevelSetLayers L;
+  std::string err;
+  if (!dn::classify_levelset(dn::overlap_patch(c->patches[id].d), G, num_inner_layers, num_outer_layers,
+                             min_inner_rel_dist, L, err))
+    return fail(c, DN_ERR_ARG, "%s", err.c_str());
+  c->ls[id] = std::move(L);
+  c->ls_on[id] = 1;
+  c->ls_dirty = true;
+  return DN_OK;
+}
+
+int dn_patch_levelset_count(dn_ctx* c, int id, int inner, int layer, int64_t* n)
+{
+  int s = check_patch(c, id);
+  if (s) return s;
+  if (!n) return fail(c, DN_ERR_ARG, "n is NULL");
+  const auto& lists = inner ? c->ls[id].inner : c->ls[id].outer;
+  if (layer < 0 || layer >= (int)lists.size()) return fail(c, DN_ERR_ARG, "layer %d does not exist", layer);
+  *n = (int64_t)lists[layer].size();
+  return DN_OK;
+}
+
+int dn_patch_levelset_get(dn_ctx* c, int id, int inner, int layer, uint64_t* cells, double* g, double* grad,
+                          uint64_t* donors, double* weights)
+{
+  int s = check_patch(c, id);
+  if (s) return s;
+  const auto& lists = inner ? c->ls[id].inner : c->ls[id].outer;
+  if (layer < 0 || layer >= (int)lists.size()) return fail(c, DN_ERR_ARG, "layer %d does not exist", layer);
+  size_t q = 0;
+  for (const dn::LayerCell& lc : lists[layer]) {
+    if (cells) cells[q] = lc.cell;
+    if (g) g[q] = lc.g;
+    for (int a = 0; a < 3; ++a) if (grad) grad[3 * q + a] = lc.grad[a];
+    for (int t = 0; t < 8; ++t) {
+      if (donors) donors[8 * q + t] = lc.donor[t];
+      if (weights) weights[8 * q + t] = lc.weight[t];
+    }
+    ++q;
+  }
+  return DN_OK;
+}
+
+int dn_apply_levelset_bc(dn_ctx* c, int field)
+{
+  if (!c) return DN_ERR_ARG;
+  int s;
+  if ((s = check_field(c, field))) return s;
+  if (set_device(c) != DN_OK) return DN_ERR_CUDA;
+  return levelset_bc(c, c->fmap[field]);
 }
 
 int dn_copy_donor_data(dn_ctx* c, int field)

@@ -84,7 +84,7 @@ typedef std::pair<size_t, double> Contrib;
 // `dz`, cleaned like the reference: merge equal indices in sorted order, drop
 // |w| < 10*eps, shift so the weights sum to one.  Returns 1 (weights), 0 (the
 // point is outside the donor zone) or -1 (see linear_coeff).
-int donor_weights(const Zone& dz, const double xyz[3], std::vector<Contrib>& ws)
+int donor_weights(const Zone& dz, const double xyz[3], std::vector<Contrib>& ws, size_t* pad_index = nullptr)
 {
   size_t ref[3];
   double c[3];
@@ -127,15 +127,22 @@ int donor_weights(const Zone& dz, const double xyz[3], std::vector<Contrib>& ws)
     else ws[++keep] = ws[it];
   }
   ws.resize(keep + 1);
-  // drop small weights (absolute threshold 10 * 1e-5)
+  // drop small weights (absolute threshold 10 * 1e-5), erasing in place:
+  // the slot just past the shortened list then holds the last entry before
+  // the final erase, which the reference's fixed-size transfer reads as its
+  // padding index (WeightedSet::tranferToFixedArrays, weightedset.h:655-659)
   const double eps = 10 * 1.e-5;
-  size_t o = 0;
-  for (size_t it = 0; it < ws.size(); ++it) {
+  size_t it = 0;
+  while (it < ws.size()) {
     double t = ws[it].second;
     if (t < 0.) t = -t;
-    if (!(t < eps)) ws[o++] = ws[it];
+    if (t < eps) {
+      if (pad_index) *pad_index = ws.back().first;
+      ws.erase(ws.begin() + (long)it);
+    } else {
+      ++it;
+    }
   }
-  ws.resize(o);
   // shift to a weight sum of one
   if (!ws.empty()) {
     double sum = 0.;
@@ -162,6 +169,12 @@ struct Entry {
 };
 
 } // namespace
+
+int cc_interpolation_weights(const OverlapPatch& p, const double xyz[3], std::vector<std::pair<size_t, double>>& ws,
+                             size_t* pad_index)
+{
+  return donor_weights(make_zone(p), xyz, ws, pad_index);
+}
 
 bool build_overlap(const std::vector<OverlapPatch>& patches, std::vector<DonorTables>& out, std::string& err)
 {

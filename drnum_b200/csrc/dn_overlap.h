@@ -56,6 +56,15 @@ struct DonorTables {
 // patch description is invalid.
 bool build_overlap(const std::vector<OverlapPatch>& patches, std::vector<DonorTables>& out, std::string& err);
 
+// Cell-centred trilinear interpolation weights of point xyz (patch frame)
+// inside the donor zone of patch p (CartesianPatch::computeCCDataInterpolCoeffs_V1,
+// cartesianpatch.cpp:1166-1299).  Returns 1 with the weights, 0 outside the
+// donor zone, -1 where the reference stops with a BUG.  *pad_index (when
+// given and some weight was dropped) receives the index the reference's
+// fixed-size transfer pads with.
+int cc_interpolation_weights(const OverlapPatch& p, const double xyz[3], std::vector<std::pair<size_t, double>>& ws,
+                             size_t* pad_index);
+
 // Cell spacing of a patch description: length/n where a length is given
 // (CartesianPatch::computeDeltas, cartesianpatch.cpp:160-165), else dx/dy/dz.
 void desc_spacing(const struct dn_patch_desc& d, double out[3]);

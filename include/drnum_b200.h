@@ -22,6 +22,8 @@
  *   Patch::computeVariableDifference (patch.cpp:733-746)     dn_field_difference
  *   PatchGrid::computeDependencies (patchgrid.cpp:119-268)   dn_grid_compute_dependencies
  *   PatchIterator::copyDonorData (patchiterator.h:106-111)   dn_copy_donor_data
+ *   LevelSetObject + CPU_LevelSetObjectBC                    dn_patch_set_levelset,
+ *     (levelsetobject.cpp:44-388, cpu_levelsetobjectbc.h)    dn_apply_levelset_bc
  *
  * Conventions
  *   - Every call returns an int status: DN_OK (0) or a negative DN_ERR_*.
@@ -216,6 +218,45 @@ int dn_overlap_destroy(dn_overlap* ov);
  * (patchiterator.h:106-111) -> Patch::accessDonorDataDirect (patch.cpp:573-653),
  * GPU_PatchIterator::copyDonorData (gpu_patchiterator.h:190-233). */
 int dn_copy_donor_data(dn_ctx* ctx, int field);
+
+/* Level-set slip wall of one patch: classifies the cell layers next to the
+ * zero level of the signed-distance field G ([ni][nj][nk], host, FP64 values;
+ * an FP32 field is passed widened) and, from then on, applies the slip-wall
+ * mirror condition to the inner layers after every RK stage (after the
+ * donor copy, as a post-operation).  num_inner_layers/num_outer_layers and
+ * min_inner_rel_dist as LevelSetObject's constructor; G = NULL removes the
+ * wall.  The layer lists equal the reference's.
+ * Replaces: LevelSetObject::update/extractBCellLayers (levelsetobject.cpp:44-388),
+ * LevelSetObjectBC::transferCellLayerData (levelsetobjectbc.cpp:38-134) and
+ * CPU_LevelSetObjectBC<LSOBCCompressibleEulerOp> (cpu_levelsetobjectbc.h:58-90,
+ * lsobccompressibleeulerop.h:49-144). */
+int dn_patch_set_levelset(dn_ctx* ctx, int patch_id, const double* G, int num_inner_layers,
+                          int num_outer_layers, double min_inner_rel_dist);
+
+/* Size and contents of one layer of a patch's level-set classification
+ * (inner = 1: G < 0 layers, 0: outer layers), in the reference's order:
+ * cell index, G, normalised gradient [n][3], mirror-point donors and weights
+ * [n][8] (inner layers; outer layers carry zeros).  Any output may be NULL.
+ * Replaces: LevelSetObject::getInnerCellsLayers/getOuterCellsLayers
+ * (levelsetobject.h:128-131), LSLayerDataExtrapol (lslayerdataextrapol.h:19-34). */
+int dn_patch_levelset_count(dn_ctx* ctx, int patch_id, int inner, int layer, int64_t* n);
+int dn_patch_levelset_get(dn_ctx* ctx, int patch_id, int inner, int layer, uint64_t* cells, double* g,
+                          double* grad, uint64_t* donors, double* weights);
+
+/* The level-set wall condition alone, on field `field` of every patch with a
+ * level set.  Replaces: CPU_LevelSetObjectBC::operator() (cpu_levelsetobjectbc.h:58-90). */
+int dn_apply_levelset_bc(dn_ctx* ctx, int field);
+
+/* Host-only form of the classification (no context, no GPU): the layers of
+ * one patch description.  Read with dn_lslayers_count/dn_lslayers_get (same
+ * layout as dn_patch_levelset_get), free with dn_lslayers_destroy. */
+typedef struct dn_lslayers dn_lslayers;
+int dn_levelset_classify(const dn_patch_desc* patch, const double* G, int num_inner_layers,
+                         int num_outer_layers, double min_inner_rel_dist, dn_lslayers** out);
+int dn_lslayers_count(const dn_lslayers* ls, int inner, int layer, int64_t* n);
+int dn_lslayers_get(const dn_lslayers* ls, int inner, int layer, uint64_t* cells, double* g, double* grad,
+                    uint64_t* donors, double* weights);
+int dn_lslayers_destroy(dn_lslayers* ls);
 
 /* Number of device kernel launches the context has issued so far. */
 int dn_launch_count(const dn_ctx* ctx, int64_t* count);

@@ -200,10 +200,14 @@ class RefGrid:
     reference library): donor tables from PatchGrid::computeDependencies and
     RK steps with Patch::accessDonorDataDirect after every stage."""
 
-    def __init__(self, patches, add_protect=0, threads=1):
+    def __init__(self, patches, add_protect=0, threads=1, num_vars=5):
         lib = ref_lib()
-        lib.dnref_grid_create.restype = c_void_p
-        lib.dnref_grid_create.argtypes = [c_int, POINTER(c_int), _P, _P, POINTER(c_int), c_int, c_int]
+        lib.dnref_grid_create_nv.restype = c_void_p
+        lib.dnref_grid_create_nv.argtypes = [c_int, POINTER(c_int), _P, _P, POINTER(c_int), c_int, c_int, c_int]
+        lib.dnref_grid_levelset.restype = c_int
+        lib.dnref_grid_levelset.argtypes = [c_void_p, POINTER(_P), c_int, c_int, c_double]
+        lib.dnref_grid_levelset_layer.restype = c_int
+        lib.dnref_grid_levelset_layer.argtypes = [c_void_p, c_int, c_int, c_int, c_void_p] + [c_void_p] * 5
         lib.dnref_grid_tables.restype = c_int
         lib.dnref_grid_tables.argtypes = [c_void_p, c_int] + [c_void_p] * 8
         for nm in ("dnref_grid_set_state", "dnref_grid_get_state"):
@@ -218,9 +222,9 @@ class RefGrid:
         self.lib = lib
         self.patches = patches
         n, o, L, s = _grid_arrays(patches)
-        self.h = lib.dnref_grid_create(len(patches), n.ctypes.data_as(POINTER(c_int)), o.ctypes.data_as(_P),
-                                       L.ctypes.data_as(_P), s.ctypes.data_as(POINTER(c_int)),
-                                       int(add_protect), int(threads))
+        self.h = lib.dnref_grid_create_nv(len(patches), n.ctypes.data_as(POINTER(c_int)), o.ctypes.data_as(_P),
+                                          L.ctypes.data_as(_P), s.ctypes.data_as(POINTER(c_int)),
+                                          int(add_protect), int(threads), int(num_vars))
         if not self.h:
             raise RuntimeError("reference grid creation failed")
 
@@ -251,6 +255,29 @@ class RefGrid:
                                         None if ta is None else ta.ctypes.data_as(_P))
         if rc != 0:
             raise RuntimeError(f"reference set_bc failed: {rc}")
+
+    def levelset(self, G, num_inner, num_outer, min_inner_rel_dist):
+        """G: list per patch of [ni][nj][nk] level-set values or None (the
+        grid must have num_vars=6)."""
+        keep = [None if g is None else np.ascontiguousarray(g, dtype=np.float64) for g in G]
+        arr = (_P * len(keep))(*[None if g is None else g.ctypes.data_as(_P) for g in keep])
+        rc = self.lib.dnref_grid_levelset(self.h, arr, int(num_inner), int(num_outer), float(min_inner_rel_dist))
+        if rc != 0:
+            raise RuntimeError(f"reference level set failed: {rc}")
+
+    def levelset_layer(self, p, inner, layer):
+        n = ctypes.c_longlong()
+        rc = self.lib.dnref_grid_levelset_layer(self.h, p, inner, layer, ctypes.addressof(n), None, None, None,
+                                                None, None)
+        if rc != 0:
+            raise RuntimeError(f"reference level-set layer failed: {rc}")
+        m = n.value
+        d = {"cells": np.zeros(m, np.uint64), "g": np.zeros(m), "grad": np.zeros((m, 3)),
+             "donors": np.zeros((m, 8), np.uint64), "weights": np.zeros((m, 8))}
+        self.lib.dnref_grid_levelset_layer(self.h, p, inner, layer, ctypes.addressof(n), d["cells"].ctypes.data,
+                                           d["g"].ctypes.data, d["grad"].ctypes.data, d["donors"].ctypes.data,
+                                           d["weights"].ctypes.data)
+        return d
 
     def set_state(self, p, U):
         U = np.ascontiguousarray(U, dtype=np.float64)
@@ -317,7 +344,43 @@ def oracle_donor_copy(states, tables):
             Ur[:, c] = a
 
 
-def oracle_grid_run(states, spacings, tables, dt, steps, alpha=(0.25, 0.5, 1.0), bcs=None):
+def oracle_levelset_bc(states, layers):
+    """Slip-wall mirror condition (CPU_LevelSetObjectBC<LSOBCCompressibleEulerOp>,
+    cpu_levelsetobjectbc.h:58-90, lsobccompressibleeulerop.h:49-144) in place:
+    layers[p] = list of inner layer dicts (cells, grad, donors, weights) or None.
+    Pass 1 gathers every layer cell's mirror state, pass 2 writes the cells."""
+    acc = {}
+    for p, L in enumerate(layers):
+        if not L:
+            continue
+        U = states[p].reshape(5, -1)
+        for li, d in enumerate(L):
+            a = np.zeros((5, len(d["cells"])))
+            for t in range(8):
+                idx = d["donors"][:, t].astype(np.int64)
+                a = a + d["weights"][:, t] * U[:, idx]
+            acc[(p, li)] = a
+    relax, eps = 0.5, 1.e-6
+    for p, L in enumerate(layers):
+        if not L:
+            continue
+        U = states[p].reshape(5, -1)
+        for li, d in enumerate(L):
+            a = acc[(p, li)]
+            c = d["cells"].astype(np.int64)
+            gx, gy, gz = d["grad"][:, 0], d["grad"][:, 1], d["grad"][:, 2]
+            n = a[1] * gx + a[2] * gy + a[3] * gz
+            for m, g in ((1, gx), (2, gy), (3, gz)):
+                cur = U[m, c]
+                hard = a[m] - 2. * n * g
+                damp = np.abs(cur - hard) / (np.abs(cur) + eps)
+                damp = np.where(damp > (1. - relax), 1. - relax, damp)
+                U[m, c] = (1. - damp) * hard + damp * cur
+            U[0, c] = a[0]
+            U[4, c] = a[4]
+
+
+def oracle_grid_run(states, spacings, tables, dt, steps, alpha=(0.25, 0.5, 1.0), bcs=None, layers=None):
     """RK steps of a patch grid with the C restatement of the residual
     (closed patch faces, with the patch-face fluxes of bcs[p] = {side: (kind,
     params, table)}) and the numpy donor copy, in the order of
@@ -326,11 +389,15 @@ def oracle_grid_run(states, spacings, tables, dt, steps, alpha=(0.25, 0.5, 1.0),
     for _ in range(steps):
         oracle_donor_copy(U, tables)
         Un = [u.copy() for u in U]
-        for a in alpha:
+        for q, a in enumerate(alpha):
+            if q > 0:
+                oracle_donor_copy(U, tables)   # repeats the last copy unless a post-operation changed donors
             for p, u in enumerate(U):
                 hx, hy, hz = spacings[p]
                 res = oracle_residual_bc(u, (hx, hy, hz), (bcs or {}).get(p, {}))
                 pf = (a * dt) / (hx * hy * hz)
                 U[p] = Un[p] + pf * res
             oracle_donor_copy(U, tables)
+            if layers is not None:
+                oracle_levelset_bc(U, layers)
     return U

@@ -26,6 +26,9 @@
 #include "reconstruction/upwind2.h"
 #include "reconstruction/vanalbada.h"
 #include "iterators/cartesianiterator.h"
+#include "levelsetobject.h"
+#include "cpu_levelsetobjectbc.h"
+#include "lsobccompressibleeulerop.h"
 
 #include <chrono>
 #include <sstream>
@@ -345,16 +348,29 @@ int dnref_max_threads()
 // RungeKutta + CartesianIterator + Patch::accessDonorDataDirect step it.
 // Patch faces carry zero flux (closed); receiving cells are overwritten by
 // the donor copy after every stage.
+void* dnref_grid_create_nv(int np, const int* n, const double* origin, const double* length, const int* seek,
+                           int add_protect, int threads, int num_vars);
+
 struct DnRefGrid
 {
   PatchGrid grid;
   std::vector<CartesianPatch*> patches;
   GridBC bc;
+  LevelSetObject* lso = nullptr;
+  CPU_LevelSetObjectBC<LSOBCCompressibleEulerOp>* lsbc = nullptr;
 };
 
 // n[3*np], origin[3*np], length[3*np], seek[6*np] (imin imax jmin jmax kmin kmax)
 void* dnref_grid_create(int np, const int* n, const double* origin, const double* length, const int* seek,
                         int add_protect, int threads)
+{
+  return dnref_grid_create_nv(np, n, origin, length, seek, add_protect, threads, 5);
+}
+
+// As dnref_grid_create with num_vars variables per cell (6 keeps the level-set
+// field G in variable 5, as the test application does, testBlockObjects/main.h:384-388).
+void* dnref_grid_create_nv(int np, const int* n, const double* origin, const double* length, const int* seek,
+                           int add_protect, int threads, int num_vars)
 {
   if (sizeof(real) != 8 || np < 1) return nullptr;
 #ifdef OPEN_MP
@@ -362,7 +378,7 @@ void* dnref_grid_create(int np, const int* n, const double* origin, const double
 #endif
   DnRefGrid* g = new DnRefGrid();
   g->grid.setNumberOfFields(3);
-  g->grid.setNumberOfVariables(5);
+  g->grid.setNumberOfVariables(size_t(num_vars));
   g->grid.defineVectorVar(1);
   g->grid.setInterpolateData();
   g->grid.setNumSeekLayers(2);
@@ -435,6 +451,50 @@ int dnref_grid_tables(void* handle, int p, long long* counts, unsigned long long
   return 0;
 }
 
+// Level-set slip wall: G per patch (NULL entries: no wall, G = 1) into
+// variable 5 of field 0, the reference's LevelSetObject classification
+// (extractBCellLayers) and CPU_LevelSetObjectBC<LSOBCCompressibleEulerOp>
+// with abuse field 2 as a post-operation of every stage.  Needs num_vars 6.
+int dnref_grid_levelset(void* handle, const double* const* G, int num_inner, int num_outer, double min_inner_rel_dist)
+{
+  DnRefGrid* g = (DnRefGrid*)handle;
+  if (!g || g->patches.empty() || g->patches[0]->numVariables() < 6) return -1;
+  for (size_t p = 0; p < g->patches.size(); ++p) {
+    CartesianPatch* P = g->patches[p];
+    real* var = P->getVariable(0, 5);
+    for (size_t c = 0; c < P->variableSize(); ++c) var[c] = G[p] ? G[p][c] : 1.0;
+  }
+  g->lso = new LevelSetObject(nullptr, &g->grid, 0, 5, size_t(num_inner), size_t(num_outer), min_inner_rel_dist, -1.);
+  g->lso->extractBCellLayers();
+  LSOBCCompressibleEulerOp op;
+  g->lsbc = new CPU_LevelSetObjectBC<LSOBCCompressibleEulerOp>(0, g->lso, 2, op);
+  g->lsbc->transferCellLayerData();
+  return 0;
+}
+
+// One layer of patch p's classification: *n cells; arrays may be NULL.
+int dnref_grid_levelset_layer(void* handle, int p, int inner, int layer, long long* n, unsigned long long* cells,
+                              double* gv, double* grad, unsigned long long* donors, double* weights)
+{
+  DnRefGrid* g = (DnRefGrid*)handle;
+  if (!g || !g->lso || p < 0 || p >= int(g->patches.size())) return -1;
+  vector<vector<vector<LSLayerDataExtrapol> > >& L =
+      inner ? g->lso->getInnerCellsLayers() : g->lso->getOuterCellsLayers();
+  if (layer < 0 || layer >= int(L[p].size())) return -2;
+  const vector<LSLayerDataExtrapol>& cl = L[p][layer];
+  *n = (long long)cl.size();
+  for (size_t q = 0; q < cl.size(); ++q) {
+    if (cells) cells[q] = cl[q].m_Cell;
+    if (gv) gv[q] = cl[q].m_G;
+    if (grad) { grad[3*q] = cl[q].m_Gx; grad[3*q + 1] = cl[q].m_Gy; grad[3*q + 2] = cl[q].m_Gz; }
+    for (int t = 0; t < 8; ++t) {
+      if (donors) donors[8*q + t] = inner ? cl[q].m_MirrorDonor[t] : 0;
+      if (weights) weights[8*q + t] = inner ? cl[q].m_MirrorWeight[t] : 0.;
+    }
+  }
+  return 0;
+}
+
 // Field 0 of patch p, [5][ni][nj][nk].
 int dnref_grid_set_state(void* handle, int p, const double* U)
 {
@@ -479,6 +539,7 @@ int dnref_grid_run(void* handle, int steps, double dt, const double* alpha, int 
   RungeKutta rk;
   for (int a = 0; a < n_alpha; ++a) rk.addAlpha(alpha[a]);
   rk.addIterator(&iterator);
+  if (g->lsbc) rk.addPostOperation(g->lsbc);
   auto t0 = std::chrono::steady_clock::now();
   for (int s = 0; s < steps; ++s) rk(dt);
   auto t1 = std::chrono::steady_clock::now();

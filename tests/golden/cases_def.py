@@ -80,20 +80,42 @@ def grid_layout(name):
         return grid_layout("octants_8")
     if name == "bc_box":
         return [dict(n=(10, 8, 9), origin=(0.0, 0.0, 0.0), length=(1.0, 0.8, 0.9), seek=(0, 0, 0, 0, 0, 0))]
+    if name == "sphere_box":
+        return [dict(n=(20, 16, 16), origin=(0.0, 0.0, 0.0), length=(1.25, 1.0, 1.0), seek=(0, 0, 0, 0, 0, 0))]
+    if name == "sphere_pair":
+        return [dict(n=(14, 16, 16), origin=(0.0, 0.0, 0.0), length=(0.875, 1.0, 1.0), seek=(0, 2, 0, 0, 0, 0)),
+                dict(n=(14, 16, 16), origin=(0.5, 0.0, 0.0), length=(0.875, 1.0, 1.0), seek=(2, 0, 0, 0, 0, 0))]
     raise KeyError(name)
 
 
 GRID_ADD_PROTECT = {"random6_prot1": 1}
 # layouts whose donor tables are fixtures; the octant grids also store RK steps
 GRID_TABLES = ["pair_x", "embedded", "random6", "random6_prot1", "octants_8", "octants_ragged", "octants_jet",
-               "bc_box"]
-GRID_STEPS = {"octants_8": 3, "octants_ragged": 2, "octants_jet": 3, "bc_box": 3}
+               "bc_box", "sphere_box", "sphere_pair"]
+GRID_STEPS = {"octants_8": 3, "octants_ragged": 2, "octants_jet": 3, "bc_box": 3, "sphere_box": 3, "sphere_pair": 3}
+# level-set walls: name -> (centre, radius); 3 inner layers, no outer layer,
+# min_inner_rel_dist 0.1 (testBlockObjects/main.h:384-388), FP32 distance field
+LEVELSET = {"sphere_box": ((0.4, 0.5, 0.5), 0.2), "sphere_pair": ((0.6, 0.5, 0.5), 0.2)}
+LS_INNER, LS_OUTER, LS_MIN_REL = 3, 0, 0.1
+
+
+def grid_levelset(name):
+    """Per-patch level-set fields of a grid case (None without a wall)."""
+    if name not in LEVELSET:
+        return None
+    centre, radius = LEVELSET[name]
+    return [cases.sphere_sdf(p, centre, radius) for p in grid_layout(name)]
 
 
 def grid_case(name):
     """Layout, initial states, spacings and time step of a stepped grid case."""
     patches = grid_layout(name)
-    states = cases.grid_state(patches, centre=(0.45, 0.4, 0.45)) if name == "bc_box" else cases.grid_state(patches)
+    if name == "bc_box":
+        states = cases.grid_state(patches, centre=(0.45, 0.4, 0.45))
+    elif name in LEVELSET:
+        states = cases.uniform_state(patches, mach=0.5)
+    else:
+        states = cases.grid_state(patches)
     dt = cases.grid_dt(patches, states)
     spacings = [tuple(p["length"][a] / p["n"][a] for a in range(3)) for p in patches]
     return patches, states, spacings, dt, GRID_STEPS[name]
@@ -101,6 +123,8 @@ def grid_case(name):
 
 # grids with patch-face fluxes: layout name -> boundary conditions
 def grid_bcs(name):
+    if name in LEVELSET:
+        return cases.outer_farfield_bcs(grid_layout(name), (cases.P_INF, cases.T_INF, 0.5 * cases.A_INF, 0.0, 0.0))
     if name == "octants_jet":
         return cases.jet_bcs(grid_layout("octants_8"), radius=0.12, noise=1e-3)
     if name == "bc_box":

@@ -64,12 +64,20 @@ def make_grids():
     CartesianIterator + Patch::accessDonorDataDirect) for the octant grids."""
     for name in cases_def.GRID_TABLES:
         patches = cases_def.grid_layout(name)
-        g = pyoracle.RefGrid(patches, cases_def.GRID_ADD_PROTECT.get(name, 0), threads=1)
+        G = cases_def.grid_levelset(name)
+        g = pyoracle.RefGrid(patches, cases_def.GRID_ADD_PROTECT.get(name, 0), threads=1,
+                             num_vars=6 if G is not None else 5)
         arrays = {}
         for p in range(len(patches)):
             t = g.tables(p)
             for k, v in t.items():
                 arrays[f"p{p}_{k}"] = v
+        if G is not None:
+            g.levelset(G, cases_def.LS_INNER, cases_def.LS_OUTER, cases_def.LS_MIN_REL)
+            for p in range(len(patches)):
+                for layer in range(cases_def.LS_INNER):
+                    for k, v in g.levelset_layer(p, 1, layer).items():
+                        arrays[f"p{p}_ls{layer}_{k}"] = v
         bcs = cases_def.grid_bcs(name) or {}
         for p, sides in bcs.items():
             for side, (kind, params, table) in sides.items():

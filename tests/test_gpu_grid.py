@@ -11,7 +11,8 @@ import cases_def
 import pyoracle
 from drnum_b200 import _lib, cases
 from drnum_b200._lib import DN_FP32, DN_FP64
-from drnum_b200.api import AusmPlus, B200CartesianIterator, CartesianPatch, PatchGrid, RungeKutta
+from drnum_b200.api import (AusmPlus, B200CartesianIterator, B200LevelSetObjectBC, CartesianPatch, PatchGrid,
+                            RungeKutta)
 
 pytestmark = pytest.mark.gpu
 
@@ -31,12 +32,15 @@ def make_grid(name, precision, states=None):
     grid = PatchGrid()
     objs = []
     bcs = cases_def.grid_bcs(name) or {}
+    G = cases_def.grid_levelset(name)
     for q, (p, U) in enumerate(zip(patches, states)):
         cp = CartesianPatch(*p["n"], lengths=p["length"], origin=p["origin"], periodic=(False, False, False),
                             seek=p["seek"])
         cp.setField(0, U)
         for side, (kind, params, table) in bcs.get(q, {}).items():
             cp.setBoundary(side, kind, params, table)
+        if G is not None:
+            cp.setLevelSet(G[q], cases_def.LS_INNER, cases_def.LS_OUTER, cases_def.LS_MIN_REL)
         grid.insertPatch(cp)
         objs.append(cp)
     grid.computeDependencies()
@@ -105,7 +109,7 @@ def test_grid_stagewise_api_equals_fused_step(golden_dir):
         assert np.array_equal(cp.getField(0), z[f"p{p}_out"]), p
 
 
-@pytest.mark.parametrize("name,steps", [("octants_ragged", 6), ("octants_jet", 30)])
+@pytest.mark.parametrize("name,steps", [("octants_ragged", 6), ("octants_jet", 30), ("sphere_pair", 30)])
 def test_grid_fp32_against_fp64(name, steps):
     out = {}
     for prec in (DN_FP64, DN_FP32):
@@ -168,3 +172,35 @@ def test_boundary_kinds_rejected_where_invalid():
     assert lib.dn_patch_set_bc(ctx, pid, 2, _lib.DN_BC_FARFIELD, _lib.dptr(bad), None) == _lib.DN_ERR_ARG
     assert lib.dn_patch_set_bc(ctx, pid, 3, _lib.DN_BC_FARFIELD, _lib.dptr(ff), None) == _lib.DN_OK
     it.close()
+
+
+@pytest.mark.parametrize("name", sorted(cases_def.LEVELSET))
+def test_context_levelset_layers_equal_reference(golden_dir, name):
+    z = _fixture(golden_dir, name)
+    it, objs, _, _, _ = make_grid(name, DN_FP64)
+    for p in range(len(objs)):
+        L = it.levelSetLayers(p)
+        for layer in range(cases_def.LS_INNER):
+            for k in ("cells", "g", "grad", "donors", "weights"):
+                a, b = L["inner"][layer][k], z[f"p{p}_ls{layer}_{k}"]
+                if a.dtype == np.float64:
+                    a, b = a.view(np.uint64), b.view(np.uint64)
+                assert np.array_equal(a, b), (name, p, layer, k)
+    it.close()
+
+
+def test_levelset_stagewise_post_operation_equals_fused_step(golden_dir):
+    name = "sphere_pair"
+    z = _fixture(golden_dir, name)
+    it, objs, _, dt, steps = make_grid(name, DN_FP64)
+    rk = RungeKutta()
+    for a in cases.RK3_ALPHA:
+        rk.addAlpha(a)
+    rk.addIterator(it)
+    rk.addPostOperation(B200LevelSetObjectBC(it))
+    for _ in range(steps):
+        rk(dt)
+    it.updateHost(fields=(0,))
+    it.close()
+    for p, cp in enumerate(objs):
+        assert np.array_equal(cp.getField(0), z[f"p{p}_out"]), p

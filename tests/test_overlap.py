@@ -14,7 +14,7 @@ import pytest
 
 import cases_def
 import pyoracle
-from drnum_b200 import _lib
+from drnum_b200 import _lib, cases
 
 TABLE_KEYS = ("rec_unique", "donor_patch", "num_receivers", "stride", "rec_concat", "donor_idx", "weight")
 
@@ -100,7 +100,9 @@ def test_oracle_grid_steps_equal_reference(golden_dir, name):
     patches, states, spacings, dt, steps = cases_def.grid_case(name)
     assert float(z["dt"]) == dt and int(z["steps"]) == steps
     tables = [{k: z[f"p{p}_{k}"] for k in TABLE_KEYS} for p in range(len(patches))]
-    out = pyoracle.oracle_grid_run(states, spacings, tables, dt, steps, cases_def.ALPHA, cases_def.grid_bcs(name))
+    layers = _ls_tables(z, name, len(patches)) if name in cases_def.LEVELSET else None
+    out = pyoracle.oracle_grid_run(states, spacings, tables, dt, steps, cases_def.ALPHA, cases_def.grid_bcs(name),
+                                   layers)
     for p in range(len(patches)):
         assert np.array_equal(out[p], z[f"p{p}_out"]), (name, p, np.abs(out[p] - z[f"p{p}_out"]).max())
 
@@ -137,3 +139,75 @@ def test_overlap_build_rejects_invalid_layouts():
     assert lib.dn_overlap_build(None, 1, ctypes.byref(h), None) == _lib.DN_ERR_ARG
     assert lib.dn_overlap_build(_descs(bad), 0, ctypes.byref(h), None) == _lib.DN_ERR_ARG
     assert lib.dn_overlap_counts(None, 0, None) == _lib.DN_ERR_ARG
+
+
+# ------------------------------------------------------------------ level sets
+
+LS_KEYS = ("cells", "g", "grad", "donors", "weights")
+
+
+def classify(patch, G, num_inner, num_outer, min_rel):
+    lib = _lib.load()
+    h = ctypes.c_void_p()
+    rc = lib.dn_levelset_classify(ctypes.byref(_descs([patch])[0]), _lib.dptr(np.ascontiguousarray(G)),
+                                  num_inner, num_outer, min_rel, ctypes.byref(h))
+    assert rc == _lib.DN_OK
+    try:
+        return _lib.read_levelset_layers(lib.dn_lslayers_count, lib.dn_lslayers_get, h, (), num_inner, num_outer)
+    finally:
+        lib.dn_lslayers_destroy(h)
+
+
+@pytest.mark.parametrize("name", sorted(cases_def.LEVELSET))
+def test_levelset_layers_equal_reference_fixtures(golden_dir, name):
+    z = _fixture(golden_dir, name)
+    patches = cases_def.grid_layout(name)
+    for p, G in enumerate(cases_def.grid_levelset(name)):
+        L = classify(patches[p], G, cases_def.LS_INNER, cases_def.LS_OUTER, cases_def.LS_MIN_REL)
+        for layer in range(cases_def.LS_INNER):
+            for k in LS_KEYS:
+                assert _same(L["inner"][layer][k], z[f"p{p}_ls{layer}_{k}"]), (name, p, layer, k)
+
+
+@pytest.mark.skipif(not pyoracle.ref_available(), reason="compiled reference (oracle/_ref) not built")
+@pytest.mark.parametrize("seed", [21, 22, 23, 24])
+def test_levelset_layers_equal_live_reference(seed):
+    # random spheres, layer counts, replacement distances, inner and outer layers
+    rng = np.random.default_rng(seed)
+    n = tuple(int(x) for x in rng.integers(12, 20, 3))
+    patch = dict(n=n, origin=(0.0, 0.0, 0.0), length=tuple(x / 16 for x in n), seek=(0, 0, 0, 0, 0, 0))
+    centre = tuple(float(x) for x in rng.uniform(0.3, 0.5, 3))
+    G = cases.sphere_sdf(patch, centre, float(rng.uniform(0.15, 0.3)), fp32=bool(seed % 2))
+    ni, no, mr = int(rng.integers(1, 4)), int(rng.integers(0, 3)), float(rng.choice([0.0, 0.1, 0.4]))
+    ref = pyoracle.RefGrid([patch], num_vars=6)
+    ref.levelset([G], ni, no, mr)
+    mine = classify(patch, G, ni, no, mr)
+    for inner, num in ((1, ni), (0, no)):
+        for layer in range(num):
+            r = ref.levelset_layer(0, inner, layer)
+            m = mine["inner" if inner else "outer"][layer]
+            for k in LS_KEYS:
+                if not inner and k in ("donors", "weights"):
+                    continue
+                assert _same(m[k], r[k]), (seed, inner, layer, k)
+
+
+def test_levelset_classify_rejects_invalid_input():
+    lib = _lib.load()
+    patch = dict(n=(8, 8, 8), origin=(0.0, 0.0, 0.0), length=(0.5, 0.5, 0.5), seek=(0, 0, 0, 0, 0, 0))
+    G = cases.sphere_sdf(patch, (0.25, 0.25, 0.25), 0.1)
+    h = ctypes.c_void_p()
+    d = _descs([patch])[0]
+    assert lib.dn_levelset_classify(ctypes.byref(d), None, 3, 0, 0.1, ctypes.byref(h)) == _lib.DN_ERR_ARG
+    assert lib.dn_levelset_classify(ctypes.byref(d), _lib.dptr(G), 0, 0, 0.1, ctypes.byref(h)) == _lib.DN_ERR_ARG
+    assert lib.dn_levelset_classify(ctypes.byref(d), _lib.dptr(G), -1, 0, 0.0, ctypes.byref(h)) == _lib.DN_ERR_ARG
+
+
+def _ls_tables(z, name, num_patches):
+    out = []
+    for p in range(num_patches):
+        if f"p{p}_ls0_cells" not in z:
+            out.append(None)
+            continue
+        out.append([{k: z[f"p{p}_ls{layer}_{k}"] for k in LS_KEYS} for layer in range(cases_def.LS_INNER)])
+    return out
