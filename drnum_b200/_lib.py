@@ -27,6 +27,9 @@ DN_FP32 = 1
 DN_FACE_PERIODIC = 0
 DN_FACE_CLOSED = 1
 
+DN_OPT_BATCHED = 0
+DN_OPT_GRAPH = 1
+
 DN_BC_ZERO_FLUX = 0
 DN_BC_FARFIELD = 1
 DN_BC_SLIP = 2
@@ -92,6 +95,9 @@ SIGNATURES = {
     "dn_lslayers_get": (c_int, [c_void_p, c_int, c_int, POINTER(c_uint64), POINTER(c_double), POINTER(c_double),
                                 POINTER(c_uint64), POINTER(c_double)]),
     "dn_lslayers_destroy": (c_int, [c_void_p]),
+    "dn_set_option": (c_int, [c_void_p, c_int, c_int]),
+    "dn_patch_set_tile": (c_int, [c_void_p, c_int, c_int]),
+    "dn_autotune": (c_int, [c_void_p, ctypes.c_char_p, POINTER(c_double)]),
 }
 
 _lib = None

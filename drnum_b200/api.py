@@ -378,6 +378,22 @@ class B200CartesianIterator:
                                                      ctypes.byref(mx), ctypes.byref(l2)))
         return mx.value, l2.value
 
+    def setOption(self, option, value):
+        """dn_set_option: DN_OPT_BATCHED (one launch per stage over all
+        patches) or DN_OPT_GRAPH (CUDA-graph replay of whole steps)."""
+        check(self.ctx, self.lib.dn_set_option(self.ctx, int(option), int(value)))
+
+    def setTile(self, i_patch, shape):
+        check(self.ctx, self.lib.dn_patch_set_tile(self.ctx, int(i_patch), int(shape)))
+
+    def autotune(self, cache_path=None):
+        """Measures the tile shapes on this case and picks one per patch;
+        returns the measured cost per padded cell (ns) of each shape."""
+        cost = np.zeros(2)
+        path = None if cache_path is None else str(cache_path).encode()
+        check(self.ctx, self.lib.dn_autotune(self.ctx, path, _lib.dptr(cost)))
+        return cost
+
     def launchCount(self):
         n = ctypes.c_int64()
         check(self.ctx, self.lib.dn_launch_count(self.ctx, ctypes.byref(n)))

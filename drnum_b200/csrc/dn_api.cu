@@ -15,6 +15,7 @@
 #include "dn_overlap.h"
 #include "dn_levelset.h"
 #include "dn_lsbc.cuh"
+#include "fv_batch.cuh"
 
 #include <cmath>
 #include <cstdarg>
@@ -38,6 +39,19 @@ struct DnPatch {
 };
 
 } // namespace
+
+// A captured RK step and what it was captured for.
+struct GraphEntry {
+  int A = 0, X = 0, Y = 0, n = 0;
+  double dt = 0, alpha[16] = {};
+  cudaGraphExec_t exec = nullptr;
+  int64_t launches = 0;
+  bool same(const GraphEntry& o) const
+  {
+    if (A != o.A || X != o.X || Y != o.Y || n != o.n || std::memcmp(&dt, &o.dt, sizeof dt)) return false;
+    return std::memcmp(alpha, o.alpha, sizeof(double) * n) == 0;
+  }
+};
 
 struct dn_ctx {
   int device = 0;
@@ -66,6 +80,19 @@ struct dn_ctx {
   bool ls_dirty = true;
   std::vector<void*> ls_mem;
   dn::LsPlan ls_plan{};
+  // batched stage launch: per-patch tile shape, patch records and work lists
+  bool batched = true;
+  std::vector<int> shape;
+  bool batch_dirty = true;
+  void* d_records = nullptr;
+  void* d_items[dn::kNumShapes] = {nullptr, nullptr};
+  int n_items[dn::kNumShapes] = {0, 0};
+  // CUDA graphs of whole RK steps; any change of the case bumps generation
+  bool use_graph = false;
+  std::vector<GraphEntry> graphs;
+  cudaStream_t graph_stream = nullptr;
+  int64_t generation = 0;
+  int64_t graph_generation = -1;
 };
 
 namespace {
@@ -547,6 +574,215 @@ int donor_copy(dn_ctx* c, int b)
   return DN_OK;
 }
 
+// ------------------------------------------------------------ RK step
+
+bool any_levelset(const dn_ctx* c)
+{
+  for (char on : c->ls_on) if (on) return true;
+  return false;
+}
+
+int stage_all(dn_ctx* c, int in_b, int un_b, int out_b, double factor);
+
+// Launches of one RK step (RungeKutta::operator(), rungekutta.cpp:27-42)
+// from step-start buffer A through the other two buffers X, Y.
+int rk_step_enqueue(dn_ctx* c, double dt, const double* alpha, int n_alpha, int A, int X, int Y)
+{
+  int in = A;
+  int st;
+  // copyDonorData(0) before the step-start copy (rungekutta.cpp:30); the
+  // copy before each later stage (:34-36) repeats the previous stage's, so
+  // it is skipped unless a post-operation (the level-set wall) may have
+  // changed donor cells since
+  const bool post_op = any_levelset(c);
+  if ((st = donor_copy(c, A))) return st;
+  for (int s = 0; s < n_alpha; ++s) {
+    const int out = (s & 1) ? Y : X;
+    const double factor = alpha[s] * dt;   // (*i)*dt, rungekutta.cpp:37
+    if (s > 0 && post_op && (st = donor_copy(c, in))) return st;
+    if ((st = stage_all(c, in, A, out, factor))) return st;
+    if ((st = donor_copy(c, out))) return st;   // copyDonorData(0) after the stage (:38)
+    if ((st = levelset_bc(c, out))) return st;   // runPostOperations() (:39)
+    in = out;
+  }
+  return DN_OK;
+}
+
+void free_graphs(dn_ctx* c)
+{
+  for (auto& gc : c->graphs) if (gc.exec) cudaGraphExecDestroy(gc.exec);
+  c->graphs.clear();
+}
+
+int build_batch(dn_ctx* c);
+int build_plan(dn_ctx* c);
+int build_ls_plan(dn_ctx* c);
+
+// The step as a CUDA graph: captured once per (buffer rotation, dt, alphas)
+// and replayed; everything that allocates (tables, work lists) is built
+// before the capture.
+int rk_step_graph(dn_ctx* c, double dt, const double* alpha, int n_alpha, int A, int X, int Y)
+{
+  int st;
+  if (c->batched && c->batch_dirty && (st = build_batch(c))) return st;
+  if (has_donors(c) && c->plan_dirty && (st = build_plan(c))) return st;
+  if (any_levelset(c) && c->ls_dirty && (st = build_ls_plan(c))) return st;
+  if (c->graph_stream != c->stream || c->graph_generation != c->generation) {
+    free_graphs(c);
+    c->graph_stream = c->stream;
+    c->graph_generation = c->generation;
+  }
+  GraphEntry key;
+  key.A = A; key.X = X; key.Y = Y; key.dt = dt; key.n = n_alpha;
+  for (int q = 0; q < n_alpha; ++q) key.alpha[q] = alpha[q];
+  GraphEntry* hit = nullptr;
+  for (auto& gc : c->graphs) if (gc.same(key)) hit = &gc;
+  if (!hit) {
+    if (c->graphs.size() >= 6) free_graphs(c);
+    cudaError_t e = cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeRelaxed);
+    if (e != cudaSuccess) return cuda_fail(c, e, "begin graph capture");
+    const int64_t l0 = c->launches;
+    st = rk_step_enqueue(c, dt, alpha, n_alpha, A, X, Y);
+    cudaGraph_t g = nullptr;
+    e = cudaStreamEndCapture(c->stream, &g);
+    if (st) { if (g) cudaGraphDestroy(g); return st; }
+    if (e != cudaSuccess) return cuda_fail(c, e, "end graph capture");
+    key.launches = c->launches - l0;
+    c->launches = l0;
+    e = cudaGraphInstantiate(&key.exec, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) return cuda_fail(c, e, "graph instantiate");
+    c->graphs.push_back(key);
+    hit = &c->graphs.back();
+  }
+  cudaError_t e = cudaGraphLaunch(hit->exec, c->stream);
+  if (e != cudaSuccess) return cuda_fail(c, e, "graph launch");
+  c->launches += hit->launches;
+  return DN_OK;
+}
+
+// ------------------------------------------------------------ batched stage
+
+void free_batch(dn_ctx* c)
+{
+  if (c->d_records) cudaFree(c->d_records);
+  c->d_records = nullptr;
+  for (int q = 0; q < dn::kNumShapes; ++q) {
+    if (c->d_items[q]) cudaFree(c->d_items[q]);
+    c->d_items[q] = nullptr;
+    c->n_items[q] = 0;
+  }
+}
+
+// Default tile shape of a patch: the one that wastes fewer k lanes
+// (k is the coalesced axis); ties go to the wider tile.
+int default_shape(const DnPatch& p)
+{
+  const int nk = p.d.nk;
+  const double e32 = (double)nk / (double)(((nk + 31) / 32) * 32);
+  const double e16 = (double)nk / (double)(((nk + 15) / 16) * 16);
+  return e16 > e32 + 1e-12 ? 1 : 0;
+}
+
+// Patch records and work items (patch, column tile, plane range) of every
+// patch, grouped by tile shape; plane ranges are sized so that the launch
+// holds about four waves of CTAs.
+int build_batch(dn_ctx* c)
+{
+  free_batch(c);
+  const size_t np = c->patches.size();
+  if (np == 0) { c->batch_dirty = false; return DN_OK; }
+  const bool fp64 = c->precision == DN_FP64;
+  std::vector<dn::BatchPatch> rec(np);
+  long tiles = 0;
+  for (size_t q = 0; q < np; ++q) {
+    const DnPatch& P = c->patches[q];
+    dn::BatchPatch& r = rec[q];
+    std::memset(&r, 0, sizeof(r));
+    for (int b = 0; b < 3; ++b) r.buf[b] = P.buf[b];
+    r.active = P.active;
+    r.ni = P.d.ni; r.nj = P.d.nj; r.nk = P.d.nk;
+    r.per_x = P.d.face[0] == DN_FACE_PERIODIC;
+    r.per_y = P.d.face[1] == DN_FACE_PERIODIC;
+    r.per_z = P.d.face[2] == DN_FACE_PERIODIC;
+    r.dx = P.d.dx; r.dy = P.d.dy; r.dz = P.d.dz;
+    for (int v = 0; v < 5; ++v) { r.base[v] = P.base[v]; r.quantum[v] = P.quantum[v]; }
+    r.wall = P.wall;
+    int tj, tk;
+    dn::shape_tile(fp64, c->shape[q], &tj, &tk);
+    tiles += (long)((P.d.nj + tj - 1) / tj) * ((P.d.nk + tk - 1) / tk);
+  }
+  const long want = (long)c->num_sms * 2 * 4;
+  long chunks = (want + tiles - 1) / tiles;
+  if (chunks < 1) chunks = 1;
+  std::vector<dn::WorkItem> items[dn::kNumShapes];
+  for (size_t q = 0; q < np; ++q) {
+    const DnPatch& P = c->patches[q];
+    const int sh = c->shape[q];
+    int tj, tk;
+    dn::shape_tile(fp64, sh, &tj, &tk);
+    long ic = (P.d.ni + chunks - 1) / chunks;
+    if (ic < 8) ic = 8;
+    if (ic > P.d.ni) ic = P.d.ni;
+    for (int i0 = 0; i0 < P.d.ni; i0 += (int)ic)
+      for (int j0 = 0; j0 < P.d.nj; j0 += tj)
+        for (int k0 = 0; k0 < P.d.nk; k0 += tk)
+          items[sh].push_back(dn::WorkItem{(int)q, j0, k0, i0, std::min(P.d.ni, i0 + (int)ic)});
+  }
+  cudaError_t e = cudaMalloc(&c->d_records, np * sizeof(dn::BatchPatch));
+  if (e != cudaSuccess) return fail(c, DN_ERR_NOMEM, "cudaMalloc(patch records)");
+  e = cudaMemcpyAsync(c->d_records, rec.data(), np * sizeof(dn::BatchPatch), cudaMemcpyHostToDevice, c->stream);
+  if (e != cudaSuccess) return cuda_fail(c, e, "patch record upload");
+  for (int q = 0; q < dn::kNumShapes; ++q) {
+    if (items[q].empty()) continue;
+    if (items[q].size() > (size_t)INT32_MAX) return fail(c, DN_ERR_RANGE, "too many work items");
+    e = cudaMalloc(&c->d_items[q], items[q].size() * sizeof(dn::WorkItem));
+    if (e != cudaSuccess) return fail(c, DN_ERR_NOMEM, "cudaMalloc(work items)");
+    e = cudaMemcpyAsync(c->d_items[q], items[q].data(), items[q].size() * sizeof(dn::WorkItem),
+                        cudaMemcpyHostToDevice, c->stream);
+    if (e != cudaSuccess) return cuda_fail(c, e, "work item upload");
+    c->n_items[q] = (int)items[q].size();
+  }
+  e = cudaStreamSynchronize(c->stream);   // host vectors go out of scope
+  if (e != cudaSuccess) return cuda_fail(c, e, "batch upload");
+  c->batch_dirty = false;
+  return DN_OK;
+}
+
+int stage_patch(dn_ctx* c, DnPatch& p, int in_b, int un_b, int out_b, double factor);
+
+// One RK stage of every patch: in_b -> out_b with step-start state un_b.
+int stage_all(dn_ctx* c, int in_b, int un_b, int out_b, double factor)
+{
+  // a single patch keeps its parameters in the kernel's constant bank (the
+  // batched form reads them from shared memory); the results are identical
+  if (!c->batched || c->patches.size() == 1) {
+    for (auto& p : c->patches) {
+      int s = stage_patch(c, p, in_b, un_b, out_b, factor);
+      if (s) return s;
+    }
+    return DN_OK;
+  }
+  int s;
+  if (c->batch_dirty && (s = build_batch(c))) return s;
+  for (int q = 0; q < dn::kNumShapes; ++q) {
+    if (!c->n_items[q]) continue;
+    dn::Batch b;
+    b.patches = static_cast<const dn::BatchPatch*>(c->d_records);
+    b.items = static_cast<const dn::WorkItem*>(c->d_items[q]);
+    b.n_items = c->n_items[q];
+    b.in_b = in_b; b.un_b = un_b; b.out_b = out_b;
+    b.factor = factor;
+    b.err = c->d_err;
+    b.err_info = c->d_err_info;
+    cudaError_t e = c->precision == DN_FP64 ? dn::launch_stage_f64_batched(b, q, c->stream)
+                                            : dn::launch_stage_fx32_batched(b, q, c->stream);
+    c->launches++;
+    if (e != cudaSuccess) return cuda_fail(c, e, "batched stage launch");
+  }
+  return DN_OK;
+}
+
 int stage_patch(dn_ctx* c, DnPatch& p, int in_b, int un_b, int out_b, double factor)
 {
   const double dx = p.d.dx, dy = p.d.dy, dz = p.d.dz;
@@ -619,6 +855,8 @@ int upload_impl(dn_ctx* c, int id, int field, const H* host)
     derive_base(p, host);
     c->plan_dirty = true;
   c->ls_dirty = true;
+  c->batch_dirty = true;
+  c->generation++;
   }
   if ((s = ensure_staging(c, n * sizeof(H)))) return s;
   e = cudaMemcpyAsync(c->staging, host, n * sizeof(H), cudaMemcpyHostToDevice, c->stream);
@@ -705,8 +943,10 @@ int dn_ctx_destroy(dn_ctx* c)
     if (p.active) cudaFree(p.active);
     for (int sd = 0; sd < 6; ++sd) if (p.wall.table[sd]) cudaFree((void*)p.wall.table[sd]);
   }
+  free_graphs(c);
   free_plan(c);
   free_ls_plan(c);
+  free_batch(c);
   if (c->staging) cudaFree(c->staging);
   if (c->d_partials) cudaFree(c->d_partials);
   if (c->d_err) cudaFree(c->d_err);
@@ -776,8 +1016,11 @@ int dn_patch_add(dn_ctx* c, const dn_patch_desc* d, int* id)
   c->tables.resize(c->patches.size());
   c->ls.resize(c->patches.size());
   c->ls_on.resize(c->patches.size(), 0);
+  c->shape.push_back(default_shape(c->patches.back()));
   c->plan_dirty = true;
   c->ls_dirty = true;
+  c->batch_dirty = true;
+  c->generation++;
   *id = (int)c->patches.size() - 1;
   return DN_OK;
 }
@@ -799,6 +1042,8 @@ int dn_patch_set_base(dn_ctx* c, int id, const double base[5], const double rang
   p.base_set = true;
   c->plan_dirty = true;
   c->ls_dirty = true;
+  c->batch_dirty = true;
+  c->generation++;
   return DN_OK;
 }
 
@@ -813,6 +1058,8 @@ int dn_patch_set_active(dn_ctx* c, int id, const uint8_t* mask)
   if (s) return s;
   if (set_device(c) != DN_OK) return DN_ERR_CUDA;
   DnPatch& p = c->patches[id];
+  c->batch_dirty = true;
+  c->generation++;
   if (!mask) {
     if (p.active) {
       cudaStreamSynchronize(c->stream);
@@ -852,10 +1099,8 @@ int dn_compute(dn_ctx* c, double factor)
   if (!c) return DN_ERR_ARG;
   if (!std::isfinite(factor)) return fail(c, DN_ERR_ARG, "factor is not finite");
   if (set_device(c) != DN_OK) return DN_ERR_CUDA;
-  for (auto& p : c->patches) {
-    int s = stage_patch(c, p, c->fmap[0], c->fmap[1], c->fmap[2], factor);
-    if (s) return s;
-  }
+  int s = stage_all(c, c->fmap[0], c->fmap[1], c->fmap[2], factor);
+  if (s) return s;
   std::swap(c->fmap[0], c->fmap[2]);
   return DN_OK;
 }
@@ -865,32 +1110,18 @@ int dn_rk_step(dn_ctx* c, double dt, const double* alpha, int n_alpha)
   if (!c) return DN_ERR_ARG;
   if (!alpha || n_alpha < 1 || n_alpha > 16) return fail(c, DN_ERR_ARG, "need 1..16 RK stage coefficients");
   if (!std::isfinite(dt)) return fail(c, DN_ERR_ARG, "dt is not finite");
+  for (int q = 0; q < n_alpha; ++q) if (!std::isfinite(alpha[q])) return fail(c, DN_ERR_ARG, "alpha not finite");
   if (set_device(c) != DN_OK) return DN_ERR_CUDA;
   // A = step-start state, X/Y = the two other buffers
   const int A = c->fmap[0], X = c->fmap[2], Y = c->fmap[1];
-  int in = A;
   int st;
-  // copyDonorData(0) before the step-start copy (rungekutta.cpp:30); the
-  // copy before each later stage (:34-36) repeats the previous stage's, so
-  // it is skipped unless a post-operation (the level-set wall) may have
-  // changed donor cells since
-  bool post_op = false;
-  for (char on : c->ls_on) post_op = post_op || on;
-  if ((st = donor_copy(c, A))) return st;
-  for (int s = 0; s < n_alpha; ++s) {
-    const int out = (s & 1) ? Y : X;
-    const double factor = alpha[s] * dt;   // (*i)*dt, rungekutta.cpp:37
-    if (s > 0 && post_op && (st = donor_copy(c, in))) return st;
-    for (auto& p : c->patches) {
-      if ((st = stage_patch(c, p, in, A, out, factor))) return st;
-    }
-    if ((st = donor_copy(c, out))) return st;   // copyDonorData(0) after the stage (:38)
-    if ((st = levelset_bc(c, out))) return st;   // runPostOperations() (:39)
-    in = out;
-  }
-  c->fmap[0] = in;
+  if (c->use_graph) st = rk_step_graph(c, dt, alpha, n_alpha, A, X, Y);
+  else st = rk_step_enqueue(c, dt, alpha, n_alpha, A, X, Y);
+  if (st) return st;
+  const int last = ((n_alpha - 1) & 1) ? Y : X;
+  c->fmap[0] = last;
   c->fmap[1] = A;
-  c->fmap[2] = (in == X) ? Y : X;
+  c->fmap[2] = (last == X) ? Y : X;
   return DN_OK;
 }
 
@@ -1040,6 +1271,8 @@ int dn_patch_set_bc(dn_ctx* c, int id, int side, int kind, const double* params,
   P.wall.kind[side] = kind;
   P.wall.any = 0;
   for (int q = 0; q < 6; ++q) if (P.wall.kind[q] != DN_BC_ZERO_FLUX) P.wall.any = 1;
+  c->batch_dirty = true;
+  c->generation++;
   return DN_OK;
 }
 
@@ -1056,6 +1289,8 @@ int dn_grid_compute_dependencies(dn_ctx* c, int64_t* no_donor)
   c->tables.swap(t);
   c->plan_dirty = true;
   c->ls_dirty = true;
+  c->batch_dirty = true;
+  c->generation++;
   if (no_donor) *no_donor = nd;
   return DN_OK;
 }
@@ -1142,6 +1377,8 @@ int dn_patch_set_donors(dn_ctx* c, int id, const int64_t counts[4], const uint64
   c->tables[id] = std::move(t);
   c->plan_dirty = true;
   c->ls_dirty = true;
+  c->batch_dirty = true;
+  c->generation++;
   return DN_OK;
 }
 
@@ -1154,6 +1391,7 @@ int dn_patch_set_levelset(dn_ctx* c, int id, const double* G, int num_inner_laye
     c->ls_on[id] = 0;
     c->ls[id] = dn::LevelSetLayers();
     c->ls_dirty = true;
+    c->generation++;
     return DN_OK;
   }
   if (!(min_inner_rel_dist <= 0) && !std::isfinite(min_inner_rel_dist))
@@ -1168,6 +1406,7 @@ int dn_patch_set_levelset(dn_ctx* c, int id, const double* G, int num_inner_laye
   c->ls[id] = std::move(L);
   c->ls_on[id] = 1;
   c->ls_dirty = true;
+  c->generation++;
   return DN_OK;
 }
 
@@ -1219,6 +1458,141 @@ int dn_copy_donor_data(dn_ctx* c, int field)
   if ((s = check_field(c, field))) return s;
   if (set_device(c) != DN_OK) return DN_ERR_CUDA;
   return donor_copy(c, c->fmap[field]);
+}
+
+int dn_set_option(dn_ctx* c, int option, int value)
+{
+  if (!c) return DN_ERR_ARG;
+  if (option == DN_OPT_BATCHED) {
+    c->batched = value != 0;
+    c->generation++;
+    return DN_OK;
+  }
+  if (option == DN_OPT_GRAPH) {
+    c->use_graph = value != 0;
+    return DN_OK;
+  }
+  return fail(c, DN_ERR_ARG, "unknown option %d", option);
+}
+
+int dn_patch_set_tile(dn_ctx* c, int id, int shape)
+{
+  int s = check_patch(c, id);
+  if (s) return s;
+  if (shape < 0 || shape >= dn::kNumShapes) return fail(c, DN_ERR_ARG, "tile shape %d is not 0..%d", shape, dn::kNumShapes - 1);
+  c->shape[id] = shape;
+  c->batch_dirty = true;
+  c->generation++;
+  return DN_OK;
+}
+
+namespace {
+
+// padded cells a patch occupies with tile shape `shape`
+double padded_cells(const dn_ctx* c, const DnPatch& p, int shape)
+{
+  int tj, tk;
+  dn::shape_tile(c->precision == DN_FP64, shape, &tj, &tk);
+  return (double)p.d.ni * (double)(((p.d.nj + tj - 1) / tj) * tj) * (double)(((p.d.nk + tk - 1) / tk) * tk);
+}
+
+std::string device_name(int dev)
+{
+  cudaDeviceProp prop;
+  if (cudaGetDeviceProperties(&prop, dev) != cudaSuccess) return "unknown";
+  return prop.name;
+}
+
+// cache lines: "<device>|<precision>|<cost shape 0>|<cost shape 1>"
+bool read_tune_cache(const char* path, const std::string& dev, int precision, double cost[2])
+{
+  if (!path) return false;
+  FILE* f = std::fopen(path, "r");
+  if (!f) return false;
+  char line[512];
+  bool found = false;
+  while (std::fgets(line, sizeof line, f)) {
+    char name[256];
+    int prec;
+    double c0, c1;
+    if (std::sscanf(line, "%255[^|]|%d|%lf|%lf", name, &prec, &c0, &c1) == 4 && dev == name && prec == precision) {
+      cost[0] = c0;
+      cost[1] = c1;
+      found = true;
+    }
+  }
+  std::fclose(f);
+  return found;
+}
+
+void write_tune_cache(const char* path, const std::string& dev, int precision, const double cost[2])
+{
+  if (!path) return;
+  FILE* f = std::fopen(path, "a");
+  if (!f) return;
+  std::fprintf(f, "%s|%d|%.17g|%.17g\n", dev.c_str(), precision, cost[0], cost[1]);
+  std::fclose(f);
+}
+
+} // namespace
+
+int dn_autotune(dn_ctx* c, const char* cache_path, double cost_out[2])
+{
+  if (!c) return DN_ERR_ARG;
+  if (c->patches.empty()) return fail(c, DN_ERR_STATE, "no patches to tune for");
+  if (set_device(c) != DN_OK) return DN_ERR_CUDA;
+  const std::string dev = device_name(c->device);
+  double cost[2] = {0, 0};
+  if (!read_tune_cache(cache_path, dev, c->precision, cost)) {
+    // measure each tile shape on the case itself: one stage of every patch
+    // into the scratch field (field 2), factor 0
+    const std::vector<int> saved = c->shape;
+    const bool saved_batched = c->batched;
+    c->batched = true;
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    int st = DN_OK;
+    for (int sh = 0; sh < dn::kNumShapes && st == DN_OK; ++sh) {
+      double padded = 0;
+      for (size_t q = 0; q < c->patches.size(); ++q) {
+        c->shape[q] = sh;
+        padded += padded_cells(c, c->patches[q], sh);
+      }
+      c->batch_dirty = true;
+      const int reps = 5;
+      for (int r = 0; r < 2 + reps && st == DN_OK; ++r) {
+        if (r == 2) cudaEventRecord(e0, c->stream);
+        st = stage_all(c, c->fmap[0], c->fmap[1], c->fmap[2], 0.0);
+      }
+      cudaEventRecord(e1, c->stream);
+      cudaEventSynchronize(e1);
+      float ms = 0;
+      cudaEventElapsedTime(&ms, e0, e1);
+      cost[sh] = (double)ms * 1e6 / reps / padded;      // ns per padded cell and stage
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    c->batched = saved_batched;
+    c->shape = saved;
+    if (st != DN_OK) { c->batch_dirty = true; c->generation++; return st; }
+    int s2 = read_device_error(c);
+    if (s2 != DN_OK) return s2;
+    write_tune_cache(cache_path, dev, c->precision, cost);
+  }
+  for (size_t q = 0; q < c->patches.size(); ++q) {
+    int best = 0;
+    double best_t = cost[0] * padded_cells(c, c->patches[q], 0);
+    for (int sh = 1; sh < dn::kNumShapes; ++sh) {
+      const double t = cost[sh] * padded_cells(c, c->patches[q], sh);
+      if (t < best_t) { best_t = t; best = sh; }
+    }
+    c->shape[q] = best;
+  }
+  c->batch_dirty = true;
+  c->generation++;
+  if (cost_out) { cost_out[0] = cost[0]; cost_out[1] = cost[1]; }
+  return DN_OK;
 }
 
 int dn_launch_count(const dn_ctx* c, int64_t* count)

@@ -2,6 +2,7 @@
 // operation order of fv_numerics.cuh this reproduces the reference CPU
 // iterator (compiled with -ffp-contract=off) bit for bit.
 #include "fv_launch.h"
+#include "fv_batch.cuh"
 
 namespace dn {
 
@@ -22,6 +23,25 @@ cudaError_t launch_stage_f64(const StageArgs<PolicyF64>& a, const StageShape& s,
             (a.g.ni + a.g.i_chunk - 1) / a.g.i_chunk);
   kern<<<grid, block, sizeof(Smem), st>>>(a);
   return cudaGetLastError();
+}
+
+namespace {
+template <int TJ, int TK>
+cudaError_t launch_f64_batched(const Batch& b, cudaStream_t st)
+{
+  using Smem = StageSmem<PolicyF64, TJ, TK>;
+  auto kern = fv_stage_batched_f64<TJ, TK>;
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(Smem));
+  if (e != cudaSuccess) return e;
+  kern<<<b.n_items, dim3(TK, TJ, 1), sizeof(Smem), st>>>(b);
+  return cudaGetLastError();
+}
+} // namespace
+
+cudaError_t launch_stage_f64_batched(const Batch& b, int shape, cudaStream_t st)
+{
+  if (b.n_items <= 0) return cudaSuccess;
+  return shape == 0 ? launch_f64_batched<4, 32>(b, st) : launch_f64_batched<8, 16>(b, st);
 }
 
 } // namespace dn

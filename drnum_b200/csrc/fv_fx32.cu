@@ -1,6 +1,7 @@
 // FX32 (FP32 bulk, fixed-point storage) stage kernel instantiation.
 #include "fv_launch.h"
 #include "fv_fx32.cuh"
+#include "fv_batch.cuh"
 
 namespace dn {
 
@@ -23,6 +24,25 @@ cudaError_t launch_stage_fx32(const FxArgs& a, cudaStream_t st)
 }
 
 void fx32_tile(int* tj, int* tk) { *tj = FX_TJ; *tk = FX_TK; }
+
+namespace {
+template <int TJ, int TK>
+cudaError_t launch_fx_batched(const Batch& b, cudaStream_t st)
+{
+  using Smem = FxSmem<TJ, TK>;
+  auto kern = fx_stage_batched<TJ, TK>;
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(Smem));
+  if (e != cudaSuccess) return e;
+  kern<<<b.n_items, dim3(TK, TJ, 1), sizeof(Smem), st>>>(b);
+  return cudaGetLastError();
+}
+} // namespace
+
+cudaError_t launch_stage_fx32_batched(const Batch& b, int shape, cudaStream_t st)
+{
+  if (b.n_items <= 0) return cudaSuccess;
+  return shape == 0 ? launch_fx_batched<8, 32>(b, st) : launch_fx_batched<16, 16>(b, st);
+}
 
 int default_i_chunk(int ni, int nj, int nk, int tj, int tk, int num_sms, int ctas_per_sm)
 {

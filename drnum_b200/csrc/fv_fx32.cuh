@@ -196,9 +196,9 @@ struct FxSmem {
   int qz[5][TJ][TK + 1];              // z face integers, face below col kk
 };
 
+// One tile of one patch: columns (j0 .. j0+TJ-1, k0 .. k0+TK-1), planes i0 .. i1-1.
 template <int TJ, int TK>
-__global__ void __launch_bounds__(TJ * TK)
-fx_stage_kernel(const FxArgs a)
+__device__ __forceinline__ void fx_stage_tile(const FxArgs& a, int j0, int k0, int i0, int i1)
 {
   constexpr int NT = TJ * TK;
   constexpr int PJ = TJ + 4, PK = TK + 4;
@@ -212,9 +212,6 @@ fx_stage_kernel(const FxArgs a)
   const FxParams& P = a.p;
   const int tx = threadIdx.x, ty = threadIdx.y;
   const int tid = ty * TK + tx;
-  const int k0 = blockIdx.x * TK, j0 = blockIdx.y * TJ;
-  const int i0 = blockIdx.z * g.i_chunk;
-  const int i1 = min(g.ni, i0 + g.i_chunk);
   const int j = j0 + ty, k = k0 + tx;
   const bool own = (j < g.nj) && (k < g.nk);
   const int njk = g.nj * g.nk;
@@ -519,6 +516,15 @@ fx_stage_kernel(const FxArgs a)
     fetch(i + 4);
     __syncthreads();
   }
+}
+
+// One patch per launch: grid (k tiles, j tiles, i chunks).
+template <int TJ, int TK>
+__global__ void __launch_bounds__(TJ * TK)
+fx_stage_kernel(const FxArgs a)
+{
+  const int i0 = blockIdx.z * a.g.i_chunk;
+  fx_stage_tile<TJ, TK>(a, blockIdx.y * TJ, blockIdx.x * TK, i0, min(a.g.ni, i0 + a.g.i_chunk));
 }
 
 } // namespace dn

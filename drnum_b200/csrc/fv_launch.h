@@ -20,6 +20,18 @@ struct FxArgs;
 cudaError_t launch_stage_fx32(const FxArgs& a, cudaStream_t st);
 void fx32_tile(int* tj, int* tk);
 
+// Batched launches over a work list (fv_batch.cuh).  Tile shapes:
+//   FX32: 0 = 8 x 32, 1 = 16 x 16 (j x k);  FP64: 0 = 4 x 32, 1 = 8 x 16.
+struct Batch;
+constexpr int kNumShapes = 2;
+cudaError_t launch_stage_fx32_batched(const Batch& b, int shape, cudaStream_t st);
+cudaError_t launch_stage_f64_batched(const Batch& b, int shape, cudaStream_t st);
+inline void shape_tile(bool fp64, int shape, int* tj, int* tk)
+{
+  *tk = shape == 0 ? 32 : 16;
+  *tj = fp64 ? (shape == 0 ? 4 : 8) : (shape == 0 ? 8 : 16);
+}
+
 // Chooses the i-chunk so that the grid holds enough CTAs to fill the GPU.
 int default_i_chunk(int ni, int nj, int nk, int tj, int tk, int num_sms, int ctas_per_sm);
 

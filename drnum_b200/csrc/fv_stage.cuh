@@ -113,9 +113,9 @@ __device__ __forceinline__ void load_plane(StageSmem<Policy, TJ, TK>& sm, int sl
   }
 }
 
+// One tile of one patch: columns (j0 .. j0+TJ-1, k0 .. k0+TK-1), planes i0 .. i1-1.
 template <class Policy, int TJ, int TK>
-__global__ void __launch_bounds__(TJ * TK)
-fv_stage_kernel(const StageArgs<Policy> a)
+__device__ __forceinline__ void fv_stage_tile(const StageArgs<Policy>& a, int j0, int k0, int i0, int i1)
 {
   using Real = typename Policy::Real;
   using FaceT = typename Policy::FaceT;
@@ -125,9 +125,6 @@ fv_stage_kernel(const StageArgs<Policy> a)
 
   const StageGeom& g = a.g;
   const int tx = threadIdx.x, ty = threadIdx.y;
-  const int k0 = blockIdx.x * TK, j0 = blockIdx.y * TJ;
-  const int i0 = blockIdx.z * g.i_chunk;
-  const int i1 = min(g.ni, i0 + g.i_chunk);
   const int j = j0 + ty, k = k0 + tx;
   const bool own = (j < g.nj) && (k < g.nk);
   const size_t nc = (size_t)g.ni * g.nj * g.nk;
@@ -301,6 +298,15 @@ fv_stage_kernel(const StageArgs<Policy> a)
     #pragma unroll
     for (int v = 0; v < 5; ++v) fx_lo[v] = fx_hi[v];
   }
+}
+
+// One patch per launch: grid (k tiles, j tiles, i chunks).
+template <class Policy, int TJ, int TK>
+__global__ void __launch_bounds__(TJ * TK)
+fv_stage_kernel(const StageArgs<Policy> a)
+{
+  const int i0 = blockIdx.z * a.g.i_chunk;
+  fv_stage_tile<Policy, TJ, TK>(a, blockIdx.y * TJ, blockIdx.x * TK, i0, min(a.g.ni, i0 + a.g.i_chunk));
 }
 
 } // namespace dn

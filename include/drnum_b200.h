@@ -258,6 +258,31 @@ int dn_lslayers_get(const dn_lslayers* ls, int inner, int layer, uint64_t* cells
                     uint64_t* donors, double* weights);
 int dn_lslayers_destroy(dn_lslayers* ls);
 
+/* Context options.
+ *   DN_OPT_BATCHED (default 1): one launch per RK stage and tile shape over a
+ *     work list of (patch, column tile, plane range) items of all patches;
+ *     0 = one launch per patch.  Results are identical.
+ *   DN_OPT_GRAPH (default 0): dn_rk_step captures the whole step (stages,
+ *     donor copies, level-set wall) as a CUDA graph once per buffer rotation,
+ *     dt and alphas, and replays it.
+ * No reference counterpart (the reference launches 10 kernels per patch and
+ * stage, each followed by a device synchronisation, gpu_cartesianiterator.h:218-304). */
+#define DN_OPT_BATCHED    0
+#define DN_OPT_GRAPH      1
+int dn_set_option(dn_ctx* ctx, int option, int value);
+
+/* Tile shape of a patch in the batched launch: 0 = 8 x 32 (j x k; FP64 4 x 32),
+ * 1 = 16 x 16 (FP64 8 x 16).  The default wastes the fewest k lanes. */
+int dn_patch_set_tile(dn_ctx* ctx, int patch_id, int shape);
+
+/* Autotuner: measures each tile shape's cost per padded cell on the
+ * context's own patches (one stage into the scratch field 2, which it
+ * overwrites), then gives every patch the shape of least predicted time.
+ * cache_path (may be NULL) holds measured costs per device and precision and
+ * is reused on the next call; cost_out[2] (may be NULL) returns them in ns per
+ * padded cell and stage.  No reference counterpart. */
+int dn_autotune(dn_ctx* ctx, const char* cache_path, double cost_out[2]);
+
 /* Number of device kernel launches the context has issued so far. */
 int dn_launch_count(const dn_ctx* ctx, int64_t* count);
 
