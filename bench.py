@@ -304,6 +304,12 @@ def run_ours(args, rank, world, local_rank):
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(U0, h, dt)
 
+    # ---- the multi-patch workloads (overlap interpolation, boundary fluxes,
+    # level-set wall, many uneven patches)
+    extra = {}
+    for name in [w for w in args.workloads.split(",") if w]:
+        extra[name] = run_workload(name, args, dev, stream, rank, world, barrier, max_over_ranks)
+
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -329,9 +335,92 @@ def run_ours(args, rank, world, local_rank):
                     "path": "dn_patch_upload_f32 (pinned host) + dn_rk_step + dn_patch_download_f32 per step"},
             "gpu_launches": int(launches),
             "clocks": clock_info,
+            "workloads": extra,
         }
         print(json.dumps(line), flush=True)
     return 0
+
+
+def run_workload(name, args, dev, stream, rank, world, barrier, max_over_ranks):
+    """One multi-patch workload (drnum_b200.workloads): FP32 bulk batched
+    (autotuned tiles, CUDA-graph steps) and plain FP64 from the same state,
+    timed over args.steps steps after args.warmup; error of FP32 against FP64."""
+    import torch
+    from drnum_b200 import _lib, cases, workloads
+
+    case = workloads.build(name)
+    grid, objs = workloads.make_grid(case)
+    del case["states"]
+    cells = sum(int(np.prod(p["n"])) for p in case["patches"])
+    out = {"description": case["description"], "patches": len(case["patches"]), "cells": cells,
+           "no_donor_cells": grid.no_donor, "steps": args.steps, "warmup": args.warmup, "dt": case["dt"]}
+    its = {}
+    for prec in (_lib.DN_FP32, _lib.DN_FP64):
+        it = workloads.make_iterator(objs, prec, dev.index)
+        _lib.check(it.ctx, it.lib.dn_set_stream(it.ctx, ctypes_void(stream.cuda_stream)))
+        it.setOption(_lib.DN_OPT_GRAPH, 1)
+        its[prec] = it
+    if case["levelset"] is not None:
+        out["levelset_layer_cells"] = int(sum(len(layer["cells"]) for q in range(len(objs))
+                                              for layer in its[_lib.DN_FP32].levelSetLayers(q)["inner"]))
+    out["tile_costs_ns_per_padded_cell"] = [float(x) for x in its[_lib.DN_FP32].autotune()]
+    dt = case["dt"]
+    res = {}
+    for prec, key in ((_lib.DN_FP32, "fp32_batched"), (_lib.DN_FP64, "fp64_plain")):
+        it = its[prec]
+        for _ in range(args.warmup):
+            it.rkStep(dt, cases.RK3_ALPHA)
+        it.sync()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        barrier()
+        torch.cuda.synchronize(dev)
+        l0 = it.launchCount()
+        e0.record(stream)
+        for _ in range(args.steps):
+            it.rkStep(dt, cases.RK3_ALPHA)
+        e1.record(stream)
+        torch.cuda.synchronize(dev)
+        barrier()
+        t = max_over_ranks(e0.elapsed_time(e1) / 1e3)
+        it.sync()
+        mcell = world * cells * STAGES * args.steps / t / 1e6
+        bpc = 60.0 if prec == _lib.DN_FP32 else 120.0
+        res[key] = {"value": mcell, "unit": UNIT, "ms_per_step": t / args.steps * 1e3,
+                    "launches_per_step": (it.launchCount() - l0) / args.steps,
+                    "algorithmic_gbs": mcell * 1e6 * bpc / 1e9}
+        if case["levelset"] is not None:
+            # FP64 residual norm of the last step, Patch::computeVariableDifference
+            # of density between field 0 and the step-start field 1
+            mx, l2 = 0.0, 0.0
+            for q in range(len(objs)):
+                a, b = it.computeVariableDifference(q, 0, 0, 1, 0)
+                mx, l2 = max(mx, a), l2 + b * b
+            res[key]["residual_norms_rho"] = {"max": mx, "l2": float(np.sqrt(l2))}
+    peak, _ = measured_peaks()
+    res["fp32_batched"]["hbm_frac_of_measured"] = res["fp32_batched"]["algorithmic_gbs"] / peak
+    out.update(res)
+    out["fp32_over_fp64"] = res["fp32_batched"]["value"] / res["fp64_plain"]["value"]
+    # error of the FP32 run against the FP64 run after warmup + steps
+    num_r = den = 0.0
+    lin_r = lin_p = 0.0
+    num_p = 0.0
+    for q in range(len(objs)):
+        a = its[_lib.DN_FP32].downloadField(q, 0)
+        b = its[_lib.DN_FP64].downloadField(q, 0)
+        dr = (a[0] - b[0]) / cases.RHO_INF
+        dp = (cases.cons_to_prim(a)[0] - cases.cons_to_prim(b)[0]) / cases.P_INF
+        num_r += float((dr ** 2).sum())
+        num_p += float((dp ** 2).sum())
+        den += dr.size
+        lin_r = max(lin_r, float(np.abs(dr).max()))
+        lin_p = max(lin_p, float(np.abs(dp).max()))
+    out["error_vs_fp64"] = {"l2_rho_rel": float(np.sqrt(num_r / den)), "linf_rho_rel": lin_r,
+                            "l2_p_rel": float(np.sqrt(num_p / den)), "linf_p_rel": lin_p,
+                            "steps": args.warmup + args.steps}
+    for it in its.values():
+        it.close()
+    return out
 
 
 def ctypes_void(x):
@@ -347,6 +436,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--n", type=int, default=256)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--workloads", default="jet,sphere,tiled",
+                    help="comma-separated multi-patch workloads to add to the line ('' for none)")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "ours":
         args.warmup = 3

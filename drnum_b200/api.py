@@ -345,6 +345,14 @@ class B200CartesianIterator:
                 check(self.ctx, self.lib.dn_patch_download(self.ctx, pid, f, _lib.dptr(a)))
                 p.data[f][...] = a
 
+    def downloadField(self, i_patch, i_field=0):
+        """Field i_field of one patch as a new [5][ni][nj][nk] array (the
+        host patch is left unchanged)."""
+        p = self.m_Patches[i_patch]
+        a = np.empty((5, p.m_NumI, p.m_NumJ, p.m_NumK), dtype=np.float64)
+        check(self.ctx, self.lib.dn_patch_download(self.ctx, i_patch, i_field, _lib.dptr(a)))
+        return a
+
     def copyField(self, i_src, i_dst):
         check(self.ctx, self.lib.dn_copy_field(self.ctx, i_src, i_dst))
 

@@ -276,3 +276,90 @@ def uniform_state(patches, mach=0.5, p=P_INF, T=T_INF):
                                                      np.full(shape, mach * A_INF), np.zeros(shape),
                                                      np.zeros(shape))))
     return out
+
+
+# ------------------------------------------------------- benchmark workloads
+
+def jet_grid(nf=(288, 144, 144), overlap=3):
+    """Dual-resolution jet workload: the octant grid with a core of nf cells
+    at h = 1 / (2 nf[0]) (the box is [0, 1] x [0, nf1/nf0] x [0, nf2/nf0])
+    and seven octants at 2h, `overlap` cells across each interface."""
+    return octant_grid(nf=nf, h=1.0 / (2 * nf[0]), overlap=overlap, seek=2)
+
+
+def sphere_group(n=(256, 128, 128), L=1.0, overlap=3):
+    """Level-set wall workload: a patch group of n cells over [0, 2L] x [0, L]
+    x [0, L] split into two patches along x that overlap by `overlap` cells
+    on each side of the cut (seek layers 2)."""
+    h = 2.0 * L / n[0]
+    half = n[0] // 2
+    a = dict(n=(half + overlap, n[1], n[2]), origin=(0.0, 0.0, 0.0),
+             length=((half + overlap) * h, n[1] * h, n[2] * h), seek=(0, 2, 0, 0, 0, 0))
+    b = dict(n=(n[0] - half + overlap, n[1], n[2]), origin=((half - overlap) * h, 0.0, 0.0),
+             length=((n[0] - half + overlap) * h, n[1] * h, n[2] * h), seek=(2, 0, 0, 0, 0, 0))
+    return [a, b]
+
+
+def tiled_grid(slots=(8, 8, 8), extent=(8, 40), h=1.0 / 256, overlap=2, seed=42):
+    """Uneven batched workload: a box of slots[0] x slots[1] x slots[2]
+    patches.  The extent of each slot row along each axis is drawn uniformly
+    from `extent` coarse cells (seed); patches alternate between refinement 1
+    (spacing 2h) and refinement 2 (spacing h) in a checkerboard, so cell
+    counts per axis range over 8..80 plus the overlap.  Every patch reaches
+    `overlap` of its own cells across each interior interface, with 2 seek
+    layers there."""
+    rng = np.random.default_rng(seed)
+    ext = [rng.integers(extent[0], extent[1] + 1, slots[a]) for a in range(3)]
+    H = 2.0 * h
+    starts = [np.concatenate(([0], np.cumsum(ext[a])[:-1])) * H for a in range(3)]
+    patches = []
+    for a in range(slots[0]):
+        for b in range(slots[1]):
+            for c in range(slots[2]):
+                r = 2 if (a + b + c) % 2 else 1
+                hh = H / r
+                idx = (a, b, c)
+                n, origin, sk = [], [], []
+                for ax in range(3):
+                    lo_in = idx[ax] > 0
+                    hi_in = idx[ax] < slots[ax] - 1
+                    cells = int(ext[ax][idx[ax]]) * r
+                    n.append(cells + overlap * (int(lo_in) + int(hi_in)))
+                    origin.append(float(starts[ax][idx[ax]]) - (overlap * hh if lo_in else 0.0))
+                    sk += [2 if lo_in else 0, 2 if hi_in else 0]
+                patches.append(dict(n=tuple(n), origin=tuple(origin), length=tuple(n[q] * hh for q in range(3)),
+                                    seek=tuple(sk), refinement=r))
+    return patches
+
+
+def vortex_field(patch, mach, centre, beta, radius):
+    """Isentropic vortex (axis z) of strength beta on uniform flow at `mach`
+    along x, at the patch's cell centres."""
+    x, y, z = patch_centres(patch)
+    xr = (x - centre[0]) / radius
+    yr = (y - centre[1]) / radius
+    e = np.exp(0.5 * (1.0 - (xr * xr + yr * yr)))
+    k = beta / (2.0 * math.pi)
+    shape = tuple(patch["n"])
+    u = np.broadcast_to(mach * A_INF - k * yr * e * A_INF, shape)
+    v = np.broadcast_to(k * xr * e * A_INF, shape)
+    Tn = np.broadcast_to(1.0 - (GAS_GAMMA - 1.0) * beta * beta / (8.0 * GAS_GAMMA * math.pi ** 2) * e * e, shape)
+    rho = RHO_INF * Tn ** (1.0 / (GAS_GAMMA - 1.0))
+    p = rho * GAS_R * T_INF * Tn
+    return np.ascontiguousarray(prim_to_cons(p, T_INF * Tn, u, v, np.zeros(shape)))
+
+
+def tiled_state(patches, mach=0.4, seed=42):
+    """One seeded vortex per patch (random centre in the middle of the patch,
+    strength 3..6, radius a tenth of the patch's smallest extent) on a common
+    uniform flow; the vortices decay towards the patch faces, so overlapping
+    patches nearly agree."""
+    rng = np.random.default_rng(seed + 1)
+    out = []
+    for p in patches:
+        lo = np.array(p["origin"])
+        L = np.array(p["length"])
+        centre = lo + L * rng.uniform(0.4, 0.6, 3)
+        beta = float(rng.uniform(3.0, 6.0))
+        out.append(vortex_field(p, mach, centre, beta, 0.1 * float(L.min())))
+    return out
