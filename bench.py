@@ -348,7 +348,7 @@ def run_workload(name, args, dev, stream, rank, world, barrier, max_over_ranks):
     import torch
     from drnum_b200 import _lib, cases, workloads
 
-    case = workloads.build(name)
+    case = workloads.build(name, args.workload_scale)
     grid, objs = workloads.make_grid(case)
     del case["states"]
     cells = sum(int(np.prod(p["n"])) for p in case["patches"])
@@ -438,6 +438,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--workloads", default="jet,sphere,tiled",
                     help="comma-separated multi-patch workloads to add to the line ('' for none)")
+    ap.add_argument("--workload-scale", type=float, default=1.0,
+                    help="linear scale of the multi-patch workloads (1 = the full-size cases)")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "ours":
         args.warmup = 3
