@@ -95,6 +95,10 @@ struct dn_ctx {
   int64_t graph_generation = -1;
 };
 
+#ifndef DN_FX_WAVE_CTAS
+#define DN_FX_WAVE_CTAS 2   // CTAs per SM counted in a wave when sizing FX32 plane ranges
+#endif
+
 namespace {
 
 constexpr int kSumThreads = 256;
@@ -819,7 +823,7 @@ int stage_patch(dn_ctx* c, DnPatch& p, int in_b, int un_b, int out_b, double fac
     dn::fx32_tile(&tj, &tk);
     a.g.ni = g.ni; a.g.nj = g.nj; a.g.nk = g.nk;
     a.g.per_x = g.per_x; a.g.per_y = g.per_y; a.g.per_z = g.per_z;
-    a.g.i_chunk = dn::default_i_chunk(g.ni, g.nj, g.nk, tj, tk, c->num_sms, 2);
+    a.g.i_chunk = dn::default_i_chunk(g.ni, g.nj, g.nk, tj, tk, c->num_sms, DN_FX_WAVE_CTAS);
     a.p.Ax = (float)(dy * dz); a.p.Ay = (float)(dx * dz); a.p.Az = (float)(dx * dy);
     for (int v = 0; v < 5; ++v) {
       a.p.base[v] = (float)p.base[v];

@@ -53,7 +53,7 @@ __device__ __forceinline__ void load_patch_record(BatchPatch& dst, const BatchPa
 }
 
 template <int TJ, int TK>
-__global__ void __launch_bounds__(TJ * TK)
+__global__ void __launch_bounds__(TJ * TK, DN_FX_MIN_BLOCKS)
 fx_stage_batched(const Batch b)
 {
   __shared__ __align__(16) BatchPatch rec;

@@ -6,8 +6,14 @@
 namespace dn {
 
 namespace {
-constexpr int FX_TJ = 8;
-constexpr int FX_TK = 32;
+#ifndef DN_FX_TJ
+#define DN_FX_TJ 16
+#endif
+#ifndef DN_FX_TK
+#define DN_FX_TK 16
+#endif
+constexpr int FX_TJ = DN_FX_TJ;   // tile of the single-patch launch (j x k)
+constexpr int FX_TK = DN_FX_TK;
 }
 
 cudaError_t launch_stage_fx32(const FxArgs& a, cudaStream_t st)

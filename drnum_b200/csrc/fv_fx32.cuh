@@ -94,8 +94,9 @@ __device__ __forceinline__ Prim fx_prim(float r, float ru, float rv, float rw, f
   s.w = rw * ir;
   const float ke2 = fmaf(rw, s.w, fmaf(rv, s.v, ru * s.u));   // rho |u|^2
   s.p = R_over_cv * fmaf(-0.5f, ke2, rE);
-  s.a = sqrtf(gam * s.p * ir);
-  s.H = (rE + s.p) * ir;
+  const float p_ir = s.p * ir;
+  s.a = sqrtf(gam * p_ir);
+  s.H = fmaf(rE, ir, p_ir);                                    // (rho E + p) / rho
   return s;
 }
 
@@ -128,6 +129,9 @@ __device__ __forceinline__ void fx_split(float M, float& m4, float& p5)
 }
 
 // AUSM+ flux (ausmplus.h:39-106) between face sides L and R, normal DIR.
+// The reference's convective part h0 (phi_L + phi_R) - g0 (phi_R - phi_L)
+// with h0 = f0/2, g0 = |f0|/2 is the upwind form max(f0, 0) phi_L +
+// min(f0, 0) phi_R, evaluated here with one multiply-add per variable.
 template <int DIR>
 __device__ __forceinline__ void fx_ausm(const Prim& L, const Prim& R, float A, float F[5])
 {
@@ -144,14 +148,14 @@ __device__ __forceinline__ void fx_ausm(const Prim& L, const Prim& R, float A, f
   const float Mm = fminf(M, 0.0f);
   const float p = fmaf(p5l, L.p, p5r * R.p);
   const float f0 = a * A * fmaf(L.r, Mp, R.r * Mm);
-  const float h0 = 0.5f * f0;
-  const float g0 = 0.5f * fabsf(f0);
+  const float cp = fmaxf(f0, 0.0f);
+  const float cm = fminf(f0, 0.0f);
   const float Ap = A * p;
   F[0] = f0;
-  F[1] = fmaf(h0, L.u + R.u, fmaf(-g0, R.u - L.u, DIR == 0 ? Ap : 0.0f));
-  F[2] = fmaf(h0, L.v + R.v, fmaf(-g0, R.v - L.v, DIR == 1 ? Ap : 0.0f));
-  F[3] = fmaf(h0, L.w + R.w, fmaf(-g0, R.w - L.w, DIR == 2 ? Ap : 0.0f));
-  F[4] = fmaf(h0, L.H + R.H, -g0 * (R.H - L.H));
+  F[1] = DIR == 0 ? fmaf(cp, L.u, fmaf(cm, R.u, Ap)) : fmaf(cp, L.u, cm * R.u);
+  F[2] = DIR == 1 ? fmaf(cp, L.v, fmaf(cm, R.v, Ap)) : fmaf(cp, L.v, cm * R.v);
+  F[3] = DIR == 2 ? fmaf(cp, L.w, fmaf(cm, R.w, Ap)) : fmaf(cp, L.w, cm * R.w);
+  F[4] = fmaf(cp, L.H, cm * R.H);
 }
 
 // van Albada slope shared by both face-side states of a cell
@@ -202,8 +206,8 @@ __device__ __forceinline__ void fx_stage_tile(const FxArgs& a, int j0, int k0, i
 {
   constexpr int NT = TJ * TK;
   constexpr int PJ = TJ + 4, PK = TK + 4;
-  constexpr int NE = 5 * PJ * PK;                 // elements per plane tile
-  constexpr int EPT = (NE + NT - 1) / NT;         // elements per thread
+  constexpr int NP = PJ * PK;                     // positions of a plane tile (per variable)
+  constexpr int PPT = (NP + NT - 1) / NT;         // positions per thread
   using Smem = FxSmem<TJ, TK>;
   extern __shared__ __align__(16) unsigned char fx_smem_raw[];
   Smem& sm = *reinterpret_cast<Smem*>(fx_smem_raw);
@@ -217,41 +221,43 @@ __device__ __forceinline__ void fx_stage_tile(const FxArgs& a, int j0, int k0, i
   const int njk = g.nj * g.nk;
   const size_t nc = (size_t)g.ni * njk;
 
-  // per-thread plane elements: in-plane offset (v*nc + j*nk + k) or -1, and
-  // the destination index inside a plane slot
-  int32_t eoff[EPT];
+  // per-thread plane positions: in-plane offset j*nk + k of the (wrapped)
+  // column, or -1 outside a closed patch; the variables follow at stride nc
+  int32_t poff[PPT];
   #pragma unroll
-  for (int m = 0; m < EPT; ++m) {
+  for (int m = 0; m < PPT; ++m) {
     const int e = tid + m * NT;
-    eoff[m] = -1;
-    if (e < NE) {
-      const int v = e / (PJ * PK);
-      const int rem = e - v * (PJ * PK);
-      const int jj = rem / PK;
-      const int kk = rem - jj * PK;
+    poff[m] = -1;
+    if (e < NP) {
+      const int jj = e / PK;
+      const int kk = e - jj * PK;
       const int jw = fx_wrap(j0 - 2 + jj, g.nj, g.per_y);
       const int kw = fx_wrap(k0 - 2 + kk, g.nk, g.per_z);
-      if (jw >= 0 && kw >= 0) eoff[m] = (int32_t)(v * (int32_t)nc + jw * g.nk + kw);
+      if (jw >= 0 && kw >= 0) poff[m] = jw * g.nk + kw;
     }
   }
 
-  int32_t pre[EPT];
+  int32_t pre[5][PPT];
   auto fetch = [&](int ip) {
     const int iw = fx_wrap(ip, g.ni, g.per_x);
     #pragma unroll
-    for (int m = 0; m < EPT; ++m) {
-      pre[m] = 0;
-      if (iw >= 0 && eoff[m] >= 0) pre[m] = __ldg(a.in + (eoff[m] + iw * njk));
+    for (int v = 0; v < 5; ++v) {
+      const int32_t* src = a.in + (size_t)v * nc + (size_t)(iw < 0 ? 0 : iw) * njk;
+      #pragma unroll
+      for (int m = 0; m < PPT; ++m) {
+        pre[v][m] = 0;
+        if (iw >= 0 && poff[m] >= 0) pre[v][m] = __ldg(src + poff[m]);
+      }
     }
   };
   auto commit = [&](int ip) {
     float* dst = &sm.plane[ip & 3][0][0][0];
     #pragma unroll
-    for (int m = 0; m < EPT; ++m) {
-      const int e = tid + m * NT;
-      if (e < NE) {
-        const int v = e / (PJ * PK);
-        dst[e] = fmaf(P.quantum[v], (float)pre[m], P.base[v]);
+    for (int v = 0; v < 5; ++v) {
+      #pragma unroll
+      for (int m = 0; m < PPT; ++m) {
+        const int e = tid + m * NT;
+        if (e < NP) dst[v * NP + e] = fmaf(P.quantum[v], (float)pre[v][m], P.base[v]);
       }
     }
   };
@@ -315,7 +321,7 @@ __device__ __forceinline__ void fx_stage_tile(const FxArgs& a, int j0, int k0, i
   }
 
   for (int i = i0; i < i1; ++i) {
-    const int s0 = i & 3, sp1 = (i + 1) & 3, sp2 = (i + 2) & 3;
+    const int s0 = i & 3, sp2 = (i + 2) & 3;
 
     // ---------------- x: face above cell i (between i and i+1)
     int qx_hi[5];
@@ -518,9 +524,16 @@ __device__ __forceinline__ void fx_stage_tile(const FxArgs& a, int j0, int k0, i
   }
 }
 
+// Resident CTAs per SM the register allocation is sized for: three
+// 256-thread CTAs (80 registers, 55-58 KB shared memory each) measured 26 %
+// faster than two on the 256^3 patch.
+#ifndef DN_FX_MIN_BLOCKS
+#define DN_FX_MIN_BLOCKS 3
+#endif
+
 // One patch per launch: grid (k tiles, j tiles, i chunks).
 template <int TJ, int TK>
-__global__ void __launch_bounds__(TJ * TK)
+__global__ void __launch_bounds__(TJ * TK, DN_FX_MIN_BLOCKS)
 fx_stage_kernel(const FxArgs a)
 {
   const int i0 = blockIdx.z * a.g.i_chunk;
