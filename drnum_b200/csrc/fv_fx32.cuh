@@ -200,9 +200,21 @@ struct FxSmem {
   int qz[5][TJ][TK + 1];              // z face integers, face below col kk
 };
 
-// One tile of one patch: columns (j0 .. j0+TJ-1, k0 .. k0+TK-1), planes i0 .. i1-1.
+// Is the tile "full": every own column inside the patch and, on closed j/k
+// axes, two more rows/columns of cells on both sides, so that every y/z
+// slope and face of the tile exists?  Such tiles (almost all of a large
+// patch) run a form of the tile function without the per-thread edge tests.
 template <int TJ, int TK>
-__device__ __forceinline__ void fx_stage_tile(const FxArgs& a, int j0, int k0, int i0, int i1)
+__device__ __forceinline__ bool fx_tile_full(const FxGeom& g, int j0, int k0)
+{
+  const bool fy = (j0 + TJ <= g.nj) && (g.per_y || (j0 >= 2 && j0 + TJ + 2 <= g.nj));
+  const bool fz = (k0 + TK <= g.nk) && (g.per_z || (k0 >= 2 && k0 + TK + 2 <= g.nk));
+  return fy && fz;
+}
+
+// One tile of one patch: columns (j0 .. j0+TJ-1, k0 .. k0+TK-1), planes i0 .. i1-1.
+template <int TJ, int TK, bool FULL>
+__device__ __forceinline__ void fx_stage_tile_impl(const FxArgs& a, int j0, int k0, int i0, int i1)
 {
   constexpr int NT = TJ * TK;
   constexpr int PJ = TJ + 4, PK = TK + 4;
@@ -217,7 +229,7 @@ __device__ __forceinline__ void fx_stage_tile(const FxArgs& a, int j0, int k0, i
   const int tx = threadIdx.x, ty = threadIdx.y;
   const int tid = ty * TK + tx;
   const int j = j0 + ty, k = k0 + tx;
-  const bool own = (j < g.nj) && (k < g.nk);
+  const bool own = FULL || ((j < g.nj) && (k < g.nk));
   const int njk = g.nj * g.nk;
   const size_t nc = (size_t)g.ni * njk;
 
@@ -356,8 +368,8 @@ __device__ __forceinline__ void fx_stage_tile(const FxArgs& a, int j0, int k0, i
     // ---------------- y and z face states of plane i
     float ym[5], zm[5];   // right states of the faces below the own cell
     {
-      const bool sy = fx_cell_ok(j - 1, g.nj, g.per_y) && fx_cell_ok(j + 1, g.nj, g.per_y);
-      const bool sz = fx_cell_ok(k - 1, g.nk, g.per_z) && fx_cell_ok(k + 1, g.nk, g.per_z);
+      const bool sy = FULL || (fx_cell_ok(j - 1, g.nj, g.per_y) && fx_cell_ok(j + 1, g.nj, g.per_y));
+      const bool sz = FULL || (fx_cell_ok(k - 1, g.nk, g.per_z) && fx_cell_ok(k + 1, g.nk, g.per_z));
       #pragma unroll
       for (int v = 0; v < 5; ++v) {
         const float uc = xu0[v];
@@ -387,7 +399,7 @@ __device__ __forceinline__ void fx_stage_tile(const FxArgs& a, int j0, int k0, i
           const float uc = sm.plane[s0][v][jj + 2][kk + 2];
           const float ul = sm.plane[s0][v][jj + 1][kk + 2];
           const float uh = sm.plane[s0][v][jj + 3][kk + 2];
-          const float s = (sy && kc < g.nk) ? fx_slope(uc - ul, uh - uc) : 0.0f;
+          const float s = (FULL || (sy && kc < g.nk)) ? fx_slope(uc - ul, uh - uc) : 0.0f;
           if (top) sm.sy_top[v][kk] = uc - s;
           else sm.sy[v][0][kk] = uc + s;
         }
@@ -404,7 +416,7 @@ __device__ __forceinline__ void fx_stage_tile(const FxArgs& a, int j0, int k0, i
           const float uc = sm.plane[s0][v][jj + 2][kk + 2];
           const float ul = sm.plane[s0][v][jj + 2][kk + 1];
           const float uh = sm.plane[s0][v][jj + 2][kk + 3];
-          const float s = (sz && jc < g.nj) ? fx_slope(uc - ul, uh - uc) : 0.0f;
+          const float s = (FULL || (sz && jc < g.nj)) ? fx_slope(uc - ul, uh - uc) : 0.0f;
           if (top) sm.sz_top[v][jj] = uc - s;
           else sm.sz[v][jj][0] = uc + s;
         }
@@ -416,8 +428,8 @@ __device__ __forceinline__ void fx_stage_tile(const FxArgs& a, int j0, int k0, i
     {
       // the face below row j is needed even when row j itself lies beyond a
       // periodic patch (it is the wrapped face above the last row)
-      const bool exy = k < g.nk && fx_face_exists(j, g.nj, g.per_y) && (g.per_y || j < g.nj);
-      const bool exz = j < g.nj && fx_face_exists(k, g.nk, g.per_z) && (g.per_z || k < g.nk);
+      const bool exy = FULL || (k < g.nk && fx_face_exists(j, g.nj, g.per_y) && (g.per_y || j < g.nj));
+      const bool exz = FULL || (j < g.nj && fx_face_exists(k, g.nk, g.per_z) && (g.per_z || k < g.nk));
       float F[5];
       if (exy) {
         fx_ausm<1>(fx_prim(sm.sy[0][ty][tx], sm.sy[1][ty][tx], sm.sy[2][ty][tx], sm.sy[3][ty][tx], sm.sy[4][ty][tx]),
@@ -443,7 +455,7 @@ __device__ __forceinline__ void fx_stage_tile(const FxArgs& a, int j0, int k0, i
       if (h < TK) {
         const int kk = h;
         const int jf = j0 + TJ, kf = k0 + kk;   // face below halo row TJ
-        const bool ex = kf < g.nk && fx_face_exists(jf, g.nj, g.per_y) && (g.per_y || jf < g.nj);
+        const bool ex = FULL || (kf < g.nk && fx_face_exists(jf, g.nj, g.per_y) && (g.per_y || jf < g.nj));
         if (ex) {
           fx_ausm<1>(fx_prim(sm.sy[0][TJ][kk], sm.sy[1][TJ][kk], sm.sy[2][TJ][kk], sm.sy[3][TJ][kk], sm.sy[4][TJ][kk]),
                      fx_prim(sm.sy_top[0][kk], sm.sy_top[1][kk], sm.sy_top[2][kk], sm.sy_top[3][kk], sm.sy_top[4][kk]),
@@ -457,7 +469,7 @@ __device__ __forceinline__ void fx_stage_tile(const FxArgs& a, int j0, int k0, i
       } else {
         const int jj = h - TK;
         const int jf = j0 + jj, kf = k0 + TK;   // face below halo col TK
-        const bool ex = jf < g.nj && fx_face_exists(kf, g.nk, g.per_z) && (g.per_z || kf < g.nk);
+        const bool ex = FULL || (jf < g.nj && fx_face_exists(kf, g.nk, g.per_z) && (g.per_z || kf < g.nk));
         if (ex) {
           fx_ausm<2>(fx_prim(sm.sz[0][jj][TK], sm.sz[1][jj][TK], sm.sz[2][jj][TK], sm.sz[3][jj][TK], sm.sz[4][jj][TK]),
                      fx_prim(sm.sz_top[0][jj], sm.sz_top[1][jj], sm.sz_top[2][jj], sm.sz_top[3][jj], sm.sz_top[4][jj]),
@@ -522,6 +534,13 @@ __device__ __forceinline__ void fx_stage_tile(const FxArgs& a, int j0, int k0, i
     fetch(i + 4);
     __syncthreads();
   }
+}
+
+template <int TJ, int TK>
+__device__ __forceinline__ void fx_stage_tile(const FxArgs& a, int j0, int k0, int i0, int i1)
+{
+  if (fx_tile_full<TJ, TK>(a.g, j0, k0)) fx_stage_tile_impl<TJ, TK, true>(a, j0, k0, i0, i1);
+  else fx_stage_tile_impl<TJ, TK, false>(a, j0, k0, i0, i1);
 }
 
 // Resident CTAs per SM the register allocation is sized for: three
