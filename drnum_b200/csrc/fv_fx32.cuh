@@ -187,18 +187,44 @@ __device__ __forceinline__ bool fx_cell_ok(int x, int n, int per)
   return per ? true : (x >= 0 && x < n);
 }
 
+// Shared memory of a CTA.  Every array starts on a 128-byte boundary and is
+// laid out so that a warp's accesses hit distinct banks: the plane ring
+// stores rows in interleaved pairs ([row/2][col][row%2]), since a warp of a
+// 16-wide tile spans two rows; the z arrays keep own columns at stride TK
+// and park the one extra (halo) column of each row in the bank the own
+// columns leave free.
 template <int TJ, int TK>
 struct FxSmem {
   static constexpr int PJ = TJ + 4;
   static constexpr int PK = TK + 4;
-  float plane[4][5][PJ][PK];          // dequantised state, ring over planes i-1 .. i+2
-  float sy[5][TJ + 1][TK];            // y: left state of the face above row jj-1 (row -1 .. TJ-1)
-  float sy_top[5][TK];                // y: right state of the face below row TJ (halo)
-  float sz[5][TJ][TK + 1];            // z: left state of the face above col kk-1 (col -1 .. TK-1)
-  float sz_top[5][TJ];                // z: right state of the face below col TK (halo)
-  int qy[5][TJ + 1][TK];              // y face integers, face below row jj
-  int qz[5][TJ][TK + 1];              // z face integers, face below col kk
+  static constexpr int NW = TJ * TK / 32;        // warps of a CTA
+  alignas(128) float plane[4][5][PJ / 2][PK][2]; // dequantised state, ring over planes i-1 .. i+2
+  alignas(128) float sy[5][TJ + 1][TK];          // y: left state of the face above row jj-1 (row -1 .. TJ-1)
+  alignas(128) float sy_top[5][TK];              // y: right state of the face below row TJ (halo)
+  alignas(128) float szL[5][TJ][TK];             // z: left state of the face above col kk (own columns)
+  alignas(128) float szH[5][NW][32];             // z: left state of the face above col -1 (halo), see zh_slot
+  alignas(128) float sz_top[5][TJ];              // z: right state of the face below col TK (halo)
+  alignas(128) int qy[5][TJ + 1][TK];            // y face integers, face below row jj
+  alignas(128) int qzL[5][TJ][TK];               // z face integers, face below col kk (own columns)
+  alignas(128) int qzT[5][NW][32];               // z face integers, face below col TK (halo), see zt_slot
+  alignas(128) int un[5][TJ][TK];                // f(n) of the own cells of the current plane (cp.async)
 };
+
+// bank-free slots of the per-row halo values of the z arrays
+template <int TK> __device__ __forceinline__ int zh_slot(int row) { return (row * TK + TK - 1) & 31; }
+template <int TK> __device__ __forceinline__ int zt_slot(int row) { return (row * TK) & 31; }
+template <int TK> __device__ __forceinline__ int z_warp(int row) { return (row * TK) >> 5; }
+
+__device__ __forceinline__ void fx_cp_async4(void* smem, const void* gmem)
+{
+  const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" :: "r"(s), "l"(gmem) : "memory");
+}
+
+__device__ __forceinline__ void fx_cp_async_wait_all()
+{
+  asm volatile("cp.async.wait_all;" ::: "memory");
+}
 
 // Is the tile "full": every own column inside the patch and, on closed j/k
 // axes, two more rows/columns of cells on both sides, so that every y/z
@@ -235,14 +261,17 @@ __device__ __forceinline__ void fx_stage_tile_impl(const FxArgs& a, int j0, int 
 
   // per-thread plane positions: in-plane offset j*nk + k of the (wrapped)
   // column, or -1 outside a closed patch; the variables follow at stride nc
+  // plane element (jj, kk) of variable v in ring slot sl (rows interleaved in pairs)
+  auto PL = [&](int sl, int v, int jj, int kk) -> float& { return sm.plane[sl][v][jj >> 1][kk][jj & 1]; };
+
   int32_t poff[PPT];
   #pragma unroll
   for (int m = 0; m < PPT; ++m) {
-    const int e = tid + m * NT;
+    const int e = tid + m * NT;                    // storage order: [row/2][col][row%2]
     poff[m] = -1;
     if (e < NP) {
-      const int jj = e / PK;
-      const int kk = e - jj * PK;
+      const int jj = (e / (2 * PK)) * 2 + (e & 1);
+      const int kk = (e % (2 * PK)) >> 1;
       const int jw = fx_wrap(j0 - 2 + jj, g.nj, g.per_y);
       const int kw = fx_wrap(k0 - 2 + kk, g.nk, g.per_z);
       if (jw >= 0 && kw >= 0) poff[m] = jw * g.nk + kw;
@@ -263,7 +292,7 @@ __device__ __forceinline__ void fx_stage_tile_impl(const FxArgs& a, int j0, int 
     }
   };
   auto commit = [&](int ip) {
-    float* dst = &sm.plane[ip & 3][0][0][0];
+    float* dst = &sm.plane[ip & 3][0][0][0][0];
     #pragma unroll
     for (int v = 0; v < 5; ++v) {
       #pragma unroll
@@ -273,6 +302,17 @@ __device__ __forceinline__ void fx_stage_tile_impl(const FxArgs& a, int j0, int 
       }
     }
   };
+
+  // f(n) of the own cell, plane ip, copied asynchronously into shared memory
+  // one plane ahead of its use in the update
+  auto fetch_un = [&](int ip) {
+    if (own && ip < i1) {
+      const int c = ip * njk + j * g.nk + k;
+      #pragma unroll
+      for (int v = 0; v < 5; ++v) fx_cp_async4(&sm.un[v][ty][tx], a.un + (size_t)v * nc + c);
+    }
+  };
+  fetch_un(i0);
 
   // prologue: planes i0-1 .. i0+2 in the ring
   for (int q = -1; q <= 2; ++q) {
@@ -296,9 +336,9 @@ __device__ __forceinline__ void fx_stage_tile_impl(const FxArgs& a, int j0, int 
     float U0[5];
     #pragma unroll
     for (int v = 0; v < 5; ++v) {
-      const float um = sm.plane[s_m1][v][ty + 2][tx + 2];
-      const float uc = sm.plane[s_0][v][ty + 2][tx + 2];
-      const float up = sm.plane[s_p1][v][ty + 2][tx + 2];
+      const float um = PL(s_m1, v, ty + 2, tx + 2);
+      const float uc = PL(s_0, v, ty + 2, tx + 2);
+      const float up = PL(s_p1, v, ty + 2, tx + 2);
       const float s = sx ? fx_slope(uc - um, up - uc) : 0.0f;
       U0[v] = uc;
       xu0[v] = uc;
@@ -345,7 +385,7 @@ __device__ __forceinline__ void fx_stage_tile_impl(const FxArgs& a, int j0, int 
       #pragma unroll
       for (int v = 0; v < 5; ++v) {
         const float uc = xu1[v];
-        const float up = sm.plane[sp2][v][ty + 2][tx + 2];
+        const float up = PL(sp2, v, ty + 2, tx + 2);
         xu2[v] = up;
         const float b = up - uc;
         const float s = sx ? fx_slope(xb[v], b) : 0.0f;
@@ -373,14 +413,14 @@ __device__ __forceinline__ void fx_stage_tile_impl(const FxArgs& a, int j0, int 
       #pragma unroll
       for (int v = 0; v < 5; ++v) {
         const float uc = xu0[v];
-        const float uyl = sm.plane[s0][v][ty + 1][tx + 2];
-        const float uyh = sm.plane[s0][v][ty + 3][tx + 2];
-        const float uzl = sm.plane[s0][v][ty + 2][tx + 1];
-        const float uzh = sm.plane[s0][v][ty + 2][tx + 3];
+        const float uyl = PL(s0, v, ty + 1, tx + 2);
+        const float uyh = PL(s0, v, ty + 3, tx + 2);
+        const float uzl = PL(s0, v, ty + 2, tx + 1);
+        const float uzh = PL(s0, v, ty + 2, tx + 3);
         const float s_y = sy ? fx_slope(uc - uyl, uyh - uc) : 0.0f;
         const float s_z = sz ? fx_slope(uc - uzl, uzh - uc) : 0.0f;
         sm.sy[v][ty + 1][tx] = uc + s_y;
-        sm.sz[v][ty][tx + 1] = uc + s_z;
+        sm.szL[v][ty][tx] = uc + s_z;
         ym[v] = uc - s_y;
         zm[v] = uc - s_z;
       }
@@ -396,9 +436,9 @@ __device__ __forceinline__ void fx_stage_tile_impl(const FxArgs& a, int j0, int 
                         fx_cell_ok(jc, g.nj, g.per_y);
         #pragma unroll
         for (int v = 0; v < 5; ++v) {
-          const float uc = sm.plane[s0][v][jj + 2][kk + 2];
-          const float ul = sm.plane[s0][v][jj + 1][kk + 2];
-          const float uh = sm.plane[s0][v][jj + 3][kk + 2];
+          const float uc = PL(s0, v, jj + 2, kk + 2);
+          const float ul = PL(s0, v, jj + 1, kk + 2);
+          const float uh = PL(s0, v, jj + 3, kk + 2);
           const float s = (FULL || (sy && kc < g.nk)) ? fx_slope(uc - ul, uh - uc) : 0.0f;
           if (top) sm.sy_top[v][kk] = uc - s;
           else sm.sy[v][0][kk] = uc + s;
@@ -413,12 +453,12 @@ __device__ __forceinline__ void fx_stage_tile_impl(const FxArgs& a, int j0, int 
                         fx_cell_ok(kc, g.nk, g.per_z);
         #pragma unroll
         for (int v = 0; v < 5; ++v) {
-          const float uc = sm.plane[s0][v][jj + 2][kk + 2];
-          const float ul = sm.plane[s0][v][jj + 2][kk + 1];
-          const float uh = sm.plane[s0][v][jj + 2][kk + 3];
+          const float uc = PL(s0, v, jj + 2, kk + 2);
+          const float ul = PL(s0, v, jj + 2, kk + 1);
+          const float uh = PL(s0, v, jj + 2, kk + 3);
           const float s = (FULL || (sz && jc < g.nj)) ? fx_slope(uc - ul, uh - uc) : 0.0f;
           if (top) sm.sz_top[v][jj] = uc - s;
-          else sm.sz[v][jj][0] = uc + s;
+          else sm.szH[v][z_warp<TK>(jj)][zh_slot<TK>(jj)] = uc + s;
         }
       }
     }
@@ -441,13 +481,15 @@ __device__ __forceinline__ void fx_stage_tile_impl(const FxArgs& a, int j0, int 
         for (int v = 0; v < 5; ++v) sm.qy[v][ty][tx] = 0;
       }
       if (exz) {
-        fx_ausm<2>(fx_prim(sm.sz[0][ty][tx], sm.sz[1][ty][tx], sm.sz[2][ty][tx], sm.sz[3][ty][tx], sm.sz[4][ty][tx]),
-                   fx_prim(zm[0], zm[1], zm[2], zm[3], zm[4]), P.Az, F);
+        float zl[5];
         #pragma unroll
-        for (int v = 0; v < 5; ++v) sm.qz[v][ty][tx] = __float2int_rn(F[v] * P.face_scale[v]);
+        for (int v = 0; v < 5; ++v) zl[v] = tx > 0 ? sm.szL[v][ty][tx - 1] : sm.szH[v][z_warp<TK>(ty)][zh_slot<TK>(ty)];
+        fx_ausm<2>(fx_prim(zl[0], zl[1], zl[2], zl[3], zl[4]), fx_prim(zm[0], zm[1], zm[2], zm[3], zm[4]), P.Az, F);
+        #pragma unroll
+        for (int v = 0; v < 5; ++v) sm.qzL[v][ty][tx] = __float2int_rn(F[v] * P.face_scale[v]);
       } else {
         #pragma unroll
-        for (int v = 0; v < 5; ++v) sm.qz[v][ty][tx] = 0;
+        for (int v = 0; v < 5; ++v) sm.qzL[v][ty][tx] = 0;
       }
     }
     for (int h = tid; h < TK + TJ; h += NT) {
@@ -471,14 +513,15 @@ __device__ __forceinline__ void fx_stage_tile_impl(const FxArgs& a, int j0, int 
         const int jf = j0 + jj, kf = k0 + TK;   // face below halo col TK
         const bool ex = FULL || (jf < g.nj && fx_face_exists(kf, g.nk, g.per_z) && (g.per_z || kf < g.nk));
         if (ex) {
-          fx_ausm<2>(fx_prim(sm.sz[0][jj][TK], sm.sz[1][jj][TK], sm.sz[2][jj][TK], sm.sz[3][jj][TK], sm.sz[4][jj][TK]),
+          fx_ausm<2>(fx_prim(sm.szL[0][jj][TK - 1], sm.szL[1][jj][TK - 1], sm.szL[2][jj][TK - 1], sm.szL[3][jj][TK - 1],
+                             sm.szL[4][jj][TK - 1]),
                      fx_prim(sm.sz_top[0][jj], sm.sz_top[1][jj], sm.sz_top[2][jj], sm.sz_top[3][jj], sm.sz_top[4][jj]),
                      P.Az, F);
           #pragma unroll
-          for (int v = 0; v < 5; ++v) sm.qz[v][jj][TK] = __float2int_rn(F[v] * P.face_scale[v]);
+          for (int v = 0; v < 5; ++v) sm.qzT[v][z_warp<TK>(jj)][zt_slot<TK>(jj)] = __float2int_rn(F[v] * P.face_scale[v]);
         } else {
           #pragma unroll
-          for (int v = 0; v < 5; ++v) sm.qz[v][jj][TK] = 0;
+          for (int v = 0; v < 5; ++v) sm.qzT[v][z_warp<TK>(jj)][zt_slot<TK>(jj)] = 0;
         }
       }
     }
@@ -493,24 +536,27 @@ __device__ __forceinline__ void fx_stage_tile_impl(const FxArgs& a, int j0, int 
       int res[5];
       #pragma unroll
       for (int v = 0; v < 5; ++v)
-        res[v] = qx_lo[v] + sm.qy[v][ty][tx] + sm.qz[v][ty][tx]
-               - sm.qz[v][ty][tx + 1] - sm.qy[v][ty + 1][tx] - qx_hi[v];
+        res[v] = qx_lo[v] + sm.qy[v][ty][tx] + sm.qzL[v][ty][tx]
+               - (tx < TK - 1 ? sm.qzL[v][ty][tx + 1] : sm.qzT[v][z_warp<TK>(ty)][zt_slot<TK>(ty)])
+               - sm.qy[v][ty + 1][tx] - qx_hi[v];
       if (a.wall.any && (i == 0 || i == g.ni - 1 || j == 0 || j == g.nj - 1 || k == 0 || k == g.nk - 1))
         add_wall_fluxes(a.wall, g.ni, g.nj, g.nk, g.per_x, g.per_y, g.per_z, i, j, k, xu0, P.Ax, P.Ay, P.Az, res,
                         [&](int v, float F) { return __float2int_rn(F * P.face_scale[v]); });
+      fx_cp_async_wait_all();
       #pragma unroll
       for (int v = 0; v < 5; ++v) {
         int32_t o;
         if (act) {
           const int r = res[v];
+          const int un = sm.un[v][ty][tx];
           // |un| < 2^30 and |r| < 2^30 (face integers are bounded by the
           // exact range of the update), so the int32 sum cannot overflow
-          const int on = a.un[v * ncv + c] + r;
+          const int on = un + r;
           if (on >= kFxLimit || on <= -kFxLimit) {
             bad |= 1;
             if (a.err_info && atomicCAS(&a.err_info[0], ~0ull, (unsigned long long)c) == ~0ull) {
               a.err_info[1] = (unsigned long long)v;
-              a.err_info[2] = (unsigned long long)__double_as_longlong((double)a.un[v * ncv + c]);
+              a.err_info[2] = (unsigned long long)__double_as_longlong((double)un);
               a.err_info[3] = (unsigned long long)__double_as_longlong((double)r);
             }
           }
@@ -532,6 +578,7 @@ __device__ __forceinline__ void fx_stage_tile_impl(const FxArgs& a, int j0, int 
     // ---------------- ring: plane i+3 (prefetched) replaces plane i-1
     commit(i + 3 + 4);
     fetch(i + 4);
+    fetch_un(i + 1);
     __syncthreads();
   }
 }
