@@ -375,36 +375,6 @@ __device__ __forceinline__ void fx_stage_tile_impl(const FxArgs& a, int j0, int 
   for (int i = i0; i < i1; ++i) {
     const int s0 = i & 3, sp2 = (i + 2) & 3;
 
-    // ---------------- x: face above cell i (between i and i+1)
-    int qx_hi[5];
-    float xu2[5];
-    {
-      const bool ex = own && fx_face_exists(i + 1, g.ni, g.per_x);
-      const bool sx = fx_cell_ok(i + 2, g.ni, g.per_x);   // slope of cell i+1 needs i+2 (i is in range)
-      float Sm[5], Sp[5];
-      #pragma unroll
-      for (int v = 0; v < 5; ++v) {
-        const float uc = xu1[v];
-        const float up = PL(sp2, v, ty + 2, tx + 2);
-        xu2[v] = up;
-        const float b = up - uc;
-        const float s = sx ? fx_slope(xb[v], b) : 0.0f;
-        Sm[v] = uc - s;
-        Sp[v] = uc + s;
-        xb[v] = b;
-      }
-      if (ex) {
-        float F[5];
-        fx_ausm<0>(xleft, fx_prim(Sm[0], Sm[1], Sm[2], Sm[3], Sm[4]), P.Ax, F);
-        #pragma unroll
-        for (int v = 0; v < 5; ++v) qx_hi[v] = __float2int_rn(F[v] * P.face_scale[v]);
-      } else {
-        #pragma unroll
-        for (int v = 0; v < 5; ++v) qx_hi[v] = 0;
-      }
-      xleft = fx_prim(Sp[0], Sp[1], Sp[2], Sp[3], Sp[4]);
-    }
-
     // ---------------- y and z face states of plane i
     float ym[5], zm[5];   // right states of the faces below the own cell
     {
@@ -463,6 +433,37 @@ __device__ __forceinline__ void fx_stage_tile_impl(const FxArgs& a, int j0, int 
       }
     }
     __syncthreads();
+
+    // ---------------- x: face above cell i (between i and i+1); plane i+2
+    // was committed before this iteration's first barrier
+    int qx_hi[5];
+    float xu2[5];
+    {
+      const bool ex = own && fx_face_exists(i + 1, g.ni, g.per_x);
+      const bool sx = fx_cell_ok(i + 2, g.ni, g.per_x);   // slope of cell i+1 needs i+2 (i is in range)
+      float Sm[5], Sp[5];
+      #pragma unroll
+      for (int v = 0; v < 5; ++v) {
+        const float uc = xu1[v];
+        const float up = PL(sp2, v, ty + 2, tx + 2);
+        xu2[v] = up;
+        const float b = up - uc;
+        const float s = sx ? fx_slope(xb[v], b) : 0.0f;
+        Sm[v] = uc - s;
+        Sp[v] = uc + s;
+        xb[v] = b;
+      }
+      if (ex) {
+        float F[5];
+        fx_ausm<0>(xleft, fx_prim(Sm[0], Sm[1], Sm[2], Sm[3], Sm[4]), P.Ax, F);
+        #pragma unroll
+        for (int v = 0; v < 5; ++v) qx_hi[v] = __float2int_rn(F[v] * P.face_scale[v]);
+      } else {
+        #pragma unroll
+        for (int v = 0; v < 5; ++v) qx_hi[v] = 0;
+      }
+      xleft = fx_prim(Sp[0], Sp[1], Sp[2], Sp[3], Sp[4]);
+    }
 
     // ---------------- y and z faces below the own cell (+ the top halo faces)
     {
@@ -575,11 +576,13 @@ __device__ __forceinline__ void fx_stage_tile_impl(const FxArgs& a, int j0, int 
       xu1[v] = xu2[v];
     }
 
-    // ---------------- ring: plane i+3 (prefetched) replaces plane i-1
+    // ---------------- ring: plane i+3 (prefetched) replaces plane i-1, which
+    // no phase of this or the next iteration reads; the next iteration's
+    // first barrier orders this commit before its reads of plane i+3, and
+    // the shared face arrays are written again only after that barrier
     commit(i + 3 + 4);
     fetch(i + 4);
     fetch_un(i + 1);
-    __syncthreads();
   }
 }
 
