@@ -402,22 +402,23 @@ def run_workload(name, args, dev, stream, rank, world, barrier, max_over_ranks):
     out.update(res)
     out["fp32_over_fp64"] = res["fp32_batched"]["value"] / res["fp64_plain"]["value"]
     # error of the FP32 run against the FP64 run after warmup + steps
-    num_r = den = 0.0
-    lin_r = lin_p = 0.0
-    num_p = 0.0
+    num_r = num_p = den = 0.0
+    lin_r, lin_p = [], []
+    nonfinite = 0
     for q in range(len(objs)):
         a = its[_lib.DN_FP32].downloadField(q, 0)
         b = its[_lib.DN_FP64].downloadField(q, 0)
+        nonfinite += int((~np.isfinite(a)).sum() + (~np.isfinite(b)).sum())
         dr = (a[0] - b[0]) / cases.RHO_INF
         dp = (cases.cons_to_prim(a)[0] - cases.cons_to_prim(b)[0]) / cases.P_INF
         num_r += float((dr ** 2).sum())
         num_p += float((dp ** 2).sum())
         den += dr.size
-        lin_r = max(lin_r, float(np.abs(dr).max()))
-        lin_p = max(lin_p, float(np.abs(dp).max()))
-    out["error_vs_fp64"] = {"l2_rho_rel": float(np.sqrt(num_r / den)), "linf_rho_rel": lin_r,
-                            "l2_p_rel": float(np.sqrt(num_p / den)), "linf_p_rel": lin_p,
-                            "steps": args.warmup + args.steps}
+        lin_r.append(float(np.abs(dr).max()))
+        lin_p.append(float(np.abs(dp).max()))
+    out["error_vs_fp64"] = {"l2_rho_rel": float(np.sqrt(num_r / den)), "linf_rho_rel": float(np.max(lin_r)),
+                            "l2_p_rel": float(np.sqrt(num_p / den)), "linf_p_rel": float(np.max(lin_p)),
+                            "nonfinite_values": nonfinite, "steps": args.warmup + args.steps}
     for it in its.values():
         it.close()
     return out

@@ -349,17 +349,54 @@ def vortex_field(patch, mach, centre, beta, radius):
     return np.ascontiguousarray(prim_to_cons(p, T_INF * Tn, u, v, np.zeros(shape)))
 
 
-def tiled_state(patches, mach=0.4, seed=42):
-    """One seeded vortex per patch (random centre in the middle of the patch,
-    strength 3..6, radius a tenth of the patch's smallest extent) on a common
-    uniform flow; the vortices decay towards the patch faces, so overlapping
-    patches nearly agree."""
+def tiled_state(patches, mach=0.4, seed=42, radius_cells=4.0, h=1.0 / 256, cutoff=4.0):
+    """One seeded vortex per patch (axis z, centre in the middle 40 % of the
+    patch, strength 3..6, radius `radius_cells` coarse cells of 2h, damped
+    along z over the same radius, exactly zero beyond `cutoff` radii) on a
+    common uniform flow.  The vortices superpose into one global field
+    (velocity perturbations add, temperature factors multiply) evaluated at
+    every patch's own cell centres, so overlapping patches agree."""
     rng = np.random.default_rng(seed + 1)
-    out = []
+    R = radius_cells * 2.0 * h
+    vort = []
     for p in patches:
         lo = np.array(p["origin"])
         L = np.array(p["length"])
-        centre = lo + L * rng.uniform(0.4, 0.6, 3)
-        beta = float(rng.uniform(3.0, 6.0))
-        out.append(vortex_field(p, mach, centre, beta, 0.1 * float(L.min())))
+        vort.append((lo + L * rng.uniform(0.3, 0.7, 3), float(rng.uniform(3.0, 6.0))))
+    centres = np.array([c for c, _ in vort])
+    reach = cutoff * R
+    out = []
+    for p in patches:
+        lo = np.array(p["origin"])
+        hi = lo + np.array(p["length"])
+        xs = [p["origin"][a] + (np.arange(p["n"][a]) + 0.5) * (p["length"][a] / p["n"][a]) for a in range(3)]
+        shape = tuple(p["n"])
+        du = np.zeros(shape)
+        dv = np.zeros(shape)
+        Tn = np.ones(shape)
+        near = np.all((centres > lo - reach) & (centres < hi + reach), axis=1)
+        for q in np.nonzero(near)[0]:
+            c, beta = vort[q]
+            sl = []
+            for a in range(3):                        # sub-box within reach of the centre
+                i0 = int(np.searchsorted(xs[a], c[a] - reach))
+                i1 = int(np.searchsorted(xs[a], c[a] + reach))
+                sl.append(slice(i0, i1))
+            if any(t.start >= t.stop for t in sl):
+                continue
+            x = xs[0][sl[0]][:, None, None]
+            y = xs[1][sl[1]][None, :, None]
+            z = xs[2][sl[2]][None, None, :]
+            xr, yr, zr = (x - c[0]) / R, (y - c[1]) / R, (z - c[2]) / R
+            r2 = xr * xr + yr * yr + zr * zr
+            e = np.exp(0.5 * (1.0 - (xr * xr + yr * yr))) * np.exp(-0.5 * zr * zr) * (r2 < cutoff * cutoff)
+            k = beta / (2.0 * math.pi)
+            sub = (sl[0], sl[1], sl[2])
+            du[sub] = du[sub] - k * yr * e * A_INF
+            dv[sub] = dv[sub] + k * xr * e * A_INF
+            Tn[sub] = Tn[sub] * (1.0 - (GAS_GAMMA - 1.0) * beta * beta / (8.0 * GAS_GAMMA * math.pi ** 2) * e * e)
+        rho = RHO_INF * Tn ** (1.0 / (GAS_GAMMA - 1.0))
+        pr = rho * GAS_R * T_INF * Tn
+        u = mach * A_INF + du
+        out.append(np.ascontiguousarray(prim_to_cons(pr, T_INF * Tn, u, dv, np.zeros(shape))))
     return out

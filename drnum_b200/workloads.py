@@ -58,7 +58,7 @@ def build(name, scale=1.0):
         h = min(min(p["length"][a] / p["n"][a] for a in range(3)) for p in patches)
         dt = 0.4 * h / (1.6 * cases.A_INF)
         desc = (f"uneven batched grid: {len(patches)} patches, seeded extents, refinement 1 and 2, 2-cell overlaps, "
-                "one seeded vortex (beta 3-6) per patch on Mach 0.4 flow, far field outside")
+                "one seeded vortex (beta 3-6, radius 4 coarse cells) per patch superposed on Mach 0.4 flow, far field outside")
         return dict(patches=patches, states=states, bcs=bcs, levelset=None, dt=dt, description=desc)
     raise KeyError(name)
 
