@@ -35,11 +35,12 @@
 // identical bits.
 //
 // Data flow per CTA: a TJ x TK tile of (j, k) columns marches along i.  Each
-// plane of the stencil state (int32) is prefetched into registers one step
-// ahead, dequantised once, and stored as FP32 in a four-plane shared-memory
-// ring with a two-cell halo in j and k.  x faces are evaluated per thread
-// along its own column (the left state of the next face stays in registers);
-// y and z face states and face integers are exchanged through shared memory.
+// plane of the stencil state (int32) is copied asynchronously (cp.async) into
+// a four-plane shared-memory ring with a two-cell halo in j and k, about two
+// planes ahead of its first use, and dequantised there once to FP32.  x faces
+// are evaluated per thread along its own column (the left state of the next
+// face stays in registers); y and z face states and face integers are
+// exchanged through shared memory.
 #pragma once
 
 #include <cstdint>
@@ -166,6 +167,111 @@ __device__ __forceinline__ float fx_slope(float a, float b)
   return den > 1e-30f ? __fdividef(num, den) : 0.0f;
 }
 
+// ---------------------------------------------------------------------------
+// Paired y/z evaluation.  Lane x of a pair carries a y-direction quantity of
+// a cell, lane y the z-direction one; the halo cells and faces of the two
+// directions share a thread, which halves the work of the threads that
+// handle the tile's halo.  Every y and z slope and face of the kernel, own or
+// halo, goes through these functions, so a face evaluated by two CTAs rounds
+// identically.  (The packed f32x2 instructions of sm_100 measured no faster
+// here than two scalar ones: the kernel is not FP32-pipe bound.)
+__device__ __forceinline__ float2 v2(float a) { return make_float2(a, a); }
+__device__ __forceinline__ float2 add2(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ float2 sub2(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
+__device__ __forceinline__ float2 mul2(float2 a, float2 b) { return make_float2(a.x * b.x, a.y * b.y); }
+__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c)
+{
+  return make_float2(fmaf(a.x, b.x, c.x), fmaf(a.y, b.y, c.y));
+}
+__device__ __forceinline__ float2 rcp2(float2 a) { return make_float2(__fdividef(1.0f, a.x), __fdividef(1.0f, a.y)); }
+__device__ __forceinline__ float2 max0(float2 a) { return make_float2(fmaxf(a.x, 0.0f), fmaxf(a.y, 0.0f)); }
+__device__ __forceinline__ float2 min0(float2 a) { return make_float2(fminf(a.x, 0.0f), fminf(a.y, 0.0f)); }
+
+struct Prim2 {
+  float2 r, u, v, w, p, a, H;
+};
+
+__device__ __forceinline__ Prim2 fx_prim2(float2 r, float2 ru, float2 rv, float2 rw, float2 rE)
+{
+  constexpr float R_over_cv = (float)(Gas::R / Gas::cv);
+  constexpr float gam = (float)Gas::gamma;
+  Prim2 s;
+  const float2 ir = rcp2(r);
+  s.r = r;
+  s.u = mul2(ru, ir);
+  s.v = mul2(rv, ir);
+  s.w = mul2(rw, ir);
+  const float2 ke2 = fma2(rw, s.w, fma2(rv, s.v, mul2(ru, s.u)));
+  s.p = mul2(v2(R_over_cv), fma2(v2(-0.5f), ke2, rE));
+  const float2 p_ir = mul2(s.p, ir);
+  const float2 t = mul2(v2(gam), p_ir);
+  s.a = make_float2(sqrtf(t.x), sqrtf(t.y));
+  s.H = fma2(rE, ir, p_ir);
+  return s;
+}
+
+// fx_split for a pair of Mach numbers (both lanes on the same side S)
+template <int S>
+__device__ __forceinline__ void fx_split2(float2 M, float2& m4, float2& p5)
+{
+  const float2 ap = add2(M, v2(1.0f)), am = sub2(M, v2(1.0f));
+  const float2 ap2 = mul2(ap, ap), am2 = mul2(am, am);
+  float2 sub_m4, sub_p5;
+  if (S > 0) {
+    const float2 t = mul2(v2(0.25f), ap2);
+    sub_m4 = mul2(t, fma2(v2(0.5f), am2, v2(1.0f)));
+    sub_p5 = mul2(t, fma2(mul2(v2(0.75f), M), am2, sub2(v2(2.0f), M)));
+  } else {
+    const float2 t = mul2(v2(0.25f), am2);
+    sub_m4 = mul2(v2(-1.0f), mul2(t, fma2(v2(0.5f), ap2, v2(1.0f))));
+    sub_p5 = mul2(t, fma2(mul2(v2(-0.75f), M), ap2, add2(v2(2.0f), M)));
+  }
+  const bool supx = fabsf(M.x) >= 1.0f, supy = fabsf(M.y) >= 1.0f;
+  if (S > 0) {
+    m4.x = supx ? fmaxf(M.x, 0.0f) : sub_m4.x;
+    m4.y = supy ? fmaxf(M.y, 0.0f) : sub_m4.y;
+    p5.x = supx ? (M.x > 0.0f ? 1.0f : 0.0f) : sub_p5.x;
+    p5.y = supy ? (M.y > 0.0f ? 1.0f : 0.0f) : sub_p5.y;
+  } else {
+    m4.x = supx ? fminf(M.x, 0.0f) : sub_m4.x;
+    m4.y = supy ? fminf(M.y, 0.0f) : sub_m4.y;
+    p5.x = supx ? (M.x < 0.0f ? 1.0f : 0.0f) : sub_p5.x;
+    p5.y = supy ? (M.y < 0.0f ? 1.0f : 0.0f) : sub_p5.y;
+  }
+}
+
+// fx_ausm for a y face (lane x, normal y) and a z face (lane y, normal z);
+// A = (Ay, Az)
+__device__ __forceinline__ void fx_ausm2(const Prim2& L, const Prim2& R, float2 A, float2 F[5])
+{
+  const float2 unl = make_float2(L.v.x, L.w.y);
+  const float2 unr = make_float2(R.v.x, R.w.y);
+  const float2 a = mul2(v2(0.5f), add2(L.a, R.a));
+  const float2 ia = rcp2(a);
+  float2 m4l, p5l, m4r, p5r;
+  fx_split2<1>(mul2(unl, ia), m4l, p5l);
+  fx_split2<-1>(mul2(unr, ia), m4r, p5r);
+  const float2 M = add2(m4l, m4r);
+  const float2 p = fma2(p5l, L.p, mul2(p5r, R.p));
+  const float2 f0 = mul2(mul2(a, A), fma2(L.r, max0(M), mul2(R.r, min0(M))));
+  const float2 cp = max0(f0), cm = min0(f0);
+  const float2 Ap = mul2(A, p);
+  F[0] = f0;
+  F[1] = fma2(cp, L.u, mul2(cm, R.u));
+  F[2] = fma2(cp, L.v, fma2(cm, R.v, make_float2(Ap.x, 0.0f)));
+  F[3] = fma2(cp, L.w, fma2(cm, R.w, make_float2(0.0f, Ap.y)));
+  F[4] = fma2(cp, L.H, mul2(cm, R.H));
+}
+
+// van Albada slopes of a pair of (a, b) differences
+__device__ __forceinline__ float2 fx_slope2(float2 a, float2 b)
+{
+  const float2 den = fma2(a, a, mul2(b, b));
+  const float2 num = mul2(mul2(mul2(v2(0.5f), a), b), add2(a, b));
+  const float2 q = mul2(num, rcp2(den));
+  return make_float2(den.x > 1e-30f ? q.x : 0.0f, den.y > 1e-30f ? q.y : 0.0f);
+}
+
 __device__ __forceinline__ int fx_wrap(int x, int n, int per)
 {
   if (per) {
@@ -221,9 +327,22 @@ __device__ __forceinline__ void fx_cp_async4(void* smem, const void* gmem)
   asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" :: "r"(s), "l"(gmem) : "memory");
 }
 
-__device__ __forceinline__ void fx_cp_async_wait_all()
+// 4-byte asynchronous copy that writes zero instead when ok is false
+__device__ __forceinline__ void fx_cp_async4_or_zero(void* smem, const void* gmem, bool ok)
 {
-  asm volatile("cp.async.wait_all;" ::: "memory");
+  const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;" :: "r"(s), "l"(gmem), "r"(ok ? 4 : 0) : "memory");
+}
+
+__device__ __forceinline__ void fx_cp_async_commit()
+{
+  asm volatile("cp.async.commit_group;" ::: "memory");
+}
+
+template <int N>
+__device__ __forceinline__ void fx_cp_async_wait()
+{
+  asm volatile("cp.async.wait_group %0;" :: "n"(N) : "memory");
 }
 
 // Is the tile "full": every own column inside the patch and, on closed j/k
@@ -278,27 +397,36 @@ __device__ __forceinline__ void fx_stage_tile_impl(const FxArgs& a, int j0, int 
     }
   }
 
-  int32_t pre[5][PPT];
-  auto fetch = [&](int ip) {
+  // plane ip of the stage input: copied asynchronously as int32 into its
+  // ring slot (zero outside a closed patch) ...
+  auto issue = [&](int ip) {
     const int iw = fx_wrap(ip, g.ni, g.per_x);
-    #pragma unroll
-    for (int v = 0; v < 5; ++v) {
-      const int32_t* src = a.in + (size_t)v * nc + (size_t)(iw < 0 ? 0 : iw) * njk;
-      #pragma unroll
-      for (int m = 0; m < PPT; ++m) {
-        pre[v][m] = 0;
-        if (iw >= 0 && poff[m] >= 0) pre[v][m] = __ldg(src + poff[m]);
-      }
-    }
-  };
-  auto commit = [&](int ip) {
-    float* dst = &sm.plane[ip & 3][0][0][0][0];
+    int* dst = reinterpret_cast<int*>(&sm.plane[ip & 3][0][0][0][0]);
+    const int32_t* src = a.in + (size_t)(iw < 0 ? 0 : iw) * njk;
     #pragma unroll
     for (int v = 0; v < 5; ++v) {
       #pragma unroll
       for (int m = 0; m < PPT; ++m) {
         const int e = tid + m * NT;
-        if (e < NP) dst[v * NP + e] = fmaf(P.quantum[v], (float)pre[v][m], P.base[v]);
+        if (e < NP) {
+          const bool ok = iw >= 0 && poff[m] >= 0;
+          fx_cp_async4_or_zero(dst + v * NP + e, src + (size_t)v * nc + (ok ? poff[m] : 0), ok);
+        }
+      }
+    }
+    fx_cp_async_commit();
+  };
+  // ... and dequantised in place by the thread that copied it, once its copy
+  // group has completed; a barrier then publishes it to the CTA
+  auto dequant = [&](int ip) {
+    float* f = &sm.plane[ip & 3][0][0][0][0];
+    const int* q = reinterpret_cast<const int*>(f);
+    #pragma unroll
+    for (int v = 0; v < 5; ++v) {
+      #pragma unroll
+      for (int m = 0; m < PPT; ++m) {
+        const int e = tid + m * NT;
+        if (e < NP) f[v * NP + e] = fmaf(P.quantum[v], (float)q[v * NP + e], P.base[v]);
       }
     }
   };
@@ -311,22 +439,20 @@ __device__ __forceinline__ void fx_stage_tile_impl(const FxArgs& a, int j0, int 
       #pragma unroll
       for (int v = 0; v < 5; ++v) fx_cp_async4(&sm.un[v][ty][tx], a.un + (size_t)v * nc + c);
     }
+    fx_cp_async_commit();
   };
   fetch_un(i0);
 
   // prologue: planes i0-1 .. i0+2 in the ring
-  for (int q = -1; q <= 2; ++q) {
-    fetch(i0 + q);
-    commit(i0 + q + 4);     // +4 keeps the slot index non-negative
-  }
-  fetch(i0 + 3);
+  for (int q = -1; q <= 2; ++q) issue(i0 + q);
+  fx_cp_async_wait<0>();
+  for (int q = -1; q <= 2; ++q) dequant(i0 + q);
   __syncthreads();
 
   // x direction registers: left state of the face above the current cell,
   // the downwind difference of the current cell, and the lower face integers
   Prim xleft;
   float xb[5];           // U_{i+1} - U_i of the own column (becomes a of cell i+1)
-  float xu0[5], xu1[5];  // own-column state at planes i and i+1
   int qx_lo[5];
   {
     // slope of cell i0 (needs i0-1, i0, i0+1) and the face below i0
@@ -341,8 +467,6 @@ __device__ __forceinline__ void fx_stage_tile_impl(const FxArgs& a, int j0, int 
       const float up = PL(s_p1, v, ty + 2, tx + 2);
       const float s = sx ? fx_slope(uc - um, up - uc) : 0.0f;
       U0[v] = uc;
-      xu0[v] = uc;
-      xu1[v] = up;
       Sp[v] = uc + s;
       Sm[v] = uc - s;
       xb[v] = up - uc;
@@ -373,80 +497,132 @@ __device__ __forceinline__ void fx_stage_tile_impl(const FxArgs& a, int j0, int 
   }
 
   for (int i = i0; i < i1; ++i) {
-    const int s0 = i & 3, sp2 = (i + 2) & 3;
+    const int s0 = i & 3, sp1 = (i + 1) & 3, sp2 = (i + 2) & 3;
 
     // ---------------- y and z face states of plane i
-    float ym[5], zm[5];   // right states of the faces below the own cell
+    float2 yzm[5];   // right states of the y (lane x) and z (lane y) faces below the own cell
     {
       const bool sy = FULL || (fx_cell_ok(j - 1, g.nj, g.per_y) && fx_cell_ok(j + 1, g.nj, g.per_y));
       const bool sz = FULL || (fx_cell_ok(k - 1, g.nk, g.per_z) && fx_cell_ok(k + 1, g.nk, g.per_z));
       #pragma unroll
       for (int v = 0; v < 5; ++v) {
-        const float uc = xu0[v];
-        const float uyl = PL(s0, v, ty + 1, tx + 2);
-        const float uyh = PL(s0, v, ty + 3, tx + 2);
-        const float uzl = PL(s0, v, ty + 2, tx + 1);
-        const float uzh = PL(s0, v, ty + 2, tx + 3);
-        const float s_y = sy ? fx_slope(uc - uyl, uyh - uc) : 0.0f;
-        const float s_z = sz ? fx_slope(uc - uzl, uzh - uc) : 0.0f;
-        sm.sy[v][ty + 1][tx] = uc + s_y;
-        sm.szL[v][ty][tx] = uc + s_z;
-        ym[v] = uc - s_y;
-        zm[v] = uc - s_z;
+        const float2 uc = v2(PL(s0, v, ty + 2, tx + 2));
+        const float2 ul = make_float2(PL(s0, v, ty + 1, tx + 2), PL(s0, v, ty + 2, tx + 1));
+        const float2 uh = make_float2(PL(s0, v, ty + 3, tx + 2), PL(s0, v, ty + 2, tx + 3));
+        float2 s = fx_slope2(sub2(uc, ul), sub2(uh, uc));
+        if (!FULL) s = make_float2(sy ? s.x : 0.0f, sz ? s.y : 0.0f);
+        const float2 up = add2(uc, s);
+        sm.sy[v][ty + 1][tx] = up.x;
+        sm.szL[v][ty][tx] = up.y;
+        yzm[v] = sub2(uc, s);
       }
     }
-    // halo cells: y rows -1 (left state) and TJ (right state); z cols -1 and TK
-    for (int h = tid; h < 2 * TK + 2 * TJ; h += NT) {
-      if (h < 2 * TK) {
-        const int kk = h % TK;
-        const bool top = h >= TK;
-        const int jj = top ? TJ : -1;               // tile-relative row
-        const int jc = j0 + jj, kc = k0 + kk;
-        const bool sy = fx_cell_ok(jc - 1, g.nj, g.per_y) && fx_cell_ok(jc + 1, g.nj, g.per_y) &&
-                        fx_cell_ok(jc, g.nj, g.per_y);
-        #pragma unroll
-        for (int v = 0; v < 5; ++v) {
-          const float uc = PL(s0, v, jj + 2, kk + 2);
-          const float ul = PL(s0, v, jj + 1, kk + 2);
-          const float uh = PL(s0, v, jj + 3, kk + 2);
-          const float s = (FULL || (sy && kc < g.nk)) ? fx_slope(uc - ul, uh - uc) : 0.0f;
-          if (top) sm.sy_top[v][kk] = uc - s;
-          else sm.sy[v][0][kk] = uc + s;
+    // halo cells, y and z in pairs: y rows -1 (left state) and TJ (right
+    // state), z cols -1 and TK
+    for (int h = tid; h < 2 * (TK > TJ ? TK : TJ); h += NT) {
+      const bool hy = h < 2 * TK, hz = h < 2 * TJ;
+      const int kky = h % TK;
+      const bool topy = h >= TK;
+      const int jjy = topy ? TJ : -1;                 // tile-relative row of the y cell
+      const int jjz = h % TJ;
+      const bool topz = h >= TJ;
+      const int kkz = topz ? TK : -1;                 // tile-relative col of the z cell
+      bool oky = hy, okz = hz;
+      if (!FULL) {
+        const int jc = j0 + jjy, kc = k0 + kky;
+        oky = oky && fx_cell_ok(jc - 1, g.nj, g.per_y) && fx_cell_ok(jc + 1, g.nj, g.per_y) &&
+              fx_cell_ok(jc, g.nj, g.per_y) && kc < g.nk;
+        const int jz = j0 + jjz, kz = k0 + kkz;
+        okz = okz && fx_cell_ok(kz - 1, g.nk, g.per_z) && fx_cell_ok(kz + 1, g.nk, g.per_z) &&
+              fx_cell_ok(kz, g.nk, g.per_z) && jz < g.nj;
+      }
+      // a lane without a cell evaluates the other lane's cell and stores nothing
+      const int ry = hy ? jjy + 2 : jjz + 2, cy = hy ? kky + 2 : kkz + 2;
+      const int rz = hz ? jjz + 2 : jjy + 2, cz = hz ? kkz + 2 : kky + 2;
+      #pragma unroll
+      for (int v = 0; v < 5; ++v) {
+        const float2 uc = make_float2(PL(s0, v, ry, cy), PL(s0, v, rz, cz));
+        const float2 ul = make_float2(PL(s0, v, ry - 1, cy), PL(s0, v, rz, cz - 1));
+        const float2 uh = make_float2(PL(s0, v, ry + 1, cy), PL(s0, v, rz, cz + 1));
+        float2 s = fx_slope2(sub2(uc, ul), sub2(uh, uc));
+        s = make_float2(FULL || oky ? s.x : 0.0f, FULL || okz ? s.y : 0.0f);
+        const float2 up = add2(uc, s), dn = sub2(uc, s);
+        if (hy) {
+          if (topy) sm.sy_top[v][kky] = dn.x;
+          else sm.sy[v][0][kky] = up.x;
         }
-      } else {
-        const int hh = h - 2 * TK;
-        const int jj = hh % TJ;
-        const bool top = hh >= TJ;
-        const int kk = top ? TK : -1;
-        const int jc = j0 + jj, kc = k0 + kk;
-        const bool sz = fx_cell_ok(kc - 1, g.nk, g.per_z) && fx_cell_ok(kc + 1, g.nk, g.per_z) &&
-                        fx_cell_ok(kc, g.nk, g.per_z);
-        #pragma unroll
-        for (int v = 0; v < 5; ++v) {
-          const float uc = PL(s0, v, jj + 2, kk + 2);
-          const float ul = PL(s0, v, jj + 2, kk + 1);
-          const float uh = PL(s0, v, jj + 2, kk + 3);
-          const float s = (FULL || (sz && jc < g.nj)) ? fx_slope(uc - ul, uh - uc) : 0.0f;
-          if (top) sm.sz_top[v][jj] = uc - s;
-          else sm.szH[v][z_warp<TK>(jj)][zh_slot<TK>(jj)] = uc + s;
+        if (hz) {
+          if (topz) sm.sz_top[v][jjz] = dn.y;
+          else sm.szH[v][z_warp<TK>(jjz)][zh_slot<TK>(jjz)] = up.y;
         }
       }
     }
     __syncthreads();
 
+    // the prologue's last reads of plane i0-1 preceded this barrier: its
+    // slot receives plane i0+3
+    if (i == i0) issue(i + 3);
+
+    // ---------------- y and z faces below the own cell (+ the top halo faces)
+    {
+      // the face below row j is needed even when row j itself lies beyond a
+      // periodic patch (it is the wrapped face above the last row)
+      const bool exy = FULL || (k < g.nk && fx_face_exists(j, g.nj, g.per_y) && (g.per_y || j < g.nj));
+      const bool exz = FULL || (j < g.nj && fx_face_exists(k, g.nk, g.per_z) && (g.per_z || k < g.nk));
+      float2 L[5];
+      #pragma unroll
+      for (int v = 0; v < 5; ++v)
+        L[v] = make_float2(sm.sy[v][ty][tx], tx > 0 ? sm.szL[v][ty][tx - 1] : sm.szH[v][z_warp<TK>(ty)][zh_slot<TK>(ty)]);
+      float2 F[5];
+      fx_ausm2(fx_prim2(L[0], L[1], L[2], L[3], L[4]), fx_prim2(yzm[0], yzm[1], yzm[2], yzm[3], yzm[4]),
+               make_float2(P.Ay, P.Az), F);
+      #pragma unroll
+      for (int v = 0; v < 5; ++v) {
+        const float2 q = mul2(F[v], v2(P.face_scale[v]));
+        sm.qy[v][ty][tx] = exy ? __float2int_rn(q.x) : 0;
+        sm.qzL[v][ty][tx] = exz ? __float2int_rn(q.y) : 0;
+      }
+    }
+    // halo faces, y and z in pairs: below halo row TJ (col kk = h) and below
+    // halo col TK (row jj = h)
+    for (int h = tid; h < (TK > TJ ? TK : TJ); h += NT) {
+      const bool hy = h < TK, hz = h < TJ;
+      bool exy = hy, exz = hz;
+      if (!FULL) {
+        const int jf = j0 + TJ, kf = k0 + h;
+        exy = exy && kf < g.nk && fx_face_exists(jf, g.nj, g.per_y) && (g.per_y || jf < g.nj);
+        const int jz = j0 + h, kz = k0 + TK;
+        exz = exz && jz < g.nj && fx_face_exists(kz, g.nk, g.per_z) && (g.per_z || kz < g.nk);
+      }
+      // a lane without a face evaluates the other lane's face and stores nothing
+      const int ky = hy ? h : 0, jz = hz ? h : 0;
+      float2 L[5], R[5];
+      #pragma unroll
+      for (int v = 0; v < 5; ++v) {
+        L[v] = make_float2(sm.sy[v][TJ][ky], sm.szL[v][jz][TK - 1]);
+        R[v] = make_float2(sm.sy_top[v][ky], sm.sz_top[v][jz]);
+      }
+      float2 F[5];
+      fx_ausm2(fx_prim2(L[0], L[1], L[2], L[3], L[4]), fx_prim2(R[0], R[1], R[2], R[3], R[4]),
+               make_float2(P.Ay, P.Az), F);
+      #pragma unroll
+      for (int v = 0; v < 5; ++v) {
+        const float2 q = mul2(F[v], v2(P.face_scale[v]));
+        if (hy) sm.qy[v][TJ][h] = exy ? __float2int_rn(q.x) : 0;
+        if (hz) sm.qzT[v][z_warp<TK>(h)][zt_slot<TK>(h)] = exz ? __float2int_rn(q.y) : 0;
+      }
+    }
     // ---------------- x: face above cell i (between i and i+1); plane i+2
-    // was committed before this iteration's first barrier
+    // was dequantised before this iteration's first barrier
     int qx_hi[5];
-    float xu2[5];
     {
       const bool ex = own && fx_face_exists(i + 1, g.ni, g.per_x);
       const bool sx = fx_cell_ok(i + 2, g.ni, g.per_x);   // slope of cell i+1 needs i+2 (i is in range)
       float Sm[5], Sp[5];
       #pragma unroll
       for (int v = 0; v < 5; ++v) {
-        const float uc = xu1[v];
+        const float uc = PL(sp1, v, ty + 2, tx + 2);
         const float up = PL(sp2, v, ty + 2, tx + 2);
-        xu2[v] = up;
         const float b = up - uc;
         const float s = sx ? fx_slope(xb[v], b) : 0.0f;
         Sm[v] = uc - s;
@@ -465,70 +641,11 @@ __device__ __forceinline__ void fx_stage_tile_impl(const FxArgs& a, int j0, int 
       xleft = fx_prim(Sp[0], Sp[1], Sp[2], Sp[3], Sp[4]);
     }
 
-    // ---------------- y and z faces below the own cell (+ the top halo faces)
-    {
-      // the face below row j is needed even when row j itself lies beyond a
-      // periodic patch (it is the wrapped face above the last row)
-      const bool exy = FULL || (k < g.nk && fx_face_exists(j, g.nj, g.per_y) && (g.per_y || j < g.nj));
-      const bool exz = FULL || (j < g.nj && fx_face_exists(k, g.nk, g.per_z) && (g.per_z || k < g.nk));
-      float F[5];
-      if (exy) {
-        fx_ausm<1>(fx_prim(sm.sy[0][ty][tx], sm.sy[1][ty][tx], sm.sy[2][ty][tx], sm.sy[3][ty][tx], sm.sy[4][ty][tx]),
-                   fx_prim(ym[0], ym[1], ym[2], ym[3], ym[4]), P.Ay, F);
-        #pragma unroll
-        for (int v = 0; v < 5; ++v) sm.qy[v][ty][tx] = __float2int_rn(F[v] * P.face_scale[v]);
-      } else {
-        #pragma unroll
-        for (int v = 0; v < 5; ++v) sm.qy[v][ty][tx] = 0;
-      }
-      if (exz) {
-        float zl[5];
-        #pragma unroll
-        for (int v = 0; v < 5; ++v) zl[v] = tx > 0 ? sm.szL[v][ty][tx - 1] : sm.szH[v][z_warp<TK>(ty)][zh_slot<TK>(ty)];
-        fx_ausm<2>(fx_prim(zl[0], zl[1], zl[2], zl[3], zl[4]), fx_prim(zm[0], zm[1], zm[2], zm[3], zm[4]), P.Az, F);
-        #pragma unroll
-        for (int v = 0; v < 5; ++v) sm.qzL[v][ty][tx] = __float2int_rn(F[v] * P.face_scale[v]);
-      } else {
-        #pragma unroll
-        for (int v = 0; v < 5; ++v) sm.qzL[v][ty][tx] = 0;
-      }
-    }
-    for (int h = tid; h < TK + TJ; h += NT) {
-      float F[5];
-      if (h < TK) {
-        const int kk = h;
-        const int jf = j0 + TJ, kf = k0 + kk;   // face below halo row TJ
-        const bool ex = FULL || (kf < g.nk && fx_face_exists(jf, g.nj, g.per_y) && (g.per_y || jf < g.nj));
-        if (ex) {
-          fx_ausm<1>(fx_prim(sm.sy[0][TJ][kk], sm.sy[1][TJ][kk], sm.sy[2][TJ][kk], sm.sy[3][TJ][kk], sm.sy[4][TJ][kk]),
-                     fx_prim(sm.sy_top[0][kk], sm.sy_top[1][kk], sm.sy_top[2][kk], sm.sy_top[3][kk], sm.sy_top[4][kk]),
-                     P.Ay, F);
-          #pragma unroll
-          for (int v = 0; v < 5; ++v) sm.qy[v][TJ][kk] = __float2int_rn(F[v] * P.face_scale[v]);
-        } else {
-          #pragma unroll
-          for (int v = 0; v < 5; ++v) sm.qy[v][TJ][kk] = 0;
-        }
-      } else {
-        const int jj = h - TK;
-        const int jf = j0 + jj, kf = k0 + TK;   // face below halo col TK
-        const bool ex = FULL || (jf < g.nj && fx_face_exists(kf, g.nk, g.per_z) && (g.per_z || kf < g.nk));
-        if (ex) {
-          fx_ausm<2>(fx_prim(sm.szL[0][jj][TK - 1], sm.szL[1][jj][TK - 1], sm.szL[2][jj][TK - 1], sm.szL[3][jj][TK - 1],
-                             sm.szL[4][jj][TK - 1]),
-                     fx_prim(sm.sz_top[0][jj], sm.sz_top[1][jj], sm.sz_top[2][jj], sm.sz_top[3][jj], sm.sz_top[4][jj]),
-                     P.Az, F);
-          #pragma unroll
-          for (int v = 0; v < 5; ++v) sm.qzT[v][z_warp<TK>(jj)][zt_slot<TK>(jj)] = __float2int_rn(F[v] * P.face_scale[v]);
-        } else {
-          #pragma unroll
-          for (int v = 0; v < 5; ++v) sm.qzT[v][z_warp<TK>(jj)][zt_slot<TK>(jj)] = 0;
-        }
-      }
-    }
     __syncthreads();
 
     // ---------------- residual and update of the own cell
+    // f(n) of plane i has arrived (the plane i+3 group may stay in flight)
+    fx_cp_async_wait<1>();
     if (own) {
       const int c = i * njk + j * g.nk + k;       // 5*cells < 2^31 (host check)
       const int ncv = (int)nc;
@@ -540,10 +657,16 @@ __device__ __forceinline__ void fx_stage_tile_impl(const FxArgs& a, int j0, int 
         res[v] = qx_lo[v] + sm.qy[v][ty][tx] + sm.qzL[v][ty][tx]
                - (tx < TK - 1 ? sm.qzL[v][ty][tx + 1] : sm.qzT[v][z_warp<TK>(ty)][zt_slot<TK>(ty)])
                - sm.qy[v][ty + 1][tx] - qx_hi[v];
-      if (a.wall.any && (i == 0 || i == g.ni - 1 || j == 0 || j == g.nj - 1 || k == 0 || k == g.nk - 1))
-        add_wall_fluxes(a.wall, g.ni, g.nj, g.nk, g.per_x, g.per_y, g.per_z, i, j, k, xu0, P.Ax, P.Ay, P.Az, res,
+      if (a.wall.any && (i == 0 || i == g.ni - 1 || j == 0 || j == g.nj - 1 || k == 0 || k == g.nk - 1)) {
+        // the cell's state, re-read from the stage input: the ring slot of
+        // plane i may already be receiving plane i+4 (no barrier separates
+        // this from the copies other threads issue at the end of the iteration)
+        float uc[5];
+        #pragma unroll
+        for (int v = 0; v < 5; ++v) uc[v] = fmaf(P.quantum[v], (float)a.in[v * ncv + c], P.base[v]);
+        add_wall_fluxes(a.wall, g.ni, g.nj, g.nk, g.per_x, g.per_y, g.per_z, i, j, k, uc, P.Ax, P.Ay, P.Az, res,
                         [&](int v, float F) { return __float2int_rn(F * P.face_scale[v]); });
-      fx_cp_async_wait_all();
+      }
       #pragma unroll
       for (int v = 0; v < 5; ++v) {
         int32_t o;
@@ -572,17 +695,15 @@ __device__ __forceinline__ void fx_stage_tile_impl(const FxArgs& a, int j0, int 
     #pragma unroll
     for (int v = 0; v < 5; ++v) {
       qx_lo[v] = qx_hi[v];
-      xu0[v] = xu1[v];
-      xu1[v] = xu2[v];
     }
 
-    // ---------------- ring: plane i+3 (prefetched) replaces plane i-1, which
-    // no phase of this or the next iteration reads; the next iteration's
-    // first barrier orders this commit before its reads of plane i+3, and
-    // the shared face arrays are written again only after that barrier
-    commit(i + 3 + 4);
-    fetch(i + 4);
+    // ---------------- ring: plane i+3 becomes readable (the next
+    // iteration's first barrier orders this before its reads of plane i+3);
+    // plane i, last read in this iteration, gives its slot to plane i+4
+    fx_cp_async_wait<0>();
+    dequant(i + 3);
     fetch_un(i + 1);
+    issue(i + 4);
   }
 }
 
