@@ -35,6 +35,27 @@ DN_BC_FARFIELD = 1
 DN_BC_SLIP = 2
 DN_BC_INFLOW = 3
 
+DN_FLUX_AUSMPLUS = 0
+DN_FLUX_AUSMPLUS_FUNCTOR = 1
+DN_FLUX_VANLEER = 2
+DN_FLUX_ROE = 3
+
+
+class dn_stage_launch(ctypes.Structure):
+    _fields_ = [
+        ("patch", c_int),
+        ("in_", c_void_p), ("un", c_void_p), ("out", c_void_p), ("active", c_void_p),
+        ("ni", c_int), ("nj", c_int), ("nk", c_int),
+        ("periodic", c_int * 3),
+        ("dx", c_double), ("dy", c_double), ("dz", c_double),
+        ("factor", c_double),
+        ("stream", c_void_p),
+        ("num_sms", c_int),
+    ]
+
+
+DN_STAGE_FN = ctypes.CFUNCTYPE(c_int, c_void_p, POINTER(dn_stage_launch))
+
 
 class dn_patch_desc(ctypes.Structure):
     _fields_ = [
@@ -96,6 +117,8 @@ SIGNATURES = {
                                 POINTER(c_uint64), POINTER(c_double)]),
     "dn_lslayers_destroy": (c_int, [c_void_p]),
     "dn_set_option": (c_int, [c_void_p, c_int, c_int]),
+    "dn_set_flux_scheme": (c_int, [c_void_p, c_int]),
+    "dn_set_stage_function": (c_int, [c_void_p, c_void_p, c_void_p]),
     "dn_patch_set_tile": (c_int, [c_void_p, c_int, c_int]),
     "dn_autotune": (c_int, [c_void_p, ctypes.c_char_p, POINTER(c_double)]),
 }

@@ -53,10 +53,11 @@ class PerfectGas:
     cv = 717.5
 
 
-class AusmPlus:
-    """The AUSM+ face-flux functor (fluxes/ausmplus.h:29-106) with its
-    reconstruction and gas model; the device kernels implement exactly this
-    combination."""
+class _EulerFlux:
+    """An Euler face-flux functor with its reconstruction and gas model.  The
+    device path implements the Upwind2<VanAlbada> reconstruction and
+    PerfectGas; `scheme` is the DN_FLUX_* constant of the C ABI."""
+    scheme = _lib.DN_FLUX_AUSMPLUS
 
     def __init__(self, reconstruction=None, gas=None):
         self.reconstruction = reconstruction if reconstruction is not None else Upwind2(VanAlbada())
@@ -65,6 +66,28 @@ class AusmPlus:
             raise ValueError("the device path implements Upwind2<VanAlbada> reconstruction only")
         if not isinstance(self.gas, PerfectGas):
             raise ValueError("the device path implements PerfectGas only")
+
+
+class AusmPlus(_EulerFlux):
+    """AUSM+ (fluxes/ausmplus.h:29-106): the specialised fused kernels (FP64
+    and FP32 bulk).  functor=True runs the same flux through the generic
+    functor kernel (FP64, bitwise equal)."""
+
+    def __init__(self, reconstruction=None, gas=None, functor=False):
+        super().__init__(reconstruction, gas)
+        self.scheme = _lib.DN_FLUX_AUSMPLUS_FUNCTOR if functor else _lib.DN_FLUX_AUSMPLUS
+
+
+class VanLeer(_EulerFlux):
+    """Van Leer flux-vector splitting (fluxes/vanleer.h:29-196), FP64,
+    through the generic functor kernel."""
+    scheme = _lib.DN_FLUX_VANLEER
+
+
+class Roe(_EulerFlux):
+    """Roe flux with the reference's entropy modification (fluxes/roe.h:
+    29-661), FP64, through the generic functor kernel."""
+    scheme = _lib.DN_FLUX_ROE
 
 
 # ----------------------------------------------------------------------- patches
@@ -224,12 +247,14 @@ class B200CartesianIterator:
 
     def __init__(self, op=None, cuda_device=0, precision=DN_FP64):
         self.m_Op = op if op is not None else AusmPlus()
-        if not isinstance(self.m_Op, AusmPlus):
-            raise ValueError("flux functor must be AusmPlus(Upwind2(VanAlbada()), PerfectGas())")
+        if not isinstance(self.m_Op, _EulerFlux):
+            raise ValueError("flux functor must be AusmPlus, VanLeer or Roe (Upwind2(VanAlbada()), PerfectGas())")
         self.lib = _lib.load()
         self.precision = precision
         self.ctx = ctypes.c_void_p()
         check(None, self.lib.dn_ctx_create(int(cuda_device), int(precision), ctypes.byref(self.ctx)))
+        if self.m_Op.scheme != _lib.DN_FLUX_AUSMPLUS:
+            check(self.ctx, self.lib.dn_set_flux_scheme(self.ctx, int(self.m_Op.scheme)))
         self.m_Patches: list[CartesianPatch] = []
         self.m_PatchActive: list[bool] = []
 
@@ -390,6 +415,21 @@ class B200CartesianIterator:
         """dn_set_option: DN_OPT_BATCHED (one launch per stage over all
         patches) or DN_OPT_GRAPH (CUDA-graph replay of whole steps)."""
         check(self.ctx, self.lib.dn_set_option(self.ctx, int(option), int(value)))
+
+    def setFluxScheme(self, op):
+        """Selects the Euler flux functor (AusmPlus, VanLeer, Roe) of an FP64
+        iterator: dn_set_flux_scheme."""
+        if not isinstance(op, _EulerFlux):
+            raise ValueError("flux functor must be AusmPlus, VanLeer or Roe")
+        check(self.ctx, self.lib.dn_set_flux_scheme(self.ctx, int(op.scheme)))
+        self.m_Op = op
+
+    def setStageFunction(self, fn, user=None):
+        """Installs a caller-written stage function (dn_set_stage_function):
+        `fn` is the address of an `int fn(void* user, const dn_stage_launch*)`
+        (e.g. from a shared library built on drnum_b200_functor.cuh), `user`
+        an address passed through; None restores the built-in scheme."""
+        check(self.ctx, self.lib.dn_set_stage_function(self.ctx, fn, user))
 
     def setTile(self, i_patch, shape):
         check(self.ctx, self.lib.dn_patch_set_tile(self.ctx, int(i_patch), int(shape)))

@@ -6,8 +6,9 @@ Every CUDA translation unit is compiled for sm_100a only; the FP64 stage
 kernel gets -fmad=false (bitwise parity with the reference CPU iterator), the
 FP32 (fixed-point storage) kernel gets fast-math intrinsics without implicit
 FMA contraction (duplicated border faces must round identically); the donor
-copy and the host overlap set-up are built without contraction too (weights
-and interpolated values round like the reference's).
+copy, the host overlap set-up and the generic flux-functor schemes are built
+without contraction too (weights, interpolated values and fluxes round like
+the reference's).
 """
 from __future__ import annotations
 
@@ -38,6 +39,7 @@ UNITS = {
     "dn_overlap.cpp": ["-Xcompiler", "-ffp-contract=off"],
     "dn_levelset.cpp": ["-Xcompiler", "-ffp-contract=off"],
     "dn_lsbc.cu": ["-fmad=false"],
+    "fv_schemes.cu": ["-fmad=false"],
 }
 
 
@@ -58,6 +60,7 @@ def _sources_newer(target: str, deps: list[str]) -> bool:
 def _headers() -> list[str]:
     hs = [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".cuh", ".h"))]
     hs.append(os.path.join(INCLUDE, "drnum_b200.h"))
+    hs.append(os.path.join(INCLUDE, "drnum_b200_functor.cuh"))
     return hs
 
 
@@ -91,7 +94,27 @@ def build(verbose: bool = False, ptxas_info: bool = False) -> str:
         res = subprocess.run(cmd, capture_output=True, text=True)
         if res.returncode != 0:
             raise RuntimeError(f"link failed:\n{res.stdout}\n{res.stderr}")
+    build_example()
     return LIB
+
+
+EXAMPLE_SRC = os.path.join(HERE, "examples", "rusanov_stage.cu")
+EXAMPLE_LIB = os.path.join(HERE, "examples", "libdn_example_stage.so")
+
+
+def build_example(verbose: bool = False) -> str:
+    """The example user stage function (a caller-written flux functor on
+    include/drnum_b200_functor.cuh), as its own shared library."""
+    deps = [EXAMPLE_SRC, os.path.join(INCLUDE, "drnum_b200.h"), os.path.join(INCLUDE, "drnum_b200_functor.cuh")]
+    if _sources_newer(EXAMPLE_LIB, deps):
+        cmd = [nvcc(), *ARCH, "-O3", "-std=c++17", "-lineinfo", "-fmad=false", "-shared", "-Xcompiler", "-fPIC",
+               "-I", INCLUDE, EXAMPLE_SRC, "-o", EXAMPLE_LIB]
+        if verbose:
+            print(" ".join(cmd), flush=True)
+        res = subprocess.run(cmd, capture_output=True, text=True)
+        if res.returncode != 0:
+            raise RuntimeError(f"example build failed:\n{res.stdout}\n{res.stderr}")
+    return EXAMPLE_LIB
 
 
 if __name__ == "__main__":

@@ -16,6 +16,7 @@
 #include "dn_levelset.h"
 #include "dn_lsbc.cuh"
 #include "fv_batch.cuh"
+#include "fv_schemes.cuh"
 
 #include <cmath>
 #include <cstdarg>
@@ -93,6 +94,10 @@ struct dn_ctx {
   cudaStream_t graph_stream = nullptr;
   int64_t generation = 0;
   int64_t graph_generation = -1;
+  // FP64 flux scheme (DN_FLUX_*) or a user stage function replacing it
+  int scheme = DN_FLUX_AUSMPLUS;
+  dn_stage_fn stage_fn = nullptr;
+  void* stage_user = nullptr;
 };
 
 #ifndef DN_FX_WAVE_CTAS
@@ -759,8 +764,10 @@ int stage_patch(dn_ctx* c, DnPatch& p, int in_b, int un_b, int out_b, double fac
 int stage_all(dn_ctx* c, int in_b, int un_b, int out_b, double factor)
 {
   // a single patch keeps its parameters in the kernel's constant bank (the
-  // batched form reads them from shared memory); the results are identical
-  if (!c->batched || c->patches.size() == 1) {
+  // batched form reads them from shared memory); the results are identical.
+  // Flux functors (another scheme or a user stage function) run per patch.
+  const bool functor = c->precision == DN_FP64 && (c->scheme != DN_FLUX_AUSMPLUS || c->stage_fn);
+  if (!c->batched || c->patches.size() == 1 || functor) {
     for (auto& p : c->patches) {
       int s = stage_patch(c, p, in_b, un_b, out_b, factor);
       if (s) return s;
@@ -798,7 +805,29 @@ int stage_patch(dn_ctx* c, DnPatch& p, int in_b, int un_b, int out_b, double fac
   g.per_y = p.d.face[1] == DN_FACE_PERIODIC;
   g.per_z = p.d.face[2] == DN_FACE_PERIODIC;
   cudaError_t e;
-  if (c->precision == DN_FP64) {
+  if (c->precision == DN_FP64 && (c->scheme != DN_FLUX_AUSMPLUS || c->stage_fn)) {
+    dn_stage_launch L;
+    L.patch = (int)(&p - c->patches.data());
+    L.in = (const double*)p.buf[in_b];
+    L.un = (const double*)p.buf[un_b];
+    L.out = (double*)p.buf[out_b];
+    L.active = p.active;
+    L.ni = g.ni; L.nj = g.nj; L.nk = g.nk;
+    L.periodic[0] = g.per_x; L.periodic[1] = g.per_y; L.periodic[2] = g.per_z;
+    L.dx = dx; L.dy = dy; L.dz = dz;
+    L.factor = factor;
+    L.stream = (void*)c->stream;
+    L.num_sms = c->num_sms;
+    c->launches++;
+    if (c->stage_fn) {
+      const int rc = c->stage_fn(c->stage_user, &L);
+      if (rc) return fail(c, rc < 0 ? rc : DN_ERR_ARG, "user stage function returned %d for patch %d", rc, L.patch);
+      return DN_OK;
+    }
+    e = dn::launch_scheme_stage(c->scheme, &L, p.wall);
+    if (e != cudaSuccess) return cuda_fail(c, e, "functor stage launch");
+    return DN_OK;
+  } else if (c->precision == DN_FP64) {
     dn::StageArgs<dn::PolicyF64> a;
     a.in = (const double*)p.buf[in_b];
     a.un = (const double*)p.buf[un_b];
@@ -1477,6 +1506,27 @@ int dn_set_option(dn_ctx* c, int option, int value)
     return DN_OK;
   }
   return fail(c, DN_ERR_ARG, "unknown option %d", option);
+}
+
+int dn_set_flux_scheme(dn_ctx* c, int scheme)
+{
+  if (!c) return DN_ERR_ARG;
+  if (scheme < DN_FLUX_AUSMPLUS || scheme > DN_FLUX_ROE) return fail(c, DN_ERR_ARG, "unknown flux scheme %d", scheme);
+  if (scheme != DN_FLUX_AUSMPLUS && c->precision != DN_FP64)
+    return fail(c, DN_ERR_ARG, "flux scheme %d needs an FP64 context (FP32 runs AUSM+ only)", scheme);
+  c->scheme = scheme;
+  c->generation++;
+  return DN_OK;
+}
+
+int dn_set_stage_function(dn_ctx* c, dn_stage_fn fn, void* user)
+{
+  if (!c) return DN_ERR_ARG;
+  if (fn && c->precision != DN_FP64) return fail(c, DN_ERR_ARG, "user stage functions need an FP64 context");
+  c->stage_fn = fn;
+  c->stage_user = user;
+  c->generation++;
+  return DN_OK;
 }
 
 int dn_patch_set_tile(dn_ctx* c, int id, int shape)

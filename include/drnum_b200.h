@@ -283,6 +283,55 @@ int dn_patch_set_tile(dn_ctx* ctx, int patch_id, int shape);
  * padded cell and stage.  No reference counterpart. */
 int dn_autotune(dn_ctx* ctx, const char* cache_path, double cost_out[2]);
 
+/* Flux scheme of the stage of an FP64 context; replaces the OP template
+ * argument of GPU_CartesianIterator<DIM, OP> (gpu_cartesianiterator.h:37)
+ * for the schemes DrNUM's applications instantiate.  All use the Upwind2
+ * reconstruction with the van Albada limiter and the patch-face fluxes of
+ * dn_patch_set_bc:
+ *   DN_FLUX_AUSMPLUS   AusmPlus (fluxes/ausmplus.h), the specialised fused
+ *                      kernels (default; the only scheme of DN_FP32)
+ *   DN_FLUX_AUSMPLUS_FUNCTOR  the same flux through the generic functor
+ *                      kernel (bitwise equal to DN_FLUX_AUSMPLUS)
+ *   DN_FLUX_VANLEER    VanLeer (fluxes/vanleer.h)
+ *   DN_FLUX_ROE        Roe with its entropy fix (fluxes/roe.h)
+ * DN_ERR_ARG for an unknown scheme or a non-default scheme on DN_FP32. */
+#define DN_FLUX_AUSMPLUS          0
+#define DN_FLUX_AUSMPLUS_FUNCTOR  1
+#define DN_FLUX_VANLEER           2
+#define DN_FLUX_ROE               3
+int dn_set_flux_scheme(dn_ctx* ctx, int scheme);
+
+/* A user stage function: one RK stage of one patch, launched by the caller's
+ * own code (typically dn::launch_functor_stage<OP> of drnum_b200_functor.cuh
+ * with the caller's flux functor, the analogue of instantiating
+ * GPU_CartesianIterator<DIM, OP> with an application functor,
+ * gpu_cartesianiterator.h:37 with e.g. applications/drnumJetDemo/jetflux.h).
+ * It must enqueue its work on L->stream and return 0, or a negative value
+ * that dn_rk_step / dn_compute pass on.  It computes
+ *   out = un + factor/dV * residual(in)   (inactive cells: out = in)
+ * for the patch's ni x nj x nk cells, [5][ni][nj][nk] FP64 arrays. */
+typedef struct dn_stage_launch {
+  int patch;                  /* patch id */
+  const double* in;           /* stage input f(k-1) (device) */
+  const double* un;           /* step-start state f(n) (device) */
+  double* out;                /* stage output f(k) (device) */
+  const unsigned char* active;/* per cell, NULL = all active (device) */
+  int ni, nj, nk;
+  int periodic[3];            /* 1 = index wrap on that axis */
+  double dx, dy, dz;
+  double factor;              /* alpha * dt */
+  void* stream;               /* cudaStream_t */
+  int num_sms;
+} dn_stage_launch;
+typedef int (*dn_stage_fn)(void* user, const dn_stage_launch* L);
+
+/* Installs a user stage function for every patch of an FP64 context (NULL
+ * restores the built-in scheme).  It runs inside dn_compute / dn_rk_step in
+ * place of the built-in stage launch, one call per patch and stage, and is
+ * captured into the step's CUDA graph with DN_OPT_GRAPH.  DN_ERR_ARG on an
+ * FP32 context. */
+int dn_set_stage_function(dn_ctx* ctx, dn_stage_fn fn, void* user);
+
 /* Number of device kernel launches the context has issued so far. */
 int dn_launch_count(const dn_ctx* ctx, int64_t* count);
 

@@ -61,6 +61,8 @@ def ref_lib():
         lib.dnref_run.restype = c_int
         lib.dnref_run.argtypes = [c_int, c_int, c_int, POINTER(c_int), c_double, c_double, c_double,
                                   _P, c_void_p, c_int, c_double, _P, c_int, c_int, _P, _P]
+        lib.dnref_run_scheme.restype = c_int
+        lib.dnref_run_scheme.argtypes = [c_int] + lib.dnref_run.argtypes
         lib.dnref_real_size.restype = c_int
         _ref = lib
     return _ref
@@ -128,8 +130,10 @@ def oracle_residual(U0, h, periodic=(True, True, True)):
     return res
 
 
-def ref_run(U0, h, dt, steps, alpha=(0.25, 0.5, 1.0), periodic=(True, True, True), active=None, threads=1):
-    """Runs the compiled reference; returns (state, seconds of the RK loop)."""
+def ref_run(U0, h, dt, steps, alpha=(0.25, 0.5, 1.0), periodic=(True, True, True), active=None, threads=1,
+            scheme=0):
+    """Runs the compiled reference; returns (state, seconds of the RK loop).
+    scheme: the Euler flux, numbered as DN_FLUX_* (0 AusmPlus, 2 VanLeer, 3 Roe)."""
     U = np.ascontiguousarray(U0, dtype=np.float64)
     _, ni, nj, nk = U.shape
     hx, hy, hz = (h, h, h) if np.isscalar(h) else h
@@ -139,10 +143,10 @@ def ref_run(U0, h, dt, steps, alpha=(0.25, 0.5, 1.0), periodic=(True, True, True
     act = None
     if active is not None:
         act = np.ascontiguousarray(active, dtype=np.uint8)
-    rc = ref_lib().dnref_run(ni, nj, nk, _per(periodic), hx, hy, hz, U.ctypes.data_as(_P),
-                             act.ctypes.data if act is not None else None, int(steps), float(dt),
-                             al.ctypes.data_as(_P), len(al), int(threads), out.ctypes.data_as(_P),
-                             ctypes.byref(sec))
+    rc = ref_lib().dnref_run_scheme(int(scheme), ni, nj, nk, _per(periodic), hx, hy, hz, U.ctypes.data_as(_P),
+                                    act.ctypes.data if act is not None else None, int(steps), float(dt),
+                                    al.ctypes.data_as(_P), len(al), int(threads), out.ctypes.data_as(_P),
+                                    ctypes.byref(sec))
     if rc != 0:
         raise RuntimeError(f"reference run failed: {rc}")
     return out, sec.value
@@ -217,6 +221,8 @@ class RefGrid:
         lib.dnref_grid_copy_donor_data.argtypes = [c_void_p, c_int]
         lib.dnref_grid_run.restype = c_int
         lib.dnref_grid_run.argtypes = [c_void_p, c_int, c_double, _P, c_int, _P]
+        lib.dnref_grid_run_scheme.restype = c_int
+        lib.dnref_grid_run_scheme.argtypes = [c_void_p, c_int, c_int, c_double, _P, c_int, _P]
         lib.dnref_grid_destroy.restype = None
         lib.dnref_grid_destroy.argtypes = [c_void_p]
         self.lib = lib
@@ -295,10 +301,11 @@ class RefGrid:
         if self.lib.dnref_grid_copy_donor_data(self.h, field) != 0:
             raise RuntimeError("copy_donor_data failed")
 
-    def run(self, steps, dt, alpha=(0.25, 0.5, 1.0)):
+    def run(self, steps, dt, alpha=(0.25, 0.5, 1.0), scheme=0):
         al = np.ascontiguousarray(alpha, dtype=np.float64)
         sec = c_double()
-        rc = self.lib.dnref_grid_run(self.h, int(steps), float(dt), al.ctypes.data_as(_P), len(al), ctypes.byref(sec))
+        rc = self.lib.dnref_grid_run_scheme(self.h, int(scheme), int(steps), float(dt), al.ctypes.data_as(_P),
+                                            len(al), ctypes.byref(sec))
         if rc != 0:
             raise RuntimeError(f"reference grid run failed: {rc}")
         return sec.value

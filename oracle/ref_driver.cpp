@@ -8,6 +8,7 @@
 //   CartesianPatch / PatchGrid           (cartesianpatch.cpp, patchgrid.cpp, patch.cpp)
 //   CartesianIterator<5, OP>             (iterators/cartesianiterator.h:87-325)
 //   AusmPlus<5, Upwind2<5, VanAlbada>, PerfectGas>  (fluxes/ausmplus.h:39-106)
+//   VanLeer / Roe with the same reconstruction        (fluxes/vanleer.h, fluxes/roe.h)
 //   RungeKutta                           (rungekutta.cpp:27-42)
 // The only pieces written here are harness glue: a periodic ghost-layer copy
 // post-operation (the reference has only a k-axis GPU version,
@@ -20,6 +21,8 @@
 #include "genericoperation.h"
 #include "perfectgas.h"
 #include "fluxes/ausmplus.h"
+#include "fluxes/vanleer.h"
+#include "fluxes/roe.h"
 #include "fluxes/compressiblefarfieldflux.h"
 #include "fluxes/compressibleslipflux.h"
 #include "reconstruction/upwind1.h"
@@ -51,13 +54,16 @@ bool checkVector(vec3_t V)
 namespace {
 
 typedef AusmPlus<5, Upwind2<5, VanAlbada>, PerfectGas> RefAusm;
+typedef VanLeer<5, Upwind2<5, VanAlbada>, PerfectGas> RefVanLeer;
+typedef Roe<5, Upwind2<5, VanAlbada>, PerfectGas> RefRoe;
 
-// Flux functor with the reference's AUSM+ field fluxes and zero patch-face
-// fluxes (the ghost layers of periodic axes overwrite the outer cells; closed
-// axes are walls with no flux).
-struct PeriodicFlux
+// Flux functor with one of the reference's Euler field fluxes and zero
+// patch-face fluxes (the ghost layers of periodic axes overwrite the outer
+// cells; closed axes are walls with no flux).
+template <class E>
+struct PeriodicFluxT
 {
-  RefAusm m_Ausm;
+  E m_Ausm;
   template <typename P> void xField(P* p, size_t i, size_t j, size_t k, real x, real y, real z, real A, real* f) { m_Ausm.xField(p, i, j, k, x, y, z, A, f); }
   template <typename P> void yField(P* p, size_t i, size_t j, size_t k, real x, real y, real z, real A, real* f) { m_Ausm.yField(p, i, j, k, x, y, z, A, f); }
   template <typename P> void zField(P* p, size_t i, size_t j, size_t k, real x, real y, real z, real A, real* f) { m_Ausm.zField(p, i, j, k, x, y, z, A, f); }
@@ -68,6 +74,7 @@ struct PeriodicFlux
   template <typename P> void zWallM(P*, size_t, size_t, size_t, real, real, real, real, real*) {}
   template <typename P> void zWallP(P*, size_t, size_t, size_t, real, real, real, real, real*) {}
 };
+typedef PeriodicFluxT<RefAusm> PeriodicFlux;
 
 // Patch-face fluxes per patch and side (x-min, x-max, y-min, y-max, z-min,
 // z-max): 0 none, 1 the reference's CompressibleFarfieldFlux, 2 its
@@ -89,9 +96,10 @@ struct GridBC
   std::vector<SideConfig> patches;
 };
 
-struct SideFlux
+template <class E>
+struct SideFluxT
 {
-  RefAusm m_Ausm;
+  E m_Ausm;
   RefSlip m_Slip;
   GridBC* m_BC = nullptr;
 
@@ -146,6 +154,7 @@ struct SideFlux
   DN_SIDE(zWallP, 5, 2, i, j, k - 1, i*p->sizeJ() + j)
 #undef DN_SIDE
 };
+typedef SideFluxT<RefAusm> SideFlux;
 
 // Periodic ghost copy, field 0, for the axes flagged periodic; each such axis
 // carries G ghost layers per side (ghosted size N = n + 2G).
@@ -215,9 +224,11 @@ extern "C" {
 // edge reconstruction, zero patch-face flux).  active may be NULL.
 // init/out: [5][ni][nj][nk] conservative variables (k fastest).
 // Returns 0 on success; *seconds = steady_clock time of the RK loop only.
-int dnref_run(int ni, int nj, int nk, const int* periodic, double hx, double hy, double hz,
-              const double* init, const unsigned char* active, int steps, double dt,
-              const double* alpha, int n_alpha, int threads, double* out, double* seconds)
+extern "C++" {
+template <class E>
+int run_impl(int ni, int nj, int nk, const int* periodic, double hx, double hy, double hz,
+             const double* init, const unsigned char* active, int steps, double dt,
+             const double* alpha, int n_alpha, int threads, double* out, double* seconds)
 {
   if (sizeof(real) != 8) return -1;
   if (ni < 1 || nj < 1 || nk < 1 || n_alpha < 1) return -2;
@@ -248,8 +259,8 @@ int dnref_run(int ni, int nj, int nk, const int* periodic, double hx, double hy,
   PeriodicGhostCopy ghosts(p, G);
   ghosts();
 
-  PeriodicFlux flux;
-  CartesianIterator<5, PeriodicFlux> iterator(flux);
+  PeriodicFluxT<E> flux;
+  CartesianIterator<5, PeriodicFluxT<E>> iterator(flux);
   iterator.addPatch(p);
   RungeKutta rk;
   for (int a = 0; a < n_alpha; ++a) rk.addAlpha(alpha[a]);
@@ -267,6 +278,37 @@ int dnref_run(int ni, int nj, int nk, const int* periodic, double hx, double hy,
         for (size_t k = 0; k < size_t(nk); ++k)
           out[v*n + (i*nj + j)*nk + k] = p->f(0, v, i + G[0], j + G[1], k + G[2]);
   return 0;
+}
+
+} // extern "C++"
+
+int dnref_run(int ni, int nj, int nk, const int* periodic, double hx, double hy, double hz,
+              const double* init, const unsigned char* active, int steps, double dt,
+              const double* alpha, int n_alpha, int threads, double* out, double* seconds)
+{
+  return run_impl<RefAusm>(ni, nj, nk, periodic, hx, hy, hz, init, active, steps, dt, alpha, n_alpha, threads,
+                           out, seconds);
+}
+
+// dnref_run with the Euler flux `scheme`: 0 AusmPlus, 2 VanLeer, 3 Roe (the
+// numbering of DN_FLUX_*; all with Upwind2<5, VanAlbada> and PerfectGas).
+int dnref_run_scheme(int scheme, int ni, int nj, int nk, const int* periodic, double hx, double hy, double hz,
+                     const double* init, const unsigned char* active, int steps, double dt,
+                     const double* alpha, int n_alpha, int threads, double* out, double* seconds)
+{
+  switch (scheme) {
+    case 0: case 1:
+      return run_impl<RefAusm>(ni, nj, nk, periodic, hx, hy, hz, init, active, steps, dt, alpha, n_alpha, threads,
+                               out, seconds);
+    case 2:
+      return run_impl<RefVanLeer>(ni, nj, nk, periodic, hx, hy, hz, init, active, steps, dt, alpha, n_alpha,
+                                  threads, out, seconds);
+    case 3:
+      return run_impl<RefRoe>(ni, nj, nk, periodic, hx, hy, hz, init, active, steps, dt, alpha, n_alpha, threads,
+                              out, seconds);
+    default:
+      return -3;
+  }
 }
 
 int dnref_real_size() { return int(sizeof(real)); }
@@ -527,14 +569,13 @@ int dnref_grid_copy_donor_data(void* handle, int field)
   return 0;
 }
 
-// `steps` RK steps of all patches; *seconds = time of RungeKutta::operator() only.
-int dnref_grid_run(void* handle, int steps, double dt, const double* alpha, int n_alpha, double* seconds)
+extern "C++" {
+template <class E>
+int grid_run_impl(DnRefGrid* g, int steps, double dt, const double* alpha, int n_alpha, double* seconds)
 {
-  DnRefGrid* g = (DnRefGrid*)handle;
-  if (!g || n_alpha < 1) return -1;
-  SideFlux flux;
+  SideFluxT<E> flux;
   flux.m_BC = &g->bc;
-  CartesianIterator<5, SideFlux> iterator(flux);
+  CartesianIterator<5, SideFluxT<E>> iterator(flux);
   for (size_t p = 0; p < g->patches.size(); ++p) iterator.addPatch(g->patches[p]);
   RungeKutta rk;
   for (int a = 0; a < n_alpha; ++a) rk.addAlpha(alpha[a]);
@@ -545,6 +586,28 @@ int dnref_grid_run(void* handle, int steps, double dt, const double* alpha, int 
   auto t1 = std::chrono::steady_clock::now();
   if (seconds) *seconds = std::chrono::duration<double>(t1 - t0).count();
   return 0;
+}
+} // extern "C++"
+
+// `steps` RK steps of all patches with the Euler flux `scheme` (as in
+// dnref_run_scheme); *seconds = time of RungeKutta::operator() only.
+int dnref_grid_run_scheme(void* handle, int scheme, int steps, double dt, const double* alpha, int n_alpha,
+                          double* seconds)
+{
+  DnRefGrid* g = (DnRefGrid*)handle;
+  if (!g || n_alpha < 1) return -1;
+  switch (scheme) {
+    case 0: case 1: return grid_run_impl<RefAusm>(g, steps, dt, alpha, n_alpha, seconds);
+    case 2: return grid_run_impl<RefVanLeer>(g, steps, dt, alpha, n_alpha, seconds);
+    case 3: return grid_run_impl<RefRoe>(g, steps, dt, alpha, n_alpha, seconds);
+    default: return -3;
+  }
+}
+
+// `steps` RK steps of all patches (AUSM+); *seconds = time of RungeKutta::operator() only.
+int dnref_grid_run(void* handle, int steps, double dt, const double* alpha, int n_alpha, double* seconds)
+{
+  return dnref_grid_run_scheme(handle, 0, steps, dt, alpha, n_alpha, seconds);
 }
 
 void dnref_grid_destroy(void* handle)

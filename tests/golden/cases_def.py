@@ -40,6 +40,12 @@ def build(name):
         U = cases.random_state(3, 5, 4, seed=6, amp=0.02, mach=0.3)
         h = 1.0 / 16
         return dict(U0=U, h=h, dt=cases.cfl_dt(U, h, 0.5), steps=2, periodic=(False, False, False), active=None)
+    if name == "transonic_10":
+        # Mach ~1 with strong perturbations: faces on both sides of |M| = 1
+        # (van Leer's supersonic branches, Roe's sonic entropy modification)
+        U = cases.random_state(10, 10, 10, seed=7, amp=0.08, mach=1.0)
+        h = 1.0 / 16
+        return dict(U0=U, h=h, dt=cases.cfl_dt(U, h, 0.4), steps=2, periodic=(True, True, True), active=None)
     if name == "cfg1_64_100":
         U, h, dt = cases.periodic_box(64)
         return dict(U0=U, h=h, dt=dt, steps=100, periodic=(True, True, True), active=None)
@@ -49,6 +55,11 @@ def build(name):
 # full-field fixtures (small); the 64^3 x 100 case stores a digest
 FULL = ["rough_8", "ragged_12x10x9", "vortex_16", "closed_10x7x12", "masked_9", "thin_3x5x4"]
 DIGEST = ["cfg1_64_100"]
+
+# Euler flux schemes of the generic functor path (numbered as DN_FLUX_*) and
+# the single-patch cases each is pinned on; the bc_box grid is pinned too
+SCHEMES = {"vanleer": 2, "roe": 3}
+SCHEME_CASES = ["vortex_16", "closed_10x7x12", "masked_9", "thin_3x5x4", "transonic_10"]
 
 
 # ------------------------------------------------------------------ patch grids

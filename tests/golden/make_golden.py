@@ -1,6 +1,8 @@
 """Generates the golden fixtures of tests/golden/ from the reference itself.
 
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py              # single-patch fixtures + grids
+    python tests/golden/make_golden.py --grids      # grids only
+    python tests/golden/make_golden.py --schemes    # VanLeer / Roe fixtures
 
 Needs oracle/_ref/libdrnum_ref.so, i.e. the reference DrNUM library compiled
 (FP64) from its own sources by oracle/build_ref.sh.  Each fixture stores the
@@ -97,8 +99,41 @@ def make_grids():
         print(f"grid_{name}: {len(patches)} patches")
 
 
+def make_schemes():
+    """The reference's CartesianIterator with its VanLeer and Roe functors
+    (Upwind2<VanAlbada>, PerfectGas) on the single-patch cases, and on the
+    bc_box grid with every patch-face kind."""
+    for sname, scheme in cases_def.SCHEMES.items():
+        for name in cases_def.SCHEME_CASES:
+            c = cases_def.build(name)
+            out, sec = pyoracle.ref_run(c["U0"], c["h"], c["dt"], c["steps"], cases_def.ALPHA,
+                                        c["periodic"], c["active"], threads=1, scheme=scheme)
+            np.savez_compressed(os.path.join(HERE, f"scheme_{sname}_{name}.npz"), U0=c["U0"], out=out, h=c["h"],
+                                dt=c["dt"], steps=c["steps"], periodic=np.array(c["periodic"], dtype=np.int8),
+                                active=c["active"] if c["active"] is not None else np.ones(0, np.uint8),
+                                alpha=np.array(cases_def.ALPHA), scheme=np.array(scheme))
+            print(f"scheme_{sname}_{name}: {sec:.3f} s")
+        gname = "bc_box"
+        patches, states, _, dt, steps = cases_def.grid_case(gname)
+        g = pyoracle.RefGrid(patches, 0, threads=1)
+        for p, sides in (cases_def.grid_bcs(gname) or {}).items():
+            for side, (kind, params, table) in sides.items():
+                g.set_bc(p, side, kind, params, table)
+        for p, U in enumerate(states):
+            g.set_state(p, U)
+        g.run(steps, dt, cases_def.ALPHA, scheme=scheme)
+        arrays = {f"p{p}_out": g.get_state(p) for p in range(len(patches))}
+        g.close()
+        arrays.update(dt=np.array(dt), steps=np.array(steps), scheme=np.array(scheme),
+                      num_patches=np.array(len(patches)))
+        np.savez_compressed(os.path.join(HERE, f"grid_{gname}_{sname}.npz"), **arrays)
+        print(f"grid_{gname}_{sname}")
+
+
 if __name__ == "__main__":
     if "--grids" in sys.argv:
         make_grids()
+    elif "--schemes" in sys.argv:
+        make_schemes()
     else:
         main()

@@ -26,7 +26,7 @@ def _fixture(golden_dir, name):
     return np.load(os.path.join(golden_dir, f"grid_{name}.npz"))
 
 
-def make_grid(name, precision, states=None):
+def make_grid(name, precision, states=None, op=None):
     patches, st0, spacings, dt, steps = cases_def.grid_case(name)
     states = st0 if states is None else states
     grid = PatchGrid()
@@ -44,7 +44,7 @@ def make_grid(name, precision, states=None):
         grid.insertPatch(cp)
         objs.append(cp)
     grid.computeDependencies()
-    it = B200CartesianIterator(AusmPlus(), 0, precision)
+    it = B200CartesianIterator(op if op is not None else AusmPlus(), 0, precision)
     for cp in objs:
         it.addPatch(cp)
     it.updateDevice(fields=(0,))
