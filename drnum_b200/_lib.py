@@ -118,6 +118,13 @@ SIGNATURES = {
     "dn_lslayers_destroy": (c_int, [c_void_p]),
     "dn_set_option": (c_int, [c_void_p, c_int, c_int]),
     "dn_set_flux_scheme": (c_int, [c_void_p, c_int]),
+    "dn_grid_read": (c_int, [ctypes.c_char_p, c_double, POINTER(c_void_p)]),
+    "dn_gridfile_count": (c_int, [c_void_p, POINTER(c_int)]),
+    "dn_gridfile_patch": (c_int, [c_void_p, c_int, POINTER(dn_patch_desc), ctypes.c_char_p, c_size_t]),
+    "dn_gridfile_destroy": (c_int, [c_void_p]),
+    "dn_grid_write": (c_int, [ctypes.c_char_p, c_int, POINTER(dn_patch_desc), POINTER(ctypes.c_char_p)]),
+    "dn_write_data": (c_int, [c_void_p, c_int, ctypes.c_char_p, c_double, c_int]),
+    "dn_read_data": (c_int, [c_void_p, c_int, ctypes.c_char_p, POINTER(c_double)]),
     "dn_set_stage_function": (c_int, [c_void_p, c_void_p, c_void_p]),
     "dn_patch_set_tile": (c_int, [c_void_p, c_int, c_int]),
     "dn_autotune": (c_int, [c_void_p, ctypes.c_char_p, POINTER(c_double)]),

@@ -218,6 +218,40 @@ class PatchGrid:
     def getNumPatches(self):
         return len(self.m_Patches)
 
+    def readGrid(self, gridfilename, scale=1.0):
+        """PatchGrid::readGrid (patchgrid.cpp:479-557) through dn_grid_read:
+        inserts a closed CartesianPatch per type-1001 block of the file, with
+        its seek-layer counts; returns the patches' solver-code strings."""
+        lib = _lib.load()
+        h = ctypes.c_void_p()
+        check(None, lib.dn_grid_read(str(gridfilename).encode(), float(scale), ctypes.byref(h)))
+        codes = []
+        try:
+            n = ctypes.c_int()
+            check(None, lib.dn_gridfile_count(h, ctypes.byref(n)))
+            for i in range(n.value):
+                d = _lib.dn_patch_desc()
+                buf = ctypes.create_string_buffer(4096)
+                check(None, lib.dn_gridfile_patch(h, i, ctypes.byref(d), buf, len(buf)))
+                patch = CartesianPatch(d.ni, d.nj, d.nk, lengths=tuple(d.length), spacing=(d.dx, d.dy, d.dz),
+                                       origin=tuple(d.origin), periodic=(False, False, False),
+                                       seek=tuple(d.seek))
+                self.insertPatch(patch)
+                codes.append(buf.value.decode())
+        finally:
+            lib.dn_gridfile_destroy(h)
+        return codes
+
+    def writeGrid(self, gridfilename, codes=None):
+        """Writes the patches as a grid file (dn_grid_write; the layout of the
+        reference's grid generator, Python/drnum.py:199-244)."""
+        lib = _lib.load()
+        arr = (_lib.dn_patch_desc * len(self.m_Patches))(*[p.desc() for p in self.m_Patches])
+        cs = None
+        if codes is not None:
+            cs = (ctypes.c_char_p * len(codes))(*[c.encode() for c in codes])
+        check(None, lib.dn_grid_write(str(gridfilename).encode(), len(self.m_Patches), arr, cs))
+
     def getPatch(self, i):
         return self.m_Patches[i]
 
@@ -415,6 +449,20 @@ class B200CartesianIterator:
         """dn_set_option: DN_OPT_BATCHED (one launch per stage over all
         patches) or DN_OPT_GRAPH (CUDA-graph replay of whole steps)."""
         check(self.ctx, self.lib.dn_set_option(self.ctx, int(option), int(value)))
+
+    def writeData(self, i_field, base_file_name, time, count):
+        """PatchGrid::writeData (patchgrid.cpp:559-578) of this iterator's
+        patches: <base>_<count:06d>.dnd (dn_write_data); returns the name."""
+        check(self.ctx, self.lib.dn_write_data(self.ctx, int(i_field), str(base_file_name).encode(), float(time),
+                                               int(count)))
+        return f"{base_file_name}_{int(count):06d}.dnd"
+
+    def readData(self, i_field, file_name):
+        """PatchGrid::readData (patchgrid.cpp:580-611) into this iterator's
+        patches (dn_read_data); returns the stored time."""
+        t = ctypes.c_double()
+        check(self.ctx, self.lib.dn_read_data(self.ctx, int(i_field), str(file_name).encode(), ctypes.byref(t)))
+        return t.value
 
     def setFluxScheme(self, op):
         """Selects the Euler flux functor (AusmPlus, VanLeer, Roe) of an FP64

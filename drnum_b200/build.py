@@ -40,6 +40,7 @@ UNITS = {
     "dn_levelset.cpp": ["-Xcompiler", "-ffp-contract=off"],
     "dn_lsbc.cu": ["-fmad=false"],
     "fv_schemes.cu": ["-fmad=false"],
+    "dn_gridio.cpp": [],
 }
 
 

@@ -17,6 +17,7 @@
 #include "dn_lsbc.cuh"
 #include "fv_batch.cuh"
 #include "fv_schemes.cuh"
+#include "dn_gridio.h"
 
 #include <cmath>
 #include <cstdarg>
@@ -1506,6 +1507,55 @@ int dn_set_option(dn_ctx* c, int option, int value)
     return DN_OK;
   }
   return fail(c, DN_ERR_ARG, "unknown option %d", option);
+}
+
+int dn_write_data(dn_ctx* c, int field, const char* base, double time, int count)
+{
+  if (!c) return DN_ERR_ARG;
+  if (!base) return fail(c, DN_ERR_ARG, "base file name is NULL");
+  int s;
+  if ((s = check_field(c, field))) return s;
+  std::string bytes;
+  dn::dnd_header(bytes, 8, time);
+  std::vector<double> h;
+  for (size_t q = 0; q < c->patches.size(); ++q) {
+    h.resize(5 * c->patches[q].nc);
+    if ((s = download_impl(c, (int)q, field, h.data()))) return s;
+    dn::dnd_values(bytes, 8, h.data(), h.size());
+  }
+  const std::string name = dn::dnd_file_name(base, count);
+  if (!dn::dnd_write_file(name, bytes)) return fail(c, DN_ERR_ARG, "cannot write %s", name.c_str());
+  return DN_OK;
+}
+
+int dn_read_data(dn_ctx* c, int field, const char* file_name, double* time)
+{
+  if (!c) return DN_ERR_ARG;
+  if (!file_name) return fail(c, DN_ERR_ARG, "file name is NULL");
+  int s;
+  if ((s = check_field(c, field))) return s;
+  std::string name(file_name);
+  if (name.size() < 4 || name.compare(name.size() - 4, 4, ".dnd") != 0) name += ".dnd";
+  std::string bytes;
+  if (!dn::dnd_read_file(name, bytes)) return fail(c, DN_ERR_ARG, "cannot read %s", name.c_str());
+  int prec;
+  double t;
+  size_t off;
+  if (!dn::dnd_parse_header(bytes, &prec, &t, &off)) return fail(c, DN_ERR_ARG, "%s: truncated header", name.c_str());
+  size_t total = 0;
+  for (auto& p : c->patches) total += 5 * p.nc;
+  if (bytes.size() != off + total * (size_t)prec)
+    return fail(c, DN_ERR_ARG, "%s holds %zu bytes of values, the context's patches need %zu", name.c_str(),
+                bytes.size() - off, total * (size_t)prec);
+  std::vector<double> h;
+  for (size_t q = 0; q < c->patches.size(); ++q) {
+    h.resize(5 * c->patches[q].nc);
+    dn::dnd_get_values(bytes, off, prec, h.data(), h.size());
+    off += h.size() * (size_t)prec;
+    if ((s = upload_impl(c, (int)q, field, h.data()))) return s;
+  }
+  if (time) *time = t;
+  return DN_OK;
 }
 
 int dn_set_flux_scheme(dn_ctx* c, int scheme)

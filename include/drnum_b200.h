@@ -332,6 +332,36 @@ typedef int (*dn_stage_fn)(void* user, const dn_stage_launch* L);
  * FP32 context. */
 int dn_set_stage_function(dn_ctx* ctx, dn_stage_fn fn, void* user);
 
+/* Patch-grid files.  dn_grid_read parses a grid file as PatchGrid::readGrid
+ * (patchgrid.cpp:479-557, CartesianPatch::readFromFile, cartesianpatch.cpp:
+ * 98-133): blocks "<type> <comment> { ... }" up to type 0; type 1001 holds
+ * the reference point, base vectors i and j, IO scale, Ni Nj Nk, the six
+ * seek-layer counts, the lengths and solver codes.  Reference point and
+ * lengths are scaled by IO scale * `scale`.  Patches come back as
+ * descriptors (closed faces, seek counts in seek[6]) and their solver-code
+ * string (normalised as CodeString::buildFrom, codestring.cpp:43-100).
+ * Axis-aligned patches only: other base vectors, unknown block types or a
+ * malformed block give DN_ERR_ARG.  dn_grid_write writes descriptors in the
+ * layout of the reference's grid generator (Python/drnum.py:199-244);
+ * codes may be NULL. */
+typedef struct dn_gridfile dn_gridfile;
+int dn_grid_read(const char* path, double scale, dn_gridfile** out);
+int dn_gridfile_count(const dn_gridfile* g, int* n);
+int dn_gridfile_patch(const dn_gridfile* g, int index, dn_patch_desc* desc, char* codes, size_t n_codes);
+int dn_gridfile_destroy(dn_gridfile* g);
+int dn_grid_write(const char* path, int n, const dn_patch_desc* patches, const char* const* codes);
+
+/* Restart files.  dn_write_data writes field `field` of every patch of the
+ * context to <base>_<count, 6 digits>.dnd as PatchGrid::writeData
+ * (patchgrid.cpp:559-578): Qt QDataStream big-endian int32 precision (8),
+ * the time as a double, then each patch's [5][ni][nj][nk] values, patches
+ * in context order.  dn_read_data reads such a file (".dnd" is appended if
+ * missing; precision 4 files are read too) into field `field` and returns
+ * its time, as PatchGrid::readData (patchgrid.cpp:580-611); a file whose
+ * size does not match the context's patches gives DN_ERR_ARG. */
+int dn_write_data(dn_ctx* ctx, int field, const char* base_file_name, double time, int count);
+int dn_read_data(dn_ctx* ctx, int field, const char* file_name, double* time);
+
 /* Number of device kernel launches the context has issued so far. */
 int dn_launch_count(const dn_ctx* ctx, int64_t* count);
 

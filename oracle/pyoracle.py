@@ -204,8 +204,16 @@ class RefGrid:
     reference library): donor tables from PatchGrid::computeDependencies and
     RK steps with Patch::accessDonorDataDirect after every stage."""
 
-    def __init__(self, patches, add_protect=0, threads=1, num_vars=5):
+    def __init__(self, patches, add_protect=0, threads=1, num_vars=5, grid_file=None, scale=1.0):
+        """patches: layout dicts; or grid_file (a path relative to the
+        working directory) read by the reference's PatchGrid::readGrid."""
         lib = ref_lib()
+        lib.dnref_grid_read.restype = c_void_p
+        lib.dnref_grid_read.argtypes = [ctypes.c_char_p, c_double, c_int, c_int]
+        lib.dnref_grid_num_patches.restype = c_int
+        lib.dnref_grid_num_patches.argtypes = [c_void_p]
+        lib.dnref_grid_patch_info.restype = c_int
+        lib.dnref_grid_patch_info.argtypes = [c_void_p, c_int, c_void_p, _P, _P, ctypes.c_char_p, c_int]
         lib.dnref_grid_create_nv.restype = c_void_p
         lib.dnref_grid_create_nv.argtypes = [c_int, POINTER(c_int), _P, _P, POINTER(c_int), c_int, c_int, c_int]
         lib.dnref_grid_levelset.restype = c_int
@@ -227,12 +235,31 @@ class RefGrid:
         lib.dnref_grid_destroy.argtypes = [c_void_p]
         self.lib = lib
         self.patches = patches
+        if grid_file is not None:
+            self.h = lib.dnref_grid_read(str(grid_file).encode(), float(scale), int(add_protect), int(threads))
+            if not self.h:
+                raise RuntimeError("reference grid read failed")
+            return
         n, o, L, s = _grid_arrays(patches)
         self.h = lib.dnref_grid_create_nv(len(patches), n.ctypes.data_as(POINTER(c_int)), o.ctypes.data_as(_P),
                                           L.ctypes.data_as(_P), s.ctypes.data_as(POINTER(c_int)),
                                           int(add_protect), int(threads), int(num_vars))
         if not self.h:
             raise RuntimeError("reference grid creation failed")
+
+    def num_patches(self):
+        return self.lib.dnref_grid_num_patches(self.h)
+
+    def patch_info(self, p):
+        """(cells, reference point, spacing, solver-code string) of patch p."""
+        n = np.zeros(3, np.int64)
+        o = np.zeros(3)
+        d = np.zeros(3)
+        buf = ctypes.create_string_buffer(4096)
+        if self.lib.dnref_grid_patch_info(self.h, p, n.ctypes.data, o.ctypes.data_as(_P), d.ctypes.data_as(_P),
+                                          buf, len(buf)) != 0:
+            raise RuntimeError("patch_info failed")
+        return n, o, d, buf.value.decode()
 
     def tables(self, p):
         counts = np.zeros(4, dtype=np.int64)

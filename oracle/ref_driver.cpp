@@ -438,6 +438,52 @@ void* dnref_grid_create_nv(int np, const int* n, const double* origin, const dou
   return g;
 }
 
+// A grid read from a grid file by the reference's PatchGrid::readGrid
+// (patchgrid.cpp:479-557; `relpath` is relative to the working directory, as
+// readGrid takes it), set up like dnref_grid_create and with its
+// dependencies computed.
+void* dnref_grid_read(const char* relpath, double scale, int add_protect, int threads)
+{
+  if (sizeof(real) != 8 || !relpath) return nullptr;
+#ifdef OPEN_MP
+  if (threads > 0) omp_set_num_threads(threads);
+#endif
+  DnRefGrid* g = new DnRefGrid();
+  g->grid.setNumberOfFields(3);
+  g->grid.setNumberOfVariables(5);
+  g->grid.defineVectorVar(1);
+  g->grid.setInterpolateData();
+  g->grid.setNumSeekLayers(2);
+  g->grid.setNumAddProtectLayers(size_t(add_protect));
+  g->grid.setTransferType("padded_direct");
+  g->grid.readGrid(relpath, scale);
+  for (size_t p = 0; p < g->grid.getNumPatches(); ++p)
+    g->patches.push_back(dynamic_cast<CartesianPatch*>(g->grid.getPatch(p)));
+  g->grid.computeDependencies(true);
+  g->bc.patches.resize(g->patches.size());
+  return g;
+}
+
+int dnref_grid_num_patches(void* handle)
+{
+  DnRefGrid* g = (DnRefGrid*)handle;
+  return g ? int(g->patches.size()) : -1;
+}
+
+// Cells, reference point, spacing and solver-code string of patch p.
+int dnref_grid_patch_info(void* handle, int p, long long* n, double* origin, double* delta, char* codes, int len)
+{
+  DnRefGrid* g = (DnRefGrid*)handle;
+  if (!g || p < 0 || p >= int(g->patches.size())) return -1;
+  CartesianPatch* P = g->patches[p];
+  n[0] = (long long)P->sizeI(); n[1] = (long long)P->sizeJ(); n[2] = (long long)P->sizeK();
+  origin[0] = P->xo(); origin[1] = P->yo(); origin[2] = P->zo();
+  delta[0] = P->dx(); delta[1] = P->dy(); delta[2] = P->dz();
+  std::string c = P->accessSolverCodes();
+  if (codes && len > 0) std::snprintf(codes, size_t(len), "%s", c.c_str());
+  return 0;
+}
+
 // Patch-face flux of side `side` of patch p: kind 0 none, 1 far field
 // (params p, T, u, v, w), 2 slip wall, 3 face table ([faces][5] p or NaN, T,
 // u, v, w; x sides j*nk+k, y sides i*nk+k, z sides i*nj+j).
