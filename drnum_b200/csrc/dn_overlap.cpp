@@ -4,7 +4,10 @@
 #include "dn_overlap.h"
 
 #include <algorithm>
+#include <atomic>
 #include <cstdio>
+#include <cstdlib>
+#include <thread>
 #include <utility>
 
 namespace dn {
@@ -168,6 +171,10 @@ struct Entry {
   std::vector<Contrib> ws;
 };
 
+size_t setup_threads();
+bool receiver_tables(size_t r, const std::vector<OverlapPatch>& patches, const std::vector<Zone>& zones,
+                     DonorTables& t, std::string& err);
+
 } // namespace
 
 int cc_interpolation_weights(const OverlapPatch& p, const double xyz[3], std::vector<std::pair<size_t, double>>& ws,
@@ -193,8 +200,50 @@ bool build_overlap(const std::vector<OverlapPatch>& patches, std::vector<DonorTa
     zones[p] = make_zone(q);
   }
   out.assign(np, DonorTables());
-
+  // receiving patches are independent: spread them over the host threads
+  // (the tables of each are computed by the same code, so the result does
+  // not depend on the thread count)
+  std::vector<std::string> errs(np);
+  std::atomic<size_t> next{0};
+  std::atomic<bool> failed{false};
+  auto worker = [&]() {
+    for (size_t r; !failed.load() && (r = next.fetch_add(1)) < np;) {
+      if (!receiver_tables(r, patches, zones, out[r], errs[r])) failed.store(true);
+    }
+  };
+  const size_t nt = std::min(np, setup_threads());
+  std::vector<std::thread> pool;
+  for (size_t t = 1; t < nt; ++t) pool.emplace_back(worker);
+  worker();
+  for (std::thread& t : pool) t.join();
   for (size_t r = 0; r < np; ++r) {
+    if (!errs[r].empty()) {
+      err = errs[r];
+      return false;
+    }
+  }
+  return true;
+}
+
+namespace {
+
+// host threads of the set-up: DN_SETUP_THREADS if set, else all cores
+size_t setup_threads()
+{
+  if (const char* e = std::getenv("DN_SETUP_THREADS")) {
+    const long v = std::strtol(e, nullptr, 10);
+    if (v >= 1) return (size_t)v;
+  }
+  const unsigned hc = std::thread::hardware_concurrency();
+  return hc ? (size_t)hc : 1;
+}
+
+// Donor tables of receiving patch r against every other patch.
+bool receiver_tables(size_t r, const std::vector<OverlapPatch>& patches, const std::vector<Zone>& zones,
+                     DonorTables& t, std::string& err)
+{
+  const size_t np = patches.size();
+  {
     const OverlapPatch& R = patches[r];
     const Zone& zr = zones[r];
     const size_t ni = (size_t)R.n[0], nj = (size_t)R.n[1], nk = (size_t)R.n[2];
@@ -245,7 +294,6 @@ bool build_overlap(const std::vector<OverlapPatch>& patches, std::vector<DonorTa
       }
     }
 
-    DonorTables& t = out[r];
     for (size_t ll = 0; ll < rec.size(); ++ll) {
       if (hits[ll] > 0) t.rec_unique.push_back(rec[ll]);
       else t.no_donor++;
@@ -279,6 +327,8 @@ bool build_overlap(const std::vector<OverlapPatch>& patches, std::vector<DonorTa
   }
   return true;
 }
+
+} // namespace
 
 void desc_spacing(const dn_patch_desc& d, double out[3])
 {

@@ -211,3 +211,17 @@ def _ls_tables(z, name, num_patches):
             continue
         out.append([{k: z[f"p{p}_ls{layer}_{k}"] for k in LS_KEYS} for layer in range(cases_def.LS_INNER)])
     return out
+
+
+def test_overlap_setup_result_independent_of_thread_count(monkeypatch):
+    # receiving patches are spread over host threads; the tables must not
+    # depend on how many
+    patches = cases.tiled_grid(slots=(3, 3, 2), seed=5)
+    monkeypatch.setenv("DN_SETUP_THREADS", "1")
+    one, nd1 = build_tables(patches)
+    monkeypatch.setenv("DN_SETUP_THREADS", "5")
+    many, nd5 = build_tables(patches)
+    assert nd1 == nd5 == 0
+    for a, b in zip(one, many):
+        for k in TABLE_KEYS:
+            assert _same(a[k], b[k]), k
