@@ -326,7 +326,7 @@ def run_ours(args, rank, world, local_rank):
                                        "energy": drift[4], "steps": args.warmup + args.steps},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
-                         "kernel": "fx_stage_kernel<8,32> (FP32 arithmetic, int32 fixed-point storage)",
+                         "kernel": "fx_stage_kernel<16,16> (FP32 arithmetic, int32 fixed-point storage)",
                          "algorithmic_bytes_per_launch": bytes_per_launch,
                          "avg_launch_ms": launch_s * 1e3},
             "cpu_baseline": cpu,

@@ -272,25 +272,24 @@ __device__ __forceinline__ float2 fx_slope2(float2 a, float2 b)
   return make_float2(den.x > 1e-30f ? q.x : 0.0f, den.y > 1e-30f ? q.y : 0.0f);
 }
 
-__device__ __forceinline__ int fx_wrap(int x, int n, int per)
+// Cell whose state stands at index x of an axis: the wrapped cell on a
+// periodic axis, the nearest edge cell outside a closed one.  Copying the
+// edge cell outward makes the van Albada slope of an edge cell exactly zero
+// (one of its differences vanishes), which is the reference's first-order
+// reconstruction at a closed patch edge (upwind2.h:39-42), with no test.
+__device__ __forceinline__ int fx_index(int x, int n, int per)
 {
   if (per) {
-    if (x < 0) x += n;
-    else if (x >= n) x -= n;
-    return (x >= 0 && x < n) ? x : -1;   // n >= 3 and |shift| <= 2 keep one fold enough
+    x %= n;
+    return x < 0 ? x + n : x;
   }
-  return (x < 0 || x >= n) ? -1 : x;
+  return x < 0 ? 0 : (x >= n ? n - 1 : x);
 }
 
 __device__ __forceinline__ bool fx_face_exists(int x, int n, int per)
 {
   if (n <= 2) return false;
   return per ? true : (x >= 1 && x <= n - 1);
-}
-
-__device__ __forceinline__ bool fx_cell_ok(int x, int n, int per)
-{
-  return per ? true : (x >= 0 && x < n);
 }
 
 // Shared memory of a CTA.  Every array starts on a 128-byte boundary and is
@@ -325,13 +324,6 @@ __device__ __forceinline__ void fx_cp_async4(void* smem, const void* gmem)
 {
   const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
   asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" :: "r"(s), "l"(gmem) : "memory");
-}
-
-// 4-byte asynchronous copy that writes zero instead when ok is false
-__device__ __forceinline__ void fx_cp_async4_or_zero(void* smem, const void* gmem, bool ok)
-{
-  const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;" :: "r"(s), "l"(gmem), "r"(ok ? 4 : 0) : "memory");
 }
 
 __device__ __forceinline__ void fx_cp_async_commit()
@@ -391,27 +383,21 @@ __device__ __forceinline__ void fx_stage_tile_impl(const FxArgs& a, int j0, int 
     if (e < NP) {
       const int jj = (e / (2 * PK)) * 2 + (e & 1);
       const int kk = (e % (2 * PK)) >> 1;
-      const int jw = fx_wrap(j0 - 2 + jj, g.nj, g.per_y);
-      const int kw = fx_wrap(k0 - 2 + kk, g.nk, g.per_z);
-      if (jw >= 0 && kw >= 0) poff[m] = jw * g.nk + kw;
+      poff[m] = fx_index(j0 - 2 + jj, g.nj, g.per_y) * g.nk + fx_index(k0 - 2 + kk, g.nk, g.per_z);
     }
   }
 
-  // plane ip of the stage input: copied asynchronously as int32 into its
-  // ring slot (zero outside a closed patch) ...
+  // plane ip of the stage input (edge cells copied outward on closed axes):
+  // copied asynchronously as int32 into its ring slot ...
   auto issue = [&](int ip) {
-    const int iw = fx_wrap(ip, g.ni, g.per_x);
     int* dst = reinterpret_cast<int*>(&sm.plane[ip & 3][0][0][0][0]);
-    const int32_t* src = a.in + (size_t)(iw < 0 ? 0 : iw) * njk;
+    const int32_t* src = a.in + (size_t)fx_index(ip, g.ni, g.per_x) * njk;
     #pragma unroll
     for (int v = 0; v < 5; ++v) {
       #pragma unroll
       for (int m = 0; m < PPT; ++m) {
         const int e = tid + m * NT;
-        if (e < NP) {
-          const bool ok = iw >= 0 && poff[m] >= 0;
-          fx_cp_async4_or_zero(dst + v * NP + e, src + (size_t)v * nc + (ok ? poff[m] : 0), ok);
-        }
+        if (e < NP) fx_cp_async4(dst + v * NP + e, src + (size_t)v * nc + poff[m]);
       }
     }
     fx_cp_async_commit();
@@ -458,14 +444,13 @@ __device__ __forceinline__ void fx_stage_tile_impl(const FxArgs& a, int j0, int 
     // slope of cell i0 (needs i0-1, i0, i0+1) and the face below i0
     const int s_m1 = (i0 + 3) & 3, s_0 = i0 & 3, s_p1 = (i0 + 1) & 3;
     float Ul[5], Sp[5], Sm[5];
-    const bool sx = own && fx_cell_ok(i0 - 1, g.ni, g.per_x) && fx_cell_ok(i0 + 1, g.ni, g.per_x);
     float U0[5];
     #pragma unroll
     for (int v = 0; v < 5; ++v) {
       const float um = PL(s_m1, v, ty + 2, tx + 2);
       const float uc = PL(s_0, v, ty + 2, tx + 2);
       const float up = PL(s_p1, v, ty + 2, tx + 2);
-      const float s = sx ? fx_slope(uc - um, up - uc) : 0.0f;
+      const float s = fx_slope(uc - um, up - uc);
       U0[v] = uc;
       Sp[v] = uc + s;
       Sm[v] = uc - s;
@@ -476,15 +461,12 @@ __device__ __forceinline__ void fx_stage_tile_impl(const FxArgs& a, int j0, int 
     // face below i0: left state from cell i0-1 (slope needs i0-2)
     const bool ex = own && fx_face_exists(i0, g.ni, g.per_x);
     if (ex) {
-      const int iw2 = fx_wrap(i0 - 2, g.ni, g.per_x);
-      const bool sl = fx_cell_ok(i0 - 2, g.ni, g.per_x);
+      const int iw2 = fx_index(i0 - 2, g.ni, g.per_x);
       float Lm[5];
       #pragma unroll
       for (int v = 0; v < 5; ++v) {
-        float umm = Ul[v];
-        if (sl) umm = fmaf(P.quantum[v], (float)__ldg(a.in + (int64_t)v * nc + (int64_t)iw2 * njk + (int64_t)j * g.nk + k), P.base[v]);
-        const float s = sl ? fx_slope(Ul[v] - umm, U0[v] - Ul[v]) : 0.0f;
-        Lm[v] = Ul[v] + s;
+        const float umm = fmaf(P.quantum[v], (float)__ldg(a.in + (int64_t)v * nc + (int64_t)iw2 * njk + (int64_t)j * g.nk + k), P.base[v]);
+        Lm[v] = Ul[v] + fx_slope(Ul[v] - umm, U0[v] - Ul[v]);
       }
       float F[5];
       fx_ausm<0>(fx_prim(Lm[0], Lm[1], Lm[2], Lm[3], Lm[4]), fx_prim(Sm[0], Sm[1], Sm[2], Sm[3], Sm[4]), P.Ax, F);
@@ -502,15 +484,12 @@ __device__ __forceinline__ void fx_stage_tile_impl(const FxArgs& a, int j0, int 
     // ---------------- y and z face states of plane i
     float2 yzm[5];   // right states of the y (lane x) and z (lane y) faces below the own cell
     {
-      const bool sy = FULL || (fx_cell_ok(j - 1, g.nj, g.per_y) && fx_cell_ok(j + 1, g.nj, g.per_y));
-      const bool sz = FULL || (fx_cell_ok(k - 1, g.nk, g.per_z) && fx_cell_ok(k + 1, g.nk, g.per_z));
       #pragma unroll
       for (int v = 0; v < 5; ++v) {
         const float2 uc = v2(PL(s0, v, ty + 2, tx + 2));
         const float2 ul = make_float2(PL(s0, v, ty + 1, tx + 2), PL(s0, v, ty + 2, tx + 1));
         const float2 uh = make_float2(PL(s0, v, ty + 3, tx + 2), PL(s0, v, ty + 2, tx + 3));
-        float2 s = fx_slope2(sub2(uc, ul), sub2(uh, uc));
-        if (!FULL) s = make_float2(sy ? s.x : 0.0f, sz ? s.y : 0.0f);
+        const float2 s = fx_slope2(sub2(uc, ul), sub2(uh, uc));
         const float2 up = add2(uc, s);
         sm.sy[v][ty + 1][tx] = up.x;
         sm.szL[v][ty][tx] = up.y;
@@ -527,15 +506,6 @@ __device__ __forceinline__ void fx_stage_tile_impl(const FxArgs& a, int j0, int 
       const int jjz = h % TJ;
       const bool topz = h >= TJ;
       const int kkz = topz ? TK : -1;                 // tile-relative col of the z cell
-      bool oky = hy, okz = hz;
-      if (!FULL) {
-        const int jc = j0 + jjy, kc = k0 + kky;
-        oky = oky && fx_cell_ok(jc - 1, g.nj, g.per_y) && fx_cell_ok(jc + 1, g.nj, g.per_y) &&
-              fx_cell_ok(jc, g.nj, g.per_y) && kc < g.nk;
-        const int jz = j0 + jjz, kz = k0 + kkz;
-        okz = okz && fx_cell_ok(kz - 1, g.nk, g.per_z) && fx_cell_ok(kz + 1, g.nk, g.per_z) &&
-              fx_cell_ok(kz, g.nk, g.per_z) && jz < g.nj;
-      }
       // a lane without a cell evaluates the other lane's cell and stores nothing
       const int ry = hy ? jjy + 2 : jjz + 2, cy = hy ? kky + 2 : kkz + 2;
       const int rz = hz ? jjz + 2 : jjy + 2, cz = hz ? kkz + 2 : kky + 2;
@@ -544,8 +514,7 @@ __device__ __forceinline__ void fx_stage_tile_impl(const FxArgs& a, int j0, int 
         const float2 uc = make_float2(PL(s0, v, ry, cy), PL(s0, v, rz, cz));
         const float2 ul = make_float2(PL(s0, v, ry - 1, cy), PL(s0, v, rz, cz - 1));
         const float2 uh = make_float2(PL(s0, v, ry + 1, cy), PL(s0, v, rz, cz + 1));
-        float2 s = fx_slope2(sub2(uc, ul), sub2(uh, uc));
-        s = make_float2(FULL || oky ? s.x : 0.0f, FULL || okz ? s.y : 0.0f);
+        const float2 s = fx_slope2(sub2(uc, ul), sub2(uh, uc));
         const float2 up = add2(uc, s), dn = sub2(uc, s);
         if (hy) {
           if (topy) sm.sy_top[v][kky] = dn.x;
@@ -617,14 +586,13 @@ __device__ __forceinline__ void fx_stage_tile_impl(const FxArgs& a, int j0, int 
     int qx_hi[5];
     {
       const bool ex = own && fx_face_exists(i + 1, g.ni, g.per_x);
-      const bool sx = fx_cell_ok(i + 2, g.ni, g.per_x);   // slope of cell i+1 needs i+2 (i is in range)
       float Sm[5], Sp[5];
       #pragma unroll
       for (int v = 0; v < 5; ++v) {
         const float uc = PL(sp1, v, ty + 2, tx + 2);
         const float up = PL(sp2, v, ty + 2, tx + 2);
         const float b = up - uc;
-        const float s = sx ? fx_slope(xb[v], b) : 0.0f;
+        const float s = fx_slope(xb[v], b);
         Sm[v] = uc - s;
         Sp[v] = uc + s;
         xb[v] = b;
