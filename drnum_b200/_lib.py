@@ -124,6 +124,14 @@ SIGNATURES = {
     "dn_gridfile_destroy": (c_int, [c_void_p]),
     "dn_grid_write": (c_int, [ctypes.c_char_p, c_int, POINTER(dn_patch_desc), POINTER(ctypes.c_char_p)]),
     "dn_write_data": (c_int, [c_void_p, c_int, ctypes.c_char_p, c_double, c_int]),
+    "dn_patch_set_owned": (c_int, [c_void_p, c_int, c_int]),
+    "dn_exchange_build": (c_int, [c_void_p, POINTER(c_int32), c_int, c_int, POINTER(c_void_p)]),
+    "dn_exchange_build_ctx": (c_int, [c_void_p, POINTER(c_int32), c_int, c_int, POINTER(c_void_p)]),
+    "dn_exchange_counts": (c_int, [c_void_p, c_int, POINTER(c_int64), POINTER(c_int64)]),
+    "dn_exchange_get": (c_int, [c_void_p, c_int, c_void_p, c_void_p, c_void_p, c_void_p]),
+    "dn_exchange_pack": (c_int, [c_void_p, c_void_p, c_int, c_int, c_void_p]),
+    "dn_exchange_unpack": (c_int, [c_void_p, c_void_p, c_int, c_int, c_void_p]),
+    "dn_exchange_destroy": (c_int, [c_void_p]),
     "dn_read_data": (c_int, [c_void_p, c_int, ctypes.c_char_p, POINTER(c_double)]),
     "dn_set_stage_function": (c_int, [c_void_p, c_void_p, c_void_p]),
     "dn_patch_set_tile": (c_int, [c_void_p, c_int, c_int]),

@@ -41,6 +41,7 @@ UNITS = {
     "dn_lsbc.cu": ["-fmad=false"],
     "fv_schemes.cu": ["-fmad=false"],
     "dn_gridio.cpp": [],
+    "dn_exchange.cpp": [],
 }
 
 

@@ -38,6 +38,7 @@ struct DnPatch {
   double quantum[5] = {1, 1, 1, 1, 1};
   bool base_set = false;
   dn::WallBC wall{};                        // device view (table pointers are device memory)
+  bool owned = true;                        // false: a shadow of a patch another rank advances
 };
 
 } // namespace
@@ -431,7 +432,7 @@ int build_plan(dn_ctx* c)
     nc[r] = (int64_t)P.nc;
     for (int b = 0; b < 3; ++b) bufs[r * 3 + b] = P.buf[b];
     for (int v = 0; v < 5; ++v) { base[r * 5 + v] = P.base[v]; quantum[r * 5 + v] = P.quantum[v]; }
-    if (r >= c->tables.size()) continue;
+    if (r >= c->tables.size() || !P.owned) continue;
     const dn::DonorTables& T = c->tables[r];
     const size_t nu = T.rec_unique.size();
     if (nu == 0) continue;
@@ -525,7 +526,7 @@ int build_ls_plan(dn_ctx* c)
     nc[r] = (int64_t)P.nc;
     for (int b = 0; b < 3; ++b) bufs[r * 3 + b] = P.buf[b];
     for (int v = 0; v < 5; ++v) { base[r * 5 + v] = P.base[v]; quantum[r * 5 + v] = P.quantum[v]; }
-    if (r >= c->ls.size() || !c->ls_on[r]) continue;
+    if (r >= c->ls.size() || !c->ls_on[r] || !P.owned) continue;
     for (const auto& layer : c->ls[r].inner) {
       for (const dn::LayerCell& lc : layer) {
         patch.push_back((int32_t)r);
@@ -593,6 +594,35 @@ bool any_levelset(const dn_ctx* c)
 }
 
 int stage_all(dn_ctx* c, int in_b, int un_b, int out_b, double factor);
+
+// Exchange of donor cells between ranks: gather into / scatter from a
+// [var][item] buffer of the storage type (patch buffer table and cell
+// counts are the donor plan's).
+template <typename T>
+__global__ void k_exchange_pack(void* const* bufs, const int64_t* nc, int phys, const int32_t* patch,
+                                const uint64_t* cell, int64_t n, T* out)
+{
+  for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (int64_t)gridDim.x * blockDim.x) {
+    const int p = patch[t];
+    const T* f = static_cast<const T*>(bufs[(size_t)p * 3 + phys]);
+    const int64_t m = nc[p], c = (int64_t)cell[t];
+    #pragma unroll
+    for (int v = 0; v < 5; ++v) out[v * n + t] = f[v * m + c];
+  }
+}
+
+template <typename T>
+__global__ void k_exchange_unpack(void* const* bufs, const int64_t* nc, int phys, const int32_t* patch,
+                                  const uint64_t* cell, int64_t n, const T* in)
+{
+  for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (int64_t)gridDim.x * blockDim.x) {
+    const int p = patch[t];
+    T* f = static_cast<T*>(bufs[(size_t)p * 3 + phys]);
+    const int64_t m = nc[p], c = (int64_t)cell[t];
+    #pragma unroll
+    for (int v = 0; v < 5; ++v) f[v * m + c] = in[v * n + t];
+  }
+}
 
 // Launches of one RK step (RungeKutta::operator(), rungekutta.cpp:27-42)
 // from step-start buffer A through the other two buffers X, Y.
@@ -720,7 +750,7 @@ int build_batch(dn_ctx* c)
     r.wall = P.wall;
     int tj, tk;
     dn::shape_tile(fp64, c->shape[q], &tj, &tk);
-    tiles += (long)((P.d.nj + tj - 1) / tj) * ((P.d.nk + tk - 1) / tk);
+    if (P.owned) tiles += (long)((P.d.nj + tj - 1) / tj) * ((P.d.nk + tk - 1) / tk);
   }
   const long want = (long)c->num_sms * 2 * 4;
   long chunks = (want + tiles - 1) / tiles;
@@ -728,6 +758,7 @@ int build_batch(dn_ctx* c)
   std::vector<dn::WorkItem> items[dn::kNumShapes];
   for (size_t q = 0; q < np; ++q) {
     const DnPatch& P = c->patches[q];
+    if (!P.owned) continue;
     const int sh = c->shape[q];
     int tj, tk;
     dn::shape_tile(fp64, sh, &tj, &tk);
@@ -770,6 +801,7 @@ int stage_all(dn_ctx* c, int in_b, int un_b, int out_b, double factor)
   const bool functor = c->precision == DN_FP64 && (c->scheme != DN_FLUX_AUSMPLUS || c->stage_fn);
   if (!c->batched || c->patches.size() == 1 || functor) {
     for (auto& p : c->patches) {
+      if (!p.owned) continue;
       int s = stage_patch(c, p, in_b, un_b, out_b, factor);
       if (s) return s;
     }
@@ -1178,6 +1210,7 @@ int dn_conservation_sums(dn_ctx* c, double out[5])
   std::vector<long long> hi((size_t)kSumBlocks * 5);
   double tot[5] = {0, 0, 0, 0, 0};
   for (auto& p : c->patches) {
+    if (!p.owned) continue;
     const void* f = p.buf[c->fmap[0]];
     cudaError_t e;
     const double dV = p.d.dx * p.d.dy * p.d.dz;
@@ -1507,6 +1540,119 @@ int dn_set_option(dn_ctx* c, int option, int value)
     return DN_OK;
   }
   return fail(c, DN_ERR_ARG, "unknown option %d", option);
+}
+
+int dn_patch_set_owned(dn_ctx* c, int id, int owned)
+{
+  int s = check_patch(c, id);
+  if (s) return s;
+  c->patches[id].owned = owned != 0;
+  c->plan_dirty = true;
+  c->ls_dirty = true;
+  c->batch_dirty = true;
+  c->generation++;
+  return DN_OK;
+}
+
+int dn_exchange_build_ctx(dn_ctx* c, const int32_t* owner, int rank, int world, dn_exchange** out)
+{
+  if (!c || !owner || !out) return DN_ERR_ARG;
+  *out = nullptr;
+  std::vector<dn::DonorTables> tables(c->tables);
+  tables.resize(c->patches.size());
+  dn_exchange* e = new dn_exchange();
+  std::string err;
+  if (!dn::build_exchange(tables, owner, rank, world, e->ex, err)) {
+    delete e;
+    return fail(c, DN_ERR_ARG, "%s", err.c_str());
+  }
+  *out = e;
+  return DN_OK;
+}
+
+int dn_exchange_destroy(dn_exchange* e)
+{
+  if (!e) return DN_OK;
+  if (e->ex.device >= 0) {
+    int cur = 0;
+    cudaGetDevice(&cur);
+    cudaSetDevice(e->ex.device);
+    for (void* p : e->ex.dev) cudaFree(p);
+    cudaSetDevice(cur);
+  }
+  delete e;
+  return DN_OK;
+}
+
+namespace {
+
+// device copies of the exchange lists: [peer][send_patch, send_cell, recv_patch, recv_cell]
+int exchange_device_lists(dn_ctx* c, dn_exchange* e)
+{
+  dn::Exchange& x = e->ex;
+  if (x.device >= 0) {
+    if (x.device != c->device) return fail(c, DN_ERR_ARG, "exchange lists live on device %d, context on %d", x.device, c->device);
+    return DN_OK;
+  }
+  x.dev.assign((size_t)x.world * 4, nullptr);
+  x.device = c->device;
+  for (int q = 0; q < x.world; ++q) {
+    const void* src[4] = {x.send_patch[q].data(), x.send_cell[q].data(), x.recv_patch[q].data(), x.recv_cell[q].data()};
+    const size_t bytes[4] = {x.send_patch[q].size() * 4, x.send_cell[q].size() * 8, x.recv_patch[q].size() * 4,
+                             x.recv_cell[q].size() * 8};
+    for (int a = 0; a < 4; ++a) {
+      if (!bytes[a]) continue;
+      void* d = nullptr;
+      if (cudaMalloc(&d, bytes[a]) != cudaSuccess) return fail(c, DN_ERR_NOMEM, "cudaMalloc(exchange lists)");
+      x.dev[(size_t)q * 4 + a] = d;
+      cudaError_t er = cudaMemcpy(d, src[a], bytes[a], cudaMemcpyHostToDevice);
+      if (er != cudaSuccess) return cuda_fail(c, er, "exchange list upload");
+    }
+  }
+  return DN_OK;
+}
+
+int exchange_move(dn_ctx* c, dn_exchange* e, int field, int peer, void* buf, bool pack)
+{
+  if (!c || !e) return DN_ERR_ARG;
+  int s;
+  if ((s = check_field(c, field))) return s;
+  if (peer < 0 || peer >= e->ex.world || peer == e->ex.rank) return fail(c, DN_ERR_ARG, "peer %d is not another rank", peer);
+  if (set_device(c) != DN_OK) return DN_ERR_CUDA;
+  if (c->plan_dirty && (s = build_plan(c))) return s;
+  if ((s = exchange_device_lists(c, e))) return s;
+  const dn::Exchange& x = e->ex;
+  const int64_t n = (int64_t)(pack ? x.send_cell[peer].size() : x.recv_cell[peer].size());
+  if (n == 0) return DN_OK;
+  if (!buf) return fail(c, DN_ERR_ARG, "exchange buffer is NULL");
+  const int32_t* patch = static_cast<const int32_t*>(x.dev[(size_t)peer * 4 + (pack ? 0 : 2)]);
+  const uint64_t* cell = static_cast<const uint64_t*>(x.dev[(size_t)peer * 4 + (pack ? 1 : 3)]);
+  void* const* bufs = c->plan.bufs;
+  const int phys = c->fmap[field];
+  const int blocks = (int)std::min<int64_t>((n + 255) / 256, (int64_t)c->num_sms * 8);
+  if (c->precision == DN_FP64) {
+    if (pack) k_exchange_pack<double><<<blocks, 256, 0, c->stream>>>(bufs, c->plan.nc, phys, patch, cell, n, (double*)buf);
+    else k_exchange_unpack<double><<<blocks, 256, 0, c->stream>>>(bufs, c->plan.nc, phys, patch, cell, n, (const double*)buf);
+  } else {
+    if (pack) k_exchange_pack<int32_t><<<blocks, 256, 0, c->stream>>>(bufs, c->plan.nc, phys, patch, cell, n, (int32_t*)buf);
+    else k_exchange_unpack<int32_t><<<blocks, 256, 0, c->stream>>>(bufs, c->plan.nc, phys, patch, cell, n, (const int32_t*)buf);
+  }
+  c->launches++;
+  cudaError_t er = cudaGetLastError();
+  if (er != cudaSuccess) return cuda_fail(c, er, pack ? "exchange pack" : "exchange unpack");
+  return DN_OK;
+}
+
+} // namespace
+
+int dn_exchange_pack(dn_ctx* c, dn_exchange* e, int field, int peer, void* buf)
+{
+  return exchange_move(c, e, field, peer, buf, true);
+}
+
+int dn_exchange_unpack(dn_ctx* c, dn_exchange* e, int field, int peer, const void* buf)
+{
+  return exchange_move(c, e, field, peer, const_cast<void*>(buf), false);
 }
 
 int dn_write_data(dn_ctx* c, int field, const char* base, double time, int count)

@@ -352,9 +352,6 @@ OverlapPatch overlap_patch(const dn_patch_desc& d)
 
 // ------------------------------------------------------------ host-only C ABI
 
-struct dn_overlap {
-  std::vector<dn::DonorTables> tables;
-};
 
 extern "C" {
 

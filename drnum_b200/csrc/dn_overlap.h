@@ -72,4 +72,30 @@ void desc_spacing(const struct dn_patch_desc& d, double out[3]);
 // Overlap description of a patch description.
 OverlapPatch overlap_patch(const struct dn_patch_desc& d);
 
+// Exchange lists of a patch grid sharded over ranks (patch p on rank
+// owner[p]).  For every peer q of `rank`: recv = the donor cells of patches
+// of q that the donor tables of this rank's receiving patches read, send =
+// the donor cells of this rank's patches that q's receiving patches read;
+// each as (patch, cell) pairs, unique, ascending by patch then cell, so that
+// both sides of a pair of ranks derive the same order independently.
+struct Exchange {
+  int rank = 0, world = 1;
+  std::vector<std::vector<int32_t>> send_patch, recv_patch;   // [peer][item]
+  std::vector<std::vector<uint64_t>> send_cell, recv_cell;
+  // device copies (allocated on first use by the context that packs/unpacks)
+  int device = -1;
+  std::vector<void*> dev;
+};
+
+bool build_exchange(const std::vector<DonorTables>& tables, const int32_t* owner, int rank, int world,
+                    Exchange& ex, std::string& err);
+
 } // namespace dn
+
+struct dn_overlap {
+  std::vector<dn::DonorTables> tables;
+};
+
+struct dn_exchange {
+  dn::Exchange ex;
+};

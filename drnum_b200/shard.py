@@ -1,0 +1,163 @@
+"""Patch grids sharded over GPUs: one process per GPU, patches partitioned by
+cell count, donor cells exchanged between ranks before every donor copy.
+
+The reference advances all patches of a grid in one process; its RK step
+(RungeKutta::operator(), rungekutta.cpp:27-42) copies donor data between
+patches in memory (Patch::accessDonorDataDirect, patch.cpp:573-653).  Here
+every rank holds the whole grid in its context but owns only its share
+(dn_patch_set_owned): stages, donor copies into receiving cells and the
+level-set wall run on owned patches, the others are shadows.  Before each
+donor copy, each rank sends its peers the donor cells of its patches that
+their receiving patches read and receives the ones its own receiving patches
+read (dn_exchange_pack / _unpack around NCCL send/recv through
+torch.distributed).  The donor copy then reads local memory and the result
+equals the single-GPU step bit for bit.
+
+`rk_step_sequence` is the step itself over an operations object, so the same
+sequence drives GPU contexts (`ShardedIterator`) and, in the CPU tests, the
+numpy oracle with gloo transport.
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+from . import _lib
+from ._lib import check
+
+
+def partition(cells, world):
+    """Greedy bin packing: patches in descending cell count (ties: lower
+    index first) each to the rank with the fewest cells so far (ties: lower
+    rank).  Returns owner[patch]."""
+    order = sorted(range(len(cells)), key=lambda p: (-int(cells[p]), p))
+    load = [0] * world
+    owner = [0] * len(cells)
+    for p in order:
+        r = min(range(world), key=lambda q: (load[q], q))
+        owner[p] = r
+        load[r] += int(cells[p])
+    return owner
+
+
+class Transport:
+    """Moves the exchange buffers of one rank: for every peer with cells to
+    send, `pack(field, peer, buf)` fills a send buffer; sends and receives to
+    all peers go out as one batch of torch.distributed point-to-point ops
+    (grouped, so NCCL cannot deadlock on their order); then
+    `unpack(field, peer, buf)` drains each receive buffer.  `alloc(n)` makes
+    a buffer of n elements (a CUDA tensor for NCCL, a CPU tensor for gloo)."""
+
+    def __init__(self, rank, world, counts, alloc, pack, unpack, group=None):
+        import torch.distributed as dist
+        self.dist = dist
+        self.rank, self.world, self.group = rank, world, group
+        self.pack, self.unpack = pack, unpack
+        self.peers = [q for q in range(world) if q != rank]
+        self.send = {q: alloc(5 * counts[q][0]) for q in self.peers if counts[q][0]}
+        self.recv = {q: alloc(5 * counts[q][1]) for q in self.peers if counts[q][1]}
+
+    def exchange(self, field):
+        dist = self.dist
+        ops = []
+        for q in self.peers:
+            if q in self.send:
+                self.pack(field, q, self.send[q])
+                ops.append(dist.P2POp(dist.isend, self.send[q], q, self.group))
+            if q in self.recv:
+                ops.append(dist.P2POp(dist.irecv, self.recv[q], q, self.group))
+        if ops:
+            for req in dist.batch_isend_irecv(ops):
+                req.wait()
+        for q in self.peers:
+            if q in self.recv:
+                self.unpack(field, q, self.recv[q])
+
+
+def rk_step_sequence(ops, dt, alphas):
+    """One RK step of a sharded grid in the order of the reference's
+    RungeKutta::operator() with post-operations (rungekutta.cpp:27-42), the
+    order dn_rk_step runs: donor copy, step-start copy, then per stage
+    (after the first: donor copy again), stage, donor copy, post-operations;
+    every donor copy preceded by the exchange of donor cells.  `ops` provides
+    exchange(field), copy_donor_data(field), copy_field(src, dst),
+    compute(factor) and post_operations()."""
+    ops.exchange(0)
+    ops.copy_donor_data(0)
+    ops.copy_field(0, 1)
+    for s, a in enumerate(alphas):
+        if s > 0:
+            ops.exchange(0)
+            ops.copy_donor_data(0)
+        ops.compute(a * dt)
+        ops.exchange(0)
+        ops.copy_donor_data(0)
+        ops.post_operations()
+
+
+class ShardedIterator:
+    """The GPU side: a B200CartesianIterator holding every patch of the grid
+    (donor tables computed for all of them), owning the patches `owner`
+    assigns to this rank, with an exchange plan and NCCL transport.  The
+    process group must use the NCCL backend and this rank's GPU must be the
+    current device."""
+
+    def __init__(self, it, owner, rank, world, group=None):
+        import torch
+        self.it, self.owner, self.rank, self.world = it, list(owner), rank, world
+        lib = it.lib
+        for p in range(it.numPatches()):
+            check(it.ctx, lib.dn_patch_set_owned(it.ctx, p, 1 if self.owner[p] == rank else 0))
+        own = (ctypes.c_int32 * len(self.owner))(*self.owner)
+        self.ex = ctypes.c_void_p()
+        check(it.ctx, lib.dn_exchange_build_ctx(it.ctx, own, rank, world, ctypes.byref(self.ex)))
+        counts = {}
+        for q in range(world):
+            ns, nr = ctypes.c_int64(), ctypes.c_int64()
+            check(it.ctx, lib.dn_exchange_counts(self.ex, q, ctypes.byref(ns), ctypes.byref(nr)))
+            counts[q] = (ns.value, nr.value)
+        self.counts = counts
+        # the library's work goes on torch's current stream, which NCCL orders with
+        self.stream = torch.cuda.current_stream()
+        check(it.ctx, lib.dn_set_stream(it.ctx, ctypes.c_void_p(self.stream.cuda_stream)))
+        dtype = torch.float64 if it.precision == _lib.DN_FP64 else torch.int32
+        self.transport = Transport(rank, world, counts, lambda n: torch.empty(n, dtype=dtype, device="cuda"),
+                                   self._pack, self._unpack, group)
+        self.post = []
+
+    def _pack(self, field, peer, buf):
+        check(self.it.ctx, self.it.lib.dn_exchange_pack(self.it.ctx, self.ex, field, peer,
+                                                        ctypes.c_void_p(buf.data_ptr())))
+
+    def _unpack(self, field, peer, buf):
+        check(self.it.ctx, self.it.lib.dn_exchange_unpack(self.it.ctx, self.ex, field, peer,
+                                                          ctypes.c_void_p(buf.data_ptr())))
+
+    # operations of rk_step_sequence
+    def exchange(self, field):
+        self.transport.exchange(field)
+
+    def copy_donor_data(self, field):
+        self.it.copyDonorData(field)
+
+    def copy_field(self, src, dst):
+        self.it.copyField(src, dst)
+
+    def compute(self, factor):
+        self.it.computeAll(factor)
+
+    def post_operations(self):
+        for op in self.post:
+            op()
+
+    def addPostOperation(self, op):
+        self.post.append(op)
+
+    def rkStep(self, dt, alphas):
+        rk_step_sequence(self, dt, alphas)
+
+    def close(self):
+        if self.ex:
+            self.it.lib.dn_exchange_destroy(self.ex)
+            self.ex = None

@@ -362,6 +362,39 @@ int dn_grid_write(const char* path, int n, const dn_patch_desc* patches, const c
 int dn_write_data(dn_ctx* ctx, int field, const char* base_file_name, double time, int count);
 int dn_read_data(dn_ctx* ctx, int field, const char* file_name, double* time);
 
+/* Patch grids sharded over ranks (one process per GPU).  The reference runs
+ * every patch of a grid in one process and its donor copy reads other
+ * patches directly (Patch::accessDonorDataDirect, patch.cpp:573-653).  Here
+ * each rank adds every patch of the grid to its context, owns some
+ * (dn_patch_set_owned; default: all) and keeps the others as shadows: stages,
+ * donor copies into receiving cells and the level-set wall run on owned
+ * patches only, and conservation sums cover owned patches only.  Before each
+ * donor copy a rank sends the owners' donor cells its peers read and
+ * receives those it reads into its shadows; the donor copy then runs on
+ * local memory and gives the same bits as a single context.
+ *   dn_exchange_build (host only, from dn_overlap_build's tables) and
+ *   dn_exchange_build_ctx (from the context's tables): the exchange lists of
+ *     `rank` given owner[num_patches]; (patch, cell) pairs per peer, unique
+ *     and ascending, so both ranks of a pair derive the same order;
+ *   dn_exchange_counts / _get: the lists of one peer;
+ *   dn_exchange_pack / _unpack: gather the send cells of field `field` into,
+ *     or scatter the receive cells from, a device buffer of 5 x n elements
+ *     [var][item] of the context's storage type (8-byte double for DN_FP64,
+ *     4-byte int32 offsets for DN_FP32, whose shadows share the owner's base
+ *     and quantum), enqueued on the context's stream.
+ * Moving the buffers between ranks is the caller's (NCCL send/recv;
+ * drnum_b200/shard.py). */
+typedef struct dn_exchange dn_exchange;
+int dn_patch_set_owned(dn_ctx* ctx, int patch_id, int owned);
+int dn_exchange_build(const dn_overlap* ov, const int32_t* owner, int rank, int world, dn_exchange** out);
+int dn_exchange_build_ctx(dn_ctx* ctx, const int32_t* owner, int rank, int world, dn_exchange** out);
+int dn_exchange_counts(const dn_exchange* ex, int peer, int64_t* n_send, int64_t* n_recv);
+int dn_exchange_get(const dn_exchange* ex, int peer, int32_t* send_patch, uint64_t* send_cell, int32_t* recv_patch,
+                    uint64_t* recv_cell);
+int dn_exchange_pack(dn_ctx* ctx, dn_exchange* ex, int field, int peer, void* dev_buf);
+int dn_exchange_unpack(dn_ctx* ctx, dn_exchange* ex, int field, int peer, const void* dev_buf);
+int dn_exchange_destroy(dn_exchange* ex);
+
 /* Number of device kernel launches the context has issued so far. */
 int dn_launch_count(const dn_ctx* ctx, int64_t* count);
 

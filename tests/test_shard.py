@@ -1,0 +1,341 @@
+"""Patch grids sharded over ranks (drnum_b200/shard.py, dn_exchange_*).
+
+CPU: the partition, the exchange lists (host-only dn_exchange_build from
+the library's own donor tables), and the whole sharded RK step sequence with
+gloo transport between two and three processes, each advancing its patches
+with the oracle: the result equals the reference's single-process grid run
+(golden fixtures) bit for bit.  GPU (one device): two contexts in one
+process play two ranks, the exchange buffers handed over directly (no
+kernel waits on another); the result equals one context bit for bit."""
+import ctypes
+import multiprocessing as mp
+import os
+import socket
+
+import numpy as np
+import pytest
+
+import cases_def
+import pyoracle
+from drnum_b200 import _lib, cases, shard
+from test_overlap import TABLE_KEYS, _descs, _fixture, _ls_tables
+
+
+def exchange_lists(patches, owner, rank, world):
+    """(send, recv) per peer: arrays of (patch, cell) from dn_exchange_build."""
+    lib = _lib.load()
+    h = ctypes.c_void_p()
+    nd = ctypes.c_int64()
+    assert lib.dn_overlap_build(_descs(patches), len(patches), ctypes.byref(h), ctypes.byref(nd)) == _lib.DN_OK
+    ex = ctypes.c_void_p()
+    own = (ctypes.c_int32 * len(owner))(*owner)
+    try:
+        assert lib.dn_exchange_build(h, own, rank, world, ctypes.byref(ex)) == _lib.DN_OK
+        out = {}
+        for q in range(world):
+            ns, nr = ctypes.c_int64(), ctypes.c_int64()
+            assert lib.dn_exchange_counts(ex, q, ctypes.byref(ns), ctypes.byref(nr)) == _lib.DN_OK
+            sp, sc = np.zeros(ns.value, np.int32), np.zeros(ns.value, np.uint64)
+            rp, rc = np.zeros(nr.value, np.int32), np.zeros(nr.value, np.uint64)
+            assert lib.dn_exchange_get(ex, q, sp.ctypes.data, sc.ctypes.data, rp.ctypes.data,
+                                       rc.ctypes.data) == _lib.DN_OK
+            out[q] = ((sp, sc), (rp, rc))
+        return out
+    finally:
+        if ex:
+            lib.dn_exchange_destroy(ex)
+        lib.dn_overlap_destroy(h)
+
+
+def test_partition_balances_cells():
+    cells = [100, 90, 80, 70, 60, 10, 10, 10]
+    owner = shard.partition(cells, 3)
+    loads = [sum(c for c, o in zip(cells, owner) if o == r) for r in range(3)]
+    assert owner == shard.partition(cells, 3)
+    assert max(loads) - min(loads) <= 40
+    assert shard.partition(cells, 1) == [0] * len(cells)
+
+
+@pytest.mark.parametrize("name,world", [("octants_8", 3), ("random6", 2), ("octants_ragged", 4)])
+def test_exchange_lists_pair_up_and_cover_every_remote_donor(golden_dir, name, world):
+    patches = cases_def.grid_layout(name)
+    owner = shard.partition([int(np.prod(p["n"])) for p in patches], world)
+    lists = [exchange_lists(patches, owner, r, world) for r in range(world)]
+    z = _fixture(golden_dir, name)
+    for r in range(world):
+        for q in range(world):
+            if q == r:
+                assert len(lists[r][q][0][0]) == 0 and len(lists[r][q][1][0]) == 0
+                continue
+            (sp, sc), _ = lists[r][q]
+            _, (rp, rc) = lists[q][r]
+            assert np.array_equal(sp, rp) and np.array_equal(sc, rc)
+        # every donor cell a receiving patch of r reads from another rank arrives
+        need = set()
+        for p in range(len(patches)):
+            if owner[p] != r:
+                continue
+            donors = z[f"p{p}_donor_patch"]
+            nrec, stride, idx = z[f"p{p}_num_receivers"], z[f"p{p}_stride"], z[f"p{p}_donor_idx"]
+            pos = 0
+            for d, m, s in zip(donors, nrec, stride):
+                n = int(m) * int(s)
+                if owner[int(d)] != r:
+                    need.update((int(d), int(c)) for c in idx[pos:pos + n])
+                pos += n
+        got = set()
+        for q in range(world):
+            _, (rp, rc) = lists[r][q]
+            got.update(zip(rp.tolist(), rc.tolist()))
+        assert got == need
+
+
+def test_exchange_rejects_bad_owner():
+    lib = _lib.load()
+    patches = cases_def.grid_layout("pair_x")
+    h = ctypes.c_void_p()
+    nd = ctypes.c_int64()
+    assert lib.dn_overlap_build(_descs(patches), 2, ctypes.byref(h), ctypes.byref(nd)) == _lib.DN_OK
+    ex = ctypes.c_void_p()
+    try:
+        assert lib.dn_exchange_build(h, (ctypes.c_int32 * 2)(0, 2), 0, 2, ctypes.byref(ex)) == _lib.DN_ERR_ARG
+        assert lib.dn_exchange_build(h, (ctypes.c_int32 * 2)(0, 1), 2, 2, ctypes.byref(ex)) == _lib.DN_ERR_ARG
+    finally:
+        lib.dn_overlap_destroy(h)
+
+
+# ------------------------------------------------------------- gloo ranks on CPU
+
+class OracleShard:
+    """rk_step_sequence operations over the numpy oracle for one rank: owned
+    patches advance, the others are shadows refreshed by the exchange."""
+
+    def __init__(self, rank, world, name, golden_dir, group):
+        import torch
+        self.rank = rank
+        z = _fixture(golden_dir, name)
+        patches, states, spacings, dt, steps = cases_def.grid_case(name)
+        self.patches, self.spacings, self.dt, self.steps = patches, spacings, dt, steps
+        self.U = [np.ascontiguousarray(s, dtype=np.float64).copy() for s in states]
+        self.owner = shard.partition([int(np.prod(p["n"])) for p in patches], world)
+        empty = {k: z[f"p0_{k}"][:0] for k in TABLE_KEYS}
+        self.tables = [{k: z[f"p{p}_{k}"] for k in TABLE_KEYS} if self.owner[p] == rank else empty
+                       for p in range(len(patches))]
+        self.bcs = cases_def.grid_bcs(name) or {}
+        layers = _ls_tables(z, name, len(patches)) if name in cases_def.LEVELSET else None
+        self.layers = None if layers is None else [L if self.owner[p] == rank else None for p, L in enumerate(layers)]
+        lists = exchange_lists(patches, self.owner, rank, world)
+        self.lists = lists
+        counts = {q: (len(lists[q][0][1]), len(lists[q][1][1])) for q in range(world)}
+        self.transport = shard.Transport(rank, world, counts, lambda n: torch.zeros(n, dtype=torch.float64),
+                                         self._pack, self._unpack, group)
+
+    def _pack(self, field, peer, buf):
+        sp, sc = self.lists[peer][0]
+        out = buf.numpy().reshape(5, -1)
+        for t, (p, c) in enumerate(zip(sp, sc)):
+            out[:, t] = self.U[int(p)].reshape(5, -1)[:, int(c)]
+
+    def _unpack(self, field, peer, buf):
+        rp, rc = self.lists[peer][1]
+        inp = buf.numpy().reshape(5, -1)
+        for t, (p, c) in enumerate(zip(rp, rc)):
+            self.U[int(p)].reshape(5, -1)[:, int(c)] = inp[:, t]
+
+    def exchange(self, field):
+        self.transport.exchange(field)
+
+    def copy_donor_data(self, field):
+        pyoracle.oracle_donor_copy(self.U, self.tables)
+
+    def copy_field(self, src, dst):
+        self.Un = [u.copy() for u in self.U]
+
+    def compute(self, factor):
+        for p, u in enumerate(self.U):
+            if self.owner[p] != self.rank:
+                continue
+            hx, hy, hz = self.spacings[p]
+            res = pyoracle.oracle_residual_bc(u, (hx, hy, hz), self.bcs.get(p, {}))
+            self.U[p] = self.Un[p] + (factor / (hx * hy * hz)) * res
+
+    def post_operations(self):
+        if self.layers is not None:
+            pyoracle.oracle_levelset_bc(self.U, self.layers)
+
+
+def _gloo_rank(rank, world, port, name, golden_dir, result_path):
+    import datetime
+    import torch.distributed as dist
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=120))
+    try:
+        s = OracleShard(rank, world, name, golden_dir, None)
+        for _ in range(s.steps):
+            shard.rk_step_sequence(s, s.dt, cases_def.ALPHA)
+        mine = {p: s.U[p] for p in range(len(s.U)) if s.owner[p] == rank}
+        gathered = [None] * world
+        dist.all_gather_object(gathered, mine)
+        if rank == 0:
+            merged = {}
+            for g in gathered:
+                merged.update(g)
+            np.savez(result_path, **{f"p{p}": u for p, u in merged.items()})
+    finally:
+        dist.destroy_process_group()
+
+
+def _free_port():
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
+
+
+@pytest.mark.parametrize("name,world", [("octants_jet", 2), ("octants_8", 3), ("sphere_pair", 2)])
+def test_sharded_rk_steps_over_gloo_equal_reference(golden_dir, tmp_path, name, world):
+    z = _fixture(golden_dir, name)
+    result = str(tmp_path / "sharded.npz")
+    ctx = mp.get_context("spawn")
+    port = _free_port()
+    procs = [ctx.Process(target=_gloo_rank, args=(r, world, port, name, golden_dir, result)) for r in range(world)]
+    for p in procs:
+        p.start()
+    for p in procs:
+        p.join(timeout=300)
+    for p in procs:
+        if p.is_alive():
+            p.kill()
+    assert all(p.exitcode == 0 for p in procs), [p.exitcode for p in procs]
+    out = np.load(result)
+    for p in range(int(z["num_patches"])):
+        assert np.array_equal(out[f"p{p}"], z[f"p{p}_out"]), (name, p)
+
+
+# ------------------------------------------------------------- two contexts, one GPU
+
+class _Recorder:
+    """Records the operation sequence of one RK step."""
+
+    def __init__(self):
+        self.ops = []
+
+    def __getattr__(self, name):
+        return lambda *args: self.ops.append((name, args))
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision", [_lib.DN_FP64, _lib.DN_FP32])
+@pytest.mark.parametrize("name", ["octants_jet", "sphere_pair"])
+def test_two_contexts_as_two_ranks_equal_one_context(golden_dir, name, precision):
+    import torch
+    from drnum_b200.api import B200LevelSetObjectBC
+    from test_gpu_grid import make_grid
+    world = 2
+    one, objs1, _, dt, steps = make_grid(name, precision)
+    post1 = [B200LevelSetObjectBC(one)] if name in cases_def.LEVELSET else []
+    ranks = [make_grid(name, precision) for _ in range(world)]
+    its = [r[0] for r in ranks]
+    patches = cases_def.grid_layout(name)
+    owner = shard.partition([int(np.prod(p["n"])) for p in patches], world)
+    assert len(set(owner)) == world
+    lib = _lib.load()
+    exs, bufs = [], {}
+    dtype = torch.float64 if precision == _lib.DN_FP64 else torch.int32
+    for r, it in enumerate(its):
+        for p in range(len(patches)):
+            assert lib.dn_patch_set_owned(it.ctx, p, int(owner[p] == r)) == _lib.DN_OK
+        ex = ctypes.c_void_p()
+        own = (ctypes.c_int32 * len(owner))(*owner)
+        assert lib.dn_exchange_build_ctx(it.ctx, own, r, world, ctypes.byref(ex)) == _lib.DN_OK
+        exs.append(ex)
+        for q in range(world):
+            ns, nr = ctypes.c_int64(), ctypes.c_int64()
+            assert lib.dn_exchange_counts(ex, q, ctypes.byref(ns), ctypes.byref(nr)) == _lib.DN_OK
+            if ns.value:
+                bufs[(r, q)] = torch.empty(5 * ns.value, dtype=dtype, device="cuda")
+    assert bufs, "the partition leaves no donor cell to exchange"
+    posts = [[B200LevelSetObjectBC(it)] if name in cases_def.LEVELSET else [] for it in its]
+
+    def apply(r, op, args):
+        it = its[r]
+        if op == "copy_donor_data":
+            it.copyDonorData(*args)
+        elif op == "copy_field":
+            it.copyField(*args)
+        elif op == "compute":
+            it.computeAll(*args)
+        elif op == "post_operations":
+            for f in posts[r]:
+                f()
+
+    rec = _Recorder()
+    shard.rk_step_sequence(rec, dt, cases.RK3_ALPHA)
+    for _ in range(steps):
+        for op, args in rec.ops:
+            if op == "exchange":
+                for (r, q), b in bufs.items():
+                    assert lib.dn_exchange_pack(its[r].ctx, exs[r], args[0], q, ctypes.c_void_p(b.data_ptr())) == 0
+                for it in its:
+                    it.sync()
+                for (r, q), b in bufs.items():
+                    assert lib.dn_exchange_unpack(its[q].ctx, exs[q], args[0], r, ctypes.c_void_p(b.data_ptr())) == 0
+                for it in its:
+                    it.sync()
+            else:
+                for r in range(world):
+                    apply(r, op, args)
+        # the same step on one context (its own stage sequence)
+        one.copyDonorData(0)
+        one.copyField(0, 1)
+        for s, a in enumerate(cases.RK3_ALPHA):
+            if s > 0:
+                one.copyDonorData(0)
+            one.computeAll(a * dt)
+            one.copyDonorData(0)
+            for f in post1:
+                f()
+    one.updateHost(fields=(0,))
+    for it in its:
+        it.updateHost(fields=(0,))
+    for p in range(len(patches)):
+        got = ranks[owner[p]][1][p].getField(0)
+        assert np.array_equal(got, objs1[p].getField(0)), (name, p)
+    if precision == _lib.DN_FP64:
+        z = _fixture(golden_dir, name)
+        for p in range(len(patches)):
+            assert np.array_equal(ranks[owner[p]][1][p].getField(0), z[f"p{p}_out"]), (name, p)
+    for ex in exs:
+        lib.dn_exchange_destroy(ex)
+    for it in its + [one]:
+        it.close()
+
+
+@pytest.mark.gpu
+def test_sharded_iterator_single_rank_nccl_equals_reference(golden_dir):
+    # the GPU driver class end to end on one rank (NCCL group of one): owned
+    # flags, exchange plan, torch stream, the step sequence
+    import datetime
+    import torch
+    import torch.distributed as dist
+    from drnum_b200.api import B200LevelSetObjectBC
+    from test_gpu_grid import make_grid
+    name = "sphere_pair"
+    z = _fixture(golden_dir, name)
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(_free_port())
+    torch.cuda.set_device(0)
+    dist.init_process_group("nccl", rank=0, world_size=1, timeout=datetime.timedelta(seconds=60))
+    try:
+        it, objs, _, dt, steps = make_grid(name, _lib.DN_FP64)
+        sh = shard.ShardedIterator(it, [0] * len(objs), 0, 1)
+        sh.addPostOperation(B200LevelSetObjectBC(it))
+        for _ in range(steps):
+            sh.rkStep(dt, cases.RK3_ALPHA)
+        it.updateHost(fields=(0,))
+        for p, cp in enumerate(objs):
+            assert np.array_equal(cp.getField(0), z[f"p{p}_out"]), p
+        sh.close()
+        it.close()
+    finally:
+        dist.destroy_process_group()
