@@ -125,6 +125,10 @@ SIGNATURES = {
     "dn_grid_write": (c_int, [ctypes.c_char_p, c_int, POINTER(dn_patch_desc), POINTER(ctypes.c_char_p)]),
     "dn_write_data": (c_int, [c_void_p, c_int, ctypes.c_char_p, c_double, c_int]),
     "dn_patch_set_owned": (c_int, [c_void_p, c_int, c_int]),
+    "dn_patch_upload_async": (c_int, [c_void_p, c_int, c_int, POINTER(c_double)]),
+    "dn_patch_upload_f32_async": (c_int, [c_void_p, c_int, c_int, POINTER(c_float)]),
+    "dn_patch_download_async": (c_int, [c_void_p, c_int, c_int, POINTER(c_double)]),
+    "dn_patch_download_f32_async": (c_int, [c_void_p, c_int, c_int, POINTER(c_float)]),
     "dn_exchange_build": (c_int, [c_void_p, POINTER(c_int32), c_int, c_int, POINTER(c_void_p)]),
     "dn_exchange_build_ctx": (c_int, [c_void_p, POINTER(c_int32), c_int, c_int, POINTER(c_void_p)]),
     "dn_exchange_counts": (c_int, [c_void_p, c_int, POINTER(c_int64), POINTER(c_int64)]),

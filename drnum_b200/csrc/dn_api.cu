@@ -96,6 +96,17 @@ struct dn_ctx {
   cudaStream_t graph_stream = nullptr;
   int64_t generation = 0;
   int64_t graph_generation = -1;
+  // asynchronous host transfers: a copy-in and a copy-out stream with two
+  // staging buffers each, ordered against the context's stream by events
+  cudaStream_t s_in = nullptr, s_out = nullptr;
+  void* st_in[2] = {nullptr, nullptr};
+  size_t st_in_bytes[2] = {0, 0};
+  void* st_out[2] = {nullptr, nullptr};
+  size_t st_out_bytes[2] = {0, 0};
+  cudaEvent_t ev_in_done[2] = {nullptr, nullptr}, ev_in_free[2] = {nullptr, nullptr};
+  bool ev_in_free_set[2] = {false, false};
+  cudaEvent_t ev_main = nullptr, ev_out_read = nullptr;
+  unsigned in_seq = 0, out_seq = 0;
   // FP64 flux scheme (DN_FLUX_*) or a user stage function replacing it
   int scheme = DN_FLUX_AUSMPLUS;
   dn_stage_fn stage_fn = nullptr;
@@ -971,6 +982,109 @@ int download_impl(dn_ctx* c, int id, int field, H* host)
   return read_device_error(c);
 }
 
+int ensure_async(dn_ctx* c)
+{
+  if (c->s_in) return DN_OK;
+  bool ok = cudaStreamCreateWithFlags(&c->s_in, cudaStreamNonBlocking) == cudaSuccess &&
+            cudaStreamCreateWithFlags(&c->s_out, cudaStreamNonBlocking) == cudaSuccess &&
+            cudaEventCreateWithFlags(&c->ev_main, cudaEventDisableTiming) == cudaSuccess &&
+            cudaEventCreateWithFlags(&c->ev_out_read, cudaEventDisableTiming) == cudaSuccess;
+  for (int b = 0; b < 2 && ok; ++b)
+    ok = cudaEventCreateWithFlags(&c->ev_in_done[b], cudaEventDisableTiming) == cudaSuccess &&
+         cudaEventCreateWithFlags(&c->ev_in_free[b], cudaEventDisableTiming) == cudaSuccess;
+  return ok ? DN_OK : fail(c, DN_ERR_CUDA, "cannot create the transfer streams");
+}
+
+int ensure_buffer(dn_ctx* c, void*& buf, size_t& cap, size_t bytes)
+{
+  if (cap >= bytes) return DN_OK;
+  if (buf) cudaFree(buf);
+  buf = nullptr;
+  cap = 0;
+  cudaError_t e = cudaMalloc(&buf, bytes);
+  if (e != cudaSuccess) return cuda_fail(c, e, "cudaMalloc(transfer staging)");
+  cap = bytes;
+  return DN_OK;
+}
+
+// Upload through the copy-in stream: host -> staging[b] on s_in, then the
+// conversion into the field on the context's stream once the copy is done.
+// Staging[b] is refilled only after the conversion that read it.
+template <typename H>
+int upload_async_impl(dn_ctx* c, int id, int field, const H* host)
+{
+  int s = check_patch(c, id);
+  if (s) return s;
+  if ((s = check_field(c, field))) return s;
+  if (!host) return fail(c, DN_ERR_ARG, "host pointer is NULL");
+  if (set_device(c) != DN_OK) return DN_ERR_CUDA;
+  if ((s = ensure_async(c))) return s;
+  DnPatch& p = c->patches[id];
+  if (c->precision == DN_FP32 && !p.base_set) {
+    derive_base(p, host);
+    c->plan_dirty = true;
+    c->ls_dirty = true;
+    c->batch_dirty = true;
+    c->generation++;
+  }
+  const int b = (int)(c->in_seq++ & 1);
+  const size_t n = 5 * p.nc;
+  if ((s = ensure_buffer(c, c->st_in[b], c->st_in_bytes[b], n * sizeof(H)))) return s;
+  cudaError_t e = cudaSuccess;
+  if (c->ev_in_free_set[b]) e = cudaStreamWaitEvent(c->s_in, c->ev_in_free[b], 0);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(c->st_in[b], host, n * sizeof(H), cudaMemcpyHostToDevice, c->s_in);
+  if (e == cudaSuccess) e = cudaEventRecord(c->ev_in_done[b], c->s_in);
+  if (e == cudaSuccess) e = cudaStreamWaitEvent(c->stream, c->ev_in_done[b], 0);
+  if (e != cudaSuccess) return cuda_fail(c, e, "asynchronous upload copy");
+  void* dst = p.buf[c->fmap[field]];
+  if (c->precision == DN_FP64) {
+    k_convert<H, double><<<grid_for(n), 256, 0, c->stream>>>((const H*)c->st_in[b], (double*)dst, n);
+  } else {
+    k_quantize<H><<<grid_for(n), 256, 0, c->stream>>>((const H*)c->st_in[b], (int32_t*)dst, p.nc, qparams(p), c->d_err);
+  }
+  c->launches++;
+  e = cudaGetLastError();
+  if (e == cudaSuccess) e = cudaEventRecord(c->ev_in_free[b], c->stream);
+  if (e != cudaSuccess) return cuda_fail(c, e, "asynchronous upload conversion");
+  c->ev_in_free_set[b] = true;
+  return DN_OK;
+}
+
+// Download through the copy-out stream: once the context's stream reached
+// this point, the field is converted into staging[b] on s_out (the context's
+// stream waits for that conversion only, not for the copy), then copied to
+// the host on s_out.
+template <typename H>
+int download_async_impl(dn_ctx* c, int id, int field, H* host)
+{
+  int s = check_patch(c, id);
+  if (s) return s;
+  if ((s = check_field(c, field))) return s;
+  if (!host) return fail(c, DN_ERR_ARG, "host pointer is NULL");
+  if (set_device(c) != DN_OK) return DN_ERR_CUDA;
+  if ((s = ensure_async(c))) return s;
+  DnPatch& p = c->patches[id];
+  const int b = (int)(c->out_seq++ & 1);
+  const size_t n = 5 * p.nc;
+  if ((s = ensure_buffer(c, c->st_out[b], c->st_out_bytes[b], n * sizeof(H)))) return s;
+  cudaError_t e = cudaEventRecord(c->ev_main, c->stream);
+  if (e == cudaSuccess) e = cudaStreamWaitEvent(c->s_out, c->ev_main, 0);
+  if (e != cudaSuccess) return cuda_fail(c, e, "asynchronous download ordering");
+  const void* src = p.buf[c->fmap[field]];
+  if (c->precision == DN_FP64) {
+    k_convert<double, H><<<grid_for(n), 256, 0, c->s_out>>>((const double*)src, (H*)c->st_out[b], n);
+  } else {
+    k_dequantize<H><<<grid_for(n), 256, 0, c->s_out>>>((const int32_t*)src, (H*)c->st_out[b], p.nc, qparams(p));
+  }
+  c->launches++;
+  e = cudaGetLastError();
+  if (e == cudaSuccess) e = cudaEventRecord(c->ev_out_read, c->s_out);
+  if (e == cudaSuccess) e = cudaStreamWaitEvent(c->stream, c->ev_out_read, 0);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(host, c->st_out[b], n * sizeof(H), cudaMemcpyDeviceToHost, c->s_out);
+  if (e != cudaSuccess) return cuda_fail(c, e, "asynchronous download copy");
+  return DN_OK;
+}
+
 } // namespace
 
 extern "C" {
@@ -1014,6 +1128,18 @@ int dn_ctx_destroy(dn_ctx* c)
   free_ls_plan(c);
   free_batch(c);
   if (c->staging) cudaFree(c->staging);
+  if (c->s_in) cudaStreamSynchronize(c->s_in);
+  if (c->s_out) cudaStreamSynchronize(c->s_out);
+  for (int b = 0; b < 2; ++b) {
+    if (c->st_in[b]) cudaFree(c->st_in[b]);
+    if (c->st_out[b]) cudaFree(c->st_out[b]);
+    if (c->ev_in_done[b]) cudaEventDestroy(c->ev_in_done[b]);
+    if (c->ev_in_free[b]) cudaEventDestroy(c->ev_in_free[b]);
+  }
+  if (c->ev_main) cudaEventDestroy(c->ev_main);
+  if (c->ev_out_read) cudaEventDestroy(c->ev_out_read);
+  if (c->s_in) cudaStreamDestroy(c->s_in);
+  if (c->s_out) cudaStreamDestroy(c->s_out);
   if (c->d_partials) cudaFree(c->d_partials);
   if (c->d_err) cudaFree(c->d_err);
   if (c->d_err_info) cudaFree(c->d_err_info);
@@ -1117,6 +1243,10 @@ int dn_patch_upload(dn_ctx* c, int id, int field, const double* host) { return u
 int dn_patch_upload_f32(dn_ctx* c, int id, int field, const float* host) { return upload_impl(c, id, field, host); }
 int dn_patch_download(dn_ctx* c, int id, int field, double* host) { return download_impl(c, id, field, host); }
 int dn_patch_download_f32(dn_ctx* c, int id, int field, float* host) { return download_impl(c, id, field, host); }
+int dn_patch_upload_async(dn_ctx* c, int id, int field, const double* host) { return upload_async_impl(c, id, field, host); }
+int dn_patch_upload_f32_async(dn_ctx* c, int id, int field, const float* host) { return upload_async_impl(c, id, field, host); }
+int dn_patch_download_async(dn_ctx* c, int id, int field, double* host) { return download_async_impl(c, id, field, host); }
+int dn_patch_download_f32_async(dn_ctx* c, int id, int field, float* host) { return download_async_impl(c, id, field, host); }
 
 int dn_patch_set_active(dn_ctx* c, int id, const uint8_t* mask)
 {
@@ -1195,7 +1325,10 @@ int dn_sync(dn_ctx* c)
 {
   if (!c) return DN_ERR_ARG;
   if (set_device(c) != DN_OK) return DN_ERR_CUDA;
-  cudaError_t e = cudaStreamSynchronize(c->stream);
+  cudaError_t e = cudaSuccess;
+  if (c->s_in) e = cudaStreamSynchronize(c->s_in);
+  if (e == cudaSuccess && c->s_out) e = cudaStreamSynchronize(c->s_out);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
   if (e != cudaSuccess) return cuda_fail(c, e, "stream synchronize");
   return read_device_error(c);
 }

@@ -132,6 +132,23 @@ int dn_patch_upload_f32(dn_ctx* ctx, int patch_id, int field, const float* host)
 int dn_patch_download(dn_ctx* ctx, int patch_id, int field, double* host);
 int dn_patch_download_f32(dn_ctx* ctx, int patch_id, int field, float* host);
 
+/* Asynchronous forms of the four calls above: they return once the work is
+ * enqueued, and the host buffer must stay untouched (and, for the copy to
+ * overlap, pinned) until dn_sync.  Uploads copy on a copy-in stream and
+ * downloads on a copy-out stream, each through two device staging buffers;
+ * events keep them in order with the context's stream (an upload's
+ * conversion into the field waits for its copy, a download reads the field
+ * where the context's stream stood when it was called, and later work on the
+ * field waits for that read only).  So the download of step k, the upload of
+ * step k+1 and the stages of step k+1 overlap on the two copy engines and the
+ * SMs.  No reference counterpart (updateHost/updateDevice are synchronous,
+ * gpu_patchiterator.h:106-126); errors of the conversions surface at
+ * dn_sync. */
+int dn_patch_upload_async(dn_ctx* ctx, int patch_id, int field, const double* host);
+int dn_patch_upload_f32_async(dn_ctx* ctx, int patch_id, int field, const float* host);
+int dn_patch_download_async(dn_ctx* ctx, int patch_id, int field, double* host);
+int dn_patch_download_f32_async(dn_ctx* ctx, int patch_id, int field, float* host);
+
 /* Sets the active mask (1 = active, 0 = frozen) of a patch; NULL = all active.
  * Replaces: Patch::activate/deactivate (patch_common.h:502-504). */
 int dn_patch_set_active(dn_ctx* ctx, int patch_id, const uint8_t* mask);

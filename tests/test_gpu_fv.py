@@ -158,6 +158,49 @@ def test_upload_download_roundtrip():
                 assert np.abs(out[v] - U0[v]).max() <= scale * 2.0 ** -24, v
 
 
+@pytest.mark.parametrize("prec", [DN_FP64, DN_FP32])
+def test_async_transfer_pipeline_equals_synchronous_calls(prec):
+    # upload k+1 / stages k+1 / download k overlapping through the async
+    # calls give the same bits as the synchronous calls, every step
+    import ctypes
+    import torch
+    from drnum_b200 import _lib
+    U0, h, dt = cases.periodic_box(24)
+    ht = torch.float64 if prec == DN_FP64 else torch.float32
+    nt = np.float64 if prec == DN_FP64 else np.float32
+    ptr = _lib.dptr if prec == DN_FP64 else _lib.fptr
+    up_sync = "dn_patch_upload" if prec == DN_FP64 else "dn_patch_upload_f32"
+    dn_sync = "dn_patch_download" if prec == DN_FP64 else "dn_patch_download_f32"
+    alpha = np.ascontiguousarray(cases.RK3_ALPHA, dtype=np.float64)
+    results = []
+    for mode in ("sync", "async"):
+        patch = CartesianPatch(24, 24, 24, spacing=(h, h, h))
+        it = B200CartesianIterator(AusmPlus(), 0, prec)
+        it.addPatch(patch)
+        lib, ctx = it.lib, it.ctx
+        hin = [torch.empty(U0.shape, dtype=ht, pin_memory=True).numpy() for _ in range(2)]
+        hout = [torch.empty(U0.shape, dtype=ht, pin_memory=True).numpy() for _ in range(4)]
+        for b in hin:
+            b[...] = U0.astype(nt)
+        for k in range(4):
+            # step k starts from input (k % 2); the inputs hold the same state
+            if mode == "sync":
+                _lib.check(ctx, getattr(lib, up_sync)(ctx, 0, 0, ptr(hin[k % 2])))
+                _lib.check(ctx, lib.dn_rk_step(ctx, dt, _lib.dptr(alpha), 3))
+                _lib.check(ctx, getattr(lib, dn_sync)(ctx, 0, 0, ptr(hout[k])))
+            else:
+                _lib.check(ctx, getattr(lib, up_sync + "_async")(ctx, 0, 0, ptr(hin[k % 2])))
+                _lib.check(ctx, lib.dn_rk_step(ctx, dt, _lib.dptr(alpha), 3))
+                _lib.check(ctx, getattr(lib, dn_sync + "_async")(ctx, 0, 0, ptr(hout[k])))
+        _lib.check(ctx, lib.dn_sync(ctx))
+        results.append([o.copy() for o in hout])
+        it.close()
+    for k in range(4):
+        assert np.array_equal(results[0][k], results[1][k]), k
+        assert np.array_equal(results[1][k], results[1][0]), k
+    assert not np.array_equal(results[0][0], U0.astype(nt))
+
+
 def test_field_difference_matches_numpy():
     U0, h, dt = cases.periodic_box(16)
     patch = CartesianPatch(16, 16, 16, spacing=(h, h, h))
