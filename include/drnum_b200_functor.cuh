@@ -79,8 +79,15 @@ public:
     long long s = (long long)x;
     const long long n = (long long)m_N[a];
     if (m_Per[a]) {
-      s %= n;
-      return s < 0 ? s + n : s;
+      // stencils reach a few cells past the patch: one fold, a remainder
+      // only for indices further out
+      if (s < 0) s += n;
+      else if (s >= n) s -= n;
+      if (s < 0 || s >= n) {
+        s %= n;
+        if (s < 0) s += n;
+      }
+      return s;
     }
     return (s < 0 || s >= n) ? -1 : s;
   }
@@ -137,7 +144,7 @@ struct Args {
 };
 
 template <class OP, int TJ, int TK>
-__global__ void __launch_bounds__(TJ * TK)
+__global__ void __launch_bounds__(TJ * TK, 2)
 functor_stage_kernel(const Args a, OP op)
 {
   __shared__ Smem<TJ, TK> sm;
@@ -173,21 +180,32 @@ functor_stage_kernel(const Args a, OP op)
     } else {
       for (int v = 0; v < 5; ++v) fhi[v] = 0.0;
     }
-    for (int f = ty * TK + tx; f < (TJ + 1) * TK; f += TJ * TK) {
-      const int jj = f / TK, kk = f - jj * TK;
+    // y and z faces below the own cell; the faces below the halo row TJ and
+    // the halo column TK go to the last two warps, so that no warp
+    // evaluates more than one extra face per plane
+    auto y_face = [&](int jj, int kk) {
       const int jf = j0 + jj, kf = k0 + kk;
       double F[5] = {0, 0, 0, 0, 0};
       if (kf < nk && face_exists(jf, nj, py) && (py || jf < nj))
         op.yField(&P, (size_t)i, (size_t)jf, (size_t)kf, xc, 0.5*dy + jf*dy, 0.5*dz + kf*dz, Ay, F);
       for (int v = 0; v < 5; ++v) sm.fy[v][jj][kk] = F[v];
-    }
-    for (int f = ty * TK + tx; f < TJ * (TK + 1); f += TJ * TK) {
-      const int jj = f / (TK + 1), kk = f - jj * (TK + 1);
+    };
+    auto z_face = [&](int jj, int kk) {
       const int jf = j0 + jj, kf = k0 + kk;
       double F[5] = {0, 0, 0, 0, 0};
       if (jf < nj && face_exists(kf, nk, pz) && (pz || kf < nk))
         op.zField(&P, (size_t)i, (size_t)jf, (size_t)kf, xc, 0.5*dy + jf*dy, 0.5*dz + kf*dz, Az, F);
       for (int v = 0; v < 5; ++v) sm.fz[v][jj][kk] = F[v];
+    };
+    y_face(ty, tx);
+    z_face(ty, tx);
+    {
+      constexpr int NW = TJ * TK / 32;
+      const int warp = (ty * TK + tx) >> 5, lane = (ty * TK + tx) & 31;
+      if (warp == NW - 1)
+        for (int kk = lane; kk < TK; kk += 32) y_face(TJ, kk);
+      if (warp == (NW >= 2 ? NW - 2 : 0))
+        for (int jj = lane; jj < TJ; jj += 32) z_face(jj, TK);
     }
     __syncthreads();
     if (own) {
