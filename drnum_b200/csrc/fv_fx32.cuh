@@ -277,6 +277,16 @@ __device__ __forceinline__ float2 fx_slope2(float2 a, float2 b)
 // edge cell outward makes the van Albada slope of an edge cell exactly zero
 // (one of its differences vanishes), which is the reference's first-order
 // reconstruction at a closed patch edge (upwind2.h:39-42), with no test.
+// A face flux in whole quanta.  A face of 2^30 quanta or more (a single
+// face moving the offset by the whole representable range) or a flux that is
+// not finite would saturate or vanish in the int32 conversion; it is flagged
+// instead of passing silently.
+__device__ __forceinline__ int fx_quant(float x, bool& bad)
+{
+  bad |= !(fabsf(x) < 1073741824.0f);
+  return __float2int_rn(x);
+}
+
 __device__ __forceinline__ int fx_index(int x, int n, int per)
 {
   if (per) {
@@ -437,6 +447,7 @@ __device__ __forceinline__ void fx_stage_tile_impl(const FxArgs& a, int j0, int 
 
   // x direction registers: left state of the face above the current cell,
   // the downwind difference of the current cell, and the lower face integers
+  bool fbad = false;     // a face flux left the fixed-point range (fx_quant)
   Prim xleft;
   float xb[5];           // U_{i+1} - U_i of the own column (becomes a of cell i+1)
   int qx_lo[5];
@@ -471,7 +482,7 @@ __device__ __forceinline__ void fx_stage_tile_impl(const FxArgs& a, int j0, int 
       float F[5];
       fx_ausm<0>(fx_prim(Lm[0], Lm[1], Lm[2], Lm[3], Lm[4]), fx_prim(Sm[0], Sm[1], Sm[2], Sm[3], Sm[4]), P.Ax, F);
       #pragma unroll
-      for (int v = 0; v < 5; ++v) qx_lo[v] = __float2int_rn(F[v] * P.face_scale[v]);
+      for (int v = 0; v < 5; ++v) qx_lo[v] = fx_quant(F[v] * P.face_scale[v], fbad);
     } else {
       #pragma unroll
       for (int v = 0; v < 5; ++v) qx_lo[v] = 0;
@@ -548,8 +559,8 @@ __device__ __forceinline__ void fx_stage_tile_impl(const FxArgs& a, int j0, int 
       #pragma unroll
       for (int v = 0; v < 5; ++v) {
         const float2 q = mul2(F[v], v2(P.face_scale[v]));
-        sm.qy[v][ty][tx] = exy ? __float2int_rn(q.x) : 0;
-        sm.qzL[v][ty][tx] = exz ? __float2int_rn(q.y) : 0;
+        sm.qy[v][ty][tx] = exy ? fx_quant(q.x, fbad) : 0;
+        sm.qzL[v][ty][tx] = exz ? fx_quant(q.y, fbad) : 0;
       }
     }
     // halo faces, y and z in pairs: below halo row TJ (col kk = h) and below
@@ -577,8 +588,8 @@ __device__ __forceinline__ void fx_stage_tile_impl(const FxArgs& a, int j0, int 
       #pragma unroll
       for (int v = 0; v < 5; ++v) {
         const float2 q = mul2(F[v], v2(P.face_scale[v]));
-        if (hy) sm.qy[v][TJ][h] = exy ? __float2int_rn(q.x) : 0;
-        if (hz) sm.qzT[v][z_warp<TK>(h)][zt_slot<TK>(h)] = exz ? __float2int_rn(q.y) : 0;
+        if (hy) sm.qy[v][TJ][h] = exy ? fx_quant(q.x, fbad) : 0;
+        if (hz) sm.qzT[v][z_warp<TK>(h)][zt_slot<TK>(h)] = exz ? fx_quant(q.y, fbad) : 0;
       }
     }
     // ---------------- x: face above cell i (between i and i+1); plane i+2
@@ -601,7 +612,7 @@ __device__ __forceinline__ void fx_stage_tile_impl(const FxArgs& a, int j0, int 
         float F[5];
         fx_ausm<0>(xleft, fx_prim(Sm[0], Sm[1], Sm[2], Sm[3], Sm[4]), P.Ax, F);
         #pragma unroll
-        for (int v = 0; v < 5; ++v) qx_hi[v] = __float2int_rn(F[v] * P.face_scale[v]);
+        for (int v = 0; v < 5; ++v) qx_hi[v] = fx_quant(F[v] * P.face_scale[v], fbad);
       } else {
         #pragma unroll
         for (int v = 0; v < 5; ++v) qx_hi[v] = 0;
@@ -633,7 +644,7 @@ __device__ __forceinline__ void fx_stage_tile_impl(const FxArgs& a, int j0, int 
         #pragma unroll
         for (int v = 0; v < 5; ++v) uc[v] = fmaf(P.quantum[v], (float)a.in[v * ncv + c], P.base[v]);
         add_wall_fluxes(a.wall, g.ni, g.nj, g.nk, g.per_x, g.per_y, g.per_z, i, j, k, uc, P.Ax, P.Ay, P.Az, res,
-                        [&](int v, float F) { return __float2int_rn(F * P.face_scale[v]); });
+                        [&](int v, float F) { return fx_quant(F * P.face_scale[v], fbad); });
       }
       #pragma unroll
       for (int v = 0; v < 5; ++v) {
@@ -673,6 +684,7 @@ __device__ __forceinline__ void fx_stage_tile_impl(const FxArgs& a, int j0, int 
     fetch_un(i + 1);
     issue(i + 4);
   }
+  if (fbad && a.err) atomicOr(a.err, 16);
 }
 
 template <int TJ, int TK>

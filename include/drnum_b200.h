@@ -118,8 +118,11 @@ int dn_patch_set_bc(dn_ctx* ctx, int patch_id, int side, int kind, const double*
 
 /* DN_FP32 only: FP64 base state the FP32 offsets are stored against, and the
  * per-variable offset quantum is derived from `range` (the largest expected
- * |U - base| per variable).  Optional; dn_patch_upload derives both from the
- * uploaded data when this was not called. */
+ * |U - base| per variable, which for the momenta must also cover the scale
+ * of the pressure flux, rho*(|u| + a)).  Optional; dn_patch_upload derives
+ * both from the uploaded data when this was not called (range = 4 x max
+ * |rho|, rho*(|u| + a), |rho E|).  A state or face flux outside the range is
+ * reported as DN_ERR_RANGE, never wrapped. */
 int dn_patch_set_base(dn_ctx* ctx, int patch_id, const double base[5], const double range[5]);
 
 /* Host -> device copy of field `field` of one patch, [5][ni][nj][nk].

@@ -40,6 +40,16 @@ def build(name):
         U = cases.random_state(3, 5, 4, seed=6, amp=0.02, mach=0.3)
         h = 1.0 / 16
         return dict(U0=U, h=h, dt=cases.cfl_dt(U, h, 0.5), steps=2, periodic=(False, False, False), active=None)
+    if name == "flat_8x2x9":
+        # a closed axis of two cells: no faces along it (cartesianiterator.h:160)
+        U = cases.random_state(8, 2, 9, seed=8, amp=0.02, mach=0.4)
+        h = 1.0 / 16
+        return dict(U0=U, h=h, dt=cases.cfl_dt(U, h, 0.5), steps=2, periodic=(True, False, True), active=None)
+    if name == "column_1x1x10":
+        # two closed axes of one cell: a 1-D problem along k
+        U = cases.random_state(1, 1, 10, seed=9, amp=0.02, mach=0.4)
+        h = 1.0 / 16
+        return dict(U0=U, h=h, dt=cases.cfl_dt(U, h, 0.5), steps=3, periodic=(False, False, True), active=None)
     if name == "transonic_10":
         # Mach ~1 with strong perturbations: faces on both sides of |M| = 1
         # (van Leer's supersonic branches, Roe's sonic entropy modification)
@@ -53,7 +63,8 @@ def build(name):
 
 
 # full-field fixtures (small); the 64^3 x 100 case stores a digest
-FULL = ["rough_8", "ragged_12x10x9", "vortex_16", "closed_10x7x12", "masked_9", "thin_3x5x4"]
+FULL = ["rough_8", "ragged_12x10x9", "vortex_16", "closed_10x7x12", "masked_9", "thin_3x5x4", "flat_8x2x9",
+        "column_1x1x10"]
 DIGEST = ["cfg1_64_100"]
 
 # Euler flux schemes of the generic functor path (numbered as DN_FLUX_*) and

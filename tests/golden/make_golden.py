@@ -3,6 +3,7 @@
     python tests/golden/make_golden.py              # single-patch fixtures + grids
     python tests/golden/make_golden.py --grids      # grids only
     python tests/golden/make_golden.py --schemes    # VanLeer / Roe fixtures
+    python tests/golden/make_golden.py --cases a,b  # the named single-patch fixtures only
 
 Needs oracle/_ref/libdrnum_ref.so, i.e. the reference DrNUM library compiled
 (FP64) from its own sources by oracle/build_ref.sh.  Each fixture stores the
@@ -34,9 +35,11 @@ def digest(a: np.ndarray) -> str:
     return hashlib.sha256(np.ascontiguousarray(a, dtype=np.float64).tobytes()).hexdigest()
 
 
-def main():
+def main(only=None):
     assert pyoracle.ref_lib().dnref_real_size() == 8
     for name in cases_def.FULL:
+        if only is not None and name not in only:
+            continue
         c = cases_def.build(name)
         out, sec = pyoracle.ref_run(c["U0"], c["h"], c["dt"], c["steps"], cases_def.ALPHA,
                                     c["periodic"], c["active"], threads=1)
@@ -45,6 +48,8 @@ def main():
                             active=c["active"] if c["active"] is not None else np.ones(0, np.uint8),
                             alpha=np.array(cases_def.ALPHA))
         print(f"{name}: {sec:.3f} s")
+    if only is not None:
+        return
     meta = {}
     for name in cases_def.DIGEST:
         c = cases_def.build(name)
@@ -135,5 +140,7 @@ if __name__ == "__main__":
         make_grids()
     elif "--schemes" in sys.argv:
         make_schemes()
+    elif "--cases" in sys.argv:
+        main(only=set(sys.argv[sys.argv.index("--cases") + 1].split(",")))
     else:
         main()
