@@ -565,7 +565,8 @@ __device__ __forceinline__ void fx_stage_tile_impl(const FxArgs& a, int j0, int 
     }
     // halo faces, y and z in pairs: below halo row TJ (col kk = h) and below
     // halo col TK (row jj = h)
-    for (int h = tid; h < (TK > TJ ? TK : TJ); h += NT) {
+    // (on the second warp: the first one did the halo slopes of this plane)
+    for (int h = (tid + NT - 32) % NT; h < (TK > TJ ? TK : TJ); h += NT) {
       const bool hy = h < TK, hz = h < TJ;
       bool exy = hy, exz = hz;
       if (!FULL) {
