@@ -119,6 +119,44 @@ public:
   {
     getVar(field, i, j, k, var);
   }
+  /* Gradient along axis A at cell (i, j, k): central difference, one-sided
+     where a neighbour lies outside a closed axis (the difference is then
+     taken to the cell itself with the doubled factor), as
+     CartesianPatch::getXGrad/getYGrad/getZGrad (cartesianpatch_common.h:
+     188-312, whose y form alone returns zero on an axis of two cells or
+     fewer); the viscous functors read their transverse gradients here. */
+  template <int A>
+  __device__ __forceinline__ void grad(size_t field, size_t i, size_t j, size_t k, double* g) const
+  {
+    if (A == 1 && m_N[1] <= 2) {
+      for (int v = 0; v < 5; ++v) g[v] = 0;
+      return;
+    }
+    const size_t c[3] = {i, j, k};
+    double D = 0.5/m_D[A];
+    size_t n1 = c[A] - 1, n2 = c[A] + 1;
+    if (axis(A, n1) < 0) { n1 = c[A]; D *= 2; }
+    if (axis(A, n2) < 0) { n2 = c[A]; D *= 2; }
+    size_t a1[3] = {i, j, k}, a2[3] = {i, j, k};
+    a1[A] = n1;
+    a2[A] = n2;
+    double v1[5];
+    getVar(field, a2[0], a2[1], a2[2], g);
+    getVar(field, a1[0], a1[1], a1[2], v1);
+    for (int v = 0; v < 5; ++v) {
+      g[v] -= v1[v];
+      g[v] *= D;
+    }
+  }
+  template <typename DIMT>
+  __device__ __forceinline__ void getXGrad(DIMT, size_t field, size_t i, size_t j, size_t k, double* g) const
+  { grad<0>(field, i, j, k, g); }
+  template <typename DIMT>
+  __device__ __forceinline__ void getYGrad(DIMT, size_t field, size_t i, size_t j, size_t k, double* g) const
+  { grad<1>(field, i, j, k, g); }
+  template <typename DIMT>
+  __device__ __forceinline__ void getZGrad(DIMT, size_t field, size_t i, size_t j, size_t k, double* g) const
+  { grad<2>(field, i, j, k, g); }
 };
 
 namespace functor_detail {

@@ -41,3 +41,22 @@ for p in $pids; do wait $p; done
 $CXX $FLAGS -c "$HERE/ref_driver.cpp" -o "$OUT/obj/ref_driver.o"
 $CXX -shared -o "$OUT/libdrnum_ref.so" $OBJS "$OUT/obj/ref_driver.o" -L/usr/lib/gcc/x86_64-linux-gnu/13 -lgomp -lpthread
 echo "built $OUT/libdrnum_ref.so"
+
+# The reference's flux functors compiled for the device (sm_100a) against this
+# repository's generic functor stage.  nvcc has no -I- split, so the headers
+# are reached through a tree of symbolic links to the reference's files in
+# $OUT/tree, with the generated FP64 drnum.h in place of the original.
+if command -v nvcc > /dev/null 2>&1; then
+  rm -rf "$OUT/tree"
+  mkdir -p "$OUT/tree"
+  (cd "$LIB" && find . -type d) | while read -r d; do mkdir -p "$OUT/tree/$d"; done
+  (cd "$LIB" && find . -type f -name '*.h') | while read -r f; do ln -s "$LIB/$f" "$OUT/tree/$f"; done
+  rm -f "$OUT/tree/drnum.h"
+  cp "$OUT/gen/drnum.h" "$OUT/tree/drnum.h"
+  nvcc -gencode arch=compute_100a,code=sm_100a -O3 -std=c++14 -fmad=false -shared -Xcompiler -fPIC -w \
+       -include "$HERE/ref_fp64_shim.h" -I"$OUT/tree" -I"$HERE/ref_stubs" -I"$OUT/tree/fluxes" \
+       -I"$OUT/tree/reconstruction" -I"$OUT/tree/iterators" -I"$OUT/tree/math" -I"$HERE/../include" \
+       "$HERE/ref_functor_stage.cu" -o "$OUT/libref_functor_stage.so"
+  rm -rf "$OUT/tree"
+  echo "built $OUT/libref_functor_stage.so"
+fi

@@ -23,6 +23,7 @@
 #include "fluxes/ausmplus.h"
 #include "fluxes/vanleer.h"
 #include "fluxes/roe.h"
+#include "fluxes/compressibleviscflux.h"
 #include "fluxes/compressiblefarfieldflux.h"
 #include "fluxes/compressibleslipflux.h"
 #include "reconstruction/upwind1.h"
@@ -56,6 +57,18 @@ namespace {
 typedef AusmPlus<5, Upwind2<5, VanAlbada>, PerfectGas> RefAusm;
 typedef VanLeer<5, Upwind2<5, VanAlbada>, PerfectGas> RefVanLeer;
 typedef Roe<5, Upwind2<5, VanAlbada>, PerfectGas> RefRoe;
+typedef CompressibleViscFlux<5, PerfectGas> RefVisc;
+
+// The field fluxes of the jet application's JetFlux: the Euler flux, then
+// the viscous flux (applications/drnumJetDemo/jetflux.h:101-114).
+struct RefVanLeerVisc
+{
+  RefVanLeer m_Euler;
+  RefVisc m_Visc;
+  template <typename P> void xField(P* p, size_t i, size_t j, size_t k, real x, real y, real z, real A, real* f) { m_Euler.xField(p, i, j, k, x, y, z, A, f); m_Visc.xField(p, i, j, k, x, y, z, A, f); }
+  template <typename P> void yField(P* p, size_t i, size_t j, size_t k, real x, real y, real z, real A, real* f) { m_Euler.yField(p, i, j, k, x, y, z, A, f); m_Visc.yField(p, i, j, k, x, y, z, A, f); }
+  template <typename P> void zField(P* p, size_t i, size_t j, size_t k, real x, real y, real z, real A, real* f) { m_Euler.zField(p, i, j, k, x, y, z, A, f); m_Visc.zField(p, i, j, k, x, y, z, A, f); }
+};
 
 // Flux functor with one of the reference's Euler field fluxes and zero
 // patch-face fluxes (the ghost layers of periodic axes overwrite the outer
@@ -291,7 +304,8 @@ int dnref_run(int ni, int nj, int nk, const int* periodic, double hx, double hy,
 }
 
 // dnref_run with the Euler flux `scheme`: 0 AusmPlus, 2 VanLeer, 3 Roe (the
-// numbering of DN_FLUX_*; all with Upwind2<5, VanAlbada> and PerfectGas).
+// numbering of DN_FLUX_*; all with Upwind2<5, VanAlbada> and PerfectGas), and
+// 4 VanLeer plus CompressibleViscFlux.
 int dnref_run_scheme(int scheme, int ni, int nj, int nk, const int* periodic, double hx, double hy, double hz,
                      const double* init, const unsigned char* active, int steps, double dt,
                      const double* alpha, int n_alpha, int threads, double* out, double* seconds)
@@ -306,6 +320,9 @@ int dnref_run_scheme(int scheme, int ni, int nj, int nk, const int* periodic, do
     case 3:
       return run_impl<RefRoe>(ni, nj, nk, periodic, hx, hy, hz, init, active, steps, dt, alpha, n_alpha, threads,
                               out, seconds);
+    case 4:
+      return run_impl<RefVanLeerVisc>(ni, nj, nk, periodic, hx, hy, hz, init, active, steps, dt, alpha, n_alpha,
+                                      threads, out, seconds);
     default:
       return -3;
   }

@@ -56,6 +56,16 @@ def build(name):
         U = cases.random_state(10, 10, 10, seed=7, amp=0.08, mach=1.0)
         h = 1.0 / 16
         return dict(U0=U, h=h, dt=cases.cfl_dt(U, h, 0.4), steps=2, periodic=(True, True, True), active=None)
+    if name == "micro_12":
+        # micrometre cells: the viscous stresses are about 1 % of the pressure
+        # fluxes, so the viscous functor shows in every cell
+        U = cases.random_state(12, 12, 12, seed=12, amp=0.02, mach=0.3)
+        h = 2e-6
+        return dict(U0=U, h=h, dt=cases.cfl_dt(U, h, 0.4), steps=3, periodic=(True, True, True), active=None)
+    if name == "micro_closed_10x8x9":
+        U = cases.random_state(10, 8, 9, seed=13, amp=0.02, mach=0.3)
+        h = 2e-6
+        return dict(U0=U, h=h, dt=cases.cfl_dt(U, h, 0.4), steps=3, periodic=(False, True, False), active=None)
     if name == "cfg1_64_100":
         U, h, dt = cases.periodic_box(64)
         return dict(U0=U, h=h, dt=dt, steps=100, periodic=(True, True, True), active=None)
@@ -71,6 +81,12 @@ DIGEST = ["cfg1_64_100"]
 # the single-patch cases each is pinned on; the bc_box grid is pinned too
 SCHEMES = {"vanleer": 2, "roe": 3}
 SCHEME_CASES = ["vortex_16", "closed_10x7x12", "masked_9", "thin_3x5x4", "transonic_10"]
+
+# the reference's own VanLeer + CompressibleViscFlux functors (the field
+# fluxes of its jet application), compiled for the device against the
+# generic functor stage (oracle/ref_functor_stage.cu), pinned on these cases
+VISC_SCHEME = 4
+VISC_CASES = ["micro_12", "micro_closed_10x8x9", "vortex_16"]
 
 
 # ------------------------------------------------------------------ patch grids
