@@ -159,12 +159,15 @@ __device__ __forceinline__ void fx_ausm(const Prim& L, const Prim& R, float A, f
   F[4] = fmaf(cp, L.H, cm * R.H);
 }
 
-// van Albada slope shared by both face-side states of a cell
+// Twice the van Albada slope shared by both face-side states of a cell,
+// 2 s = a b (a + b) / (a^2 + b^2); the face states are U +- 0.5 * (2 s), one
+// multiply-add each.  The denominator carries 1e-30, far below any nonzero
+// a^2 + b^2 of offsets of at least one quantum, so that a = b = 0 gives 0
+// without a test.
 __device__ __forceinline__ float fx_slope(float a, float b)
 {
-  const float den = fmaf(a, a, b * b);
-  const float num = 0.5f * a * b * (a + b);
-  return den > 1e-30f ? __fdividef(num, den) : 0.0f;
+  const float den = fmaf(a, a, fmaf(b, b, 1e-30f));
+  return a * b * (a + b) * __fdividef(1.0f, den);
 }
 
 // ---------------------------------------------------------------------------
@@ -263,13 +266,11 @@ __device__ __forceinline__ void fx_ausm2(const Prim2& L, const Prim2& R, float2 
   F[4] = fma2(cp, L.H, mul2(cm, R.H));
 }
 
-// van Albada slopes of a pair of (a, b) differences
+// fx_slope (twice the van Albada slope) of a pair of (a, b) differences
 __device__ __forceinline__ float2 fx_slope2(float2 a, float2 b)
 {
-  const float2 den = fma2(a, a, mul2(b, b));
-  const float2 num = mul2(mul2(mul2(v2(0.5f), a), b), add2(a, b));
-  const float2 q = mul2(num, rcp2(den));
-  return make_float2(den.x > 1e-30f ? q.x : 0.0f, den.y > 1e-30f ? q.y : 0.0f);
+  const float2 den = fma2(a, a, fma2(b, b, v2(1e-30f)));
+  return mul2(mul2(mul2(a, b), add2(a, b)), rcp2(den));
 }
 
 // Cell whose state stands at index x of an axis: the wrapped cell on a
@@ -463,8 +464,8 @@ __device__ __forceinline__ void fx_stage_tile_impl(const FxArgs& a, int j0, int 
       const float up = PL(s_p1, v, ty + 2, tx + 2);
       const float s = fx_slope(uc - um, up - uc);
       U0[v] = uc;
-      Sp[v] = uc + s;
-      Sm[v] = uc - s;
+      Sp[v] = fmaf(s, 0.5f, uc);
+      Sm[v] = fmaf(s, -0.5f, uc);
       xb[v] = up - uc;
       Ul[v] = um;
     }
@@ -477,7 +478,7 @@ __device__ __forceinline__ void fx_stage_tile_impl(const FxArgs& a, int j0, int 
       #pragma unroll
       for (int v = 0; v < 5; ++v) {
         const float umm = fmaf(P.quantum[v], (float)__ldg(a.in + (int64_t)v * nc + (int64_t)iw2 * njk + (int64_t)j * g.nk + k), P.base[v]);
-        Lm[v] = Ul[v] + fx_slope(Ul[v] - umm, U0[v] - Ul[v]);
+        Lm[v] = fmaf(fx_slope(Ul[v] - umm, U0[v] - Ul[v]), 0.5f, Ul[v]);
       }
       float F[5];
       fx_ausm<0>(fx_prim(Lm[0], Lm[1], Lm[2], Lm[3], Lm[4]), fx_prim(Sm[0], Sm[1], Sm[2], Sm[3], Sm[4]), P.Ax, F);
@@ -501,10 +502,10 @@ __device__ __forceinline__ void fx_stage_tile_impl(const FxArgs& a, int j0, int 
         const float2 ul = make_float2(PL(s0, v, ty + 1, tx + 2), PL(s0, v, ty + 2, tx + 1));
         const float2 uh = make_float2(PL(s0, v, ty + 3, tx + 2), PL(s0, v, ty + 2, tx + 3));
         const float2 s = fx_slope2(sub2(uc, ul), sub2(uh, uc));
-        const float2 up = add2(uc, s);
+        const float2 up = fma2(s, v2(0.5f), uc);
         sm.sy[v][ty + 1][tx] = up.x;
         sm.szL[v][ty][tx] = up.y;
-        yzm[v] = sub2(uc, s);
+        yzm[v] = fma2(s, v2(-0.5f), uc);
       }
     }
     // halo cells, y and z in pairs: y rows -1 (left state) and TJ (right
@@ -526,7 +527,7 @@ __device__ __forceinline__ void fx_stage_tile_impl(const FxArgs& a, int j0, int 
         const float2 ul = make_float2(PL(s0, v, ry - 1, cy), PL(s0, v, rz, cz - 1));
         const float2 uh = make_float2(PL(s0, v, ry + 1, cy), PL(s0, v, rz, cz + 1));
         const float2 s = fx_slope2(sub2(uc, ul), sub2(uh, uc));
-        const float2 up = add2(uc, s), dn = sub2(uc, s);
+        const float2 up = fma2(s, v2(0.5f), uc), dn = fma2(s, v2(-0.5f), uc);
         if (hy) {
           if (topy) sm.sy_top[v][kky] = dn.x;
           else sm.sy[v][0][kky] = up.x;
@@ -605,8 +606,8 @@ __device__ __forceinline__ void fx_stage_tile_impl(const FxArgs& a, int j0, int 
         const float up = PL(sp2, v, ty + 2, tx + 2);
         const float b = up - uc;
         const float s = fx_slope(xb[v], b);
-        Sm[v] = uc - s;
-        Sp[v] = uc + s;
+        Sm[v] = fmaf(s, -0.5f, uc);
+        Sp[v] = fmaf(s, 0.5f, uc);
         xb[v] = b;
       }
       if (ex) {
