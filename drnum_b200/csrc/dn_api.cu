@@ -18,6 +18,7 @@
 #include "fv_batch.cuh"
 #include "fv_schemes.cuh"
 #include "dn_gridio.h"
+#include <nvtx3/nvToolsExt.h>
 
 #include <cmath>
 #include <cstdarg>
@@ -28,6 +29,15 @@
 #include <vector>
 
 namespace {
+
+// NVTX range over a scope: the library's host-side phases appear by name in
+// Nsight timelines (no cost unless a tool is attached)
+struct NvtxRange {
+  explicit NvtxRange(const char* name) { nvtxRangePushA(name); }
+  ~NvtxRange() { nvtxRangePop(); }
+  NvtxRange(const NvtxRange&) = delete;
+  NvtxRange& operator=(const NvtxRange&) = delete;
+};
 
 struct DnPatch {
   dn_patch_desc d;
@@ -574,6 +584,7 @@ int build_ls_plan(dn_ctx* c)
 // Level-set slip-wall condition on physical buffer `b` of every patch.
 int levelset_bc(dn_ctx* c, int b)
 {
+  NvtxRange nvtx("dn level-set wall");
   bool any = false;
   for (char on : c->ls_on) any = any || on;
   if (!any) return DN_OK;
@@ -588,6 +599,7 @@ int levelset_bc(dn_ctx* c, int b)
 // Donor copy into physical buffer `b` of every patch.
 int donor_copy(dn_ctx* c, int b)
 {
+  NvtxRange nvtx("dn donor copy");
   if (!has_donors(c)) return DN_OK;
   int s;
   if (c->plan_dirty && (s = build_plan(c))) return s;
@@ -808,6 +820,7 @@ int stage_patch(dn_ctx* c, DnPatch& p, int in_b, int un_b, int out_b, double fac
 // One RK stage of every patch: in_b -> out_b with step-start state un_b.
 int stage_all(dn_ctx* c, int in_b, int un_b, int out_b, double factor)
 {
+  NvtxRange nvtx("dn stage");
   // a single patch keeps its parameters in the kernel's constant bank (the
   // batched form reads them from shared memory); the results are identical.
   // Flux functors (another scheme or a user stage function) run per patch.
@@ -916,6 +929,7 @@ int stage_patch(dn_ctx* c, DnPatch& p, int in_b, int un_b, int out_b, double fac
 template <typename H>
 int upload_impl(dn_ctx* c, int id, int field, const H* host)
 {
+  NvtxRange nvtx("dn upload");
   int s = check_patch(c, id);
   if (s) return s;
   if ((s = check_field(c, field))) return s;
@@ -955,6 +969,7 @@ int upload_impl(dn_ctx* c, int id, int field, const H* host)
 template <typename H>
 int download_impl(dn_ctx* c, int id, int field, H* host)
 {
+  NvtxRange nvtx("dn download");
   int s = check_patch(c, id);
   if (s) return s;
   if ((s = check_field(c, field))) return s;
@@ -1015,6 +1030,7 @@ int ensure_buffer(dn_ctx* c, void*& buf, size_t& cap, size_t bytes)
 template <typename H>
 int upload_async_impl(dn_ctx* c, int id, int field, const H* host)
 {
+  NvtxRange nvtx("dn upload (async)");
   int s = check_patch(c, id);
   if (s) return s;
   if ((s = check_field(c, field))) return s;
@@ -1059,6 +1075,7 @@ int upload_async_impl(dn_ctx* c, int id, int field, const H* host)
 template <typename H>
 int download_async_impl(dn_ctx* c, int id, int field, H* host)
 {
+  NvtxRange nvtx("dn download (async)");
   int s = check_patch(c, id);
   if (s) return s;
   if ((s = check_field(c, field))) return s;
@@ -1306,6 +1323,7 @@ int dn_compute(dn_ctx* c, double factor)
 int dn_rk_step(dn_ctx* c, double dt, const double* alpha, int n_alpha)
 {
   if (!c) return DN_ERR_ARG;
+  NvtxRange nvtx("dn_rk_step");
   if (!alpha || n_alpha < 1 || n_alpha > 16) return fail(c, DN_ERR_ARG, "need 1..16 RK stage coefficients");
   if (!std::isfinite(dt)) return fail(c, DN_ERR_ARG, "dt is not finite");
   for (int q = 0; q < n_alpha; ++q) if (!std::isfinite(alpha[q])) return fail(c, DN_ERR_ARG, "alpha not finite");
@@ -1480,6 +1498,7 @@ int dn_patch_set_bc(dn_ctx* c, int id, int side, int kind, const double* params,
 
 int dn_grid_compute_dependencies(dn_ctx* c, int64_t* no_donor)
 {
+  NvtxRange nvtx("dn overlap set-up");
   if (!c) return DN_ERR_ARG;
   std::vector<dn::OverlapPatch> ops;
   for (const DnPatch& p : c->patches) ops.push_back(dn::overlap_patch(p.d));
@@ -1749,6 +1768,7 @@ int exchange_device_lists(dn_ctx* c, dn_exchange* e)
 
 int exchange_move(dn_ctx* c, dn_exchange* e, int field, int peer, void* buf, bool pack)
 {
+  NvtxRange nvtx("dn exchange");
   if (!c || !e) return DN_ERR_ARG;
   int s;
   if ((s = check_field(c, field))) return s;
@@ -1923,6 +1943,7 @@ void write_tune_cache(const char* path, const std::string& dev, int precision, c
 
 int dn_autotune(dn_ctx* c, const char* cache_path, double cost_out[2])
 {
+  NvtxRange nvtx("dn autotune");
   if (!c) return DN_ERR_ARG;
   if (c->patches.empty()) return fail(c, DN_ERR_STATE, "no patches to tune for");
   if (set_device(c) != DN_OK) return DN_ERR_CUDA;

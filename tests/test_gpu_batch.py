@@ -66,3 +66,15 @@ def test_autotune_cache_is_reused(tmp_path):
     it.close()
     assert np.array_equal(c1, c2)
     assert len(path.read_text().strip().splitlines()) == 1
+
+
+@pytest.mark.parametrize("precision", [DN_FP64, DN_FP32])
+def test_runs_are_deterministic(precision):
+    # the same case twice on fresh contexts: bit-identical states (owner-computes
+    # residuals, no atomics on the state, fixed summation orders)
+    a, _ = _run("bc_box", precision, 5, graph=1)
+    b, _ = _run("bc_box", precision, 5, graph=1)
+    c, _ = _run("octants_jet", precision, 3)
+    d, _ = _run("octants_jet", precision, 3)
+    for x, y in zip(a + c, b + d):
+        assert np.array_equal(x, y)
