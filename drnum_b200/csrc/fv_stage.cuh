@@ -81,7 +81,7 @@ struct StageSmem {
   using FaceT = typename Policy::FaceT;
   static constexpr int PJ = TJ + 4;
   static constexpr int PK = TK + 4;
-  Real plane[4][5][PJ][PK];
+  Real plane[3][5][PJ][PK];   // planes i .. i+2 (plane i-1 of the own column is kept in registers)
   FaceT fy[5][TJ + 1][TK];
   FaceT fz[5][TJ][TK + 1];
 };
@@ -130,8 +130,12 @@ __device__ __forceinline__ void fv_stage_tile(const StageArgs<Policy>& a, int j0
   const size_t nc = (size_t)g.ni * g.nj * g.nk;
   const Real Ax = a.p.Ax, Ay = a.p.Ay, Az = a.p.Az;
 
-  // prologue: planes i0-2 .. i0+1 and the x face below cell i0
-  for (int q = -2; q <= 1; ++q) load_plane<Policy, TJ, TK>(sm, (i0 + q + 8) & 3, a.in, a.p, g, i0 + q, j0, k0);
+  // a three-plane ring, slot of plane p = p mod 3, rotated by hand: sa, sb,
+  // sc hold planes i-1, i, i+1 at the top of iteration i
+  int sa = (i0 + 2) % 3, sb = i0 % 3, sc = (i0 + 1) % 3;
+  // prologue: planes i0-1 .. i0+1 and the x face below cell i0; the own
+  // column of plane i0-2 comes straight from memory
+  for (int q = -1; q <= 1; ++q) load_plane<Policy, TJ, TK>(sm, (i0 + q + 3) % 3, a.in, a.p, g, i0 + q, j0, k0);
   __syncthreads();
 
   FaceT fx_lo[5];
@@ -141,12 +145,13 @@ __device__ __forceinline__ void fv_stage_tile(const StageArgs<Policy>& a, int j0
       Real vl[5], vr[5], F[5];
       const bool sl = cell_ok(i0 - 2, g.ni, g.per_x);
       const bool sr = cell_ok(i0 + 1, g.ni, g.per_x);
+      const int im2 = axis_idx(i0 - 2, g.ni, g.per_x);
       #pragma unroll
       for (int v = 0; v < 5; ++v) {
-        const Real um2 = sm.plane[(i0 + 6) & 3][v][ty + 2][tx + 2];
-        const Real um1 = sm.plane[(i0 + 7) & 3][v][ty + 2][tx + 2];
-        const Real up0 = sm.plane[(i0 + 8) & 3][v][ty + 2][tx + 2];
-        const Real up1 = sm.plane[(i0 + 9) & 3][v][ty + 2][tx + 2];
+        const Real um2 = sl ? Policy::load(a.p, v, a.in[v * nc + ((size_t)im2 * g.nj + j) * g.nk + k]) : Real(0);
+        const Real um1 = sm.plane[sa][v][ty + 2][tx + 2];
+        const Real up0 = sm.plane[sb][v][ty + 2][tx + 2];
+        const Real up1 = sm.plane[sc][v][ty + 2][tx + 2];
         vl[v] = upwind2_left(um2, um1, up0, sl);
         vr[v] = upwind2_right(um1, up0, up1, sr);
       }
@@ -160,11 +165,15 @@ __device__ __forceinline__ void fv_stage_tile(const StageArgs<Policy>& a, int j0
   }
 
   for (int i = i0; i < i1; ++i) {
-    // plane i+2 replaces plane i-2 in the ring
+    // plane i+2 replaces plane i-1 in the ring; the own column of plane i-1
+    // (the x face above cell i reads it) moves to registers first
+    Real xm1[5];
+    #pragma unroll
+    for (int v = 0; v < 5; ++v) xm1[v] = sm.plane[sa][v][ty + 2][tx + 2];
     __syncthreads();
-    load_plane<Policy, TJ, TK>(sm, (i + 2) & 3, a.in, a.p, g, i + 2, j0, k0);
+    load_plane<Policy, TJ, TK>(sm, sa, a.in, a.p, g, i + 2, j0, k0);
     __syncthreads();
-    const int sm1 = (i + 3) & 3, s0 = i & 3, sp1 = (i + 1) & 3, sp2 = (i + 2) & 3;
+    const int s0 = sb, sp1 = sc, sp2 = sa;
 
     // x face above cell i (between i and i+1), own column
     FaceT fx_hi[5];
@@ -176,7 +185,7 @@ __device__ __forceinline__ void fv_stage_tile(const StageArgs<Policy>& a, int j0
         const bool sr = cell_ok(i + 2, g.ni, g.per_x);
         #pragma unroll
         for (int v = 0; v < 5; ++v) {
-          const Real um2 = sm.plane[sm1][v][ty + 2][tx + 2];
+          const Real um2 = xm1[v];
           const Real um1 = sm.plane[s0][v][ty + 2][tx + 2];
           const Real up0 = sm.plane[sp1][v][ty + 2][tx + 2];
           const Real up1 = sm.plane[sp2][v][ty + 2][tx + 2];
@@ -297,6 +306,9 @@ __device__ __forceinline__ void fv_stage_tile(const StageArgs<Policy>& a, int j0
     }
     #pragma unroll
     for (int v = 0; v < 5; ++v) fx_lo[v] = fx_hi[v];
+    sa = sb;
+    sb = sc;
+    sc = sp2;
   }
 }
 
