@@ -202,7 +202,10 @@ __device__ __forceinline__ void fv_stage_tile(const StageArgs<Policy>& a, int j0
     }
 
     // y faces of plane i: face at row jj (0..TJ) lies below cell j0+jj
-    for (int f = ty * TK + tx; f < (TJ + 1) * TK; f += TJ * TK) {
+    // (the items beyond one per thread, the faces below halo row TJ, fall to
+    // the last warp, and those of the z loop below to the one before it, so
+    // that no warp evaluates more than one extra face per plane)
+    for (int f = (ty * TK + tx + 32) % (TJ * TK); f < (TJ + 1) * TK; f += TJ * TK) {
       const int jj = f / TK, kk = f - jj * TK;
       const int jf = j0 + jj, kf = k0 + kk;
       FaceT out[5];
@@ -232,7 +235,7 @@ __device__ __forceinline__ void fv_stage_tile(const StageArgs<Policy>& a, int j0
     }
 
     // z faces of plane i: face at column kk (0..TK) lies below cell k0+kk
-    for (int f = ty * TK + tx; f < TJ * (TK + 1); f += TJ * TK) {
+    for (int f = (ty * TK + tx + 64) % (TJ * TK); f < TJ * (TK + 1); f += TJ * TK) {
       const int jj = f / (TK + 1), kk = f - jj * (TK + 1);
       const int jf = j0 + jj, kf = k0 + kk;
       FaceT out[5];
