@@ -24,6 +24,7 @@
 #include "fluxes/vanleer.h"
 #include "fluxes/roe.h"
 #include "fluxes/compressibleviscflux.h"
+#include "fluxes/compressiblesmagorinskyflux.h"
 #include "fluxes/compressiblefarfieldflux.h"
 #include "fluxes/compressibleslipflux.h"
 #include "reconstruction/upwind1.h"
@@ -65,6 +66,19 @@ struct RefVanLeerVisc
 {
   RefVanLeer m_Euler;
   RefVisc m_Visc;
+  template <typename P> void xField(P* p, size_t i, size_t j, size_t k, real x, real y, real z, real A, real* f) { m_Euler.xField(p, i, j, k, x, y, z, A, f); m_Visc.xField(p, i, j, k, x, y, z, A, f); }
+  template <typename P> void yField(P* p, size_t i, size_t j, size_t k, real x, real y, real z, real A, real* f) { m_Euler.yField(p, i, j, k, x, y, z, A, f); m_Visc.yField(p, i, j, k, x, y, z, A, f); }
+  template <typename P> void zField(P* p, size_t i, size_t j, size_t k, real x, real y, real z, real A, real* f) { m_Euler.zField(p, i, j, k, x, y, z, A, f); m_Visc.zField(p, i, j, k, x, y, z, A, f); }
+};
+
+// The field fluxes of the base-flow application's BaseFlowFlux: Roe, then the
+// Smagorinsky flux with C_s = 0.24 (applications/drnumBaseFlowDemo/
+// baseflowflux.h:26-27).
+typedef CompressibleSmagorinskyFlux<5, 2400, PerfectGas> RefSmag;
+struct RefRoeSmag
+{
+  RefRoe m_Euler;
+  RefSmag m_Visc;
   template <typename P> void xField(P* p, size_t i, size_t j, size_t k, real x, real y, real z, real A, real* f) { m_Euler.xField(p, i, j, k, x, y, z, A, f); m_Visc.xField(p, i, j, k, x, y, z, A, f); }
   template <typename P> void yField(P* p, size_t i, size_t j, size_t k, real x, real y, real z, real A, real* f) { m_Euler.yField(p, i, j, k, x, y, z, A, f); m_Visc.yField(p, i, j, k, x, y, z, A, f); }
   template <typename P> void zField(P* p, size_t i, size_t j, size_t k, real x, real y, real z, real A, real* f) { m_Euler.zField(p, i, j, k, x, y, z, A, f); m_Visc.zField(p, i, j, k, x, y, z, A, f); }
@@ -305,7 +319,7 @@ int dnref_run(int ni, int nj, int nk, const int* periodic, double hx, double hy,
 
 // dnref_run with the Euler flux `scheme`: 0 AusmPlus, 2 VanLeer, 3 Roe (the
 // numbering of DN_FLUX_*; all with Upwind2<5, VanAlbada> and PerfectGas), and
-// 4 VanLeer plus CompressibleViscFlux.
+// 4 VanLeer plus CompressibleViscFlux, 5 Roe plus CompressibleSmagorinskyFlux.
 int dnref_run_scheme(int scheme, int ni, int nj, int nk, const int* periodic, double hx, double hy, double hz,
                      const double* init, const unsigned char* active, int steps, double dt,
                      const double* alpha, int n_alpha, int threads, double* out, double* seconds)
@@ -323,6 +337,9 @@ int dnref_run_scheme(int scheme, int ni, int nj, int nk, const int* periodic, do
     case 4:
       return run_impl<RefVanLeerVisc>(ni, nj, nk, periodic, hx, hy, hz, init, active, steps, dt, alpha, n_alpha,
                                       threads, out, seconds);
+    case 5:
+      return run_impl<RefRoeSmag>(ni, nj, nk, periodic, hx, hy, hz, init, active, steps, dt, alpha, n_alpha,
+                                  threads, out, seconds);
     default:
       return -3;
   }

@@ -88,6 +88,14 @@ SCHEME_CASES = ["vortex_16", "closed_10x7x12", "masked_9", "thin_3x5x4", "transo
 VISC_SCHEME = 4
 VISC_CASES = ["micro_12", "micro_closed_10x8x9", "vortex_16"]
 
+# the reference's own Roe + CompressibleSmagorinskyFlux<5, 2400> functors (the
+# field fluxes of its base-flow application), pinned the same way
+SMAG_SCHEME = 5
+SMAG_CASES = ["micro_12", "micro_closed_10x8x9", "vortex_16"]
+
+# fixture prefix -> (reference scheme number, cases) of the viscous functor sets
+VISCOUS_SETS = {"visc": (VISC_SCHEME, VISC_CASES), "smag": (SMAG_SCHEME, SMAG_CASES)}
+
 
 # ------------------------------------------------------------------ patch grids
 

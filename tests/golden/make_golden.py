@@ -2,7 +2,8 @@
 
     python tests/golden/make_golden.py              # single-patch fixtures + grids
     python tests/golden/make_golden.py --grids      # grids only
-    python tests/golden/make_golden.py --schemes    # VanLeer / Roe / VanLeer+viscous fixtures
+    python tests/golden/make_golden.py --schemes    # VanLeer / Roe / viscous fixtures
+    python tests/golden/make_golden.py --viscous smag   # one viscous set (visc, smag)
     python tests/golden/make_golden.py --cases a,b  # the named single-patch fixtures only
 
 Needs oracle/_ref/libdrnum_ref.so, i.e. the reference DrNUM library compiled
@@ -133,15 +134,24 @@ def make_schemes():
                       num_patches=np.array(len(patches)))
         np.savez_compressed(os.path.join(HERE, f"grid_{gname}_{sname}.npz"), **arrays)
         print(f"grid_{gname}_{sname}")
-    for name in cases_def.VISC_CASES:
-        c = cases_def.build(name)
-        out, sec = pyoracle.ref_run(c["U0"], c["h"], c["dt"], c["steps"], cases_def.ALPHA, c["periodic"],
-                                    c["active"], threads=1, scheme=cases_def.VISC_SCHEME)
-        np.savez_compressed(os.path.join(HERE, f"visc_{name}.npz"), U0=c["U0"], out=out, h=c["h"], dt=c["dt"],
-                            steps=c["steps"], periodic=np.array(c["periodic"], dtype=np.int8),
-                            active=np.ones(0, np.uint8), alpha=np.array(cases_def.ALPHA),
-                            scheme=np.array(cases_def.VISC_SCHEME))
-        print(f"visc_{name}: {sec:.3f} s")
+    make_viscous()
+
+
+def make_viscous(only=None):
+    """The reference's viscous functor sets (VanLeer + CompressibleViscFlux,
+    Roe + CompressibleSmagorinskyFlux) on their single-patch cases."""
+    for prefix, (scheme, names) in cases_def.VISCOUS_SETS.items():
+        if only and prefix not in only:
+            continue
+        for name in names:
+            c = cases_def.build(name)
+            out, sec = pyoracle.ref_run(c["U0"], c["h"], c["dt"], c["steps"], cases_def.ALPHA, c["periodic"],
+                                        c["active"], threads=1, scheme=scheme)
+            np.savez_compressed(os.path.join(HERE, f"{prefix}_{name}.npz"), U0=c["U0"], out=out, h=c["h"],
+                                dt=c["dt"], steps=c["steps"], periodic=np.array(c["periodic"], dtype=np.int8),
+                                active=np.ones(0, np.uint8), alpha=np.array(cases_def.ALPHA),
+                                scheme=np.array(scheme))
+            print(f"{prefix}_{name}: {sec:.3f} s")
 
 
 if __name__ == "__main__":
@@ -149,6 +159,8 @@ if __name__ == "__main__":
         make_grids()
     elif "--schemes" in sys.argv:
         make_schemes()
+    elif "--viscous" in sys.argv:
+        make_viscous(set(sys.argv[sys.argv.index("--viscous") + 1].split(",")))
     elif "--cases" in sys.argv:
         main(only=set(sys.argv[sys.argv.index("--cases") + 1].split(",")))
     else:

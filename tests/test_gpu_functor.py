@@ -216,3 +216,19 @@ def test_reference_viscous_jet_functors_compiled_for_the_device(golden_dir, name
     # and the viscous terms are really there: the inviscid functor differs
     inviscid = run_stage_fn(z, "dnref_stage_vanleer")
     assert (np.abs(inviscid - z["out"]) / scale).max() > 1e-9
+
+
+@needs_ref_plugin
+@pytest.mark.parametrize("name", cases_def.SMAG_CASES)
+def test_reference_smagorinsky_baseflow_functors_compiled_for_the_device(golden_dir, name):
+    # Roe + CompressibleSmagorinskyFlux<5, 2400> (the field fluxes of the
+    # base-flow application): the eddy viscosity takes a square root and the
+    # viscosity law calls pow, so the bound is 1e-12 relative to each
+    # variable's magnitude, as for the jet functors
+    z = np.load(os.path.join(golden_dir, f"smag_{name}.npz"))
+    out = run_stage_fn(z, "dnref_stage_roe_smag")
+    scale = np.abs(z["out"]).reshape(5, -1).max(axis=1)[:, None, None, None]
+    rel = (np.abs(out - z["out"]) / scale).max()
+    assert rel < 1e-12, (name, rel)
+    inviscid = run_stage_fn(z, "dnref_stage_roe")
+    assert (np.abs(inviscid - z["out"]) / scale).max() > 1e-9

@@ -84,3 +84,23 @@ def test_schemes_differ_from_each_other(golden_dir):
     for a in range(len(outs)):
         for b in range(a + 1, len(outs)):
             assert not np.array_equal(outs[a], outs[b])
+
+
+@pytest.mark.skipif(not pyoracle.ref_available(), reason="compiled reference (oracle/_ref) not built")
+@pytest.mark.parametrize("prefix", sorted(cases_def.VISCOUS_SETS))
+def test_viscous_fixtures_reproduce_and_carry_their_viscous_terms(golden_dir, prefix):
+    # the viscous fixtures (VanLeer + CompressibleViscFlux, Roe +
+    # CompressibleSmagorinskyFlux) are the compiled reference's own outputs,
+    # and differ from the same Euler flux without the viscous part
+    inviscid = {cases_def.VISC_SCHEME: cases_def.SCHEMES["vanleer"], cases_def.SMAG_SCHEME: cases_def.SCHEMES["roe"]}
+    scheme, names = cases_def.VISCOUS_SETS[prefix]
+    for name in names:
+        z, active = _load(golden_dir, f"{prefix}_{name}")
+        assert int(z["scheme"]) == scheme
+        args = (z["U0"], float(z["h"]), float(z["dt"]), int(z["steps"]), tuple(z["alpha"]),
+                tuple(bool(p) for p in z["periodic"]), active)
+        out, _ = pyoracle.ref_run(*args, threads=1, scheme=scheme)
+        assert np.array_equal(out, z["out"]), (prefix, name)
+        euler, _ = pyoracle.ref_run(*args, threads=1, scheme=inviscid[scheme])
+        scale = np.abs(z["out"]).reshape(5, -1).max(axis=1)[:, None, None, None]
+        assert (np.abs(euler - z["out"]) / scale).max() > 1e-9, (prefix, name)
