@@ -370,6 +370,7 @@ int read_device_error(dn_ctx* c)
     if (h & 8) return fail(c, DN_ERR_RANGE, "a level-set wall cell left the offset range of its patch");
     if (h & 16) return fail(c, DN_ERR_RANGE, "a face flux of a stage was not finite or reached 2^30 offset quanta "
                             "(the state or its fluxes left the fixed-point range of the patch)");
+    if (h & 32) return fail(c, DN_ERR_DEVICE, "a TMA transfer of a stage did not complete within its bounded wait");
     return fail(c, DN_ERR_DEVICE, "device error word 0x%x", h);
   }
   return DN_OK;

@@ -87,7 +87,7 @@ fx_stage_batched(const Batch b)
   // form made two code paths compete for the instruction cache of an SM
   // running tiles of many patches (the general form alone measured 4-8 %
   // faster on the multi-patch workloads)
-  fx_stage_tile_impl<TJ, TK, false>(args, w.j0, w.k0, w.i0, w.i1);
+  fx_stage_tile_impl<TJ, TK, false>(args, nullptr, nullptr, w.j0, w.k0, w.i0, w.i1);
 }
 
 template <int TJ, int TK>

@@ -1,4 +1,6 @@
 // FX32 (FP32 bulk, fixed-point storage) stage kernel instantiation.
+#include <cstdlib>
+#include <cstring>
 #include "fv_launch.h"
 #include "fv_fx32.cuh"
 #include "fv_batch.cuh"
@@ -16,16 +18,67 @@ constexpr int FX_TJ = DN_FX_TJ;   // tile of the single-patch launch (j x k)
 constexpr int FX_TK = DN_FX_TK;
 }
 
+namespace {
+
+// cuTensorMapEncodeTiled of the driver, reached through the runtime's entry
+// point query (no link-time dependency on the driver library)
+using EncodeTiled = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                 const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                 CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+EncodeTiled encode_tiled()
+{
+  static const EncodeTiled fn = [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &p, 12000, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess)
+      return (EncodeTiled) nullptr;
+    return reinterpret_cast<EncodeTiled>(p);
+  }();
+  return fn;
+}
+
+// Tensor map of one field of a patch, [5][ni][nj][nk] int32, with box
+// (bk, bj, 1, 5).  The caller has checked nk % 4 == 0 (16-byte row stride)
+// and the 16-byte alignment of the base.
+bool encode_field_map(CUtensorMap* m, const int32_t* base, const FxGeom& g, unsigned bk, unsigned bj)
+{
+  const EncodeTiled enc = encode_tiled();
+  if (!enc) return false;
+  const cuuint64_t dims[4] = {(cuuint64_t)g.nk, (cuuint64_t)g.nj, (cuuint64_t)g.ni, 5};
+  const cuuint64_t strides[3] = {(cuuint64_t)g.nk * 4, (cuuint64_t)g.nj * g.nk * 4, (cuuint64_t)g.ni * g.nj * g.nk * 4};
+  const cuuint32_t box[4] = {bk, bj, 1, 5};
+  const cuuint32_t estr[4] = {1, 1, 1, 1};
+  return enc(m, CU_TENSOR_MAP_DATA_TYPE_INT32, 4, const_cast<int32_t*>(base), dims, strides, box, estr,
+             CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+} // namespace
+
 cudaError_t launch_stage_fx32(const FxArgs& a, cudaStream_t st)
 {
   using Smem = FxSmem<FX_TJ, FX_TK>;
   auto kern = fx_stage_kernel<FX_TJ, FX_TK>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(Smem));
   if (e != cudaSuccess) return e;
+  FxLaunch L;
+  std::memset(&L, 0, sizeof L);
+  L.a = a;
+  // TMA staging when the rows are 16-byte strided and aligned and the patch
+  // has interior tiles (halo inside the patch on j and k); with
+  // DN_FX_NO_TMA=1 in the environment every tile copies cell by cell
+  const char* nt = std::getenv("DN_FX_NO_TMA");
+  const bool no_tma = nt && nt[0] == '1';
+  const bool aligned = ((reinterpret_cast<uintptr_t>(a.in) | reinterpret_cast<uintptr_t>(a.un)) & 15) == 0;
+  if (!no_tma && aligned && a.g.nk % 4 == 0 && a.g.nj >= 2 * FX_TJ + 2 && a.g.nk >= 2 * FX_TK + 2)
+    L.tma = encode_field_map(&L.tm_plane, a.in, a.g, FX_TK + 8, FX_TJ + 4) &&
+            encode_field_map(&L.tm_un, a.un, a.g, FX_TK, FX_TJ);
   dim3 block(FX_TK, FX_TJ, 1);
   dim3 grid((a.g.nk + FX_TK - 1) / FX_TK, (a.g.nj + FX_TJ - 1) / FX_TJ,
             (a.g.ni + a.g.i_chunk - 1) / a.g.i_chunk);
-  kern<<<grid, block, sizeof(Smem), st>>>(a);
+  kern<<<grid, block, sizeof(Smem), st>>>(L);
   return cudaGetLastError();
 }
 

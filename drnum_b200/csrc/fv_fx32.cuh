@@ -35,17 +35,20 @@
 // identical bits.
 //
 // Data flow per CTA: a TJ x TK tile of (j, k) columns marches along i.  Each
-// plane of the stencil state (int32) is copied asynchronously (cp.async) into
-// a four-plane shared-memory ring with a two-cell halo in j and k, about two
-// planes ahead of its first use, and dequantised there once to FP32.  x faces
-// are evaluated per thread along its own column (the left state of the next
-// face stays in registers); y and z face states and face integers are
-// exchanged through shared memory.
+// plane of the stencil state (int32) with a two-cell halo in j and k is
+// loaded into a shared-memory staging plane one iteration before its first
+// use, by one TMA box load where the halo lies inside the patch, else cell
+// by cell with cp.async (wrapped or clamped cells), and dequantised from
+// there once into a three-plane FP32 ring; f(n) of the own cells arrives the
+// same way.  x faces are evaluated per thread along its own column (the
+// left state of the next face stays in registers); y and z face states and
+// face integers are exchanged through shared memory.
 #pragma once
 
 #include <cstdint>
 #include "fv_numerics.cuh"
 #include "fv_wall.cuh"
+#include "fv_tma.cuh"
 
 namespace dn {
 
@@ -308,13 +311,18 @@ __device__ __forceinline__ bool fx_face_exists(int x, int n, int per)
 // stores rows in interleaved pairs ([row/2][col][row%2]), since a warp of a
 // 16-wide tile spans two rows; the z arrays keep own columns at stride TK
 // and park the one extra (halo) column of each row in the bank the own
-// columns leave free.
+// columns leave free.  The staging plane holds the next plane as stored
+// (int32, plain rows starting at column k0-4, so that a TMA box starts on a
+// 16-byte boundary) until it is dequantised into the ring.
 template <int TJ, int TK>
 struct FxSmem {
   static constexpr int PJ = TJ + 4;
   static constexpr int PK = TK + 4;
+  static constexpr int SK = TK + 8;              // staging row: columns k0-4 .. k0+TK+3
   static constexpr int NW = TJ * TK / 32;        // warps of a CTA
-  alignas(128) float plane[4][5][PJ / 2][PK][2]; // dequantised state, ring over planes i-1 .. i+2
+  alignas(128) float plane[3][5][PJ / 2][PK][2]; // dequantised state, ring over planes i .. i+2
+  alignas(128) int stage[5][PJ][SK];             // plane i+3 as stored, on its way into the ring
+  alignas(128) int un[5][TJ][TK];                // f(n) of the own cells of the current plane
   alignas(128) float sy[5][TJ + 1][TK];          // y: left state of the face above row jj-1 (row -1 .. TJ-1)
   alignas(128) float sy_top[5][TK];              // y: right state of the face below row TJ (halo)
   alignas(128) float szL[5][TJ][TK];             // z: left state of the face above col kk (own columns)
@@ -323,7 +331,7 @@ struct FxSmem {
   alignas(128) int qy[5][TJ + 1][TK];            // y face integers, face below row jj
   alignas(128) int qzL[5][TJ][TK];               // z face integers, face below col kk (own columns)
   alignas(128) int qzT[5][NW][32];               // z face integers, face below col TK (halo), see zt_slot
-  alignas(128) int un[5][TJ][TK];                // f(n) of the own cells of the current plane (cp.async)
+  alignas(8) uint64_t bar[2];                    // mbarriers of the TMA loads: staging plane, f(n)
 };
 
 // bank-free slots of the per-row halo values of the z arrays
@@ -360,16 +368,27 @@ __device__ __forceinline__ bool fx_tile_full(const FxGeom& g, int j0, int k0)
   return fy && fz;
 }
 
+// Device error bit of a TMA transfer that did not complete within the
+// bounded wait.
+constexpr int kFxErrTma = 32;
+
 // One tile of one patch: columns (j0 .. j0+TJ-1, k0 .. k0+TK-1), planes i0 .. i1-1.
+// tm_plane / tm_un: tensor maps of the stage input (box TK+8 x TJ+4 x 1 x 5)
+// and of f(n) (box TK x TJ x 1 x 5), or null; they are used for tiles whose
+// halo lies inside the patch on j and k (no wrapped or clamped cells), the
+// other tiles copy cell by cell.
 template <int TJ, int TK, bool FULL>
-__device__ __forceinline__ void fx_stage_tile_impl(const FxArgs& a, int j0, int k0, int i0, int i1)
+__device__ __forceinline__ void fx_stage_tile_impl(const FxArgs& a, const CUtensorMap* tm_plane,
+                                                   const CUtensorMap* tm_un, int j0, int k0, int i0, int i1)
 {
   constexpr int NT = TJ * TK;
   constexpr int PJ = TJ + 4, PK = TK + 4;
   constexpr int NP = PJ * PK;                     // positions of a plane tile (per variable)
   constexpr int PPT = (NP + NT - 1) / NT;         // positions per thread
   using Smem = FxSmem<TJ, TK>;
-  extern __shared__ __align__(16) unsigned char fx_smem_raw[];
+  constexpr int SK = Smem::SK;
+  constexpr int SP = PJ * SK;                     // staging elements per variable
+  extern __shared__ __align__(128) unsigned char fx_smem_raw[];
   Smem& sm = *reinterpret_cast<Smem*>(fx_smem_raw);
 
   const FxGeom& g = a.g;
@@ -380,28 +399,37 @@ __device__ __forceinline__ void fx_stage_tile_impl(const FxArgs& a, int j0, int 
   const bool own = FULL || ((j < g.nj) && (k < g.nk));
   const int njk = g.nj * g.nk;
   const size_t nc = (size_t)g.ni * njk;
+  // TMA boxes: staging rows j0-2 .. j0+TJ+1 and columns k0-4 .. k0+TK+3 (the
+  // last two may lie beyond the patch: zero-filled, never read); x = k0-4 is
+  // a multiple of 4 int32 since TK is; destinations 128-byte aligned
+  const bool tma = FULL && tm_plane != nullptr && j0 >= 2 && j0 + TJ + 2 <= g.nj && k0 >= 4 &&
+                   k0 + TK + 2 <= g.nk && ((smem_u32(&sm.stage[0][0][0]) | smem_u32(&sm.un[0][0][0])) & 127) == 0;
 
-  // per-thread plane positions: in-plane offset j*nk + k of the (wrapped)
-  // column, or -1 outside a closed patch; the variables follow at stride nc
   // plane element (jj, kk) of variable v in ring slot sl (rows interleaved in pairs)
   auto PL = [&](int sl, int v, int jj, int kk) -> float& { return sm.plane[sl][v][jj >> 1][kk][jj & 1]; };
 
+  // per-thread plane positions e = tid + m*NT in ring order [row/2][col][row%2]:
+  // in-plane offset j*nk + k of the (wrapped, or on closed axes clamped)
+  // column, and the position's offset in a staging plane
   int32_t poff[PPT];
+  int32_t soff[PPT];
   #pragma unroll
   for (int m = 0; m < PPT; ++m) {
-    const int e = tid + m * NT;                    // storage order: [row/2][col][row%2]
+    const int e = tid + m * NT;
     poff[m] = -1;
+    soff[m] = 0;
     if (e < NP) {
       const int jj = (e / (2 * PK)) * 2 + (e & 1);
       const int kk = (e % (2 * PK)) >> 1;
       poff[m] = fx_index(j0 - 2 + jj, g.nj, g.per_y) * g.nk + fx_index(k0 - 2 + kk, g.nk, g.per_z);
+      soff[m] = jj * SK + kk + 2;
     }
   }
 
-  // plane ip of the stage input (edge cells copied outward on closed axes):
-  // copied asynchronously as int32 into its ring slot ...
-  auto issue = [&](int ip) {
-    int* dst = reinterpret_cast<int*>(&sm.plane[ip & 3][0][0][0][0]);
+  // plane ip of the stage input, copied cell by cell (cp.async) as int32
+  // into ring slot sl, then dequantised there in place by the copying thread
+  auto issue_ring = [&](int sl, int ip) {
+    int* dst = reinterpret_cast<int*>(&sm.plane[sl][0][0][0][0]);
     const int32_t* src = a.in + (size_t)fx_index(ip, g.ni, g.per_x) * njk;
     #pragma unroll
     for (int v = 0; v < 5; ++v) {
@@ -411,12 +439,9 @@ __device__ __forceinline__ void fx_stage_tile_impl(const FxArgs& a, int j0, int 
         if (e < NP) fx_cp_async4(dst + v * NP + e, src + (size_t)v * nc + poff[m]);
       }
     }
-    fx_cp_async_commit();
   };
-  // ... and dequantised in place by the thread that copied it, once its copy
-  // group has completed; a barrier then publishes it to the CTA
-  auto dequant = [&](int ip) {
-    float* f = &sm.plane[ip & 3][0][0][0][0];
+  auto dequant_ring = [&](int sl) {
+    float* f = &sm.plane[sl][0][0][0][0];
     const int* q = reinterpret_cast<const int*>(f);
     #pragma unroll
     for (int v = 0; v < 5; ++v) {
@@ -427,41 +452,86 @@ __device__ __forceinline__ void fx_stage_tile_impl(const FxArgs& a, int j0, int 
       }
     }
   };
-
-  // f(n) of the own cell, plane ip, copied asynchronously into shared memory
-  // one plane ahead of its use in the update
+  // plane ip into the staging plane, cell by cell (tiles without TMA)
+  auto issue_stage = [&](int ip) {
+    int* dst = &sm.stage[0][0][0];
+    const int32_t* src = a.in + (size_t)fx_index(ip, g.ni, g.per_x) * njk;
+    #pragma unroll
+    for (int v = 0; v < 5; ++v) {
+      #pragma unroll
+      for (int m = 0; m < PPT; ++m) {
+        const int e = tid + m * NT;
+        if (e < NP) fx_cp_async4(dst + v * SP + soff[m], src + (size_t)v * nc + poff[m]);
+      }
+    }
+  };
+  // the staging plane, dequantised into ring slot sl
+  auto dequant_stage = [&](int sl) {
+    float* f = &sm.plane[sl][0][0][0][0];
+    const int* q = &sm.stage[0][0][0];
+    #pragma unroll
+    for (int v = 0; v < 5; ++v) {
+      #pragma unroll
+      for (int m = 0; m < PPT; ++m) {
+        const int e = tid + m * NT;
+        if (e < NP) f[v * NP + e] = fmaf(P.quantum[v], (float)q[v * SP + soff[m]], P.base[v]);
+      }
+    }
+  };
+  // f(n) of the own cell, plane ip, cell by cell (tiles without TMA)
   auto fetch_un = [&](int ip) {
-    if (own && ip < i1) {
+    if (own) {
       const int c = ip * njk + j * g.nk + k;
       #pragma unroll
       for (int v = 0; v < 5; ++v) fx_cp_async4(&sm.un[v][ty][tx], a.un + (size_t)v * nc + c);
     }
-    fx_cp_async_commit();
   };
-  fetch_un(i0);
+  // TMA loads of f(n) of plane ip and, if wanted, of stage-input plane ip+3
+  // (one thread; the barrier before it ended every read of both buffers)
+  auto issue_tma = [&](int ip, bool plane_too) {
+    fence_proxy_async_smem();
+    mbar_arrive_expect_tx(&sm.bar[1], 5u * TJ * TK * 4u);
+    tma_load_4d(&sm.un[0][0][0], tm_un, &sm.bar[1], k0, j0, ip, 0);
+    if (plane_too) {
+      mbar_arrive_expect_tx(&sm.bar[0], 5u * PJ * SK * 4u);
+      tma_load_4d(&sm.stage[0][0][0], tm_plane, &sm.bar[0], k0 - 4, j0 - 2, fx_index(ip + 3, g.ni, g.per_x), 0);
+    }
+  };
 
-  // prologue: planes i0-1 .. i0+2 in the ring
-  for (int q = -1; q <= 2; ++q) issue(i0 + q);
+  if (tma && tid == 0) {
+    mbar_init(&sm.bar[0], 1);
+    mbar_init(&sm.bar[1], 1);
+    mbar_init_fence();
+  }
+
+  // prologue: planes i0 .. i0+2 in the ring (the barrier below also
+  // publishes the mbarrier initialisation)
+  for (int q = 0; q <= 2; ++q) issue_ring(q, i0 + q);
+  fx_cp_async_commit();
   fx_cp_async_wait<0>();
-  for (int q = -1; q <= 2; ++q) dequant(i0 + q);
+  for (int q = 0; q <= 2; ++q) dequant_ring(q);
   __syncthreads();
 
   // x direction registers: left state of the face above the current cell,
   // the downwind difference of the current cell, and the lower face integers
   bool fbad = false;     // a face flux left the fixed-point range (fx_quant)
+  bool tbad = false;     // a TMA wait ran out
   Prim xleft;
   float xb[5];           // U_{i+1} - U_i of the own column (becomes a of cell i+1)
   int qx_lo[5];
   {
-    // slope of cell i0 (needs i0-1, i0, i0+1) and the face below i0
-    const int s_m1 = (i0 + 3) & 3, s_0 = i0 & 3, s_p1 = (i0 + 1) & 3;
+    // slope of cell i0 (needs i0-1, i0, i0+1) and the face below i0; planes
+    // i0-1 and i0-2 of the own column come straight from the stage input
+    const int64_t col = (int64_t)j * g.nk + k;
+    const int iw1 = fx_index(i0 - 1, g.ni, g.per_x);
     float Ul[5], Sp[5], Sm[5];
     float U0[5];
     #pragma unroll
     for (int v = 0; v < 5; ++v) {
-      const float um = PL(s_m1, v, ty + 2, tx + 2);
-      const float uc = PL(s_0, v, ty + 2, tx + 2);
-      const float up = PL(s_p1, v, ty + 2, tx + 2);
+      const float um = own ? fmaf(P.quantum[v], (float)__ldg(a.in + (int64_t)v * nc + (int64_t)iw1 * njk + col), P.base[v])
+                           : 0.0f;
+      const float uc = PL(0, v, ty + 2, tx + 2);
+      const float up = PL(1, v, ty + 2, tx + 2);
       const float s = fx_slope(uc - um, up - uc);
       U0[v] = uc;
       Sp[v] = fmaf(s, 0.5f, uc);
@@ -477,7 +547,7 @@ __device__ __forceinline__ void fx_stage_tile_impl(const FxArgs& a, int j0, int 
       float Lm[5];
       #pragma unroll
       for (int v = 0; v < 5; ++v) {
-        const float umm = fmaf(P.quantum[v], (float)__ldg(a.in + (int64_t)v * nc + (int64_t)iw2 * njk + (int64_t)j * g.nk + k), P.base[v]);
+        const float umm = fmaf(P.quantum[v], (float)__ldg(a.in + (int64_t)v * nc + (int64_t)iw2 * njk + col), P.base[v]);
         Lm[v] = fmaf(fx_slope(Ul[v] - umm, U0[v] - Ul[v]), 0.5f, Ul[v]);
       }
       float F[5];
@@ -490,8 +560,10 @@ __device__ __forceinline__ void fx_stage_tile_impl(const FxArgs& a, int j0, int 
     }
   }
 
+  int s0 = 0, sp1 = 1, sp2 = 2;       // ring slots of planes i, i+1, i+2
+  unsigned ph_plane = 0, ph_un = 0;   // parities of the next TMA completions
   for (int i = i0; i < i1; ++i) {
-    const int s0 = i & 3, sp1 = (i + 1) & 3, sp2 = (i + 2) & 3;
+    const bool more = i + 3 <= i1 + 1;  // plane i+3 is read by a later iteration
 
     // ---------------- y and z face states of plane i
     float2 yzm[5];   // right states of the y (lane x) and z (lane y) faces below the own cell
@@ -540,9 +612,17 @@ __device__ __forceinline__ void fx_stage_tile_impl(const FxArgs& a, int j0, int 
     }
     __syncthreads();
 
-    // the prologue's last reads of plane i0-1 preceded this barrier: its
-    // slot receives plane i0+3
-    if (i == i0) issue(i + 3);
+    // every read of the staging plane (dequantised at the end of the last
+    // iteration) and of f(n) (the last update) preceded this barrier: load
+    // f(n) of plane i and stage-input plane i+3 into them
+    if (tma) {
+      if (tid == 0) issue_tma(i, more);
+    } else {
+      fetch_un(i);
+      fx_cp_async_commit();
+      if (more) issue_stage(i + 3);
+      fx_cp_async_commit();
+    }
 
     // ---------------- y and z faces below the own cell (+ the top halo faces)
     {
@@ -594,8 +674,7 @@ __device__ __forceinline__ void fx_stage_tile_impl(const FxArgs& a, int j0, int 
         if (hz) sm.qzT[v][z_warp<TK>(h)][zt_slot<TK>(h)] = exz ? fx_quant(q.y, fbad) : 0;
       }
     }
-    // ---------------- x: face above cell i (between i and i+1); plane i+2
-    // was dequantised before this iteration's first barrier
+    // ---------------- x: face above cell i (between i and i+1)
     int qx_hi[5];
     {
       const bool ex = own && fx_face_exists(i + 1, g.ni, g.per_x);
@@ -625,8 +704,13 @@ __device__ __forceinline__ void fx_stage_tile_impl(const FxArgs& a, int j0, int 
     __syncthreads();
 
     // ---------------- residual and update of the own cell
-    // f(n) of plane i has arrived (the plane i+3 group may stay in flight)
-    fx_cp_async_wait<1>();
+    // f(n) of plane i has arrived (the staging copy may stay in flight)
+    if (tma) {
+      tbad |= !mbar_wait(&sm.bar[1], ph_un);
+      ph_un ^= 1u;
+    } else {
+      fx_cp_async_wait<1>();
+    }
     if (own) {
       const int c = i * njk + j * g.nk + k;       // 5*cells < 2^31 (host check)
       const int ncv = (int)nc;
@@ -640,8 +724,7 @@ __device__ __forceinline__ void fx_stage_tile_impl(const FxArgs& a, int j0, int 
                - sm.qy[v][ty + 1][tx] - qx_hi[v];
       if (a.wall.any && (i == 0 || i == g.ni - 1 || j == 0 || j == g.nj - 1 || k == 0 || k == g.nk - 1)) {
         // the cell's state, re-read from the stage input: the ring slot of
-        // plane i may already be receiving plane i+4 (no barrier separates
-        // this from the copies other threads issue at the end of the iteration)
+        // plane i receives plane i+3 below, with no barrier in between
         float uc[5];
         #pragma unroll
         for (int v = 0; v < 5; ++v) uc[v] = fmaf(P.quantum[v], (float)a.in[v * ncv + c], P.base[v]);
@@ -678,22 +761,33 @@ __device__ __forceinline__ void fx_stage_tile_impl(const FxArgs& a, int j0, int 
       qx_lo[v] = qx_hi[v];
     }
 
-    // ---------------- ring: plane i+3 becomes readable (the next
-    // iteration's first barrier orders this before its reads of plane i+3);
-    // plane i, last read in this iteration, gives its slot to plane i+4
-    fx_cp_async_wait<0>();
-    dequant(i + 3);
-    fetch_un(i + 1);
-    issue(i + 4);
+    // ---------------- ring: plane i (last read before this iteration's
+    // first barrier) gives its slot to plane i+3, dequantised from the
+    // staging plane; the next iteration's first barrier publishes it
+    if (more) {
+      if (tma) {
+        tbad |= !mbar_wait(&sm.bar[0], ph_plane);
+        ph_plane ^= 1u;
+      } else {
+        fx_cp_async_wait<0>();
+      }
+      dequant_stage(s0);
+    }
+    const int t = s0;
+    s0 = sp1;
+    sp1 = sp2;
+    sp2 = t;
   }
   if (fbad && a.err) atomicOr(a.err, 16);
+  if (tbad && a.err) atomicOr(a.err, kFxErrTma);
 }
 
 template <int TJ, int TK>
-__device__ __forceinline__ void fx_stage_tile(const FxArgs& a, int j0, int k0, int i0, int i1)
+__device__ __forceinline__ void fx_stage_tile(const FxArgs& a, const CUtensorMap* tm_plane, const CUtensorMap* tm_un,
+                                              int j0, int k0, int i0, int i1)
 {
-  if (fx_tile_full<TJ, TK>(a.g, j0, k0)) fx_stage_tile_impl<TJ, TK, true>(a, j0, k0, i0, i1);
-  else fx_stage_tile_impl<TJ, TK, false>(a, j0, k0, i0, i1);
+  if (fx_tile_full<TJ, TK>(a.g, j0, k0)) fx_stage_tile_impl<TJ, TK, true>(a, tm_plane, tm_un, j0, k0, i0, i1);
+  else fx_stage_tile_impl<TJ, TK, false>(a, nullptr, nullptr, j0, k0, i0, i1);
 }
 
 // Resident CTAs per SM the register allocation is sized for: three
@@ -703,13 +797,23 @@ __device__ __forceinline__ void fx_stage_tile(const FxArgs& a, int j0, int k0, i
 #define DN_FX_MIN_BLOCKS 3
 #endif
 
+// Parameters of the single-patch launch: the stage arguments and the tensor
+// maps of the stage input and of f(n) (valid when tma != 0).
+struct FxLaunch {
+  CUtensorMap tm_plane;
+  CUtensorMap tm_un;
+  FxArgs a;
+  int tma;
+};
+
 // One patch per launch: grid (k tiles, j tiles, i chunks).
 template <int TJ, int TK>
 __global__ void __launch_bounds__(TJ * TK, DN_FX_MIN_BLOCKS)
-fx_stage_kernel(const FxArgs a)
+fx_stage_kernel(const __grid_constant__ FxLaunch L)
 {
-  const int i0 = blockIdx.z * a.g.i_chunk;
-  fx_stage_tile<TJ, TK>(a, blockIdx.y * TJ, blockIdx.x * TK, i0, min(a.g.ni, i0 + a.g.i_chunk));
+  const int i0 = blockIdx.z * L.a.g.i_chunk;
+  fx_stage_tile<TJ, TK>(L.a, L.tma ? &L.tm_plane : nullptr, L.tma ? &L.tm_un : nullptr, blockIdx.y * TJ,
+                        blockIdx.x * TK, i0, min(L.a.g.ni, i0 + L.a.g.i_chunk));
 }
 
 } // namespace dn
