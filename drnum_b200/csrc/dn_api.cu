@@ -98,6 +98,7 @@ struct dn_ctx {
   std::vector<int> shape;
   bool batch_dirty = true;
   void* d_records = nullptr;
+  void* d_maps = nullptr;                     // FX32 batched: dn::BatchMaps per patch
   void* d_items[dn::kNumShapes] = {nullptr, nullptr};
   int n_items[dn::kNumShapes] = {0, 0};
   // CUDA graphs of whole RK steps; any change of the case bumps generation
@@ -733,6 +734,8 @@ void free_batch(dn_ctx* c)
 {
   if (c->d_records) cudaFree(c->d_records);
   c->d_records = nullptr;
+  if (c->d_maps) cudaFree(c->d_maps);
+  c->d_maps = nullptr;
   for (int q = 0; q < dn::kNumShapes; ++q) {
     if (c->d_items[q]) cudaFree(c->d_items[q]);
     c->d_items[q] = nullptr;
@@ -760,6 +763,7 @@ int build_batch(dn_ctx* c)
   if (np == 0) { c->batch_dirty = false; return DN_OK; }
   const bool fp64 = c->precision == DN_FP64;
   std::vector<dn::BatchPatch> rec(np);
+  std::vector<dn::BatchMaps> maps(fp64 ? 0 : np);
   long tiles = 0;
   for (size_t q = 0; q < np; ++q) {
     const DnPatch& P = c->patches[q];
@@ -777,6 +781,14 @@ int build_batch(dn_ctx* c)
     int tj, tk;
     dn::shape_tile(fp64, c->shape[q], &tj, &tk);
     if (P.owned) tiles += (long)((P.d.nj + tj - 1) / tj) * ((P.d.nk + tk - 1) / tk);
+    if (!fp64) {
+      dn::FxGeom g{};
+      g.ni = P.d.ni; g.nj = P.d.nj; g.nk = P.d.nk;
+      r.tma = 1;
+      for (int b = 0; b < 3 && r.tma; ++b)
+        r.tma = dn::encode_stage_maps(maps[q].in[b], &maps[q].un[b], (const int32_t*)P.buf[b],
+                                      (const int32_t*)P.buf[b], g, tj, tk) ? 1 : 0;
+    }
   }
   const long want = (long)c->num_sms * 2 * 4;
   long chunks = (want + tiles - 1) / tiles;
@@ -800,6 +812,12 @@ int build_batch(dn_ctx* c)
   if (e != cudaSuccess) return fail(c, DN_ERR_NOMEM, "cudaMalloc(patch records)");
   e = cudaMemcpyAsync(c->d_records, rec.data(), np * sizeof(dn::BatchPatch), cudaMemcpyHostToDevice, c->stream);
   if (e != cudaSuccess) return cuda_fail(c, e, "patch record upload");
+  if (!maps.empty()) {
+    e = cudaMalloc(&c->d_maps, np * sizeof(dn::BatchMaps));
+    if (e != cudaSuccess) return fail(c, DN_ERR_NOMEM, "cudaMalloc(tensor maps)");
+    e = cudaMemcpyAsync(c->d_maps, maps.data(), np * sizeof(dn::BatchMaps), cudaMemcpyHostToDevice, c->stream);
+    if (e != cudaSuccess) return cuda_fail(c, e, "tensor map upload");
+  }
   for (int q = 0; q < dn::kNumShapes; ++q) {
     if (items[q].empty()) continue;
     if (items[q].size() > (size_t)INT32_MAX) return fail(c, DN_ERR_RANGE, "too many work items");
@@ -840,6 +858,7 @@ int stage_all(dn_ctx* c, int in_b, int un_b, int out_b, double factor)
     if (!c->n_items[q]) continue;
     dn::Batch b;
     b.patches = static_cast<const dn::BatchPatch*>(c->d_records);
+    b.maps = static_cast<const dn::BatchMaps*>(c->d_maps);
     b.items = static_cast<const dn::WorkItem*>(c->d_items[q]);
     b.n_items = c->n_items[q];
     b.in_b = in_b; b.un_b = un_b; b.out_b = out_b;

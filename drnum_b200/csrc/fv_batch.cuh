@@ -23,6 +23,7 @@ struct BatchPatch {
   const uint8_t* active;        // NULL = all active
   int ni, nj, nk;
   int per_x, per_y, per_z;
+  int tma;                      // FX32: the patch's entry of Batch::maps is valid
   double dx, dy, dz;
   double base[5], quantum[5];   // FP32-bulk fixed-point base and quantum
   WallBC wall;
@@ -32,8 +33,16 @@ struct WorkItem {
   int patch, j0, k0, i0, i1;
 };
 
+// Tensor maps of an FX32 patch for its tile shape, per physical buffer:
+// the staging boxes of a stage input and the box of f(n).
+struct BatchMaps {
+  CUtensorMap in[3][kFxMaps];
+  CUtensorMap un[3];
+};
+
 struct Batch {
   const BatchPatch* patches;
+  const BatchMaps* maps;        // FX32: per patch, or NULL
   const WorkItem* items;
   int n_items;
   int in_b, un_b, out_b;        // physical buffers: stage input, step start, output
@@ -87,7 +96,9 @@ fx_stage_batched(const Batch b)
   // form made two code paths compete for the instruction cache of an SM
   // running tiles of many patches (the general form alone measured 4-8 %
   // faster on the multi-patch workloads)
-  fx_stage_tile_impl<TJ, TK, false>(args, nullptr, nullptr, w.j0, w.k0, w.i0, w.i1);
+  const BatchMaps* M = (b.maps && rec.tma) ? b.maps + w.patch : nullptr;
+  fx_stage_tile_impl<TJ, TK, false>(args, M ? M->in[b.in_b] : nullptr, M ? &M->un[b.un_b] : nullptr, w.j0, w.k0,
+                                    w.i0, w.i1);
 }
 
 template <int TJ, int TK>

@@ -57,6 +57,21 @@ bool encode_field_map(CUtensorMap* m, const int32_t* base, const FxGeom& g, unsi
 
 } // namespace
 
+bool encode_stage_maps(CUtensorMap* tm_in, CUtensorMap* tm_un, const int32_t* in, const int32_t* un, const FxGeom& g,
+                       int tj, int tk)
+{
+  // TMA staging when the rows are 16-byte strided and the fields 16-byte
+  // aligned; with DN_FX_NO_TMA=1 in the environment every tile copies cell
+  // by cell (the two give identical results)
+  const char* nt = std::getenv("DN_FX_NO_TMA");
+  if (nt && nt[0] == '1') return false;
+  if (((reinterpret_cast<uintptr_t>(in) | reinterpret_cast<uintptr_t>(un)) & 15) != 0 || g.nk % 4 != 0) return false;
+  const unsigned bj = tj + 4, bk = tk + 8;
+  return encode_field_map(&tm_in[kFxMapMain], in, g, bk, bj) && encode_field_map(&tm_in[kFxMapK], in, g, 4, bj) &&
+         encode_field_map(&tm_in[kFxMapJ], in, g, bk, 2) && encode_field_map(&tm_in[kFxMapC], in, g, 4, 2) &&
+         encode_field_map(tm_un, un, g, tk, tj);
+}
+
 cudaError_t launch_stage_fx32(const FxArgs& a, cudaStream_t st)
 {
   using Smem = FxSmem<FX_TJ, FX_TK>;
@@ -66,15 +81,7 @@ cudaError_t launch_stage_fx32(const FxArgs& a, cudaStream_t st)
   FxLaunch L;
   std::memset(&L, 0, sizeof L);
   L.a = a;
-  // TMA staging when the rows are 16-byte strided and aligned and the patch
-  // has interior tiles (halo inside the patch on j and k); with
-  // DN_FX_NO_TMA=1 in the environment every tile copies cell by cell
-  const char* nt = std::getenv("DN_FX_NO_TMA");
-  const bool no_tma = nt && nt[0] == '1';
-  const bool aligned = ((reinterpret_cast<uintptr_t>(a.in) | reinterpret_cast<uintptr_t>(a.un)) & 15) == 0;
-  if (!no_tma && aligned && a.g.nk % 4 == 0 && a.g.nj >= 2 * FX_TJ + 2 && a.g.nk >= 2 * FX_TK + 2)
-    L.tma = encode_field_map(&L.tm_plane, a.in, a.g, FX_TK + 8, FX_TJ + 4) &&
-            encode_field_map(&L.tm_un, a.un, a.g, FX_TK, FX_TJ);
+  L.tma = encode_stage_maps(L.tm_in, &L.tm_un, a.in, a.un, a.g, FX_TJ, FX_TK);
   dim3 block(FX_TK, FX_TJ, 1);
   dim3 grid((a.g.nk + FX_TK - 1) / FX_TK, (a.g.nj + FX_TJ - 1) / FX_TJ,
             (a.g.ni + a.g.i_chunk - 1) / a.g.i_chunk);

@@ -311,17 +311,26 @@ __device__ __forceinline__ bool fx_face_exists(int x, int n, int per)
 // stores rows in interleaved pairs ([row/2][col][row%2]), since a warp of a
 // 16-wide tile spans two rows; the z arrays keep own columns at stride TK
 // and park the one extra (halo) column of each row in the bank the own
-// columns leave free.  The staging plane holds the next plane as stored
-// (int32, plain rows starting at column k0-4, so that a TMA box starts on a
-// 16-byte boundary) until it is dequantised into the ring.
+// columns leave free.  The staging area holds the next plane as stored
+// (int32) until it is dequantised into the ring: a main box of rows j0-2 ..
+// j0+TJ+1 and columns k0-4 .. k0+TK+3 (plain rows; the column origin k0-4
+// keeps a TMA box on a 16-byte boundary), and, for tiles at the seam of a
+// periodic axis, the wrapped columns (k side box, 4 wide), the wrapped rows
+// (j side box, 2 high) and their corner.
 template <int TJ, int TK>
 struct FxSmem {
   static constexpr int PJ = TJ + 4;
   static constexpr int PK = TK + 4;
-  static constexpr int SK = TK + 8;              // staging row: columns k0-4 .. k0+TK+3
+  static constexpr int SK = TK + 8;              // main box row: columns k0-4 .. k0+TK+3
   static constexpr int NW = TJ * TK / 32;        // warps of a CTA
+  static constexpr int up128(int n) { return (n + 31) / 32 * 32; }   // int32 count to 128 bytes
+  static constexpr int ST_M = 0;                                   // main box [5][PJ][SK]
+  static constexpr int ST_K = ST_M + up128(5 * PJ * SK);           // k side box [5][PJ][4]
+  static constexpr int ST_J = ST_K + up128(5 * PJ * 4);            // j side box [5][2][SK]
+  static constexpr int ST_C = ST_J + up128(5 * 2 * SK);            // corner box [5][2][4]
+  static constexpr int ST_N = ST_C + up128(5 * 2 * 4);
   alignas(128) float plane[3][5][PJ / 2][PK][2]; // dequantised state, ring over planes i .. i+2
-  alignas(128) int stage[5][PJ][SK];             // plane i+3 as stored, on its way into the ring
+  alignas(128) int stage[ST_N];                  // plane i+3 as stored, on its way into the ring
   alignas(128) int un[5][TJ][TK];                // f(n) of the own cells of the current plane
   alignas(128) float sy[5][TJ + 1][TK];          // y: left state of the face above row jj-1 (row -1 .. TJ-1)
   alignas(128) float sy_top[5][TK];              // y: right state of the face below row TJ (halo)
@@ -372,13 +381,32 @@ __device__ __forceinline__ bool fx_tile_full(const FxGeom& g, int j0, int k0)
 // bounded wait.
 constexpr int kFxErrTma = 32;
 
+// Tensor maps of the stage input of a patch, one per box: main (TK+8 x
+// TJ+4), k side (4 x TJ+4), j side (TK+8 x 2), corner (4 x 2), each x 1
+// plane x 5 variables.
+constexpr int kFxMapMain = 0, kFxMapK = 1, kFxMapJ = 2, kFxMapC = 3, kFxMaps = 4;
+
+// Where a tile's halo along one axis comes from when its planes are staged
+// by TMA: 0 inside the patch or clamped (closed axis), 1 wrapped below the
+// first cell, 2 wrapped above the last cell; -1 not stageable by TMA (a
+// periodic axis whose tile needs both ends, or a ragged tile at the seam).
+__device__ __forceinline__ int fx_seam(int t0, int T, int n, int per)
+{
+  if (!per || (t0 >= 2 && t0 + T + 2 <= n)) return 0;
+  if (t0 == 0 && n >= T + 2) return 1;
+  if (t0 >= 2 && t0 + T == n) return 2;
+  return -1;
+}
+
 // One tile of one patch: columns (j0 .. j0+TJ-1, k0 .. k0+TK-1), planes i0 .. i1-1.
-// tm_plane / tm_un: tensor maps of the stage input (box TK+8 x TJ+4 x 1 x 5)
-// and of f(n) (box TK x TJ x 1 x 5), or null; they are used for tiles whose
-// halo lies inside the patch on j and k (no wrapped or clamped cells), the
-// other tiles copy cell by cell.
+// tm_in: the kFxMaps tensor maps of the stage input, tm_un: the map of f(n)
+// (box TK x TJ x 1 x 5), or null.  With maps, a tile stages its planes by
+// TMA box loads unless fx_seam excludes it; closed-axis cells outside the
+// patch then read the edge cell's slot of the main box, and the cells across
+// the seam of a periodic axis come from the side boxes.  Other tiles copy
+// cell by cell.
 template <int TJ, int TK, bool FULL>
-__device__ __forceinline__ void fx_stage_tile_impl(const FxArgs& a, const CUtensorMap* tm_plane,
+__device__ __forceinline__ void fx_stage_tile_impl(const FxArgs& a, const CUtensorMap* tm_in,
                                                    const CUtensorMap* tm_un, int j0, int k0, int i0, int i1)
 {
   constexpr int NT = TJ * TK;
@@ -387,7 +415,6 @@ __device__ __forceinline__ void fx_stage_tile_impl(const FxArgs& a, const CUtens
   constexpr int PPT = (NP + NT - 1) / NT;         // positions per thread
   using Smem = FxSmem<TJ, TK>;
   constexpr int SK = Smem::SK;
-  constexpr int SP = PJ * SK;                     // staging elements per variable
   extern __shared__ __align__(128) unsigned char fx_smem_raw[];
   Smem& sm = *reinterpret_cast<Smem*>(fx_smem_raw);
 
@@ -399,30 +426,52 @@ __device__ __forceinline__ void fx_stage_tile_impl(const FxArgs& a, const CUtens
   const bool own = FULL || ((j < g.nj) && (k < g.nk));
   const int njk = g.nj * g.nk;
   const size_t nc = (size_t)g.ni * njk;
-  // TMA boxes: staging rows j0-2 .. j0+TJ+1 and columns k0-4 .. k0+TK+3 (the
-  // last two may lie beyond the patch: zero-filled, never read); x = k0-4 is
-  // a multiple of 4 int32 since TK is; destinations 128-byte aligned
-  const bool tma = FULL && tm_plane != nullptr && j0 >= 2 && j0 + TJ + 2 <= g.nj && k0 >= 4 &&
-                   k0 + TK + 2 <= g.nk && ((smem_u32(&sm.stage[0][0][0]) | smem_u32(&sm.un[0][0][0])) & 127) == 0;
+  // TMA boxes start at x = k0-4 (main, a multiple of 4 int32 since TK is),
+  // nk-4 or 0 (k side; the host gives maps only when nk % 4 == 0); box cells
+  // beyond the patch are zero-filled and never read; destinations 128-byte
+  // aligned
+  const int seam_j = fx_seam(j0, TJ, g.nj, g.per_y);
+  const int seam_k = fx_seam(k0, TK, g.nk, g.per_z);
+  const bool tma = tm_in != nullptr && seam_j >= 0 && seam_k >= 0 &&
+                   ((smem_u32(&sm.stage[0]) | smem_u32(&sm.un[0][0][0])) & 127) == 0;
 
   // plane element (jj, kk) of variable v in ring slot sl (rows interleaved in pairs)
   auto PL = [&](int sl, int v, int jj, int kk) -> float& { return sm.plane[sl][v][jj >> 1][kk][jj & 1]; };
 
   // per-thread plane positions e = tid + m*NT in ring order [row/2][col][row%2]:
   // in-plane offset j*nk + k of the (wrapped, or on closed axes clamped)
-  // column, and the position's offset in a staging plane
+  // column, and where the position's cell lies in the staging area: offset
+  // of variable 0 and the stride between variables of its box (cell copies
+  // fill the main box position by position)
   int32_t poff[PPT];
   int32_t soff[PPT];
+  int32_t svar[PPT];
   #pragma unroll
   for (int m = 0; m < PPT; ++m) {
     const int e = tid + m * NT;
     poff[m] = -1;
     soff[m] = 0;
+    svar[m] = PJ * SK;
     if (e < NP) {
       const int jj = (e / (2 * PK)) * 2 + (e & 1);
       const int kk = (e % (2 * PK)) >> 1;
-      poff[m] = fx_index(j0 - 2 + jj, g.nj, g.per_y) * g.nk + fx_index(k0 - 2 + kk, g.nk, g.per_z);
-      soff[m] = jj * SK + kk + 2;
+      const int jg = j0 - 2 + jj, kg = k0 - 2 + kk;
+      poff[m] = fx_index(jg, g.nj, g.per_y) * g.nk + fx_index(kg, g.nk, g.per_z);
+      soff[m] = Smem::ST_M + jj * SK + kk + 2;
+      if (tma) {
+        // row: in the main box (clamped on a closed axis) or across the seam
+        const bool jside = g.per_y && (jg < 0 || jg >= g.nj);
+        const int jr = jside ? (jg < 0 ? jg + 2 : jg - g.nj) : (g.per_y ? jg : min(max(jg, 0), g.nj - 1)) - (j0 - 2);
+        const bool kside = g.per_z && (kg < 0 || kg >= g.nk);
+        const int kr = kside ? (kg < 0 ? kg + 4 : kg - g.nk) : (g.per_z ? kg : min(max(kg, 0), g.nk - 1)) - (k0 - 4);
+        if (jside) {
+          soff[m] = (kside ? Smem::ST_C + jr * 4 : Smem::ST_J + jr * SK) + kr;
+          svar[m] = kside ? 2 * 4 : 2 * SK;
+        } else {
+          soff[m] = (kside ? Smem::ST_K + jr * 4 : Smem::ST_M + jr * SK) + kr;
+          svar[m] = kside ? PJ * 4 : PJ * SK;
+        }
+      }
     }
   }
 
@@ -454,27 +503,27 @@ __device__ __forceinline__ void fx_stage_tile_impl(const FxArgs& a, const CUtens
   };
   // plane ip into the staging plane, cell by cell (tiles without TMA)
   auto issue_stage = [&](int ip) {
-    int* dst = &sm.stage[0][0][0];
+    int* dst = &sm.stage[0];
     const int32_t* src = a.in + (size_t)fx_index(ip, g.ni, g.per_x) * njk;
     #pragma unroll
     for (int v = 0; v < 5; ++v) {
       #pragma unroll
       for (int m = 0; m < PPT; ++m) {
         const int e = tid + m * NT;
-        if (e < NP) fx_cp_async4(dst + v * SP + soff[m], src + (size_t)v * nc + poff[m]);
+        if (e < NP) fx_cp_async4(dst + soff[m] + v * svar[m], src + (size_t)v * nc + poff[m]);
       }
     }
   };
-  // the staging plane, dequantised into ring slot sl
+  // the staging area, dequantised into ring slot sl
   auto dequant_stage = [&](int sl) {
     float* f = &sm.plane[sl][0][0][0][0];
-    const int* q = &sm.stage[0][0][0];
+    const int* q = &sm.stage[0];
     #pragma unroll
     for (int v = 0; v < 5; ++v) {
       #pragma unroll
       for (int m = 0; m < PPT; ++m) {
         const int e = tid + m * NT;
-        if (e < NP) f[v * NP + e] = fmaf(P.quantum[v], (float)q[v * SP + soff[m]], P.base[v]);
+        if (e < NP) f[v * NP + e] = fmaf(P.quantum[v], (float)q[soff[m] + v * svar[m]], P.base[v]);
       }
     }
   };
@@ -493,8 +542,16 @@ __device__ __forceinline__ void fx_stage_tile_impl(const FxArgs& a, const CUtens
     mbar_arrive_expect_tx(&sm.bar[1], 5u * TJ * TK * 4u);
     tma_load_4d(&sm.un[0][0][0], tm_un, &sm.bar[1], k0, j0, ip, 0);
     if (plane_too) {
-      mbar_arrive_expect_tx(&sm.bar[0], 5u * PJ * SK * 4u);
-      tma_load_4d(&sm.stage[0][0][0], tm_plane, &sm.bar[0], k0 - 4, j0 - 2, fx_index(ip + 3, g.ni, g.per_x), 0);
+      const int pl = fx_index(ip + 3, g.ni, g.per_x);
+      const int xs = seam_k == 1 ? g.nk - 4 : 0;     // k side box: the wrapped columns
+      const int ys = seam_j == 1 ? g.nj - 2 : 0;     // j side box: the wrapped rows
+      const unsigned bytes = 5u * 4u * (PJ * SK + (seam_k ? PJ * 4 : 0) + (seam_j ? 2 * SK : 0) +
+                                        (seam_j && seam_k ? 2 * 4 : 0));
+      mbar_arrive_expect_tx(&sm.bar[0], bytes);
+      tma_load_4d(&sm.stage[Smem::ST_M], tm_in + kFxMapMain, &sm.bar[0], k0 - 4, j0 - 2, pl, 0);
+      if (seam_k) tma_load_4d(&sm.stage[Smem::ST_K], tm_in + kFxMapK, &sm.bar[0], xs, j0 - 2, pl, 0);
+      if (seam_j) tma_load_4d(&sm.stage[Smem::ST_J], tm_in + kFxMapJ, &sm.bar[0], k0 - 4, ys, pl, 0);
+      if (seam_j && seam_k) tma_load_4d(&sm.stage[Smem::ST_C], tm_in + kFxMapC, &sm.bar[0], xs, ys, pl, 0);
     }
   };
 
@@ -783,11 +840,11 @@ __device__ __forceinline__ void fx_stage_tile_impl(const FxArgs& a, const CUtens
 }
 
 template <int TJ, int TK>
-__device__ __forceinline__ void fx_stage_tile(const FxArgs& a, const CUtensorMap* tm_plane, const CUtensorMap* tm_un,
+__device__ __forceinline__ void fx_stage_tile(const FxArgs& a, const CUtensorMap* tm_in, const CUtensorMap* tm_un,
                                               int j0, int k0, int i0, int i1)
 {
-  if (fx_tile_full<TJ, TK>(a.g, j0, k0)) fx_stage_tile_impl<TJ, TK, true>(a, tm_plane, tm_un, j0, k0, i0, i1);
-  else fx_stage_tile_impl<TJ, TK, false>(a, nullptr, nullptr, j0, k0, i0, i1);
+  if (fx_tile_full<TJ, TK>(a.g, j0, k0)) fx_stage_tile_impl<TJ, TK, true>(a, tm_in, tm_un, j0, k0, i0, i1);
+  else fx_stage_tile_impl<TJ, TK, false>(a, tm_in, tm_un, j0, k0, i0, i1);
 }
 
 // Resident CTAs per SM the register allocation is sized for: three
@@ -800,7 +857,7 @@ __device__ __forceinline__ void fx_stage_tile(const FxArgs& a, const CUtensorMap
 // Parameters of the single-patch launch: the stage arguments and the tensor
 // maps of the stage input and of f(n) (valid when tma != 0).
 struct FxLaunch {
-  CUtensorMap tm_plane;
+  CUtensorMap tm_in[kFxMaps];
   CUtensorMap tm_un;
   FxArgs a;
   int tma;
@@ -812,7 +869,7 @@ __global__ void __launch_bounds__(TJ * TK, DN_FX_MIN_BLOCKS)
 fx_stage_kernel(const __grid_constant__ FxLaunch L)
 {
   const int i0 = blockIdx.z * L.a.g.i_chunk;
-  fx_stage_tile<TJ, TK>(L.a, L.tma ? &L.tm_plane : nullptr, L.tma ? &L.tm_un : nullptr, blockIdx.y * TJ,
+  fx_stage_tile<TJ, TK>(L.a, L.tma ? L.tm_in : nullptr, L.tma ? &L.tm_un : nullptr, blockIdx.y * TJ,
                         blockIdx.x * TK, i0, min(L.a.g.ni, i0 + L.a.g.i_chunk));
 }
 

@@ -2,7 +2,9 @@
 // arithmetic form so each gets its own floating-point compile flags).
 #pragma once
 
+#include <cuda.h>
 #include <cuda_runtime.h>
+#include <cstdint>
 #include "fv_policies.cuh"
 #include "fv_stage.cuh"
 
@@ -17,8 +19,15 @@ struct StageShape {
 cudaError_t launch_stage_f64(const StageArgs<PolicyF64>& a, const StageShape& s, cudaStream_t st);
 
 struct FxArgs;
+struct FxGeom;
 cudaError_t launch_stage_fx32(const FxArgs& a, cudaStream_t st);
 void fx32_tile(int* tj, int* tk);
+// Tensor maps for TMA staging of an FX32 stage with tj x tk tiles: the
+// kFxMaps boxes of the stage input `in` and the box of f(n) `un`; false when
+// the patch does not allow them (rows not 16-byte strided, unaligned fields)
+// or DN_FX_NO_TMA=1 is set.
+bool encode_stage_maps(CUtensorMap* tm_in, CUtensorMap* tm_un, const int32_t* in, const int32_t* un, const FxGeom& g,
+                       int tj, int tk);
 
 // Batched launches over a work list (fv_batch.cuh).  Tile shapes:
 //   FX32: 0 = 8 x 32, 1 = 16 x 16 (j x k);  FP64: 0 = 4 x 32, 1 = 8 x 16.

@@ -66,3 +66,40 @@ def test_tma_staging_with_inactive_cells_and_vortex_box():
     a, _ = run_fx32(U0, h, dt, 4, (True, True, True), active)
     b, _ = run_fx32(U0, h, dt, 4, (True, True, True), active, no_tma=True)
     assert np.array_equal(a, b)
+
+
+def run_workload_fx32(name, scale, steps, no_tma, shapes=None):
+    from drnum_b200 import _lib, workloads
+    old = os.environ.get("DN_FX_NO_TMA")
+    os.environ["DN_FX_NO_TMA"] = "1" if no_tma else "0"
+    try:
+        case = workloads.build(name, scale)
+        _, objs = workloads.make_grid(case)
+        it = workloads.make_iterator(objs, DN_FP32)
+        it.setOption(_lib.DN_OPT_BATCHED, 1)
+        if shapes is not None:
+            for p in range(len(objs)):
+                it.setTile(p, shapes[p % len(shapes)])
+        for _ in range(steps):
+            it.rkStep(case["dt"], cases.RK3_ALPHA)
+        it.updateHost(fields=(0,))
+        out = [o.getField(0).copy() for o in objs]
+        it.close()
+        return out
+    finally:
+        if old is None:
+            del os.environ["DN_FX_NO_TMA"]
+        else:
+            os.environ["DN_FX_NO_TMA"] = old
+
+
+@pytest.mark.parametrize("name,scale,shapes", [
+    ("sphere", 0.25, None),          # closed patches, level-set wall
+    ("tiled", 0.25, [0, 1]),         # 8 uneven patches, both tile shapes
+    ("jet", 0.125, [1]),             # far field and inflow faces
+])
+def test_batched_tma_staging_equals_cell_copies(name, scale, shapes):
+    a = run_workload_fx32(name, scale, 3, False, shapes)
+    b = run_workload_fx32(name, scale, 3, True, shapes)
+    for x, y in zip(a, b):
+        assert np.array_equal(x, y)
