@@ -323,12 +323,16 @@ struct FxSmem {
   static constexpr int PK = TK + 4;
   static constexpr int SK = TK + 8;              // main box row: columns k0-4 .. k0+TK+3
   static constexpr int NW = TJ * TK / 32;        // warps of a CTA
+  // Side boxes only for 16-wide tiles: with them the 32-wide tile's shared
+  // memory would leave room for two CTAs per SM instead of three (its
+  // tiles at a periodic seam copy cell by cell).
+  static constexpr bool SEAMS = TK <= 16;
   static constexpr int up128(int n) { return (n + 31) / 32 * 32; }   // int32 count to 128 bytes
   static constexpr int ST_M = 0;                                   // main box [5][PJ][SK]
   static constexpr int ST_K = ST_M + up128(5 * PJ * SK);           // k side box [5][PJ][4]
-  static constexpr int ST_J = ST_K + up128(5 * PJ * 4);            // j side box [5][2][SK]
-  static constexpr int ST_C = ST_J + up128(5 * 2 * SK);            // corner box [5][2][4]
-  static constexpr int ST_N = ST_C + up128(5 * 2 * 4);
+  static constexpr int ST_J = ST_K + (SEAMS ? up128(5 * PJ * 4) : 0);   // j side box [5][2][SK]
+  static constexpr int ST_C = ST_J + (SEAMS ? up128(5 * 2 * SK) : 0);   // corner box [5][2][4]
+  static constexpr int ST_N = ST_C + (SEAMS ? up128(5 * 2 * 4) : 0);
   alignas(128) float plane[3][5][PJ / 2][PK][2]; // dequantised state, ring over planes i .. i+2
   alignas(128) int stage[ST_N];                  // plane i+3 as stored, on its way into the ring
   alignas(128) int un[5][TJ][TK];                // f(n) of the own cells of the current plane
@@ -432,7 +436,7 @@ __device__ __forceinline__ void fx_stage_tile_impl(const FxArgs& a, const CUtens
   // aligned
   const int seam_j = fx_seam(j0, TJ, g.nj, g.per_y);
   const int seam_k = fx_seam(k0, TK, g.nk, g.per_z);
-  const bool tma = tm_in != nullptr && seam_j >= 0 && seam_k >= 0 &&
+  const bool tma = tm_in != nullptr && seam_j >= 0 && seam_k >= 0 && (Smem::SEAMS || (seam_j | seam_k) == 0) &&
                    ((smem_u32(&sm.stage[0]) | smem_u32(&sm.un[0][0][0])) & 127) == 0;
 
   // plane element (jj, kk) of variable v in ring slot sl (rows interleaved in pairs)
