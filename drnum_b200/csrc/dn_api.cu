@@ -763,7 +763,7 @@ int build_batch(dn_ctx* c)
   if (np == 0) { c->batch_dirty = false; return DN_OK; }
   const bool fp64 = c->precision == DN_FP64;
   std::vector<dn::BatchPatch> rec(np);
-  std::vector<dn::BatchMaps> maps(fp64 ? 0 : np);
+  std::vector<dn::BatchMaps> maps(np);
   long tiles = 0;
   for (size_t q = 0; q < np; ++q) {
     const DnPatch& P = c->patches[q];
@@ -781,13 +781,17 @@ int build_batch(dn_ctx* c)
     int tj, tk;
     dn::shape_tile(fp64, c->shape[q], &tj, &tk);
     if (P.owned) tiles += (long)((P.d.nj + tj - 1) / tj) * ((P.d.nk + tk - 1) / tk);
+    r.tma = 1;
     if (!fp64) {
       dn::FxGeom g{};
       g.ni = P.d.ni; g.nj = P.d.nj; g.nk = P.d.nk;
-      r.tma = 1;
       for (int b = 0; b < 3 && r.tma; ++b)
         r.tma = dn::encode_stage_maps(maps[q].in[b], &maps[q].un[b], (const int32_t*)P.buf[b],
                                       (const int32_t*)P.buf[b], g, tj, tk) ? 1 : 0;
+    } else {
+      for (int b = 0; b < 3 && r.tma; ++b)
+        r.tma = dn::encode_stage_map_f64(&maps[q].in[b][0], (const double*)P.buf[b], P.d.ni, P.d.nj, P.d.nk, tj,
+                                         tk) ? 1 : 0;
     }
   }
   const long want = (long)c->num_sms * 2 * 4;

@@ -33,8 +33,9 @@ struct WorkItem {
   int patch, j0, k0, i0, i1;
 };
 
-// Tensor maps of an FX32 patch for its tile shape, per physical buffer:
-// the staging boxes of a stage input and the box of f(n).
+// Tensor maps of a patch for its tile shape, per physical buffer.  FX32:
+// the staging boxes of a stage input (in[b][0 .. kFxMaps-1]) and the box of
+// f(n) (un[b]).  FP64: the plane box (TK+4 x TJ+4 x 1 x 5) in in[b][0].
 struct BatchMaps {
   CUtensorMap in[3][kFxMaps];
   CUtensorMap un[3];
@@ -127,7 +128,8 @@ fv_stage_batched_f64(const Batch b)
     args.wall = rec.wall;
   }
   __syncthreads();
-  fv_stage_tile<PolicyF64, TJ, TK>(args, w.j0, w.k0, w.i0, w.i1);
+  const BatchMaps* M = (b.maps && rec.tma) ? b.maps + w.patch : nullptr;
+  fv_stage_tile<PolicyF64, TJ, TK>(args, M ? &M->in[b.in_b][0] : nullptr, w.j0, w.k0, w.i0, w.i1);
 }
 
 } // namespace dn

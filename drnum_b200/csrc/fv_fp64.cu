@@ -1,7 +1,9 @@
 // FP64 stage kernel instantiation.  Built with -fmad=false: together with the
 // operation order of fv_numerics.cuh this reproduces the reference CPU
 // iterator (compiled with -ffp-contract=off) bit for bit.
+#include <cstring>
 #include "fv_launch.h"
+#include "fv_tma_host.h"
 #include "fv_batch.cuh"
 
 namespace dn {
@@ -11,6 +13,12 @@ constexpr int F64_TJ = 4;
 constexpr int F64_TK = 32;
 }
 
+bool encode_stage_map_f64(CUtensorMap* tm, const double* in, int ni, int nj, int nk, int tj, int tk)
+{
+  if (tma_disabled()) return false;
+  return encode_patch_field_map(tm, in, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 8, ni, nj, nk, tk + 4, tj + 4);
+}
+
 cudaError_t launch_stage_f64(const StageArgs<PolicyF64>& a, const StageShape& s, cudaStream_t st)
 {
   using Smem = StageSmem<PolicyF64, F64_TJ, F64_TK>;
@@ -18,10 +26,14 @@ cudaError_t launch_stage_f64(const StageArgs<PolicyF64>& a, const StageShape& s,
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(Smem));
   if (e != cudaSuccess) return e;
   (void)s;
+  StageLaunch<PolicyF64> L;
+  std::memset(&L, 0, sizeof L);
+  L.a = a;
+  L.tma = encode_stage_map_f64(&L.tm, a.in, a.g.ni, a.g.nj, a.g.nk, F64_TJ, F64_TK);
   dim3 block(F64_TK, F64_TJ, 1);
   dim3 grid((a.g.nk + F64_TK - 1) / F64_TK, (a.g.nj + F64_TJ - 1) / F64_TJ,
             (a.g.ni + a.g.i_chunk - 1) / a.g.i_chunk);
-  kern<<<grid, block, sizeof(Smem), st>>>(a);
+  kern<<<grid, block, sizeof(Smem), st>>>(L);
   return cudaGetLastError();
 }
 

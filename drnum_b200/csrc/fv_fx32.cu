@@ -2,6 +2,7 @@
 #include <cstdlib>
 #include <cstring>
 #include "fv_launch.h"
+#include "fv_tma_host.h"
 #include "fv_fx32.cuh"
 #include "fv_batch.cuh"
 
@@ -20,39 +21,9 @@ constexpr int FX_TK = DN_FX_TK;
 
 namespace {
 
-// cuTensorMapEncodeTiled of the driver, reached through the runtime's entry
-// point query (no link-time dependency on the driver library)
-using EncodeTiled = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
-                                 const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
-                                 CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
-
-EncodeTiled encode_tiled()
-{
-  static const EncodeTiled fn = [] {
-    void* p = nullptr;
-    cudaDriverEntryPointQueryResult q;
-    if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &p, 12000, cudaEnableDefault, &q) != cudaSuccess ||
-        q != cudaDriverEntryPointSuccess)
-      return (EncodeTiled) nullptr;
-    return reinterpret_cast<EncodeTiled>(p);
-  }();
-  return fn;
-}
-
-// Tensor map of one field of a patch, [5][ni][nj][nk] int32, with box
-// (bk, bj, 1, 5).  The caller has checked nk % 4 == 0 (16-byte row stride)
-// and the 16-byte alignment of the base.
 bool encode_field_map(CUtensorMap* m, const int32_t* base, const FxGeom& g, unsigned bk, unsigned bj)
 {
-  const EncodeTiled enc = encode_tiled();
-  if (!enc) return false;
-  const cuuint64_t dims[4] = {(cuuint64_t)g.nk, (cuuint64_t)g.nj, (cuuint64_t)g.ni, 5};
-  const cuuint64_t strides[3] = {(cuuint64_t)g.nk * 4, (cuuint64_t)g.nj * g.nk * 4, (cuuint64_t)g.ni * g.nj * g.nk * 4};
-  const cuuint32_t box[4] = {bk, bj, 1, 5};
-  const cuuint32_t estr[4] = {1, 1, 1, 1};
-  return enc(m, CU_TENSOR_MAP_DATA_TYPE_INT32, 4, const_cast<int32_t*>(base), dims, strides, box, estr,
-             CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
-             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+  return encode_patch_field_map(m, base, CU_TENSOR_MAP_DATA_TYPE_INT32, 4, g.ni, g.nj, g.nk, bk, bj);
 }
 
 } // namespace
@@ -61,11 +32,8 @@ bool encode_stage_maps(CUtensorMap* tm_in, CUtensorMap* tm_un, const int32_t* in
                        int tj, int tk)
 {
   // TMA staging when the rows are 16-byte strided and the fields 16-byte
-  // aligned; with DN_FX_NO_TMA=1 in the environment every tile copies cell
-  // by cell (the two give identical results)
-  const char* nt = std::getenv("DN_FX_NO_TMA");
-  if (nt && nt[0] == '1') return false;
-  if (((reinterpret_cast<uintptr_t>(in) | reinterpret_cast<uintptr_t>(un)) & 15) != 0 || g.nk % 4 != 0) return false;
+  // aligned (checked by encode_patch_field_map)
+  if (tma_disabled()) return false;
   const unsigned bj = tj + 4, bk = tk + 8;
   return encode_field_map(&tm_in[kFxMapMain], in, g, bk, bj) && encode_field_map(&tm_in[kFxMapK], in, g, 4, bj) &&
          encode_field_map(&tm_in[kFxMapJ], in, g, bk, 2) && encode_field_map(&tm_in[kFxMapC], in, g, 4, 2) &&

@@ -17,6 +17,10 @@ struct StageShape {
 };
 
 cudaError_t launch_stage_f64(const StageArgs<PolicyF64>& a, const StageShape& s, cudaStream_t st);
+// Tensor map of an FP64 stage input for tj x tk tiles (box tk+4 x tj+4 x 1 x
+// 5); false when the patch does not allow it (rows not 16-byte strided,
+// unaligned field) or DN_FX_NO_TMA=1 is set.
+bool encode_stage_map_f64(CUtensorMap* tm, const double* in, int ni, int nj, int nk, int tj, int tk);
 
 struct FxArgs;
 struct FxGeom;

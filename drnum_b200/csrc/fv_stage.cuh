@@ -8,7 +8,11 @@
 //   - a CTA owns a TJ x TK tile of (j, k) columns (k fastest, coalesced) and
 //     marches along i through a chunk of planes;
 //   - each plane of the stencil state is staged once in shared memory with a
-//     two-cell halo in j and k (a ring of four planes covers i-1 .. i+2);
+//     two-cell halo in j and k, in a ring of three planes (i .. i+2; the own
+//     column of plane i-1 is kept in registers); plane i+2 is loaded while
+//     the y and z faces of plane i are evaluated: by one TMA box load where
+//     no periodic seam crosses the tile's halo, else cell by cell with
+//     cp.async;
 //   - every face flux is evaluated exactly once: x faces per thread along its
 //     own column (the upper face of cell i is kept in registers as the lower
 //     face of cell i+1), y and z faces of the current plane into shared
@@ -30,6 +34,7 @@
 #include <cstdint>
 #include "fv_numerics.cuh"
 #include "fv_wall.cuh"
+#include "fv_tma.cuh"
 
 namespace dn {
 
@@ -81,10 +86,43 @@ struct StageSmem {
   using FaceT = typename Policy::FaceT;
   static constexpr int PJ = TJ + 4;
   static constexpr int PK = TK + 4;
-  Real plane[3][5][PJ][PK];   // planes i .. i+2 (plane i-1 of the own column is kept in registers)
+  alignas(128) Real plane[3][5][PJ][PK];   // planes i .. i+2 (plane i-1 of the own column is kept in registers)
   FaceT fy[5][TJ + 1][TK];
   FaceT fz[5][TJ][TK + 1];
+  alignas(8) uint64_t bar;                 // mbarrier of the TMA plane loads
 };
+
+// Plane ip into ring slot `slot` cell by cell: cp.async of the cells inside
+// the patch (wrapped on periodic axes), zero for cells outside a closed one
+// (never read).  The caller commits and waits.
+template <class Policy, int TJ, int TK>
+__device__ __forceinline__ void load_plane_async(StageSmem<Policy, TJ, TK>& sm, int slot,
+                                                 const typename Policy::Store* __restrict__ in,
+                                                 const StageGeom& g, int i, int j0, int k0)
+{
+  static_assert(sizeof(typename Policy::Store) == 8 && sizeof(typename Policy::Real) == 8,
+                "cell copies move the stored 8-byte value unchanged");
+  constexpr int PJ = TJ + 4, PK = TK + 4;
+  const size_t nc = (size_t)g.ni * g.nj * g.nk;
+  const int tid = threadIdx.y * TK + threadIdx.x;
+  for (int e = tid; e < 5 * PJ * PK; e += TJ * TK) {
+    const int v = e / (PJ * PK);
+    const int rem = e - v * (PJ * PK);
+    const int jj = rem / PK;
+    const int kk = rem - jj * PK;
+    const int j = axis_idx(j0 - 2 + jj, g.nj, g.per_y);
+    const int k = axis_idx(k0 - 2 + kk, g.nk, g.per_z);
+    typename Policy::Real* dst = &sm.plane[slot][v][jj][kk];
+    if (j >= 0 && k >= 0) {
+      const unsigned sa = smem_u32(dst);
+      asm volatile("cp.async.ca.shared.global [%0], [%1], 8;"
+                   :: "r"(sa), "l"(in + v * nc + ((size_t)i * g.nj + j) * g.nk + k) : "memory");
+    } else {
+      *dst = typename Policy::Real(0);
+    }
+  }
+  asm volatile("cp.async.commit_group;" ::: "memory");
+}
 
 template <class Policy, int TJ, int TK>
 __device__ __forceinline__ void load_plane(StageSmem<Policy, TJ, TK>& sm, int slot,
@@ -114,13 +152,15 @@ __device__ __forceinline__ void load_plane(StageSmem<Policy, TJ, TK>& sm, int sl
 }
 
 // One tile of one patch: columns (j0 .. j0+TJ-1, k0 .. k0+TK-1), planes i0 .. i1-1.
+// tm: tensor map of the stage input with box (TK+4, TJ+4, 1, 5), or null.
 template <class Policy, int TJ, int TK>
-__device__ __forceinline__ void fv_stage_tile(const StageArgs<Policy>& a, int j0, int k0, int i0, int i1)
+__device__ __forceinline__ void fv_stage_tile(const StageArgs<Policy>& a, const CUtensorMap* tm, int j0, int k0,
+                                              int i0, int i1)
 {
   using Real = typename Policy::Real;
   using FaceT = typename Policy::FaceT;
   using Smem = StageSmem<Policy, TJ, TK>;
-  extern __shared__ __align__(16) unsigned char dn_smem_raw[];
+  extern __shared__ __align__(128) unsigned char dn_smem_raw[];
   Smem& sm = *reinterpret_cast<Smem*>(dn_smem_raw);
 
   const StageGeom& g = a.g;
@@ -129,6 +169,20 @@ __device__ __forceinline__ void fv_stage_tile(const StageArgs<Policy>& a, int j0
   const bool own = (j < g.nj) && (k < g.nk);
   const size_t nc = (size_t)g.ni * g.nj * g.nk;
   const Real Ax = a.p.Ax, Ay = a.p.Ay, Az = a.p.Az;
+  const int tid = ty * TK + tx;
+  // TMA plane loads where no periodic seam crosses the tile's halo (on a
+  // closed axis the box cells outside the patch are zero-filled, as the
+  // cell copies write them); the box starts at column k0-2, a multiple of 2
+  // elements (16 bytes) since TK is even
+  constexpr unsigned kPlaneBytes = 5u * (TJ + 4) * (TK + 4) * sizeof(Real);
+  const bool tma = tm != nullptr && (!g.per_y || (j0 >= 2 && j0 + TJ + 2 <= g.nj)) &&
+                   (!g.per_z || (k0 >= 2 && k0 + TK + 2 <= g.nk)) && (smem_u32(&sm.plane[0][0][0][0]) & 127) == 0;
+  if (tma && tid == 0) {
+    mbar_init(&sm.bar, 1);
+    mbar_init_fence();
+  }
+  unsigned phase = 0;
+  bool tbad = false;
 
   // a three-plane ring, slot of plane p = p mod 3, rotated by hand: sa, sb,
   // sc hold planes i-1, i, i+1 at the top of iteration i
@@ -171,35 +225,21 @@ __device__ __forceinline__ void fv_stage_tile(const StageArgs<Policy>& a, int j0
     #pragma unroll
     for (int v = 0; v < 5; ++v) xm1[v] = sm.plane[sa][v][ty + 2][tx + 2];
     __syncthreads();
-    load_plane<Policy, TJ, TK>(sm, sa, a.in, a.p, g, i + 2, j0, k0);
-    __syncthreads();
-    const int s0 = sb, sp1 = sc, sp2 = sa;
-
-    // x face above cell i (between i and i+1), own column
-    FaceT fx_hi[5];
-    {
-      const bool ex = face_exists(i + 1, g.ni, g.per_x);
-      if (ex && own) {
-        Real vl[5], vr[5], F[5];
-        const bool sl = cell_ok(i - 1, g.ni, g.per_x);
-        const bool sr = cell_ok(i + 2, g.ni, g.per_x);
-        #pragma unroll
-        for (int v = 0; v < 5; ++v) {
-          const Real um2 = xm1[v];
-          const Real um1 = sm.plane[s0][v][ty + 2][tx + 2];
-          const Real up0 = sm.plane[sp1][v][ty + 2][tx + 2];
-          const Real up1 = sm.plane[sp2][v][ty + 2][tx + 2];
-          vl[v] = upwind2_left(um2, um1, up0, sl);
-          vr[v] = upwind2_right(um1, up0, up1, sr);
+    // plane i+2 into the freed slot, arriving while the y and z faces of
+    // plane i are evaluated (a plane outside a closed patch is never read)
+    const int ip2 = axis_idx(i + 2, g.ni, g.per_x);
+    if (ip2 >= 0) {
+      if (tma) {
+        if (tid == 0) {
+          fence_proxy_async_smem();
+          mbar_arrive_expect_tx(&sm.bar, kPlaneBytes);
+          tma_load_4d(&sm.plane[sa][0][0][0], tm, &sm.bar, k0 - 2, j0 - 2, ip2, 0);
         }
-        ausm_plus<0>(face_side(vl), face_side(vr), Ax, F);
-        #pragma unroll
-        for (int v = 0; v < 5; ++v) fx_hi[v] = Policy::face(a.p, v, F[v]);
       } else {
-        #pragma unroll
-        for (int v = 0; v < 5; ++v) fx_hi[v] = FaceT(0);
+        load_plane_async<Policy, TJ, TK>(sm, sa, a.in, g, ip2, j0, k0);
       }
     }
+    const int s0 = sb, sp1 = sc, sp2 = sa;
 
     // y faces of plane i: face at row jj (0..TJ) lies below cell j0+jj
     // (the items beyond one per thread, the faces below halo row TJ, fall to
@@ -263,7 +303,45 @@ __device__ __forceinline__ void fv_stage_tile(const StageArgs<Policy>& a, int j0
       #pragma unroll
       for (int v = 0; v < 5; ++v) sm.fz[v][jj][kk] = out[v];
     }
+    // plane i+2 has arrived (this thread's copies, or the TMA box); the
+    // barrier publishes it and the y and z faces
+    if (ip2 >= 0) {
+      if (tma) {
+        tbad |= !mbar_wait(&sm.bar, phase);
+        phase ^= 1u;
+      } else {
+        asm volatile("cp.async.wait_group 0;" ::: "memory");
+      }
+    }
     __syncthreads();
+
+    // x face above cell i (between i and i+1), own column
+    FaceT fx_hi[5];
+    {
+
+      const bool ex = face_exists(i + 1, g.ni, g.per_x);
+      if (ex && own) {
+        Real vl[5], vr[5], F[5];
+        const bool sl = cell_ok(i - 1, g.ni, g.per_x);
+        const bool sr = cell_ok(i + 2, g.ni, g.per_x);
+        #pragma unroll
+        for (int v = 0; v < 5; ++v) {
+          const Real um2 = xm1[v];
+          const Real um1 = sm.plane[s0][v][ty + 2][tx + 2];
+          const Real up0 = sm.plane[sp1][v][ty + 2][tx + 2];
+          const Real up1 = sm.plane[sp2][v][ty + 2][tx + 2];
+          vl[v] = upwind2_left(um2, um1, up0, sl);
+          vr[v] = upwind2_right(um1, up0, up1, sr);
+        }
+        ausm_plus<0>(face_side(vl), face_side(vr), Ax, F);
+        #pragma unroll
+        for (int v = 0; v < 5; ++v) fx_hi[v] = Policy::face(a.p, v, F[v]);
+      } else {
+        #pragma unroll
+        for (int v = 0; v < 5; ++v) fx_hi[v] = FaceT(0);
+      }
+    }
+
 
     if (own) {
       const size_t c = ((size_t)i * g.nj + j) * g.nk + k;
@@ -313,15 +391,26 @@ __device__ __forceinline__ void fv_stage_tile(const StageArgs<Policy>& a, int j0
     sb = sc;
     sc = sp2;
   }
+  if (tbad && a.err) atomicOr(a.err, 32);
 }
+
+// Parameters of the single-patch launch: the stage arguments and the tensor
+// map of the stage input (valid when tma != 0).
+template <class Policy>
+struct StageLaunch {
+  CUtensorMap tm;
+  StageArgs<Policy> a;
+  int tma;
+};
 
 // One patch per launch: grid (k tiles, j tiles, i chunks).
 template <class Policy, int TJ, int TK>
 __global__ void __launch_bounds__(TJ * TK)
-fv_stage_kernel(const StageArgs<Policy> a)
+fv_stage_kernel(const __grid_constant__ StageLaunch<Policy> L)
 {
-  const int i0 = blockIdx.z * a.g.i_chunk;
-  fv_stage_tile<Policy, TJ, TK>(a, blockIdx.y * TJ, blockIdx.x * TK, i0, min(a.g.ni, i0 + a.g.i_chunk));
+  const int i0 = blockIdx.z * L.a.g.i_chunk;
+  fv_stage_tile<Policy, TJ, TK>(L.a, L.tma ? &L.tm : nullptr, blockIdx.y * TJ, blockIdx.x * TK, i0,
+                                min(L.a.g.ni, i0 + L.a.g.i_chunk));
 }
 
 } // namespace dn

@@ -1,6 +1,6 @@
-"""The two ways the FP32 bulk stage stages its planes give identical bits:
-TMA box loads for tiles whose halo lies inside the patch, and cell-by-cell
-asynchronous copies (with wrapped or clamped cells) for the others.  With
+"""The two ways the stage kernels stage their planes give identical bits:
+TMA box loads, and cell-by-cell asynchronous copies (with wrapped or
+clamped cells) for the tiles TMA cannot serve.  With
 DN_FX_NO_TMA=1 every tile copies cell by cell; the results must not
 change, on periodic, closed and mixed patches, with inactive cells, and
 with the per-stage residual and conservation sums."""
@@ -10,13 +10,13 @@ import numpy as np
 import pytest
 
 from drnum_b200 import cases
-from drnum_b200._lib import DN_FP32
+from drnum_b200._lib import DN_FP32, DN_FP64
 from drnum_b200.api import AusmPlus, B200CartesianIterator, CartesianPatch
 
 pytestmark = pytest.mark.gpu
 
 
-def run_fx32(U0, h, dt, steps, periodic, active=None, no_tma=False):
+def run_fx32(U0, h, dt, steps, periodic, active=None, no_tma=False, precision=DN_FP32):
     old = os.environ.get("DN_FX_NO_TMA")
     os.environ["DN_FX_NO_TMA"] = "1" if no_tma else "0"
     try:
@@ -25,7 +25,7 @@ def run_fx32(U0, h, dt, steps, periodic, active=None, no_tma=False):
         p.setField(0, U0)
         if active is not None:
             p.active[...] = active
-        it = B200CartesianIterator(AusmPlus(), 0, DN_FP32)
+        it = B200CartesianIterator(AusmPlus(), 0, precision)
         it.addPatch(p)
         it.updateDevice(fields=(0,))
         for _ in range(steps):
@@ -103,3 +103,19 @@ def test_batched_tma_staging_equals_cell_copies(name, scale, shapes):
     b = run_workload_fx32(name, scale, 3, True, shapes)
     for x, y in zip(a, b):
         assert np.array_equal(x, y)
+
+
+@pytest.mark.parametrize("shape,periodic", [
+    ((24, 40, 72), (True, True, True)),      # 4 x 32 tiles: interior, seam and ragged
+    ((20, 18, 40), (False, False, False)),   # closed: every tile by TMA, zero-filled halo
+    ((16, 22, 66), (False, True, True)),
+])
+def test_fp64_tma_staging_equals_cell_copies(shape, periodic):
+    ni, nj, nk = shape
+    U0 = cases.random_state(ni, nj, nk, seed=3 * ni + nk, amp=0.03, mach=0.4)
+    h = 1.0 / 32
+    dt = cases.cfl_dt(U0, h, 0.5)
+    a, sa = run_fx32(U0, h, dt, 2, periodic, precision=DN_FP64)
+    b, sb = run_fx32(U0, h, dt, 2, periodic, no_tma=True, precision=DN_FP64)
+    assert np.array_equal(a, b)
+    assert not np.array_equal(a, U0)
