@@ -27,6 +27,11 @@
  * The PATCH a functor sees is dn::FunctorPatch, a device view of the stage
  * input with the accessors the reference's functors and reconstructions call
  * (f, getVar, checkRange, index, isSplitFace, sizeI/J/K, dx/dy/dz, ...).
+ * Inside the stage kernel the view reads from a shared-memory copy of the
+ * CTA's tile: planes i-1 .. i+2 of the current plane i with a two-cell halo
+ * in j and k, copied asynchronously one plane ahead (the stencils of the
+ * reference's reconstructions and viscous gradients stay inside it); reads
+ * outside that window go to global memory.
  * Periodic axes wrap indices (size_t arithmetic that went below zero wraps
  * too), so a functor needs no ghost layers; closed axes behave as the
  * reference's patch edges (checkRange false outside).  Field 0 is the stage
@@ -58,6 +63,13 @@ public:
   double m_D[3] = {1, 1, 1};
   size_t m_NC = 0;
   int m_Id = 0;
+  /* shared-memory window (set by the stage kernel, null elsewhere): planes
+     m_P0 .. m_P0+3 in ring slots m_S0, m_S0+1, ... (mod kSlots), rows
+     m_J0 .. m_J0+m_WJ-1, columns m_K0 .. m_K0+m_WK-1, [slot][var][row][col] */
+  static constexpr int kSlots = 5;
+  const double* m_Tile = nullptr;
+  long long m_P0 = 0, m_J0 = 0, m_K0 = 0;
+  int m_S0 = 0, m_WJ = 0, m_WK = 0;
 
   __device__ __forceinline__ size_t sizeI() const { return m_N[0]; }
   __device__ __forceinline__ size_t sizeJ() const { return m_N[1]; }
@@ -108,6 +120,17 @@ public:
      functors read field 0) */
   __device__ __forceinline__ double f(size_t, size_t var, size_t i, size_t j, size_t k) const
   {
+    if (m_Tile) {
+      /* indices that went below zero wrapped as size_t; as signed values
+         they address the halo, which holds the wrapped cells */
+      const long long dp = (long long)i - m_P0, dj = (long long)j - m_J0, dk = (long long)k - m_K0;
+      if ((unsigned long long)dp < 4ull && (unsigned long long)dj < (unsigned long long)m_WJ &&
+          (unsigned long long)dk < (unsigned long long)m_WK) {
+        int sl = m_S0 + (int)dp;
+        if (sl >= kSlots) sl -= kSlots;
+        return m_Tile[(((size_t)sl*5 + var)*m_WJ + (size_t)dj)*m_WK + (size_t)dk];
+      }
+    }
     return __ldg(m_In + var*m_NC + index(i, j, k));
   }
   __device__ __forceinline__ void getVar(size_t field, size_t i, size_t j, size_t k, double* var) const
@@ -169,9 +192,42 @@ __device__ __forceinline__ bool face_exists(int x, int n, int per)
 
 template <int TJ, int TK>
 struct Smem {
+  static constexpr int PJ = TJ + 4, PK = TK + 4;
+  double plane[FunctorPatch::kSlots][5][PJ][PK];   /* ring of planes, rows j0-2.., columns k0-2.. */
   double fy[5][TJ + 1][TK];                  /* face below row jj of the tile */
   double fz[5][TJ][TK + 1];                  /* face below column kk */
 };
+
+/* ring slot of plane p >= -1 */
+__device__ __forceinline__ int ring_slot(int p) { return (p + FunctorPatch::kSlots) % FunctorPatch::kSlots; }
+
+/* Plane p of the stage input into its ring slot, cell by cell with cp.async:
+   cells inside the patch (wrapped on periodic axes), zero for cells outside
+   a closed one.  Commits one copy group. */
+template <int TJ, int TK>
+__device__ __forceinline__ void load_plane(Smem<TJ, TK>& sm, const FunctorPatch& P, int p, int j0, int k0)
+{
+  constexpr int PJ = TJ + 4, PK = TK + 4;
+  const int sl = ring_slot(p);
+  const long long ip = P.axis(0, (size_t)(long long)p);
+  const int tid = threadIdx.y * TK + threadIdx.x;
+  for (int e = tid; e < 5 * PJ * PK; e += TJ * TK) {
+    const int v = e / (PJ * PK);
+    const int rem = e - v * (PJ * PK);
+    const int jj = rem / PK, kk = rem - jj * PK;
+    const long long jg = P.axis(1, (size_t)(long long)(j0 - 2 + jj));
+    const long long kg = P.axis(2, (size_t)(long long)(k0 - 2 + kk));
+    double* dst = &sm.plane[sl][v][jj][kk];
+    if (ip >= 0 && jg >= 0 && kg >= 0) {
+      const double* src = P.m_In + v*P.m_NC + ((size_t)ip*P.m_N[1] + (size_t)jg)*P.m_N[2] + (size_t)kg;
+      const unsigned sa = (unsigned)__cvta_generic_to_shared(dst);
+      asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" :: "r"(sa), "l"(src) : "memory");
+    } else {
+      *dst = 0.0;
+    }
+  }
+  asm volatile("cp.async.commit_group;" ::: "memory");
+}
 
 struct Args {
   FunctorPatch view;
@@ -185,8 +241,9 @@ template <class OP, int TJ, int TK>
 __global__ void __launch_bounds__(TJ * TK, 2)
 functor_stage_kernel(const Args a, OP op)
 {
-  __shared__ Smem<TJ, TK> sm;
-  const FunctorPatch& P = a.view;
+  extern __shared__ __align__(16) unsigned char functor_smem_raw[];
+  Smem<TJ, TK>& sm = *reinterpret_cast<Smem<TJ, TK>*>(functor_smem_raw);
+  FunctorPatch P = a.view;
   const int ni = (int)P.m_N[0], nj = (int)P.m_N[1], nk = (int)P.m_N[2];
   const int px = P.m_Per[0], py = P.m_Per[1], pz = P.m_Per[2];
   const int tx = threadIdx.x, ty = threadIdx.y;
@@ -199,6 +256,19 @@ functor_stage_kernel(const Args a, OP op)
   const double Ax = dy*dz, Ay = dx*dz, Az = dx*dy;   /* cartesianiterator.h:96-98 */
   const double yc = 0.5*dy + j*dy, zc = 0.5*dz + k*dz;
 
+  /* planes i0-1 .. i0+2 into the ring; the first x face (below i0) reads
+     plane i0-2 from global memory */
+  for (int p = i0 - 1; p <= i0 + 2; ++p) load_plane<TJ, TK>(sm, P, p, j0, k0);
+  asm volatile("cp.async.wait_group 0;" ::: "memory");
+  __syncthreads();
+  P.m_Tile = &sm.plane[0][0][0][0];
+  P.m_J0 = j0 - 2;
+  P.m_K0 = k0 - 2;
+  P.m_WJ = TJ + 4;
+  P.m_WK = TK + 4;
+  P.m_P0 = i0 - 1;
+  P.m_S0 = ring_slot(i0 - 1);
+
   double flo[5];
   if (own && face_exists(i0, ni, px)) {
     double F[5] = {0, 0, 0, 0, 0};
@@ -209,6 +279,11 @@ functor_stage_kernel(const Args a, OP op)
   }
 
   for (int i = i0; i < i1; ++i) {
+    /* plane i+3 into the slot of plane i-2 (last read in the previous
+       iteration, before its final barrier); the window moves to i-1 .. i+2 */
+    if (i + 3 <= i1 + 1) load_plane<TJ, TK>(sm, P, i + 3, j0, k0);
+    P.m_P0 = i - 1;
+    P.m_S0 = ring_slot(i - 1);
     const double xc = 0.5*dx + i*dx;
     double fhi[5];
     if (own && face_exists(i + 1, ni, px)) {
@@ -302,6 +377,9 @@ functor_stage_kernel(const Args a, OP op)
       }
     }
     for (int v = 0; v < 5; ++v) flo[v] = fhi[v];
+    /* plane i+3 has arrived; the barrier publishes it and ends the reads of
+       the face arrays and of plane i-1 */
+    asm volatile("cp.async.wait_group 0;" ::: "memory");
     __syncthreads();
   }
 }
@@ -333,7 +411,11 @@ cudaError_t launch_functor_stage(const dn_stage_launch* L, const OP& op)
   a.i_chunk = (int)((L->ni + chunks - 1) / chunks);
   const dim3 grid(tk, tj, (L->ni + a.i_chunk - 1) / a.i_chunk);
   const dim3 block(TK, TJ);
-  functor_detail::functor_stage_kernel<OP, TJ, TK><<<grid, block, 0, (cudaStream_t)L->stream>>>(a, op);
+  auto kern = functor_detail::functor_stage_kernel<OP, TJ, TK>;
+  const int smem = (int)sizeof(functor_detail::Smem<TJ, TK>);
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  if (e != cudaSuccess) return e;
+  kern<<<grid, block, smem, (cudaStream_t)L->stream>>>(a, op);
   return cudaGetLastError();
 }
 
