@@ -46,37 +46,119 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
+# Polling loop of the clock sampler, run as its own process (its own
+# interpreter lock: the timing thread may hold the parent's while it waits
+# on the GPU).  argv: GPU UUID, output path.  NVML read-only queries only.
+_CLOCK_POLLER = r"""
+import sys, time, pynvml
+pynvml.nvmlInit()
+want = sys.argv[1].lower().replace("gpu-", "")
+h = None
+for q in range(pynvml.nvmlDeviceGetCount()):
+    c = pynvml.nvmlDeviceGetHandleByIndex(q)
+    u = pynvml.nvmlDeviceGetUUID(c)
+    u = (u.decode() if isinstance(u, bytes) else u).lower().replace("gpu-", "")
+    if u == want:
+        h = c
+if h is None:
+    sys.exit(3)
+smax = pynvml.nvmlDeviceGetMaxClockInfo(h, pynvml.NVML_CLOCK_SM)
+with open(sys.argv[2], "w", buffering=1) as f:
+    f.write("time,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons\n")
+    while True:
+        sm = pynvml.nvmlDeviceGetClockInfo(h, pynvml.NVML_CLOCK_SM)
+        rs = pynvml.nvmlDeviceGetCurrentClocksEventReasons(h)
+        pw = pynvml.nvmlDeviceGetPowerUsage(h) / 1000.0
+        f.write(f"{time.time():.6f},{sm},{smax},{pw:.1f},{rs}\n")
+        time.sleep(0.001)
+"""
+
+
 class ClockSampler:
-    """Samples nvidia-smi clocks and throttle reasons while running."""
+    """Samples the SM clock, power and clock-event reasons of this rank's GPU
+    during a timed region: a separate process polls NVML's read-only queries
+    about every millisecond, and the samples whose timestamps fall between
+    start() returning and stop() being called are kept (the file
+    gpurun_out/clocks_bench_rank<r>.csv holds them all).  Falls back to
+    nvidia-smi where NVML is unavailable."""
 
     QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    # NVML clock-event reason bits (nvmlClocksEventReason*)
+    REASONS = (("hw_slowdown", 0x8), ("hw_thermal_slowdown", 0x40), ("sw_thermal_slowdown", 0x20),
+               ("sw_power_cap", 0x4))
 
     def __init__(self, device_index):
         self.device_index = device_index
         self.proc = None
+        self.mode = None
         self.path = os.path.join(ROOT, "gpurun_out", f"clocks_bench_rank{device_index}.csv")
 
     def start(self):
+        os.makedirs(os.path.dirname(self.path), exist_ok=True)
         try:
-            os.makedirs(os.path.dirname(self.path), exist_ok=True)
+            import torch
+            uuid = str(torch.cuda.get_device_properties(self.device_index).uuid)
+            if os.path.exists(self.path):
+                os.remove(self.path)
+            self.proc = subprocess.Popen([sys.executable, "-c", _CLOCK_POLLER, uuid, self.path],
+                                         stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
+            # ready once the first sample is written (at most a few seconds)
+            t_end = time.time() + 20.0
+            while time.time() < t_end and self.proc.poll() is None:
+                if os.path.exists(self.path) and sum(1 for _ in open(self.path)) >= 2:
+                    self.mode = "nvml"
+                    self.t0 = time.time()
+                    return
+                time.sleep(0.01)
+            self._kill()
+        except Exception:
+            self._kill()
+        try:
             self.f = open(self.path, "w")
             self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.device_index}", f"--query-gpu={self.QUERY}",
                                           "--format=csv,noheader,nounits", "-lms", "100"],
                                          stdout=self.f, stderr=subprocess.DEVNULL)
+            self.mode = "nvidia-smi"
         except OSError:
             self.proc = None
 
+    def _kill(self):
+        if self.proc is not None and self.proc.poll() is None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+        self.proc = None
+
     def stop(self):
+        if self.mode == "nvml":
+            t1 = time.time()
+            time.sleep(0.005)
+            self._kill()
+            sm, smax, reasons = [], [], set()
+            for line in open(self.path).readlines()[1:]:
+                parts = line.strip().split(",")
+                if len(parts) < 5:
+                    continue
+                try:
+                    t, c, cm, rs = float(parts[0]), float(parts[1]), float(parts[2]), int(parts[4])
+                except ValueError:
+                    continue
+                if self.t0 <= t <= t1:
+                    sm.append(c)
+                    smax.append(cm)
+                    reasons.update(nm for nm, bit in self.REASONS if rs & bit)
+            if not sm:
+                return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"], "source": "nvml"}
+            return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": float(max(smax)), "reasons": sorted(reasons),
+                    "samples": len(sm), "source": "nvml"}
         if self.proc is None:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
         time.sleep(0.25)
-        self.proc.terminate()
-        try:
-            self.proc.wait(timeout=5)
-        except subprocess.TimeoutExpired:
-            self.proc.kill()
+        self._kill()
         self.f.close()
         sm, smax, reasons = [], [], set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
@@ -95,7 +177,7 @@ class ClockSampler:
         if not sm:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
         return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": float(max(smax)), "reasons": sorted(reasons),
-                "samples": len(sm)}
+                "samples": len(sm), "source": "nvidia-smi"}
 
 
 def cpu_baseline(U0, h, dt, budget_s=20.0):
