@@ -445,6 +445,18 @@ class B200CartesianIterator:
                                                      ctypes.byref(mx), ctypes.byref(l2)))
         return mx.value, l2.value
 
+    def flowStats(self, i_field, dt, patches=None):
+        """The reference applications' output-step diagnostics over the
+        given patches (default: all): (CFL_max, rho_min, rho_max) with
+        CFL = max(|u|, |u+a|, |u-a|) dt / dx per cell
+        (drnumBaseFlowDemo/main.h:255-284), reduced over the patches."""
+        cfl, rmin, rmax = 0.0, 1000.0, 0.0
+        out = np.zeros(3)
+        for p in (range(self.numPatches()) if patches is None else patches):
+            check(self.ctx, self.lib.dn_flow_stats(self.ctx, p, i_field, float(dt), _lib.dptr(out)))
+            cfl, rmin, rmax = max(cfl, out[0]), min(rmin, out[1]), max(rmax, out[2])
+        return cfl, rmin, rmax
+
     def setOption(self, option, value):
         """dn_set_option: DN_OPT_BATCHED (one launch per stage over all
         patches) or DN_OPT_GRAPH (CUDA-graph replay of whole steps)."""

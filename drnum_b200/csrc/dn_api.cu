@@ -279,6 +279,60 @@ k_partial_sums_i32(const int32_t* __restrict__ f, size_t nc, long long* __restri
   if (threadIdx.x < 5) partials[blockIdx.x * 5 + threadIdx.x] = red[threadIdx.x][0];
 }
 
+// Flow diagnostics of the reference applications' output step
+// (drnumBaseFlowDemo/main.h:255-284, drnumBasicAero/main.h:608-637): per
+// cell PerfectGas::conservativeToPrimitive (perfectgas.h:84-93),
+// a = sqrt(gamma R T), CFL = max(|u|, |u+a|, |u-a|) dt / dx, and the density
+// range.  Written with round-to-nearest intrinsics (no contraction), so each
+// cell's values equal the reference's FP64 loop and the extrema are exact.
+// Per-block partials: [cfl_max, rho_min, rho_max].
+template <typename T>
+__global__ void __launch_bounds__(kSumThreads)
+k_flow_stats(const T* __restrict__ f, size_t nc, QParams q, int quantized, double dt, double dx,
+             double* __restrict__ partials)
+{
+  __shared__ double s_cfl[kSumThreads], s_rmin[kSumThreads], s_rmax[kSumThreads];
+  const size_t per = (nc + gridDim.x - 1) / gridDim.x;
+  const size_t c0 = blockIdx.x * per;
+  const size_t c1 = c0 + per < nc ? c0 + per : nc;
+  double cfl = 0.0, rmin = 1000.0, rmax = 0.0;   // the applications' start values
+  for (size_t c = c0 + threadIdx.x; c < c1; c += blockDim.x) {
+    double var[5];
+    #pragma unroll
+    for (int v = 0; v < 5; ++v) {
+      const double x = (double)f[v * nc + c];
+      var[v] = quantized ? __dadd_rn(q.base[v], __dmul_rn(q.q[v], x)) : x;
+    }
+    rmin = fmin(var[0], rmin);
+    rmax = fmax(var[0], rmax);
+    const double ir = __ddiv_rn(1.0, var[0]);
+    const double u = __dmul_rn(var[1], ir), v = __dmul_rn(var[2], ir), w = __dmul_rn(var[3], ir);
+    const double ke = __dadd_rn(__dadd_rn(__dmul_rn(u, u), __dmul_rn(v, v)), __dmul_rn(w, w));
+    const double T = __ddiv_rn(__dsub_rn(__dmul_rn(var[4], ir), __dmul_rn(0.5, ke)), dn::Gas::cv);
+    const double a = __dsqrt_rn(__dmul_rn(__dmul_rn(dn::Gas::gamma, dn::Gas::R), T));
+    cfl = fmax(cfl, __ddiv_rn(__dmul_rn(fabs(u), dt), dx));
+    cfl = fmax(cfl, __ddiv_rn(__dmul_rn(fabs(__dadd_rn(u, a)), dt), dx));
+    cfl = fmax(cfl, __ddiv_rn(__dmul_rn(fabs(__dsub_rn(u, a)), dt), dx));
+  }
+  s_cfl[threadIdx.x] = cfl;
+  s_rmin[threadIdx.x] = rmin;
+  s_rmax[threadIdx.x] = rmax;
+  __syncthreads();
+  for (int st = kSumThreads / 2; st > 0; st >>= 1) {
+    if ((int)threadIdx.x < st) {
+      s_cfl[threadIdx.x] = fmax(s_cfl[threadIdx.x], s_cfl[threadIdx.x + st]);
+      s_rmin[threadIdx.x] = fmin(s_rmin[threadIdx.x], s_rmin[threadIdx.x + st]);
+      s_rmax[threadIdx.x] = fmax(s_rmax[threadIdx.x], s_rmax[threadIdx.x + st]);
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    partials[blockIdx.x * 3] = s_cfl[0];
+    partials[blockIdx.x * 3 + 1] = s_rmin[0];
+    partials[blockIdx.x * 3 + 2] = s_rmax[0];
+  }
+}
+
 // max and sum of squared differences of two variables (Patch::computeVariableDifference)
 template <typename T>
 __global__ void __launch_bounds__(kSumThreads)
@@ -1455,6 +1509,41 @@ int dn_field_difference(dn_ctx* c, int id, int f1, int v1, int f2, int v2, doubl
   *max_norm = std::sqrt(mx);
   *l2_norm = std::sqrt(sm);
   return DN_OK;
+}
+
+int dn_flow_stats(dn_ctx* c, int id, int field, double dt, double out[3])
+{
+  int s = check_patch(c, id);
+  if (s) return s;
+  if ((s = check_field(c, field))) return s;
+  if (!out) return fail(c, DN_ERR_ARG, "output pointer is NULL");
+  if (set_device(c) != DN_OK) return DN_ERR_CUDA;
+  if ((s = ensure_partials(c, (size_t)kSumBlocks * 3))) return s;
+  DnPatch& p = c->patches[id];
+  QParams q = qparams(p);
+  const void* f = p.buf[c->fmap[field]];
+  if (c->precision == DN_FP64)
+    k_flow_stats<double><<<kSumBlocks, kSumThreads, 0, c->stream>>>((const double*)f, p.nc, q, 0, dt, p.d.dx,
+                                                                   c->d_partials);
+  else
+    k_flow_stats<int32_t><<<kSumBlocks, kSumThreads, 0, c->stream>>>((const int32_t*)f, p.nc, q, 1, dt, p.d.dx,
+                                                                    c->d_partials);
+  c->launches++;
+  std::vector<double> h((size_t)kSumBlocks * 3);
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess) e = cudaMemcpyAsync(h.data(), c->d_partials, h.size() * sizeof(double), cudaMemcpyDeviceToHost, c->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+  if (e != cudaSuccess) return cuda_fail(c, e, "flow statistics");
+  double cfl = 0.0, rmin = 1000.0, rmax = 0.0;
+  for (int b = 0; b < kSumBlocks; ++b) {
+    cfl = std::max(cfl, h[(size_t)b * 3]);
+    rmin = std::min(rmin, h[(size_t)b * 3 + 1]);
+    rmax = std::max(rmax, h[(size_t)b * 3 + 2]);
+  }
+  out[0] = cfl;
+  out[1] = rmin;
+  out[2] = rmax;
+  return read_device_error(c);
 }
 
 int dn_patch_set_bc(dn_ctx* c, int id, int side, int kind, const double* params, const double* table)

@@ -96,6 +96,19 @@ def rk_step_sequence(ops, dt, alphas):
         ops.post_operations()
 
 
+def reduce_flow_stats(local, group=None):
+    """Max of the CFL numbers and the density maxima, min of the density
+    minima over the ranks of `group` (CPU tensors: the values are three
+    doubles; gloo and NCCL groups both take them through all_reduce on the
+    group's device)."""
+    import torch
+    import torch.distributed as dist
+    dev = "cuda" if dist.get_backend(group) == "nccl" else "cpu"
+    t = torch.tensor([local[0], -local[1], local[2]], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX, group=group)
+    return float(t[0]), float(-t[1]), float(t[2])
+
+
 class ShardedIterator:
     """The GPU side: a B200CartesianIterator holding every patch of the grid
     (donor tables computed for all of them), owning the patches `owner`
@@ -105,7 +118,7 @@ class ShardedIterator:
 
     def __init__(self, it, owner, rank, world, group=None):
         import torch
-        self.it, self.owner, self.rank, self.world = it, list(owner), rank, world
+        self.it, self.owner, self.rank, self.world, self.group = it, list(owner), rank, world, group
         lib = it.lib
         for p in range(it.numPatches()):
             check(it.ctx, lib.dn_patch_set_owned(it.ctx, p, 1 if self.owner[p] == rank else 0))
@@ -156,6 +169,12 @@ class ShardedIterator:
 
     def rkStep(self, dt, alphas):
         rk_step_sequence(self, dt, alphas)
+
+    def flowStats(self, field, dt):
+        """(CFL_max, rho_min, rho_max) of the whole grid: this rank's owned
+        patches on its GPU, then a max / min all-reduce over the ranks."""
+        local = self.it.flowStats(field, dt, [p for p in range(len(self.owner)) if self.owner[p] == self.rank])
+        return reduce_flow_stats(local, self.group)
 
     def close(self):
         if self.ex:

@@ -20,6 +20,8 @@
  *     (patchiterator.h:80-87, gpu_cartesianiterator.h:218-304)
  *   RungeKutta::operator()(dt) (rungekutta.cpp:27-42)        dn_rk_step
  *   Patch::computeVariableDifference (patch.cpp:733-746)     dn_field_difference
+ *   the applications' CFL / density diagnostics              dn_flow_stats
+ *     (drnumBaseFlowDemo/main.h:255-284)
  *   PatchGrid::computeDependencies (patchgrid.cpp:119-268)   dn_grid_compute_dependencies
  *   PatchIterator::copyDonorData (patchiterator.h:106-111)   dn_copy_donor_data
  *   LevelSetObject + CPU_LevelSetObjectBC                    dn_patch_set_levelset,
@@ -183,6 +185,15 @@ int dn_conservation_sums(dn_ctx* ctx, double out[5]);
  * Replaces: Patch::computeVariableDifference (patch.cpp:733-746). */
 int dn_field_difference(dn_ctx* ctx, int patch_id, int i_field1, int i_var1,
                         int i_field2, int i_var2, double* max_norm, double* l2_norm);
+
+/* Diagnostics of one patch's field as the reference applications compute
+ * them at each output step: out[0] = max over cells of max(|u|, |u+a|,
+ * |u-a|) * dt / dx (the CFL number of time step dt), out[1] = min(1000,
+ * min rho), out[2] = max(0, max rho); per cell in FP64 with the reference's
+ * operation order, so the values equal the reference's loop.
+ * Replaces: the loop of drnumBaseFlowDemo/main.h:255-284 and
+ * drnumBasicAero/main.h:608-637 over a host copy of the field. */
+int dn_flow_stats(dn_ctx* ctx, int patch_id, int i_field, double dt, double out[3]);
 
 /* Builds the donor tables of every patch from the patches' geometry and seek
  * and protection layers: receiving cells, donor patches, 8-point trilinear

@@ -435,3 +435,21 @@ def oracle_grid_run(states, spacings, tables, dt, steps, alpha=(0.25, 0.5, 1.0),
             if layers is not None:
                 oracle_levelset_bc(U, layers)
     return U
+
+
+def oracle_flow_stats(U, dt, dx):
+    """The reference applications' output-step diagnostics of one patch
+    (drnumBaseFlowDemo/main.h:255-284; PerfectGas::conservativeToPrimitive,
+    perfectgas.h:84-93, with R = 287.2, gamma = 1.4, cv = 717.5): CFL_max
+    over the cells of max(|u|, |u+a|, |u-a|) * dt / dx, and the density
+    range started from 1000 and 0.  numpy evaluates each operation in FP64
+    with IEEE rounding and no contraction, in the reference's order."""
+    R, gamma, cv = 287.2, 1.4, 717.5
+    U = np.asarray(U, dtype=np.float64).reshape(5, -1)
+    ir = 1.0 / U[0]
+    u, v, w = U[1] * ir, U[2] * ir, U[3] * ir
+    T = (U[4] * ir - 0.5 * ((u * u + v * v) + w * w)) / cv
+    a = np.sqrt((gamma * R) * T)
+    cfl = max(0.0, float(np.max(np.abs(u) * dt / dx)), float(np.max(np.abs(u + a) * dt / dx)),
+              float(np.max(np.abs(u - a) * dt / dx)))
+    return cfl, min(1000.0, float(U[0].min())), max(0.0, float(U[0].max()))

@@ -212,6 +212,39 @@ def test_sharded_rk_steps_over_gloo_equal_reference(golden_dir, tmp_path, name, 
         assert np.array_equal(out[f"p{p}"], z[f"p{p}_out"]), (name, p)
 
 
+def _gloo_stats_rank(rank, world, port, result_path):
+    import datetime
+    import torch.distributed as dist
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=120))
+    try:
+        local = (0.1 * (rank + 1), 1.0 - 0.01 * rank, 1.0 + 0.02 * (world - rank))
+        out = shard.reduce_flow_stats(local)
+        if rank == 0:
+            np.save(result_path, np.array(out))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_flow_stats_reduce_over_gloo_ranks(tmp_path):
+    world = 3
+    result = str(tmp_path / "stats.npy")
+    ctx = mp.get_context("spawn")
+    port = _free_port()
+    procs = [ctx.Process(target=_gloo_stats_rank, args=(r, world, port, result)) for r in range(world)]
+    for p in procs:
+        p.start()
+    for p in procs:
+        p.join(timeout=120)
+    for p in procs:
+        if p.is_alive():
+            p.kill()
+    assert all(p.exitcode == 0 for p in procs), [p.exitcode for p in procs]
+    out = np.load(result)
+    assert out.tolist() == [0.1 * world, 1.0 - 0.01 * (world - 1), 1.0 + 0.02 * world]
+
+
 # ------------------------------------------------------------- two contexts, one GPU
 
 class _Recorder:
@@ -335,6 +368,8 @@ def test_sharded_iterator_single_rank_nccl_equals_reference(golden_dir):
         it.updateHost(fields=(0,))
         for p, cp in enumerate(objs):
             assert np.array_equal(cp.getField(0), z[f"p{p}_out"]), p
+        # the grid's diagnostics through the NCCL reduction equal the local ones
+        assert sh.flowStats(0, dt) == it.flowStats(0, dt)
         sh.close()
         it.close()
     finally:
