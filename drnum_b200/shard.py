@@ -109,6 +109,23 @@ def reduce_flow_stats(local, group=None):
     return float(t[0]), float(-t[1]), float(t[2])
 
 
+def gather_sums(local, group=None):
+    """Sum of the ranks' 5-vectors, added in rank order after an
+    all-gather (deterministic, unlike a reduction whose order the
+    collective chooses)."""
+    import torch
+    import torch.distributed as dist
+    dev = "cuda" if dist.get_backend(group) == "nccl" else "cpu"
+    world = dist.get_world_size(group)
+    mine = torch.tensor(np.asarray(local, dtype=np.float64), device=dev)
+    parts = [torch.empty_like(mine) for _ in range(world)]
+    dist.all_gather(parts, mine, group=group)
+    out = np.zeros(len(local))
+    for t in parts:
+        out = out + t.cpu().numpy()
+    return out
+
+
 class ShardedIterator:
     """The GPU side: a B200CartesianIterator holding every patch of the grid
     (donor tables computed for all of them), owning the patches `owner`
@@ -169,6 +186,13 @@ class ShardedIterator:
 
     def rkStep(self, dt, alphas):
         rk_step_sequence(self, dt, alphas)
+
+    def conservationSums(self):
+        """FP64 conservation sums (mass, momenta, energy) of the whole grid:
+        this rank's owned patches (the context sums owned patches only),
+        gathered over the ranks and added in rank order, so every rank gets
+        the same bits whatever the collective's own order."""
+        return gather_sums(self.it.conservationSums(), self.group)
 
     def flowStats(self, field, dt):
         """(CFL_max, rho_min, rho_max) of the whole grid: this rank's owned

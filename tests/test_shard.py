@@ -221,13 +221,14 @@ def _gloo_stats_rank(rank, world, port, result_path):
     try:
         local = (0.1 * (rank + 1), 1.0 - 0.01 * rank, 1.0 + 0.02 * (world - rank))
         out = shard.reduce_flow_stats(local)
+        sums = shard.gather_sums(np.arange(5, dtype=np.float64) * (rank + 1) + 0.1)
         if rank == 0:
-            np.save(result_path, np.array(out))
+            np.save(result_path, np.concatenate([np.array(out), sums]))
     finally:
         dist.destroy_process_group()
 
 
-def test_flow_stats_reduce_over_gloo_ranks(tmp_path):
+def test_flow_stats_and_sums_reduce_over_gloo_ranks(tmp_path):
     world = 3
     result = str(tmp_path / "stats.npy")
     ctx = mp.get_context("spawn")
@@ -242,7 +243,11 @@ def test_flow_stats_reduce_over_gloo_ranks(tmp_path):
             p.kill()
     assert all(p.exitcode == 0 for p in procs), [p.exitcode for p in procs]
     out = np.load(result)
-    assert out.tolist() == [0.1 * world, 1.0 - 0.01 * (world - 1), 1.0 + 0.02 * world]
+    assert out[:3].tolist() == [0.1 * world, 1.0 - 0.01 * (world - 1), 1.0 + 0.02 * world]
+    want = np.zeros(5)
+    for r in range(world):
+        want = want + (np.arange(5, dtype=np.float64) * (r + 1) + 0.1)
+    assert np.array_equal(out[3:], want)
 
 
 # ------------------------------------------------------------- two contexts, one GPU
@@ -368,8 +373,9 @@ def test_sharded_iterator_single_rank_nccl_equals_reference(golden_dir):
         it.updateHost(fields=(0,))
         for p, cp in enumerate(objs):
             assert np.array_equal(cp.getField(0), z[f"p{p}_out"]), p
-        # the grid's diagnostics through the NCCL reduction equal the local ones
+        # the grid's diagnostics and sums through the NCCL collectives equal the local ones
         assert sh.flowStats(0, dt) == it.flowStats(0, dt)
+        assert np.array_equal(sh.conservationSums(), it.conservationSums())
         sh.close()
         it.close()
     finally:
