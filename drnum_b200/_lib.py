@@ -91,6 +91,7 @@ SIGNATURES = {
                                     POINTER(c_double), POINTER(c_double)]),
     "dn_flow_stats": (c_int, [c_void_p, c_int, c_int, c_double, POINTER(c_double)]),
     "dn_launch_count": (c_int, [c_void_p, POINTER(c_int64)]),
+    "dn_tma_patch_count": (c_int, [c_void_p, POINTER(c_int64)]),
     "dn_field_sums_noalloc": (c_int, [c_void_p, c_int64, c_double, POINTER(c_double), c_void_p]),
     "dn_grid_compute_dependencies": (c_int, [c_void_p, POINTER(c_int64)]),
     "dn_patch_donor_counts": (c_int, [c_void_p, c_int, POINTER(c_int64)]),

@@ -507,6 +507,12 @@ class B200CartesianIterator:
         check(self.ctx, self.lib.dn_launch_count(self.ctx, ctypes.byref(n)))
         return n.value
 
+    def tmaPatchCount(self):
+        """dn_tma_patch_count: patches whose planes are staged by TMA."""
+        n = ctypes.c_int64()
+        check(self.ctx, self.lib.dn_tma_patch_count(self.ctx, ctypes.byref(n)))
+        return n.value
+
 
 class B200LevelSetObjectBC:
     """Post-operation form of the level-set wall (CPU_LevelSetObjectBC::operator(),

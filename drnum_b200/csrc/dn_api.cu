@@ -41,7 +41,10 @@ struct NvtxRange {
 
 struct DnPatch {
   dn_patch_desc d;
-  size_t nc = 0;
+  size_t nc = 0;                            // cells, ni*nj*nk
+  int kp = 0;                               // row pitch along k in elements: FX32 nk rounded up to a
+                                            // multiple of 4 (16-byte rows for TMA boxes), FP64 nk
+  size_t ncp = 0;                           // device elements per variable, ni*nj*kp
   void* buf[3] = {nullptr, nullptr, nullptr};
   uint8_t* active = nullptr;
   double base[5] = {0, 0, 0, 0, 0};
@@ -50,6 +53,13 @@ struct DnPatch {
   dn::WallBC wall{};                        // device view (table pointers are device memory)
   bool owned = true;                        // false: a shadow of a patch another rank advances
 };
+
+// Device offset of cell index c = (i*nj + j)*nk + k in the patch's rows of kp elements.
+inline uint64_t pad_cell(const DnPatch& p, uint64_t c)
+{
+  const uint64_t nk = (uint64_t)p.d.nk;
+  return (c / nk) * (uint64_t)p.kp + c % nk;
+}
 
 } // namespace
 
@@ -192,28 +202,34 @@ struct QParams {
   double q[5];
 };
 
+// Host layout [v][i][j][k] (element e) <-> device rows of kp elements:
+// e = row*nk + k  ->  row*kp + k (rows never straddle variables).
 template <typename Src>
-__global__ void k_quantize(const Src* __restrict__ src, int32_t* __restrict__ dst, size_t nc, QParams qp, int* err)
+__global__ void k_quantize(const Src* __restrict__ src, int32_t* __restrict__ dst, size_t nc, int nk, int kp,
+                           QParams qp, int* err)
 {
   const size_t n = 5 * nc;
   for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < n; e += (size_t)gridDim.x * blockDim.x) {
     const int v = (int)(e / nc);
+    const size_t row = e / (size_t)nk;
     double o = rint(((double)src[e] - qp.base[v]) * qp.inv_q[v]);
     if (!(fabs(o) < (double)dn::kFxLimit)) {
       atomicOr(err, 2);
       o = 0.0;
     }
-    dst[e] = (int32_t)o;
+    dst[row * (size_t)kp + (e - row * (size_t)nk)] = (int32_t)o;
   }
 }
 
 template <typename Dst>
-__global__ void k_dequantize(const int32_t* __restrict__ src, Dst* __restrict__ dst, size_t nc, QParams qp)
+__global__ void k_dequantize(const int32_t* __restrict__ src, Dst* __restrict__ dst, size_t nc, int nk, int kp,
+                             QParams qp)
 {
   const size_t n = 5 * nc;
   for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < n; e += (size_t)gridDim.x * blockDim.x) {
     const int v = (int)(e / nc);
-    dst[e] = (Dst)(qp.base[v] + qp.q[v] * (double)src[e]);
+    const size_t row = e / (size_t)nk;
+    dst[e] = (Dst)(qp.base[v] + qp.q[v] * (double)src[row * (size_t)kp + (e - row * (size_t)nk)]);
   }
 }
 
@@ -288,7 +304,7 @@ k_partial_sums_i32(const int32_t* __restrict__ f, size_t nc, long long* __restri
 // Per-block partials: [cfl_max, rho_min, rho_max].
 template <typename T>
 __global__ void __launch_bounds__(kSumThreads)
-k_flow_stats(const T* __restrict__ f, size_t nc, QParams q, int quantized, double dt, double dx,
+k_flow_stats(const T* __restrict__ f, size_t nc, int nk, int kp, QParams q, int quantized, double dt, double dx,
              double* __restrict__ partials)
 {
   __shared__ double s_cfl[kSumThreads], s_rmin[kSumThreads], s_rmax[kSumThreads];
@@ -297,6 +313,7 @@ k_flow_stats(const T* __restrict__ f, size_t nc, QParams q, int quantized, doubl
   const size_t c1 = c0 + per < nc ? c0 + per : nc;
   double cfl = 0.0, rmin = 1000.0, rmax = 0.0;   // the applications' start values
   for (size_t c = c0 + threadIdx.x; c < c1; c += blockDim.x) {
+    if (kp != nk && (int)(c % (size_t)kp) >= nk) continue;   // row padding
     double var[5];
     #pragma unroll
     for (int v = 0; v < 5; ++v) {
@@ -508,7 +525,7 @@ int build_plan(dn_ctx* c)
   std::vector<void*> bufs(np * 3);
   for (size_t r = 0; r < np; ++r) {
     const DnPatch& P = c->patches[r];
-    nc[r] = (int64_t)P.nc;
+    nc[r] = (int64_t)P.ncp;
     for (int b = 0; b < 3; ++b) bufs[r * 3 + b] = P.buf[b];
     for (int v = 0; v < 5; ++v) { base[r * 5 + v] = P.base[v]; quantum[r * 5 + v] = P.quantum[v]; }
     if (r >= c->tables.size() || !P.owned) continue;
@@ -534,11 +551,20 @@ int build_plan(dn_ctx* c)
       rc_off += (size_t)T.num_receivers[q];
       wi_off += T.num_receivers[q] * T.stride[q];
     }
-    idx.insert(idx.end(), T.donor_idx.begin(), T.donor_idx.end());
+    // donor cells at their device offsets (rows of kp elements)
+    {
+      size_t o = 0;
+      for (size_t q = 0; q < T.donor_patch.size(); ++q) {
+        const DnPatch& D = c->patches[(size_t)T.donor_patch[q]];
+        const size_t m = (size_t)(T.num_receivers[q] * T.stride[q]);
+        for (size_t e = 0; e < m; ++e) idx.push_back((int64_t)pad_cell(D, T.donor_idx[o + e]));
+        o += m;
+      }
+    }
     w.insert(w.end(), T.weight.begin(), T.weight.end());
     for (size_t u = 0; u < nu; ++u) {
       rv_patch.push_back((int32_t)r);
-      rv_cell.push_back((int64_t)T.rec_unique[u]);
+      rv_cell.push_back((int64_t)pad_cell(P, T.rec_unique[u]));
       for (size_t g : groups[u]) {
         gp_donor.push_back(ld[g]);
         gp_stride.push_back(ls[g]);
@@ -602,16 +628,16 @@ int build_ls_plan(dn_ctx* c)
   std::vector<void*> bufs(np * 3);
   for (size_t r = 0; r < np; ++r) {
     const DnPatch& P = c->patches[r];
-    nc[r] = (int64_t)P.nc;
+    nc[r] = (int64_t)P.ncp;
     for (int b = 0; b < 3; ++b) bufs[r * 3 + b] = P.buf[b];
     for (int v = 0; v < 5; ++v) { base[r * 5 + v] = P.base[v]; quantum[r * 5 + v] = P.quantum[v]; }
     if (r >= c->ls.size() || !c->ls_on[r] || !P.owned) continue;
     for (const auto& layer : c->ls[r].inner) {
       for (const dn::LayerCell& lc : layer) {
         patch.push_back((int32_t)r);
-        cell.push_back((int64_t)lc.cell);
+        cell.push_back((int64_t)pad_cell(P, lc.cell));
         for (int a = 0; a < 3; ++a) grad.push_back(lc.grad[a]);
-        for (int q = 0; q < 8; ++q) { donor.push_back((int64_t)lc.donor[q]); w.push_back(lc.weight[q]); }
+        for (int q = 0; q < 8; ++q) { donor.push_back((int64_t)pad_cell(P, lc.donor[q])); w.push_back(lc.weight[q]); }
       }
     }
   }
@@ -825,7 +851,7 @@ int build_batch(dn_ctx* c)
     std::memset(&r, 0, sizeof(r));
     for (int b = 0; b < 3; ++b) r.buf[b] = P.buf[b];
     r.active = P.active;
-    r.ni = P.d.ni; r.nj = P.d.nj; r.nk = P.d.nk;
+    r.ni = P.d.ni; r.nj = P.d.nj; r.nk = P.d.nk; r.kp = P.kp;
     r.per_x = P.d.face[0] == DN_FACE_PERIODIC;
     r.per_y = P.d.face[1] == DN_FACE_PERIODIC;
     r.per_z = P.d.face[2] == DN_FACE_PERIODIC;
@@ -838,7 +864,7 @@ int build_batch(dn_ctx* c)
     r.tma = 1;
     if (!fp64) {
       dn::FxGeom g{};
-      g.ni = P.d.ni; g.nj = P.d.nj; g.nk = P.d.nk;
+      g.ni = P.d.ni; g.nj = P.d.nj; g.nk = P.d.nk; g.kp = P.kp;
       for (int b = 0; b < 3 && r.tma; ++b)
         r.tma = dn::encode_stage_maps(maps[q].in[b], &maps[q].un[b], (const int32_t*)P.buf[b],
                                       (const int32_t*)P.buf[b], g, tj, tk) ? 1 : 0;
@@ -987,7 +1013,7 @@ int stage_patch(dn_ctx* c, DnPatch& p, int in_b, int un_b, int out_b, double fac
     a.err_info = c->d_err_info;
     int tj, tk;
     dn::fx32_tile(&tj, &tk);
-    a.g.ni = g.ni; a.g.nj = g.nj; a.g.nk = g.nk;
+    a.g.ni = g.ni; a.g.nj = g.nj; a.g.nk = g.nk; a.g.kp = p.kp;
     a.g.per_x = g.per_x; a.g.per_y = g.per_y; a.g.per_z = g.per_z;
     a.g.i_chunk = dn::default_i_chunk(g.ni, g.nj, g.nk, tj, tk, c->num_sms, DN_FX_WAVE_CTAS);
     a.p.Ax = (float)(dy * dz); a.p.Ay = (float)(dx * dz); a.p.Az = (float)(dx * dy);
@@ -1035,7 +1061,8 @@ int upload_impl(dn_ctx* c, int id, int field, const H* host)
   if (c->precision == DN_FP64) {
     k_convert<H, double><<<grid_for(n), 256, 0, c->stream>>>((const H*)c->staging, (double*)dst, n);
   } else {
-    k_quantize<H><<<grid_for(n), 256, 0, c->stream>>>((const H*)c->staging, (int32_t*)dst, p.nc, qparams(p), c->d_err);
+    k_quantize<H><<<grid_for(n), 256, 0, c->stream>>>((const H*)c->staging, (int32_t*)dst, p.nc, p.d.nk, p.kp,
+                                                   qparams(p), c->d_err);
   }
   c->launches++;
   e = cudaGetLastError();
@@ -1064,7 +1091,8 @@ int download_impl(dn_ctx* c, int id, int field, H* host)
     if (c->precision == DN_FP64) {
       k_convert<double, H><<<grid_for(n), 256, 0, c->stream>>>((const double*)src, (H*)c->staging, n);
     } else {
-      k_dequantize<H><<<grid_for(n), 256, 0, c->stream>>>((const int32_t*)src, (H*)c->staging, p.nc, qparams(p));
+      k_dequantize<H><<<grid_for(n), 256, 0, c->stream>>>((const int32_t*)src, (H*)c->staging, p.nc, p.d.nk,
+                                                     p.kp, qparams(p));
     }
     c->launches++;
     e = cudaGetLastError();
@@ -1136,7 +1164,8 @@ int upload_async_impl(dn_ctx* c, int id, int field, const H* host)
   if (c->precision == DN_FP64) {
     k_convert<H, double><<<grid_for(n), 256, 0, c->stream>>>((const H*)c->st_in[b], (double*)dst, n);
   } else {
-    k_quantize<H><<<grid_for(n), 256, 0, c->stream>>>((const H*)c->st_in[b], (int32_t*)dst, p.nc, qparams(p), c->d_err);
+    k_quantize<H><<<grid_for(n), 256, 0, c->stream>>>((const H*)c->st_in[b], (int32_t*)dst, p.nc, p.d.nk, p.kp,
+                                                   qparams(p), c->d_err);
   }
   c->launches++;
   e = cudaGetLastError();
@@ -1171,7 +1200,8 @@ int download_async_impl(dn_ctx* c, int id, int field, H* host)
   if (c->precision == DN_FP64) {
     k_convert<double, H><<<grid_for(n), 256, 0, c->s_out>>>((const double*)src, (H*)c->st_out[b], n);
   } else {
-    k_dequantize<H><<<grid_for(n), 256, 0, c->s_out>>>((const int32_t*)src, (H*)c->st_out[b], p.nc, qparams(p));
+    k_dequantize<H><<<grid_for(n), 256, 0, c->s_out>>>((const int32_t*)src, (H*)c->st_out[b], p.nc, p.d.nk,
+                                                     p.kp, qparams(p));
   }
   c->launches++;
   e = cudaGetLastError();
@@ -1286,13 +1316,20 @@ int dn_patch_add(dn_ctx* c, const dn_patch_desc* d, int* id)
   }
   const size_t nc = (size_t)d->ni * d->nj * d->nk;
   if (nc > ((size_t)1 << 40)) return fail(c, DN_ERR_ARG, "patch too large");
-  if (c->precision == DN_FP32 && 5 * nc >= ((size_t)1 << 31))
-    return fail(c, DN_ERR_ARG, "FP32 patch limited to 5*cells < 2^31 (32-bit element offsets)");
+  // FX32 rows padded to a multiple of 4 int32 (16 bytes): every row of every
+  // patch can then be staged by TMA boxes
+  const int kp = c->precision == DN_FP32 ? (d->nk + 3) / 4 * 4 : d->nk;
+  const size_t ncp = (size_t)d->ni * d->nj * kp;
+  if (c->precision == DN_FP32 && 5 * ncp >= ((size_t)1 << 31))
+    return fail(c, DN_ERR_ARG, "FP32 patch limited to 5*ni*nj*nk < 2^31 (32-bit element offsets; nk rounded up to "
+                "a multiple of 4)");
   if (set_device(c) != DN_OK) return DN_ERR_CUDA;
   DnPatch p;
   p.d = dd;
   p.nc = nc;
-  const size_t bytes = 5 * nc * elem_size(c);
+  p.kp = kp;
+  p.ncp = ncp;
+  const size_t bytes = 5 * ncp * elem_size(c);
   for (int b = 0; b < 3; ++b) {
     cudaError_t e = cudaMalloc(&p.buf[b], bytes);
     if (e != cudaSuccess) {
@@ -1363,10 +1400,14 @@ int dn_patch_set_active(dn_ctx* c, int id, const uint8_t* mask)
   }
   cudaError_t e;
   if (!p.active) {
-    e = cudaMalloc(&p.active, p.nc);
+    e = cudaMalloc(&p.active, p.ncp);
     if (e != cudaSuccess) return fail(c, DN_ERR_NOMEM, "cudaMalloc(active mask)");
+    e = cudaMemsetAsync(p.active, 1, p.ncp, c->stream);
+    if (e != cudaSuccess) return cuda_fail(c, e, "active mask");
   }
-  e = cudaMemcpyAsync(p.active, mask, p.nc, cudaMemcpyHostToDevice, c->stream);
+  // rows of nk flags into rows of kp (the padding stays set, never read)
+  e = cudaMemcpy2DAsync(p.active, (size_t)p.kp, mask, (size_t)p.d.nk, (size_t)p.d.nk, (size_t)p.d.ni * p.d.nj,
+                        cudaMemcpyHostToDevice, c->stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
   if (e != cudaSuccess) return cuda_fail(c, e, "active mask upload");
   return DN_OK;
@@ -1380,7 +1421,7 @@ int dn_copy_field(dn_ctx* c, int i_src, int i_dst)
   if (i_src == i_dst) return DN_OK;
   if (set_device(c) != DN_OK) return DN_ERR_CUDA;
   for (auto& p : c->patches) {
-    cudaError_t e = cudaMemcpyAsync(p.buf[c->fmap[i_dst]], p.buf[c->fmap[i_src]], 5 * p.nc * elem_size(c),
+    cudaError_t e = cudaMemcpyAsync(p.buf[c->fmap[i_dst]], p.buf[c->fmap[i_src]], 5 * p.ncp * elem_size(c),
                                     cudaMemcpyDeviceToDevice, c->stream);
     if (e != cudaSuccess) return cuda_fail(c, e, "copyField");
   }
@@ -1446,11 +1487,12 @@ int dn_conservation_sums(dn_ctx* c, double out[5])
     cudaError_t e;
     const double dV = p.d.dx * p.d.dy * p.d.dz;
     if (c->precision == DN_FP64) {
-      k_partial_sums<double><<<kSumBlocks, kSumThreads, 0, c->stream>>>((const double*)f, p.nc, c->d_partials);
+      k_partial_sums<double><<<kSumBlocks, kSumThreads, 0, c->stream>>>((const double*)f, p.ncp, c->d_partials);
       e = cudaGetLastError();
       if (e == cudaSuccess) e = cudaMemcpyAsync(h.data(), c->d_partials, h.size() * sizeof(double), cudaMemcpyDeviceToHost, c->stream);
     } else {
-      k_partial_sums_i32<<<kSumBlocks, kSumThreads, 0, c->stream>>>((const int32_t*)f, p.nc, (long long*)c->d_partials);
+      // the row padding holds zero offsets: it adds nothing
+      k_partial_sums_i32<<<kSumBlocks, kSumThreads, 0, c->stream>>>((const int32_t*)f, p.ncp, (long long*)c->d_partials);
       e = cudaGetLastError();
       if (e == cudaSuccess) e = cudaMemcpyAsync(hi.data(), c->d_partials, hi.size() * sizeof(long long), cudaMemcpyDeviceToHost, c->stream);
     }
@@ -1487,13 +1529,14 @@ int dn_field_difference(dn_ctx* c, int id, int f1, int v1, int f2, int v2, doubl
   DnPatch& p = c->patches[id];
   QParams q = qparams(p);
   if (c->precision == DN_FP64) {
-    const double* a = (const double*)p.buf[c->fmap[f1]] + (size_t)v1 * p.nc;
-    const double* b = (const double*)p.buf[c->fmap[f2]] + (size_t)v2 * p.nc;
-    k_diff<double><<<kSumBlocks, kSumThreads, 0, c->stream>>>(a, b, p.nc, q, v1, q, v2, 0, c->d_partials);
+    const double* a = (const double*)p.buf[c->fmap[f1]] + (size_t)v1 * p.ncp;
+    const double* b = (const double*)p.buf[c->fmap[f2]] + (size_t)v2 * p.ncp;
+    k_diff<double><<<kSumBlocks, kSumThreads, 0, c->stream>>>(a, b, p.ncp, q, v1, q, v2, 0, c->d_partials);
   } else {
-    const int32_t* a = (const int32_t*)p.buf[c->fmap[f1]] + (size_t)v1 * p.nc;
-    const int32_t* b = (const int32_t*)p.buf[c->fmap[f2]] + (size_t)v2 * p.nc;
-    k_diff<int32_t><<<kSumBlocks, kSumThreads, 0, c->stream>>>(a, b, p.nc, q, v1, q, v2, 1, c->d_partials);
+    // the row padding holds zero offsets in every field: its differences are 0
+    const int32_t* a = (const int32_t*)p.buf[c->fmap[f1]] + (size_t)v1 * p.ncp;
+    const int32_t* b = (const int32_t*)p.buf[c->fmap[f2]] + (size_t)v2 * p.ncp;
+    k_diff<int32_t><<<kSumBlocks, kSumThreads, 0, c->stream>>>(a, b, p.ncp, q, v1, q, v2, 1, c->d_partials);
   }
   c->launches++;
   std::vector<double> h((size_t)kSumBlocks * 2);
@@ -1523,11 +1566,11 @@ int dn_flow_stats(dn_ctx* c, int id, int field, double dt, double out[3])
   QParams q = qparams(p);
   const void* f = p.buf[c->fmap[field]];
   if (c->precision == DN_FP64)
-    k_flow_stats<double><<<kSumBlocks, kSumThreads, 0, c->stream>>>((const double*)f, p.nc, q, 0, dt, p.d.dx,
-                                                                   c->d_partials);
+    k_flow_stats<double><<<kSumBlocks, kSumThreads, 0, c->stream>>>((const double*)f, p.ncp, p.d.nk, p.kp, q, 0, dt,
+                                                                   p.d.dx, c->d_partials);
   else
-    k_flow_stats<int32_t><<<kSumBlocks, kSumThreads, 0, c->stream>>>((const int32_t*)f, p.nc, q, 1, dt, p.d.dx,
-                                                                    c->d_partials);
+    k_flow_stats<int32_t><<<kSumBlocks, kSumThreads, 0, c->stream>>>((const int32_t*)f, p.ncp, p.d.nk, p.kp, q, 1, dt,
+                                                                    p.d.dx, c->d_partials);
   c->launches++;
   std::vector<double> h((size_t)kSumBlocks * 3);
   cudaError_t e = cudaGetLastError();
@@ -1864,7 +1907,11 @@ int exchange_device_lists(dn_ctx* c, dn_exchange* e)
   x.dev.assign((size_t)x.world * 4, nullptr);
   x.device = c->device;
   for (int q = 0; q < x.world; ++q) {
-    const void* src[4] = {x.send_patch[q].data(), x.send_cell[q].data(), x.recv_patch[q].data(), x.recv_cell[q].data()};
+    // cells at their device offsets (rows of kp elements)
+    std::vector<uint64_t> sc(x.send_cell[q].size()), rc(x.recv_cell[q].size());
+    for (size_t t = 0; t < sc.size(); ++t) sc[t] = pad_cell(c->patches[(size_t)x.send_patch[q][t]], x.send_cell[q][t]);
+    for (size_t t = 0; t < rc.size(); ++t) rc[t] = pad_cell(c->patches[(size_t)x.recv_patch[q][t]], x.recv_cell[q][t]);
+    const void* src[4] = {x.send_patch[q].data(), sc.data(), x.recv_patch[q].data(), rc.data()};
     const size_t bytes[4] = {x.send_patch[q].size() * 4, x.send_cell[q].size() * 8, x.recv_patch[q].size() * 4,
                              x.recv_cell[q].size() * 8};
     for (int a = 0; a < 4; ++a) {
@@ -2118,6 +2165,29 @@ int dn_launch_count(const dn_ctx* c, int64_t* count)
 {
   if (!c || !count) return DN_ERR_ARG;
   *count = c->launches;
+  return DN_OK;
+}
+
+int dn_tma_patch_count(dn_ctx* c, int64_t* count)
+{
+  if (!c || !count) return DN_ERR_ARG;
+  int64_t n = 0;
+  for (const DnPatch& P : c->patches) {
+    int tj, tk;
+    dn::shape_tile(c->precision == DN_FP64, 0, &tj, &tk);
+    bool ok;
+    if (c->precision == DN_FP64) {
+      CUtensorMap m;
+      ok = dn::encode_stage_map_f64(&m, (const double*)P.buf[0], P.d.ni, P.d.nj, P.d.nk, tj, tk);
+    } else {
+      dn::FxGeom g{};
+      g.ni = P.d.ni; g.nj = P.d.nj; g.nk = P.d.nk; g.kp = P.kp;
+      CUtensorMap mi[dn::kFxMaps], mu;
+      ok = dn::encode_stage_maps(mi, &mu, (const int32_t*)P.buf[0], (const int32_t*)P.buf[0], g, tj, tk);
+    }
+    n += ok ? 1 : 0;
+  }
+  *count = n;
   return DN_OK;
 }
 

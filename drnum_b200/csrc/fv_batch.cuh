@@ -22,6 +22,7 @@ struct BatchPatch {
   void* buf[3];                 // physical field buffers
   const uint8_t* active;        // NULL = all active
   int ni, nj, nk;
+  int kp;                       // row pitch along k (FX32: nk rounded up to a multiple of 4; FP64: nk)
   int per_x, per_y, per_z;
   int tma;                      // FX32: the patch's entry of Batch::maps is valid
   double dx, dy, dz;
@@ -78,7 +79,7 @@ fx_stage_batched(const Batch b)
     args.active = rec.active;
     args.err = b.err;
     args.err_info = b.err_info;
-    args.g.ni = rec.ni; args.g.nj = rec.nj; args.g.nk = rec.nk;
+    args.g.ni = rec.ni; args.g.nj = rec.nj; args.g.nk = rec.nk; args.g.kp = rec.kp;
     args.g.per_x = rec.per_x; args.g.per_y = rec.per_y; args.g.per_z = rec.per_z;
     args.g.i_chunk = w.i1 - w.i0;
     args.p.Ax = (float)(rec.dy * rec.dz);

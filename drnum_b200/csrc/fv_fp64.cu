@@ -16,7 +16,7 @@ constexpr int F64_TK = 32;
 bool encode_stage_map_f64(CUtensorMap* tm, const double* in, int ni, int nj, int nk, int tj, int tk)
 {
   if (tma_disabled()) return false;
-  return encode_patch_field_map(tm, in, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 8, ni, nj, nk, tk + 4, tj + 4);
+  return encode_patch_field_map(tm, in, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 8, ni, nj, nk, nk, tk + 4, tj + 4);
 }
 
 cudaError_t launch_stage_f64(const StageArgs<PolicyF64>& a, const StageShape& s, cudaStream_t st)

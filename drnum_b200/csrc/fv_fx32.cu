@@ -23,7 +23,7 @@ namespace {
 
 bool encode_field_map(CUtensorMap* m, const int32_t* base, const FxGeom& g, unsigned bk, unsigned bj)
 {
-  return encode_patch_field_map(m, base, CU_TENSOR_MAP_DATA_TYPE_INT32, 4, g.ni, g.nj, g.nk, bk, bj);
+  return encode_patch_field_map(m, base, CU_TENSOR_MAP_DATA_TYPE_INT32, 4, g.ni, g.nj, g.nk, g.kp, bk, bj);
 }
 
 } // namespace

@@ -26,7 +26,9 @@
 // both states.  s = 0 where c-1 or c+1 lies outside a closed patch (the
 // reference's first-order fallback, upwind2.h:39-42).
 //
-// Element offsets are 32-bit: the host limits an FX32 patch to 5*cells < 2^31.
+// Element offsets are 32-bit: the host limits an FX32 patch to 5*ni*nj*kp <
+// 2^31, kp being the row pitch along k (nk rounded up to a multiple of 4, so
+// that every row starts on a 16-byte boundary, as TMA boxes need).
 //
 // Faces on tile and chunk borders are evaluated by both neighbouring CTAs;
 // conservation needs both evaluations to give the same integer, so the
@@ -61,6 +63,7 @@ struct FxParams {
 
 struct FxGeom {
   int ni, nj, nk;
+  int kp;                // row pitch along k in elements (nk rounded up to a multiple of 4)
   int per_x, per_y, per_z;
   int i_chunk;
 };
@@ -428,15 +431,17 @@ __device__ __forceinline__ void fx_stage_tile_impl(const FxArgs& a, const CUtens
   const int tid = ty * TK + tx;
   const int j = j0 + ty, k = k0 + tx;
   const bool own = FULL || ((j < g.nj) && (k < g.nk));
-  const int njk = g.nj * g.nk;
-  const size_t nc = (size_t)g.ni * njk;
-  // TMA boxes start at x = k0-4 (main, a multiple of 4 int32 since TK is),
-  // nk-4 or 0 (k side; the host gives maps only when nk % 4 == 0); box cells
-  // beyond the patch are zero-filled and never read; destinations 128-byte
-  // aligned
+  const int njk = g.nj * g.kp;                    // plane stride (rows of kp elements)
+  const size_t nc = (size_t)g.ni * njk;           // variable stride
+  // TMA boxes start at x = k0-4 (main; a multiple of 4 int32 since TK is),
+  // k0 (f(n)), and nk-4 or 0 (k side box): the first seam tile of a periodic
+  // k axis needs nk % 4 == 0 for its side box (the last one has k0+TK = nk,
+  // a multiple of 4 already); box cells beyond the patch are zero-filled and
+  // never read; destinations 128-byte aligned
   const int seam_j = fx_seam(j0, TJ, g.nj, g.per_y);
   const int seam_k = fx_seam(k0, TK, g.nk, g.per_z);
   const bool tma = tm_in != nullptr && seam_j >= 0 && seam_k >= 0 && (Smem::SEAMS || (seam_j | seam_k) == 0) &&
+                   (seam_k != 1 || (g.nk & 3) == 0) &&
                    ((smem_u32(&sm.stage[0]) | smem_u32(&sm.un[0][0][0])) & 127) == 0;
 
   // plane element (jj, kk) of variable v in ring slot sl (rows interleaved in pairs)
@@ -460,7 +465,7 @@ __device__ __forceinline__ void fx_stage_tile_impl(const FxArgs& a, const CUtens
       const int jj = (e / (2 * PK)) * 2 + (e & 1);
       const int kk = (e % (2 * PK)) >> 1;
       const int jg = j0 - 2 + jj, kg = k0 - 2 + kk;
-      poff[m] = fx_index(jg, g.nj, g.per_y) * g.nk + fx_index(kg, g.nk, g.per_z);
+      poff[m] = fx_index(jg, g.nj, g.per_y) * g.kp + fx_index(kg, g.nk, g.per_z);
       soff[m] = Smem::ST_M + jj * SK + kk + 2;
       if (tma) {
         // row: in the main box (clamped on a closed axis) or across the seam
@@ -534,7 +539,7 @@ __device__ __forceinline__ void fx_stage_tile_impl(const FxArgs& a, const CUtens
   // f(n) of the own cell, plane ip, cell by cell (tiles without TMA)
   auto fetch_un = [&](int ip) {
     if (own) {
-      const int c = ip * njk + j * g.nk + k;
+      const int c = ip * njk + j * g.kp + k;
       #pragma unroll
       for (int v = 0; v < 5; ++v) fx_cp_async4(&sm.un[v][ty][tx], a.un + (size_t)v * nc + c);
     }
@@ -583,7 +588,7 @@ __device__ __forceinline__ void fx_stage_tile_impl(const FxArgs& a, const CUtens
   {
     // slope of cell i0 (needs i0-1, i0, i0+1) and the face below i0; planes
     // i0-1 and i0-2 of the own column come straight from the stage input
-    const int64_t col = (int64_t)j * g.nk + k;
+    const int64_t col = (int64_t)j * g.kp + k;
     const int iw1 = fx_index(i0 - 1, g.ni, g.per_x);
     float Ul[5], Sp[5], Sm[5];
     float U0[5];
@@ -773,7 +778,7 @@ __device__ __forceinline__ void fx_stage_tile_impl(const FxArgs& a, const CUtens
       fx_cp_async_wait<1>();
     }
     if (own) {
-      const int c = i * njk + j * g.nk + k;       // 5*cells < 2^31 (host check)
+      const int c = i * njk + j * g.kp + k;       // 5*ni*nj*kp < 2^31 (host check)
       const int ncv = (int)nc;
       const bool act = a.active ? (a.active[c] != 0) : true;
       int bad = 0;

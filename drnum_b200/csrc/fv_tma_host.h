@@ -36,16 +36,17 @@ inline bool tma_disabled()
 }
 
 // Tensor map of one field of a patch, [5][ni][nj][nk] elements of `elem`
-// bytes, with box (bk, bj, 1, 5).  False unless the rows are 16-byte
-// strided and the base is 16-byte aligned, or when the driver refuses.
+// bytes stored in rows of kp >= nk elements, with box (bk, bj, 1, 5).  False
+// unless the rows are 16-byte strided and the base is 16-byte aligned, or
+// when the driver refuses.
 inline bool encode_patch_field_map(CUtensorMap* m, const void* base, CUtensorMapDataType type, unsigned elem,
-                                   int ni, int nj, int nk, unsigned bk, unsigned bj)
+                                   int ni, int nj, int nk, int kp, unsigned bk, unsigned bj)
 {
-  if ((reinterpret_cast<uintptr_t>(base) & 15) != 0 || ((uint64_t)nk * elem) % 16 != 0) return false;
+  if ((reinterpret_cast<uintptr_t>(base) & 15) != 0 || ((uint64_t)kp * elem) % 16 != 0 || kp < nk) return false;
   const EncodeTiledFn enc = encode_tiled_fn();
   if (!enc) return false;
   const cuuint64_t dims[4] = {(cuuint64_t)nk, (cuuint64_t)nj, (cuuint64_t)ni, 5};
-  const cuuint64_t strides[3] = {(cuuint64_t)nk * elem, (cuuint64_t)nj * nk * elem, (cuuint64_t)ni * nj * nk * elem};
+  const cuuint64_t strides[3] = {(cuuint64_t)kp * elem, (cuuint64_t)nj * kp * elem, (cuuint64_t)ni * nj * kp * elem};
   const cuuint32_t box[4] = {bk, bj, 1, 5};
   const cuuint32_t estr[4] = {1, 1, 1, 1};
   return enc(m, type, 4, const_cast<void*>(base), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,

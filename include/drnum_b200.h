@@ -429,6 +429,12 @@ int dn_exchange_destroy(dn_exchange* ex);
 /* Number of device kernel launches the context has issued so far. */
 int dn_launch_count(const dn_ctx* ctx, int64_t* count);
 
+/* Number of the context's patches whose stage planes are staged by TMA box
+ * loads (FP32 bulk: every patch, its rows padded to 16 bytes; FP64: patches
+ * with an even nk), 0 with DN_FX_NO_TMA=1 in the environment.  The other
+ * patches stage cell by cell; the results are identical. */
+int dn_tma_patch_count(dn_ctx* ctx, int64_t* count);
+
 /* No counterpart in the reference.  The FP64 sums of dn_conservation_sums
  * (sum of U * dV per variable) over a caller-owned device field
  * [5][ncells] (FP64), for callers that cannot allocate device memory, such as

@@ -32,6 +32,8 @@ def run_fx32(U0, h, dt, steps, periodic, active=None, no_tma=False, precision=DN
             it.rkStep(dt, cases.RK3_ALPHA)
         it.updateHost(fields=(0,))
         sums = it.conservationSums()
+        want = 0 if no_tma or (precision == DN_FP64 and nk % 2) else 1
+        assert it.tmaPatchCount() == want
         it.close()
         return p.getField(0).copy(), sums
     finally:
@@ -46,6 +48,9 @@ def run_fx32(U0, h, dt, steps, periodic, active=None, no_tma=False, precision=DN
     ((24, 72, 80), (False, False, False)),   # closed on every axis
     ((20, 50, 68), (True, False, True)),     # ragged tiles, mixed axes
     ((16, 36, 36), (False, True, False)),    # the smallest patch with an interior tile
+    ((18, 40, 37), (True, True, True)),      # nk % 4 != 0: padded rows, periodic seams
+    ((12, 35, 42), (False, False, False)),   # padded rows, closed
+    ((10, 19, 5), (True, False, True)),      # one ragged k tile of 5 cells in rows of 8
 ])
 def test_tma_staging_equals_cell_copies(shape, periodic):
     ni, nj, nk = shape
@@ -84,6 +89,8 @@ def run_workload_fx32(name, scale, steps, no_tma, shapes=None):
             it.rkStep(case["dt"], cases.RK3_ALPHA)
         it.updateHost(fields=(0,))
         out = [o.getField(0).copy() for o in objs]
+        # every FP32 patch (rows padded to 16 bytes) is staged by TMA unless it is turned off
+        assert it.tmaPatchCount() == (0 if no_tma else len(objs))
         it.close()
         return out
     finally:
@@ -109,6 +116,7 @@ def test_batched_tma_staging_equals_cell_copies(name, scale, shapes):
     ((24, 40, 72), (True, True, True)),      # 4 x 32 tiles: interior, seam and ragged
     ((20, 18, 40), (False, False, False)),   # closed: every tile by TMA, zero-filled halo
     ((16, 22, 66), (False, True, True)),
+    ((12, 20, 37), (True, True, True)),      # odd nk: no TMA map, both runs copy cell by cell
 ])
 def test_fp64_tma_staging_equals_cell_copies(shape, periodic):
     ni, nj, nk = shape
