@@ -78,9 +78,9 @@ class ClockSampler:
     """Samples the SM clock, power and clock-event reasons of this rank's GPU
     during a timed region: a separate process polls NVML's read-only queries
     about every millisecond, and the samples whose timestamps fall between
-    start() returning and stop() being called are kept (the file
-    gpurun_out/clocks_bench_rank<r>.csv holds them all).  Falls back to
-    nvidia-smi where NVML is unavailable."""
+    start() returning and stop() being called are kept (the CSV file
+    clocks_bench_rank<r>.csv beside the run's other outputs holds them all).
+    Falls back to nvidia-smi where NVML is unavailable."""
 
     QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
