@@ -211,13 +211,17 @@ __global__ void k_quantize(const Src* __restrict__ src, int32_t* __restrict__ ds
   const size_t n = 5 * nc;
   for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < n; e += (size_t)gridDim.x * blockDim.x) {
     const int v = (int)(e / nc);
-    const size_t row = e / (size_t)nk;
     double o = rint(((double)src[e] - qp.base[v]) * qp.inv_q[v]);
     if (!(fabs(o) < (double)dn::kFxLimit)) {
       atomicOr(err, 2);
       o = 0.0;
     }
-    dst[row * (size_t)kp + (e - row * (size_t)nk)] = (int32_t)o;
+    size_t d = e;
+    if (kp != nk) {                       // padded rows
+      const size_t row = e / (size_t)nk;
+      d = row * (size_t)kp + (e - row * (size_t)nk);
+    }
+    dst[d] = (int32_t)o;
   }
 }
 
@@ -228,8 +232,12 @@ __global__ void k_dequantize(const int32_t* __restrict__ src, Dst* __restrict__ 
   const size_t n = 5 * nc;
   for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < n; e += (size_t)gridDim.x * blockDim.x) {
     const int v = (int)(e / nc);
-    const size_t row = e / (size_t)nk;
-    dst[e] = (Dst)(qp.base[v] + qp.q[v] * (double)src[row * (size_t)kp + (e - row * (size_t)nk)]);
+    size_t d = e;
+    if (kp != nk) {                       // padded rows
+      const size_t row = e / (size_t)nk;
+      d = row * (size_t)kp + (e - row * (size_t)nk);
+    }
+    dst[e] = (Dst)(qp.base[v] + qp.q[v] * (double)src[d]);
   }
 }
 
