@@ -383,12 +383,13 @@ def run_ours(args, rank, world, local_rank):
     bytes_per_launch = 60.0 * cells      # read f(k-1) + read f(n) + write f(k), 5 x FP32 each
     launch_s = t32 / (STAGES * args.steps)
     achieved = bytes_per_launch / launch_s / 1e9
-    traffic = None
-    tp = os.path.join(ROOT, "profiles", "traffic_fv_stage_f32.json")
-    if os.path.exists(tp):
-        with open(tp) as f:
-            tj = json.load(f)
-        traffic = tj.get("dram_bytes_per_launch_scaled", {}).get(str(n))
+    # DRAM traffic of the kernel per launch, from one ncu capture of the three
+    # stage launches of an RK step on the periodic 192^3 patch (dram__bytes_read
+    # + dram__bytes_write: 36.8, 59.1 and 59.0 B per cell; stage 1 reads f(k-1)
+    # = f(n) once), averaged and scaled by the cells of this launch: the kernel
+    # streams each plane once, so the traffic grows with the cell count
+    TRAFFIC_BYTES_PER_CELL = 51.64
+    traffic = TRAFFIC_BYTES_PER_CELL * cells
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
