@@ -495,8 +495,9 @@ class B200CartesianIterator:
         check(self.ctx, self.lib.dn_patch_set_tile(self.ctx, int(i_patch), int(shape)))
 
     def autotune(self, cache_path=None):
-        """Measures the tile shapes on this case and picks one per patch;
-        returns the measured cost per padded cell (ns) of each shape."""
+        """Measures the tile shapes on this case and picks one per patch (and,
+        for FP32-bulk single-patch launches, the plane-chunk length of the
+        CTAs); returns the measured cost per padded cell (ns) of each shape."""
         cost = np.zeros(2)
         path = None if cache_path is None else str(cache_path).encode()
         check(self.ctx, self.lib.dn_autotune(self.ctx, path, _lib.dptr(cost)))

@@ -45,6 +45,7 @@ struct DnPatch {
   int kp = 0;                               // row pitch along k in elements: FX32 nk rounded up to a
                                             // multiple of 4 (16-byte rows for TMA boxes), FP64 nk
   size_t ncp = 0;                           // device elements per variable, ni*nj*kp
+  int i_chunk = 0;                          // FX32 single-patch launch: planes per CTA (0: default)
   void* buf[3] = {nullptr, nullptr, nullptr};
   uint8_t* active = nullptr;
   double base[5] = {0, 0, 0, 0, 0};
@@ -1023,7 +1024,8 @@ int stage_patch(dn_ctx* c, DnPatch& p, int in_b, int un_b, int out_b, double fac
     dn::fx32_tile(&tj, &tk);
     a.g.ni = g.ni; a.g.nj = g.nj; a.g.nk = g.nk; a.g.kp = p.kp;
     a.g.per_x = g.per_x; a.g.per_y = g.per_y; a.g.per_z = g.per_z;
-    a.g.i_chunk = dn::default_i_chunk(g.ni, g.nj, g.nk, tj, tk, c->num_sms, DN_FX_WAVE_CTAS);
+    a.g.i_chunk = p.i_chunk > 0 ? std::min(p.i_chunk, g.ni)
+                                : dn::default_i_chunk(g.ni, g.nj, g.nk, tj, tk, c->num_sms, DN_FX_WAVE_CTAS);
     a.p.Ax = (float)(dy * dz); a.p.Ay = (float)(dx * dz); a.p.Az = (float)(dx * dy);
     for (int v = 0; v < 5; ++v) {
       a.p.base[v] = (float)p.base[v];
@@ -2153,6 +2155,45 @@ int dn_autotune(dn_ctx* c, const char* cache_path, double cost_out[2])
     int s2 = read_device_error(c);
     if (s2 != DN_OK) return s2;
     write_tune_cache(cache_path, dev, c->precision, cost);
+  }
+  // FX32 stages that run the single-patch kernel (one patch, or batching
+  // off): the plane-chunk length of its CTAs, measured among a few
+  // candidates on the patch itself (one stage into the scratch field,
+  // factor 0; the chunking changes no result)
+  if (c->precision == DN_FP32 && (c->patches.size() == 1 || !c->batched)) {
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    for (size_t q = 0; q < c->patches.size(); ++q) {
+      DnPatch& P = c->patches[q];
+      if (!P.owned) continue;
+      int tj, tk;
+      dn::fx32_tile(&tj, &tk);
+      const int def = dn::default_i_chunk(P.d.ni, P.d.nj, P.d.nk, tj, tk, c->num_sms, DN_FX_WAVE_CTAS);
+      const int cand[6] = {def, 16, 24, 32, 48, 64};
+      int best = def;
+      double best_ms = 1e300;
+      for (int k = 0; k < 6; ++k) {
+        if (cand[k] > P.d.ni || (k > 0 && cand[k] == def)) continue;
+        P.i_chunk = cand[k];
+        int st = DN_OK;
+        for (int r = 0; r < 7 && st == DN_OK; ++r) {
+          if (r == 2) cudaEventRecord(e0, c->stream);
+          st = stage_patch(c, P, c->fmap[0], c->fmap[1], c->fmap[2], 0.0);
+        }
+        cudaEventRecord(e1, c->stream);
+        cudaEventSynchronize(e1);
+        if (st != DN_OK) { P.i_chunk = 0; cudaEventDestroy(e0); cudaEventDestroy(e1); return st; }
+        float ms = 0;
+        cudaEventElapsedTime(&ms, e0, e1);
+        if (ms < best_ms) { best_ms = ms; best = cand[k]; }
+      }
+      P.i_chunk = best;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    int s3 = read_device_error(c);
+    if (s3 != DN_OK) return s3;
   }
   for (size_t q = 0; q < c->patches.size(); ++q) {
     int best = 0;

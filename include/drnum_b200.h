@@ -311,7 +311,10 @@ int dn_patch_set_tile(dn_ctx* ctx, int patch_id, int shape);
  * overwrites), then gives every patch the shape of least predicted time.
  * cache_path (may be NULL) holds measured costs per device and precision and
  * is reused on the next call; cost_out[2] (may be NULL) returns them in ns per
- * padded cell and stage.  No reference counterpart. */
+ * padded cell and stage.  FP32-bulk stages that run one patch per launch (a
+ * single patch, or batching off) also get the plane-chunk length of their
+ * CTAs, measured among a few candidates on the patch itself.  Neither choice
+ * changes a result.  No reference counterpart. */
 int dn_autotune(dn_ctx* ctx, const char* cache_path, double cost_out[2]);
 
 /* Flux scheme of the stage of an FP64 context; replaces the OP template

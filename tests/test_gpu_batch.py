@@ -78,3 +78,25 @@ def test_runs_are_deterministic(precision):
     d, _ = _run("octants_jet", precision, 3)
     for x, y in zip(a + c, b + d):
         assert np.array_equal(x, y)
+
+
+def test_single_patch_chunk_autotune_changes_no_result():
+    # the plane-chunk length the autotuner picks for a single-patch FP32
+    # launch changes the CTA decomposition, not a bit of the result
+    from drnum_b200.api import AusmPlus, B200CartesianIterator, CartesianPatch
+    U0, h, dt = cases.periodic_box(48)
+    outs = []
+    for tune in (False, True):
+        p = CartesianPatch(48, 48, 48, spacing=(h, h, h))
+        p.setField(0, U0)
+        it = B200CartesianIterator(AusmPlus(), 0, DN_FP32)
+        it.addPatch(p)
+        it.updateDevice(fields=(0,))
+        if tune:
+            it.autotune()
+        for _ in range(3):
+            it.rkStep(dt, cases.RK3_ALPHA)
+        it.updateHost(fields=(0,))
+        outs.append(p.getField(0).copy())
+        it.close()
+    assert np.array_equal(outs[0], outs[1])
