@@ -119,15 +119,18 @@ struct dn_ctx {
   int64_t generation = 0;
   int64_t graph_generation = -1;
   // asynchronous host transfers: a copy-in and a copy-out stream with two
-  // staging buffers each, ordered against the context's stream by events
-  cudaStream_t s_in = nullptr, s_out = nullptr;
+  // staging buffers each, and a conversion stream for downloads, ordered
+  // against the context's stream by events
+  cudaStream_t s_in = nullptr, s_out = nullptr, s_conv = nullptr;
   void* st_in[2] = {nullptr, nullptr};
   size_t st_in_bytes[2] = {0, 0};
   void* st_out[2] = {nullptr, nullptr};
   size_t st_out_bytes[2] = {0, 0};
   cudaEvent_t ev_in_done[2] = {nullptr, nullptr}, ev_in_free[2] = {nullptr, nullptr};
   bool ev_in_free_set[2] = {false, false};
-  cudaEvent_t ev_main = nullptr, ev_out_read = nullptr;
+  cudaEvent_t ev_main = nullptr;
+  cudaEvent_t ev_out_read[2] = {nullptr, nullptr}, ev_d2h_done[2] = {nullptr, nullptr};
+  bool ev_d2h_done_set[2] = {false, false};
   unsigned in_seq = 0, out_seq = 0;
   // FP64 flux scheme (DN_FLUX_*) or a user stage function replacing it
   int scheme = DN_FLUX_AUSMPLUS;
@@ -1120,11 +1123,13 @@ int ensure_async(dn_ctx* c)
   if (c->s_in) return DN_OK;
   bool ok = cudaStreamCreateWithFlags(&c->s_in, cudaStreamNonBlocking) == cudaSuccess &&
             cudaStreamCreateWithFlags(&c->s_out, cudaStreamNonBlocking) == cudaSuccess &&
-            cudaEventCreateWithFlags(&c->ev_main, cudaEventDisableTiming) == cudaSuccess &&
-            cudaEventCreateWithFlags(&c->ev_out_read, cudaEventDisableTiming) == cudaSuccess;
+            cudaStreamCreateWithFlags(&c->s_conv, cudaStreamNonBlocking) == cudaSuccess &&
+            cudaEventCreateWithFlags(&c->ev_main, cudaEventDisableTiming) == cudaSuccess;
   for (int b = 0; b < 2 && ok; ++b)
     ok = cudaEventCreateWithFlags(&c->ev_in_done[b], cudaEventDisableTiming) == cudaSuccess &&
-         cudaEventCreateWithFlags(&c->ev_in_free[b], cudaEventDisableTiming) == cudaSuccess;
+         cudaEventCreateWithFlags(&c->ev_in_free[b], cudaEventDisableTiming) == cudaSuccess &&
+         cudaEventCreateWithFlags(&c->ev_out_read[b], cudaEventDisableTiming) == cudaSuccess &&
+         cudaEventCreateWithFlags(&c->ev_d2h_done[b], cudaEventDisableTiming) == cudaSuccess;
   return ok ? DN_OK : fail(c, DN_ERR_CUDA, "cannot create the transfer streams");
 }
 
@@ -1185,10 +1190,12 @@ int upload_async_impl(dn_ctx* c, int id, int field, const H* host)
   return DN_OK;
 }
 
-// Download through the copy-out stream: once the context's stream reached
-// this point, the field is converted into staging[b] on s_out (the context's
-// stream waits for that conversion only, not for the copy), then copied to
-// the host on s_out.
+// Download: once the context's stream reached this point, the field is
+// converted into staging[b] on the conversion stream (after the previous
+// copy out of staging[b] has finished); the context's stream waits for that
+// conversion only, and the copy to the host runs on s_out.  A conversion
+// never queues behind an earlier host copy, so the copies of consecutive
+// downloads run back to back while the stages continue.
 template <typename H>
 int download_async_impl(dn_ctx* c, int id, int field, H* host)
 {
@@ -1204,21 +1211,25 @@ int download_async_impl(dn_ctx* c, int id, int field, H* host)
   const size_t n = 5 * p.nc;
   if ((s = ensure_buffer(c, c->st_out[b], c->st_out_bytes[b], n * sizeof(H)))) return s;
   cudaError_t e = cudaEventRecord(c->ev_main, c->stream);
-  if (e == cudaSuccess) e = cudaStreamWaitEvent(c->s_out, c->ev_main, 0);
+  if (e == cudaSuccess) e = cudaStreamWaitEvent(c->s_conv, c->ev_main, 0);
+  if (e == cudaSuccess && c->ev_d2h_done_set[b]) e = cudaStreamWaitEvent(c->s_conv, c->ev_d2h_done[b], 0);
   if (e != cudaSuccess) return cuda_fail(c, e, "asynchronous download ordering");
   const void* src = p.buf[c->fmap[field]];
   if (c->precision == DN_FP64) {
-    k_convert<double, H><<<grid_for(n), 256, 0, c->s_out>>>((const double*)src, (H*)c->st_out[b], n);
+    k_convert<double, H><<<grid_for(n), 256, 0, c->s_conv>>>((const double*)src, (H*)c->st_out[b], n);
   } else {
-    k_dequantize<H><<<grid_for(n), 256, 0, c->s_out>>>((const int32_t*)src, (H*)c->st_out[b], p.nc, p.d.nk,
-                                                     p.kp, qparams(p));
+    k_dequantize<H><<<grid_for(n), 256, 0, c->s_conv>>>((const int32_t*)src, (H*)c->st_out[b], p.nc, p.d.nk,
+                                                      p.kp, qparams(p));
   }
   c->launches++;
   e = cudaGetLastError();
-  if (e == cudaSuccess) e = cudaEventRecord(c->ev_out_read, c->s_out);
-  if (e == cudaSuccess) e = cudaStreamWaitEvent(c->stream, c->ev_out_read, 0);
+  if (e == cudaSuccess) e = cudaEventRecord(c->ev_out_read[b], c->s_conv);
+  if (e == cudaSuccess) e = cudaStreamWaitEvent(c->stream, c->ev_out_read[b], 0);
+  if (e == cudaSuccess) e = cudaStreamWaitEvent(c->s_out, c->ev_out_read[b], 0);
   if (e == cudaSuccess) e = cudaMemcpyAsync(host, c->st_out[b], n * sizeof(H), cudaMemcpyDeviceToHost, c->s_out);
+  if (e == cudaSuccess) e = cudaEventRecord(c->ev_d2h_done[b], c->s_out);
   if (e != cudaSuccess) return cuda_fail(c, e, "asynchronous download copy");
+  c->ev_d2h_done_set[b] = true;
   return DN_OK;
 }
 
@@ -1266,16 +1277,19 @@ int dn_ctx_destroy(dn_ctx* c)
   free_batch(c);
   if (c->staging) cudaFree(c->staging);
   if (c->s_in) cudaStreamSynchronize(c->s_in);
+  if (c->s_conv) cudaStreamSynchronize(c->s_conv);
   if (c->s_out) cudaStreamSynchronize(c->s_out);
   for (int b = 0; b < 2; ++b) {
     if (c->st_in[b]) cudaFree(c->st_in[b]);
     if (c->st_out[b]) cudaFree(c->st_out[b]);
     if (c->ev_in_done[b]) cudaEventDestroy(c->ev_in_done[b]);
     if (c->ev_in_free[b]) cudaEventDestroy(c->ev_in_free[b]);
+    if (c->ev_out_read[b]) cudaEventDestroy(c->ev_out_read[b]);
+    if (c->ev_d2h_done[b]) cudaEventDestroy(c->ev_d2h_done[b]);
   }
   if (c->ev_main) cudaEventDestroy(c->ev_main);
-  if (c->ev_out_read) cudaEventDestroy(c->ev_out_read);
   if (c->s_in) cudaStreamDestroy(c->s_in);
+  if (c->s_conv) cudaStreamDestroy(c->s_conv);
   if (c->s_out) cudaStreamDestroy(c->s_out);
   if (c->d_partials) cudaFree(c->d_partials);
   if (c->d_err) cudaFree(c->d_err);
@@ -1476,6 +1490,7 @@ int dn_sync(dn_ctx* c)
   if (set_device(c) != DN_OK) return DN_ERR_CUDA;
   cudaError_t e = cudaSuccess;
   if (c->s_in) e = cudaStreamSynchronize(c->s_in);
+  if (e == cudaSuccess && c->s_conv) e = cudaStreamSynchronize(c->s_conv);
   if (e == cudaSuccess && c->s_out) e = cudaStreamSynchronize(c->s_out);
   if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
   if (e != cudaSuccess) return cuda_fail(c, e, "stream synchronize");
