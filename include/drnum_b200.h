@@ -102,7 +102,11 @@ int dn_last_error(const dn_ctx* ctx, char* buf, size_t n);
  * NULL for the context's own stream). */
 int dn_set_stream(dn_ctx* ctx, void* stream);
 
-/* Adds a patch; allocates its three fields and active mask on the device.
+/* Adds a patch; allocates its three fields on the device (the active mask
+ * on the first dn_patch_set_active).  FP32-bulk fields are stored in rows
+ * padded to a multiple of 4 cells (16 bytes) along k, invisible through the
+ * API; such a patch is limited to 5*ni*nj*nk' < 2^31 with nk' = nk rounded
+ * up to a multiple of 4 (32-bit element offsets, DN_ERR_ARG otherwise).
  * Replaces: GPU_PatchIterator::addPatch + GPU_Patch ctor
  * (iterators/gpu_patchiterator.h:86-95, gpu_patch.h:43-129). */
 int dn_patch_add(dn_ctx* ctx, const dn_patch_desc* desc, int* patch_id);
