@@ -590,11 +590,29 @@ int build_plan(dn_ctx* c)
   int s;
   dn::DonorPlan& P = c->plan;
   P.n_recv = (int32_t)rv_patch.size();
-  if ((s = plan_upload(c, rv_patch, &P.rv_patch)) || (s = plan_upload(c, rv_cell, &P.rv_cell)) ||
-      (s = plan_upload(c, rv_grp, &P.rv_grp)) || (s = plan_upload(c, gp_donor, &P.gp_donor)) ||
-      (s = plan_upload(c, gp_stride, &P.gp_stride)) || (s = plan_upload(c, gp_wi, &P.gp_wi)) ||
-      (s = plan_upload(c, idx, &P.idx)) || (s = plan_upload(c, w, &P.w)) || (s = plan_upload(c, nc, &P.nc)) ||
+  if ((s = plan_upload(c, rv_patch, &P.rv_patch)) || (s = plan_upload(c, rv_grp, &P.rv_grp)) ||
+      (s = plan_upload(c, gp_donor, &P.gp_donor)) || (s = plan_upload(c, gp_stride, &P.gp_stride)) ||
+      (s = plan_upload(c, w, &P.w)) || (s = plan_upload(c, nc, &P.nc)) ||
       (s = plan_upload(c, base, &P.base)) || (s = plan_upload(c, quantum, &P.quantum))) {
+    free_plan(c);
+    return s;
+  }
+  // cell offsets and contribution offsets in 32 bits when they all fit
+  auto fits32 = [](const std::vector<int64_t>& v) {
+    for (int64_t x : v) if (x < 0 || x > (int64_t)UINT32_MAX) return false;
+    return true;
+  };
+  P.narrow = fits32(rv_cell) && fits32(gp_wi) && fits32(idx) ? 1 : 0;
+  if (P.narrow) {
+    const std::vector<uint32_t> rc(rv_cell.begin(), rv_cell.end()), gw(gp_wi.begin(), gp_wi.end()),
+        ix(idx.begin(), idx.end());
+    if ((s = plan_upload(c, rc, &P.rv_cell32)) || (s = plan_upload(c, gw, &P.gp_wi32)) ||
+        (s = plan_upload(c, ix, &P.idx32))) {
+      free_plan(c);
+      return s;
+    }
+  } else if ((s = plan_upload(c, rv_cell, &P.rv_cell)) || (s = plan_upload(c, gp_wi, &P.gp_wi)) ||
+             (s = plan_upload(c, idx, &P.idx))) {
     free_plan(c);
     return s;
   }
