@@ -131,6 +131,13 @@ public:
         return m_Tile[(((size_t)sl*5 + var)*m_WJ + (size_t)dj)*m_WK + (size_t)dk];
       }
     }
+    return f_global(var, i, j, k);
+  }
+  /* the read outside the shared-memory window, kept out of line: the
+     functors call f() at dozens of sites, and inlining the index folding
+     at each of them filled the instruction cache */
+  __device__ __noinline__ double f_global(size_t var, size_t i, size_t j, size_t k) const
+  {
     return __ldg(m_In + var*m_NC + index(i, j, k));
   }
   __device__ __forceinline__ void getVar(size_t field, size_t i, size_t j, size_t k, double* var) const
