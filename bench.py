@@ -19,6 +19,7 @@ import argparse
 import json
 import os
 import subprocess
+import tempfile
 import sys
 import time
 
@@ -79,7 +80,7 @@ class ClockSampler:
     during a timed region: a separate process polls NVML's read-only queries
     about every millisecond, and the samples whose timestamps fall between
     start() returning and stop() being called are kept (the CSV file
-    clocks_bench_rank<r>.csv beside the run's other outputs holds them all).
+    clocks_bench_rank<r>.csv in the --clock-dir directory holds them all).
     Falls back to nvidia-smi where NVML is unavailable."""
 
     QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
@@ -89,11 +90,11 @@ class ClockSampler:
     REASONS = (("hw_slowdown", 0x8), ("hw_thermal_slowdown", 0x40), ("sw_thermal_slowdown", 0x20),
                ("sw_power_cap", 0x4))
 
-    def __init__(self, device_index):
+    def __init__(self, device_index, out_dir):
         self.device_index = device_index
         self.proc = None
         self.mode = None
-        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_bench_rank{device_index}.csv")
+        self.path = os.path.join(out_dir, f"clocks_bench_rank{device_index}.csv")
 
     def start(self):
         os.makedirs(os.path.dirname(self.path), exist_ok=True)
@@ -313,7 +314,7 @@ def run_ours(args, rank, world, local_rank):
     for _ in range(args.warmup):
         it32.rkStep(dt, cases.RK3_ALPHA)
     it32.sync()
-    clocks = ClockSampler(local_rank)
+    clocks = ClockSampler(local_rank, args.clock_dir)
     clocks.start()
     t32, launches = timed_steps(it32, args.steps)
     clock_info = clocks.stop()
@@ -532,6 +533,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--n", type=int, default=256)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--clock-dir", default=os.environ.get("DN_CLOCK_DIR", tempfile.gettempdir()),
+                    help="directory of the clock-sample CSV written during the timed region")
     ap.add_argument("--workloads", default="jet,sphere,tiled",
                     help="comma-separated multi-patch workloads to add to the line ('' for none)")
     ap.add_argument("--workload-scale", type=float, default=1.0,

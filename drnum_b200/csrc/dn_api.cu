@@ -904,6 +904,11 @@ int build_batch(dn_ctx* c)
                                          tk) ? 1 : 0;
     }
   }
+  if (tiles == 0) {
+    // no owned patch (a rank whose share of the grid is empty): nothing to launch
+    c->batch_dirty = false;
+    return DN_OK;
+  }
   const long want = (long)c->num_sms * 2 * 4;
   long chunks = (want + tiles - 1) / tiles;
   if (chunks < 1) chunks = 1;
@@ -1047,12 +1052,7 @@ int stage_patch(dn_ctx* c, DnPatch& p, int in_b, int un_b, int out_b, double fac
     a.g.per_x = g.per_x; a.g.per_y = g.per_y; a.g.per_z = g.per_z;
     a.g.i_chunk = p.i_chunk > 0 ? std::min(p.i_chunk, g.ni)
                                 : dn::default_i_chunk(g.ni, g.nj, g.nk, tj, tk, c->num_sms, DN_FX_WAVE_CTAS);
-    a.p.Ax = (float)(dy * dz); a.p.Ay = (float)(dx * dz); a.p.Az = (float)(dx * dy);
-    for (int v = 0; v < 5; ++v) {
-      a.p.base[v] = (float)p.base[v];
-      a.p.quantum[v] = (float)p.quantum[v];
-      a.p.face_scale[v] = (float)(pf / p.quantum[v]);
-    }
+    dn::fx_set_params(a.p, dx, dy, dz, factor, p.base, p.quantum);
     a.wall = p.wall;
     e = dn::launch_stage_fx32(a, c->stream);
   }

@@ -18,7 +18,13 @@
 //    be serialised by the caller;
 //  * the first call on a device, with that device current, resolves the
 //    device address of the array (cudaGetSymbolAddress); make that first
-//    call before any stream capture on that device.
+//    call before any stream capture on that device.  The address is kept
+//    for the life of the process: after a cudaDeviceReset of that device it
+//    is stale, so do not call this function on a device that was reset;
+//  * the field is an unpadded FP64 array [5][ncells] (the layout of an FP64
+//    context's buffers and of DrNUM's host fields); the int32 fixed-point
+//    buffers of an FP32-bulk context, whose rows are padded, cannot be
+//    passed.
 #include "drnum_b200.h"
 
 #include <cuda_runtime.h>
@@ -100,9 +106,17 @@ extern "C" int dn_field_sums_noalloc(const double* field, int64_t ncells, double
   if (s != DN_OK) return s;
   const int blocks = (int)((ncells + kNoAllocCellsPerBlock - 1) / kNoAllocCellsPerBlock);
   cudaStream_t st = static_cast<cudaStream_t>(stream);
-  k_sums_noalloc<<<blocks, kNoAllocThreads, 0, st>>>(field, (long long)ncells, partials);
-  k_sums_noalloc_finish<<<1, 32, 0, st>>>(partials, blocks);
-  if (cudaGetLastError() != cudaSuccess) return DN_ERR_CUDA;
+  // each launch's own status (cudaGetLastError would also return, and clear,
+  // an unrelated error left by an earlier launch of the caller)
+  long long nc = (long long)ncells;
+  void* sum_args[] = {(void*)&field, (void*)&nc, (void*)&partials};
+  if (cudaLaunchKernel((const void*)k_sums_noalloc, dim3(blocks), dim3(kNoAllocThreads), sum_args, 0, st) !=
+      cudaSuccess)
+    return DN_ERR_CUDA;
+  int nb = blocks;
+  void* fin_args[] = {(void*)&partials, (void*)&nb};
+  if (cudaLaunchKernel((const void*)k_sums_noalloc_finish, dim3(1), dim3(32), fin_args, 0, st) != cudaSuccess)
+    return DN_ERR_CUDA;
   double tot[5];
   if (cudaMemcpyAsync(tot, partials + kNoAllocMaxBlocks * 5, sizeof(tot), cudaMemcpyDeviceToHost, st) != cudaSuccess)
     return DN_ERR_CUDA;

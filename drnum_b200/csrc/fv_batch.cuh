@@ -64,7 +64,7 @@ __device__ __forceinline__ void load_patch_record(BatchPatch& dst, const BatchPa
 }
 
 template <int TJ, int TK>
-__global__ void __launch_bounds__(TJ * TK, DN_FX_MIN_BLOCKS)
+__global__ void __launch_bounds__(TJ * TK / 2, FxOccupancy<TJ * TK / 2>::min_blocks)
 fx_stage_batched(const Batch b)
 {
   __shared__ __align__(16) BatchPatch rec;
@@ -82,15 +82,7 @@ fx_stage_batched(const Batch b)
     args.g.ni = rec.ni; args.g.nj = rec.nj; args.g.nk = rec.nk; args.g.kp = rec.kp;
     args.g.per_x = rec.per_x; args.g.per_y = rec.per_y; args.g.per_z = rec.per_z;
     args.g.i_chunk = w.i1 - w.i0;
-    args.p.Ax = (float)(rec.dy * rec.dz);
-    args.p.Ay = (float)(rec.dx * rec.dz);
-    args.p.Az = (float)(rec.dx * rec.dy);
-    const double pf = b.factor / (rec.dx * rec.dy * rec.dz);
-    for (int v = 0; v < 5; ++v) {
-      args.p.base[v] = (float)rec.base[v];
-      args.p.quantum[v] = (float)rec.quantum[v];
-      args.p.face_scale[v] = (float)(pf / rec.quantum[v]);
-    }
+    fx_set_params(args.p, rec.dx, rec.dy, rec.dz, b.factor, rec.base, rec.quantum);
     args.wall = rec.wall;
   }
   __syncthreads();

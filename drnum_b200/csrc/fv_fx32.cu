@@ -13,7 +13,7 @@ namespace {
 #define DN_FX_TJ 16
 #endif
 #ifndef DN_FX_TK
-#define DN_FX_TK 16
+#define DN_FX_TK 32
 #endif
 constexpr int FX_TJ = DN_FX_TJ;   // tile of the single-patch launch (j x k)
 constexpr int FX_TK = DN_FX_TK;
@@ -50,7 +50,7 @@ cudaError_t launch_stage_fx32(const FxArgs& a, cudaStream_t st)
   std::memset(&L, 0, sizeof L);
   L.a = a;
   L.tma = encode_stage_maps(L.tm_in, &L.tm_un, a.in, a.un, a.g, FX_TJ, FX_TK);
-  dim3 block(FX_TK, FX_TJ, 1);
+  dim3 block(FX_TK / 2, FX_TJ, 1);
   dim3 grid((a.g.nk + FX_TK - 1) / FX_TK, (a.g.nj + FX_TJ - 1) / FX_TJ,
             (a.g.ni + a.g.i_chunk - 1) / a.g.i_chunk);
   kern<<<grid, block, sizeof(Smem), st>>>(L);
@@ -67,7 +67,7 @@ cudaError_t launch_fx_batched(const Batch& b, cudaStream_t st)
   auto kern = fx_stage_batched<TJ, TK>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(Smem));
   if (e != cudaSuccess) return e;
-  kern<<<b.n_items, dim3(TK, TJ, 1), sizeof(Smem), st>>>(b);
+  kern<<<b.n_items, dim3(TK / 2, TJ, 1), sizeof(Smem), st>>>(b);
   return cudaGetLastError();
 }
 } // namespace

@@ -33,18 +33,30 @@
 // Faces on tile and chunk borders are evaluated by both neighbouring CTAs;
 // conservation needs both evaluations to give the same integer, so the
 // translation unit is compiled without implicit multiply-add contraction
-// (every FMA is written out with fmaf) and identical inputs always produce
-// identical bits.
+// (every FMA is written out) and identical inputs always produce identical
+// bits.
 //
-// Data flow per CTA: a TJ x TK tile of (j, k) columns marches along i.  Each
-// plane of the stencil state (int32) with a two-cell halo in j and k is
-// loaded into a shared-memory staging plane one iteration before its first
-// use, by one TMA box load where the halo lies inside the patch, else cell
-// by cell with cp.async (wrapped or clamped cells), and dequantised from
-// there once into a three-plane FP32 ring; f(n) of the own cells arrives the
-// same way.  x faces are evaluated per thread along its own column (the
-// left state of the next face stays in registers); y and z face states and
-// face integers are exchanged through shared memory.
+// Work decomposition.  A thread owns two neighbouring cells of a row, (j, k)
+// and (j, k+1) with k even, and evaluates everything of the pair with the
+// packed FP32 instructions of sm_100 (__ffma2_rn, __fmul2_rn, __fadd2_rn: one
+// instruction for both cells): the kernel is bound by instruction issue, not
+// by memory bandwidth or the FP32 pipes, so halving the arithmetic
+// instructions is what speeds it up.  A CTA owns a TJ x TK tile of (j, k)
+// columns and marches along i through a range of planes.  Each plane of the
+// stencil state (int32) with a two-cell halo in j and k is loaded into a
+// shared-memory staging plane one iteration before its first use, by TMA box
+// loads where the halo lies inside the patch or across a periodic seam, else
+// cell by cell with cp.async, and dequantised from there once into a
+// three-plane FP32 ring; f(n) of the own cells arrives the same way.  Per
+// plane:
+//   A  slopes of the own pair in y and z (and of the tile's halo rows and
+//      columns); the face-side states the neighbours need go to shared memory
+//   B  y and z faces below the own cells (the z face between the two cells
+//      of a pair never leaves the thread) and the x face above them, along
+//      the thread's own column (the left state of the next x face stays in
+//      registers); face integers go to shared memory
+//   C  residual and update of the own cells, then the plane three ahead is
+//      dequantised into the ring slot this plane leaves.
 #pragma once
 
 #include <cstdint>
@@ -54,12 +66,33 @@
 
 namespace dn {
 
+// Stage parameters, each held twice (as the pair arithmetic consumes them:
+// one 64-bit constant load per use).
 struct FxParams {
-  float Ax, Ay, Az;
-  float base[5];        // B_v rounded to FP32
-  float quantum[5];     // q_v
-  float face_scale[5];  // (factor/dV)/q_v
+  float2 A[3];          // face areas of the x, y and z faces
+  float2 base[5];       // B_v rounded to FP32
+  float2 quantum[5];    // q_v
+  float2 face_scale[5]; // (factor/dV)/q_v
 };
+
+// The parameters of a stage with RK factor alpha*dt of a patch with spacings
+// (dx, dy, dz) and fixed-point base and quantum (the single-patch launch and
+// the batched kernel both call this, so their parameters are identical).
+__host__ __device__ inline void fx_set_params(FxParams& p, double dx, double dy, double dz, double factor,
+                                              const double* base, const double* quantum)
+{
+  const float ax = (float)(dy * dz), ay = (float)(dx * dz), az = (float)(dx * dy);
+  p.A[0] = make_float2(ax, ax);
+  p.A[1] = make_float2(ay, ay);
+  p.A[2] = make_float2(az, az);
+  const double pf = factor / (dx * dy * dz);
+  for (int v = 0; v < 5; ++v) {
+    const float b = (float)base[v], q = (float)quantum[v], f = (float)(pf / quantum[v]);
+    p.base[v] = make_float2(b, b);
+    p.quantum[v] = make_float2(q, q);
+    p.face_scale[v] = make_float2(f, f);
+  }
+}
 
 struct FxGeom {
   int ni, nj, nk;
@@ -69,7 +102,7 @@ struct FxGeom {
 };
 
 struct FxArgs {
-  const int32_t* in;     // f(k-1) offsets, [5][ni][nj][nk]
+  const int32_t* in;     // f(k-1) offsets, [5][ni][nj][kp]
   const int32_t* un;     // f(n) offsets (own cell)
   int32_t* out;          // f(k) offsets
   const uint8_t* active; // NULL = all active
@@ -82,120 +115,40 @@ struct FxArgs {
 
 constexpr int kFxLimit = 1 << 30;   // |o| must stay below this
 
-// Primitive face-side state (COMPRESSIBLE_*_VARS): density, velocity,
-// pressure, speed of sound and total enthalpy.  p = rho R T with
-// T = (rE/rho - |u|^2/2)/cv, written as p = (R/cv) (rE - rho|u|^2/2).
-struct Prim {
-  float r, u, v, w, p, a, H;
-};
-
-__device__ __forceinline__ Prim fx_prim(float r, float ru, float rv, float rw, float rE)
-{
-  constexpr float R_over_cv = (float)(Gas::R / Gas::cv);
-  constexpr float gam = (float)Gas::gamma;
-  Prim s;
-  const float ir = __fdividef(1.0f, r);
-  s.r = r;
-  s.u = ru * ir;
-  s.v = rv * ir;
-  s.w = rw * ir;
-  const float ke2 = fmaf(rw, s.w, fmaf(rv, s.v, ru * s.u));   // rho |u|^2
-  s.p = R_over_cv * fmaf(-0.5f, ke2, rE);
-  const float p_ir = s.p * ir;
-  s.a = sqrtf(gam * p_ir);
-  s.H = fmaf(rE, ir, p_ir);                                    // (rho E + p) / rho
-  return s;
-}
-
-// AUSM+ split Mach number and pressure polynomials of one face side
-// (compressibleflux.h:46-75) in closed form:
-//   s = +1:  M4 = 1/4 (M+1)^2 (1 + 1/2 (M-1)^2),  P5 = 1/4 (M+1)^2 ((2-M) + 3/4 M (M-1)^2)
-//   s = -1:  M4 = -1/4 (M-1)^2 (1 + 1/2 (M+1)^2), P5 = 1/4 (M-1)^2 ((2+M) - 3/4 M (M+1)^2)
-// for |M| < 1; for |M| >= 1, M4 = M1 = (M + s|M|)/2 and P5 = M1/M, which is
-// exactly 1 when s*M > 0 and 0 otherwise (no division needed).
-template <int S>
-__device__ __forceinline__ void fx_split(float M, float& m4, float& p5)
-{
-  const float ap = M + 1.0f, am = M - 1.0f;
-  const float ap2 = ap * ap, am2 = am * am;
-  float sub_m4, sub_p5, sup_m4, sup_p5;
-  if (S > 0) {
-    sub_m4 = 0.25f * ap2 * fmaf(0.5f, am2, 1.0f);
-    sub_p5 = 0.25f * ap2 * fmaf(0.75f * M, am2, 2.0f - M);
-    sup_m4 = fmaxf(M, 0.0f);
-    sup_p5 = M > 0.0f ? 1.0f : 0.0f;
-  } else {
-    sub_m4 = -0.25f * am2 * fmaf(0.5f, ap2, 1.0f);
-    sub_p5 = 0.25f * am2 * fmaf(-0.75f * M, ap2, 2.0f + M);
-    sup_m4 = fminf(M, 0.0f);
-    sup_p5 = M < 0.0f ? 1.0f : 0.0f;
-  }
-  const bool sup = fabsf(M) >= 1.0f;
-  m4 = sup ? sup_m4 : sub_m4;
-  p5 = sup ? sup_p5 : sub_p5;
-}
-
-// AUSM+ flux (ausmplus.h:39-106) between face sides L and R, normal DIR.
-// The reference's convective part h0 (phi_L + phi_R) - g0 (phi_R - phi_L)
-// with h0 = f0/2, g0 = |f0|/2 is the upwind form max(f0, 0) phi_L +
-// min(f0, 0) phi_R, evaluated here with one multiply-add per variable.
-template <int DIR>
-__device__ __forceinline__ void fx_ausm(const Prim& L, const Prim& R, float A, float F[5])
-{
-  const float unl = DIR == 0 ? L.u : (DIR == 1 ? L.v : L.w);
-  const float unr = DIR == 0 ? R.u : (DIR == 1 ? R.v : R.w);
-  const float a = 0.5f * (L.a + R.a);
-  const float ia = __fdividef(1.0f, a);
-  const float Ml = unl * ia, Mr = unr * ia;
-  float m4l, p5l, m4r, p5r;
-  fx_split<1>(Ml, m4l, p5l);
-  fx_split<-1>(Mr, m4r, p5r);
-  const float M = m4l + m4r;
-  const float Mp = fmaxf(M, 0.0f);
-  const float Mm = fminf(M, 0.0f);
-  const float p = fmaf(p5l, L.p, p5r * R.p);
-  const float f0 = a * A * fmaf(L.r, Mp, R.r * Mm);
-  const float cp = fmaxf(f0, 0.0f);
-  const float cm = fminf(f0, 0.0f);
-  const float Ap = A * p;
-  F[0] = f0;
-  F[1] = DIR == 0 ? fmaf(cp, L.u, fmaf(cm, R.u, Ap)) : fmaf(cp, L.u, cm * R.u);
-  F[2] = DIR == 1 ? fmaf(cp, L.v, fmaf(cm, R.v, Ap)) : fmaf(cp, L.v, cm * R.v);
-  F[3] = DIR == 2 ? fmaf(cp, L.w, fmaf(cm, R.w, Ap)) : fmaf(cp, L.w, cm * R.w);
-  F[4] = fmaf(cp, L.H, cm * R.H);
-}
-
-// Twice the van Albada slope shared by both face-side states of a cell,
-// 2 s = a b (a + b) / (a^2 + b^2); the face states are U +- 0.5 * (2 s), one
-// multiply-add each.  The denominator carries 1e-30, far below any nonzero
-// a^2 + b^2 of offsets of at least one quantum, so that a = b = 0 gives 0
-// without a test.
-__device__ __forceinline__ float fx_slope(float a, float b)
-{
-  const float den = fmaf(a, a, fmaf(b, b, 1e-30f));
-  return a * b * (a + b) * __fdividef(1.0f, den);
-}
+// Face integers of at most this magnitude keep any cell's residual (at most
+// six faces) inside int32: 6 * 1.25 * 2^28 < 2^31.  While every face of a
+// CTA's plane stays below it the residuals are summed in 32 bits; otherwise
+// that plane sums them in 64 bits.  Either way the result is exact.
+constexpr float kFxNarrowFace = 335544320.0f;    // 1.25 * 2^28
+constexpr float kFxFaceLimit = 1073741824.0f;    // 2^30: a face this large is an error
 
 // ---------------------------------------------------------------------------
-// Paired y/z evaluation.  Lane x of a pair carries a y-direction quantity of
-// a cell, lane y the z-direction one; the halo cells and faces of the two
-// directions share a thread, which halves the work of the threads that
-// handle the tile's halo.  Every y and z slope and face of the kernel, own or
-// halo, goes through these functions, so a face evaluated by two CTAs rounds
-// identically.  (The packed f32x2 instructions of sm_100 measured no faster
-// here than two scalar ones: the kernel is not FP32-pipe bound.)
+// Packed pair arithmetic: lane x belongs to the cell (or face) at k, lane y
+// to the one at k+1.
 __device__ __forceinline__ float2 v2(float a) { return make_float2(a, a); }
-__device__ __forceinline__ float2 add2(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
-__device__ __forceinline__ float2 sub2(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
-__device__ __forceinline__ float2 mul2(float2 a, float2 b) { return make_float2(a.x * b.x, a.y * b.y); }
-__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c)
-{
-  return make_float2(fmaf(a.x, b.x, c.x), fmaf(a.y, b.y, c.y));
-}
+__device__ __forceinline__ float2 add2(float2 a, float2 b) { return __fadd2_rn(a, b); }
+// a - b as one packed multiply-add, b * (-1) + a (the product is exact, so
+// the result is the correctly rounded difference)
+__device__ __forceinline__ float2 sub2(float2 a, float2 b) { return __ffma2_rn(b, make_float2(-1.0f, -1.0f), a); }
+__device__ __forceinline__ float2 mul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
 __device__ __forceinline__ float2 rcp2(float2 a) { return make_float2(__fdividef(1.0f, a.x), __fdividef(1.0f, a.y)); }
+__device__ __forceinline__ float2 sqrt2(float2 a) { return make_float2(sqrtf(a.x), sqrtf(a.y)); }
 __device__ __forceinline__ float2 max0(float2 a) { return make_float2(fmaxf(a.x, 0.0f), fmaxf(a.y, 0.0f)); }
 __device__ __forceinline__ float2 min0(float2 a) { return make_float2(fminf(a.x, 0.0f), fminf(a.y, 0.0f)); }
 
+// max that propagates NaN (PTX max.NaN.f32): a face flux that is not finite
+// makes the running maximum NaN
+__device__ __forceinline__ float fmax_nan(float a, float b)
+{
+  float d;
+  asm("max.NaN.f32 %0, %1, %2;" : "=f"(d) : "f"(a), "f"(b));
+  return d;
+}
+
+// Primitive face-side state (COMPRESSIBLE_*_VARS) of a pair: density,
+// velocity, pressure, speed of sound and total enthalpy.  p = rho R T with
+// T = (rE/rho - |u|^2/2)/cv, written as p = (R/cv) (rE - rho|u|^2/2).
 struct Prim2 {
   float2 r, u, v, w, p, a, H;
 };
@@ -210,51 +163,50 @@ __device__ __forceinline__ Prim2 fx_prim2(float2 r, float2 ru, float2 rv, float2
   s.u = mul2(ru, ir);
   s.v = mul2(rv, ir);
   s.w = mul2(rw, ir);
-  const float2 ke2 = fma2(rw, s.w, fma2(rv, s.v, mul2(ru, s.u)));
+  const float2 ke2 = fma2(rw, s.w, fma2(rv, s.v, mul2(ru, s.u)));   // rho |u|^2
   s.p = mul2(v2(R_over_cv), fma2(v2(-0.5f), ke2, rE));
   const float2 p_ir = mul2(s.p, ir);
-  const float2 t = mul2(v2(gam), p_ir);
-  s.a = make_float2(sqrtf(t.x), sqrtf(t.y));
-  s.H = fma2(rE, ir, p_ir);
+  s.a = sqrt2(mul2(v2(gam), p_ir));
+  s.H = fma2(rE, ir, p_ir);                                          // (rho E + p) / rho
   return s;
 }
 
-// fx_split for a pair of Mach numbers (both lanes on the same side S)
+// AUSM+ split Mach number and pressure polynomials of one face side
+// (compressibleflux.h:46-75) for a pair of Mach numbers, side S = +1 (left)
+// or -1 (right).  With z = (1 + S M)/2 clamped to [0, 1] both sides share
+// one form:
+//   |M4| = z^2 (1 + 2 (z-1)^2),   P5 = z^2 (3 - 2z + 3 (2z-1) (z-1)^2),
+// which for |M| < 1 is the reference's 1/4 (M+S)^2 (1 + 1/2 (M-S)^2) and
+// 1/4 (M+S)^2 ((2 - S M) + 3/4 S M (M-S)^2); the clamp makes P5 exactly 1
+// (S M >= 1) or 0 (S M <= -1) as the reference's M1/M ratio is, and M4
+// becomes M1 = (M + S|M|)/2 with the added term max(M-1, 0) (S = +1) or
+// min(M+1, 0) (S = -1).
 template <int S>
 __device__ __forceinline__ void fx_split2(float2 M, float2& m4, float2& p5)
 {
-  const float2 ap = add2(M, v2(1.0f)), am = sub2(M, v2(1.0f));
-  const float2 ap2 = mul2(ap, ap), am2 = mul2(am, am);
-  float2 sub_m4, sub_p5;
+  const float2 z = make_float2(__saturatef(fmaf(0.5f * S, M.x, 0.5f)), __saturatef(fmaf(0.5f * S, M.y, 0.5f)));
+  const float2 zm1 = add2(z, v2(-1.0f));
+  const float2 w = mul2(zm1, zm1);
+  const float2 z2 = mul2(z, z);
+  const float2 mag = mul2(z2, fma2(v2(2.0f), w, v2(1.0f)));
+  const float2 t = fma2(v2(2.0f), z, v2(-1.0f));
+  p5 = mul2(z2, fma2(mul2(v2(3.0f), t), w, fma2(v2(-2.0f), z, v2(3.0f))));
   if (S > 0) {
-    const float2 t = mul2(v2(0.25f), ap2);
-    sub_m4 = mul2(t, fma2(v2(0.5f), am2, v2(1.0f)));
-    sub_p5 = mul2(t, fma2(mul2(v2(0.75f), M), am2, sub2(v2(2.0f), M)));
+    m4 = add2(mag, max0(add2(M, v2(-1.0f))));
   } else {
-    const float2 t = mul2(v2(0.25f), am2);
-    sub_m4 = mul2(v2(-1.0f), mul2(t, fma2(v2(0.5f), ap2, v2(1.0f))));
-    sub_p5 = mul2(t, fma2(mul2(v2(-0.75f), M), ap2, add2(v2(2.0f), M)));
-  }
-  const bool supx = fabsf(M.x) >= 1.0f, supy = fabsf(M.y) >= 1.0f;
-  if (S > 0) {
-    m4.x = supx ? fmaxf(M.x, 0.0f) : sub_m4.x;
-    m4.y = supy ? fmaxf(M.y, 0.0f) : sub_m4.y;
-    p5.x = supx ? (M.x > 0.0f ? 1.0f : 0.0f) : sub_p5.x;
-    p5.y = supy ? (M.y > 0.0f ? 1.0f : 0.0f) : sub_p5.y;
-  } else {
-    m4.x = supx ? fminf(M.x, 0.0f) : sub_m4.x;
-    m4.y = supy ? fminf(M.y, 0.0f) : sub_m4.y;
-    p5.x = supx ? (M.x < 0.0f ? 1.0f : 0.0f) : sub_p5.x;
-    p5.y = supy ? (M.y < 0.0f ? 1.0f : 0.0f) : sub_p5.y;
+    m4 = sub2(min0(add2(M, v2(1.0f))), mag);
   }
 }
 
-// fx_ausm for a y face (lane x, normal y) and a z face (lane y, normal z);
-// A = (Ay, Az)
+// AUSM+ flux (ausmplus.h:39-106) of a pair of faces with normal DIR between
+// face sides L and R.  The reference's convective part h0 (phi_L + phi_R) -
+// g0 (phi_R - phi_L) with h0 = f0/2, g0 = |f0|/2 is the upwind form
+// max(f0, 0) phi_L + min(f0, 0) phi_R.
+template <int DIR>
 __device__ __forceinline__ void fx_ausm2(const Prim2& L, const Prim2& R, float2 A, float2 F[5])
 {
-  const float2 unl = make_float2(L.v.x, L.w.y);
-  const float2 unr = make_float2(R.v.x, R.w.y);
+  const float2 unl = DIR == 0 ? L.u : (DIR == 1 ? L.v : L.w);
+  const float2 unr = DIR == 0 ? R.u : (DIR == 1 ? R.v : R.w);
   const float2 a = mul2(v2(0.5f), add2(L.a, R.a));
   const float2 ia = rcp2(a);
   float2 m4l, p5l, m4r, p5r;
@@ -266,17 +218,57 @@ __device__ __forceinline__ void fx_ausm2(const Prim2& L, const Prim2& R, float2 
   const float2 cp = max0(f0), cm = min0(f0);
   const float2 Ap = mul2(A, p);
   F[0] = f0;
-  F[1] = fma2(cp, L.u, mul2(cm, R.u));
-  F[2] = fma2(cp, L.v, fma2(cm, R.v, make_float2(Ap.x, 0.0f)));
-  F[3] = fma2(cp, L.w, fma2(cm, R.w, make_float2(0.0f, Ap.y)));
+  F[1] = DIR == 0 ? fma2(cp, L.u, fma2(cm, R.u, Ap)) : fma2(cp, L.u, mul2(cm, R.u));
+  F[2] = DIR == 1 ? fma2(cp, L.v, fma2(cm, R.v, Ap)) : fma2(cp, L.v, mul2(cm, R.v));
+  F[3] = DIR == 2 ? fma2(cp, L.w, fma2(cm, R.w, Ap)) : fma2(cp, L.w, mul2(cm, R.w));
   F[4] = fma2(cp, L.H, mul2(cm, R.H));
 }
 
-// fx_slope (twice the van Albada slope) of a pair of (a, b) differences
+// Twice the van Albada slope shared by both face-side states of a cell,
+// 2 s = a b (a + b) / (a^2 + b^2), for a pair; the face states are
+// U +- 0.5 * (2 s).  The denominator carries 1e-30, far below any nonzero
+// a^2 + b^2 of offsets of at least one quantum, so that a = b = 0 gives 0
+// without a test.
 __device__ __forceinline__ float2 fx_slope2(float2 a, float2 b)
 {
   const float2 den = fma2(a, a, fma2(b, b, v2(1e-30f)));
   return mul2(mul2(mul2(a, b), add2(a, b)), rcp2(den));
+}
+
+// Range of the face fluxes (in quanta) a thread has converted: the largest
+// and smallest value, NaN once a flux is not finite (PTX max.NaN / min.NaN,
+// three inputs).
+struct FaceRange {
+  float hi = 0.0f, lo = 0.0f;
+  __device__ __forceinline__ void add2(float a, float b)
+  {
+    asm("max.NaN.f32 %0, %1, %2, %3;" : "=f"(hi) : "f"(hi), "f"(a), "f"(b));
+    asm("min.NaN.f32 %0, %1, %2, %3;" : "=f"(lo) : "f"(lo), "f"(a), "f"(b));
+  }
+  __device__ __forceinline__ void add(const FaceRange& o)
+  {
+    asm("max.NaN.f32 %0, %1, %2;" : "=f"(hi) : "f"(hi), "f"(o.hi));
+    asm("min.NaN.f32 %0, %1, %2;" : "=f"(lo) : "f"(lo), "f"(o.lo));
+  }
+  // largest magnitude (NaN if any flux was not finite)
+  __device__ __forceinline__ float mag() const { return fmax_nan(hi, -lo); }
+};
+
+// A pair of face fluxes in whole quanta, recorded in r.  A face of 2^30
+// quanta or more (a single face moving the offset by the whole
+// representable range) would saturate in the int32 conversion; the caller
+// flags it instead of passing it on.
+__device__ __forceinline__ int2 fx_quant2(float2 x, FaceRange& r)
+{
+  r.add2(x.x, x.y);
+  return make_int2(__float2int_rn(x.x), __float2int_rn(x.y));
+}
+
+// A single face flux in whole quanta (patch-face fluxes), recorded in r.
+__device__ __forceinline__ int fx_quant1(float x, FaceRange& r)
+{
+  r.add2(x, x);
+  return __float2int_rn(x);
 }
 
 // Cell whose state stands at index x of an axis: the wrapped cell on a
@@ -284,16 +276,6 @@ __device__ __forceinline__ float2 fx_slope2(float2 a, float2 b)
 // edge cell outward makes the van Albada slope of an edge cell exactly zero
 // (one of its differences vanishes), which is the reference's first-order
 // reconstruction at a closed patch edge (upwind2.h:39-42), with no test.
-// A face flux in whole quanta.  A face of 2^30 quanta or more (a single
-// face moving the offset by the whole representable range) or a flux that is
-// not finite would saturate or vanish in the int32 conversion; it is flagged
-// instead of passing silently.
-__device__ __forceinline__ int fx_quant(float x, bool& bad)
-{
-  bad |= !(fabsf(x) < 1073741824.0f);
-  return __float2int_rn(x);
-}
-
 __device__ __forceinline__ int fx_index(int x, int n, int per)
 {
   if (per) {
@@ -309,51 +291,46 @@ __device__ __forceinline__ bool fx_face_exists(int x, int n, int per)
   return per ? true : (x >= 1 && x <= n - 1);
 }
 
-// Shared memory of a CTA.  Every array starts on a 128-byte boundary and is
-// laid out so that a warp's accesses hit distinct banks: the plane ring
-// stores rows in interleaved pairs ([row/2][col][row%2]), since a warp of a
-// 16-wide tile spans two rows; the z arrays keep own columns at stride TK
-// and park the one extra (halo) column of each row in the bank the own
-// columns leave free.  The staging area holds the next plane as stored
-// (int32) until it is dequantised into the ring: a main box of rows j0-2 ..
-// j0+TJ+1 and columns k0-4 .. k0+TK+3 (plain rows; the column origin k0-4
-// keeps a TMA box on a 16-byte boundary), and, for tiles at the seam of a
-// periodic axis, the wrapped columns (k side box, 4 wide), the wrapped rows
-// (j side box, 2 high) and their corner.
+// Resident CTAs per SM the register allocation is sized for: two 256-thread
+// or three 128-thread CTAs (the shared memory of the tile allows no more).
+template <int NT>
+struct FxOccupancy {
+  static constexpr int min_blocks = NT >= 256 ? 2 : 3;
+};
+
+// Shared memory of a CTA.  Every array starts on a 128-byte boundary.  The
+// staging area holds the next plane as stored (int32) until it is
+// dequantised into the ring: a main box of rows j0-2 .. j0+TJ+1 and columns
+// k0-4 .. k0+TK+3 (the column origin k0-4 keeps a TMA box on a 16-byte
+// boundary), and, for tiles at the seam of a periodic axis, the wrapped
+// columns (k side box, 4 wide), the wrapped rows (j side box, 2 high) and
+// their corner.  Pairs are read and written as 8-byte words: a half-warp
+// then covers one row of a 32-wide tile, 32 consecutive banks.
 template <int TJ, int TK>
 struct FxSmem {
-  static constexpr int PJ = TJ + 4;
-  static constexpr int PK = TK + 4;
+  static constexpr int PJ = TJ + 4;              // ring rows j0-2 .. j0+TJ+1
+  static constexpr int PK = TK + 4;              // ring columns k0-2 .. k0+TK+1
   static constexpr int SK = TK + 8;              // main box row: columns k0-4 .. k0+TK+3
-  static constexpr int NW = TJ * TK / 32;        // warps of a CTA
-  // Side boxes only for 16-wide tiles: with them the 32-wide tile's shared
-  // memory would leave room for two CTAs per SM instead of three (its
-  // tiles at a periodic seam copy cell by cell).
-  static constexpr bool SEAMS = TK <= 16;
+  static constexpr int TP = TK / 2;              // pairs (threads) per row
+  static constexpr int NT = TJ * TP;             // threads of a CTA
   static constexpr int up128(int n) { return (n + 31) / 32 * 32; }   // int32 count to 128 bytes
   static constexpr int ST_M = 0;                                   // main box [5][PJ][SK]
   static constexpr int ST_K = ST_M + up128(5 * PJ * SK);           // k side box [5][PJ][4]
-  static constexpr int ST_J = ST_K + (SEAMS ? up128(5 * PJ * 4) : 0);   // j side box [5][2][SK]
-  static constexpr int ST_C = ST_J + (SEAMS ? up128(5 * 2 * SK) : 0);   // corner box [5][2][4]
-  static constexpr int ST_N = ST_C + (SEAMS ? up128(5 * 2 * 4) : 0);
-  alignas(128) float plane[3][5][PJ / 2][PK][2]; // dequantised state, ring over planes i .. i+2
+  static constexpr int ST_J = ST_K + up128(5 * PJ * 4);            // j side box [5][2][SK]
+  static constexpr int ST_C = ST_J + up128(5 * 2 * SK);            // corner box [5][2][4]
+  static constexpr int ST_N = ST_C + up128(5 * 2 * 4);
+  alignas(128) float plane[3][5][PJ][PK];        // dequantised state, ring over planes i .. i+2
   alignas(128) int stage[ST_N];                  // plane i+3 as stored, on its way into the ring
   alignas(128) int un[5][TJ][TK];                // f(n) of the own cells of the current plane
-  alignas(128) float sy[5][TJ + 1][TK];          // y: left state of the face above row jj-1 (row -1 .. TJ-1)
-  alignas(128) float sy_top[5][TK];              // y: right state of the face below row TJ (halo)
-  alignas(128) float szL[5][TJ][TK];             // z: left state of the face above col kk (own columns)
-  alignas(128) float szH[5][NW][32];             // z: left state of the face above col -1 (halo), see zh_slot
-  alignas(128) float sz_top[5][TJ];              // z: right state of the face below col TK (halo)
+  alignas(128) float sy[5][TJ + 1][TK];          // y: left state of the face below row jj (jj = 0 .. TJ)
+  alignas(128) float sy_top[5][TK];              // y: right state of the face below halo row TJ
+  alignas(128) float szp[5][TJ][TP + 1];         // z: left state of the face below column 2p (p = 0 .. TP)
+  alignas(128) float sz_top[5][TJ];              // z: right state of the face below halo column TK
   alignas(128) int qy[5][TJ + 1][TK];            // y face integers, face below row jj
-  alignas(128) int qzL[5][TJ][TK];               // z face integers, face below col kk (own columns)
-  alignas(128) int qzT[5][NW][32];               // z face integers, face below col TK (halo), see zt_slot
+  alignas(128) int2 qz[5][TJ][TP + 1];           // z face integers below columns 2p and 2p+1
   alignas(8) uint64_t bar[2];                    // mbarriers of the TMA loads: staging plane, f(n)
+  int wide[2];                                   // a face of the plane reached kFxNarrowFace
 };
-
-// bank-free slots of the per-row halo values of the z arrays
-template <int TK> __device__ __forceinline__ int zh_slot(int row) { return (row * TK + TK - 1) & 31; }
-template <int TK> __device__ __forceinline__ int zt_slot(int row) { return (row * TK) & 31; }
-template <int TK> __device__ __forceinline__ int z_warp(int row) { return (row * TK) >> 5; }
 
 __device__ __forceinline__ void fx_cp_async4(void* smem, const void* gmem)
 {
@@ -405,34 +382,66 @@ __device__ __forceinline__ int fx_seam(int t0, int T, int n, int per)
   return -1;
 }
 
+// Where ring position (row jj, column c) of a tile reads its cell in the
+// staging area: offset of variable 0 (*soff) and stride between variables
+// (*svar).  Cell copies fill the main box position by position; TMA boxes
+// hold the main box plus the side boxes of a periodic seam, and on a closed
+// axis the cells outside the patch read the edge cell's slot of the box.
+template <int TJ, int TK>
+__device__ __forceinline__ void fx_stage_slot(const FxGeom& g, bool tma, int j0, int k0, int jj, int c, int* soff,
+                                              int* svar)
+{
+  using Smem = FxSmem<TJ, TK>;
+  constexpr int PJ = Smem::PJ, SK = Smem::SK;
+  *soff = Smem::ST_M + jj * SK + c + 2;
+  *svar = PJ * SK;
+  if (!tma) return;
+  const int jg = j0 - 2 + jj, kg = k0 - 2 + c;
+  const bool jside = g.per_y && (jg < 0 || jg >= g.nj);
+  const int jr = jside ? (jg < 0 ? jg + 2 : jg - g.nj) : (g.per_y ? jg : min(max(jg, 0), g.nj - 1)) - (j0 - 2);
+  const bool kside = g.per_z && (kg < 0 || kg >= g.nk);
+  const int kr = kside ? (kg < 0 ? kg + 4 : kg - g.nk) : (g.per_z ? kg : min(max(kg, 0), g.nk - 1)) - (k0 - 4);
+  if (jside) {
+    *soff = (kside ? Smem::ST_C + jr * 4 : Smem::ST_J + jr * SK) + kr;
+    *svar = kside ? 2 * 4 : 2 * SK;
+  } else {
+    *soff = (kside ? Smem::ST_K + jr * 4 : Smem::ST_M + jr * SK) + kr;
+    *svar = kside ? PJ * 4 : PJ * SK;
+  }
+}
+
 // One tile of one patch: columns (j0 .. j0+TJ-1, k0 .. k0+TK-1), planes i0 .. i1-1.
 // tm_in: the kFxMaps tensor maps of the stage input, tm_un: the map of f(n)
 // (box TK x TJ x 1 x 5), or null.  With maps, a tile stages its planes by
-// TMA box loads unless fx_seam excludes it; closed-axis cells outside the
-// patch then read the edge cell's slot of the main box, and the cells across
-// the seam of a periodic axis come from the side boxes.  Other tiles copy
-// cell by cell.
+// TMA box loads unless fx_seam excludes it; other tiles copy cell by cell.
+// FULL tiles (fx_tile_full) skip every edge test, and their ring positions
+// come in adjacent pairs in every staging form (no clamping; a periodic seam
+// falls between pairs), so they dequantise pairwise.
 template <int TJ, int TK, bool FULL>
 __device__ __forceinline__ void fx_stage_tile_impl(const FxArgs& a, const CUtensorMap* tm_in,
                                                    const CUtensorMap* tm_un, int j0, int k0, int i0, int i1)
 {
-  constexpr int NT = TJ * TK;
-  constexpr int PJ = TJ + 4, PK = TK + 4;
+  using Smem = FxSmem<TJ, TK>;
+  constexpr int PJ = Smem::PJ, PK = Smem::PK, SK = Smem::SK, TP = Smem::TP, NT = Smem::NT;
   constexpr int NP = PJ * PK;                     // positions of a plane tile (per variable)
   constexpr int PPT = (NP + NT - 1) / NT;         // positions per thread
-  using Smem = FxSmem<TJ, TK>;
-  constexpr int SK = Smem::SK;
+  constexpr int NPP = PJ * (PK / 2);              // position pairs of a plane tile
+  constexpr int PPT2 = (NPP + NT - 1) / NT;       // position pairs per thread
+  static_assert(TK % 4 == 0 && TJ % 2 == 0 && TP <= 32 && TJ / 2 <= 32 && NT >= 64 && TK + TJ <= NT,
+                "tile shape");
   extern __shared__ __align__(128) unsigned char fx_smem_raw[];
   Smem& sm = *reinterpret_cast<Smem*>(fx_smem_raw);
 
   const FxGeom& g = a.g;
   const FxParams& P = a.p;
-  const int tx = threadIdx.x, ty = threadIdx.y;
-  const int tid = ty * TK + tx;
-  const int j = j0 + ty, k = k0 + tx;
-  const bool own = FULL || ((j < g.nj) && (k < g.nk));
+  const int tp = threadIdx.x, ty = threadIdx.y;
+  const int tid = ty * TP + tp;
+  const int kk = 2 * tp;                          // tile column of the pair's first cell
+  const int j = j0 + ty, ka = k0 + kk, kb = ka + 1;
+  const bool own_a = FULL || ((j < g.nj) && (ka < g.nk));
+  const bool own_b = FULL || ((j < g.nj) && (kb < g.nk));
   const int njk = g.nj * g.kp;                    // plane stride (rows of kp elements)
-  const size_t nc = (size_t)g.ni * njk;           // variable stride
+  const int nc = g.ni * njk;                      // variable stride (5 * nc < 2^31, host check)
   // TMA boxes start at x = k0-4 (main; a multiple of 4 int32 since TK is),
   // k0 (f(n)), and nk-4 or 0 (k side box): the first seam tile of a periodic
   // k axis needs nk % 4 == 0 for its side box (the last one has k0+TK = nk,
@@ -440,108 +449,123 @@ __device__ __forceinline__ void fx_stage_tile_impl(const FxArgs& a, const CUtens
   // never read; destinations 128-byte aligned
   const int seam_j = fx_seam(j0, TJ, g.nj, g.per_y);
   const int seam_k = fx_seam(k0, TK, g.nk, g.per_z);
-  const bool tma = tm_in != nullptr && seam_j >= 0 && seam_k >= 0 && (Smem::SEAMS || (seam_j | seam_k) == 0) &&
-                   (seam_k != 1 || (g.nk & 3) == 0) &&
+  const bool tma = tm_in != nullptr && seam_j >= 0 && seam_k >= 0 && (seam_k != 1 || (g.nk & 3) == 0) &&
                    ((smem_u32(&sm.stage[0]) | smem_u32(&sm.un[0][0][0])) & 127) == 0;
 
-  // plane element (jj, kk) of variable v in ring slot sl (rows interleaved in pairs)
-  auto PL = [&](int sl, int v, int jj, int kk) -> float& { return sm.plane[sl][v][jj >> 1][kk][jj & 1]; };
+  auto PL2 = [&](int sl, int v, int jj, int c) -> float2& {
+    return *reinterpret_cast<float2*>(&sm.plane[sl][v][jj][c]);
+  };
+  // the own pair's ring position (row ty+2, column kk+2) in slot 0,
+  // variable 0; a slot's own pair of variable v, dj rows and dk columns away,
+  // is then (base + v*VS + dj*PK + dk) with compile-time offsets
+  constexpr int VS = PJ * PK, SS = 5 * VS;
+  const float* const ring_me = &sm.plane[0][0][ty + 2][kk + 2];
+  auto RP = [&](const float* base, int v, int dj, int dk) -> float2 {
+    return *reinterpret_cast<const float2*>(base + v * VS + dj * PK + dk);
+  };
 
-  // per-thread plane positions e = tid + m*NT in ring order [row/2][col][row%2]:
-  // in-plane offset j*nk + k of the (wrapped, or on closed axes clamped)
-  // column, and where the position's cell lies in the staging area: offset
-  // of variable 0 and the stride between variables of its box (cell copies
-  // fill the main box position by position)
+  // per-thread staging positions: single positions e = tid + m*NT in ring
+  // order [row][column] with the in-plane offset j*kp + k of their (wrapped
+  // or clamped) cell for cell copies; the edge form also keeps their
+  // staging slots, the FULL form the staging slots of position pairs
   int32_t poff[PPT];
-  int32_t soff[PPT];
-  int32_t svar[PPT];
+  int32_t soff[FULL ? PPT2 : PPT];
+  int32_t svar[FULL ? PPT2 : PPT];
   #pragma unroll
   for (int m = 0; m < PPT; ++m) {
     const int e = tid + m * NT;
     poff[m] = -1;
-    soff[m] = 0;
-    svar[m] = PJ * SK;
     if (e < NP) {
-      const int jj = (e / (2 * PK)) * 2 + (e & 1);
-      const int kk = (e % (2 * PK)) >> 1;
-      const int jg = j0 - 2 + jj, kg = k0 - 2 + kk;
-      poff[m] = fx_index(jg, g.nj, g.per_y) * g.kp + fx_index(kg, g.nk, g.per_z);
-      soff[m] = Smem::ST_M + jj * SK + kk + 2;
-      if (tma) {
-        // row: in the main box (clamped on a closed axis) or across the seam
-        const bool jside = g.per_y && (jg < 0 || jg >= g.nj);
-        const int jr = jside ? (jg < 0 ? jg + 2 : jg - g.nj) : (g.per_y ? jg : min(max(jg, 0), g.nj - 1)) - (j0 - 2);
-        const bool kside = g.per_z && (kg < 0 || kg >= g.nk);
-        const int kr = kside ? (kg < 0 ? kg + 4 : kg - g.nk) : (g.per_z ? kg : min(max(kg, 0), g.nk - 1)) - (k0 - 4);
-        if (jside) {
-          soff[m] = (kside ? Smem::ST_C + jr * 4 : Smem::ST_J + jr * SK) + kr;
-          svar[m] = kside ? 2 * 4 : 2 * SK;
-        } else {
-          soff[m] = (kside ? Smem::ST_K + jr * 4 : Smem::ST_M + jr * SK) + kr;
-          svar[m] = kside ? PJ * 4 : PJ * SK;
-        }
-      }
+      const int jj = e / PK, c = e % PK;
+      poff[m] = fx_index(j0 - 2 + jj, g.nj, g.per_y) * g.kp + fx_index(k0 - 2 + c, g.nk, g.per_z);
+      if (!FULL) fx_stage_slot<TJ, TK>(g, tma, j0, k0, jj, c, &soff[m], &svar[m]);
+    }
+  }
+  if (FULL) {
+    #pragma unroll
+    for (int m = 0; m < PPT2; ++m) {
+      const int e = tid + m * NT;
+      soff[m] = 0;
+      svar[m] = 0;
+      if (e < NPP) fx_stage_slot<TJ, TK>(g, tma, j0, k0, e / (PK / 2), 2 * (e % (PK / 2)), &soff[m], &svar[m]);
     }
   }
 
   // plane ip of the stage input, copied cell by cell (cp.async) as int32
   // into ring slot sl, then dequantised there in place by the copying thread
   auto issue_ring = [&](int sl, int ip) {
-    int* dst = reinterpret_cast<int*>(&sm.plane[sl][0][0][0][0]);
-    const int32_t* src = a.in + (size_t)fx_index(ip, g.ni, g.per_x) * njk;
+    int* dst = reinterpret_cast<int*>(&sm.plane[sl][0][0][0]);
+    const int32_t* src = a.in + fx_index(ip, g.ni, g.per_x) * njk;
     #pragma unroll
     for (int v = 0; v < 5; ++v) {
       #pragma unroll
       for (int m = 0; m < PPT; ++m) {
         const int e = tid + m * NT;
-        if (e < NP) fx_cp_async4(dst + v * NP + e, src + (size_t)v * nc + poff[m]);
+        if (e < NP) fx_cp_async4(dst + v * NP + e, src + v * nc + poff[m]);
       }
     }
   };
   auto dequant_ring = [&](int sl) {
-    float* f = &sm.plane[sl][0][0][0][0];
+    float* f = &sm.plane[sl][0][0][0];
     const int* q = reinterpret_cast<const int*>(f);
     #pragma unroll
     for (int v = 0; v < 5; ++v) {
       #pragma unroll
       for (int m = 0; m < PPT; ++m) {
         const int e = tid + m * NT;
-        if (e < NP) f[v * NP + e] = fmaf(P.quantum[v], (float)q[v * NP + e], P.base[v]);
+        if (e < NP) f[v * NP + e] = fmaf(P.quantum[v].x, (float)q[v * NP + e], P.base[v].x);
       }
     }
   };
-  // plane ip into the staging plane, cell by cell (tiles without TMA)
+  // plane ip into the staging plane's main box, cell by cell (tiles without TMA)
   auto issue_stage = [&](int ip) {
-    int* dst = &sm.stage[0];
-    const int32_t* src = a.in + (size_t)fx_index(ip, g.ni, g.per_x) * njk;
+    int* dst = &sm.stage[Smem::ST_M];
+    const int32_t* src = a.in + fx_index(ip, g.ni, g.per_x) * njk;
     #pragma unroll
     for (int v = 0; v < 5; ++v) {
       #pragma unroll
       for (int m = 0; m < PPT; ++m) {
         const int e = tid + m * NT;
-        if (e < NP) fx_cp_async4(dst + soff[m] + v * svar[m], src + (size_t)v * nc + poff[m]);
+        if (e < NP) fx_cp_async4(dst + v * (PJ * SK) + (e / PK) * SK + e % PK + 2, src + v * nc + poff[m]);
       }
     }
   };
   // the staging area, dequantised into ring slot sl
   auto dequant_stage = [&](int sl) {
-    float* f = &sm.plane[sl][0][0][0][0];
     const int* q = &sm.stage[0];
-    #pragma unroll
-    for (int v = 0; v < 5; ++v) {
+    if (FULL) {
+      // pair e of a ring slot starts at float 2e of its variable's plane
+      float2* f = reinterpret_cast<float2*>(&sm.plane[sl][0][0][0]);
       #pragma unroll
-      for (int m = 0; m < PPT; ++m) {
-        const int e = tid + m * NT;
-        if (e < NP) f[v * NP + e] = fmaf(P.quantum[v], (float)q[soff[m] + v * svar[m]], P.base[v]);
+      for (int v = 0; v < 5; ++v) {
+        #pragma unroll
+        for (int m = 0; m < PPT2; ++m) {
+          const int e = tid + m * NT;
+          if (e < NPP) {
+            const int2 o = *reinterpret_cast<const int2*>(q + soff[m] + v * svar[m]);
+            f[v * NPP + e] = fma2(P.quantum[v], make_float2((float)o.x, (float)o.y), P.base[v]);
+          }
+        }
+      }
+    } else {
+      float* f = &sm.plane[sl][0][0][0];
+      #pragma unroll
+      for (int v = 0; v < 5; ++v) {
+        #pragma unroll
+        for (int m = 0; m < PPT; ++m) {
+          const int e = tid + m * NT;
+          if (e < NP) f[v * NP + e] = fmaf(P.quantum[v].x, (float)q[soff[m] + v * svar[m]], P.base[v].x);
+        }
       }
     }
   };
-  // f(n) of the own cell, plane ip, cell by cell (tiles without TMA)
+  // f(n) of the own cells, plane ip, cell by cell (tiles without TMA)
   auto fetch_un = [&](int ip) {
-    if (own) {
-      const int c = ip * njk + j * g.kp + k;
-      #pragma unroll
-      for (int v = 0; v < 5; ++v) fx_cp_async4(&sm.un[v][ty][tx], a.un + (size_t)v * nc + c);
+    const int c = ip * njk + j * g.kp + ka;
+    #pragma unroll
+    for (int v = 0; v < 5; ++v) {
+      if (own_a) fx_cp_async4(&sm.un[v][ty][kk], a.un + v * nc + c);
+      if (own_b) fx_cp_async4(&sm.un[v][ty][kk + 1], a.un + v * nc + c + 1);
     }
   };
   // TMA loads of f(n) of plane ip and, if wanted, of stage-input plane ip+3
@@ -564,115 +588,138 @@ __device__ __forceinline__ void fx_stage_tile_impl(const FxArgs& a, const CUtens
     }
   };
 
-  if (tma && tid == 0) {
-    mbar_init(&sm.bar[0], 1);
-    mbar_init(&sm.bar[1], 1);
-    mbar_init_fence();
+  if (tid == 0) {
+    if (tma) {
+      mbar_init(&sm.bar[0], 1);
+      mbar_init(&sm.bar[1], 1);
+      mbar_init_fence();
+    }
+    sm.wide[0] = 0;
+    sm.wide[1] = 0;
   }
 
   // prologue: planes i0 .. i0+2 in the ring (the barrier below also
-  // publishes the mbarrier initialisation)
+  // publishes the mbarrier initialisation and the cleared flags)
   for (int q = 0; q <= 2; ++q) issue_ring(q, i0 + q);
   fx_cp_async_commit();
   fx_cp_async_wait<0>();
   for (int q = 0; q <= 2; ++q) dequant_ring(q);
   __syncthreads();
 
-  // x direction registers: left state of the face above the current cell,
-  // the downwind difference of the current cell, and the lower face integers
-  bool fbad = false;     // a face flux left the fixed-point range (fx_quant)
+  // x direction registers: prim of the left state of the face above the
+  // current cells, the downwind difference and the state of the next plane,
+  // and the lower face integers
+  FaceRange fmag;        // face fluxes in quanta of the current plane
+  FaceRange xmag;        // the same of the x faces below the current cells (the last plane's upper ones)
+  bool fbad = false;     // a face flux reached 2^30 quanta or was not finite
   bool tbad = false;     // a TMA wait ran out
-  Prim xleft;
-  float xb[5];           // U_{i+1} - U_i of the own column (becomes a of cell i+1)
-  int qx_lo[5];
+  Prim2 xleft;
+  float2 xb[5];          // U_{i+1} - U_i of the own pair (becomes a of cell i+1)
+  int2 qx_lo[5];
   {
     // slope of cell i0 (needs i0-1, i0, i0+1) and the face below i0; planes
     // i0-1 and i0-2 of the own column come straight from the stage input
-    const int64_t col = (int64_t)j * g.kp + k;
+    // (read as a pair when the first cell is inside: the second of a partial
+    // pair lies in the row padding)
+    const int col = j * g.kp + ka;
     const int iw1 = fx_index(i0 - 1, g.ni, g.per_x);
-    float Ul[5], Sp[5], Sm[5];
-    float U0[5];
+    float2 Ul[5], Sp[5], Sm[5], U0[5];
     #pragma unroll
     for (int v = 0; v < 5; ++v) {
-      const float um = own ? fmaf(P.quantum[v], (float)__ldg(a.in + (int64_t)v * nc + (int64_t)iw1 * njk + col), P.base[v])
-                           : 0.0f;
-      const float uc = PL(0, v, ty + 2, tx + 2);
-      const float up = PL(1, v, ty + 2, tx + 2);
-      const float s = fx_slope(uc - um, up - uc);
+      float2 um = v2(0.0f);
+      if (own_a) {
+        const int2 o = __ldg(reinterpret_cast<const int2*>(a.in + v * nc + iw1 * njk + col));
+        um = fma2(P.quantum[v], make_float2((float)o.x, (float)o.y), P.base[v]);
+      }
+      const float2 uc = PL2(0, v, ty + 2, kk + 2);
+      const float2 up = PL2(1, v, ty + 2, kk + 2);
+      const float2 s = fx_slope2(sub2(uc, um), sub2(up, uc));
       U0[v] = uc;
-      Sp[v] = fmaf(s, 0.5f, uc);
-      Sm[v] = fmaf(s, -0.5f, uc);
-      xb[v] = up - uc;
+      Sp[v] = fma2(s, v2(0.5f), uc);
+      Sm[v] = fma2(s, v2(-0.5f), uc);
+      xb[v] = sub2(up, uc);
       Ul[v] = um;
     }
-    xleft = fx_prim(Sp[0], Sp[1], Sp[2], Sp[3], Sp[4]);
+    xleft = fx_prim2(Sp[0], Sp[1], Sp[2], Sp[3], Sp[4]);
     // face below i0: left state from cell i0-1 (slope needs i0-2)
-    const bool ex = own && fx_face_exists(i0, g.ni, g.per_x);
-    if (ex) {
+    if (own_a && fx_face_exists(i0, g.ni, g.per_x)) {
       const int iw2 = fx_index(i0 - 2, g.ni, g.per_x);
-      float Lm[5];
+      float2 Lm[5];
       #pragma unroll
       for (int v = 0; v < 5; ++v) {
-        const float umm = fmaf(P.quantum[v], (float)__ldg(a.in + (int64_t)v * nc + (int64_t)iw2 * njk + col), P.base[v]);
-        Lm[v] = fmaf(fx_slope(Ul[v] - umm, U0[v] - Ul[v]), 0.5f, Ul[v]);
+        const int2 o = __ldg(reinterpret_cast<const int2*>(a.in + v * nc + iw2 * njk + col));
+        const float2 umm = fma2(P.quantum[v], make_float2((float)o.x, (float)o.y), P.base[v]);
+        Lm[v] = fma2(fx_slope2(sub2(Ul[v], umm), sub2(U0[v], Ul[v])), v2(0.5f), Ul[v]);
       }
-      float F[5];
-      fx_ausm<0>(fx_prim(Lm[0], Lm[1], Lm[2], Lm[3], Lm[4]), fx_prim(Sm[0], Sm[1], Sm[2], Sm[3], Sm[4]), P.Ax, F);
+      float2 F[5];
+      fx_ausm2<0>(fx_prim2(Lm[0], Lm[1], Lm[2], Lm[3], Lm[4]), fx_prim2(Sm[0], Sm[1], Sm[2], Sm[3], Sm[4]), P.A[0],
+                  F);
       #pragma unroll
-      for (int v = 0; v < 5; ++v) qx_lo[v] = fx_quant(F[v] * P.face_scale[v], fbad);
+      for (int v = 0; v < 5; ++v) {
+        qx_lo[v] = fx_quant2(mul2(F[v], P.face_scale[v]), xmag);
+        if (!own_b) qx_lo[v].y = 0;
+      }
     } else {
       #pragma unroll
-      for (int v = 0; v < 5; ++v) qx_lo[v] = 0;
+      for (int v = 0; v < 5; ++v) qx_lo[v] = make_int2(0, 0);
     }
   }
 
   int s0 = 0, sp1 = 1, sp2 = 2;       // ring slots of planes i, i+1, i+2
   unsigned ph_plane = 0, ph_un = 0;   // parities of the next TMA completions
+  int par = 0;                        // plane parity: slot of sm.wide
   for (int i = i0; i < i1; ++i) {
     const bool more = i + 3 <= i1 + 1;  // plane i+3 is read by a later iteration
 
-    // ---------------- y and z face states of plane i
-    float2 yzm[5];   // right states of the y (lane x) and z (lane y) faces below the own cell
-    {
-      #pragma unroll
-      for (int v = 0; v < 5; ++v) {
-        const float2 uc = v2(PL(s0, v, ty + 2, tx + 2));
-        const float2 ul = make_float2(PL(s0, v, ty + 1, tx + 2), PL(s0, v, ty + 2, tx + 1));
-        const float2 uh = make_float2(PL(s0, v, ty + 3, tx + 2), PL(s0, v, ty + 2, tx + 3));
-        const float2 s = fx_slope2(sub2(uc, ul), sub2(uh, uc));
-        const float2 up = fma2(s, v2(0.5f), uc);
-        sm.sy[v][ty + 1][tx] = up.x;
-        sm.szL[v][ty][tx] = up.y;
-        yzm[v] = fma2(s, v2(-0.5f), uc);
+    // ---------------- A: y and z slopes of plane i
+    float2 ym[5];    // right states of the y faces below the own pair
+    float2 zm[5];    // right states of the z faces below the own pair
+    float zpx[5];    // left state of the z face between the pair's cells
+    const float* const r0 = ring_me + s0 * SS;
+    #pragma unroll
+    for (int v = 0; v < 5; ++v) {
+      const float2 C = RP(r0, v, 0, 0);
+      {
+        const float2 lo = RP(r0, v, -1, 0), hi = RP(r0, v, 1, 0);
+        const float2 s = fx_slope2(sub2(C, lo), sub2(hi, C));
+        *reinterpret_cast<float2*>(&sm.sy[v][ty + 1][kk]) = fma2(s, v2(0.5f), C);
+        ym[v] = fma2(s, v2(-0.5f), C);
+      }
+      {
+        const float zl = RP(r0, v, 0, -2).y, zh = RP(r0, v, 0, 2).x;
+        const float d1 = C.y - C.x;
+        const float2 s = fx_slope2(make_float2(C.x - zl, d1), make_float2(d1, zh - C.y));
+        const float2 zp = fma2(s, v2(0.5f), C);
+        zm[v] = fma2(s, v2(-0.5f), C);
+        zpx[v] = zp.x;
+        sm.szp[v][ty][tp + 1] = zp.y;
       }
     }
-    // halo cells, y and z in pairs: y rows -1 (left state) and TJ (right
-    // state), z cols -1 and TK
-    for (int h = tid; h < 2 * (TK > TJ ? TK : TJ); h += NT) {
-      const bool hy = h < 2 * TK, hz = h < 2 * TJ;
-      const int kky = h % TK;
-      const bool topy = h >= TK;
-      const int jjy = topy ? TJ : -1;                 // tile-relative row of the y cell
-      const int jjz = h % TJ;
-      const bool topz = h >= TJ;
-      const int kkz = topz ? TK : -1;                 // tile-relative col of the z cell
-      // a lane without a cell evaluates the other lane's cell and stores nothing
-      const int ry = hy ? jjy + 2 : jjz + 2, cy = hy ? kky + 2 : kkz + 2;
-      const int rz = hz ? jjz + 2 : jjy + 2, cz = hz ? kkz + 2 : kky + 2;
-      #pragma unroll
-      for (int v = 0; v < 5; ++v) {
-        const float2 uc = make_float2(PL(s0, v, ry, cy), PL(s0, v, rz, cz));
-        const float2 ul = make_float2(PL(s0, v, ry - 1, cy), PL(s0, v, rz, cz - 1));
-        const float2 uh = make_float2(PL(s0, v, ry + 1, cy), PL(s0, v, rz, cz + 1));
-        const float2 s = fx_slope2(sub2(uc, ul), sub2(uh, uc));
-        const float2 up = fma2(s, v2(0.5f), uc), dn = fma2(s, v2(-0.5f), uc);
-        if (hy) {
-          if (topy) sm.sy_top[v][kky] = dn.x;
-          else sm.sy[v][0][kky] = up.x;
+    // halo slopes (first warps): y rows -1 (left states) and TJ (right
+    // states) in column pairs; z columns -1 (left state, lane x) and TK
+    // (right state, lane y) of a row
+    if (tid < TK + TJ) {
+      if (tid < TK) {
+        const bool top = tid >= TP;
+        const int c = 2 * (tid % TP);
+        const int r = top ? TJ + 2 : 1;             // ring row of the halo cell
+        #pragma unroll
+        for (int v = 0; v < 5; ++v) {
+          const float2 C = PL2(s0, v, r, c + 2);
+          const float2 s = fx_slope2(sub2(C, PL2(s0, v, r - 1, c + 2)), sub2(PL2(s0, v, r + 1, c + 2), C));
+          if (top) *reinterpret_cast<float2*>(&sm.sy_top[v][c]) = fma2(s, v2(-0.5f), C);
+          else *reinterpret_cast<float2*>(&sm.sy[v][0][c]) = fma2(s, v2(0.5f), C);
         }
-        if (hz) {
-          if (topz) sm.sz_top[v][jjz] = dn.y;
-          else sm.szH[v][z_warp<TK>(jjz)][zh_slot<TK>(jjz)] = up.y;
+      } else {
+        const int jj = tid - TK;
+        #pragma unroll
+        for (int v = 0; v < 5; ++v) {
+          const float* row = &sm.plane[s0][v][jj + 2][0];
+          const float2 C = make_float2(row[1], row[TK + 2]);
+          const float2 s = fx_slope2(sub2(C, make_float2(row[0], row[TK + 1])),
+                                     sub2(make_float2(row[2], row[TK + 3]), C));
+          sm.szp[v][jj][0] = fmaf(s.x, 0.5f, C.x);
+          sm.sz_top[v][jj] = fmaf(s.y, -0.5f, C.y);
         }
       }
     }
@@ -689,87 +736,145 @@ __device__ __forceinline__ void fx_stage_tile_impl(const FxArgs& a, const CUtens
       if (more) issue_stage(i + 3);
       fx_cp_async_commit();
     }
+    if (tid == 0) sm.wide[par ^ 1] = 0;   // flag of the next plane (its last reader passed the barrier)
+    fmag = xmag;                          // the x faces below the own cells count for this plane too
 
-    // ---------------- y and z faces below the own cell (+ the top halo faces)
+    // ---------------- B: faces
+    // y faces below the own pair; the face below row j is needed even when
+    // row j itself lies beyond a periodic patch (it is the wrapped face above
+    // the last row)
     {
-      // the face below row j is needed even when row j itself lies beyond a
-      // periodic patch (it is the wrapped face above the last row)
-      const bool exy = FULL || (k < g.nk && fx_face_exists(j, g.nj, g.per_y) && (g.per_y || j < g.nj));
-      const bool exz = FULL || (j < g.nj && fx_face_exists(k, g.nk, g.per_z) && (g.per_z || k < g.nk));
       float2 L[5];
       #pragma unroll
-      for (int v = 0; v < 5; ++v)
-        L[v] = make_float2(sm.sy[v][ty][tx], tx > 0 ? sm.szL[v][ty][tx - 1] : sm.szH[v][z_warp<TK>(ty)][zh_slot<TK>(ty)]);
+      for (int v = 0; v < 5; ++v) L[v] = *reinterpret_cast<const float2*>(&sm.sy[v][ty][kk]);
       float2 F[5];
-      fx_ausm2(fx_prim2(L[0], L[1], L[2], L[3], L[4]), fx_prim2(yzm[0], yzm[1], yzm[2], yzm[3], yzm[4]),
-               make_float2(P.Ay, P.Az), F);
-      #pragma unroll
-      for (int v = 0; v < 5; ++v) {
-        const float2 q = mul2(F[v], v2(P.face_scale[v]));
-        sm.qy[v][ty][tx] = exy ? fx_quant(q.x, fbad) : 0;
-        sm.qzL[v][ty][tx] = exz ? fx_quant(q.y, fbad) : 0;
-      }
-    }
-    // halo faces, y and z in pairs: below halo row TJ (col kk = h) and below
-    // halo col TK (row jj = h)
-    // (on the second warp: the first one did the halo slopes of this plane)
-    for (int h = (tid + NT - 32) % NT; h < (TK > TJ ? TK : TJ); h += NT) {
-      const bool hy = h < TK, hz = h < TJ;
-      bool exy = hy, exz = hz;
+      fx_ausm2<1>(fx_prim2(L[0], L[1], L[2], L[3], L[4]), fx_prim2(ym[0], ym[1], ym[2], ym[3], ym[4]), P.A[1], F);
+      bool exa = true, exb = true;
       if (!FULL) {
-        const int jf = j0 + TJ, kf = k0 + h;
-        exy = exy && kf < g.nk && fx_face_exists(jf, g.nj, g.per_y) && (g.per_y || jf < g.nj);
-        const int jz = j0 + h, kz = k0 + TK;
-        exz = exz && jz < g.nj && fx_face_exists(kz, g.nk, g.per_z) && (g.per_z || kz < g.nk);
+        const bool ey = fx_face_exists(j, g.nj, g.per_y) && (g.per_y || j < g.nj);
+        exa = ey && ka < g.nk;
+        exb = ey && kb < g.nk;
       }
-      // a lane without a face evaluates the other lane's face and stores nothing
-      const int ky = hy ? h : 0, jz = hz ? h : 0;
-      float2 L[5], R[5];
       #pragma unroll
       for (int v = 0; v < 5; ++v) {
-        L[v] = make_float2(sm.sy[v][TJ][ky], sm.szL[v][jz][TK - 1]);
-        R[v] = make_float2(sm.sy_top[v][ky], sm.sz_top[v][jz]);
-      }
-      float2 F[5];
-      fx_ausm2(fx_prim2(L[0], L[1], L[2], L[3], L[4]), fx_prim2(R[0], R[1], R[2], R[3], R[4]),
-               make_float2(P.Ay, P.Az), F);
-      #pragma unroll
-      for (int v = 0; v < 5; ++v) {
-        const float2 q = mul2(F[v], v2(P.face_scale[v]));
-        if (hy) sm.qy[v][TJ][h] = exy ? fx_quant(q.x, fbad) : 0;
-        if (hz) sm.qzT[v][z_warp<TK>(h)][zt_slot<TK>(h)] = exz ? fx_quant(q.y, fbad) : 0;
+        int2 q = fx_quant2(mul2(F[v], P.face_scale[v]), fmag);
+        if (!exa) q.x = 0;
+        if (!exb) q.y = 0;
+        *reinterpret_cast<int2*>(&sm.qy[v][ty][kk]) = q;
       }
     }
-    // ---------------- x: face above cell i (between i and i+1)
-    int qx_hi[5];
+    // z faces below the pair's two cells
     {
-      const bool ex = own && fx_face_exists(i + 1, g.ni, g.per_x);
-      float Sm[5], Sp[5];
+      float2 L[5];
+      #pragma unroll
+      for (int v = 0; v < 5; ++v) L[v] = make_float2(sm.szp[v][ty][tp], zpx[v]);
+      float2 F[5];
+      fx_ausm2<2>(fx_prim2(L[0], L[1], L[2], L[3], L[4]), fx_prim2(zm[0], zm[1], zm[2], zm[3], zm[4]), P.A[2], F);
+      bool exa = true, exb = true;
+      if (!FULL) {
+        const bool rowin = j < g.nj;
+        exa = rowin && fx_face_exists(ka, g.nk, g.per_z) && (g.per_z || ka < g.nk);
+        exb = rowin && fx_face_exists(kb, g.nk, g.per_z) && (g.per_z || kb < g.nk);
+      }
       #pragma unroll
       for (int v = 0; v < 5; ++v) {
-        const float uc = PL(sp1, v, ty + 2, tx + 2);
-        const float up = PL(sp2, v, ty + 2, tx + 2);
-        const float b = up - uc;
-        const float s = fx_slope(xb[v], b);
-        Sm[v] = fmaf(s, -0.5f, uc);
-        Sp[v] = fmaf(s, 0.5f, uc);
+        int2 q = fx_quant2(mul2(F[v], P.face_scale[v]), fmag);
+        if (!exa) q.x = 0;
+        if (!exb) q.y = 0;
+        sm.qz[v][ty][tp] = q;
+      }
+    }
+    // halo faces: below halo row TJ in column pairs (second-to-last warp)
+    // and below halo column TK for rows jj and jj + TJ/2 (last warp)
+    {
+      const int h = tid - (NT - 64);
+      if (h >= 0 && h < TP) {
+        const int c = 2 * h;
+        float2 L[5], R[5];
+        #pragma unroll
+        for (int v = 0; v < 5; ++v) {
+          L[v] = *reinterpret_cast<const float2*>(&sm.sy[v][TJ][c]);
+          R[v] = *reinterpret_cast<const float2*>(&sm.sy_top[v][c]);
+        }
+        float2 F[5];
+        fx_ausm2<1>(fx_prim2(L[0], L[1], L[2], L[3], L[4]), fx_prim2(R[0], R[1], R[2], R[3], R[4]), P.A[1], F);
+        bool exa = true, exb = true;
+        if (!FULL) {
+          const int jf = j0 + TJ;
+          const bool ey = fx_face_exists(jf, g.nj, g.per_y) && (g.per_y || jf < g.nj);
+          exa = ey && k0 + c < g.nk;
+          exb = ey && k0 + c + 1 < g.nk;
+        }
+        #pragma unroll
+        for (int v = 0; v < 5; ++v) {
+          int2 q = fx_quant2(mul2(F[v], P.face_scale[v]), fmag);
+          if (!exa) q.x = 0;
+          if (!exb) q.y = 0;
+          *reinterpret_cast<int2*>(&sm.qy[v][TJ][c]) = q;
+        }
+      } else if (h >= 32 && h < 32 + TJ / 2) {
+        const int ja = h - 32, jb = ja + TJ / 2;
+        float2 L[5], R[5];
+        #pragma unroll
+        for (int v = 0; v < 5; ++v) {
+          L[v] = make_float2(sm.szp[v][ja][TP], sm.szp[v][jb][TP]);
+          R[v] = make_float2(sm.sz_top[v][ja], sm.sz_top[v][jb]);
+        }
+        float2 F[5];
+        fx_ausm2<2>(fx_prim2(L[0], L[1], L[2], L[3], L[4]), fx_prim2(R[0], R[1], R[2], R[3], R[4]), P.A[2], F);
+        bool exa = true, exb = true;
+        if (!FULL) {
+          const int kz = k0 + TK;
+          const bool ez = fx_face_exists(kz, g.nk, g.per_z) && (g.per_z || kz < g.nk);
+          exa = ez && j0 + ja < g.nj;
+          exb = ez && j0 + jb < g.nj;
+        }
+        #pragma unroll
+        for (int v = 0; v < 5; ++v) {
+          const int2 q = fx_quant2(mul2(F[v], P.face_scale[v]), fmag);
+          sm.qz[v][ja][TP].x = exa ? q.x : 0;
+          sm.qz[v][jb][TP].x = exb ? q.y : 0;
+        }
+      }
+    }
+    // x: face above cell i (between i and i+1), along the own column
+    int2 qx_hi[5];
+    {
+      float2 Sm[5], Sp[5];
+      const float* const r1 = ring_me + sp1 * SS;
+      const float* const r2 = ring_me + sp2 * SS;
+      #pragma unroll
+      for (int v = 0; v < 5; ++v) {
+        const float2 uc = RP(r1, v, 0, 0);
+        const float2 up = RP(r2, v, 0, 0);
+        const float2 b = sub2(up, uc);
+        const float2 s = fx_slope2(xb[v], b);
+        Sm[v] = fma2(s, v2(-0.5f), uc);
+        Sp[v] = fma2(s, v2(0.5f), uc);
         xb[v] = b;
       }
-      if (ex) {
-        float F[5];
-        fx_ausm<0>(xleft, fx_prim(Sm[0], Sm[1], Sm[2], Sm[3], Sm[4]), P.Ax, F);
-        #pragma unroll
-        for (int v = 0; v < 5; ++v) qx_hi[v] = fx_quant(F[v] * P.face_scale[v], fbad);
-      } else {
-        #pragma unroll
-        for (int v = 0; v < 5; ++v) qx_hi[v] = 0;
+      const bool ex = fx_face_exists(i + 1, g.ni, g.per_x);
+      float2 F[5];
+      fx_ausm2<0>(xleft, fx_prim2(Sm[0], Sm[1], Sm[2], Sm[3], Sm[4]), P.A[0], F);
+      xmag = FaceRange();
+      #pragma unroll
+      for (int v = 0; v < 5; ++v) {
+        qx_hi[v] = fx_quant2(mul2(F[v], P.face_scale[v]), xmag);
+        if (!ex || !own_a) qx_hi[v].x = 0;
+        if (!ex || !own_b) qx_hi[v].y = 0;
       }
-      xleft = fx_prim(Sp[0], Sp[1], Sp[2], Sp[3], Sp[4]);
+      fmag.add(xmag);
+      xleft = fx_prim2(Sp[0], Sp[1], Sp[2], Sp[3], Sp[4]);
     }
+    // faces of 2^30 quanta or more, or not finite, are errors; faces beyond
+    // the narrow bound make the plane sum its residuals in 64 bits
+    const float m = fmag.mag();
+    fbad |= !(m < kFxFaceLimit);
+    if (!(m < kFxNarrowFace)) sm.wide[par] = 1;
 
     __syncthreads();
 
-    // ---------------- residual and update of the own cell
+    // ---------------- C: residual and update of the own cells
     // f(n) of plane i has arrived (the staging copy may stay in flight)
     if (tma) {
       tbad |= !mbar_wait(&sm.bar[1], ph_un);
@@ -777,55 +882,99 @@ __device__ __forceinline__ void fx_stage_tile_impl(const FxArgs& a, const CUtens
     } else {
       fx_cp_async_wait<1>();
     }
-    if (own) {
-      const int c = i * njk + j * g.kp + k;       // 5*ni*nj*kp < 2^31 (host check)
-      const int ncv = (int)nc;
-      const bool act = a.active ? (a.active[c] != 0) : true;
-      int bad = 0;
-      int res[5];
-      #pragma unroll
-      for (int v = 0; v < 5; ++v)
-        res[v] = qx_lo[v] + sm.qy[v][ty][tx] + sm.qzL[v][ty][tx]
-               - (tx < TK - 1 ? sm.qzL[v][ty][tx + 1] : sm.qzT[v][z_warp<TK>(ty)][zt_slot<TK>(ty)])
-               - sm.qy[v][ty + 1][tx] - qx_hi[v];
-      if (a.wall.any && (i == 0 || i == g.ni - 1 || j == 0 || j == g.nj - 1 || k == 0 || k == g.nk - 1)) {
-        // the cell's state, re-read from the stage input: the ring slot of
-        // plane i receives plane i+3 below, with no barrier in between
-        float uc[5];
-        #pragma unroll
-        for (int v = 0; v < 5; ++v) uc[v] = fmaf(P.quantum[v], (float)a.in[v * ncv + c], P.base[v]);
-        add_wall_fluxes(a.wall, g.ni, g.nj, g.nk, g.per_x, g.per_y, g.per_z, i, j, k, uc, P.Ax, P.Ay, P.Az, res,
-                        [&](int v, float F) { return fx_quant(F * P.face_scale[v], fbad); });
+    if (own_a) {
+      const int c = i * njk + j * g.kp + ka;      // even: rows start on 16-byte boundaries
+      const bool wide = sm.wide[par] != 0;
+      bool act_a = true, act_b = own_b;
+      if (a.active) {
+        act_a = a.active[c] != 0;
+        act_b = act_b && a.active[c + 1] != 0;
       }
+      // patch-face fluxes: boundary cells of a patch with wall fluxes sum
+      // their residual in 64 bits together with the wall terms
+      const bool edge_ijk = a.wall.any && (i == 0 || i == g.ni - 1 || j == 0 || j == g.nj - 1);
+      const bool wall_a = a.wall.any && (edge_ijk || ka == 0 || ka == g.nk - 1);
+      const bool wall_b = own_b && a.wall.any && (edge_ijk || kb == g.nk - 1);
+      int2 o[5];
+      if (!wide && !wall_a && !wall_b) {
+        // every face of the plane below kFxNarrowFace: |residual| < 2^31
+        // fits int32, and |un + residual| < 3 * 2^30, so the wrapped 32-bit
+        // sum lies in (-2^30, 2^30) exactly when the true one does
+        #pragma unroll
+        for (int v = 0; v < 5; ++v) {
+          const int2 ylo = *reinterpret_cast<const int2*>(&sm.qy[v][ty][kk]);
+          const int2 yhi = *reinterpret_cast<const int2*>(&sm.qy[v][ty + 1][kk]);
+          const int2 zlo = sm.qz[v][ty][tp];
+          const int zhi = sm.qz[v][ty][tp + 1].x;
+          const int2 un = *reinterpret_cast<const int2*>(&sm.un[v][ty][kk]);
+          const unsigned ra = (unsigned)qx_lo[v].x - (unsigned)qx_hi[v].x + (unsigned)ylo.x - (unsigned)yhi.x +
+                              (unsigned)zlo.x - (unsigned)zlo.y;
+          const unsigned rb = (unsigned)qx_lo[v].y - (unsigned)qx_hi[v].y + (unsigned)ylo.y - (unsigned)yhi.y +
+                              (unsigned)zlo.y - (unsigned)zhi;
+          o[v].x = (int)((unsigned)un.x + ra);
+          o[v].y = (int)((unsigned)un.y + rb);
+        }
+      } else {
+        // 64-bit residuals: a face of the plane beyond the narrow bound, or
+        // a boundary cell with patch-face fluxes
+        long long ra[5], rb[5];
+        #pragma unroll
+        for (int v = 0; v < 5; ++v) {
+          const int2 ylo = *reinterpret_cast<const int2*>(&sm.qy[v][ty][kk]);
+          const int2 yhi = *reinterpret_cast<const int2*>(&sm.qy[v][ty + 1][kk]);
+          const int2 zlo = sm.qz[v][ty][tp];
+          const int zhi = sm.qz[v][ty][tp + 1].x;
+          ra[v] = (long long)qx_lo[v].x - qx_hi[v].x + ylo.x - yhi.x + zlo.x - zlo.y;
+          rb[v] = (long long)qx_lo[v].y - qx_hi[v].y + ylo.y - yhi.y + zlo.y - zhi;
+        }
+        FaceRange wmag;
+        #pragma unroll
+        for (int q = 0; q < 2; ++q) {
+          if (q == 0 ? !wall_a : !wall_b) continue;
+          // the cell's state, re-read from the stage input: the ring slot of
+          // plane i receives plane i+3 below, with no barrier in between
+          float uc[5];
+          #pragma unroll
+          for (int v = 0; v < 5; ++v) uc[v] = fmaf(P.quantum[v].x, (float)a.in[v * nc + c + q], P.base[v].x);
+          add_wall_fluxes(a.wall, g.ni, g.nj, g.nk, g.per_x, g.per_y, g.per_z, i, j, ka + q, uc, P.A[0].x, P.A[1].x,
+                          P.A[2].x, q == 0 ? ra : rb,
+                          [&](int v, float F) { return fx_quant1(F * P.face_scale[v].x, wmag); });
+        }
+        fbad |= !(wmag.mag() < kFxFaceLimit);
+        #pragma unroll
+        for (int v = 0; v < 5; ++v) {
+          const int2 un = *reinterpret_cast<const int2*>(&sm.un[v][ty][kk]);
+          const long long oa = (long long)un.x + ra[v], ob = (long long)un.y + rb[v];
+          // results outside the range are clamped to its edge and flagged below
+          o[v].x = (int)(oa >= kFxLimit ? kFxLimit : (oa <= -kFxLimit ? -kFxLimit : oa));
+          o[v].y = (int)(ob >= kFxLimit ? kFxLimit : (ob <= -kFxLimit ? -kFxLimit : ob));
+        }
+      }
+      int bad = 0;
       #pragma unroll
       for (int v = 0; v < 5; ++v) {
-        int32_t o;
-        if (act) {
-          const int r = res[v];
-          const int un = sm.un[v][ty][tx];
-          // |un| < 2^30 and |r| < 2^30 (face integers are bounded by the
-          // exact range of the update), so the int32 sum cannot overflow
-          const int on = un + r;
-          if (on >= kFxLimit || on <= -kFxLimit) {
-            bad |= 1;
-            if (a.err_info && atomicCAS(&a.err_info[0], ~0ull, (unsigned long long)c) == ~0ull) {
-              a.err_info[1] = (unsigned long long)v;
-              a.err_info[2] = (unsigned long long)__double_as_longlong((double)un);
-              a.err_info[3] = (unsigned long long)__double_as_longlong((double)r);
-            }
+        if (!act_a) o[v].x = a.in[v * nc + c];
+        if (!act_b) o[v].y = own_b ? a.in[v * nc + c + 1] : 0;
+        const bool ba = act_a && (o[v].x >= kFxLimit || o[v].x <= -kFxLimit);
+        const bool bb = act_b && (o[v].y >= kFxLimit || o[v].y <= -kFxLimit);
+        if (ba || bb) {
+          bad |= 1;
+          const int q = ba ? 0 : 1;
+          const int2 un = *reinterpret_cast<const int2*>(&sm.un[v][ty][kk]);
+          const int u = q == 0 ? un.x : un.y;
+          if (a.err_info && atomicCAS(&a.err_info[0], ~0ull, (unsigned long long)(c + q)) == ~0ull) {
+            a.err_info[1] = (unsigned long long)v;
+            a.err_info[2] = (unsigned long long)__double_as_longlong((double)u);
+            a.err_info[3] = (unsigned long long)__double_as_longlong((double)((long long)(q == 0 ? o[v].x : o[v].y) - u));
           }
-          o = on;
-        } else {
-          o = a.in[v * ncv + c];
         }
-        a.out[v * ncv + c] = o;
+        if (own_b) *reinterpret_cast<int2*>(a.out + v * nc + c) = o[v];
+        else a.out[v * nc + c] = o[v].x;
       }
       if (bad && a.err) atomicOr(a.err, bad);
     }
     #pragma unroll
-    for (int v = 0; v < 5; ++v) {
-      qx_lo[v] = qx_hi[v];
-    }
+    for (int v = 0; v < 5; ++v) qx_lo[v] = qx_hi[v];
 
     // ---------------- ring: plane i (last read before this iteration's
     // first barrier) gives its slot to plane i+3, dequantised from the
@@ -843,6 +992,7 @@ __device__ __forceinline__ void fx_stage_tile_impl(const FxArgs& a, const CUtens
     s0 = sp1;
     sp1 = sp2;
     sp2 = t;
+    par ^= 1;
   }
   if (fbad && a.err) atomicOr(a.err, 16);
   if (tbad && a.err) atomicOr(a.err, kFxErrTma);
@@ -856,13 +1006,6 @@ __device__ __forceinline__ void fx_stage_tile(const FxArgs& a, const CUtensorMap
   else fx_stage_tile_impl<TJ, TK, false>(a, tm_in, tm_un, j0, k0, i0, i1);
 }
 
-// Resident CTAs per SM the register allocation is sized for: three
-// 256-thread CTAs (80 registers, 55-58 KB shared memory each) measured 26 %
-// faster than two on the 256^3 patch.
-#ifndef DN_FX_MIN_BLOCKS
-#define DN_FX_MIN_BLOCKS 3
-#endif
-
 // Parameters of the single-patch launch: the stage arguments and the tensor
 // maps of the stage input and of f(n) (valid when tma != 0).
 struct FxLaunch {
@@ -872,9 +1015,9 @@ struct FxLaunch {
   int tma;
 };
 
-// One patch per launch: grid (k tiles, j tiles, i chunks).
+// One patch per launch: grid (k tiles, j tiles, i chunks), block (TK/2, TJ).
 template <int TJ, int TK>
-__global__ void __launch_bounds__(TJ * TK, DN_FX_MIN_BLOCKS)
+__global__ void __launch_bounds__(TJ * TK / 2, FxOccupancy<TJ * TK / 2>::min_blocks)
 fx_stage_kernel(const __grid_constant__ FxLaunch L)
 {
   const int i0 = blockIdx.z * L.a.g.i_chunk;

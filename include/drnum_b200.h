@@ -452,7 +452,12 @@ int dn_tma_patch_count(dn_ctx* ctx, int64_t* count);
  * host array; the call synchronises `stream` (a cudaStream_t, NULL = legacy
  * default stream).  All calls on a device share that array: calls that
  * overlap on the GPU race.  The first call on a device (with it current)
- * resolves the array's device address; make it before any stream capture. */
+ * resolves the array's device address; make it before any stream capture.
+ * That address is kept for the life of the process and is stale after a
+ * cudaDeviceReset of the device: do not call this on a device that was
+ * reset.  The field must be unpadded FP64 [5][ncells] (an FP64 context's
+ * buffers, DrNUM's host layout); the padded int32 fixed-point buffers of an
+ * FP32-bulk context cannot be passed. */
 int dn_field_sums_noalloc(const double* field, int64_t ncells, double dV, double out[5], void* stream);
 
 #ifdef __cplusplus

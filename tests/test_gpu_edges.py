@@ -153,3 +153,46 @@ def test_level_set_wall_outside_the_patch_changes_nothing(prec):
         it.close()
         outs.append(p.getField(0).copy())
     assert np.array_equal(outs[0], outs[1])
+
+
+def test_fp32_residual_sum_beyond_int32_is_reported():
+    """Six neighbours flow into one cell, advanced with an oversized step:
+    each of the cell's six mass faces stays below the per-face limit of 2^30
+    quanta, but their sum lies between 3 * 2^30 and 4 * 2^30, which an int32
+    sum would wrap back into the valid offset range.  The stage must report
+    that the offset left its range."""
+    import sys, os
+    sys.path.insert(0, os.path.join(os.path.dirname(__file__), "..", "oracle"))
+    import pyoracle
+    n, h, c = 8, 1.0 / 8, 4
+    U0 = np.zeros((5, n, n, n))
+    U0[0] = cases.RHO_INF
+    U0[4] = cases.P_INF / (cases.GAS_GAMMA - 1.0)
+    V = 0.3 * cases.A_INF
+    for ax in range(3):
+        for side in (-1, 1):
+            idx = [c, c, c]
+            idx[ax] += side
+            U0[1 + ax][tuple(idx)] = -side * V * cases.RHO_INF   # towards the centre cell
+            U0[4][tuple(idx)] += 0.5 * cases.RHO_INF * V * V
+    # mass change of the centre cell per unit dt of one forward-Euler stage (FP64 oracle)
+    dM = pyoracle.oracle_run(U0, h, 1.0, 1, alpha=(1.0,))[0, c, c, c] - U0[0, c, c, c]
+    assert dM > 0
+    base = U0.reshape(5, -1).mean(axis=1)
+    # momenta and energy get wide ranges: their faces stay far below the limits
+    scale = np.array([4 * cases.RHO_INF, 1e6, 1e6, 1e6, 1e12])
+    q0 = 2.0 ** np.ceil(np.log2(scale[0] / 2 ** 30))
+    dt = 3.5 * 2 ** 30 * q0 / dM               # the centre's mass update: 3.5 * 2^30 quanta
+    assert 3.5 * 2 ** 30 / 6 < 2 ** 30         # so no single (symmetric) face reaches the limit
+    p = CartesianPatch(n, n, n, spacing=(h, h, h))
+    p.setField(0, U0)
+    it = B200CartesianIterator(AusmPlus(), 0, DN_FP32)
+    it.addPatch(p)
+    it.setBase(0, base, scale)
+    it.updateDevice(fields=(0,))
+    with pytest.raises(DnError) as e:
+        it.rkStep(dt, (1.0,))
+        it.sync()
+    assert e.value.code == DN_ERR_RANGE
+    assert "offset left its range" in str(e.value)
+    it.close()

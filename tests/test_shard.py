@@ -380,3 +380,22 @@ def test_sharded_iterator_single_rank_nccl_equals_reference(golden_dir):
         it.close()
     finally:
         dist.destroy_process_group()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision", [_lib.DN_FP64, _lib.DN_FP32])
+def test_rank_without_owned_patches_steps_without_error(precision):
+    # a rank whose share of the grid is empty (more ranks than patches): the
+    # batched step has no work item and launches no stage kernel (the
+    # patches are shadows, filled only by the exchange)
+    from test_gpu_grid import make_grid
+    it, objs, _, dt, _ = make_grid("octants_jet", precision)
+    lib = _lib.load()
+    for p in range(len(objs)):
+        assert lib.dn_patch_set_owned(it.ctx, p, 0) == _lib.DN_OK
+    l0 = it.launchCount()
+    it.rkStep(dt, cases.RK3_ALPHA)
+    it.sync()
+    # at most the donor copies of the step (one per copy, nothing to receive)
+    assert it.launchCount() - l0 <= 1 + 2 * len(cases.RK3_ALPHA)
+    it.close()
