@@ -280,11 +280,38 @@ def uniform_state(patches, mach=0.5, p=P_INF, T=T_INF):
 
 # ------------------------------------------------------- benchmark workloads
 
-def jet_grid(nf=(288, 144, 144), overlap=3):
-    """Dual-resolution jet workload: the octant grid with a core of nf cells
-    at h = 1 / (2 nf[0]) (the box is [0, 1] x [0, nf1/nf0] x [0, nf2/nf0])
-    and seven octants at 2h, `overlap` cells across each interface."""
-    return octant_grid(nf=nf, h=1.0 / (2 * nf[0]), overlap=overlap, seek=2)
+def jet_grid(core=(192, 96, 96), box=(128, 256, 256), overlap=3, seek=2):
+    """Dual-resolution jet workload: a core patch of `core` cells at spacing
+    h and seven patches at 2h around it.  The seven tile a box of `box`
+    cells at 2h (x length 1, so h = 1 / (2 box[0])): 2 x 2 x 2 blocks split
+    at half the box on each axis, the two blocks of the upper (y, z) quadrant
+    merged along x, so every side spans box/2 or box cells.  The core starts
+    at the box's x-min face, centred in y and z, where the jet enters; it is
+    nested in the coarse patches and receives data in `seek` layers on its
+    five other faces.  Coarse patches reach `overlap` of their own cells
+    across each interface between them, with `seek` layers there; the box
+    faces carry none."""
+    H = 1.0 / box[0]                 # coarse spacing 2h
+    h = 0.5 * H
+    half = [box[a] // 2 for a in range(3)]
+    cy, cz = 0.5 * box[1] * H, 0.5 * box[2] * H
+    patches = [dict(n=tuple(core), origin=(0.0, cy - 0.5 * core[1] * h, cz - 0.5 * core[2] * h),
+                    length=tuple(core[a] * h for a in range(3)), seek=(0, seek, seek, seek, seek, seek))]
+    for b in range(2):
+        for c in range(2):
+            xs = [(0, box[0])] if (b, c) == (1, 1) else [(0, half[0]), (half[0], box[0])]
+            for x0, x1 in xs:
+                lo = [x0, b * half[1], c * half[2]]
+                hi = [x1, (b + 1) * half[1], (c + 1) * half[2]]
+                n, origin, sk = [], [], []
+                for a in range(3):
+                    lo_in, hi_in = lo[a] > 0, hi[a] < box[a]
+                    n.append(hi[a] - lo[a] + overlap * (int(lo_in) + int(hi_in)))
+                    origin.append((lo[a] - (overlap if lo_in else 0)) * H)
+                    sk += [seek if lo_in else 0, seek if hi_in else 0]
+                patches.append(dict(n=tuple(n), origin=tuple(origin), length=tuple(n[a] * H for a in range(3)),
+                                    seek=tuple(sk)))
+    return patches
 
 
 def sphere_group(n=(256, 128, 128), L=1.0, overlap=3):
@@ -300,16 +327,16 @@ def sphere_group(n=(256, 128, 128), L=1.0, overlap=3):
     return [a, b]
 
 
-def tiled_grid(slots=(8, 8, 8), extent=(8, 40), h=1.0 / 256, overlap=2, seed=42):
+def tiled_grid(slots=(8, 8, 8), extent=(16, 96), h=1.0 / 256, overlap=2, seed=42):
     """Uneven batched workload: a box of slots[0] x slots[1] x slots[2]
     patches.  The extent of each slot row along each axis is drawn uniformly
-    from `extent` coarse cells (seed); patches alternate between refinement 1
-    (spacing 2h) and refinement 2 (spacing h) in a checkerboard, so cell
-    counts per axis range over 8..80 plus the overlap.  Every patch reaches
-    `overlap` of its own cells across each interior interface, with 2 seek
-    layers there."""
+    from the even numbers of `extent` cells of spacing h (seed); patches
+    alternate between refinement 2 (spacing h: the drawn count of cells) and
+    refinement 1 (spacing 2h: half of it) in a checkerboard.  Every patch
+    reaches `overlap` of its own cells across each interior interface, with
+    2 seek layers there."""
     rng = np.random.default_rng(seed)
-    ext = [rng.integers(extent[0], extent[1] + 1, slots[a]) for a in range(3)]
+    ext = [rng.integers(extent[0] // 2, extent[1] // 2 + 1, slots[a]) for a in range(3)]   # in cells of 2h
     H = 2.0 * h
     starts = [np.concatenate(([0], np.cumsum(ext[a])[:-1])) * H for a in range(3)]
     patches = []

@@ -1,15 +1,18 @@
 """The multi-patch benchmark workloads, built through the reference-style API.
 
-    jet     dual-resolution jet: core patch at h, seven octant patches at 2h,
-            3-cell overlaps, Mach 0.8 top-hat jet (radius 0.05, seeded 1e-3
-            white noise) on the core's x-min face, far field at rest elsewhere
+    jet     dual-resolution jet: a 192 x 96 x 96 core patch at h nested at the
+            inlet of a box tiled by seven patches at 2h (64 to 128 cells per
+            axis), 3-cell overlaps, Mach 0.8 top-hat jet (radius 0.05, seeded
+            1e-3 white noise) on the core's x-min face, far field at rest
+            elsewhere
     sphere  level-set wall: 256 x 128 x 128 cells over [0, 2] x [0, 1]^2 in two
             overlapping patches, free stream at Mach 0.5, a sphere of radius
             0.08 at (0.3, 0.5, 0.5) as an FP32 signed-distance field with the
             slip-wall mirror condition (3 inner layers, min_inner_rel_dist 0.1)
-    tiled   uneven batched grid: 8 x 8 x 8 patches with seeded per-axis extents,
-            refinement 1 and 2 in a checkerboard, 2-cell overlaps, one seeded
-            isentropic vortex per patch on a Mach 0.4 stream, far field outside
+    tiled   uneven batched grid: 8 x 8 x 8 patches with per-axis extents drawn
+            from U{16..96} (seeded), refinement 1 and 2 in a checkerboard,
+            2-cell overlaps, one seeded isentropic vortex per patch on a Mach
+            0.4 stream, far field outside
 
 Every state is synthetic and seeded; the reference ships no cases.
 """
@@ -28,14 +31,17 @@ def build(name, scale=1.0):
     """Returns dict(patches, states, bcs, levelset, dt, description).
     scale < 1 shrinks the case (for tests)."""
     if name == "jet":
-        nf = tuple(max(8, int(round(x * scale)) // 2 * 2) for x in (288, 144, 144))
-        patches = cases.jet_grid(nf=nf)
+        core = tuple(max(8, int(round(x * scale)) // 4 * 4) for x in (192, 96, 96))
+        box = tuple(max(16, int(round(x * scale)) // 4 * 4) for x in (128, 256, 256))
+        patches = cases.jet_grid(core=core, box=box)
         states = cases.uniform_state(patches, mach=0.0)
         bcs = cases.jet_bcs(patches, radius=0.05, noise=1e-3, seed=1234)
-        h = 1.0 / (2 * nf[0])
+        h = 0.5 / box[0]
         dt = 0.5 * h / ((0.8 + 1.0) * cases.A_INF)
-        desc = (f"dual-resolution jet: core {patches[0]['n']} at h=1/{2 * nf[0]}, 7 octant patches at 2h, "
-                "3-cell overlaps, Mach 0.8 top-hat jet r=0.05 + 1e-3 seeded noise, far field at rest")
+        desc = (f"dual-resolution jet: 8 overlapping patches, core {core[0]}x{core[1]}x{core[2]} at h=1/{2 * box[0]} "
+                f"nested at the inlet of a {box[0]}x{box[1]}x{box[2]}-cell box at 2h tiled by seven patches of "
+                f"{box[0] // 2}-{box[0]} cells per axis, 3-cell overlaps, Mach 0.8 top-hat jet r=0.05 + 1e-3 seeded "
+                "noise, far field at rest")
         return dict(patches=patches, states=states, bcs=bcs, levelset=None, dt=dt, description=desc)
     if name == "sphere":
         n = tuple(max(16, int(round(x * scale)) // 2 * 2) for x in (256, 128, 128))
@@ -57,8 +63,11 @@ def build(name, scale=1.0):
         bcs = cases.outer_farfield_bcs(patches, ff)
         h = min(min(p["length"][a] / p["n"][a] for a in range(3)) for p in patches)
         dt = 0.4 * h / (1.6 * cases.A_INF)
-        desc = (f"uneven batched grid: {len(patches)} patches, seeded extents, refinement 1 and 2, 2-cell overlaps, "
-                "one seeded vortex (beta 3-6, radius 4 coarse cells) per patch superposed on Mach 0.4 flow, far field outside")
+        cells = sum(int(np.prod(p["n"])) for p in patches)
+        desc = (f"uneven batched grid: {len(patches)} patches ({cells / 1e6:.1f} M cells), per-axis extents drawn "
+                "from U{16..96} (seed 42), half at refinement 1 and half at refinement 2, tiled box with 2-cell "
+                "overlaps, one seeded isentropic vortex (strength 3-6, radius 4 coarse cells) per patch on Mach 0.4 "
+                "flow, far field outside")
         return dict(patches=patches, states=states, bcs=bcs, levelset=None, dt=dt, description=desc)
     raise KeyError(name)
 

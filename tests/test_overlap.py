@@ -225,3 +225,48 @@ def test_overlap_setup_result_independent_of_thread_count(monkeypatch):
     for a, b in zip(one, many):
         for k in TABLE_KEYS:
             assert _same(a[k], b[k]), k
+
+
+# ------------------------------------------------- full-size benchmark layouts
+
+@pytest.mark.skipif(not pyoracle.ref_available(), reason="compiled reference (oracle/_ref) not built")
+def test_levelset_classification_full_size_sphere_group_equals_reference():
+    # the level-set wall workload at its stated size: 256 x 128 x 128 cells in
+    # two overlapping patches, sphere r = 0.08 at (0.3, 0.5, 0.5) as an FP32
+    # distance field, 3 inner layers, min_inner_rel_dist 0.1: cell lists,
+    # distances, gradients, mirror donors and weights bit for bit
+    from drnum_b200 import workloads
+    case = workloads.build("sphere")
+    G, ni, no, mr = case["levelset"]
+    assert [p["n"] for p in case["patches"]] == [(131, 128, 128), (131, 128, 128)]
+    ref = pyoracle.RefGrid(case["patches"], num_vars=6)
+    ref.levelset(G, ni, no, mr)
+    total = 0
+    for p, patch in enumerate(case["patches"]):
+        mine = classify(patch, G[p], ni, no, mr)
+        for layer in range(ni):
+            r = ref.levelset_layer(p, 1, layer)
+            m = mine["inner"][layer]
+            total += len(m["cells"])
+            for k in LS_KEYS:
+                assert _same(m[k], r[k]), (p, layer, k)
+    assert total > 1000
+    ref.close()
+
+
+@pytest.mark.skipif(not pyoracle.ref_available(), reason="compiled reference (oracle/_ref) not built")
+@pytest.mark.parametrize("name", ["jet", "tiled"])
+def test_donor_tables_full_size_workloads_equal_reference(name):
+    # the donor tables of the dual-resolution jet (8 patches, 10.9 M cells)
+    # and of the 512-patch uneven grid (69.8 M cells) at their stated sizes,
+    # against the reference's PatchGrid::computeDependencies, bit for bit
+    from drnum_b200 import workloads
+    patches = workloads.build(name)["patches"]
+    mine, nd = build_tables(patches)
+    assert nd == 0
+    ref = pyoracle.RefGrid(patches, 0, threads=0)
+    for p in range(len(patches)):
+        t = ref.tables(p)
+        for k in TABLE_KEYS:
+            assert _same(mine[p][k], t[k]), (name, p, k)
+    ref.close()

@@ -18,11 +18,31 @@ def test_workload_layouts_have_donors_for_every_seek_cell(name):
 
 
 def test_tiled_workload_full_size_layout():
+    # 512 patches; per-axis extents drawn from the even numbers of 16..96
+    # cells at the fine spacing (refinement 2), half as many at refinement 1
     patches = cases.tiled_grid()
     cells = sum(int(np.prod(p["n"])) for p in patches)
-    assert len(patches) == 512 and 35e6 < cells < 50e6
+    assert len(patches) == 512 and 60e6 < cells < 80e6
     assert {p["refinement"] for p in patches} == {1, 2}
-    assert min(min(p["n"]) for p in patches) >= 8
+    for p in patches:
+        inner = [p["n"][a] - 2 * ((p["seek"][2 * a] > 0) + (p["seek"][2 * a + 1] > 0)) for a in range(3)]
+        for x in inner:
+            assert 16 <= x * (3 - p["refinement"]) <= 96 and x * (3 - p["refinement"]) % 2 == 0, (p, x)
+
+
+def test_jet_workload_full_size_layout():
+    # core 192 x 96 x 96 at h; seven patches at 2h of 64..128 cells per axis
+    # (plus their 3-cell overlaps)
+    patches = workloads.build("jet")["patches"]
+    assert len(patches) == 8 and patches[0]["n"] == (192, 96, 96)
+    h = patches[0]["length"][0] / 192
+    for p in patches[1:]:
+        assert abs(p["length"][0] / p["n"][0] - 2 * h) < 1e-15
+        for a in range(3):
+            inner = p["n"][a] - 3 * ((p["seek"][2 * a] > 0) + (p["seek"][2 * a + 1] > 0))
+            assert 64 <= inner <= 128, p
+    cells = sum(int(np.prod(p["n"])) for p in patches)
+    assert 10e6 < cells < 13e6
 
 
 @pytest.mark.gpu
