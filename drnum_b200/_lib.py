@@ -84,6 +84,10 @@ SIGNATURES = {
     "dn_patch_set_active": (c_int, [c_void_p, c_int, POINTER(c_uint8)]),
     "dn_copy_field": (c_int, [c_void_p, c_int, c_int]),
     "dn_compute": (c_int, [c_void_p, c_double]),
+    "dn_compute_patches": (c_int, [c_void_p, c_double, c_void_p, c_int]),
+    "dn_patch_activate": (c_int, [c_void_p, c_int, c_int]),
+    "dn_patch_set_levelset_layers": (c_int, [c_void_p, c_int, c_int, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p,
+                                             c_void_p]),
     "dn_rk_step": (c_int, [c_void_p, c_double, POINTER(c_double), c_int]),
     "dn_sync": (c_int, [c_void_p]),
     "dn_conservation_sums": (c_int, [c_void_p, POINTER(c_double)]),

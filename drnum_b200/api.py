@@ -317,14 +317,22 @@ class B200CartesianIterator:
         return self.m_Patches[i]
 
     def activatePatch(self, i):
+        """PatchIterator::activatePatch (patchiterator.h:119-125)."""
+        if not 0 <= i < len(self.m_Patches):
+            raise IndexError(i)
+        check(self.ctx, self.lib.dn_patch_activate(self.ctx, i, 1))
         self.m_PatchActive[i] = True
 
     def deactivatePatch(self, i):
+        """PatchIterator::deactivatePatch (patchiterator.h:127-133): the patch
+        keeps its state through later stages (dn_patch_activate)."""
         if not 0 <= i < len(self.m_Patches):
             raise IndexError(i)
+        check(self.ctx, self.lib.dn_patch_activate(self.ctx, i, 0))
         self.m_PatchActive[i] = False
-        if not all(self.m_PatchActive):
-            raise NotImplementedError("per-patch deactivation is not supported by the fused path")
+
+    def patchActive(self, i):
+        return self.m_PatchActive[i]
 
     def setBase(self, i_patch, base, scale):
         b = np.ascontiguousarray(base, dtype=np.float64)
@@ -416,9 +424,14 @@ class B200CartesianIterator:
         check(self.ctx, self.lib.dn_copy_field(self.ctx, i_src, i_dst))
 
     def compute(self, factor, patches=None):
-        if patches is not None and list(patches) != list(range(len(self.m_Patches))):
-            raise NotImplementedError("the fused path computes all patches of the iterator")
-        check(self.ctx, self.lib.dn_compute(self.ctx, float(factor)))
+        """PatchIterator::compute(factor, patches) (patchiterator.h:50): one
+        stage of the listed patches (all when None); the others keep their
+        state."""
+        if patches is None or list(patches) == list(range(len(self.m_Patches))):
+            check(self.ctx, self.lib.dn_compute(self.ctx, float(factor)))
+            return
+        ids = np.ascontiguousarray(list(patches), dtype=np.int32)
+        check(self.ctx, self.lib.dn_compute_patches(self.ctx, float(factor), ids.ctypes.data, len(ids)))
 
     def computeAll(self, factor):
         self.compute(factor)

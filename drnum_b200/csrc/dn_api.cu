@@ -53,6 +53,7 @@ struct DnPatch {
   bool base_set = false;
   dn::WallBC wall{};                        // device view (table pointers are device memory)
   bool owned = true;                        // false: a shadow of a patch another rank advances
+  bool patch_active = true;                 // false: left out of stages, its state carried over
 };
 
 // Device offset of cell index c = (i*nj + j)*nk + k in the patch's rows of kp elements.
@@ -890,7 +891,7 @@ int build_batch(dn_ctx* c)
     r.wall = P.wall;
     int tj, tk;
     dn::shape_tile(fp64, c->shape[q], &tj, &tk);
-    if (P.owned) tiles += (long)((P.d.nj + tj - 1) / tj) * ((P.d.nk + tk - 1) / tk);
+    if (P.owned && P.patch_active) tiles += (long)((P.d.nj + tj - 1) / tj) * ((P.d.nk + tk - 1) / tk);
     r.tma = 1;
     if (!fp64) {
       dn::FxGeom g{};
@@ -915,7 +916,7 @@ int build_batch(dn_ctx* c)
   std::vector<dn::WorkItem> items[dn::kNumShapes];
   for (size_t q = 0; q < np; ++q) {
     const DnPatch& P = c->patches[q];
-    if (!P.owned) continue;
+    if (!P.owned || !P.patch_active) continue;
     const int sh = c->shape[q];
     int tj, tk;
     dn::shape_tile(fp64, sh, &tj, &tk);
@@ -955,23 +956,36 @@ int build_batch(dn_ctx* c)
 
 int stage_patch(dn_ctx* c, DnPatch& p, int in_b, int un_b, int out_b, double factor);
 
-// One RK stage of every patch: in_b -> out_b with step-start state un_b.
+// An inactive (or unlisted) patch's state carried from buffer in_b into out_b.
+int carry_patch(dn_ctx* c, DnPatch& p, int in_b, int out_b)
+{
+  if (in_b == out_b) return DN_OK;
+  cudaError_t e = cudaMemcpyAsync(p.buf[out_b], p.buf[in_b], 5 * p.ncp * elem_size(c), cudaMemcpyDeviceToDevice,
+                                  c->stream);
+  return e == cudaSuccess ? DN_OK : cuda_fail(c, e, "inactive patch copy");
+}
+
+// One RK stage of every active patch: in_b -> out_b with step-start state
+// un_b; inactive patches carry their state into out_b.
 int stage_all(dn_ctx* c, int in_b, int un_b, int out_b, double factor)
 {
   NvtxRange nvtx("dn stage");
+  int s;
+  for (auto& p : c->patches) {
+    if (p.owned && !p.patch_active && (s = carry_patch(c, p, in_b, out_b))) return s;
+  }
   // a single patch keeps its parameters in the kernel's constant bank (the
   // batched form reads them from shared memory); the results are identical.
   // Flux functors (another scheme or a user stage function) run per patch.
   const bool functor = c->precision == DN_FP64 && (c->scheme != DN_FLUX_AUSMPLUS || c->stage_fn);
   if (!c->batched || c->patches.size() == 1 || functor) {
     for (auto& p : c->patches) {
-      if (!p.owned) continue;
-      int s = stage_patch(c, p, in_b, un_b, out_b, factor);
+      if (!p.owned || !p.patch_active) continue;
+      s = stage_patch(c, p, in_b, un_b, out_b, factor);
       if (s) return s;
     }
     return DN_OK;
   }
-  int s;
   if (c->batch_dirty && (s = build_batch(c))) return s;
   for (int q = 0; q < dn::kNumShapes; ++q) {
     if (!c->n_items[q]) continue;
@@ -1481,6 +1495,43 @@ int dn_compute(dn_ctx* c, double factor)
   return DN_OK;
 }
 
+int dn_compute_patches(dn_ctx* c, double factor, const int32_t* ids, int n)
+{
+  if (!c) return DN_ERR_ARG;
+  if (n < 0 || (n > 0 && !ids)) return fail(c, DN_ERR_ARG, "invalid patch list");
+  if (!std::isfinite(factor)) return fail(c, DN_ERR_ARG, "factor is not finite");
+  std::vector<char> listed(c->patches.size(), 0);
+  for (int q = 0; q < n; ++q) {
+    if (ids[q] < 0 || ids[q] >= (int)c->patches.size()) return fail(c, DN_ERR_ARG, "invalid patch id %d", ids[q]);
+    if (listed[ids[q]]) return fail(c, DN_ERR_ARG, "patch %d listed twice", ids[q]);
+    listed[ids[q]] = 1;
+  }
+  if (set_device(c) != DN_OK) return DN_ERR_CUDA;
+  NvtxRange nvtx("dn stage (patch list)");
+  const int in_b = c->fmap[0], un_b = c->fmap[1], out_b = c->fmap[2];
+  int s;
+  for (size_t q = 0; q < c->patches.size(); ++q) {
+    DnPatch& p = c->patches[q];
+    if (!p.owned) continue;
+    s = (listed[q] && p.patch_active) ? stage_patch(c, p, in_b, un_b, out_b, factor) : carry_patch(c, p, in_b, out_b);
+    if (s) return s;
+  }
+  std::swap(c->fmap[0], c->fmap[2]);
+  return DN_OK;
+}
+
+int dn_patch_activate(dn_ctx* c, int id, int active)
+{
+  int s = check_patch(c, id);
+  if (s) return s;
+  if (c->patches[id].patch_active != (active != 0)) {
+    c->patches[id].patch_active = active != 0;
+    c->batch_dirty = true;
+    c->generation++;
+  }
+  return DN_OK;
+}
+
 int dn_rk_step(dn_ctx* c, double dt, const double* alpha, int n_alpha)
 {
   if (!c) return DN_ERR_ARG;
@@ -1825,6 +1876,46 @@ int dn_patch_set_levelset(dn_ctx* c, int id, const double* G, int num_inner_laye
     return fail(c, DN_ERR_ARG, "%s", err.c_str());
   c->ls[id] = std::move(L);
   c->ls_on[id] = 1;
+  c->ls_dirty = true;
+  c->generation++;
+  return DN_OK;
+}
+
+int dn_patch_set_levelset_layers(dn_ctx* c, int id, int num_inner_layers, const int64_t* counts,
+                                 const uint64_t* cells, const double* g, const double* grad, const uint64_t* donors,
+                                 const double* weights)
+{
+  int s = check_patch(c, id);
+  if (s) return s;
+  if (num_inner_layers < 0 || (num_inner_layers > 0 && !counts)) return fail(c, DN_ERR_ARG, "invalid layer counts");
+  int64_t total = 0;
+  for (int l = 0; l < num_inner_layers; ++l) {
+    if (counts[l] < 0) return fail(c, DN_ERR_ARG, "negative layer count");
+    total += counts[l];
+  }
+  if (total > 0 && !(cells && g && grad && donors && weights)) return fail(c, DN_ERR_ARG, "layer arrays missing");
+  const uint64_t nc = c->patches[id].nc;
+  dn::LevelSetLayers L;
+  L.inner.resize(num_inner_layers);
+  int64_t q = 0;
+  for (int l = 0; l < num_inner_layers; ++l) {
+    for (int64_t e = 0; e < counts[l]; ++e, ++q) {
+      dn::LayerCell lc;
+      lc.cell = cells[q];
+      lc.g = g[q];
+      for (int a = 0; a < 3; ++a) lc.grad[a] = grad[3 * q + a];
+      for (int t = 0; t < 8; ++t) {
+        lc.donor[t] = donors[8 * q + t];
+        lc.weight[t] = weights[8 * q + t];
+        if (lc.donor[t] >= nc) return fail(c, DN_ERR_ARG, "mirror donor %llu outside patch %d",
+                                           (unsigned long long)lc.donor[t], id);
+      }
+      if (lc.cell >= nc) return fail(c, DN_ERR_ARG, "layer cell %llu outside patch %d", (unsigned long long)lc.cell, id);
+      L.inner[l].push_back(lc);
+    }
+  }
+  c->ls[id] = std::move(L);
+  c->ls_on[id] = num_inner_layers > 0 ? 1 : 0;
   c->ls_dirty = true;
   c->generation++;
   return DN_OK;

@@ -16,8 +16,10 @@
  *     (patchiterator.h:43-44, gpu_patchiterator.h:106-126)   dn_patch_download[_f32]
  *   Patch::deactivate / m_Active (patch_common.h:502-504)    dn_patch_set_active
  *   PatchIterator::copyField (patchiterator.h:97-103)        dn_copy_field
- *   PatchIterator::computeAll / compute                      dn_compute
- *     (patchiterator.h:80-87, gpu_cartesianiterator.h:218-304)
+ *   PatchIterator::computeAll / compute                      dn_compute, dn_compute_patches
+ *     (patchiterator.h:50,80-87, gpu_cartesianiterator.h:218-304)
+ *   PatchIterator::activatePatch / deactivatePatch           dn_patch_activate
+ *     (patchiterator.h:56-57,119-133)
  *   RungeKutta::operator()(dt) (rungekutta.cpp:27-42)        dn_rk_step
  *   Patch::computeVariableDifference (patch.cpp:733-746)     dn_field_difference
  *   the applications' CFL / density diagnostics              dn_flow_stats
@@ -171,6 +173,24 @@ int dn_copy_field(dn_ctx* ctx, int i_src, int i_dst);
  * (patchiterator.h:80-87, gpu_cartesianiterator.h:218-304). */
 int dn_compute(dn_ctx* ctx, double factor);
 
+/* One RK stage of the listed patches only (ids, n of them; each once),
+ * skipping inactive ones: every other patch keeps its field 0 (the stage's
+ * output buffer receives a copy of its input).  DN_ERR_ARG for an id out of
+ * range or listed twice.
+ * Replaces: PatchIterator::compute(factor, patches) (patchiterator.h:50;
+ * the reference's CPU iterator, cartesianiterator.h:87-93, walks the list). */
+int dn_compute_patches(dn_ctx* ctx, double factor, const int32_t* patches, int n);
+
+/* Takes a patch out of (active = 0) or back into (1) every later stage of
+ * dn_compute, dn_compute_patches and dn_rk_step: an inactive patch keeps
+ * its state (its output buffers receive copies of the input), while donor
+ * copies and the level-set wall still write its receiving cells, as the
+ * reference's copyDonorData does for every patch.  Patches start active.
+ * Replaces: PatchIterator::activatePatch / deactivatePatch
+ * (patchiterator.h:56-57,119-133), read by the stage loop of
+ * GPU_CartesianIterator::compute (gpu_cartesianiterator.h:226). */
+int dn_patch_activate(dn_ctx* ctx, int patch, int active);
+
 /* One full low-storage RK time step with stage factors alpha[0..n-1]*dt,
  * without the field 0 -> 1 copy (field 1 holds the step-start state after
  * the call, as after the reference's step).  With donor tables it runs the
@@ -267,6 +287,18 @@ int dn_copy_donor_data(dn_ctx* ctx, int field);
  * lsobccompressibleeulerop.h:49-144). */
 int dn_patch_set_levelset(dn_ctx* ctx, int patch_id, const double* G, int num_inner_layers,
                           int num_outer_layers, double min_inner_rel_dist);
+
+/* A patch's level-set wall from layers classified elsewhere (for example by
+ * the reference's LevelSetObject::extractBCellLayers): num_inner_layers inner
+ * (G < 0) layers of counts[layer] cells, concatenated in layer order: cell
+ * index, G, normalised gradient [n][3], mirror-point donors and weights
+ * [n][8] (the layout of dn_patch_levelset_get).  From then on the slip-wall
+ * mirror condition runs on them as after dn_patch_set_levelset.
+ * Replaces: LevelSetObjectBC::transferCellLayerData (levelsetobjectbc.cpp:38-134)
+ * reading LevelSetObject::getInnerCellsLayers (levelsetobject.h:128). */
+int dn_patch_set_levelset_layers(dn_ctx* ctx, int patch_id, int num_inner_layers, const int64_t* counts,
+                                 const uint64_t* cells, const double* g, const double* grad, const uint64_t* donors,
+                                 const double* weights);
 
 /* Size and contents of one layer of a patch's level-set classification
  * (inner = 1: G < 0 layers, 0: outer layers), in the reference's order:

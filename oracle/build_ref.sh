@@ -42,6 +42,39 @@ $CXX $FLAGS -c "$HERE/ref_driver.cpp" -o "$OUT/obj/ref_driver.o"
 $CXX -shared -o "$OUT/libdrnum_ref.so" $OBJS "$OUT/obj/ref_driver.o" -L/usr/lib/gcc/x86_64-linux-gnu/13 -lgomp -lpthread
 echo "built $OUT/libdrnum_ref.so"
 
+# The reference in its shipped precision (drnum.h:43 defines
+# DRNUM_SINGLE_PRECISION: `real` is float), unchanged header, for the
+# like-for-like CPU baseline of the FP32-bulk path (timing sessions only).
+FLAGS32="-O2 -std=c++14 -fPIC -fpermissive -w -fopenmp -DOPEN_MP -ffp-contract=off
+         -I$HERE/ref_stubs -I- -I$HERE/ref_stubs -I$LIB -I$LIB/math -I$LIB/iterators
+         -I$LIB/fluxes -I$LIB/reconstruction"
+mkdir -p "$OUT/obj32"
+OBJS32=""
+pids=""
+for s in $SRCS; do
+  o="$OUT/obj32/$(echo "$s" | tr '/' '_' | sed 's/\.cpp$/.o/')"
+  OBJS32="$OBJS32 $o"
+  $CXX $FLAGS32 -c "$LIB/$s" -o "$o" &
+  pids="$pids $!"
+done
+for p in $pids; do wait $p; done
+$CXX $FLAGS32 -c "$HERE/ref_driver.cpp" -o "$OUT/obj32/ref_driver.o"
+$CXX -shared -o "$OUT/libdrnum_ref_f32.so" $OBJS32 "$OUT/obj32/ref_driver.o" -L/usr/lib/gcc/x86_64-linux-gnu/13 \
+     -lgomp -lpthread
+echo "built $OUT/libdrnum_ref_f32.so"
+
+# A DrNUM application driving drnum_b200 through the C++ binding
+# include/drnum_b200_iterator.h: the reference's own RungeKutta and PatchGrid
+# (from libdrnum_ref.so) over the product library (built first by
+# drnum_b200/build.py).
+B200="$HERE/../drnum_b200"
+if [ -f "$B200/libdrnum_b200.so" ]; then
+  $CXX $FLAGS -I"$HERE/../include" -c "$HERE/ref_app_b200.cpp" -o "$OUT/obj/ref_app_b200.o"
+  $CXX -shared -o "$OUT/libdrnum_refapp.so" "$OUT/obj/ref_app_b200.o" -L"$OUT" -ldrnum_ref -L"$B200" -ldrnum_b200 \
+       -Wl,-rpath,'$ORIGIN' -Wl,-rpath,'$ORIGIN/../../drnum_b200' -L/usr/lib/gcc/x86_64-linux-gnu/13 -lgomp -lpthread
+  echo "built $OUT/libdrnum_refapp.so"
+fi
+
 # The reference's flux functors compiled for the device (sm_100a) against this
 # repository's generic functor stage.  nvcc has no -I- split, so the headers
 # are reached through a tree of symbolic links to the reference's files in

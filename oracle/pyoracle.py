@@ -328,6 +328,14 @@ class RefGrid:
         if self.lib.dnref_grid_copy_donor_data(self.h, field) != 0:
             raise RuntimeError("copy_donor_data failed")
 
+    def deactivate(self, p, inactive=True):
+        """Patch p left out of the following runs' stages (the iterator's
+        deactivatePatch, iterators/patchiterator.h:127-133)."""
+        self.lib.dnref_grid_deactivate.restype = c_int
+        self.lib.dnref_grid_deactivate.argtypes = [c_void_p, c_int, c_int]
+        if self.lib.dnref_grid_deactivate(self.h, int(p), int(bool(inactive))) != 0:
+            raise RuntimeError("deactivate failed")
+
     def run(self, steps, dt, alpha=(0.25, 0.5, 1.0), scheme=0):
         al = np.ascontiguousarray(alpha, dtype=np.float64)
         sec = c_double()

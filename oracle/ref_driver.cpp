@@ -358,10 +358,12 @@ struct DnRefSession
   size_t G[3];
 };
 
+// The state is converted to `real` cell by cell, so a session also runs in
+// the reference's single-precision build (libdrnum_ref_f32.so).
 void* dnref_session_create(int ni, int nj, int nk, const int* periodic, double hx, double hy, double hz,
                            const double* init, const double* alpha, int n_alpha, int threads)
 {
-  if (sizeof(real) != 8 || ni < 1 || nj < 1 || nk < 1 || n_alpha < 1) return nullptr;
+  if (ni < 1 || nj < 1 || nk < 1 || n_alpha < 1) return nullptr;
 #ifdef OPEN_MP
   if (threads > 0) omp_set_num_threads(threads);
 #endif
@@ -434,6 +436,7 @@ struct DnRefGrid
   GridBC bc;
   LevelSetObject* lso = nullptr;
   CPU_LevelSetObjectBC<LSOBCCompressibleEulerOp>* lsbc = nullptr;
+  std::vector<char> inactive;   // patches the runs deactivate (PatchIterator::deactivatePatch)
 };
 
 // n[3*np], origin[3*np], length[3*np], seek[6*np] (imin imax jmin jmax kmin kmax)
@@ -657,6 +660,7 @@ int grid_run_impl(DnRefGrid* g, int steps, double dt, const double* alpha, int n
   flux.m_BC = &g->bc;
   CartesianIterator<5, SideFluxT<E>> iterator(flux);
   for (size_t p = 0; p < g->patches.size(); ++p) iterator.addPatch(g->patches[p]);
+  for (size_t p = 0; p < g->inactive.size(); ++p) if (g->inactive[p]) iterator.deactivatePatch(p);
   RungeKutta rk;
   for (int a = 0; a < n_alpha; ++a) rk.addAlpha(alpha[a]);
   rk.addIterator(&iterator);
@@ -668,6 +672,17 @@ int grid_run_impl(DnRefGrid* g, int steps, double dt, const double* alpha, int n
   return 0;
 }
 } // extern "C++"
+
+// Marks patch p inactive (1) or active (0) for the following runs: the
+// iterator's deactivatePatch (iterators/patchiterator.h:127-133).
+int dnref_grid_deactivate(void* handle, int p, int inactive)
+{
+  DnRefGrid* g = (DnRefGrid*)handle;
+  if (!g || p < 0 || p >= int(g->patches.size())) return -1;
+  g->inactive.resize(g->patches.size(), 0);
+  g->inactive[p] = char(inactive != 0);
+  return 0;
+}
 
 // `steps` RK steps of all patches with the Euler flux `scheme` (as in
 // dnref_run_scheme); *seconds = time of RungeKutta::operator() only.
