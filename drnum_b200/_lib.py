@@ -29,6 +29,7 @@ DN_FACE_CLOSED = 1
 
 DN_OPT_BATCHED = 0
 DN_OPT_GRAPH = 1
+DN_NUM_TILE_SHAPES = 3
 
 DN_BC_ZERO_FLUX = 0
 DN_BC_FARFIELD = 1
@@ -86,6 +87,8 @@ SIGNATURES = {
     "dn_compute": (c_int, [c_void_p, c_double]),
     "dn_compute_patches": (c_int, [c_void_p, c_double, c_void_p, c_int]),
     "dn_patch_activate": (c_int, [c_void_p, c_int, c_int]),
+    "dn_patch_set_levelset_gpu": (c_int, [c_void_p, c_int, c_void_p]),
+    "dn_patch_levelset_gpu_counts": (c_int, [c_void_p, c_int, c_void_p]),
     "dn_patch_set_levelset_layers": (c_int, [c_void_p, c_int, c_int, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p,
                                              c_void_p]),
     "dn_rk_step": (c_int, [c_void_p, c_double, POINTER(c_double), c_int]),

@@ -511,7 +511,7 @@ class B200CartesianIterator:
         """Measures the tile shapes on this case and picks one per patch (and,
         for FP32-bulk single-patch launches, the plane-chunk length of the
         CTAs); returns the measured cost per padded cell (ns) of each shape."""
-        cost = np.zeros(2)
+        cost = np.zeros(_lib.DN_NUM_TILE_SHAPES)
         path = None if cache_path is None else str(cache_path).encode()
         check(self.ctx, self.lib.dn_autotune(self.ctx, path, _lib.dptr(cost)))
         return cost

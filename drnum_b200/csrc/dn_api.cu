@@ -102,6 +102,8 @@ struct dn_ctx {
   // level-set layers per patch and their device form
   std::vector<dn::LevelSetLayers> ls;
   std::vector<char> ls_on;
+  std::vector<dn::LevelSetGpu> lsg;           // the reference's GPU level-set path, per patch
+  std::vector<char> lsg_on;
   bool ls_dirty = true;
   std::vector<void*> ls_mem;
   dn::LsPlan ls_plan{};
@@ -111,8 +113,11 @@ struct dn_ctx {
   bool batch_dirty = true;
   void* d_records = nullptr;
   void* d_maps = nullptr;                     // FX32 batched: dn::BatchMaps per patch
-  void* d_items[dn::kNumShapes] = {nullptr, nullptr};
-  int n_items[dn::kNumShapes] = {0, 0};
+  void* d_items[2][dn::kNumShapes] = {};      // FX32: [0] edge tiles, [1] full tiles; FP64: all in [0]
+  int n_items[2][dn::kNumShapes] = {};
+  cudaStream_t s_aux = nullptr;               // second branch of a batched stage (edge tiles)
+  int batch_min_planes = 8;                   // shortest plane range of a batched work item (autotuned)
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   // CUDA graphs of whole RK steps; any change of the case bumps generation
   bool use_graph = false;
   std::vector<GraphEntry> graphs;
@@ -456,6 +461,9 @@ int read_device_error(dn_ctx* c)
     if (h & 16) return fail(c, DN_ERR_RANGE, "a face flux of a stage was not finite or reached 2^30 offset quanta "
                             "(the state or its fluxes left the fixed-point range of the patch)");
     if (h & 32) return fail(c, DN_ERR_DEVICE, "a TMA transfer of a stage did not complete within its bounded wait");
+    if (h & dn::kErrLsAverage)
+      return fail(c, DN_ERR_DEVICE, "an inside-cell average of the GPU level-set path was not finite "
+                  "(the reference's kernel traps there)");
     return fail(c, DN_ERR_DEVICE, "device error word 0x%x", h);
   }
   return DN_OK;
@@ -672,39 +680,82 @@ int build_ls_plan(dn_ctx* c)
       }
     }
   }
-  if (patch.size() >= (size_t)INT32_MAX) return fail(c, DN_ERR_RANGE, "too many level-set layer cells");
+  // the GPU level-set path: deactivated cells that no donor copy writes, and
+  // the inside cells with their neighbours
+  std::vector<int32_t> rpatch, apatch;
+  std::vector<int64_t> rcell, acell, astart(1, 0), anbr;
+  std::vector<double> aw;
+  for (size_t r = 0; r < np && r < c->lsg.size(); ++r) {
+    const DnPatch& P = c->patches[r];
+    if (!c->lsg_on[r] || !P.owned) continue;
+    const std::vector<uint64_t>* rec = r < c->tables.size() ? &c->tables[r].rec_unique : nullptr;
+    for (uint64_t cb : c->lsg[r].below) {
+      if (rec && std::binary_search(rec->begin(), rec->end(), cb)) continue;
+      rpatch.push_back((int32_t)r);
+      rcell.push_back((int64_t)pad_cell(P, cb));
+    }
+    for (const dn::LsInsideCell& ic : c->lsg[r].inside) {
+      apatch.push_back((int32_t)r);
+      acell.push_back((int64_t)pad_cell(P, ic.cell));
+      for (size_t m = 0; m < ic.nbr.size(); ++m) {
+        anbr.push_back((int64_t)pad_cell(P, ic.nbr[m]));
+        aw.push_back(ic.w[m]);
+      }
+      astart.push_back((int64_t)anbr.size());
+    }
+  }
+  if (patch.size() >= (size_t)INT32_MAX || rpatch.size() >= (size_t)INT32_MAX || apatch.size() >= (size_t)INT32_MAX)
+    return fail(c, DN_ERR_RANGE, "too many level-set cells");
   dn::LsPlan& L = c->ls_plan;
   L.n = (int32_t)patch.size();
+  L.n_reset = (int32_t)rpatch.size();
+  L.n_avg = (int32_t)apatch.size();
   int s;
   if ((s = ls_upload(c, patch, &L.patch)) || (s = ls_upload(c, cell, &L.cell)) || (s = ls_upload(c, grad, &L.grad)) ||
       (s = ls_upload(c, donor, &L.donor)) || (s = ls_upload(c, w, &L.w)) || (s = ls_upload(c, nc, &L.nc)) ||
       (s = ls_upload(c, base, &L.base)) || (s = ls_upload(c, quantum, &L.quantum)) ||
-      (s = ls_upload(c, bufs, &L.bufs))) {
+      (s = ls_upload(c, bufs, &L.bufs)) || (s = ls_upload(c, rpatch, &L.reset_patch)) ||
+      (s = ls_upload(c, rcell, &L.reset_cell)) || (s = ls_upload(c, apatch, &L.avg_patch)) ||
+      (s = ls_upload(c, acell, &L.avg_cell)) || (L.n_avg > 0 && (s = ls_upload(c, astart, &L.avg_start))) ||
+      (s = ls_upload(c, anbr, &L.avg_nbr)) || (s = ls_upload(c, aw, &L.avg_w))) {
     free_ls_plan(c);
     return s;
   }
-  if (L.n > 0) {
+  for (int q = 0; q < 2; ++q) {
+    const size_t n = q == 0 ? (size_t)L.n : (size_t)L.n_avg;
+    if (n == 0) continue;
     void* d = nullptr;
-    cudaError_t e = cudaMalloc(&d, (size_t)L.n * 5 * sizeof(double));
+    cudaError_t e = cudaMalloc(&d, n * 5 * sizeof(double));
     if (e != cudaSuccess) { free_ls_plan(c); return fail(c, DN_ERR_NOMEM, "cudaMalloc(level-set scratch)"); }
     c->ls_mem.push_back(d);
-    L.acc = static_cast<double*>(d);
+    (q == 0 ? L.acc : L.avg_acc) = static_cast<double*>(d);
   }
   c->ls_dirty = false;
   return DN_OK;
 }
 
-// Level-set slip-wall condition on physical buffer `b` of every patch.
-int levelset_bc(dn_ctx* c, int b)
+// Level-set wall conditions on physical buffer `b` of every patch (step_b:
+// the step-start state, which the GPU level-set path resets its
+// deactivated cells to).
+int levelset_bc(dn_ctx* c, int b, int step_b)
 {
   NvtxRange nvtx("dn level-set wall");
-  bool any = false;
+  bool any = false, any_gpu = false;
   for (char on : c->ls_on) any = any || on;
-  if (!any) return DN_OK;
+  for (char on : c->lsg_on) any_gpu = any_gpu || on;
+  if (!any && !any_gpu) return DN_OK;
   int s;
   if (c->ls_dirty && (s = build_ls_plan(c))) return s;
-  cudaError_t e = dn::launch_levelset_bc(c->ls_plan, b, c->precision != DN_FP64, c->d_err, c->stream);
-  c->launches += 2;
+  const dn::LsPlan& L = c->ls_plan;
+  cudaError_t e = cudaSuccess;
+  if (any && L.n > 0) {
+    e = dn::launch_levelset_bc(L, b, c->precision != DN_FP64, c->d_err, c->stream);
+    c->launches += 2;
+  }
+  if (e == cudaSuccess && any_gpu) {
+    e = dn::launch_levelset_gpu(L, b, step_b, c->precision != DN_FP64, c->d_err, c->stream);
+    c->launches += (L.n_reset > 0 ? 1 : 0) + (L.n_avg > 0 ? 2 : 0);
+  }
   if (e != cudaSuccess) return cuda_fail(c, e, "level-set boundary launch");
   return DN_OK;
 }
@@ -728,6 +779,7 @@ int donor_copy(dn_ctx* c, int b)
 bool any_levelset(const dn_ctx* c)
 {
   for (char on : c->ls_on) if (on) return true;
+  for (char on : c->lsg_on) if (on) return true;
   return false;
 }
 
@@ -780,7 +832,7 @@ int rk_step_enqueue(dn_ctx* c, double dt, const double* alpha, int n_alpha, int 
     if (s > 0 && post_op && (st = donor_copy(c, in))) return st;
     if ((st = stage_all(c, in, A, out, factor))) return st;
     if ((st = donor_copy(c, out))) return st;   // copyDonorData(0) after the stage (:38)
-    if ((st = levelset_bc(c, out))) return st;   // runPostOperations() (:39)
+    if ((st = levelset_bc(c, out, A))) return st;   // runPostOperations() (:39)
     in = out;
   }
   return DN_OK;
@@ -847,21 +899,25 @@ void free_batch(dn_ctx* c)
   c->d_records = nullptr;
   if (c->d_maps) cudaFree(c->d_maps);
   c->d_maps = nullptr;
-  for (int q = 0; q < dn::kNumShapes; ++q) {
-    if (c->d_items[q]) cudaFree(c->d_items[q]);
-    c->d_items[q] = nullptr;
-    c->n_items[q] = 0;
+  for (int f = 0; f < 2; ++f) {
+    for (int q = 0; q < dn::kNumShapes; ++q) {
+      if (c->d_items[f][q]) cudaFree(c->d_items[f][q]);
+      c->d_items[f][q] = nullptr;
+      c->n_items[f][q] = 0;
+    }
   }
 }
 
-// Default tile shape of a patch: the one that wastes fewer k lanes
-// (k is the coalesced axis); ties go to the wider tile.
+// Default tile shape of a patch: the one that wastes fewer k lanes (k is
+// the coalesced axis; ties go to the wider tile), 16 rows where the patch
+// has that many.
 int default_shape(const DnPatch& p)
 {
   const int nk = p.d.nk;
   const double e32 = (double)nk / (double)(((nk + 31) / 32) * 32);
   const double e16 = (double)nk / (double)(((nk + 15) / 16) * 16);
-  return e16 > e32 + 1e-12 ? 1 : 0;
+  if (e16 > e32 + 1e-12) return 1;
+  return p.d.nj >= 16 ? 2 : 0;
 }
 
 // Patch records and work items (patch, column tile, plane range) of every
@@ -913,20 +969,28 @@ int build_batch(dn_ctx* c)
   const long want = (long)c->num_sms * 2 * 4;
   long chunks = (want + tiles - 1) / tiles;
   if (chunks < 1) chunks = 1;
-  std::vector<dn::WorkItem> items[dn::kNumShapes];
+  // FX32 items of tiles whose every y/z slope and face exists (the tile
+  // form without edge tests, fx_tile_full) go to their own list: a launch
+  // per form keeps one code path per kernel
+  std::vector<dn::WorkItem> items[2][dn::kNumShapes];
   for (size_t q = 0; q < np; ++q) {
     const DnPatch& P = c->patches[q];
     if (!P.owned || !P.patch_active) continue;
     const int sh = c->shape[q];
     int tj, tk;
     dn::shape_tile(fp64, sh, &tj, &tk);
+    const bool per_y = P.d.face[1] == DN_FACE_PERIODIC, per_z = P.d.face[2] == DN_FACE_PERIODIC;
     long ic = (P.d.ni + chunks - 1) / chunks;
-    if (ic < 8) ic = 8;
+    if (ic < c->batch_min_planes) ic = c->batch_min_planes;   // amortise each item's 3-plane prologue
     if (ic > P.d.ni) ic = P.d.ni;
     for (int i0 = 0; i0 < P.d.ni; i0 += (int)ic)
       for (int j0 = 0; j0 < P.d.nj; j0 += tj)
-        for (int k0 = 0; k0 < P.d.nk; k0 += tk)
-          items[sh].push_back(dn::WorkItem{(int)q, j0, k0, i0, std::min(P.d.ni, i0 + (int)ic)});
+        for (int k0 = 0; k0 < P.d.nk; k0 += tk) {
+          const bool fy = (j0 + tj <= P.d.nj) && (per_y || (j0 >= 2 && j0 + tj + 2 <= P.d.nj));
+          const bool fz = (k0 + tk <= P.d.nk) && (per_z || (k0 >= 2 && k0 + tk + 2 <= P.d.nk));
+          const int form = (!fp64 && fy && fz) ? 1 : 0;
+          items[form][sh].push_back(dn::WorkItem{(int)q, j0, k0, i0, std::min(P.d.ni, i0 + (int)ic)});
+        }
   }
   cudaError_t e = cudaMalloc(&c->d_records, np * sizeof(dn::BatchPatch));
   if (e != cudaSuccess) return fail(c, DN_ERR_NOMEM, "cudaMalloc(patch records)");
@@ -938,15 +1002,18 @@ int build_batch(dn_ctx* c)
     e = cudaMemcpyAsync(c->d_maps, maps.data(), np * sizeof(dn::BatchMaps), cudaMemcpyHostToDevice, c->stream);
     if (e != cudaSuccess) return cuda_fail(c, e, "tensor map upload");
   }
-  for (int q = 0; q < dn::kNumShapes; ++q) {
-    if (items[q].empty()) continue;
-    if (items[q].size() > (size_t)INT32_MAX) return fail(c, DN_ERR_RANGE, "too many work items");
-    e = cudaMalloc(&c->d_items[q], items[q].size() * sizeof(dn::WorkItem));
-    if (e != cudaSuccess) return fail(c, DN_ERR_NOMEM, "cudaMalloc(work items)");
-    e = cudaMemcpyAsync(c->d_items[q], items[q].data(), items[q].size() * sizeof(dn::WorkItem),
-                        cudaMemcpyHostToDevice, c->stream);
-    if (e != cudaSuccess) return cuda_fail(c, e, "work item upload");
-    c->n_items[q] = (int)items[q].size();
+  for (int f = 0; f < 2; ++f) {
+    for (int q = 0; q < dn::kNumShapes; ++q) {
+      const std::vector<dn::WorkItem>& it = items[f][q];
+      if (it.empty()) continue;
+      if (it.size() > (size_t)INT32_MAX) return fail(c, DN_ERR_RANGE, "too many work items");
+      e = cudaMalloc(&c->d_items[f][q], it.size() * sizeof(dn::WorkItem));
+      if (e != cudaSuccess) return fail(c, DN_ERR_NOMEM, "cudaMalloc(work items)");
+      e = cudaMemcpyAsync(c->d_items[f][q], it.data(), it.size() * sizeof(dn::WorkItem), cudaMemcpyHostToDevice,
+                          c->stream);
+      if (e != cudaSuccess) return cuda_fail(c, e, "work item upload");
+      c->n_items[f][q] = (int)it.size();
+    }
   }
   e = cudaStreamSynchronize(c->stream);   // host vectors go out of scope
   if (e != cudaSuccess) return cuda_fail(c, e, "batch upload");
@@ -987,21 +1054,50 @@ int stage_all(dn_ctx* c, int in_b, int un_b, int out_b, double factor)
     return DN_OK;
   }
   if (c->batch_dirty && (s = build_batch(c))) return s;
+  // full-tile launches on the context's stream, edge-tile launches on a
+  // second branch forked from it and joined after (they write disjoint
+  // tiles), so the two forms overlap instead of queueing behind each other
+  bool any_edge = false, any_full = false;
   for (int q = 0; q < dn::kNumShapes; ++q) {
-    if (!c->n_items[q]) continue;
-    dn::Batch b;
-    b.patches = static_cast<const dn::BatchPatch*>(c->d_records);
-    b.maps = static_cast<const dn::BatchMaps*>(c->d_maps);
-    b.items = static_cast<const dn::WorkItem*>(c->d_items[q]);
-    b.n_items = c->n_items[q];
-    b.in_b = in_b; b.un_b = un_b; b.out_b = out_b;
-    b.factor = factor;
-    b.err = c->d_err;
-    b.err_info = c->d_err_info;
-    cudaError_t e = c->precision == DN_FP64 ? dn::launch_stage_f64_batched(b, q, c->stream)
-                                            : dn::launch_stage_fx32_batched(b, q, c->stream);
-    c->launches++;
-    if (e != cudaSuccess) return cuda_fail(c, e, "batched stage launch");
+    any_edge = any_edge || c->n_items[0][q] > 0;
+    any_full = any_full || c->n_items[1][q] > 0;
+  }
+  const bool fork = any_edge && any_full;
+  cudaError_t e = cudaSuccess;
+  if (fork) {
+    if (!c->s_aux) {
+      e = cudaStreamCreateWithFlags(&c->s_aux, cudaStreamNonBlocking);
+      if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming);
+      if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->ev_join, cudaEventDisableTiming);
+      if (e != cudaSuccess) return cuda_fail(c, e, "stage branch stream");
+    }
+    e = cudaEventRecord(c->ev_fork, c->stream);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(c->s_aux, c->ev_fork, 0);
+    if (e != cudaSuccess) return cuda_fail(c, e, "stage branch fork");
+  }
+  for (int f = 1; f >= 0; --f) {
+    cudaStream_t st = (fork && f == 0) ? c->s_aux : c->stream;
+    for (int q = 0; q < dn::kNumShapes; ++q) {
+      if (!c->n_items[f][q]) continue;
+      dn::Batch b;
+      b.patches = static_cast<const dn::BatchPatch*>(c->d_records);
+      b.maps = static_cast<const dn::BatchMaps*>(c->d_maps);
+      b.items = static_cast<const dn::WorkItem*>(c->d_items[f][q]);
+      b.n_items = c->n_items[f][q];
+      b.in_b = in_b; b.un_b = un_b; b.out_b = out_b;
+      b.factor = factor;
+      b.err = c->d_err;
+      b.err_info = c->d_err_info;
+      e = c->precision == DN_FP64 ? dn::launch_stage_f64_batched(b, q, st)
+                                  : dn::launch_stage_fx32_batched(b, q, f == 1, st);
+      c->launches++;
+      if (e != cudaSuccess) return cuda_fail(c, e, "batched stage launch");
+    }
+  }
+  if (fork) {
+    e = cudaEventRecord(c->ev_join, c->s_aux);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(c->stream, c->ev_join, 0);
+    if (e != cudaSuccess) return cuda_fail(c, e, "stage branch join");
   }
   return DN_OK;
 }
@@ -1320,6 +1416,10 @@ int dn_ctx_destroy(dn_ctx* c)
     if (c->ev_d2h_done[b]) cudaEventDestroy(c->ev_d2h_done[b]);
   }
   if (c->ev_main) cudaEventDestroy(c->ev_main);
+  if (c->s_aux) cudaStreamSynchronize(c->s_aux);
+  if (c->ev_fork) cudaEventDestroy(c->ev_fork);
+  if (c->ev_join) cudaEventDestroy(c->ev_join);
+  if (c->s_aux) cudaStreamDestroy(c->s_aux);
   if (c->s_in) cudaStreamDestroy(c->s_in);
   if (c->s_conv) cudaStreamDestroy(c->s_conv);
   if (c->s_out) cudaStreamDestroy(c->s_out);
@@ -1398,6 +1498,8 @@ int dn_patch_add(dn_ctx* c, const dn_patch_desc* d, int* id)
   c->tables.resize(c->patches.size());
   c->ls.resize(c->patches.size());
   c->ls_on.resize(c->patches.size(), 0);
+  c->lsg.resize(c->patches.size());
+  c->lsg_on.resize(c->patches.size(), 0);
   c->shape.push_back(default_shape(c->patches.back()));
   c->plan_dirty = true;
   c->ls_dirty = true;
@@ -1876,6 +1978,8 @@ int dn_patch_set_levelset(dn_ctx* c, int id, const double* G, int num_inner_laye
     return fail(c, DN_ERR_ARG, "%s", err.c_str());
   c->ls[id] = std::move(L);
   c->ls_on[id] = 1;
+  c->lsg_on[id] = 0;
+  c->lsg[id] = dn::LevelSetGpu();
   c->ls_dirty = true;
   c->generation++;
   return DN_OK;
@@ -1921,6 +2025,58 @@ int dn_patch_set_levelset_layers(dn_ctx* c, int id, int num_inner_layers, const 
   return DN_OK;
 }
 
+int dn_patch_set_levelset_gpu(dn_ctx* c, int id, const double* G)
+{
+  int s = check_patch(c, id);
+  if (s) return s;
+  if (set_device(c) != DN_OK) return DN_ERR_CUDA;
+  DnPatch& P = c->patches[id];
+  if (!G) {
+    c->lsg_on[id] = 0;
+    c->lsg[id] = dn::LevelSetGpu();
+    c->ls_dirty = true;
+    c->generation++;
+    return DN_OK;
+  }
+  for (size_t l = 0; l < P.nc; ++l)
+    if (!std::isfinite(G[l])) return fail(c, DN_ERR_ARG, "level-set value of cell %zu is not finite", l);
+  dn::LevelSetGpu L;
+  std::string err;
+  if (!dn::classify_levelset_gpu(dn::overlap_patch(P.d), G, L, err)) return fail(c, DN_ERR_ARG, "%s", err.c_str());
+  // deactivate the G < 0 cells (GPU_CartesianLevelSetBC's constructor),
+  // keeping cells the patch's mask already deactivated
+  std::vector<uint8_t> mask(P.nc, 1);
+  if (P.active) {
+    std::vector<uint8_t> dev(P.ncp);
+    cudaError_t e = cudaMemcpyAsync(dev.data(), P.active, P.ncp, cudaMemcpyDeviceToHost, c->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    if (e != cudaSuccess) return cuda_fail(c, e, "active mask download");
+    for (size_t l = 0; l < P.nc; ++l) mask[l] = dev[pad_cell(P, l)];
+  }
+  for (uint64_t l : L.below) mask[l] = 0;
+  if ((s = dn_patch_set_active(c, id, mask.data()))) return s;
+  c->lsg[id] = std::move(L);
+  c->lsg_on[id] = 1;
+  c->ls_on[id] = 0;
+  c->ls[id] = dn::LevelSetLayers();
+  c->ls_dirty = true;
+  c->generation++;
+  return DN_OK;
+}
+
+int dn_patch_levelset_gpu_counts(dn_ctx* c, int id, int64_t counts[3])
+{
+  int s = check_patch(c, id);
+  if (s) return s;
+  if (!counts) return fail(c, DN_ERR_ARG, "counts is NULL");
+  counts[0] = (int64_t)c->lsg[id].below.size();
+  counts[1] = (int64_t)c->lsg[id].inside.size();
+  int64_t nb = 0;
+  for (const auto& ic : c->lsg[id].inside) nb += (int64_t)ic.nbr.size();
+  counts[2] = nb;
+  return DN_OK;
+}
+
 int dn_patch_levelset_count(dn_ctx* c, int id, int inner, int layer, int64_t* n)
 {
   int s = check_patch(c, id);
@@ -1959,7 +2115,7 @@ int dn_apply_levelset_bc(dn_ctx* c, int field)
   int s;
   if ((s = check_field(c, field))) return s;
   if (set_device(c) != DN_OK) return DN_ERR_CUDA;
-  return levelset_bc(c, c->fmap[field]);
+  return levelset_bc(c, c->fmap[field], c->fmap[1]);
 }
 
 int dn_copy_donor_data(dn_ctx* c, int field)
@@ -2202,47 +2358,59 @@ std::string device_name(int dev)
   return prop.name;
 }
 
-// cache lines: "<device>|<precision>|<cost shape 0>|<cost shape 1>"
-bool read_tune_cache(const char* path, const std::string& dev, int precision, double cost[2])
+// cache lines: "<device>|<precision>|<shapes>|<cost shape 0>|<cost shape 1>|..."
+bool read_tune_cache(const char* path, const std::string& dev, int precision, double cost[dn::kNumShapes])
 {
   if (!path) return false;
   FILE* f = std::fopen(path, "r");
   if (!f) return false;
-  char line[512];
+  char line[1024];
   bool found = false;
   while (std::fgets(line, sizeof line, f)) {
     char name[256];
-    int prec;
-    double c0, c1;
-    if (std::sscanf(line, "%255[^|]|%d|%lf|%lf", name, &prec, &c0, &c1) == 4 && dev == name && prec == precision) {
-      cost[0] = c0;
-      cost[1] = c1;
-      found = true;
+    int prec, ns, pos = 0;
+    if (std::sscanf(line, "%255[^|]|%d|%d%n", name, &prec, &ns, &pos) != 3 || dev != name || prec != precision ||
+        ns != dn::kNumShapes)
+      continue;
+    double c[dn::kNumShapes];
+    const char* q = line + pos;
+    int got = 0;
+    for (int k = 0; k < dn::kNumShapes; ++k) {
+      int m = 0;
+      if (std::sscanf(q, "|%lf%n", &c[k], &m) != 1) break;
+      q += m;
+      ++got;
     }
+    if (got != dn::kNumShapes) continue;
+    for (int k = 0; k < dn::kNumShapes; ++k) cost[k] = c[k];
+    found = true;
   }
   std::fclose(f);
   return found;
 }
 
-void write_tune_cache(const char* path, const std::string& dev, int precision, const double cost[2])
+void write_tune_cache(const char* path, const std::string& dev, int precision, const double cost[dn::kNumShapes])
 {
   if (!path) return;
   FILE* f = std::fopen(path, "a");
   if (!f) return;
-  std::fprintf(f, "%s|%d|%.17g|%.17g\n", dev.c_str(), precision, cost[0], cost[1]);
+  std::fprintf(f, "%s|%d|%d", dev.c_str(), precision, dn::kNumShapes);
+  for (int k = 0; k < dn::kNumShapes; ++k) std::fprintf(f, "|%.17g", cost[k]);
+  std::fprintf(f, "\n");
   std::fclose(f);
 }
 
 } // namespace
 
-int dn_autotune(dn_ctx* c, const char* cache_path, double cost_out[2])
+int dn_autotune(dn_ctx* c, const char* cache_path, double cost_out[DN_NUM_TILE_SHAPES])
 {
   NvtxRange nvtx("dn autotune");
   if (!c) return DN_ERR_ARG;
   if (c->patches.empty()) return fail(c, DN_ERR_STATE, "no patches to tune for");
   if (set_device(c) != DN_OK) return DN_ERR_CUDA;
   const std::string dev = device_name(c->device);
-  double cost[2] = {0, 0};
+  static_assert(DN_NUM_TILE_SHAPES == dn::kNumShapes, "tile shape count");
+  double cost[dn::kNumShapes] = {};
   if (!read_tune_cache(cache_path, dev, c->precision, cost)) {
     // measure each tile shape on the case itself: one stage of every patch
     // into the scratch field (field 2), factor 0
@@ -2330,7 +2498,42 @@ int dn_autotune(dn_ctx* c, const char* cache_path, double cost_out[2])
   }
   c->batch_dirty = true;
   c->generation++;
-  if (cost_out) { cost_out[0] = cost[0]; cost_out[1] = cost[1]; }
+  // batched stages: the shortest plane range of a work item, measured among
+  // a few candidates with the shapes just chosen (one stage of every patch
+  // into the scratch field, factor 0; the ranges change no result)
+  if (c->batched && c->patches.size() > 1) {
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    const int cand[5] = {8, 16, 24, 32, 48};
+    int best = c->batch_min_planes;
+    double best_ms = 1e300;
+    int st = DN_OK;
+    for (int k = 0; k < 5 && st == DN_OK; ++k) {
+      c->batch_min_planes = cand[k];
+      c->batch_dirty = true;
+      for (int r = 0; r < 5 && st == DN_OK; ++r) {
+        if (r == 2) cudaEventRecord(e0, c->stream);
+        st = stage_all(c, c->fmap[0], c->fmap[1], c->fmap[2], 0.0);
+      }
+      cudaEventRecord(e1, c->stream);
+      cudaEventSynchronize(e1);
+      float ms = 0;
+      cudaEventElapsedTime(&ms, e0, e1);
+      if (st == DN_OK && ms < best_ms) { best_ms = ms; best = cand[k]; }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    c->batch_min_planes = best;
+    c->batch_dirty = true;
+    c->generation++;
+    if (st != DN_OK) return st;
+    int s4 = read_device_error(c);
+    if (s4 != DN_OK) return s4;
+  }
+  if (cost_out) {
+    for (int k = 0; k < dn::kNumShapes; ++k) cost_out[k] = cost[k];
+  }
   return DN_OK;
 }
 

@@ -4,6 +4,7 @@
 #include "dn_levelset.h"
 
 #include <cmath>
+#include <cstdio>
 #include <utility>
 
 namespace dn {
@@ -208,6 +209,94 @@ bool classify_levelset(const OverlapPatch& patch, const double* G, int num_inner
   }
   for (int layer = 0; layer < num_outer; ++layer)
     for (LayerCell& c : out.outer[layer]) normalised_gradient(gr, G, c.cell, patch.d, c.grad);
+  return true;
+}
+
+bool classify_levelset_gpu(const OverlapPatch& patch, const double* G, LevelSetGpu& out, std::string& err)
+{
+  if (!G) { err = "level-set field is NULL"; return false; }
+  const long imax = patch.n[0], jmax = patch.n[1], kmax = patch.n[2];
+  out = LevelSetGpu();
+  auto idx = [&](long i, long j, long k) -> size_t { return (size_t)((i * jmax + j) * kmax + k); };
+  auto g = [&](long i, long j, long k) { return G[idx(i, j, k)]; };
+  // GPU_CartesianPatch::idx() etc.: 1 / spacing (CartesianPatch::computeDeltas,
+  // cartesianpatch.cpp:167-174)
+  const double dx = patch.d[0], dy = patch.d[1], dz = patch.d[2];
+  const double idx_ = 1.0 / dx, idy = 1.0 / dy, idz = 1.0 / dz;
+  for (long i = 0; i < imax; ++i) {
+    for (long j = 0; j < jmax; ++j) {
+      for (long k = 0; k < kmax; ++k) {
+        if (!(g(i, j, k) < 0)) continue;
+        out.below.push_back(idx(i, j, k));
+        bool extrapolate = true;
+        long i_stt = -2, i_end = 2, j_stt = -2, j_end = 2, k_stt = -2, k_end = 2;
+        if (i < 2) i_stt += 2 - i;
+        if (i == imax - 1) i_end = 0;
+        if (i == imax - 2) i_end = 1;
+        if (j < 2) j_stt += 2 - j;
+        if (j == jmax - 1) j_end = 0;
+        if (j == jmax - 2) j_end = 1;
+        if (k < 2) k_stt += 2 - k;
+        if (k == kmax - 1) k_end = 0;
+        if (k == kmax - 2) k_end = 1;
+        for (long di = i_stt; di <= i_end; ++di) {
+          for (long dj = j_stt; dj <= j_end; ++dj) {
+            for (long dk = k_stt; dk <= k_end; ++dk) {
+              if (di == 0 && dj == 0 && dk == 0) continue;
+              const long i2 = i + 2 * di, j2 = j + 2 * dj, k2 = k + 2 * dk;
+              if (i2 < 0 || j2 < 0 || k2 < 0 || i2 >= imax || j2 >= jmax || k2 >= kmax) {
+                char buf[200];
+                std::snprintf(buf, sizeof buf,
+                              "cell (%ld, %ld, %ld) with G < 0 lies too close to the patch edge for the GPU "
+                              "level-set path (its search reaches (%ld, %ld, %ld))", i, j, k, i2, j2, k2);
+                err = buf;
+                return false;
+              }
+              if (g(i + di, j + dj, k + dk) >= 0) {
+                extrapolate = false;
+                break;   // the reference leaves only the innermost loop
+              }
+            }
+          }
+        }
+        if (!extrapolate) continue;
+        if (i < 2) i_stt = 0;
+        if (i >= imax - 2) i_end = 0;
+        if (j < 2) j_stt = 0;
+        if (j >= jmax - 2) j_end = 0;
+        if (k < 2) k_stt = 0;
+        if (k >= kmax - 2) k_end = 0;
+        // gradient of G (GPU_CartesianLevelSetBC::grad)
+        double gx, gy, gz;
+        if (i == 0) gx = idx_ * (g(i + 1, j, k) - g(i, j, k));
+        else if (i == imax - 1) gx = idx_ * (g(i, j, k) - g(i - 1, j, k));
+        else gx = 0.5 * idx_ * (g(i + 1, j, k) - g(i - 1, j, k));
+        if (j == 0) gy = idy * (g(i, j + 1, k) - g(i, j, k));
+        else if (j == jmax - 1) gy = idy * (g(i, j, k) - g(i, j - 1, k));
+        else gy = 0.5 * idy * (g(i, j + 1, k) - g(i, j - 1, k));
+        if (k == 0) gz = idz * (g(i, j, k + 1) - g(i, j, k));
+        else if (k == kmax - 1) gz = idz * (g(i, j, k) - g(i, j, k - 1));
+        else gz = 0.5 * idz * (g(i, j, k + 1) - g(i, j, k - 1));
+        LsInsideCell c;
+        c.cell = idx(i, j, k);
+        const double g0 = g(i, j, k);
+        for (long di = i_stt; di <= i_end; ++di) {
+          for (long dj = j_stt; dj <= j_end; ++dj) {
+            for (long dk = k_stt; dk <= k_end; ++dk) {
+              if (di == 0 && dj == 0 && dk == 0) continue;
+              const double gn = g(i + di, j + dj, k + dk);
+              if (gn >= 0 || gn > g0) {
+                const double ddx = (double)di * dx, ddy = (double)dj * dy, ddz = (double)dk * dz;
+                c.nbr.push_back(idx(i + di, j + dj, k + dk));
+                c.w.push_back(std::fabs(ddx * gx + ddy * gy + ddz * gz) / std::sqrt(ddx * ddx + ddy * ddy + ddz * ddz));
+              }
+            }
+          }
+        }
+        out.inside.push_back(std::move(c));
+      }
+    }
+  }
   return true;
 }
 

@@ -50,4 +50,32 @@ struct LevelSetLayers {
 bool classify_levelset(const OverlapPatch& patch, const double* G, int num_inner, int num_outer,
                        double min_inner_rel_dist, LevelSetLayers& out, std::string& err);
 
+// The reference's GPU level-set path (GPU_CartesianLevelSetBC, with
+// StoredLevelSet and CompressibleLsSlip; gpu_cartesianlevelsetbc.h:106-125,
+// 129-229, 414-487):
+//   - every cell with G < 0 is deactivated (its constructor, :106-125);
+//   - such a cell with a G >= 0 cell within two cells (the 5x5x5 box the
+//     search walks, limited at the patch edges, :150-202) is a boundary cell
+//     whose kernel writes nothing (its state-writing part is commented out,
+//     :358-410, and it is launched on the other list, :509);
+//   - every other G < 0 cell ("inside") is replaced after each stage by the
+//     weighted mean of the cells of its (edge-limited) box whose G is larger,
+//     weight |d . grad G| / |d| (:414-487), grad G by central differences
+//     (one-sided at the patch edge, :78-93).
+struct LsInsideCell {
+  uint64_t cell;
+  std::vector<uint64_t> nbr;   // averaged neighbours, in the kernel's loop order (di, dj, dk)
+  std::vector<double> w;       // their weights
+};
+
+struct LevelSetGpu {
+  std::vector<uint64_t> below;           // cells with G < 0, ascending
+  std::vector<LsInsideCell> inside;      // inside cells, ascending
+};
+
+// Classifies one patch for the GPU level-set path.  Returns false with a
+// message where the reference stops with a BUG (a G < 0 cell whose search
+// box reaches, at twice its offset, beyond the patch: gpu_cartesianlevelsetbc.h:170-179).
+bool classify_levelset_gpu(const OverlapPatch& patch, const double* G, LevelSetGpu& out, std::string& err);
+
 } // namespace dn

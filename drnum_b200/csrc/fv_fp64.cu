@@ -53,7 +53,9 @@ cudaError_t launch_f64_batched(const Batch& b, cudaStream_t st)
 cudaError_t launch_stage_f64_batched(const Batch& b, int shape, cudaStream_t st)
 {
   if (b.n_items <= 0) return cudaSuccess;
-  return shape == 0 ? launch_f64_batched<4, 32>(b, st) : launch_f64_batched<8, 16>(b, st);
+  if (shape == 0) return launch_f64_batched<4, 32>(b, st);
+  if (shape == 1) return launch_f64_batched<8, 16>(b, st);
+  return launch_f64_batched<8, 32>(b, st);
 }
 
 } // namespace dn

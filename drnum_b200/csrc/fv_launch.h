@@ -33,16 +33,19 @@ void fx32_tile(int* tj, int* tk);
 bool encode_stage_maps(CUtensorMap* tm_in, CUtensorMap* tm_un, const int32_t* in, const int32_t* un, const FxGeom& g,
                        int tj, int tk);
 
-// Batched launches over a work list (fv_batch.cuh).  Tile shapes:
-//   FX32: 0 = 8 x 32, 1 = 16 x 16 (j x k);  FP64: 0 = 4 x 32, 1 = 8 x 16.
+// Batched launches over a work list (fv_batch.cuh).  Tile shapes (j x k):
+//   FX32: 0 = 8 x 32, 1 = 16 x 16, 2 = 16 x 32;  FP64: 0 = 4 x 32, 1 = 8 x 16, 2 = 8 x 32.
 struct Batch;
-constexpr int kNumShapes = 2;
-cudaError_t launch_stage_fx32_batched(const Batch& b, int shape, cudaStream_t st);
+constexpr int kNumShapes = 3;
+// full: every item's tile is full (fx_tile_full), run by the tile form
+// without edge tests
+cudaError_t launch_stage_fx32_batched(const Batch& b, int shape, bool full, cudaStream_t st);
 cudaError_t launch_stage_f64_batched(const Batch& b, int shape, cudaStream_t st);
 inline void shape_tile(bool fp64, int shape, int* tj, int* tk)
 {
-  *tk = shape == 0 ? 32 : 16;
-  *tj = fp64 ? (shape == 0 ? 4 : 8) : (shape == 0 ? 8 : 16);
+  *tk = shape == 1 ? 16 : 32;
+  if (fp64) *tj = shape == 0 ? 4 : 8;
+  else *tj = shape == 0 ? 8 : 16;
 }
 
 // Chooses the i-chunk so that the grid holds enough CTAs to fill the GPU.

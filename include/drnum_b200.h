@@ -300,6 +300,28 @@ int dn_patch_set_levelset_layers(dn_ctx* ctx, int patch_id, int num_inner_layers
                                  const uint64_t* cells, const double* g, const double* grad, const uint64_t* donors,
                                  const double* weights);
 
+/* The level-set wall of the reference's GPU path instead, for applications
+ * that use GPU_CartesianLevelSetBC<DIM, NUM_LS, StoredLevelSet,
+ * CompressibleLsSlip> (e.g. drnumBasicAero): every cell with G < 0 is
+ * deactivated (gpu_cartesianlevelsetbc.h:106-125; cells the patch's mask
+ * already deactivated stay so) and, like the reference's GPU iterator
+ * (gpu_cartesianiterator.h:199-205), holds the step-start state through the
+ * stages unless a donor copy writes it; after every stage each "inside" cell
+ * (G < 0 with no G >= 0 cell in its two-cell box) takes the weighted mean of
+ * its box cells of larger G, weight |d . grad G| / |d|
+ * (gpu_cartesianlevelsetbc.h:129-229,414-487).  The reference's boundary-cell
+ * kernel writes nothing (:316-411) and has no counterpart.  A mean that is not
+ * finite is reported as DN_ERR_DEVICE where the reference traps.  Returns
+ * DN_ERR_ARG where the reference stops with a BUG (a G < 0 cell within two
+ * cells of the patch edge, :170-179).  Replaces the patch's other level-set
+ * wall; G = NULL removes it (the cells stay deactivated: dn_patch_set_active
+ * restores the mask). */
+int dn_patch_set_levelset_gpu(dn_ctx* ctx, int patch_id, const double* G);
+
+/* Sizes of a patch's GPU level-set path: counts[0] deactivated cells,
+ * counts[1] inside cells, counts[2] averaged neighbour entries. */
+int dn_patch_levelset_gpu_counts(dn_ctx* ctx, int patch_id, int64_t counts[3]);
+
 /* Size and contents of one layer of a patch's level-set classification
  * (inner = 1: G < 0 layers, 0: outer layers), in the reference's order:
  * cell index, G, normalised gradient [n][3], mirror-point donors and weights
@@ -338,20 +360,24 @@ int dn_lslayers_destroy(dn_lslayers* ls);
 #define DN_OPT_GRAPH      1
 int dn_set_option(dn_ctx* ctx, int option, int value);
 
-/* Tile shape of a patch in the batched launch: 0 = 8 x 32 (j x k; FP64 4 x 32),
- * 1 = 16 x 16 (FP64 8 x 16).  The default wastes the fewest k lanes. */
+/* Tile shape of a patch in the batched launch (j x k): 0 = 8 x 32 (FP64
+ * 4 x 32), 1 = 16 x 16 (FP64 8 x 16), 2 = 16 x 32 (FP64 8 x 32).  The default
+ * wastes the fewest k lanes and takes the 16-row tile where the patch has
+ * at least 16 rows. */
+#define DN_NUM_TILE_SHAPES 3
 int dn_patch_set_tile(dn_ctx* ctx, int patch_id, int shape);
 
 /* Autotuner: measures each tile shape's cost per padded cell on the
  * context's own patches (one stage into the scratch field 2, which it
  * overwrites), then gives every patch the shape of least predicted time.
  * cache_path (may be NULL) holds measured costs per device and precision and
- * is reused on the next call; cost_out[2] (may be NULL) returns them in ns per
+ * is reused on the next call; cost_out[DN_NUM_TILE_SHAPES] (may be NULL) returns them in ns per
  * padded cell and stage.  FP32-bulk stages that run one patch per launch (a
  * single patch, or batching off) also get the plane-chunk length of their
- * CTAs, measured among a few candidates on the patch itself.  Neither choice
- * changes a result.  No reference counterpart. */
-int dn_autotune(dn_ctx* ctx, const char* cache_path, double cost_out[2]);
+ * CTAs, measured among a few candidates on the patch itself; batched stages
+ * of several patches get the shortest plane range of a work item the same
+ * way.  None of the choices changes a result.  No reference counterpart. */
+int dn_autotune(dn_ctx* ctx, const char* cache_path, double cost_out[DN_NUM_TILE_SHAPES]);
 
 /* Flux scheme of the stage of an FP64 context; replaces the OP template
  * argument of GPU_CartesianIterator<DIM, OP> (gpu_cartesianiterator.h:37)

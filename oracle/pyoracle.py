@@ -11,6 +11,7 @@ module, as the checker; the drnum_b200 package never imports it.
 from __future__ import annotations
 
 import ctypes
+import math
 import os
 import subprocess
 from ctypes import POINTER, c_double, c_int, c_void_p
@@ -20,6 +21,8 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_LIB = os.path.join(HERE, "liboracle_fv.so")
 REF_LIB = os.path.join(HERE, "_ref", "libdrnum_ref.so")
+# the reference in its shipped single precision (`real` = float, drnum.h:43)
+REF_LIB_F32 = os.path.join(HERE, "_ref", "libdrnum_ref_f32.so")
 
 _P = POINTER(c_double)
 
@@ -152,11 +155,32 @@ def ref_run(U0, h, dt, steps, alpha=(0.25, 0.5, 1.0), periodic=(True, True, True
     return out, sec.value
 
 
-class RefSession:
-    """A persistent reference run (compiled reference library) for timing."""
+_ref32 = None
 
-    def __init__(self, U0, h, alpha=(0.25, 0.5, 1.0), periodic=(True, True, True), threads=0):
-        lib = ref_lib()
+
+def ref_f32_available() -> bool:
+    return os.path.exists(REF_LIB_F32)
+
+
+class RefSession:
+    """A persistent reference run (compiled reference library) for timing.
+    precision "f64": the FP64 build (the parity checker); "f32": the
+    reference's shipped single-precision build.  The periodic axes carry two
+    ghost layers per side: the iterator computes (n+4) cells along each of
+    them (`computed_cells`)."""
+
+    def __init__(self, U0, h, alpha=(0.25, 0.5, 1.0), periodic=(True, True, True), threads=0, precision="f64"):
+        global _ref32
+        if precision == "f32":
+            if _ref32 is None:
+                if not ref_f32_available():
+                    raise RuntimeError("single-precision reference not found: run oracle/build_ref.sh")
+                _ref32 = ctypes.CDLL(REF_LIB_F32)
+            lib = _ref32
+        else:
+            lib = ref_lib()
+        lib.dnref_real_size.restype = c_int
+        self.real_bytes = lib.dnref_real_size()
         lib.dnref_session_create.restype = c_void_p
         lib.dnref_session_create.argtypes = [c_int, c_int, c_int, POINTER(c_int), c_double, c_double, c_double,
                                              _P, _P, c_int, c_int]
@@ -175,6 +199,7 @@ class RefSession:
         if not self.s:
             raise RuntimeError("reference session creation failed")
         self.threads = lib.dnref_max_threads()
+        self.computed_cells = int(np.prod([x + (4 if p else 0) for x, p in zip((ni, nj, nk), periodic)]))
 
     def step(self, steps, dt):
         return self.lib.dnref_session_step(self.s, int(steps), float(dt))
@@ -461,3 +486,108 @@ def oracle_flow_stats(U, dt, dx):
     cfl = max(0.0, float(np.max(np.abs(u) * dt / dx)), float(np.max(np.abs(u + a) * dt / dx)),
               float(np.max(np.abs(u - a) * dt / dx)))
     return cfl, min(1000.0, float(U[0].min())), max(0.0, float(U[0].max()))
+
+
+# --------------------------------------------- the reference's GPU level-set path
+
+def oracle_levelset_gpu_setup(G, h):
+    """GPU_CartesianLevelSetBC's set-up (gpu_cartesianlevelsetbc.h:106-125,
+    129-229) on one patch: the G < 0 cells (deactivated) and the inside cells
+    (no G >= 0 cell in the edge-limited two-cell box) with the neighbours the
+    inside-cell kernel averages and their weights |d . grad G| / |d| (:414-487),
+    grad G as GPU_CartesianLevelSetBC::grad (:78-93).  Raises where the
+    reference stops with a BUG (:170-179)."""
+    G = np.asarray(G, dtype=np.float64)
+    imax, jmax, kmax = G.shape
+    hx, hy, hz = (h, h, h) if np.isscalar(h) else h
+    idx, idy, idz = 1.0 / hx, 1.0 / hy, 1.0 / hz
+    below, inside = [], []
+    for i in range(imax):
+        for j in range(jmax):
+            for k in range(kmax):
+                if not G[i, j, k] < 0:
+                    continue
+                below.append((i * jmax + j) * kmax + k)
+                ext = True
+                i0, i1, j0, j1, k0, k1 = -2, 2, -2, 2, -2, 2
+                if i < 2: i0 += 2 - i
+                if i == imax - 1: i1 = 0
+                if i == imax - 2: i1 = 1
+                if j < 2: j0 += 2 - j
+                if j == jmax - 1: j1 = 0
+                if j == jmax - 2: j1 = 1
+                if k < 2: k0 += 2 - k
+                if k == kmax - 1: k1 = 0
+                if k == kmax - 2: k1 = 1
+                for di in range(i0, i1 + 1):
+                    for dj in range(j0, j1 + 1):
+                        for dk in range(k0, k1 + 1):
+                            if di == 0 and dj == 0 and dk == 0:
+                                continue
+                            a, b, c = i + 2 * di, j + 2 * dj, k + 2 * dk
+                            if min(a, b, c) < 0 or a >= imax or b >= jmax or c >= kmax:
+                                raise ValueError(f"G < 0 cell {(i, j, k)} too close to the patch edge")
+                            if G[i + di, j + dj, k + dk] >= 0:
+                                ext = False
+                                break
+                if not ext:
+                    continue
+                if i < 2: i0 = 0
+                if i >= imax - 2: i1 = 0
+                if j < 2: j0 = 0
+                if j >= jmax - 2: j1 = 0
+                if k < 2: k0 = 0
+                if k >= kmax - 2: k1 = 0
+                g = lambda a, b, c: float(G[a, b, c])
+                if i == 0: gx = idx * (g(i + 1, j, k) - g(i, j, k))
+                elif i == imax - 1: gx = idx * (g(i, j, k) - g(i - 1, j, k))
+                else: gx = 0.5 * idx * (g(i + 1, j, k) - g(i - 1, j, k))
+                if j == 0: gy = idy * (g(i, j + 1, k) - g(i, j, k))
+                elif j == jmax - 1: gy = idy * (g(i, j, k) - g(i, j - 1, k))
+                else: gy = 0.5 * idy * (g(i, j + 1, k) - g(i, j - 1, k))
+                if k == 0: gz = idz * (g(i, j, k + 1) - g(i, j, k))
+                elif k == kmax - 1: gz = idz * (g(i, j, k) - g(i, j, k - 1))
+                else: gz = 0.5 * idz * (g(i, j, k + 1) - g(i, j, k - 1))
+                nbr, w = [], []
+                for di in range(i0, i1 + 1):
+                    for dj in range(j0, j1 + 1):
+                        for dk in range(k0, k1 + 1):
+                            if di == 0 and dj == 0 and dk == 0:
+                                continue
+                            gn = g(i + di, j + dj, k + dk)
+                            if gn >= 0 or gn > g(i, j, k):
+                                ddx, ddy, ddz = float(di) * hx, float(dj) * hy, float(dk) * hz
+                                nbr.append(((i + di) * jmax + j + dj) * kmax + k + dk)
+                                w.append(abs(ddx * gx + ddy * gy + ddz * gz) / math.sqrt(ddx * ddx + ddy * ddy + ddz * ddz))
+                inside.append(((i * jmax + j) * kmax + k, nbr, w))
+    return below, inside
+
+
+def oracle_levelset_gpu_apply(U, Un, setup, receivers=()):
+    """GPU_CartesianLevelSetBC::operator() after a stage (in place on U):
+    the deactivated cells hold the step-start state Un, as the reference's
+    GPU advance kernel leaves inactive cells (gpu_cartesianiterator.h:199-205),
+    except cells a donor copy writes (`receivers`); then every inside cell
+    with neighbours takes their weighted mean, all read before any is written
+    (the reference writes field 2 and copies it back)."""
+    below, inside = setup
+    u = U.reshape(5, -1)
+    un = Un.reshape(5, -1)
+    rec = set(int(x) for x in receivers)
+    for c in below:
+        if c not in rec:
+            u[:, c] = un[:, c]
+    out = []
+    for c, nbr, w in inside:
+        if not nbr:
+            continue
+        var = np.zeros(5)
+        total = 0.0
+        for n, wt in zip(nbr, w):
+            total += wt
+            var = var + wt * u[:, n]
+        out.append((c, var / total))
+    for c, v in out:
+        if not np.isfinite(v).all():
+            raise FloatingPointError("inside-cell average not finite")
+        u[:, c] = v
