@@ -113,9 +113,11 @@ struct dn_ctx {
   bool batch_dirty = true;
   void* d_records = nullptr;
   void* d_maps = nullptr;                     // FX32 batched: dn::BatchMaps per patch
-  void* d_items[2][dn::kNumShapes] = {};      // FX32: [0] edge tiles, [1] full tiles; FP64: all in [0]
-  int n_items[2][dn::kNumShapes] = {};
-  cudaStream_t s_aux = nullptr;               // second branch of a batched stage (edge tiles)
+  // work items per tile form (dn::kFxEdge, kFxInside, kFxFull; FP64: all in
+  // [kFxEdge]) and tile shape
+  void* d_items[3][dn::kNumShapes] = {};
+  int n_items[3][dn::kNumShapes] = {};
+  cudaStream_t s_aux = nullptr;               // second branch of a batched stage (edge and inside tiles)
   int batch_min_planes = 8;                   // shortest plane range of a batched work item (autotuned)
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   // CUDA graphs of whole RK steps; any change of the case bumps generation
@@ -899,7 +901,7 @@ void free_batch(dn_ctx* c)
   c->d_records = nullptr;
   if (c->d_maps) cudaFree(c->d_maps);
   c->d_maps = nullptr;
-  for (int f = 0; f < 2; ++f) {
+  for (int f = 0; f < 3; ++f) {
     for (int q = 0; q < dn::kNumShapes; ++q) {
       if (c->d_items[f][q]) cudaFree(c->d_items[f][q]);
       c->d_items[f][q] = nullptr;
@@ -969,10 +971,11 @@ int build_batch(dn_ctx* c)
   const long want = (long)c->num_sms * 2 * 4;
   long chunks = (want + tiles - 1) / tiles;
   if (chunks < 1) chunks = 1;
-  // FX32 items of tiles whose every y/z slope and face exists (the tile
-  // form without edge tests, fx_tile_full) go to their own list: a launch
-  // per form keeps one code path per kernel
-  std::vector<dn::WorkItem> items[2][dn::kNumShapes];
+  // FX32 items go to one list per tile form: full tiles (every y/z slope
+  // and face exists: no edge test), tiles inside the patch next to a closed
+  // face (per-thread face masks), tiles that reach beyond the patch; a
+  // launch per form keeps one code path per kernel
+  std::vector<dn::WorkItem> items[3][dn::kNumShapes];
   for (size_t q = 0; q < np; ++q) {
     const DnPatch& P = c->patches[q];
     if (!P.owned || !P.patch_active) continue;
@@ -988,7 +991,8 @@ int build_batch(dn_ctx* c)
         for (int k0 = 0; k0 < P.d.nk; k0 += tk) {
           const bool fy = (j0 + tj <= P.d.nj) && (per_y || (j0 >= 2 && j0 + tj + 2 <= P.d.nj));
           const bool fz = (k0 + tk <= P.d.nk) && (per_z || (k0 >= 2 && k0 + tk + 2 <= P.d.nk));
-          const int form = (!fp64 && fy && fz) ? 1 : 0;
+          const bool inside = j0 + tj <= P.d.nj && k0 + tk <= P.d.nk;
+          const int form = fp64 ? dn::kFxEdge : (fy && fz) ? dn::kFxFull : inside ? dn::kFxInside : dn::kFxEdge;
           items[form][sh].push_back(dn::WorkItem{(int)q, j0, k0, i0, std::min(P.d.ni, i0 + (int)ic)});
         }
   }
@@ -1002,7 +1006,7 @@ int build_batch(dn_ctx* c)
     e = cudaMemcpyAsync(c->d_maps, maps.data(), np * sizeof(dn::BatchMaps), cudaMemcpyHostToDevice, c->stream);
     if (e != cudaSuccess) return cuda_fail(c, e, "tensor map upload");
   }
-  for (int f = 0; f < 2; ++f) {
+  for (int f = 0; f < 3; ++f) {
     for (int q = 0; q < dn::kNumShapes; ++q) {
       const std::vector<dn::WorkItem>& it = items[f][q];
       if (it.empty()) continue;
@@ -1054,13 +1058,14 @@ int stage_all(dn_ctx* c, int in_b, int un_b, int out_b, double factor)
     return DN_OK;
   }
   if (c->batch_dirty && (s = build_batch(c))) return s;
-  // full-tile launches on the context's stream, edge-tile launches on a
-  // second branch forked from it and joined after (they write disjoint
-  // tiles), so the two forms overlap instead of queueing behind each other
+  // full-tile launches on the context's stream, inside- and edge-tile
+  // launches on a second branch forked from it and joined after (they write
+  // disjoint tiles), so the forms overlap instead of queueing behind each
+  // other
   bool any_edge = false, any_full = false;
   for (int q = 0; q < dn::kNumShapes; ++q) {
-    any_edge = any_edge || c->n_items[0][q] > 0;
-    any_full = any_full || c->n_items[1][q] > 0;
+    any_edge = any_edge || c->n_items[dn::kFxEdge][q] > 0 || c->n_items[dn::kFxInside][q] > 0;
+    any_full = any_full || c->n_items[dn::kFxFull][q] > 0;
   }
   const bool fork = any_edge && any_full;
   cudaError_t e = cudaSuccess;
@@ -1075,8 +1080,8 @@ int stage_all(dn_ctx* c, int in_b, int un_b, int out_b, double factor)
     if (e == cudaSuccess) e = cudaStreamWaitEvent(c->s_aux, c->ev_fork, 0);
     if (e != cudaSuccess) return cuda_fail(c, e, "stage branch fork");
   }
-  for (int f = 1; f >= 0; --f) {
-    cudaStream_t st = (fork && f == 0) ? c->s_aux : c->stream;
+  for (int f = dn::kFxFull; f >= dn::kFxEdge; --f) {
+    cudaStream_t st = (fork && f != dn::kFxFull) ? c->s_aux : c->stream;
     for (int q = 0; q < dn::kNumShapes; ++q) {
       if (!c->n_items[f][q]) continue;
       dn::Batch b;
@@ -1089,7 +1094,7 @@ int stage_all(dn_ctx* c, int in_b, int un_b, int out_b, double factor)
       b.err = c->d_err;
       b.err_info = c->d_err_info;
       e = c->precision == DN_FP64 ? dn::launch_stage_f64_batched(b, q, st)
-                                  : dn::launch_stage_fx32_batched(b, q, f == 1, st);
+                                  : dn::launch_stage_fx32_batched(b, q, f, st);
       c->launches++;
       if (e != cudaSuccess) return cuda_fail(c, e, "batched stage launch");
     }

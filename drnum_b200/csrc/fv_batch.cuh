@@ -63,13 +63,14 @@ __device__ __forceinline__ void load_patch_record(BatchPatch& dst, const BatchPa
   for (int w = t; w < (int)(sizeof(BatchPatch) / 4); w += nt) d[w] = s[w];
 }
 
-// FULL = false: every item runs the tile form with edge tests; FULL = true:
-// the items' tiles are full (the host sorts them so), run by the form
-// without edge tests (the device re-checks each tile and falls back).  One
-// form per kernel keeps one code path per launch: both forms in one kernel
-// made them compete for the instruction cache of an SM running tiles of many
-// patches (13-17 % slower on the jet and sphere workloads).
-template <int TJ, int TK, bool FULL>
+// MODE (kFxEdge, kFxInside, kFxFull): the tile form every item of the
+// launch runs; the host sorts the items by form (fx_tile_full,
+// fx_tile_inside), and the device re-checks each tile and falls back to the
+// edge form.  One form per kernel keeps one code path per launch: several
+// forms in one kernel made them compete for the instruction cache of an SM
+// running tiles of many patches (13-17 % slower on the jet and sphere
+// workloads).
+template <int TJ, int TK, int MODE>
 __global__ void __launch_bounds__(TJ * TK / 2, FxOccupancy<TJ * TK / 2>::min_blocks)
 fx_stage_batched(const Batch b)
 {
@@ -95,10 +96,12 @@ fx_stage_batched(const Batch b)
   const BatchMaps* M = (b.maps && rec.tma) ? b.maps + w.patch : nullptr;
   const CUtensorMap* tm_in = M ? M->in[b.in_b] : nullptr;
   const CUtensorMap* tm_un = M ? &M->un[b.un_b] : nullptr;
-  if (FULL && fx_tile_full<TJ, TK>(args.g, w.j0, w.k0))
-    fx_stage_tile_impl<TJ, TK, true>(args, tm_in, tm_un, w.j0, w.k0, w.i0, w.i1);
+  if (MODE == kFxFull && fx_tile_full<TJ, TK>(args.g, w.j0, w.k0))
+    fx_stage_tile_impl<TJ, TK, kFxFull>(args, tm_in, tm_un, w.j0, w.k0, w.i0, w.i1);
+  else if (MODE == kFxInside && fx_tile_inside<TJ, TK>(args.g, w.j0, w.k0))
+    fx_stage_tile_impl<TJ, TK, kFxInside>(args, tm_in, tm_un, w.j0, w.k0, w.i0, w.i1);
   else
-    fx_stage_tile_impl<TJ, TK, false>(args, tm_in, tm_un, w.j0, w.k0, w.i0, w.i1);
+    fx_stage_tile_impl<TJ, TK, kFxEdge>(args, tm_in, tm_un, w.j0, w.k0, w.i0, w.i1);
 }
 
 template <int TJ, int TK>

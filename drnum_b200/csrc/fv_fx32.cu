@@ -60,30 +60,32 @@ cudaError_t launch_stage_fx32(const FxArgs& a, cudaStream_t st)
 void fx32_tile(int* tj, int* tk) { *tj = FX_TJ; *tk = FX_TK; }
 
 namespace {
-template <int TJ, int TK, bool FULL>
+template <int TJ, int TK, int MODE>
 cudaError_t launch_fx_batched(const Batch& b, cudaStream_t st)
 {
   using Smem = FxSmem<TJ, TK>;
-  auto kern = fx_stage_batched<TJ, TK, FULL>;
+  auto kern = fx_stage_batched<TJ, TK, MODE>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(Smem));
   if (e != cudaSuccess) return e;
   kern<<<b.n_items, dim3(TK / 2, TJ, 1), sizeof(Smem), st>>>(b);
   return cudaGetLastError();
 }
 
-template <bool FULL>
+template <int MODE>
 cudaError_t launch_fx_batched_shape(const Batch& b, int shape, cudaStream_t st)
 {
-  if (shape == 0) return launch_fx_batched<8, 32, FULL>(b, st);
-  if (shape == 1) return launch_fx_batched<16, 16, FULL>(b, st);
-  return launch_fx_batched<16, 32, FULL>(b, st);
+  if (shape == 0) return launch_fx_batched<8, 32, MODE>(b, st);
+  if (shape == 1) return launch_fx_batched<16, 16, MODE>(b, st);
+  return launch_fx_batched<16, 32, MODE>(b, st);
 }
 } // namespace
 
-cudaError_t launch_stage_fx32_batched(const Batch& b, int shape, bool full, cudaStream_t st)
+cudaError_t launch_stage_fx32_batched(const Batch& b, int shape, int form, cudaStream_t st)
 {
   if (b.n_items <= 0) return cudaSuccess;
-  return full ? launch_fx_batched_shape<true>(b, shape, st) : launch_fx_batched_shape<false>(b, shape, st);
+  if (form == kFxFull) return launch_fx_batched_shape<kFxFull>(b, shape, st);
+  if (form == kFxInside) return launch_fx_batched_shape<kFxInside>(b, shape, st);
+  return launch_fx_batched_shape<kFxEdge>(b, shape, st);
 }
 
 int default_i_chunk(int ni, int nj, int nk, int tj, int tk, int num_sms, int ctas_per_sm)

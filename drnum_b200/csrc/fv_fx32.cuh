@@ -137,15 +137,6 @@ __device__ __forceinline__ float2 sqrt2(float2 a) { return make_float2(sqrtf(a.x
 __device__ __forceinline__ float2 max0(float2 a) { return make_float2(fmaxf(a.x, 0.0f), fmaxf(a.y, 0.0f)); }
 __device__ __forceinline__ float2 min0(float2 a) { return make_float2(fminf(a.x, 0.0f), fminf(a.y, 0.0f)); }
 
-// max that propagates NaN (PTX max.NaN.f32): a face flux that is not finite
-// makes the running maximum NaN
-__device__ __forceinline__ float fmax_nan(float a, float b)
-{
-  float d;
-  asm("max.NaN.f32 %0, %1, %2;" : "=f"(d) : "f"(a), "f"(b));
-  return d;
-}
-
 // Primitive face-side state (COMPRESSIBLE_*_VARS) of a pair: density,
 // velocity, pressure, speed of sound and total enthalpy.  p = rho R T with
 // T = (rE/rho - |u|^2/2)/cv, written as p = (R/cv) (rE - rho|u|^2/2).
@@ -236,22 +227,20 @@ __device__ __forceinline__ float2 fx_slope2(float2 a, float2 b)
 }
 
 // Range of the face fluxes (in quanta) a thread has converted: the largest
-// and smallest value, NaN once a flux is not finite (PTX max.NaN / min.NaN,
-// three inputs).
+// magnitude, NaN once a flux is not finite (PTX max.NaN, three inputs; the
+// absolute values fold into the operands).
 struct FaceRange {
-  float hi = 0.0f, lo = 0.0f;
+  float hi = 0.0f;
   __device__ __forceinline__ void add2(float a, float b)
   {
-    asm("max.NaN.f32 %0, %1, %2, %3;" : "=f"(hi) : "f"(hi), "f"(a), "f"(b));
-    asm("min.NaN.f32 %0, %1, %2, %3;" : "=f"(lo) : "f"(lo), "f"(a), "f"(b));
+    asm("max.NaN.f32 %0, %1, %2, %3;" : "=f"(hi) : "f"(hi), "f"(fabsf(a)), "f"(fabsf(b)));
   }
   __device__ __forceinline__ void add(const FaceRange& o)
   {
     asm("max.NaN.f32 %0, %1, %2;" : "=f"(hi) : "f"(hi), "f"(o.hi));
-    asm("min.NaN.f32 %0, %1, %2;" : "=f"(lo) : "f"(lo), "f"(o.lo));
   }
   // largest magnitude (NaN if any flux was not finite)
-  __device__ __forceinline__ float mag() const { return fmax_nan(hi, -lo); }
+  __device__ __forceinline__ float mag() const { return hi; }
 };
 
 // A pair of face fluxes in whole quanta, recorded in r.  A face of 2^30
@@ -361,6 +350,21 @@ __device__ __forceinline__ bool fx_tile_full(const FxGeom& g, int j0, int k0)
   return fy && fz;
 }
 
+// Is every own cell of the tile inside the patch?  Such tiles that are not
+// full lie next to a closed patch face: their faces on that patch face do
+// not exist and their halo there repeats the edge cell, but every thread
+// owns both cells of its pair.
+template <int TJ, int TK>
+__device__ __forceinline__ bool fx_tile_inside(const FxGeom& g, int j0, int k0)
+{
+  return j0 + TJ <= g.nj && k0 + TK <= g.nk;
+}
+
+// Forms of the tile function: tiles that reach beyond the patch (every test
+// per cell), tiles inside the patch next to a closed face (face masks per
+// thread, clamped halo pairs), full tiles (no test).
+constexpr int kFxEdge = 0, kFxInside = 1, kFxFull = 2;
+
 // Device error bit of a TMA transfer that did not complete within the
 // bounded wait.
 constexpr int kFxErrTma = 32;
@@ -414,10 +418,12 @@ __device__ __forceinline__ void fx_stage_slot(const FxGeom& g, bool tma, int j0,
 // tm_in: the kFxMaps tensor maps of the stage input, tm_un: the map of f(n)
 // (box TK x TJ x 1 x 5), or null.  With maps, a tile stages its planes by
 // TMA box loads unless fx_seam excludes it; other tiles copy cell by cell.
-// FULL tiles (fx_tile_full) skip every edge test, and their ring positions
-// come in adjacent pairs in every staging form (no clamping; a periodic seam
-// falls between pairs), so they dequantise pairwise.
-template <int TJ, int TK, bool FULL>
+// MODE kFxFull tiles (fx_tile_full) skip every edge test, and their ring
+// positions come in adjacent pairs in every staging form (no clamping; a
+// periodic seam falls between pairs), so they dequantise pairwise.  MODE
+// kFxInside tiles (fx_tile_inside) dequantise pairwise too: a pair whose two
+// positions clamp to one edge cell of a closed k axis reads that cell twice.
+template <int TJ, int TK, int MODE>
 __device__ __forceinline__ void fx_stage_tile_impl(const FxArgs& a, const CUtensorMap* tm_in,
                                                    const CUtensorMap* tm_un, int j0, int k0, int i0, int i1)
 {
@@ -429,6 +435,8 @@ __device__ __forceinline__ void fx_stage_tile_impl(const FxArgs& a, const CUtens
   constexpr int PPT2 = (NPP + NT - 1) / NT;       // position pairs per thread
   static_assert(TK % 4 == 0 && TJ % 2 == 0 && TP <= 32 && TJ / 2 <= 32 && NT >= 64 && TK + TJ <= NT,
                 "tile shape");
+  constexpr bool FULL = MODE == kFxFull;
+  constexpr bool PAIRS = MODE != kFxEdge;         // own pairs inside the patch, pairwise dequantisation
   extern __shared__ __align__(128) unsigned char fx_smem_raw[];
   Smem& sm = *reinterpret_cast<Smem*>(fx_smem_raw);
 
@@ -438,8 +446,8 @@ __device__ __forceinline__ void fx_stage_tile_impl(const FxArgs& a, const CUtens
   const int tid = ty * TP + tp;
   const int kk = 2 * tp;                          // tile column of the pair's first cell
   const int j = j0 + ty, ka = k0 + kk, kb = ka + 1;
-  const bool own_a = FULL || ((j < g.nj) && (ka < g.nk));
-  const bool own_b = FULL || ((j < g.nj) && (kb < g.nk));
+  const bool own_a = PAIRS || ((j < g.nj) && (ka < g.nk));
+  const bool own_b = PAIRS || ((j < g.nj) && (kb < g.nk));
   const int njk = g.nj * g.kp;                    // plane stride (rows of kp elements)
   const int nc = g.ni * njk;                      // variable stride (5 * nc < 2^31, host check)
   // TMA boxes start at x = k0-4 (main; a multiple of 4 int32 since TK is),
@@ -467,10 +475,12 @@ __device__ __forceinline__ void fx_stage_tile_impl(const FxArgs& a, const CUtens
   // per-thread staging positions: single positions e = tid + m*NT in ring
   // order [row][column] with the in-plane offset j*kp + k of their (wrapped
   // or clamped) cell for cell copies; the edge form also keeps their
-  // staging slots, the FULL form the staging slots of position pairs
+  // staging slots, the pair forms the staging slots of position pairs (bit
+  // m of `dup`: pair m reads one clamped edge cell for both positions)
   int32_t poff[PPT];
-  int32_t soff[FULL ? PPT2 : PPT];
-  int32_t svar[FULL ? PPT2 : PPT];
+  int32_t soff[PAIRS ? PPT2 : PPT];
+  int32_t svar[PAIRS ? PPT2 : PPT];
+  unsigned dup = 0;
   #pragma unroll
   for (int m = 0; m < PPT; ++m) {
     const int e = tid + m * NT;
@@ -478,16 +488,25 @@ __device__ __forceinline__ void fx_stage_tile_impl(const FxArgs& a, const CUtens
     if (e < NP) {
       const int jj = e / PK, c = e % PK;
       poff[m] = fx_index(j0 - 2 + jj, g.nj, g.per_y) * g.kp + fx_index(k0 - 2 + c, g.nk, g.per_z);
-      if (!FULL) fx_stage_slot<TJ, TK>(g, tma, j0, k0, jj, c, &soff[m], &svar[m]);
+      if (!PAIRS) fx_stage_slot<TJ, TK>(g, tma, j0, k0, jj, c, &soff[m], &svar[m]);
     }
   }
-  if (FULL) {
+  if (PAIRS) {
     #pragma unroll
     for (int m = 0; m < PPT2; ++m) {
       const int e = tid + m * NT;
       soff[m] = 0;
       svar[m] = 0;
-      if (e < NPP) fx_stage_slot<TJ, TK>(g, tma, j0, k0, e / (PK / 2), 2 * (e % (PK / 2)), &soff[m], &svar[m]);
+      if (e < NPP) {
+        const int jj = e / (PK / 2), c = 2 * (e % (PK / 2));
+        fx_stage_slot<TJ, TK>(g, tma, j0, k0, jj, c, &soff[m], &svar[m]);
+        if (MODE == kFxInside) {
+          // the second position reads the same slot (a clamped edge cell) or the next one
+          int s1, v1;
+          fx_stage_slot<TJ, TK>(g, tma, j0, k0, jj, c + 1, &s1, &v1);
+          if (s1 == soff[m]) dup |= 1u << m;
+        }
+      }
     }
   }
 
@@ -533,8 +552,10 @@ __device__ __forceinline__ void fx_stage_tile_impl(const FxArgs& a, const CUtens
   // the staging area, dequantised into ring slot sl
   auto dequant_stage = [&](int sl) {
     const int* q = &sm.stage[0];
-    if (FULL) {
-      // pair e of a ring slot starts at float 2e of its variable's plane
+    if (PAIRS) {
+      // pair e of a ring slot starts at float 2e of its variable's plane;
+      // a pair of two positions starts on an even slot (8-byte aligned), a
+      // clamped pair reads its one cell from the aligned word holding it
       float2* f = reinterpret_cast<float2*>(&sm.plane[sl][0][0][0]);
       #pragma unroll
       for (int v = 0; v < 5; ++v) {
@@ -542,7 +563,11 @@ __device__ __forceinline__ void fx_stage_tile_impl(const FxArgs& a, const CUtens
         for (int m = 0; m < PPT2; ++m) {
           const int e = tid + m * NT;
           if (e < NPP) {
-            const int2 o = *reinterpret_cast<const int2*>(q + soff[m] + v * svar[m]);
+            int2 o = *reinterpret_cast<const int2*>(q + (soff[m] & ~1) + v * svar[m]);
+            if (MODE == kFxInside && ((dup >> m) & 1u)) {
+              const int x = (soff[m] & 1) ? o.y : o.x;
+              o = make_int2(x, x);
+            }
             f[v * NPP + e] = fma2(P.quantum[v], make_float2((float)o.x, (float)o.y), P.base[v]);
           }
         }
@@ -751,9 +776,9 @@ __device__ __forceinline__ void fx_stage_tile_impl(const FxArgs& a, const CUtens
       fx_ausm2<1>(fx_prim2(L[0], L[1], L[2], L[3], L[4]), fx_prim2(ym[0], ym[1], ym[2], ym[3], ym[4]), P.A[1], F);
       bool exa = true, exb = true;
       if (!FULL) {
-        const bool ey = fx_face_exists(j, g.nj, g.per_y) && (g.per_y || j < g.nj);
-        exa = ey && ka < g.nk;
-        exb = ey && kb < g.nk;
+        const bool ey = fx_face_exists(j, g.nj, g.per_y) && (PAIRS || g.per_y || j < g.nj);
+        exa = ey && (PAIRS || ka < g.nk);
+        exb = ey && (PAIRS || kb < g.nk);
       }
       #pragma unroll
       for (int v = 0; v < 5; ++v) {
@@ -772,9 +797,9 @@ __device__ __forceinline__ void fx_stage_tile_impl(const FxArgs& a, const CUtens
       fx_ausm2<2>(fx_prim2(L[0], L[1], L[2], L[3], L[4]), fx_prim2(zm[0], zm[1], zm[2], zm[3], zm[4]), P.A[2], F);
       bool exa = true, exb = true;
       if (!FULL) {
-        const bool rowin = j < g.nj;
-        exa = rowin && fx_face_exists(ka, g.nk, g.per_z) && (g.per_z || ka < g.nk);
-        exb = rowin && fx_face_exists(kb, g.nk, g.per_z) && (g.per_z || kb < g.nk);
+        const bool rowin = PAIRS || j < g.nj;
+        exa = rowin && fx_face_exists(ka, g.nk, g.per_z) && (PAIRS || g.per_z || ka < g.nk);
+        exb = rowin && fx_face_exists(kb, g.nk, g.per_z) && (PAIRS || g.per_z || kb < g.nk);
       }
       #pragma unroll
       for (int v = 0; v < 5; ++v) {
@@ -802,8 +827,8 @@ __device__ __forceinline__ void fx_stage_tile_impl(const FxArgs& a, const CUtens
         if (!FULL) {
           const int jf = j0 + TJ;
           const bool ey = fx_face_exists(jf, g.nj, g.per_y) && (g.per_y || jf < g.nj);
-          exa = ey && k0 + c < g.nk;
-          exb = ey && k0 + c + 1 < g.nk;
+          exa = ey && (PAIRS || k0 + c < g.nk);
+          exb = ey && (PAIRS || k0 + c + 1 < g.nk);
         }
         #pragma unroll
         for (int v = 0; v < 5; ++v) {
@@ -826,8 +851,8 @@ __device__ __forceinline__ void fx_stage_tile_impl(const FxArgs& a, const CUtens
         if (!FULL) {
           const int kz = k0 + TK;
           const bool ez = fx_face_exists(kz, g.nk, g.per_z) && (g.per_z || kz < g.nk);
-          exa = ez && j0 + ja < g.nj;
-          exb = ez && j0 + jb < g.nj;
+          exa = ez && (PAIRS || j0 + ja < g.nj);
+          exb = ez && (PAIRS || j0 + jb < g.nj);
         }
         #pragma unroll
         for (int v = 0; v < 5; ++v) {
@@ -950,28 +975,35 @@ __device__ __forceinline__ void fx_stage_tile_impl(const FxArgs& a, const CUtens
           o[v].y = (int)(ob >= kFxLimit ? kFxLimit : (ob <= -kFxLimit ? -kFxLimit : ob));
         }
       }
-      int bad = 0;
+      // offsets outside (-kFxLimit, kFxLimit): bit 2v (cell a) or 2v+1
+      // (cell b) of `bad`, without a branch per variable
+      unsigned bad = 0;
       #pragma unroll
       for (int v = 0; v < 5; ++v) {
         if (!act_a) o[v].x = a.in[v * nc + c];
         if (!act_b) o[v].y = own_b ? a.in[v * nc + c + 1] : 0;
-        const bool ba = act_a && (o[v].x >= kFxLimit || o[v].x <= -kFxLimit);
-        const bool bb = act_b && (o[v].y >= kFxLimit || o[v].y <= -kFxLimit);
-        if (ba || bb) {
-          bad |= 1;
-          const int q = ba ? 0 : 1;
-          const int2 un = *reinterpret_cast<const int2*>(&sm.un[v][ty][kk]);
-          const int u = q == 0 ? un.x : un.y;
-          if (a.err_info && atomicCAS(&a.err_info[0], ~0ull, (unsigned long long)(c + q)) == ~0ull) {
-            a.err_info[1] = (unsigned long long)v;
-            a.err_info[2] = (unsigned long long)__double_as_longlong((double)u);
-            a.err_info[3] = (unsigned long long)__double_as_longlong((double)((long long)(q == 0 ? o[v].x : o[v].y) - u));
-          }
-        }
+        const bool ba = act_a && (unsigned)o[v].x + (unsigned)(kFxLimit - 1) > 2u * (unsigned)(kFxLimit - 1);
+        const bool bb = act_b && (unsigned)o[v].y + (unsigned)(kFxLimit - 1) > 2u * (unsigned)(kFxLimit - 1);
+        bad |= (ba ? 1u : 0u) << (2 * v);
+        bad |= (bb ? 2u : 0u) << (2 * v);
         if (own_b) *reinterpret_cast<int2*>(a.out + v * nc + c) = o[v];
         else a.out[v * nc + c] = o[v].x;
       }
-      if (bad && a.err) atomicOr(a.err, bad);
+      if (bad) {
+        // the first failing (variable, cell) of this pair is recorded
+        const int bit = __ffs(bad) - 1, v = bit >> 1, q = bit & 1;
+        const int2 un = *reinterpret_cast<const int2*>(&sm.un[v][ty][kk]);
+        const int u = q == 0 ? un.x : un.y;
+        int ov = o[0].x;
+        #pragma unroll
+        for (int w = 0; w < 5; ++w) if (w == v) ov = q == 0 ? o[w].x : o[w].y;
+        if (a.err_info && atomicCAS(&a.err_info[0], ~0ull, (unsigned long long)(c + q)) == ~0ull) {
+          a.err_info[1] = (unsigned long long)v;
+          a.err_info[2] = (unsigned long long)__double_as_longlong((double)u);
+          a.err_info[3] = (unsigned long long)__double_as_longlong((double)((long long)ov - u));
+        }
+        if (a.err) atomicOr(a.err, 1);
+      }
     }
     #pragma unroll
     for (int v = 0; v < 5; ++v) qx_lo[v] = qx_hi[v];
@@ -1002,8 +1034,10 @@ template <int TJ, int TK>
 __device__ __forceinline__ void fx_stage_tile(const FxArgs& a, const CUtensorMap* tm_in, const CUtensorMap* tm_un,
                                               int j0, int k0, int i0, int i1)
 {
-  if (fx_tile_full<TJ, TK>(a.g, j0, k0)) fx_stage_tile_impl<TJ, TK, true>(a, tm_in, tm_un, j0, k0, i0, i1);
-  else fx_stage_tile_impl<TJ, TK, false>(a, tm_in, tm_un, j0, k0, i0, i1);
+  if (fx_tile_full<TJ, TK>(a.g, j0, k0)) fx_stage_tile_impl<TJ, TK, kFxFull>(a, tm_in, tm_un, j0, k0, i0, i1);
+  else if (fx_tile_inside<TJ, TK>(a.g, j0, k0))
+    fx_stage_tile_impl<TJ, TK, kFxInside>(a, tm_in, tm_un, j0, k0, i0, i1);
+  else fx_stage_tile_impl<TJ, TK, kFxEdge>(a, tm_in, tm_un, j0, k0, i0, i1);
 }
 
 // Parameters of the single-patch launch: the stage arguments and the tensor

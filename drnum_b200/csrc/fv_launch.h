@@ -39,7 +39,8 @@ struct Batch;
 constexpr int kNumShapes = 3;
 // full: every item's tile is full (fx_tile_full), run by the tile form
 // without edge tests
-cudaError_t launch_stage_fx32_batched(const Batch& b, int shape, bool full, cudaStream_t st);
+// form: kFxEdge, kFxInside or kFxFull (the tile form of every item of b)
+cudaError_t launch_stage_fx32_batched(const Batch& b, int shape, int form, cudaStream_t st);
 cudaError_t launch_stage_f64_batched(const Batch& b, int shape, cudaStream_t st);
 inline void shape_tile(bool fp64, int shape, int* tj, int* tk)
 {

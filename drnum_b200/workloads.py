@@ -2,7 +2,7 @@
 
     jet     dual-resolution jet: a 192 x 96 x 96 core patch at h nested at the
             inlet of a box tiled by seven patches at 2h (64 to 128 cells per
-            axis), 3-cell overlaps, Mach 0.8 top-hat jet (radius 0.05, seeded
+            axis, their 3-cell overlaps included), Mach 0.8 top-hat jet (radius 0.05, seeded
             1e-3 white noise) on the core's x-min face, far field at rest
             elsewhere
     sphere  level-set wall: 256 x 128 x 128 cells over [0, 2] x [0, 1]^2 in two
@@ -32,7 +32,11 @@ def build(name, scale=1.0):
     scale < 1 shrinks the case (for tests)."""
     if name == "jet":
         core = tuple(max(8, int(round(x * scale)) // 4 * 4) for x in (192, 96, 96))
-        box = tuple(max(16, int(round(x * scale)) // 4 * 4) for x in (128, 256, 256))
+        # the seven coarse patches span 64 (x halves) and 128 (y, z halves)
+        # cells including their 3-cell overlaps: the box is twice that less
+        # the overlap (122 x 250 x 250 cells at full size)
+        nx, ny = (max(12, int(round(x * scale / 4)) * 4) for x in (64, 128))
+        box = (2 * (nx - 3), 2 * (ny - 3), 2 * (ny - 3))
         patches = cases.jet_grid(core=core, box=box)
         states = cases.uniform_state(patches, mach=0.0)
         bcs = cases.jet_bcs(patches, radius=0.05, noise=1e-3, seed=1234)
@@ -40,7 +44,7 @@ def build(name, scale=1.0):
         dt = 0.5 * h / ((0.8 + 1.0) * cases.A_INF)
         desc = (f"dual-resolution jet: 8 overlapping patches, core {core[0]}x{core[1]}x{core[2]} at h=1/{2 * box[0]} "
                 f"nested at the inlet of a {box[0]}x{box[1]}x{box[2]}-cell box at 2h tiled by seven patches of "
-                f"{box[0] // 2}-{box[0]} cells per axis, 3-cell overlaps, Mach 0.8 top-hat jet r=0.05 + 1e-3 seeded "
+                f"{nx}-{ny} cells per axis (3-cell overlaps included), Mach 0.8 top-hat jet r=0.05 + 1e-3 seeded "
                 "noise, far field at rest")
         return dict(patches=patches, states=states, bcs=bcs, levelset=None, dt=dt, description=desc)
     if name == "sphere":

@@ -31,16 +31,14 @@ def test_tiled_workload_full_size_layout():
 
 
 def test_jet_workload_full_size_layout():
-    # core 192 x 96 x 96 at h; seven patches at 2h of 64..128 cells per axis
-    # (plus their 3-cell overlaps)
+    # core 192 x 96 x 96 at h; seven patches at 2h of 64..128 cells per axis,
+    # their 3-cell overlaps included
     patches = workloads.build("jet")["patches"]
     assert len(patches) == 8 and patches[0]["n"] == (192, 96, 96)
     h = patches[0]["length"][0] / 192
     for p in patches[1:]:
         assert abs(p["length"][0] / p["n"][0] - 2 * h) < 1e-15
-        for a in range(3):
-            inner = p["n"][a] - 3 * ((p["seek"][2 * a] > 0) + (p["seek"][2 * a + 1] > 0))
-            assert 64 <= inner <= 128, p
+        assert all(64 <= x <= 128 for x in p["n"]), p
     cells = sum(int(np.prod(p["n"])) for p in patches)
     assert 10e6 < cells < 13e6
 
