@@ -134,6 +134,9 @@ SIGNATURES = {
     "dn_grid_write": (c_int, [ctypes.c_char_p, c_int, POINTER(dn_patch_desc), POINTER(ctypes.c_char_p)]),
     "dn_write_data": (c_int, [c_void_p, c_int, ctypes.c_char_p, c_double, c_int]),
     "dn_patch_set_owned": (c_int, [c_void_p, c_int, c_int]),
+    "dn_patch_add_shadow": (c_int, [c_void_p, POINTER(dn_patch_desc), POINTER(c_int)]),
+    "dn_shadow_alloc": (c_int, [c_void_p, c_void_p]),
+    "dn_patch_device_cells": (c_int, [c_void_p, c_int, POINTER(c_int64)]),
     "dn_patch_upload_async": (c_int, [c_void_p, c_int, c_int, POINTER(c_double)]),
     "dn_patch_upload_f32_async": (c_int, [c_void_p, c_int, c_int, POINTER(c_float)]),
     "dn_patch_download_async": (c_int, [c_void_p, c_int, c_int, POINTER(c_double)]),

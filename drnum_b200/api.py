@@ -291,6 +291,7 @@ class B200CartesianIterator:
             check(self.ctx, self.lib.dn_set_flux_scheme(self.ctx, int(self.m_Op.scheme)))
         self.m_Patches: list[CartesianPatch] = []
         self.m_PatchActive: list[bool] = []
+        self.m_Shadow: list[bool] = []
 
     def __del__(self):
         ctx = getattr(self, "ctx", None)
@@ -302,13 +303,27 @@ class B200CartesianIterator:
         self.__del__()
 
     # PatchIterator interface (patchiterator.h:43-54)
-    def addPatch(self, patch: CartesianPatch) -> int:
+    def addPatch(self, patch: CartesianPatch, shadow=False) -> int:
+        """Adds a patch; shadow=True adds another rank's patch as a compact
+        shadow (dn_patch_add_shadow: no field memory until dn_shadow_alloc
+        gives it the donor cells this rank receives; see shard.py)."""
         pid = ctypes.c_int()
         d = patch.desc()
-        check(self.ctx, self.lib.dn_patch_add(self.ctx, ctypes.byref(d), ctypes.byref(pid)))
+        add = self.lib.dn_patch_add_shadow if shadow else self.lib.dn_patch_add
+        check(self.ctx, add(self.ctx, ctypes.byref(d), ctypes.byref(pid)))
         self.m_Patches.append(patch)
         self.m_PatchActive.append(True)
+        self.m_Shadow.append(bool(shadow))
         return pid.value
+
+    def isShadow(self, i):
+        return self.m_Shadow[i]
+
+    def deviceCells(self, i):
+        """Cells per variable patch i holds on the device (dn_patch_device_cells)."""
+        n = ctypes.c_int64()
+        check(self.ctx, self.lib.dn_patch_device_cells(self.ctx, int(i), ctypes.byref(n)))
+        return n.value
 
     def numPatches(self):
         return len(self.m_Patches)
@@ -355,6 +370,16 @@ class B200CartesianIterator:
             check(self.ctx, self.lib.dn_patch_set_donors(self.ctx, pid, _lib.ptr(counts, ctypes.c_int64),
                                                          *[_lib.ptr(a, ct) for a, ct in zip(args, types)]))
 
+    def setDonorTablesOf(self, i_patch, t):
+        """Hands donor tables built elsewhere to patch i_patch
+        (dn_patch_set_donors): a dict in the layout of donorTables(), donor
+        patches given as this iterator's patch ids."""
+        counts = np.ascontiguousarray(t["counts"], dtype=np.int64)
+        arrs = [np.ascontiguousarray(t[name], dtype=dt) for name, dt, _, _ in _lib.DONOR_FIELDS]
+        types = [c for _, _, c, _ in _lib.DONOR_FIELDS]
+        check(self.ctx, self.lib.dn_patch_set_donors(self.ctx, int(i_patch), _lib.ptr(counts, ctypes.c_int64),
+                                                     *[_lib.ptr(a, ct) for a, ct in zip(arrs, types)]))
+
     def computeDependencies(self):
         """Builds the donor tables of the iterator's patches on the context
         (dn_grid_compute_dependencies); returns the number of seek cells
@@ -378,7 +403,7 @@ class B200CartesianIterator:
     def setLevelSets(self):
         """Hands every patch's level-set wall to the device (dn_patch_set_levelset)."""
         for pid, p in enumerate(self.m_Patches):
-            if p.levelset is None:
+            if p.levelset is None or self.m_Shadow[pid]:
                 check(self.ctx, self.lib.dn_patch_set_levelset(self.ctx, pid, None, 0, 0, 0.0))
             else:
                 G, ni, no, mr = p.levelset
@@ -399,14 +424,17 @@ class B200CartesianIterator:
             for f in fields:
                 a = np.ascontiguousarray(p.data[f], dtype=np.float64)
                 check(self.ctx, self.lib.dn_patch_upload(self.ctx, pid, f, _lib.dptr(a)))
-            if p.active.all():
+            if p.active.all() or self.m_Shadow[pid]:
                 check(self.ctx, self.lib.dn_patch_set_active(self.ctx, pid, None))
             else:
                 m = np.ascontiguousarray(p.active, dtype=np.uint8)
                 check(self.ctx, self.lib.dn_patch_set_active(self.ctx, pid, _lib.u8ptr(m)))
 
     def updateHost(self, fields=(0, 1)):
+        """Downloads every patch but the compact shadows (another rank's)."""
         for pid, p in enumerate(self.m_Patches):
+            if self.m_Shadow[pid]:
+                continue
             for f in fields:
                 a = np.empty(p.data[f].shape, dtype=np.float64)
                 check(self.ctx, self.lib.dn_patch_download(self.ctx, pid, f, _lib.dptr(a)))

@@ -54,6 +54,11 @@ struct DnPatch {
   dn::WallBC wall{};                        // device view (table pointers are device memory)
   bool owned = true;                        // false: a shadow of a patch another rank advances
   bool patch_active = true;                 // false: left out of stages, its state carried over
+  // compact shadow (dn_patch_add_shadow): another rank's patch of which this
+  // context holds only `held` (ascending cell indices, the donor cells its
+  // own patches read), stored [var][held position]; ncp = held.size()
+  bool compact = false;
+  std::vector<uint64_t> held;
 };
 
 // Device offset of cell index c = (i*nj + j)*nk + k in the patch's rows of kp elements.
@@ -61,6 +66,20 @@ inline uint64_t pad_cell(const DnPatch& p, uint64_t c)
 {
   const uint64_t nk = (uint64_t)p.d.nk;
   return (c / nk) * (uint64_t)p.kp + c % nk;
+}
+
+// Device offset of cell c: its padded row position, or for a compact shadow
+// its position among the held cells (false where the shadow does not hold it).
+inline bool dev_cell(const DnPatch& p, uint64_t c, uint64_t* out)
+{
+  if (!p.compact) {
+    *out = pad_cell(p, c);
+    return true;
+  }
+  auto it = std::lower_bound(p.held.begin(), p.held.end(), c);
+  if (it == p.held.end() || *it != c) return false;
+  *out = (uint64_t)(it - p.held.begin());
+  return true;
 }
 
 } // namespace
@@ -197,6 +216,17 @@ int check_patch(dn_ctx* c, int id)
 {
   if (!c) return DN_ERR_ARG;
   if (id < 0 || id >= (int)c->patches.size()) return fail(c, DN_ERR_ARG, "invalid patch id %d", id);
+  return DN_OK;
+}
+
+// Entry points that read or write a patch's whole state refuse a compact
+// shadow: it holds only the donor cells of another rank's patch.
+int check_whole(dn_ctx* c, int id)
+{
+  int s = check_patch(c, id);
+  if (s) return s;
+  if (c->patches[id].compact)
+    return fail(c, DN_ERR_STATE, "patch %d is a compact shadow (another rank's patch; only its donor cells are held)", id);
   return DN_OK;
 }
 
@@ -574,13 +604,23 @@ int build_plan(dn_ctx* c)
       rc_off += (size_t)T.num_receivers[q];
       wi_off += T.num_receivers[q] * T.stride[q];
     }
-    // donor cells at their device offsets (rows of kp elements)
+    // donor cells at their device offsets (rows of kp elements, or the held
+    // position in a compact shadow)
     {
       size_t o = 0;
       for (size_t q = 0; q < T.donor_patch.size(); ++q) {
         const DnPatch& D = c->patches[(size_t)T.donor_patch[q]];
         const size_t m = (size_t)(T.num_receivers[q] * T.stride[q]);
-        for (size_t e = 0; e < m; ++e) idx.push_back((int64_t)pad_cell(D, T.donor_idx[o + e]));
+        for (size_t e = 0; e < m; ++e) {
+          uint64_t dc;
+          if (!dev_cell(D, T.donor_idx[o + e], &dc)) {
+            free_plan(c);
+            return fail(c, DN_ERR_STATE, "donor cell %llu of patch %d is not held by its compact shadow "
+                        "(dn_shadow_alloc with the exchange that delivers it)",
+                        (unsigned long long)T.donor_idx[o + e], T.donor_patch[q]);
+          }
+          idx.push_back((int64_t)dc);
+        }
         o += m;
       }
     }
@@ -950,7 +990,8 @@ int build_batch(dn_ctx* c)
     int tj, tk;
     dn::shape_tile(fp64, c->shape[q], &tj, &tk);
     if (P.owned && P.patch_active) tiles += (long)((P.d.nj + tj - 1) / tj) * ((P.d.nk + tk - 1) / tk);
-    r.tma = 1;
+    // shadows are never staged: no tensor maps
+    r.tma = P.owned ? 1 : 0;
     if (!fp64) {
       dn::FxGeom g{};
       g.ni = P.d.ni; g.nj = P.d.nj; g.nk = P.d.nk; g.kp = P.kp;
@@ -1176,6 +1217,44 @@ int stage_patch(dn_ctx* c, DnPatch& p, int in_b, int un_b, int out_b, double fac
   return DN_OK;
 }
 
+// Upload into a compact shadow: the FP32-bulk base and quantum derived from
+// the whole host state (as its owner derives them), then the held cells,
+// gathered on the host.
+template <typename H>
+int upload_shadow(dn_ctx* c, DnPatch& p, int field, const H* host)
+{
+  if (c->precision == DN_FP32 && !p.base_set) {
+    derive_base(p, host);
+    c->plan_dirty = true;
+    c->ls_dirty = true;
+    c->batch_dirty = true;
+    c->generation++;
+  }
+  const size_t m = p.held.size();
+  if (m == 0) return DN_OK;
+  std::vector<H> g(5 * m);
+  for (int v = 0; v < 5; ++v)
+    for (size_t t = 0; t < m; ++t) g[(size_t)v * m + t] = host[(size_t)v * p.nc + p.held[t]];
+  int s;
+  if ((s = ensure_staging(c, g.size() * sizeof(H)))) return s;
+  cudaError_t e = cudaMemcpyAsync(c->staging, g.data(), g.size() * sizeof(H), cudaMemcpyHostToDevice, c->stream);
+  if (e != cudaSuccess) return cuda_fail(c, e, "shadow upload copy");
+  void* dst = p.buf[c->fmap[field]];
+  if (c->precision == DN_FP64) {
+    k_convert<H, double><<<grid_for(5 * m), 256, 0, c->stream>>>((const H*)c->staging, (double*)dst, 5 * m);
+  } else {
+    // held positions are consecutive: rows of m cells, pitch m
+    k_quantize<H><<<grid_for(5 * m), 256, 0, c->stream>>>((const H*)c->staging, (int32_t*)dst, m, (int)m, (int)m,
+                                                       qparams(p), c->d_err);
+  }
+  c->launches++;
+  e = cudaGetLastError();
+  if (e != cudaSuccess) return cuda_fail(c, e, "shadow upload conversion");
+  e = cudaStreamSynchronize(c->stream);     // the gathered host vector goes out of scope
+  if (e != cudaSuccess) return cuda_fail(c, e, "shadow upload");
+  return read_device_error(c);
+}
+
 template <typename H>
 int upload_impl(dn_ctx* c, int id, int field, const H* host)
 {
@@ -1186,6 +1265,7 @@ int upload_impl(dn_ctx* c, int id, int field, const H* host)
   if (!host) return fail(c, DN_ERR_ARG, "host pointer is NULL");
   if (set_device(c) != DN_OK) return DN_ERR_CUDA;
   DnPatch& p = c->patches[id];
+  if (p.compact) return upload_shadow(c, p, field, host);
   void* dst = p.buf[c->fmap[field]];
   const size_t n = 5 * p.nc;
   cudaError_t e;
@@ -1221,7 +1301,7 @@ template <typename H>
 int download_impl(dn_ctx* c, int id, int field, H* host)
 {
   NvtxRange nvtx("dn download");
-  int s = check_patch(c, id);
+  int s = check_whole(c, id);
   if (s) return s;
   if ((s = check_field(c, field))) return s;
   if (!host) return fail(c, DN_ERR_ARG, "host pointer is NULL");
@@ -1285,7 +1365,7 @@ template <typename H>
 int upload_async_impl(dn_ctx* c, int id, int field, const H* host)
 {
   NvtxRange nvtx("dn upload (async)");
-  int s = check_patch(c, id);
+  int s = check_whole(c, id);
   if (s) return s;
   if ((s = check_field(c, field))) return s;
   if (!host) return fail(c, DN_ERR_ARG, "host pointer is NULL");
@@ -1333,7 +1413,7 @@ template <typename H>
 int download_async_impl(dn_ctx* c, int id, int field, H* host)
 {
   NvtxRange nvtx("dn download (async)");
-  int s = check_patch(c, id);
+  int s = check_whole(c, id);
   if (s) return s;
   if ((s = check_field(c, field))) return s;
   if (!host) return fail(c, DN_ERR_ARG, "host pointer is NULL");
@@ -1451,7 +1531,9 @@ int dn_set_stream(dn_ctx* c, void* stream)
   return DN_OK;
 }
 
-int dn_patch_add(dn_ctx* c, const dn_patch_desc* d, int* id)
+namespace {
+
+int add_patch(dn_ctx* c, const dn_patch_desc* d, int* id, bool compact)
 {
   if (!c || !d || !id) return DN_ERR_ARG;
   if (d->ni < 1 || d->nj < 1 || d->nk < 1) return fail(c, DN_ERR_ARG, "patch size must be positive");
@@ -1489,9 +1571,11 @@ int dn_patch_add(dn_ctx* c, const dn_patch_desc* d, int* id)
   p.d = dd;
   p.nc = nc;
   p.kp = kp;
-  p.ncp = ncp;
-  const size_t bytes = 5 * ncp * elem_size(c);
-  for (int b = 0; b < 3; ++b) {
+  p.ncp = compact ? 0 : ncp;
+  p.compact = compact;
+  p.owned = !compact;
+  const size_t bytes = 5 * p.ncp * elem_size(c);
+  for (int b = 0; b < 3 && bytes; ++b) {
     cudaError_t e = cudaMalloc(&p.buf[b], bytes);
     if (e != cudaSuccess) {
       for (int q = 0; q < b; ++q) cudaFree(p.buf[q]);
@@ -1511,6 +1595,21 @@ int dn_patch_add(dn_ctx* c, const dn_patch_desc* d, int* id)
   c->batch_dirty = true;
   c->generation++;
   *id = (int)c->patches.size() - 1;
+  return DN_OK;
+}
+
+} // namespace
+
+int dn_patch_add(dn_ctx* c, const dn_patch_desc* d, int* id) { return add_patch(c, d, id, false); }
+
+int dn_patch_add_shadow(dn_ctx* c, const dn_patch_desc* d, int* id) { return add_patch(c, d, id, true); }
+
+int dn_patch_device_cells(dn_ctx* c, int id, int64_t* cells)
+{
+  int s = check_patch(c, id);
+  if (s) return s;
+  if (!cells) return fail(c, DN_ERR_ARG, "output pointer is NULL");
+  *cells = (int64_t)c->patches[id].ncp;
   return DN_OK;
 }
 
@@ -1547,7 +1646,7 @@ int dn_patch_download_f32_async(dn_ctx* c, int id, int field, float* host) { ret
 
 int dn_patch_set_active(dn_ctx* c, int id, const uint8_t* mask)
 {
-  int s = check_patch(c, id);
+  int s = (mask ? check_whole : check_patch)(c, id);
   if (s) return s;
   if (set_device(c) != DN_OK) return DN_ERR_CUDA;
   DnPatch& p = c->patches[id];
@@ -1584,6 +1683,7 @@ int dn_copy_field(dn_ctx* c, int i_src, int i_dst)
   if (i_src == i_dst) return DN_OK;
   if (set_device(c) != DN_OK) return DN_ERR_CUDA;
   for (auto& p : c->patches) {
+    if (p.ncp == 0) continue;               // a compact shadow that holds no cell
     cudaError_t e = cudaMemcpyAsync(p.buf[c->fmap[i_dst]], p.buf[c->fmap[i_src]], 5 * p.ncp * elem_size(c),
                                     cudaMemcpyDeviceToDevice, c->stream);
     if (e != cudaSuccess) return cuda_fail(c, e, "copyField");
@@ -1720,7 +1820,7 @@ int dn_conservation_sums(dn_ctx* c, double out[5])
 
 int dn_field_difference(dn_ctx* c, int id, int f1, int v1, int f2, int v2, double* max_norm, double* l2_norm)
 {
-  int s = check_patch(c, id);
+  int s = check_whole(c, id);
   if (s) return s;
   if ((s = check_field(c, f1)) || (s = check_field(c, f2))) return s;
   if (v1 < 0 || v1 > 4 || v2 < 0 || v2 > 4) return fail(c, DN_ERR_ARG, "variable index out of range");
@@ -1757,7 +1857,7 @@ int dn_field_difference(dn_ctx* c, int id, int f1, int v1, int f2, int v2, doubl
 
 int dn_flow_stats(dn_ctx* c, int id, int field, double dt, double out[3])
 {
-  int s = check_patch(c, id);
+  int s = check_whole(c, id);
   if (s) return s;
   if ((s = check_field(c, field))) return s;
   if (!out) return fail(c, DN_ERR_ARG, "output pointer is NULL");
@@ -1963,7 +2063,7 @@ int dn_patch_set_donors(dn_ctx* c, int id, const int64_t counts[4], const uint64
 int dn_patch_set_levelset(dn_ctx* c, int id, const double* G, int num_inner_layers, int num_outer_layers,
                           double min_inner_rel_dist)
 {
-  int s = check_patch(c, id);
+  int s = (G ? check_whole : check_patch)(c, id);
   if (s) return s;
   if (!G) {
     c->ls_on[id] = 0;
@@ -1994,7 +2094,7 @@ int dn_patch_set_levelset_layers(dn_ctx* c, int id, int num_inner_layers, const 
                                  const uint64_t* cells, const double* g, const double* grad, const uint64_t* donors,
                                  const double* weights)
 {
-  int s = check_patch(c, id);
+  int s = (num_inner_layers > 0 ? check_whole : check_patch)(c, id);
   if (s) return s;
   if (num_inner_layers < 0 || (num_inner_layers > 0 && !counts)) return fail(c, DN_ERR_ARG, "invalid layer counts");
   int64_t total = 0;
@@ -2032,7 +2132,7 @@ int dn_patch_set_levelset_layers(dn_ctx* c, int id, int num_inner_layers, const 
 
 int dn_patch_set_levelset_gpu(dn_ctx* c, int id, const double* G)
 {
-  int s = check_patch(c, id);
+  int s = (G ? check_whole : check_patch)(c, id);
   if (s) return s;
   if (set_device(c) != DN_OK) return DN_ERR_CUDA;
   DnPatch& P = c->patches[id];
@@ -2151,6 +2251,10 @@ int dn_patch_set_owned(dn_ctx* c, int id, int owned)
 {
   int s = check_patch(c, id);
   if (s) return s;
+  if (c->patches[id].compact) {
+    if (owned) return fail(c, DN_ERR_STATE, "patch %d is a compact shadow and stays another rank's", id);
+    return DN_OK;
+  }
   c->patches[id].owned = owned != 0;
   c->plan_dirty = true;
   c->ls_dirty = true;
@@ -2172,6 +2276,50 @@ int dn_exchange_build_ctx(dn_ctx* c, const int32_t* owner, int rank, int world, 
     return fail(c, DN_ERR_ARG, "%s", err.c_str());
   }
   *out = e;
+  return DN_OK;
+}
+
+int dn_shadow_alloc(dn_ctx* c, dn_exchange* e)
+{
+  if (!c || !e) return DN_ERR_ARG;
+  const dn::Exchange& x = e->ex;
+  if (x.device >= 0)
+    return fail(c, DN_ERR_STATE, "allocate the shadows before the exchange's first pack or unpack");
+  if (set_device(c) != DN_OK) return DN_ERR_CUDA;
+  // the cells each compact shadow receives, over all peers
+  std::vector<std::vector<uint64_t>> held(c->patches.size());
+  for (int q = 0; q < x.world; ++q) {
+    for (size_t t = 0; t < x.recv_patch[q].size(); ++t) {
+      const int32_t p = x.recv_patch[q][t];
+      if (p < 0 || p >= (int)c->patches.size()) return fail(c, DN_ERR_ARG, "exchange names patch %d", p);
+      held[(size_t)p].push_back(x.recv_cell[q][t]);
+    }
+  }
+  for (size_t p = 0; p < c->patches.size(); ++p) {
+    DnPatch& P = c->patches[p];
+    if (!P.compact) continue;
+    std::vector<uint64_t>& h = held[p];
+    std::sort(h.begin(), h.end());
+    h.erase(std::unique(h.begin(), h.end()), h.end());
+    if (!h.empty() && h.back() >= P.nc) return fail(c, DN_ERR_ARG, "exchange cell outside patch %zu", p);
+    for (int b = 0; b < 3; ++b) {
+      if (P.buf[b]) cudaFree(P.buf[b]);
+      P.buf[b] = nullptr;
+    }
+    P.held.swap(h);
+    P.ncp = P.held.size();
+    const size_t bytes = 5 * P.ncp * elem_size(c);
+    for (int b = 0; b < 3 && bytes; ++b) {
+      cudaError_t er = cudaMalloc(&P.buf[b], bytes);
+      if (er != cudaSuccess) return fail(c, DN_ERR_NOMEM, "cudaMalloc of %zu bytes for a shadow field failed", bytes);
+      er = cudaMemsetAsync(P.buf[b], 0, bytes, c->stream);
+      if (er != cudaSuccess) return cuda_fail(c, er, "shadow field clear");
+    }
+  }
+  c->plan_dirty = true;
+  c->ls_dirty = true;
+  c->batch_dirty = true;
+  c->generation++;
   return DN_OK;
 }
 
@@ -2199,14 +2347,31 @@ int exchange_device_lists(dn_ctx* c, dn_exchange* e)
     if (x.device != c->device) return fail(c, DN_ERR_ARG, "exchange lists live on device %d, context on %d", x.device, c->device);
     return DN_OK;
   }
+  for (int q = 0; q < x.world; ++q) {
+    for (size_t t = 0; t < x.send_patch[q].size(); ++t)
+      if (c->patches[(size_t)x.send_patch[q][t]].compact)
+        return fail(c, DN_ERR_STATE, "the exchange sends from patch %d, a compact shadow of this context",
+                    x.send_patch[q][t]);
+  }
+  // cells at their device offsets (rows of kp elements; held positions in
+  // compact shadows)
+  std::vector<std::vector<uint64_t>> sc(x.world), rc(x.world);
+  for (int q = 0; q < x.world; ++q) {
+    sc[q].resize(x.send_cell[q].size());
+    rc[q].resize(x.recv_cell[q].size());
+    for (size_t t = 0; t < sc[q].size(); ++t)
+      sc[q][t] = pad_cell(c->patches[(size_t)x.send_patch[q][t]], x.send_cell[q][t]);
+    for (size_t t = 0; t < rc[q].size(); ++t) {
+      if (!dev_cell(c->patches[(size_t)x.recv_patch[q][t]], x.recv_cell[q][t], &rc[q][t]))
+        return fail(c, DN_ERR_STATE, "cell %llu of patch %d is received but not held by its compact shadow "
+                    "(dn_shadow_alloc with this exchange first)", (unsigned long long)x.recv_cell[q][t],
+                    x.recv_patch[q][t]);
+    }
+  }
   x.dev.assign((size_t)x.world * 4, nullptr);
   x.device = c->device;
   for (int q = 0; q < x.world; ++q) {
-    // cells at their device offsets (rows of kp elements)
-    std::vector<uint64_t> sc(x.send_cell[q].size()), rc(x.recv_cell[q].size());
-    for (size_t t = 0; t < sc.size(); ++t) sc[t] = pad_cell(c->patches[(size_t)x.send_patch[q][t]], x.send_cell[q][t]);
-    for (size_t t = 0; t < rc.size(); ++t) rc[t] = pad_cell(c->patches[(size_t)x.recv_patch[q][t]], x.recv_cell[q][t]);
-    const void* src[4] = {x.send_patch[q].data(), sc.data(), x.recv_patch[q].data(), rc.data()};
+    const void* src[4] = {x.send_patch[q].data(), sc[q].data(), x.recv_patch[q].data(), rc[q].data()};
     const size_t bytes[4] = {x.send_patch[q].size() * 4, x.send_cell[q].size() * 8, x.recv_patch[q].size() * 4,
                              x.recv_cell[q].size() * 8};
     for (int a = 0; a < 4; ++a) {
@@ -2430,7 +2595,7 @@ int dn_autotune(dn_ctx* c, const char* cache_path, double cost_out[DN_NUM_TILE_S
       double padded = 0;
       for (size_t q = 0; q < c->patches.size(); ++q) {
         c->shape[q] = sh;
-        padded += padded_cells(c, c->patches[q], sh);
+        if (c->patches[q].owned && c->patches[q].patch_active) padded += padded_cells(c, c->patches[q], sh);
       }
       c->batch_dirty = true;
       const int reps = 5;
@@ -2554,6 +2719,7 @@ int dn_tma_patch_count(dn_ctx* c, int64_t* count)
   if (!c || !count) return DN_ERR_ARG;
   int64_t n = 0;
   for (const DnPatch& P : c->patches) {
+    if (P.compact) continue;
     int tj, tk;
     dn::shape_tile(c->precision == DN_FP64, 0, &tj, &tk);
     bool ok;

@@ -4,9 +4,14 @@ cell count, donor cells exchanged between ranks before every donor copy.
 The reference advances all patches of a grid in one process; its RK step
 (RungeKutta::operator(), rungekutta.cpp:27-42) copies donor data between
 patches in memory (Patch::accessDonorDataDirect, patch.cpp:573-653).  Here
-every rank holds the whole grid in its context but owns only its share
+every rank knows the whole grid but owns only its share
 (dn_patch_set_owned): stages, donor copies into receiving cells and the
-level-set wall run on owned patches, the others are shadows.  Before each
+level-set wall run on owned patches, the others are shadows.  A shadow is
+either a full copy (a patch added with dn_patch_add and marked unowned) or,
+with `make_sharded(..., compact=True)`, a compact shadow that holds only the
+donor cells this rank's receiving cells read (dn_patch_add_shadow +
+dn_shadow_alloc): device memory then scales with the rank's share of the
+grid plus its halo of donor cells.  Before each
 donor copy, each rank sends its peers the donor cells of its patches that
 their receiving patches read and receives the ones its own receiving patches
 read (dn_exchange_pack / _unpack around NCCL send/recv through
@@ -138,10 +143,15 @@ class ShardedIterator:
         self.it, self.owner, self.rank, self.world, self.group = it, list(owner), rank, world, group
         lib = it.lib
         for p in range(it.numPatches()):
+            if it.isShadow(p) and self.owner[p] == rank:
+                raise ValueError(f"patch {p} is owned by rank {rank} but was added as a compact shadow")
             check(it.ctx, lib.dn_patch_set_owned(it.ctx, p, 1 if self.owner[p] == rank else 0))
         own = (ctypes.c_int32 * len(self.owner))(*self.owner)
         self.ex = ctypes.c_void_p()
         check(it.ctx, lib.dn_exchange_build_ctx(it.ctx, own, rank, world, ctypes.byref(self.ex)))
+        if any(it.isShadow(p) for p in range(it.numPatches())):
+            # compact shadows: field memory for exactly the donor cells received
+            check(it.ctx, lib.dn_shadow_alloc(it.ctx, self.ex))
         counts = {}
         for q in range(world):
             ns, nr = ctypes.c_int64(), ctypes.c_int64()
@@ -200,7 +210,96 @@ class ShardedIterator:
         local = self.it.flowStats(field, dt, [p for p in range(len(self.owner)) if self.owner[p] == self.rank])
         return reduce_flow_stats(local, self.group)
 
+    def deviceCells(self):
+        """Cells per variable this rank holds on its GPU (owned patches and
+        shadows)."""
+        return sum(self.it.deviceCells(p) for p in range(self.it.numPatches()))
+
     def close(self):
         if self.ex:
             self.it.lib.dn_exchange_destroy(self.ex)
             self.ex = None
+
+
+def make_sharded(objs, owner, rank, world, precision, device=0, group=None, op=None, compact=True, fields=(0,)):
+    """A ShardedIterator over the patches `objs` (CartesianPatch objects of one
+    PatchGrid whose donor tables are computed) for `rank`: owned patches in
+    full, the others as compact shadows (compact=True) or full copies; the
+    host state of `fields` uploaded.  The process group must use NCCL and
+    `device` must be this rank's GPU."""
+    from .api import AusmPlus, B200CartesianIterator
+    it = B200CartesianIterator(op if op is not None else AusmPlus(), device, precision)
+    for p, cp in enumerate(objs):
+        it.addPatch(cp, shadow=compact and owner[p] != rank)
+    it.updateDevice(fields=fields)
+    return ShardedIterator(it, owner, rank, world, group)
+
+
+def slab_split(n, world, halo=2):
+    """Splits one patch of n = (ni, nj, nk) cells, periodic along i, into
+    `world` i-slabs for as many ranks (the single-patch case of the sharded
+    grid).  Slab s owns the global planes [a_s, a_{s+1}) with a_s = s*ni//world
+    and carries `halo` seek planes on either side, copied before every stage
+    from the neighbouring slab's owned planes (across the periodic seam for
+    the first and last slab) by donor tables of weight 1.  With the
+    reference's two seek layers the stencil of every owned cell (two cells
+    each way along i) reads only owned or freshly copied planes, so the owned
+    planes advance exactly as in the unsplit patch; the seek planes' own
+    updates are overwritten by the copy.
+
+    Returns per slab a dict: n (cells), plane0 (global plane of local plane
+    0, modulo ni), owned (a, b), tables (the dn_patch_set_donors layout; donor
+    patch ids are slab indices)."""
+    ni, nj, nk = (int(x) for x in n)
+    if world < 2:
+        raise ValueError("an i-slab split needs at least two slabs")
+    bounds = [s * ni // world for s in range(world + 1)]
+    if min(bounds[s + 1] - bounds[s] for s in range(world)) < halo:
+        raise ValueError(f"{ni} planes cannot give {world} slabs of at least {halo} planes each")
+    owner_of = np.empty(ni, dtype=np.int64)
+    for s in range(world):
+        owner_of[bounds[s]:bounds[s + 1]] = s
+    plane_cells = nj * nk
+    out = []
+    for s in range(world):
+        a, b = bounds[s], bounds[s + 1]
+        n_s = b - a + 2 * halo
+        seek = list(range(halo)) + list(range(n_s - halo, n_s))
+        g = [(a - halo + l) % ni for l in seek]
+        donors = {}
+        for l, gp in zip(seek, g):
+            t = int(owner_of[gp])
+            lt = (gp - (bounds[t] - halo)) % ni          # the donor slab's local plane
+            donors.setdefault(t, []).append((l, lt))
+        rec_unique = np.concatenate([l * plane_cells + np.arange(plane_cells, dtype=np.uint64) for l in seek])
+        dp, nr, st, rc, di = [], [], [], [], []
+        for t in sorted(donors):
+            pairs = donors[t]
+            dp.append(t)
+            nr.append(len(pairs) * plane_cells)
+            st.append(1)
+            for l, lt in pairs:
+                rc.append(l * plane_cells + np.arange(plane_cells, dtype=np.uint64))
+                di.append(lt * plane_cells + np.arange(plane_cells, dtype=np.uint64))
+        rc = np.concatenate(rc).astype(np.uint64)
+        di = np.concatenate(di).astype(np.uint64)
+        tables = {"rec_unique": rec_unique.astype(np.uint64), "donor_patch": np.asarray(dp, dtype=np.int32),
+                  "num_receivers": np.asarray(nr, dtype=np.int64), "stride": np.asarray(st, dtype=np.int32),
+                  "rec_concat": rc, "donor_idx": di, "weight": np.ones(len(di), dtype=np.float64)}
+        tables["counts"] = np.array([len(rec_unique), len(dp), len(rc), len(di)], dtype=np.int64)
+        out.append({"n": (n_s, nj, nk), "plane0": (a - halo) % ni, "owned": (a, b), "tables": tables})
+    return out
+
+
+def slab_state(U, slab):
+    """The state [5][ni][nj][nk] of one slab of `slab_split`, cut from the
+    whole patch's state U (planes wrapped across the periodic seam)."""
+    ni = U.shape[1]
+    planes = [(slab["plane0"] + l) % ni for l in range(slab["n"][0])]
+    return np.ascontiguousarray(U[:, planes])
+
+
+def slab_owned(U_slab, slab, halo=2):
+    """The owned planes of a slab's state."""
+    a, b = slab["owned"]
+    return U_slab[:, halo:halo + (b - a)]

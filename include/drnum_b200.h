@@ -479,9 +479,28 @@ int dn_read_data(dn_ctx* ctx, int field, const char* file_name, double* time);
  *     4-byte int32 offsets for DN_FP32, whose shadows share the owner's base
  *     and quantum), enqueued on the context's stream.
  * Moving the buffers between ranks is the caller's (NCCL send/recv;
- * drnum_b200/shard.py). */
+ * drnum_b200/shard.py).
+ *
+ * Memory that scales with the rank's share: a rank adds the patches it owns
+ * with dn_patch_add and every other patch with dn_patch_add_shadow (no field
+ * memory), sets the donor tables, builds the exchange and then calls
+ * dn_shadow_alloc, which gives each compact shadow field memory for exactly
+ * the cells the exchange delivers to it, [var][position among the received
+ * cells in ascending order].  Device memory is then the owned patches plus
+ * the donor cells their receiving cells read, not the whole grid.  A compact
+ * shadow refuses the calls that need its whole state (downloads,
+ * asynchronous uploads, active masks, level sets, flow statistics, field
+ * differences, restart files: DN_ERR_STATE); dn_patch_upload on it derives
+ * the FP32-bulk base and quantum from the whole host state, as its owner does,
+ * and copies the held cells.  dn_shadow_alloc must precede the exchange's
+ * first pack or unpack.  dn_patch_device_cells gives the cells per variable
+ * a patch holds on the device (rows padded for FP32 bulk).
+ * The reference has no counterpart (one process holds the whole grid). */
 typedef struct dn_exchange dn_exchange;
 int dn_patch_set_owned(dn_ctx* ctx, int patch_id, int owned);
+int dn_patch_add_shadow(dn_ctx* ctx, const dn_patch_desc* desc, int* patch_id);
+int dn_shadow_alloc(dn_ctx* ctx, dn_exchange* ex);
+int dn_patch_device_cells(dn_ctx* ctx, int patch_id, int64_t* cells);
 int dn_exchange_build(const dn_overlap* ov, const int32_t* owner, int rank, int world, dn_exchange** out);
 int dn_exchange_build_ctx(dn_ctx* ctx, const int32_t* owner, int rank, int world, dn_exchange** out);
 int dn_exchange_counts(const dn_exchange* ex, int peer, int64_t* n_send, int64_t* n_recv);

@@ -26,7 +26,7 @@ def _fixture(golden_dir, name):
     return np.load(os.path.join(golden_dir, f"grid_{name}.npz"))
 
 
-def make_grid(name, precision, states=None, op=None):
+def make_grid(name, precision, states=None, op=None, shadows=None):
     patches, st0, spacings, dt, steps = cases_def.grid_case(name)
     states = st0 if states is None else states
     grid = PatchGrid()
@@ -45,8 +45,8 @@ def make_grid(name, precision, states=None, op=None):
         objs.append(cp)
     grid.computeDependencies()
     it = B200CartesianIterator(op if op is not None else AusmPlus(), 0, precision)
-    for cp in objs:
-        it.addPatch(cp)
+    for q, cp in enumerate(objs):
+        it.addPatch(cp, shadow=bool(shadows and shadows[q]))
     it.updateDevice(fields=(0,))
     return it, objs, grid, dt, steps
 

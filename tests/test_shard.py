@@ -263,20 +263,24 @@ class _Recorder:
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("compact", [False, True])
 @pytest.mark.parametrize("precision", [_lib.DN_FP64, _lib.DN_FP32])
 @pytest.mark.parametrize("name", ["octants_jet", "sphere_pair"])
-def test_two_contexts_as_two_ranks_equal_one_context(golden_dir, name, precision):
+def test_two_contexts_as_two_ranks_equal_one_context(golden_dir, name, precision, compact):
+    # compact: every rank holds its own patches and, of the others, only the
+    # donor cells its receiving cells read (dn_patch_add_shadow, dn_shadow_alloc)
     import torch
     from drnum_b200.api import B200LevelSetObjectBC
     from test_gpu_grid import make_grid
     world = 2
     one, objs1, _, dt, steps = make_grid(name, precision)
     post1 = [B200LevelSetObjectBC(one)] if name in cases_def.LEVELSET else []
-    ranks = [make_grid(name, precision) for _ in range(world)]
-    its = [r[0] for r in ranks]
     patches = cases_def.grid_layout(name)
     owner = shard.partition([int(np.prod(p["n"])) for p in patches], world)
     assert len(set(owner)) == world
+    ranks = [make_grid(name, precision, shadows=[compact and owner[p] != r for p in range(len(patches))])
+             for r in range(world)]
+    its = [r[0] for r in ranks]
     lib = _lib.load()
     exs, bufs = [], {}
     dtype = torch.float64 if precision == _lib.DN_FP64 else torch.int32
@@ -286,6 +290,21 @@ def test_two_contexts_as_two_ranks_equal_one_context(golden_dir, name, precision
         ex = ctypes.c_void_p()
         own = (ctypes.c_int32 * len(owner))(*owner)
         assert lib.dn_exchange_build_ctx(it.ctx, own, r, world, ctypes.byref(ex)) == _lib.DN_OK
+        if compact:
+            assert lib.dn_shadow_alloc(it.ctx, ex) == _lib.DN_OK
+            held = [it.deviceCells(p) for p in range(len(patches))]
+            full = [one.deviceCells(p) for p in range(len(patches))]
+            for p in range(len(patches)):
+                if owner[p] == r:
+                    assert held[p] == full[p]
+                else:
+                    assert held[p] < full[p], (p, held[p], full[p])   # donor cells only
+            assert sum(held[p] for p in range(len(patches)) if owner[p] != r) > 0
+            # a compact shadow is another rank's: its whole state stays out of reach
+            q = next(p for p in range(len(patches)) if owner[p] != r)
+            assert lib.dn_patch_download(it.ctx, q, 0, _lib.dptr(np.empty(5 * int(np.prod(patches[q]["n"]))))) \
+                == _lib.DN_ERR_STATE
+            assert lib.dn_patch_set_owned(it.ctx, q, 1) == _lib.DN_ERR_STATE
         exs.append(ex)
         for q in range(world):
             ns, nr = ctypes.c_int64(), ctypes.c_int64()
@@ -399,3 +418,183 @@ def test_rank_without_owned_patches_steps_without_error(precision):
     # at most the donor copies of the step (one per copy, nothing to receive)
     assert it.launchCount() - l0 <= 1 + 2 * len(cases.RK3_ALPHA)
     it.close()
+
+
+# ---------------------------------------------------------------- i-slab split
+
+def _slab_oracle_run(U0, h, dt, steps, slabs):
+    """The slabs of shard.slab_split advanced with the oracle's residual
+    (closed x axis, periodic y and z) and the numpy donor copy, in the order
+    of RungeKutta::operator() (rungekutta.cpp:27-42)."""
+    U = [shard.slab_state(U0, s) for s in slabs]
+    tables = [s["tables"] for s in slabs]
+    for _ in range(steps):
+        pyoracle.oracle_donor_copy(U, tables)
+        Un = [u.copy() for u in U]
+        for q, a in enumerate(cases.RK3_ALPHA):
+            if q > 0:
+                pyoracle.oracle_donor_copy(U, tables)
+            for p, u in enumerate(U):
+                res = pyoracle.oracle_residual_bc(u, h, {}, periodic=(False, True, True))
+                U[p] = Un[p] + (a * dt) / (h * h * h) * res
+            pyoracle.oracle_donor_copy(U, tables)
+    return U
+
+
+@pytest.mark.parametrize("world", [2, 3])
+def test_slab_split_tables_reproduce_the_unsplit_patch(world):
+    # one periodic patch cut into i-slabs with two seek planes per side:
+    # the owned planes advance bit for bit as in the unsplit patch (oracle)
+    U0, h, dt = cases.periodic_box(12)
+    steps = 2
+    ref = pyoracle.oracle_run(U0, h, dt, steps)
+    slabs = shard.slab_split(U0.shape[1:], world)
+    got = _slab_oracle_run(U0, h, dt, steps, slabs)
+    for s, u in zip(slabs, got):
+        a, b = s["owned"]
+        assert np.array_equal(shard.slab_owned(u, s), ref[:, a:b]), s["owned"]
+    assert sum(s["owned"][1] - s["owned"][0] for s in slabs) == 12
+
+
+def test_slab_split_rejects_thin_slabs():
+    with pytest.raises(ValueError):
+        shard.slab_split((5, 4, 4), 3)
+    with pytest.raises(ValueError):
+        shard.slab_split((8, 4, 4), 1)
+
+
+def _slab_context(U0, h, slabs, which, precision, compact_owner=None, base=None):
+    """A context holding the slabs `which` (the others as compact shadows
+    when compact_owner is given: slab p is owned by compact_owner[p])."""
+    from drnum_b200.api import AusmPlus, B200CartesianIterator, CartesianPatch
+    it = B200CartesianIterator(AusmPlus(), 0, precision)
+    objs = []
+    for p, s in enumerate(slabs):
+        cp = CartesianPatch(*s["n"], spacing=(h, h, h), periodic=(False, True, True))
+        cp.setField(0, shard.slab_state(U0, s))
+        it.addPatch(cp, shadow=compact_owner is not None and compact_owner[p] != which)
+        objs.append(cp)
+    for p, s in enumerate(slabs):
+        t = s["tables"]
+        it.setDonorTablesOf(p, t)
+        if base is not None:
+            it.setBase(p, *base)
+    it.updateDevice(fields=(0,))
+    return it, objs
+
+
+def _fx_base(U0):
+    # one fixed-point base and range for the unsplit patch and every slab:
+    # the mean state and four times the variables' magnitude scales (density,
+    # rho (|u| + a) for the momenta, total energy), as a first upload derives
+    # them for a patch
+    U = U0.reshape(5, -1)
+    base = U.mean(axis=1)
+    r = U[0]
+    q2 = (U[1] ** 2 + U[2] ** 2 + U[3] ** 2) / r ** 2
+    T = (U[4] / r - 0.5 * q2) / 717.5
+    mm = (r * (np.sqrt(q2) + np.sqrt(1.4 * 287.2 * T))).max()
+    return base, 4.0 * np.array([np.abs(r).max(), mm, mm, mm, np.abs(U[4]).max()])
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision", [_lib.DN_FP64, _lib.DN_FP32])
+def test_slab_split_on_one_context_equals_unsplit_patch(precision):
+    from drnum_b200.api import AusmPlus, B200CartesianIterator, CartesianPatch
+    n, world, steps = 32, 3, 4
+    U0, h, dt = cases.periodic_box(n)
+    base = _fx_base(U0) if precision == _lib.DN_FP32 else None
+    one = B200CartesianIterator(AusmPlus(), 0, precision)
+    cp = CartesianPatch(n, n, n, spacing=(h, h, h))
+    cp.setField(0, U0)
+    one.addPatch(cp)
+    if base is not None:
+        one.setBase(0, *base)
+    one.updateDevice(fields=(0,))
+    for _ in range(steps):
+        one.rkStep(dt, cases.RK3_ALPHA)
+    ref = one.downloadField(0)
+    one.close()
+    slabs = shard.slab_split((n, n, n), world)
+    it, _ = _slab_context(U0, h, slabs, 0, precision, base=base)
+    for _ in range(steps):
+        it.rkStep(dt, cases.RK3_ALPHA)
+    for p, s in enumerate(slabs):
+        a, b = s["owned"]
+        assert np.array_equal(shard.slab_owned(it.downloadField(p), s), ref[:, a:b]), (p, s["owned"])
+    it.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision", [_lib.DN_FP64, _lib.DN_FP32])
+def test_slab_split_over_two_contexts_with_compact_shadows(precision):
+    # two contexts play two ranks of a 32^3 patch split into two slabs; each
+    # holds its slab and the two seek-plane sources of the other as a compact
+    # shadow; the exchange buffers are handed over between launches
+    import torch
+    from drnum_b200.api import AusmPlus, B200CartesianIterator, CartesianPatch
+    n, world, steps = 32, 2, 3
+    U0, h, dt = cases.periodic_box(n)
+    base = _fx_base(U0) if precision == _lib.DN_FP32 else None
+    one = B200CartesianIterator(AusmPlus(), 0, precision)
+    cp = CartesianPatch(n, n, n, spacing=(h, h, h))
+    cp.setField(0, U0)
+    one.addPatch(cp)
+    if base is not None:
+        one.setBase(0, *base)
+    one.updateDevice(fields=(0,))
+    for _ in range(steps):
+        one.rkStep(dt, cases.RK3_ALPHA)
+    ref = one.downloadField(0)
+    one.close()
+    slabs = shard.slab_split((n, n, n), world)
+    owner = list(range(world))
+    lib = _lib.load()
+    its, exs, bufs = [], [], {}
+    dtype = torch.float64 if precision == _lib.DN_FP64 else torch.int32
+    for r in range(world):
+        it, _ = _slab_context(U0, h, slabs, r, precision, compact_owner=owner, base=base)
+        for p in range(world):
+            assert lib.dn_patch_set_owned(it.ctx, p, int(owner[p] == r)) == _lib.DN_OK
+        ex = ctypes.c_void_p()
+        own = (ctypes.c_int32 * world)(*owner)
+        assert lib.dn_exchange_build_ctx(it.ctx, own, r, world, ctypes.byref(ex)) == _lib.DN_OK
+        assert lib.dn_shadow_alloc(it.ctx, ex) == _lib.DN_OK
+        q = 1 - r
+        # the shadow holds the neighbour's two planes on each side: 4 of its 20 planes
+        assert it.deviceCells(q) == 4 * n * n
+        for peer in range(world):
+            ns, nr = ctypes.c_int64(), ctypes.c_int64()
+            assert lib.dn_exchange_counts(ex, peer, ctypes.byref(ns), ctypes.byref(nr)) == _lib.DN_OK
+            if ns.value:
+                bufs[(r, peer)] = torch.empty(5 * ns.value, dtype=dtype, device="cuda")
+        its.append(it)
+        exs.append(ex)
+    rec = _Recorder()
+    shard.rk_step_sequence(rec, dt, cases.RK3_ALPHA)
+    for _ in range(steps):
+        for op, args in rec.ops:
+            if op == "exchange":
+                for (r, q), b in bufs.items():
+                    assert lib.dn_exchange_pack(its[r].ctx, exs[r], args[0], q, ctypes.c_void_p(b.data_ptr())) == 0
+                for it in its:
+                    it.sync()
+                for (r, q), b in bufs.items():
+                    assert lib.dn_exchange_unpack(its[q].ctx, exs[q], args[0], r, ctypes.c_void_p(b.data_ptr())) == 0
+                for it in its:
+                    it.sync()
+            elif op == "copy_donor_data":
+                for it in its:
+                    it.copyDonorData(*args)
+            elif op == "copy_field":
+                for it in its:
+                    it.copyField(*args)
+            elif op == "compute":
+                for it in its:
+                    it.computeAll(*args)
+    for r, s in enumerate(slabs):
+        a, b = s["owned"]
+        assert np.array_equal(shard.slab_owned(its[r].downloadField(r), s), ref[:, a:b]), r
+    for it, ex in zip(its, exs):
+        lib.dn_exchange_destroy(ex)
+        it.close()
