@@ -18,6 +18,7 @@ from __future__ import annotations
 import argparse
 import json
 import os
+import socket
 import subprocess
 import tempfile
 import sys
@@ -428,10 +429,18 @@ def run_ours(args, rank, world, local_rank):
         cpu = cpu_baseline(U0, h, dt)
 
     # ---- the multi-patch workloads (overlap interpolation, boundary fluxes,
-    # level-set wall, many uneven patches)
-    extra = {}
-    for name in [w for w in args.workloads.split(",") if w]:
-        extra[name] = run_workload(name, args, dev, stream, rank, world, barrier, max_over_ranks)
+    # level-set wall, many uneven patches): on one GPU each workload whole;
+    # on several GPUs each workload sharded over the ranks (its patches
+    # partitioned, compact shadows, NCCL exchange of donor cells) and the
+    # periodic patch split into one i-slab per rank
+    extra, sharded = {}, {}
+    names = [w for w in args.workloads.split(",") if w]
+    if world == 1 and not args.sharded:
+        for name in names:
+            extra[name] = run_workload(name, args, dev, stream, rank, world, barrier, max_over_ranks)
+    else:
+        for name in (["slab"] if world > 1 else []) + names:
+            sharded[name] = run_sharded(name, args, dev, rank, world, barrier, max_over_ranks)
 
     if rank == 0:
         line = {
@@ -461,6 +470,8 @@ def run_ours(args, rank, world, local_rank):
             "clocks": clock_info,
             "workloads": extra,
         }
+        if sharded:
+            line["sharded"] = sharded
         print(json.dumps(line), flush=True)
     return 0
 
@@ -548,6 +559,65 @@ def run_workload(name, args, dev, stream, rank, world, barrier, max_over_ranks):
     return out
 
 
+def run_sharded(name, args, dev, rank, world, barrier, max_over_ranks):
+    """One workload sharded over the ranks (strong scaling: the whole grid's
+    cells are fixed): patches partitioned by cell count (`slab`: the periodic
+    n^3 patch split into one i-slab per rank), each rank holding its own
+    patches and compact shadows of the donor cells it reads, donor cells
+    exchanged by NCCL send/recv before every donor copy (drnum_b200.shard).
+    FP32 bulk; timed over args.steps steps after args.warmup, max over ranks."""
+    import torch
+    from drnum_b200 import _lib, cases, shard, workloads
+    tables = None
+    if name == "slab":
+        U0, h, dt = cases.periodic_box(args.n)
+        slabs = shard.slab_split((args.n,) * 3, world)
+        objs = shard.slab_patches(U0, h, slabs)
+        tables = [s["tables"] for s in slabs]
+        owner = list(range(world))
+        cells = args.n ** 3
+        desc = (f"periodic {args.n}^3 patch of the headline workload split into {world} i-slabs (2 seek planes "
+                "per side, copied from the neighbouring slab before every stage)")
+    else:
+        case = workloads.build(name, args.workload_scale)
+        _, objs = workloads.make_grid(case)
+        dt = case["dt"]
+        cells = sum(int(np.prod(p["n"])) for p in case["patches"])
+        owner = shard.partition([int(np.prod(p["n"])) for p in case["patches"]], world)
+        desc = case["description"]
+        del case
+    # one dn_rk_step per step (the level-set wall of the sphere is the
+    # context's own post-operation), the exchange in its donor-copy hook
+    sh = shard.make_sharded(objs, owner, rank, world, _lib.DN_FP32, dev.index, compact=True, tables=tables)
+    if any(o == rank for o in owner):
+        sh.it.autotune()
+    for _ in range(args.warmup):
+        sh.rkStep(dt, cases.RK3_ALPHA)
+    torch.cuda.synchronize(dev)
+    barrier()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(sh.stream)
+    for _ in range(args.steps):
+        sh.rkStep(dt, cases.RK3_ALPHA)
+    e1.record(sh.stream)
+    torch.cuda.synchronize(dev)
+    barrier()
+    t = max_over_ranks(e0.elapsed_time(e1) / 1e3)
+    held = max_over_ranks(float(sh.deviceCells()))
+    exchanges = 2 * len(cases.RK3_ALPHA)        # one before every donor copy of dn_rk_step
+    sent = max_over_ranks(float(sum(n_send for n_send, _ in sh.counts.values()) * 5 * 4 * exchanges))
+    sums = sh.conservationSums()
+    sh.close()
+    sh.it.close()
+    value = cells * STAGES * args.steps / t / 1e6
+    return {"description": desc, "cells": cells, "patches": len(objs), "ranks": world, "scaling": "strong",
+            "value": value, "unit": UNIT, "ms_per_step": t / args.steps * 1e3, "steps": args.steps,
+            "warmup": args.warmup, "max_device_cells_per_rank": held,
+            "device_cells_fraction_of_grid": held / cells,
+            "exchange_bytes_per_step_max_rank": sent, "mass_sum": float(sums[0])}
+
+
 def ctypes_void(x):
     import ctypes
     return ctypes.c_void_p(x)
@@ -567,6 +637,9 @@ def main():
                     help="comma-separated multi-patch workloads to add to the line ('' for none)")
     ap.add_argument("--workload-scale", type=float, default=1.0,
                     help="linear scale of the multi-patch workloads (1 = the full-size cases)")
+    ap.add_argument("--sharded", action="store_true",
+                    help="run the multi-patch workloads through the sharded path also on one GPU "
+                         "(always on several GPUs)")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "ours":
         args.warmup = 3
@@ -575,18 +648,26 @@ def main():
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
         return run_reference(args, rank, world)
-    if world > 1:
+    group = world > 1 or args.sharded
+    if group:
         import datetime
 
         import torch
         import torch.distributed as dist
         torch.cuda.set_device(local_rank)
+        kw = {}
+        if world == 1:
+            # a group of one for the sharded path on one GPU
+            with socket.socket() as sk:
+                sk.bind(("127.0.0.1", 0))
+                port = sk.getsockname()[1]
+            kw = {"init_method": f"tcp://127.0.0.1:{port}", "world_size": 1, "rank": 0}
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
-                                device_id=torch.device("cuda", local_rank))
+                                device_id=torch.device("cuda", local_rank), **kw)
     try:
         return run_ours(args, rank, world, local_rank)
     finally:
-        if world > 1:
+        if group:
             import torch.distributed as dist
             dist.destroy_process_group()
 

@@ -56,6 +56,8 @@ class dn_stage_launch(ctypes.Structure):
 
 
 DN_STAGE_FN = ctypes.CFUNCTYPE(c_int, c_void_p, POINTER(dn_stage_launch))
+DN_EXCHANGE_FN = ctypes.CFUNCTYPE(c_int, c_void_p)
+DN_FIELD_DONOR_COPY = -1
 
 
 class dn_patch_desc(ctypes.Structure):
@@ -136,6 +138,7 @@ SIGNATURES = {
     "dn_patch_set_owned": (c_int, [c_void_p, c_int, c_int]),
     "dn_patch_add_shadow": (c_int, [c_void_p, POINTER(dn_patch_desc), POINTER(c_int)]),
     "dn_shadow_alloc": (c_int, [c_void_p, c_void_p]),
+    "dn_set_exchange_hook": (c_int, [c_void_p, DN_EXCHANGE_FN, c_void_p]),
     "dn_patch_device_cells": (c_int, [c_void_p, c_int, POINTER(c_int64)]),
     "dn_patch_upload_async": (c_int, [c_void_p, c_int, c_int, POINTER(c_double)]),
     "dn_patch_upload_f32_async": (c_int, [c_void_p, c_int, c_int, POINTER(c_float)]),

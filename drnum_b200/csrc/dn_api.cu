@@ -159,6 +159,11 @@ struct dn_ctx {
   cudaEvent_t ev_out_read[2] = {nullptr, nullptr}, ev_d2h_done[2] = {nullptr, nullptr};
   bool ev_d2h_done_set[2] = {false, false};
   unsigned in_seq = 0, out_seq = 0;
+  // exchange hook of a sharded grid: called before every donor copy, with
+  // exch_phys the physical buffer about to receive the copy
+  dn_exchange_fn exch_fn = nullptr;
+  void* exch_user = nullptr;
+  int exch_phys = -1;
   // FP64 flux scheme (DN_FLUX_*) or a user stage function replacing it
   int scheme = DN_FLUX_AUSMPLUS;
   dn_stage_fn stage_fn = nullptr;
@@ -802,12 +807,20 @@ int levelset_bc(dn_ctx* c, int b, int step_b)
   return DN_OK;
 }
 
-// Donor copy into physical buffer `b` of every patch.
+// Donor copy into physical buffer `b` of every patch, preceded by the
+// exchange hook where one is set (every rank of a sharded grid exchanges
+// before every donor copy, whether or not its own patches receive).
 int donor_copy(dn_ctx* c, int b)
 {
   NvtxRange nvtx("dn donor copy");
-  if (!has_donors(c)) return DN_OK;
   int s;
+  if (c->exch_fn) {
+    c->exch_phys = b;
+    const int rc = c->exch_fn(c->exch_user);
+    c->exch_phys = -1;
+    if (rc) return fail(c, rc < 0 ? rc : DN_ERR_ARG, "exchange hook returned %d", rc);
+  }
+  if (!has_donors(c)) return DN_OK;
   if (c->plan_dirty && (s = build_plan(c))) return s;
   cudaError_t e = c->precision == DN_FP64 ? dn::launch_donor_copy_f64(c->plan, b, c->stream)
                                           : dn::launch_donor_copy_fx32(c->plan, b, c->d_err, c->stream);
@@ -866,7 +879,9 @@ int rk_step_enqueue(dn_ctx* c, double dt, const double* alpha, int n_alpha, int 
   // copy before each later stage (:34-36) repeats the previous stage's, so
   // it is skipped unless a post-operation (the level-set wall) may have
   // changed donor cells since
-  const bool post_op = any_levelset(c);
+  // (a sharded grid never skips it: a level-set wall on another rank may
+  // have changed donor cells this rank reads)
+  const bool post_op = any_levelset(c) || c->exch_fn != nullptr;
   if ((st = donor_copy(c, A))) return st;
   for (int s = 0; s < n_alpha; ++s) {
     const int out = (s & 1) ? Y : X;
@@ -1750,7 +1765,9 @@ int dn_rk_step(dn_ctx* c, double dt, const double* alpha, int n_alpha)
   // A = step-start state, X/Y = the two other buffers
   const int A = c->fmap[0], X = c->fmap[2], Y = c->fmap[1];
   int st;
-  if (c->use_graph) st = rk_step_graph(c, dt, alpha, n_alpha, A, X, Y);
+  // a step with an exchange hook runs its launches directly: the hook's
+  // transfers belong to the caller's library, not to a captured graph
+  if (c->use_graph && !c->exch_fn) st = rk_step_graph(c, dt, alpha, n_alpha, A, X, Y);
   else st = rk_step_enqueue(c, dt, alpha, n_alpha, A, X, Y);
   if (st) return st;
   const int last = ((n_alpha - 1) & 1) ? Y : X;
@@ -2391,7 +2408,11 @@ int exchange_move(dn_ctx* c, dn_exchange* e, int field, int peer, void* buf, boo
   NvtxRange nvtx("dn exchange");
   if (!c || !e) return DN_ERR_ARG;
   int s;
-  if ((s = check_field(c, field))) return s;
+  if (field == DN_FIELD_DONOR_COPY) {
+    if (c->exch_phys < 0) return fail(c, DN_ERR_STATE, "DN_FIELD_DONOR_COPY is valid only inside the exchange hook");
+  } else if ((s = check_field(c, field))) {
+    return s;
+  }
   if (peer < 0 || peer >= e->ex.world || peer == e->ex.rank) return fail(c, DN_ERR_ARG, "peer %d is not another rank", peer);
   if (set_device(c) != DN_OK) return DN_ERR_CUDA;
   if (c->plan_dirty && (s = build_plan(c))) return s;
@@ -2403,7 +2424,7 @@ int exchange_move(dn_ctx* c, dn_exchange* e, int field, int peer, void* buf, boo
   const int32_t* patch = static_cast<const int32_t*>(x.dev[(size_t)peer * 4 + (pack ? 0 : 2)]);
   const uint64_t* cell = static_cast<const uint64_t*>(x.dev[(size_t)peer * 4 + (pack ? 1 : 3)]);
   void* const* bufs = c->plan.bufs;
-  const int phys = c->fmap[field];
+  const int phys = field == DN_FIELD_DONOR_COPY ? c->exch_phys : c->fmap[field];
   const int blocks = (int)std::min<int64_t>((n + 255) / 256, (int64_t)c->num_sms * 8);
   if (c->precision == DN_FP64) {
     if (pack) k_exchange_pack<double><<<blocks, 256, 0, c->stream>>>(bufs, c->plan.nc, phys, patch, cell, n, (double*)buf);
@@ -2486,6 +2507,15 @@ int dn_set_flux_scheme(dn_ctx* c, int scheme)
   if (scheme != DN_FLUX_AUSMPLUS && c->precision != DN_FP64)
     return fail(c, DN_ERR_ARG, "flux scheme %d needs an FP64 context (FP32 runs AUSM+ only)", scheme);
   c->scheme = scheme;
+  c->generation++;
+  return DN_OK;
+}
+
+int dn_set_exchange_hook(dn_ctx* c, dn_exchange_fn fn, void* user)
+{
+  if (!c) return DN_ERR_ARG;
+  c->exch_fn = fn;
+  c->exch_user = user;
   c->generation++;
   return DN_OK;
 }

@@ -158,13 +158,30 @@ class ShardedIterator:
             check(it.ctx, lib.dn_exchange_counts(self.ex, q, ctypes.byref(ns), ctypes.byref(nr)))
             counts[q] = (ns.value, nr.value)
         self.counts = counts
-        # the library's work goes on torch's current stream, which NCCL orders with
-        self.stream = torch.cuda.current_stream()
+        # the library's work goes on a stream of its own (a real stream: a null
+        # handle would select the context's internal stream), made torch's
+        # current stream around every exchange, so that NCCL's send waits for
+        # the pack kernels and the unpack kernels wait for the receive
+        self.stream = torch.cuda.Stream(torch.cuda.current_device())
         check(it.ctx, lib.dn_set_stream(it.ctx, ctypes.c_void_p(self.stream.cuda_stream)))
         dtype = torch.float64 if it.precision == _lib.DN_FP64 else torch.int32
         self.transport = Transport(rank, world, counts, lambda n: torch.empty(n, dtype=dtype, device="cuda"),
                                    self._pack, self._unpack, group)
         self.post = []
+        # the exchange runs inside the library's own step, before every donor
+        # copy (dn_set_exchange_hook): one dn_rk_step per step, fields rotated
+        # in place, no field copy
+        self._hook_error = None
+        self._hook = _lib.DN_EXCHANGE_FN(self._on_donor_copy)
+        check(it.ctx, lib.dn_set_exchange_hook(it.ctx, self._hook, None))
+
+    def _on_donor_copy(self, user):
+        try:
+            self.exchange(_lib.DN_FIELD_DONOR_COPY)
+            return 0
+        except Exception as e:       # reported by the library call that ran the hook
+            self._hook_error = e
+            return _lib.DN_ERR_STATE
 
     def _pack(self, field, peer, buf):
         check(self.it.ctx, self.it.lib.dn_exchange_pack(self.it.ctx, self.ex, field, peer,
@@ -174,9 +191,12 @@ class ShardedIterator:
         check(self.it.ctx, self.it.lib.dn_exchange_unpack(self.it.ctx, self.ex, field, peer,
                                                           ctypes.c_void_p(buf.data_ptr())))
 
-    # operations of rk_step_sequence
+    # operations of rk_step_sequence (explicit exchanges: the hook is
+    # bypassed by _HookedOps below, which leaves the exchange to it)
     def exchange(self, field):
-        self.transport.exchange(field)
+        import torch
+        with torch.cuda.stream(self.stream):
+            self.transport.exchange(field)
 
     def copy_donor_data(self, field):
         self.it.copyDonorData(field)
@@ -195,7 +215,22 @@ class ShardedIterator:
         self.post.append(op)
 
     def rkStep(self, dt, alphas):
-        rk_step_sequence(self, dt, alphas)
+        """One RK step of this rank's patches.  Without post-operations the
+        library runs the whole step (dn_rk_step; the level-set walls set on
+        the context are its post-operations) with the exchange in its hook;
+        with Python post-operations the step runs stage by stage
+        (rk_step_sequence), every donor copy still preceded by the hook's
+        exchange."""
+        try:
+            if self.post:
+                rk_step_sequence(_HookedOps(self), dt, alphas)
+            else:
+                self.it.rkStep(dt, alphas)
+        except _lib.DnError:
+            if self._hook_error is not None:
+                e, self._hook_error = self._hook_error, None
+                raise e
+            raise
 
     def conservationSums(self):
         """FP64 conservation sums (mass, momenta, energy) of the whole grid:
@@ -217,22 +252,64 @@ class ShardedIterator:
 
     def close(self):
         if self.ex:
+            self.it.lib.dn_set_exchange_hook(self.it.ctx, _lib.DN_EXCHANGE_FN(), None)
             self.it.lib.dn_exchange_destroy(self.ex)
             self.ex = None
 
 
-def make_sharded(objs, owner, rank, world, precision, device=0, group=None, op=None, compact=True, fields=(0,)):
+class _HookedOps:
+    """rk_step_sequence operations of a ShardedIterator whose context runs
+    the exchange in its donor-copy hook: the sequence's own exchanges are
+    left out."""
+
+    def __init__(self, sh):
+        self.sh = sh
+
+    def exchange(self, field):
+        pass
+
+    def copy_donor_data(self, field):
+        self.sh.copy_donor_data(field)
+
+    def copy_field(self, src, dst):
+        self.sh.copy_field(src, dst)
+
+    def compute(self, factor):
+        self.sh.compute(factor)
+
+    def post_operations(self):
+        self.sh.post_operations()
+
+
+def make_sharded(objs, owner, rank, world, precision, device=0, group=None, op=None, compact=True, fields=(0,),
+                 tables=None):
     """A ShardedIterator over the patches `objs` (CartesianPatch objects of one
-    PatchGrid whose donor tables are computed) for `rank`: owned patches in
-    full, the others as compact shadows (compact=True) or full copies; the
-    host state of `fields` uploaded.  The process group must use NCCL and
-    `device` must be this rank's GPU."""
+    PatchGrid whose donor tables are computed, or with `tables`: per patch
+    donor tables in the layout of donorTables(), as slab_split gives them)
+    for `rank`: owned patches in full, the others as compact shadows
+    (compact=True) or full copies; the host state of `fields` uploaded.  The
+    process group must use NCCL and `device` must be this rank's GPU."""
     from .api import AusmPlus, B200CartesianIterator
     it = B200CartesianIterator(op if op is not None else AusmPlus(), device, precision)
     for p, cp in enumerate(objs):
         it.addPatch(cp, shadow=compact and owner[p] != rank)
+    if tables is not None:
+        for p, t in enumerate(tables):
+            it.setDonorTablesOf(p, t)
     it.updateDevice(fields=fields)
     return ShardedIterator(it, owner, rank, world, group)
+
+
+def slab_patches(U, h, slabs):
+    """CartesianPatch objects of the slabs of `slab_split` over the state U
+    of a patch periodic in every axis, with cell spacing h."""
+    from .api import CartesianPatch
+    objs = []
+    for s in slabs:
+        cp = CartesianPatch(*s["n"], spacing=(h, h, h), periodic=(False, True, True), num_fields=1)
+        cp.setField(0, slab_state(U, s))
+        objs.append(cp)
+    return objs
 
 
 def slab_split(n, world, halo=2):

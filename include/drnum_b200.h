@@ -506,6 +506,19 @@ int dn_exchange_build_ctx(dn_ctx* ctx, const int32_t* owner, int rank, int world
 int dn_exchange_counts(const dn_exchange* ex, int peer, int64_t* n_send, int64_t* n_recv);
 int dn_exchange_get(const dn_exchange* ex, int peer, int32_t* send_patch, uint64_t* send_cell, int32_t* recv_patch,
                     uint64_t* recv_cell);
+/* Exchange hook: fn(user) is called on the host before every donor copy the
+ * context makes (dn_rk_step, dn_copy_donor_data), also where this rank's
+ * patches receive nothing, with the copy's launches not yet enqueued; inside
+ * it, dn_exchange_pack / _unpack with field DN_FIELD_DONOR_COPY address the
+ * buffer the copy is about to read and fill.  A sharded rank moves its donor
+ * cells there (pack, send/recv on the context's stream, unpack), so that
+ * dn_rk_step runs the whole step in one call with the fields rotated in
+ * place.  With a hook, dn_rk_step never captures a graph and never skips
+ * the donor copy before a stage.  A nonzero return fails the calling
+ * function with that code.  fn NULL removes the hook. */
+#define DN_FIELD_DONOR_COPY (-1)
+typedef int (*dn_exchange_fn)(void* user);
+int dn_set_exchange_hook(dn_ctx* ctx, dn_exchange_fn fn, void* user);
 int dn_exchange_pack(dn_ctx* ctx, dn_exchange* ex, int field, int peer, void* dev_buf);
 int dn_exchange_unpack(dn_ctx* ctx, dn_exchange* ex, int field, int peer, const void* dev_buf);
 int dn_exchange_destroy(dn_exchange* ex);

@@ -598,3 +598,93 @@ def test_slab_split_over_two_contexts_with_compact_shadows(precision):
     for it, ex in zip(its, exs):
         lib.dn_exchange_destroy(ex)
         it.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision", [_lib.DN_FP64, _lib.DN_FP32])
+@pytest.mark.parametrize("name", ["octants_jet", "sphere_pair"])
+def test_exchange_hook_steps_in_two_threads_equal_one_context(golden_dir, name, precision):
+    # two contexts with compact shadows play two ranks, each stepping with
+    # dn_rk_step in a host thread of its own; the exchange hook packs the
+    # donor cells, the two threads meet at a host barrier, and each unpacks
+    # the other's packed buffer (kernels never wait on one another)
+    import threading
+    import torch
+    from test_gpu_grid import make_grid
+    world = 2
+    one, objs1, _, dt, steps = make_grid(name, precision)
+    for _ in range(steps):
+        one.rkStep(dt, cases.RK3_ALPHA)
+    one.updateHost(fields=(0,))
+    patches = cases_def.grid_layout(name)
+    owner = shard.partition([int(np.prod(p["n"])) for p in patches], world)
+    ranks = [make_grid(name, precision, shadows=[owner[p] != r for p in range(len(patches))]) for r in range(world)]
+    its = [r[0] for r in ranks]
+    lib = _lib.load()
+    dtype = torch.float64 if precision == _lib.DN_FP64 else torch.int32
+    exs, send = [], {}
+    for r, it in enumerate(its):
+        for p in range(len(patches)):
+            assert lib.dn_patch_set_owned(it.ctx, p, int(owner[p] == r)) == _lib.DN_OK
+        ex = ctypes.c_void_p()
+        own = (ctypes.c_int32 * len(owner))(*owner)
+        assert lib.dn_exchange_build_ctx(it.ctx, own, r, world, ctypes.byref(ex)) == _lib.DN_OK
+        assert lib.dn_shadow_alloc(it.ctx, ex) == _lib.DN_OK
+        ns, nr = ctypes.c_int64(), ctypes.c_int64()
+        assert lib.dn_exchange_counts(ex, 1 - r, ctypes.byref(ns), ctypes.byref(nr)) == _lib.DN_OK
+        send[r] = torch.empty(max(1, 5 * ns.value), dtype=dtype, device="cuda")
+        exs.append(ex)
+    meet = threading.Barrier(world, timeout=60)
+    calls = [0, 0]
+
+    def make_hook(r):
+        def hook(user):
+            it, ex, q = its[r], exs[r], 1 - r
+            if lib.dn_exchange_pack(it.ctx, ex, _lib.DN_FIELD_DONOR_COPY, q, ctypes.c_void_p(send[r].data_ptr())):
+                return -1
+            if lib.dn_sync(it.ctx):
+                return -1
+            meet.wait()
+            if lib.dn_exchange_unpack(it.ctx, ex, _lib.DN_FIELD_DONOR_COPY, q, ctypes.c_void_p(send[q].data_ptr())):
+                return -1
+            if lib.dn_sync(it.ctx):
+                return -1
+            meet.wait()            # both unpacked before either packs again
+            calls[r] += 1
+            return 0
+        return _lib.DN_EXCHANGE_FN(hook)
+
+    hooks = [make_hook(r) for r in range(world)]
+    for r in range(world):
+        assert lib.dn_set_exchange_hook(its[r].ctx, hooks[r], None) == _lib.DN_OK
+    status = [None, None]
+
+    def run(r):
+        try:
+            for _ in range(steps):
+                its[r].rkStep(dt, cases.RK3_ALPHA)
+            its[r].sync()
+            status[r] = "ok"
+        except Exception as e:      # noqa: BLE001
+            status[r] = repr(e)
+            meet.abort()
+
+    threads = [threading.Thread(target=run, args=(r,)) for r in range(world)]
+    for t in threads:
+        t.start()
+    for t in threads:
+        t.join(timeout=120)
+    assert status == ["ok", "ok"], status
+    assert calls == [2 * len(cases.RK3_ALPHA) * steps] * world
+    for it in its:
+        it.updateHost(fields=(0,))
+    for p in range(len(patches)):
+        assert np.array_equal(ranks[owner[p]][1][p].getField(0), objs1[p].getField(0)), (name, p)
+    # outside the hook the donor-copy field is refused
+    assert lib.dn_exchange_pack(its[0].ctx, exs[0], _lib.DN_FIELD_DONOR_COPY, 1,
+                                ctypes.c_void_p(send[0].data_ptr())) == _lib.DN_ERR_STATE
+    for r in range(world):
+        lib.dn_set_exchange_hook(its[r].ctx, _lib.DN_EXCHANGE_FN(), None)
+        lib.dn_exchange_destroy(exs[r])
+        its[r].close()
+    one.close()
