@@ -136,8 +136,14 @@ struct dn_ctx {
   // [kFxEdge]) and tile shape
   void* d_items[3][dn::kNumShapes] = {};
   int n_items[3][dn::kNumShapes] = {};
-  cudaStream_t s_aux = nullptr;               // second branch of a batched stage (edge and inside tiles)
-  int batch_min_planes = 8;                   // shortest plane range of a batched work item (autotuned)
+  void* d_groups[3][dn::kNumShapes] = {};     // FX32: item ranges of the persistent CTAs
+  int n_groups[3][dn::kNumShapes] = {};
+  // schedule of a batched stage (autotuned): batch_waves > 0 (FX32 only)
+  // deals the work to that many waves of persistent CTAs; 0 launches one
+  // CTA per work item, items of at least batch_min_planes planes
+  int batch_min_planes = 8;
+  int batch_waves = 2;
+  cudaStream_t s_aux = nullptr;               // second branch of a batched stage (inside and edge tiles)
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   // CUDA graphs of whole RK steps; any change of the case bumps generation
   bool use_graph = false;
@@ -961,6 +967,9 @@ void free_batch(dn_ctx* c)
       if (c->d_items[f][q]) cudaFree(c->d_items[f][q]);
       c->d_items[f][q] = nullptr;
       c->n_items[f][q] = 0;
+      if (c->d_groups[f][q]) cudaFree(c->d_groups[f][q]);
+      c->d_groups[f][q] = nullptr;
+      c->n_groups[f][q] = 0;
     }
   }
 }
@@ -977,9 +986,61 @@ int default_shape(const DnPatch& p)
   return p.d.nj >= 16 ? 2 : 0;
 }
 
+// Work items of persistent CTAs: the column runs (patch, column tile, all
+// planes) of one launch are cut along i and dealt in order to at most
+// `slots` CTAs (one wave) so that every CTA gets about the same number of
+// planes, each item charged kProlog planes for its prologue (three planes
+// staged and dequantised before the first update).  A CTA's items follow
+// one another along the runs; no piece is shorter than kMinPiece planes
+// where its run is longer.  The share per CTA starts at the even split and
+// grows by 1 % until the deal fits the wave.  Returns the items and the
+// group offsets (groups.size() - 1 CTAs).
+constexpr double kProlog = 3.0;
+constexpr int kMinPiece = 4;
+
+void deal_greedy(const std::vector<dn::WorkItem>& runs, double target, std::vector<dn::WorkItem>& items,
+                 std::vector<int>& groups)
+{
+  items.clear();
+  groups.assign(1, 0);
+  double acc = 0;
+  for (const auto& r : runs) {
+    int i = r.i0;
+    while (i < r.i1) {
+      if (acc > 0 && acc + kProlog + kMinPiece > target) {   // this CTA is full
+        groups.push_back((int)items.size());
+        acc = 0;
+      }
+      acc += kProlog;
+      int take = std::max((int)std::ceil(target - acc), kMinPiece);
+      take = std::min(take, r.i1 - i);
+      if (r.i1 - i - take > 0 && r.i1 - i - take < kMinPiece) take = r.i1 - i;   // no short leftover
+      items.push_back(dn::WorkItem{r.patch, r.j0, r.k0, i, i + take});
+      acc += take;
+      i += take;
+    }
+  }
+  groups.push_back((int)items.size());
+}
+
+void deal_runs(const std::vector<dn::WorkItem>& runs, int slots, std::vector<dn::WorkItem>& items,
+               std::vector<int>& groups)
+{
+  long planes = 0;
+  for (const auto& r : runs) planes += r.i1 - r.i0;
+  const long want = std::max(1L, std::min<long>(slots, planes / (2 * kMinPiece)));
+  double target = ((double)planes + kProlog * (double)want) / (double)want;
+  for (int k = 0; k < 400; ++k) {
+    deal_greedy(runs, target, items, groups);
+    if ((long)groups.size() - 1 <= want) return;
+    target *= 1.01;
+  }
+}
+
 // Patch records and work items (patch, column tile, plane range) of every
-// patch, grouped by tile shape; plane ranges are sized so that the launch
-// holds about four waves of CTAs.
+// patch, grouped by tile form and shape.  FX32: each launch is one wave of
+// persistent CTAs over balanced groups of items (deal_runs).  FP64: plane
+// ranges sized so that the launch holds about four waves of CTAs.
 int build_batch(dn_ctx* c)
 {
   free_batch(c);
@@ -1032,6 +1093,7 @@ int build_batch(dn_ctx* c)
   // face (per-thread face masks), tiles that reach beyond the patch; a
   // launch per form keeps one code path per kernel
   std::vector<dn::WorkItem> items[3][dn::kNumShapes];
+  std::vector<int> groups[3][dn::kNumShapes];
   for (size_t q = 0; q < np; ++q) {
     const DnPatch& P = c->patches[q];
     if (!P.owned || !P.patch_active) continue;
@@ -1039,9 +1101,12 @@ int build_batch(dn_ctx* c)
     int tj, tk;
     dn::shape_tile(fp64, sh, &tj, &tk);
     const bool per_y = P.d.face[1] == DN_FACE_PERIODIC, per_z = P.d.face[2] == DN_FACE_PERIODIC;
+    // persistent CTAs: one run of all planes per column tile, cut by
+    // deal_runs below
+    const bool persistent = !fp64 && c->batch_waves > 0;
     long ic = (P.d.ni + chunks - 1) / chunks;
     if (ic < c->batch_min_planes) ic = c->batch_min_planes;   // amortise each item's 3-plane prologue
-    if (ic > P.d.ni) ic = P.d.ni;
+    if (ic > P.d.ni || persistent) ic = P.d.ni;
     for (int i0 = 0; i0 < P.d.ni; i0 += (int)ic)
       for (int j0 = 0; j0 < P.d.nj; j0 += tj)
         for (int k0 = 0; k0 < P.d.nk; k0 += tk) {
@@ -1051,6 +1116,18 @@ int build_batch(dn_ctx* c)
           const int form = fp64 ? dn::kFxEdge : (fy && fz) ? dn::kFxFull : inside ? dn::kFxInside : dn::kFxEdge;
           items[form][sh].push_back(dn::WorkItem{(int)q, j0, k0, i0, std::min(P.d.ni, i0 + (int)ic)});
         }
+  }
+  if (!fp64 && c->batch_waves > 0) {
+    for (int f = 0; f < 3; ++f) {
+      for (int q = 0; q < dn::kNumShapes; ++q) {
+        if (items[f][q].empty()) continue;
+        int occ = 0;
+        cudaError_t e = dn::fx32_batched_occupancy(q, f, &occ);
+        if (e != cudaSuccess) return cuda_fail(c, e, "batched stage occupancy");
+        const std::vector<dn::WorkItem> runs = items[f][q];
+        deal_runs(runs, c->num_sms * std::max(1, occ) * c->batch_waves, items[f][q], groups[f][q]);
+      }
+    }
   }
   cudaError_t e = cudaMalloc(&c->d_records, np * sizeof(dn::BatchPatch));
   if (e != cudaSuccess) return fail(c, DN_ERR_NOMEM, "cudaMalloc(patch records)");
@@ -1073,6 +1150,14 @@ int build_batch(dn_ctx* c)
                           c->stream);
       if (e != cudaSuccess) return cuda_fail(c, e, "work item upload");
       c->n_items[f][q] = (int)it.size();
+      const std::vector<int>& gr = groups[f][q];
+      if (!gr.empty()) {
+        e = cudaMalloc(&c->d_groups[f][q], gr.size() * sizeof(int));
+        if (e != cudaSuccess) return fail(c, DN_ERR_NOMEM, "cudaMalloc(work groups)");
+        e = cudaMemcpyAsync(c->d_groups[f][q], gr.data(), gr.size() * sizeof(int), cudaMemcpyHostToDevice, c->stream);
+        if (e != cudaSuccess) return cuda_fail(c, e, "work group upload");
+        c->n_groups[f][q] = (int)gr.size() - 1;
+      }
     }
   }
   e = cudaStreamSynchronize(c->stream);   // host vectors go out of scope
@@ -1145,6 +1230,8 @@ int stage_all(dn_ctx* c, int in_b, int un_b, int out_b, double factor)
       b.maps = static_cast<const dn::BatchMaps*>(c->d_maps);
       b.items = static_cast<const dn::WorkItem*>(c->d_items[f][q]);
       b.n_items = c->n_items[f][q];
+      b.groups = static_cast<const int*>(c->d_groups[f][q]);
+      b.n_groups = c->n_groups[f][q];
       b.in_b = in_b; b.un_b = un_b; b.out_b = out_b;
       b.factor = factor;
       b.err = c->d_err;
@@ -2261,6 +2348,14 @@ int dn_set_option(dn_ctx* c, int option, int value)
     c->use_graph = value != 0;
     return DN_OK;
   }
+  if (option == DN_OPT_BATCH_WAVES || option == DN_OPT_BATCH_MIN_PLANES) {
+    if (value < (option == DN_OPT_BATCH_WAVES ? 0 : 1) || value > 64)
+      return fail(c, DN_ERR_ARG, "schedule option %d out of range: %d", option, value);
+    (option == DN_OPT_BATCH_WAVES ? c->batch_waves : c->batch_min_planes) = value;
+    c->batch_dirty = true;
+    c->generation++;
+    return DN_OK;
+  }
   return fail(c, DN_ERR_ARG, "unknown option %d", option);
 }
 
@@ -2698,19 +2793,28 @@ int dn_autotune(dn_ctx* c, const char* cache_path, double cost_out[DN_NUM_TILE_S
   }
   c->batch_dirty = true;
   c->generation++;
-  // batched stages: the shortest plane range of a work item, measured among
-  // a few candidates with the shapes just chosen (one stage of every patch
-  // into the scratch field, factor 0; the ranges change no result)
+  // batched stages: the schedule of the work items, measured among a few
+  // candidates with the shapes just chosen (one stage of every patch into
+  // the scratch field, factor 0; the schedule changes no result): FP64 the
+  // shortest plane range of an item; FX32 that, or instead the waves of
+  // persistent CTAs (fewer waves save prologues, more let the hardware even
+  // out tiles of unequal cost, one CTA per item keeps neighbouring columns
+  // on the same planes at the same time)
   if (c->batched && c->patches.size() > 1) {
     cudaEvent_t e0, e1;
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
-    const int cand[5] = {8, 16, 24, 32, 48};
-    int best = c->batch_min_planes;
+    const bool fp64 = c->precision == DN_FP64;
+    // (waves, shortest item): persistent waves for FP32 bulk, or one CTA per item
+    const int cand64[5][2] = {{0, 8}, {0, 16}, {0, 24}, {0, 32}, {0, 48}};
+    const int cand32[8][2] = {{0, 8}, {0, 16}, {0, 24}, {0, 32}, {0, 48}, {1, 8}, {2, 8}, {4, 8}};
+    const int n_cand = fp64 ? 5 : 8;
+    int best_w = c->batch_waves, best_p = c->batch_min_planes;
     double best_ms = 1e300;
     int st = DN_OK;
-    for (int k = 0; k < 5 && st == DN_OK; ++k) {
-      c->batch_min_planes = cand[k];
+    for (int k = 0; k < n_cand && st == DN_OK; ++k) {
+      c->batch_waves = fp64 ? cand64[k][0] : cand32[k][0];
+      c->batch_min_planes = fp64 ? cand64[k][1] : cand32[k][1];
       c->batch_dirty = true;
       for (int r = 0; r < 5 && st == DN_OK; ++r) {
         if (r == 2) cudaEventRecord(e0, c->stream);
@@ -2720,11 +2824,12 @@ int dn_autotune(dn_ctx* c, const char* cache_path, double cost_out[DN_NUM_TILE_S
       cudaEventSynchronize(e1);
       float ms = 0;
       cudaEventElapsedTime(&ms, e0, e1);
-      if (st == DN_OK && ms < best_ms) { best_ms = ms; best = cand[k]; }
+      if (st == DN_OK && ms < best_ms) { best_ms = ms; best_w = c->batch_waves; best_p = c->batch_min_planes; }
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
-    c->batch_min_planes = best;
+    c->batch_waves = best_w;
+    c->batch_min_planes = best_p;
     c->batch_dirty = true;
     c->generation++;
     if (st != DN_OK) return st;

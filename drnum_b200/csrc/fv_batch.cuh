@@ -47,6 +47,10 @@ struct Batch {
   const BatchMaps* maps;        // FX32: per patch, or NULL
   const WorkItem* items;
   int n_items;
+  // FX32: the items of persistent CTA b are items[groups[b] ..
+  // groups[b+1]-1], taken in order (NULL: one CTA per item); n_groups CTAs
+  const int* groups;
+  int n_groups;
   int in_b, un_b, out_b;        // physical buffers: stage input, step start, output
   double factor;                // alpha * dt
   int* err;
@@ -70,6 +74,39 @@ __device__ __forceinline__ void load_patch_record(BatchPatch& dst, const BatchPa
 // forms in one kernel made them compete for the instruction cache of an SM
 // running tiles of many patches (13-17 % slower on the jet and sphere
 // workloads).
+// Stage arguments of work item w in shared memory (thread 0; the caller
+// synchronises).
+__device__ __forceinline__ void fx_item_args(FxArgs& args, const BatchPatch& rec, const Batch& b, const WorkItem& w)
+{
+  args.in = static_cast<const int32_t*>(rec.buf[b.in_b]);
+  args.un = static_cast<const int32_t*>(rec.buf[b.un_b]);
+  args.out = static_cast<int32_t*>(rec.buf[b.out_b]);
+  args.active = rec.active;
+  args.err = b.err;
+  args.err_info = b.err_info;
+  args.g.ni = rec.ni; args.g.nj = rec.nj; args.g.nk = rec.nk; args.g.kp = rec.kp;
+  args.g.per_x = rec.per_x; args.g.per_y = rec.per_y; args.g.per_z = rec.per_z;
+  args.g.i_chunk = w.i1 - w.i0;
+  fx_set_params(args.p, rec.dx, rec.dy, rec.dz, b.factor, rec.base, rec.quantum);
+  args.wall = rec.wall;
+}
+
+// The tile form MODE (falling back to the edge form where the tile does not
+// qualify) of one work item; NEXT as fx_stage_tile_impl.
+template <int TJ, int TK, int MODE, bool NEXT>
+__device__ __forceinline__ bool fx_item(const FxArgs& args, const BatchPatch& rec, const Batch& b, const WorkItem& w)
+{
+  const BatchMaps* M = (b.maps && rec.tma) ? b.maps + w.patch : nullptr;
+  const CUtensorMap* tm_in = M ? M->in[b.in_b] : nullptr;
+  const CUtensorMap* tm_un = M ? &M->un[b.un_b] : nullptr;
+  if (MODE == kFxFull && fx_tile_full<TJ, TK>(args.g, w.j0, w.k0))
+    return fx_stage_tile_impl<TJ, TK, kFxFull, NEXT>(args, tm_in, tm_un, w.j0, w.k0, w.i0, w.i1);
+  if (MODE == kFxInside && fx_tile_inside<TJ, TK>(args.g, w.j0, w.k0))
+    return fx_stage_tile_impl<TJ, TK, kFxInside, NEXT>(args, tm_in, tm_un, w.j0, w.k0, w.i0, w.i1);
+  return fx_stage_tile_impl<TJ, TK, kFxEdge, NEXT>(args, tm_in, tm_un, w.j0, w.k0, w.i0, w.i1);
+}
+
+// One CTA per work item.
 template <int TJ, int TK, int MODE>
 __global__ void __launch_bounds__(TJ * TK / 2, FxOccupancy<TJ * TK / 2>::min_blocks)
 fx_stage_batched(const Batch b)
@@ -79,29 +116,35 @@ fx_stage_batched(const Batch b)
   const WorkItem w = b.items[blockIdx.x];
   load_patch_record(rec, b.patches + w.patch);
   __syncthreads();
-  if (threadIdx.x == 0 && threadIdx.y == 0) {
-    args.in = static_cast<const int32_t*>(rec.buf[b.in_b]);
-    args.un = static_cast<const int32_t*>(rec.buf[b.un_b]);
-    args.out = static_cast<int32_t*>(rec.buf[b.out_b]);
-    args.active = rec.active;
-    args.err = b.err;
-    args.err_info = b.err_info;
-    args.g.ni = rec.ni; args.g.nj = rec.nj; args.g.nk = rec.nk; args.g.kp = rec.kp;
-    args.g.per_x = rec.per_x; args.g.per_y = rec.per_y; args.g.per_z = rec.per_z;
-    args.g.i_chunk = w.i1 - w.i0;
-    fx_set_params(args.p, rec.dx, rec.dy, rec.dz, b.factor, rec.base, rec.quantum);
-    args.wall = rec.wall;
-  }
+  if (threadIdx.x == 0 && threadIdx.y == 0) fx_item_args(args, rec, b, w);
   __syncthreads();
-  const BatchMaps* M = (b.maps && rec.tma) ? b.maps + w.patch : nullptr;
-  const CUtensorMap* tm_in = M ? M->in[b.in_b] : nullptr;
-  const CUtensorMap* tm_un = M ? &M->un[b.un_b] : nullptr;
-  if (MODE == kFxFull && fx_tile_full<TJ, TK>(args.g, w.j0, w.k0))
-    fx_stage_tile_impl<TJ, TK, kFxFull>(args, tm_in, tm_un, w.j0, w.k0, w.i0, w.i1);
-  else if (MODE == kFxInside && fx_tile_inside<TJ, TK>(args.g, w.j0, w.k0))
-    fx_stage_tile_impl<TJ, TK, kFxInside>(args, tm_in, tm_un, w.j0, w.k0, w.i0, w.i1);
-  else
-    fx_stage_tile_impl<TJ, TK, kFxEdge>(args, tm_in, tm_un, w.j0, w.k0, w.i0, w.i1);
+  fx_item<TJ, TK, MODE, false>(args, rec, b, w);
+}
+
+// Persistent CTAs: CTA b takes the items groups[b] .. groups[b+1]-1 in
+// order.  The host deals the work so that one or a few waves of CTAs hold it
+// with equal planes per CTA and a CTA's items follow one another along i
+// (one prologue per item, no tail of short items).
+template <int TJ, int TK, int MODE>
+__global__ void __launch_bounds__(TJ * TK / 2, FxOccupancy<TJ * TK / 2>::min_blocks)
+fx_stage_batched_persistent(const Batch b)
+{
+  __shared__ __align__(16) BatchPatch rec;
+  __shared__ __align__(16) FxArgs args;
+  const int w_begin = b.groups[blockIdx.x], w_end = b.groups[blockIdx.x + 1];
+  int loaded = -1;                              // patch whose record is in shared memory
+  for (int wi = w_begin; wi < w_end; ++wi) {
+    // (every thread is past the previous item's closing barrier)
+    const WorkItem w = b.items[wi];
+    if (w.patch != loaded) {
+      load_patch_record(rec, b.patches + w.patch);
+      loaded = w.patch;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0 && threadIdx.y == 0) fx_item_args(args, rec, b, w);
+    __syncthreads();
+    if (!fx_item<TJ, TK, MODE, true>(args, rec, b, w)) return;   // a transfer may still be landing
+  }
 }
 
 template <int TJ, int TK>

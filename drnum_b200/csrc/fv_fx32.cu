@@ -64,10 +64,10 @@ template <int TJ, int TK, int MODE>
 cudaError_t launch_fx_batched(const Batch& b, cudaStream_t st)
 {
   using Smem = FxSmem<TJ, TK>;
-  auto kern = fx_stage_batched<TJ, TK, MODE>;
+  auto kern = b.groups ? fx_stage_batched_persistent<TJ, TK, MODE> : fx_stage_batched<TJ, TK, MODE>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(Smem));
   if (e != cudaSuccess) return e;
-  kern<<<b.n_items, dim3(TK / 2, TJ, 1), sizeof(Smem), st>>>(b);
+  kern<<<b.groups ? b.n_groups : b.n_items, dim3(TK / 2, TJ, 1), sizeof(Smem), st>>>(b);
   return cudaGetLastError();
 }
 
@@ -78,7 +78,32 @@ cudaError_t launch_fx_batched_shape(const Batch& b, int shape, cudaStream_t st)
   if (shape == 1) return launch_fx_batched<16, 16, MODE>(b, st);
   return launch_fx_batched<16, 32, MODE>(b, st);
 }
+
+template <int TJ, int TK, int MODE>
+cudaError_t occupancy_of(int* blocks)
+{
+  using Smem = FxSmem<TJ, TK>;
+  auto kern = fx_stage_batched_persistent<TJ, TK, MODE>;
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(Smem));
+  if (e != cudaSuccess) return e;
+  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks, kern, TJ * TK / 2, sizeof(Smem));
+}
+
+template <int MODE>
+cudaError_t occupancy_shape(int shape, int* blocks)
+{
+  if (shape == 0) return occupancy_of<8, 32, MODE>(blocks);
+  if (shape == 1) return occupancy_of<16, 16, MODE>(blocks);
+  return occupancy_of<16, 32, MODE>(blocks);
+}
 } // namespace
+
+cudaError_t fx32_batched_occupancy(int shape, int form, int* blocks)
+{
+  if (form == kFxFull) return occupancy_shape<kFxFull>(shape, blocks);
+  if (form == kFxInside) return occupancy_shape<kFxInside>(shape, blocks);
+  return occupancy_shape<kFxEdge>(shape, blocks);
+}
 
 cudaError_t launch_stage_fx32_batched(const Batch& b, int shape, int form, cudaStream_t st)
 {

@@ -423,8 +423,12 @@ __device__ __forceinline__ void fx_stage_slot(const FxGeom& g, bool tma, int j0,
 // periodic seam falls between pairs), so they dequantise pairwise.  MODE
 // kFxInside tiles (fx_tile_inside) dequantise pairwise too: a pair whose two
 // positions clamp to one edge cell of a closed k axis reads that cell twice.
-template <int TJ, int TK, int MODE>
-__device__ __forceinline__ void fx_stage_tile_impl(const FxArgs& a, const CUtensorMap* tm_in,
+// NEXT: the CTA takes another work item after this one (persistent CTAs):
+// the tile then ends with a barrier and retires its mbarriers, and returns
+// false (in every thread) when a TMA wait ran out, as a transfer may still
+// be writing shared memory and the CTA must take no further item.
+template <int TJ, int TK, int MODE, bool NEXT = false>
+__device__ __forceinline__ bool fx_stage_tile_impl(const FxArgs& a, const CUtensorMap* tm_in,
                                                    const CUtensorMap* tm_un, int j0, int k0, int i0, int i1)
 {
   using Smem = FxSmem<TJ, TK>;
@@ -1028,6 +1032,15 @@ __device__ __forceinline__ void fx_stage_tile_impl(const FxArgs& a, const CUtens
   }
   if (fbad && a.err) atomicOr(a.err, 16);
   if (tbad && a.err) atomicOr(a.err, kFxErrTma);
+  if (!NEXT) return true;
+  // every transfer the tile issued has completed unless a wait ran out: the
+  // mbarriers are then retired for the next work item's initialisation
+  const bool any_tbad = __syncthreads_or(tbad) != 0;
+  if (tma && tid == 0 && !any_tbad) {
+    mbar_inval(&sm.bar[0]);
+    mbar_inval(&sm.bar[1]);
+  }
+  return !any_tbad;
 }
 
 template <int TJ, int TK>

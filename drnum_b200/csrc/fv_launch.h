@@ -41,6 +41,8 @@ constexpr int kNumShapes = 3;
 // without edge tests
 // form: kFxEdge, kFxInside or kFxFull (the tile form of every item of b)
 cudaError_t launch_stage_fx32_batched(const Batch& b, int shape, int form, cudaStream_t st);
+// resident CTAs per SM of the batched FX32 kernel of a tile shape and form
+cudaError_t fx32_batched_occupancy(int shape, int form, int* blocks);
 cudaError_t launch_stage_f64_batched(const Batch& b, int shape, cudaStream_t st);
 inline void shape_tile(bool fp64, int shape, int* tj, int* tk)
 {

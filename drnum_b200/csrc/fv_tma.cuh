@@ -25,6 +25,13 @@ __device__ __forceinline__ void mbar_init(uint64_t* bar, unsigned count)
   asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" :: "r"(smem_u32(bar)), "r"(count) : "memory");
 }
 
+// retires an mbarrier whose every phase has completed, so that its shared
+// memory can be initialised again (the next work item of a CTA)
+__device__ __forceinline__ void mbar_inval(uint64_t* bar)
+{
+  asm volatile("mbarrier.inval.shared::cta.b64 [%0];" :: "r"(smem_u32(bar)) : "memory");
+}
+
 // makes the initialised mbarriers visible to the async proxy
 __device__ __forceinline__ void mbar_init_fence()
 {

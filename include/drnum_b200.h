@@ -354,10 +354,18 @@ int dn_lslayers_destroy(dn_lslayers* ls);
  *   DN_OPT_GRAPH (default 0): dn_rk_step captures the whole step (stages,
  *     donor copies, level-set wall) as a CUDA graph once per buffer rotation,
  *     dt and alphas, and replays it.
+ *   DN_OPT_BATCH_WAVES (FP32 bulk, default 2): > 0 deals each batched launch's
+ *     work to that many waves of persistent CTAs with equal planes per CTA;
+ *     0 launches one CTA per work item.  dn_autotune measures the choices.
+ *   DN_OPT_BATCH_MIN_PLANES (default 8): shortest plane range of a work item
+ *     when one CTA takes one item.
+ *   The schedule options change no result.
  * No reference counterpart (the reference launches 10 kernels per patch and
  * stage, each followed by a device synchronisation, gpu_cartesianiterator.h:218-304). */
 #define DN_OPT_BATCHED    0
 #define DN_OPT_GRAPH      1
+#define DN_OPT_BATCH_WAVES      2
+#define DN_OPT_BATCH_MIN_PLANES 3
 int dn_set_option(dn_ctx* ctx, int option, int value);
 
 /* Tile shape of a patch in the batched launch (j x k): 0 = 8 x 32 (FP64
