@@ -43,7 +43,7 @@ bool encode_stage_maps(CUtensorMap* tm_in, CUtensorMap* tm_un, const int32_t* in
 cudaError_t launch_stage_fx32(const FxArgs& a, cudaStream_t st)
 {
   using Smem = FxSmem<FX_TJ, FX_TK>;
-  auto kern = fx_stage_kernel<FX_TJ, FX_TK>;
+  auto kern = a.wall.any ? fx_stage_kernel<FX_TJ, FX_TK, true> : fx_stage_kernel<FX_TJ, FX_TK, false>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(Smem));
   if (e != cudaSuccess) return e;
   FxLaunch L;

@@ -426,8 +426,10 @@ __device__ __forceinline__ void fx_stage_slot(const FxGeom& g, bool tma, int j0,
 // NEXT: the CTA takes another work item after this one (persistent CTAs):
 // the tile then ends with a barrier and retires its mbarriers, and returns
 // false (in every thread) when a TMA wait ran out, as a transfer may still
-// be writing shared memory and the CTA must take no further item.
-template <int TJ, int TK, int MODE, bool NEXT = false>
+// be writing shared memory and the CTA must take no further item.  WALLS =
+// false: the patch has no patch-face fluxes (a.wall.any == 0), and their
+// code is left out.
+template <int TJ, int TK, int MODE, bool NEXT = false, bool WALLS = true>
 __device__ __forceinline__ bool fx_stage_tile_impl(const FxArgs& a, const CUtensorMap* tm_in,
                                                    const CUtensorMap* tm_un, int j0, int k0, int i0, int i1)
 {
@@ -919,44 +921,16 @@ __device__ __forceinline__ bool fx_stage_tile_impl(const FxArgs& a, const CUtens
         act_a = a.active[c] != 0;
         act_b = act_b && a.active[c + 1] != 0;
       }
-      // patch-face fluxes: boundary cells of a patch with wall fluxes sum
-      // their residual in 64 bits together with the wall terms
-      const bool edge_ijk = a.wall.any && (i == 0 || i == g.ni - 1 || j == 0 || j == g.nj - 1);
-      const bool wall_a = a.wall.any && (edge_ijk || ka == 0 || ka == g.nk - 1);
-      const bool wall_b = own_b && a.wall.any && (edge_ijk || kb == g.nk - 1);
-      int2 o[5];
-      if (!wide && !wall_a && !wall_b) {
-        // every face of the plane below kFxNarrowFace: |residual| < 2^31
-        // fits int32, and |un + residual| < 3 * 2^30, so the wrapped 32-bit
-        // sum lies in (-2^30, 2^30) exactly when the true one does
-        #pragma unroll
-        for (int v = 0; v < 5; ++v) {
-          const int2 ylo = *reinterpret_cast<const int2*>(&sm.qy[v][ty][kk]);
-          const int2 yhi = *reinterpret_cast<const int2*>(&sm.qy[v][ty + 1][kk]);
-          const int2 zlo = sm.qz[v][ty][tp];
-          const int zhi = sm.qz[v][ty][tp + 1].x;
-          const int2 un = *reinterpret_cast<const int2*>(&sm.un[v][ty][kk]);
-          const unsigned ra = (unsigned)qx_lo[v].x - (unsigned)qx_hi[v].x + (unsigned)ylo.x - (unsigned)yhi.x +
-                              (unsigned)zlo.x - (unsigned)zlo.y;
-          const unsigned rb = (unsigned)qx_lo[v].y - (unsigned)qx_hi[v].y + (unsigned)ylo.y - (unsigned)yhi.y +
-                              (unsigned)zlo.y - (unsigned)zhi;
-          o[v].x = (int)((unsigned)un.x + ra);
-          o[v].y = (int)((unsigned)un.y + rb);
-        }
-      } else {
-        // 64-bit residuals: a face of the plane beyond the narrow bound, or
-        // a boundary cell with patch-face fluxes
-        long long ra[5], rb[5];
-        #pragma unroll
-        for (int v = 0; v < 5; ++v) {
-          const int2 ylo = *reinterpret_cast<const int2*>(&sm.qy[v][ty][kk]);
-          const int2 yhi = *reinterpret_cast<const int2*>(&sm.qy[v][ty + 1][kk]);
-          const int2 zlo = sm.qz[v][ty][tp];
-          const int zhi = sm.qz[v][ty][tp + 1].x;
-          ra[v] = (long long)qx_lo[v].x - qx_hi[v].x + ylo.x - yhi.x + zlo.x - zlo.y;
-          rb[v] = (long long)qx_lo[v].y - qx_hi[v].y + ylo.y - yhi.y + zlo.y - zhi;
-        }
-        FaceRange wmag;
+      // patch-face fluxes of boundary cells: whole quanta like the interior
+      // faces (a wall face replaces the cell's missing interior face, so a
+      // cell still sums six faces)
+      const bool any_wall = WALLS && a.wall.any;
+      const bool edge_ijk = any_wall && (i == 0 || i == g.ni - 1 || j == 0 || j == g.nj - 1);
+      const bool wall_a = any_wall && (edge_ijk || ka == 0 || ka == g.nk - 1);
+      const bool wall_b = own_b && any_wall && (edge_ijk || kb == g.nk - 1);
+      long long wa[5] = {0, 0, 0, 0, 0}, wb[5] = {0, 0, 0, 0, 0};
+      FaceRange wmag;
+      if (wall_a || wall_b) {
         #pragma unroll
         for (int q = 0; q < 2; ++q) {
           if (q == 0 ? !wall_a : !wall_b) continue;
@@ -966,14 +940,44 @@ __device__ __forceinline__ bool fx_stage_tile_impl(const FxArgs& a, const CUtens
           #pragma unroll
           for (int v = 0; v < 5; ++v) uc[v] = fmaf(P.quantum[v].x, (float)a.in[v * nc + c + q], P.base[v].x);
           add_wall_fluxes(a.wall, g.ni, g.nj, g.nk, g.per_x, g.per_y, g.per_z, i, j, ka + q, uc, P.A[0].x, P.A[1].x,
-                          P.A[2].x, q == 0 ? ra : rb,
+                          P.A[2].x, q == 0 ? wa : wb,
                           [&](int v, float F) { return fx_quant1(F * P.face_scale[v].x, wmag); });
         }
         fbad |= !(wmag.mag() < kFxFaceLimit);
+      }
+      int2 o[5];
+      if (!wide && wmag.mag() < kFxNarrowFace) {
+        // every face of the plane and every wall face of the pair below
+        // kFxNarrowFace: |residual| < 2^31 fits int32, and |un + residual| <
+        // 3 * 2^30, so the wrapped 32-bit sum lies in (-2^30, 2^30) exactly
+        // when the true one does
         #pragma unroll
         for (int v = 0; v < 5; ++v) {
+          const int2 ylo = *reinterpret_cast<const int2*>(&sm.qy[v][ty][kk]);
+          const int2 yhi = *reinterpret_cast<const int2*>(&sm.qy[v][ty + 1][kk]);
+          const int2 zlo = sm.qz[v][ty][tp];
+          const int zhi = sm.qz[v][ty][tp + 1].x;
           const int2 un = *reinterpret_cast<const int2*>(&sm.un[v][ty][kk]);
-          const long long oa = (long long)un.x + ra[v], ob = (long long)un.y + rb[v];
+          const unsigned ra = (unsigned)qx_lo[v].x - (unsigned)qx_hi[v].x + (unsigned)ylo.x - (unsigned)yhi.x +
+                              (unsigned)zlo.x - (unsigned)zlo.y + (unsigned)wa[v];
+          const unsigned rb = (unsigned)qx_lo[v].y - (unsigned)qx_hi[v].y + (unsigned)ylo.y - (unsigned)yhi.y +
+                              (unsigned)zlo.y - (unsigned)zhi + (unsigned)wb[v];
+          o[v].x = (int)((unsigned)un.x + ra);
+          o[v].y = (int)((unsigned)un.y + rb);
+        }
+      } else {
+        // 64-bit residuals: a face of the plane or of the pair's walls
+        // beyond the narrow bound
+        #pragma unroll
+        for (int v = 0; v < 5; ++v) {
+          const int2 ylo = *reinterpret_cast<const int2*>(&sm.qy[v][ty][kk]);
+          const int2 yhi = *reinterpret_cast<const int2*>(&sm.qy[v][ty + 1][kk]);
+          const int2 zlo = sm.qz[v][ty][tp];
+          const int zhi = sm.qz[v][ty][tp + 1].x;
+          const int2 un = *reinterpret_cast<const int2*>(&sm.un[v][ty][kk]);
+          const long long ra = (long long)qx_lo[v].x - qx_hi[v].x + ylo.x - yhi.x + zlo.x - zlo.y + wa[v];
+          const long long rb = (long long)qx_lo[v].y - qx_hi[v].y + ylo.y - yhi.y + zlo.y - zhi + wb[v];
+          const long long oa = (long long)un.x + ra, ob = (long long)un.y + rb;
           // results outside the range are clamped to its edge and flagged below
           o[v].x = (int)(oa >= kFxLimit ? kFxLimit : (oa <= -kFxLimit ? -kFxLimit : oa));
           o[v].y = (int)(ob >= kFxLimit ? kFxLimit : (ob <= -kFxLimit ? -kFxLimit : ob));
@@ -1043,14 +1047,15 @@ __device__ __forceinline__ bool fx_stage_tile_impl(const FxArgs& a, const CUtens
   return !any_tbad;
 }
 
-template <int TJ, int TK>
+template <int TJ, int TK, bool WALLS>
 __device__ __forceinline__ void fx_stage_tile(const FxArgs& a, const CUtensorMap* tm_in, const CUtensorMap* tm_un,
                                               int j0, int k0, int i0, int i1)
 {
-  if (fx_tile_full<TJ, TK>(a.g, j0, k0)) fx_stage_tile_impl<TJ, TK, kFxFull>(a, tm_in, tm_un, j0, k0, i0, i1);
+  if (fx_tile_full<TJ, TK>(a.g, j0, k0))
+    fx_stage_tile_impl<TJ, TK, kFxFull, false, WALLS>(a, tm_in, tm_un, j0, k0, i0, i1);
   else if (fx_tile_inside<TJ, TK>(a.g, j0, k0))
-    fx_stage_tile_impl<TJ, TK, kFxInside>(a, tm_in, tm_un, j0, k0, i0, i1);
-  else fx_stage_tile_impl<TJ, TK, kFxEdge>(a, tm_in, tm_un, j0, k0, i0, i1);
+    fx_stage_tile_impl<TJ, TK, kFxInside, false, WALLS>(a, tm_in, tm_un, j0, k0, i0, i1);
+  else fx_stage_tile_impl<TJ, TK, kFxEdge, false, WALLS>(a, tm_in, tm_un, j0, k0, i0, i1);
 }
 
 // Parameters of the single-patch launch: the stage arguments and the tensor
@@ -1062,14 +1067,15 @@ struct FxLaunch {
   int tma;
 };
 
-// One patch per launch: grid (k tiles, j tiles, i chunks), block (TK/2, TJ).
-template <int TJ, int TK>
+// One patch per launch: grid (k tiles, j tiles, i chunks), block (TK/2, TJ);
+// WALLS: the patch has patch-face fluxes.
+template <int TJ, int TK, bool WALLS>
 __global__ void __launch_bounds__(TJ * TK / 2, FxOccupancy<TJ * TK / 2>::min_blocks)
 fx_stage_kernel(const __grid_constant__ FxLaunch L)
 {
   const int i0 = blockIdx.z * L.a.g.i_chunk;
-  fx_stage_tile<TJ, TK>(L.a, L.tma ? L.tm_in : nullptr, L.tma ? &L.tm_un : nullptr, blockIdx.y * TJ,
-                        blockIdx.x * TK, i0, min(L.a.g.ni, i0 + L.a.g.i_chunk));
+  fx_stage_tile<TJ, TK, WALLS>(L.a, L.tma ? L.tm_in : nullptr, L.tma ? &L.tm_un : nullptr, blockIdx.y * TJ,
+                               blockIdx.x * TK, i0, min(L.a.g.ni, i0 + L.a.g.i_chunk));
 }
 
 } // namespace dn
