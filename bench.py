@@ -417,11 +417,12 @@ def run_ours(args, rank, world, local_rank):
     launch_s = t32 / (STAGES * args.steps)
     achieved = bytes_per_launch / launch_s / 1e9
     # DRAM traffic of the kernel per launch, from one ncu capture of the three
-    # stage launches of an RK step on the periodic 192^3 patch (dram__bytes_read
-    # + dram__bytes_write: 35.2, 58.4 and 58.4 B per cell; stage 1 reads f(k-1)
-    # = f(n) once), averaged and scaled by the cells of this launch: the kernel
-    # streams each plane once, so the traffic grows with the cell count
-    TRAFFIC_BYTES_PER_CELL = 50.67
+    # stage launches of a timed RK step on the periodic 192^3 patch
+    # (dram__bytes_read + dram__bytes_write: 36.6, 58.1 and 58.2 B per cell;
+    # stage 1 reads f(k-1) = f(n) once), averaged and scaled by the cells of
+    # this launch: the kernel streams each plane once, so the traffic grows
+    # with the cell count
+    TRAFFIC_BYTES_PER_CELL = 50.9
     traffic = TRAFFIC_BYTES_PER_CELL * cells
 
     cpu = None
