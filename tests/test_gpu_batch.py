@@ -100,3 +100,37 @@ def test_single_patch_chunk_autotune_changes_no_result():
         outs.append(p.getField(0).copy())
         it.close()
     assert np.array_equal(outs[0], outs[1])
+
+
+@pytest.mark.parametrize("name", ["octants_jet", "sphere_pair"])
+def test_batched_schedules_give_the_same_result(name):
+    # one CTA per work item (items of 8 or 24 planes) and persistent CTAs
+    # over balanced item ranges (1, 2 or 4 waves, every tile shape), FP32
+    # bulk: the same bits as the per-patch launches
+    def run(waves, min_planes, shapes=None):
+        it, objs, _, dt, _ = make_grid(name, DN_FP32)
+        it.setOption(_lib.DN_OPT_BATCH_WAVES, waves)
+        it.setOption(_lib.DN_OPT_BATCH_MIN_PLANES, min_planes)
+        if shapes is not None:
+            for p in range(len(objs)):
+                it.setTile(p, shapes[p % len(shapes)])
+        for _ in range(3):
+            it.rkStep(dt, cases.RK3_ALPHA)
+        it.updateHost(fields=(0,))
+        it.close()
+        return [cp.getField(0).copy() for cp in objs]
+
+    ref, _ = _run(name, DN_FP32, 3, batched=0)
+    for waves, min_planes, shapes in [(0, 8, None), (0, 24, [2]), (1, 8, [2, 1]), (2, 8, [0]), (4, 8, [1, 2, 0])]:
+        got = run(waves, min_planes, shapes)
+        for x, y in zip(ref, got):
+            assert np.array_equal(x, y), (waves, min_planes, shapes)
+
+
+def test_schedule_options_are_checked():
+    it, _, _, _, _ = make_grid("octants_jet", DN_FP32)
+    lib = it.lib
+    assert lib.dn_set_option(it.ctx, _lib.DN_OPT_BATCH_WAVES, -1) == _lib.DN_ERR_ARG
+    assert lib.dn_set_option(it.ctx, _lib.DN_OPT_BATCH_MIN_PLANES, 0) == _lib.DN_ERR_ARG
+    assert lib.dn_set_option(it.ctx, _lib.DN_OPT_BATCH_WAVES, 3) == _lib.DN_OK
+    it.close()
