@@ -134,9 +134,11 @@ def gather_sums(local, group=None):
 class ShardedIterator:
     """The GPU side: a B200CartesianIterator holding every patch of the grid
     (donor tables computed for all of them), owning the patches `owner`
-    assigns to this rank, with an exchange plan and NCCL transport.  The
-    process group must use the NCCL backend and this rank's GPU must be the
-    current device."""
+    assigns to this rank, with an exchange plan and the process group's
+    transport.  With NCCL the buffers are device tensors; with gloo they are
+    host tensors, staged through device buffers around the pack and unpack
+    kernels (for ranks that share a device or hosts without NCCL).  This
+    rank's GPU must be the current device."""
 
     def __init__(self, it, owner, rank, world, group=None):
         import torch
@@ -165,8 +167,15 @@ class ShardedIterator:
         self.stream = torch.cuda.Stream(torch.cuda.current_device())
         check(it.ctx, lib.dn_set_stream(it.ctx, ctypes.c_void_p(self.stream.cuda_stream)))
         dtype = torch.float64 if it.precision == _lib.DN_FP64 else torch.int32
-        self.transport = Transport(rank, world, counts, lambda n: torch.empty(n, dtype=dtype, device="cuda"),
-                                   self._pack, self._unpack, group)
+        import torch.distributed as dist
+        self.host_transport = dist.get_backend(group) != "nccl"
+        self.dev_send = {q: torch.empty(5 * counts[q][0], dtype=dtype, device="cuda") for q in counts if counts[q][0]}
+        self.dev_recv = {q: torch.empty(5 * counts[q][1], dtype=dtype, device="cuda") for q in counts if counts[q][1]}
+        if self.host_transport:
+            alloc = lambda n: torch.empty(n, dtype=dtype, pin_memory=True)   # noqa: E731
+        else:
+            alloc = lambda n: torch.empty(n, dtype=dtype, device="cuda")     # noqa: E731
+        self.transport = Transport(rank, world, counts, alloc, self._pack, self._unpack, group)
         self.post = []
         # the exchange runs inside the library's own step, before every donor
         # copy (dn_set_exchange_hook): one dn_rk_step per step, fields rotated
@@ -184,12 +193,19 @@ class ShardedIterator:
             return _lib.DN_ERR_STATE
 
     def _pack(self, field, peer, buf):
+        dev = self.dev_send[peer] if self.host_transport else buf
         check(self.it.ctx, self.it.lib.dn_exchange_pack(self.it.ctx, self.ex, field, peer,
-                                                        ctypes.c_void_p(buf.data_ptr())))
+                                                        ctypes.c_void_p(dev.data_ptr())))
+        if self.host_transport:
+            buf.copy_(dev)                       # waits for the pack kernel (current stream)
 
     def _unpack(self, field, peer, buf):
+        dev = buf
+        if self.host_transport:
+            dev = self.dev_recv[peer]
+            dev.copy_(buf)                       # on the current stream, before the unpack kernel
         check(self.it.ctx, self.it.lib.dn_exchange_unpack(self.it.ctx, self.ex, field, peer,
-                                                          ctypes.c_void_p(buf.data_ptr())))
+                                                          ctypes.c_void_p(dev.data_ptr())))
 
     # operations of rk_step_sequence (explicit exchanges: the hook is
     # bypassed by _HookedOps below, which leaves the exchange to it)

@@ -26,6 +26,29 @@ def _fixture(golden_dir, name):
     return np.load(os.path.join(golden_dir, f"grid_{name}.npz"))
 
 
+def make_grid_objects(name, states=None):
+    """The host patches of a grid case (fields, boundary fluxes, level sets)
+    with their donor tables computed: (patches, dt, steps)."""
+    patches, st0, spacings, dt, steps = cases_def.grid_case(name)
+    states = st0 if states is None else states
+    grid = PatchGrid()
+    objs = []
+    bcs = cases_def.grid_bcs(name) or {}
+    G = cases_def.grid_levelset(name)
+    for q, (p, U) in enumerate(zip(patches, states)):
+        cp = CartesianPatch(*p["n"], lengths=p["length"], origin=p["origin"], periodic=(False, False, False),
+                            seek=p["seek"])
+        cp.setField(0, U)
+        for side, (kind, params, table) in bcs.get(q, {}).items():
+            cp.setBoundary(side, kind, params, table)
+        if G is not None:
+            cp.setLevelSet(G[q], cases_def.LS_INNER, cases_def.LS_OUTER, cases_def.LS_MIN_REL)
+        grid.insertPatch(cp)
+        objs.append(cp)
+    grid.computeDependencies()
+    return objs, dt, steps
+
+
 def make_grid(name, precision, states=None, op=None, shadows=None):
     patches, st0, spacings, dt, steps = cases_def.grid_case(name)
     states = st0 if states is None else states

@@ -688,3 +688,75 @@ def test_exchange_hook_steps_in_two_threads_equal_one_context(golden_dir, name, 
         lib.dn_exchange_destroy(exs[r])
         its[r].close()
     one.close()
+
+
+def _gloo_gpu_rank(rank, world, port, name, precision, result_path):
+    # one rank of a sharded grid on the shared GPU: compact shadows, the
+    # library's step with the exchange in its hook, gloo between the ranks
+    # (host-staged buffers; no kernel waits on another process)
+    import datetime
+    import torch
+    import torch.distributed as dist
+    from test_gpu_grid import make_grid_objects
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    torch.cuda.set_device(0)
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=120))
+    try:
+        objs, dt, steps = make_grid_objects(name)
+        owner = shard.partition([int(np.prod(cp.data.shape[2:])) for cp in objs], world)
+        sh = shard.make_sharded(objs, owner, rank, world, precision, 0)
+        for _ in range(steps):
+            sh.rkStep(dt, cases.RK3_ALPHA)
+        sh.it.updateHost(fields=(0,))
+        sums = sh.conservationSums()
+        held = sh.deviceCells()
+        mine = {f"p{p}": objs[p].getField(0) for p in range(len(objs)) if owner[p] == rank}
+        np.savez(f"{result_path}.{rank}.npz", sums=sums, held=held, **mine)
+        sh.close()
+        sh.it.close()
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision", [_lib.DN_FP64, _lib.DN_FP32])
+@pytest.mark.parametrize("name", ["octants_jet", "sphere_pair"])
+def test_sharded_processes_on_one_gpu_equal_one_context(tmp_path, name, precision):
+    # two processes play two ranks end to end through shard.make_sharded
+    # (partition, compact shadows, exchange in the step's hook, gathered
+    # sums), their buffers moved by gloo through the host
+    from test_gpu_grid import make_grid
+    world = 2
+    one, objs1, _, dt, steps = make_grid(name, precision)
+    for _ in range(steps):
+        one.rkStep(dt, cases.RK3_ALPHA)
+    one.updateHost(fields=(0,))
+    sums1 = one.conservationSums()
+    total = sum(one.deviceCells(p) for p in range(len(objs1)))
+    one.close()
+    result = str(tmp_path / "rank")
+    ctx = mp.get_context("spawn")
+    port = _free_port()
+    procs = [ctx.Process(target=_gloo_gpu_rank, args=(r, world, port, name, precision, result)) for r in range(world)]
+    for p in procs:
+        p.start()
+    for p in procs:
+        p.join(timeout=300)
+    for p in procs:
+        if p.is_alive():
+            p.kill()
+    assert all(p.exitcode == 0 for p in procs), [p.exitcode for p in procs]
+    seen = set()
+    for r in range(world):
+        z = np.load(f"{result}.{r}.npz")
+        for k in z.files:
+            if k.startswith("p"):
+                p = int(k[1:])
+                assert np.array_equal(z[k], objs1[p].getField(0)), (name, p)
+                seen.add(p)
+        # the grid's sums, gathered in rank order: the single context's up to
+        # the order of the per-patch additions
+        assert np.allclose(z["sums"], sums1, rtol=1e-13, atol=0.0)
+        assert int(z["held"]) < total
+    assert seen == set(range(len(objs1)))
