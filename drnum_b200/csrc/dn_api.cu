@@ -26,6 +26,7 @@
 #include <algorithm>
 #include <cstring>
 #include <string>
+#include <unordered_map>
 #include <vector>
 
 namespace {
@@ -88,11 +89,14 @@ inline bool dev_cell(const DnPatch& p, uint64_t c, uint64_t* out)
 struct GraphEntry {
   int A = 0, X = 0, Y = 0, n = 0;
   double dt = 0, alpha[16] = {};
+  bool skip0 = false;                  // the step-start donor copy left out (its buffer was current)
   cudaGraphExec_t exec = nullptr;
   int64_t launches = 0;
+  int fresh_after = -1;                // the context's donor_fresh once the step has run
   bool same(const GraphEntry& o) const
   {
-    if (A != o.A || X != o.X || Y != o.Y || n != o.n || std::memcmp(&dt, &o.dt, sizeof dt)) return false;
+    if (A != o.A || X != o.X || Y != o.Y || n != o.n || skip0 != o.skip0 || std::memcmp(&dt, &o.dt, sizeof dt))
+      return false;
     return std::memcmp(alpha, o.alpha, sizeof(double) * n) == 0;
   }
 };
@@ -118,6 +122,13 @@ struct dn_ctx {
   bool plan_dirty = true;
   std::vector<void*> plan_mem;
   dn::DonorPlan plan{};
+  // physical buffer whose receiving cells hold the donor copy of its own
+  // donor cells under the current plan (-1: none known), valid while the
+  // case generation is donor_fresh_gen; plan_chained: some donor cell is a
+  // receiving cell, so a donor copy is not idempotent
+  int donor_fresh = -1;
+  int64_t donor_fresh_gen = -1;
+  bool plan_chained = false;
   // level-set layers per patch and their device form
   std::vector<dn::LevelSetLayers> ls;
   std::vector<char> ls_on;
@@ -582,6 +593,7 @@ bool has_donors(const dn_ctx* c)
 int build_plan(dn_ctx* c)
 {
   free_plan(c);
+  c->donor_fresh = -1;
   const size_t np = c->patches.size();
   std::vector<int32_t> rv_patch, rv_grp(1, 0), gp_donor, gp_stride;
   std::vector<int64_t> rv_cell, gp_wi, idx, nc(np);
@@ -649,32 +661,116 @@ int build_plan(dn_ctx* c)
   }
   if (rv_patch.size() >= (size_t)INT32_MAX || gp_donor.size() >= (size_t)INT32_MAX)
     return fail(c, DN_ERR_RANGE, "too many receiving cells or donor groups for one donor plan");
-  int s;
-  dn::DonorPlan& P = c->plan;
-  P.n_recv = (int32_t)rv_patch.size();
-  if ((s = plan_upload(c, rv_patch, &P.rv_patch)) || (s = plan_upload(c, rv_grp, &P.rv_grp)) ||
-      (s = plan_upload(c, gp_donor, &P.gp_donor)) || (s = plan_upload(c, gp_stride, &P.gp_stride)) ||
-      (s = plan_upload(c, w, &P.w)) || (s = plan_upload(c, nc, &P.nc)) ||
-      (s = plan_upload(c, base, &P.base)) || (s = plan_upload(c, quantum, &P.quantum))) {
-    free_plan(c);
-    return s;
+  // a donor cell that is also a receiving cell (of the plan) would make a
+  // repeated donor copy read what the last one wrote
+  {
+    std::vector<std::vector<bool>> recv(np);
+    for (size_t r = 0; r < np && r < c->tables.size(); ++r) {
+      const DnPatch& P = c->patches[r];
+      if (!P.owned || c->tables[r].rec_unique.empty()) continue;
+      recv[r].assign((size_t)P.d.ni * P.d.nj * P.d.nk, false);
+      for (uint64_t u : c->tables[r].rec_unique) if (u < recv[r].size()) recv[r][u] = true;
+    }
+    bool chained = false;
+    for (size_t r = 0; r < np && r < c->tables.size() && !chained; ++r) {
+      if (!c->patches[r].owned) continue;
+      const dn::DonorTables& T = c->tables[r];
+      size_t o = 0;
+      for (size_t q = 0; q < T.donor_patch.size() && !chained; ++q) {
+        const std::vector<bool>& R = recv[(size_t)T.donor_patch[q]];
+        const size_t m = (size_t)(T.num_receivers[q] * T.stride[q]);
+        if (!R.empty()) {
+          for (size_t e = 0; e < m; ++e) {
+            const uint64_t d = T.donor_idx[o + e];
+            if (d < R.size() && R[d]) { chained = true; break; }
+          }
+        }
+        o += m;
+      }
+    }
+    c->plan_chained = chained;
   }
-  // cell offsets and contribution offsets in 32 bits when they all fit
+  // pattern form: every group as (first donor cell, pattern id), the
+  // patterns (donor patch, offsets from the first donor cell, weights)
+  // listed once.  FP32-bulk plans leave zero weights out: a donor value is
+  // always finite there, and adding +-0 to a sum that starts at +0 never
+  // changes it.
   auto fits32 = [](const std::vector<int64_t>& v) {
     for (int64_t x : v) if (x < 0 || x > (int64_t)UINT32_MAX) return false;
     return true;
   };
-  P.narrow = fits32(rv_cell) && fits32(gp_wi) && fits32(idx) ? 1 : 0;
-  if (P.narrow) {
-    const std::vector<uint32_t> rc(rv_cell.begin(), rv_cell.end()), gw(gp_wi.begin(), gp_wi.end()),
-        ix(idx.begin(), idx.end());
-    if ((s = plan_upload(c, rc, &P.rv_cell32)) || (s = plan_upload(c, gw, &P.gp_wi32)) ||
-        (s = plan_upload(c, ix, &P.idx32))) {
+  bool patterned = fits32(rv_cell) && fits32(idx);
+  std::vector<uint2> gp_bp;
+  std::vector<int32_t> pt_donor, pt_start(1, 0), pt_off;
+  std::vector<double> pt_w;
+  if (patterned) {
+    const bool drop_zero = c->precision != DN_FP64;
+    std::unordered_map<std::string, int32_t> ids;
+    std::string key, last_key;
+    int32_t last_id = -1;
+    gp_bp.resize(gp_donor.size());
+    for (size_t g = 0; g < gp_donor.size() && patterned; ++g) {
+      const int64_t w0 = gp_wi[g], n = gp_stride[g];
+      const int64_t c0 = n > 0 ? idx[(size_t)w0] : 0;
+      key.assign(reinterpret_cast<const char*>(&gp_donor[g]), sizeof(int32_t));
+      for (int64_t q = 0; q < n; ++q) {
+        const double ws = w[(size_t)(w0 + q)];
+        if (drop_zero && ws == 0.0) continue;
+        const int64_t d = idx[(size_t)(w0 + q)] - c0;
+        if (d < INT32_MIN || d > INT32_MAX) { patterned = false; break; }
+        const int32_t d32 = (int32_t)d;
+        key.append(reinterpret_cast<const char*>(&d32), sizeof(d32));
+        key.append(reinterpret_cast<const char*>(&ws), sizeof(ws));
+      }
+      if (!patterned) break;
+      int32_t id = last_id;
+      if (key != last_key) {
+        auto it = ids.find(key);
+        if (it != ids.end()) {
+          id = it->second;
+        } else {
+          if (pt_donor.size() >= (size_t)INT32_MAX - 1) { patterned = false; break; }
+          id = (int32_t)pt_donor.size();
+          ids.emplace(key, id);
+          pt_donor.push_back(gp_donor[g]);
+          for (size_t o = sizeof(int32_t); o < key.size(); o += sizeof(int32_t) + sizeof(double)) {
+            int32_t d32;
+            double ws;
+            std::memcpy(&d32, key.data() + o, sizeof(d32));
+            std::memcpy(&ws, key.data() + o + sizeof(d32), sizeof(ws));
+            pt_off.push_back(d32);
+            pt_w.push_back(ws);
+          }
+          if (pt_off.size() >= (size_t)INT32_MAX) { patterned = false; break; }
+          pt_start.push_back((int32_t)pt_off.size());
+        }
+        last_key = key;
+        last_id = id;
+      }
+      gp_bp[g] = make_uint2((unsigned)c0, (unsigned)id);
+    }
+  }
+  int s;
+  dn::DonorPlan& P = c->plan;
+  P.n_recv = (int32_t)rv_patch.size();
+  P.patterned = patterned ? 1 : 0;
+  if ((s = plan_upload(c, rv_patch, &P.rv_patch)) || (s = plan_upload(c, rv_grp, &P.rv_grp)) ||
+      (s = plan_upload(c, nc, &P.nc)) || (s = plan_upload(c, base, &P.base)) ||
+      (s = plan_upload(c, quantum, &P.quantum))) {
+    free_plan(c);
+    return s;
+  }
+  if (patterned) {
+    const std::vector<uint32_t> rc(rv_cell.begin(), rv_cell.end());
+    if ((s = plan_upload(c, rc, &P.rv_cell32)) || (s = plan_upload(c, gp_bp, &P.gp_bp)) ||
+        (s = plan_upload(c, pt_donor, &P.pt_donor)) || (s = plan_upload(c, pt_start, &P.pt_start)) ||
+        (s = plan_upload(c, pt_off, &P.pt_off)) || (s = plan_upload(c, pt_w, &P.pt_w))) {
       free_plan(c);
       return s;
     }
-  } else if ((s = plan_upload(c, rv_cell, &P.rv_cell)) || (s = plan_upload(c, gp_wi, &P.gp_wi)) ||
-             (s = plan_upload(c, idx, &P.idx))) {
+  } else if ((s = plan_upload(c, rv_cell, &P.rv_cell)) || (s = plan_upload(c, gp_donor, &P.gp_donor)) ||
+             (s = plan_upload(c, gp_stride, &P.gp_stride)) || (s = plan_upload(c, gp_wi, &P.gp_wi)) ||
+             (s = plan_upload(c, idx, &P.idx)) || (s = plan_upload(c, w, &P.w))) {
     free_plan(c);
     return s;
   }
@@ -787,6 +883,8 @@ int build_ls_plan(dn_ctx* c)
   return DN_OK;
 }
 
+void donor_stale(dn_ctx* c, int b);
+
 // Level-set wall conditions on physical buffer `b` of every patch (step_b:
 // the step-start state, which the GPU level-set path resets its
 // deactivated cells to).
@@ -797,6 +895,7 @@ int levelset_bc(dn_ctx* c, int b, int step_b)
   for (char on : c->ls_on) any = any || on;
   for (char on : c->lsg_on) any_gpu = any_gpu || on;
   if (!any && !any_gpu) return DN_OK;
+  donor_stale(c, b);
   int s;
   if (c->ls_dirty && (s = build_ls_plan(c))) return s;
   const dn::LsPlan& L = c->ls_plan;
@@ -811,6 +910,23 @@ int levelset_bc(dn_ctx* c, int b, int step_b)
   }
   if (e != cudaSuccess) return cuda_fail(c, e, "level-set boundary launch");
   return DN_OK;
+}
+
+// Physical buffer b is written by something other than a donor copy (b < 0:
+// any buffer): its receiving cells may no longer match its donor cells.
+void donor_stale(dn_ctx* c, int b)
+{
+  if (b < 0 || c->donor_fresh == b) c->donor_fresh = -1;
+}
+
+// Buffer b's receiving cells hold the donor copy of its current donor cells
+// under the current plan, so a donor copy into b would rewrite the same
+// values.  Never for a sharded grid (other ranks change donor cells) or a
+// plan whose donor cells include receiving cells.
+bool donor_current(const dn_ctx* c, int b)
+{
+  return b >= 0 && c->donor_fresh == b && c->donor_fresh_gen == c->generation && !c->plan_dirty &&
+         !c->plan_chained && !c->exch_fn;
 }
 
 // Donor copy into physical buffer `b` of every patch, preceded by the
@@ -832,6 +948,8 @@ int donor_copy(dn_ctx* c, int b)
                                           : dn::launch_donor_copy_fx32(c->plan, b, c->d_err, c->stream);
   c->launches++;
   if (e != cudaSuccess) return cuda_fail(c, e, "donor copy launch");
+  c->donor_fresh = c->exch_fn ? -1 : b;
+  c->donor_fresh_gen = c->generation;
   return DN_OK;
 }
 
@@ -887,8 +1005,11 @@ int rk_step_enqueue(dn_ctx* c, double dt, const double* alpha, int n_alpha, int 
   // changed donor cells since
   // (a sharded grid never skips it: a level-set wall on another rank may
   // have changed donor cells this rank reads)
+  // (the step-start copy is also left out when A's receiving cells already
+  // hold it: the last step ended with a donor copy into A and nothing has
+  // written A since; a repeated copy would write the same bits)
   const bool post_op = any_levelset(c) || c->exch_fn != nullptr;
-  if ((st = donor_copy(c, A))) return st;
+  if (!donor_current(c, A) && (st = donor_copy(c, A))) return st;
   for (int s = 0; s < n_alpha; ++s) {
     const int out = (s & 1) ? Y : X;
     const double factor = alpha[s] * dt;   // (*i)*dt, rungekutta.cpp:37
@@ -927,6 +1048,7 @@ int rk_step_graph(dn_ctx* c, double dt, const double* alpha, int n_alpha, int A,
   }
   GraphEntry key;
   key.A = A; key.X = X; key.Y = Y; key.dt = dt; key.n = n_alpha;
+  key.skip0 = donor_current(c, A);
   for (int q = 0; q < n_alpha; ++q) key.alpha[q] = alpha[q];
   GraphEntry* hit = nullptr;
   for (auto& gc : c->graphs) if (gc.same(key)) hit = &gc;
@@ -941,6 +1063,7 @@ int rk_step_graph(dn_ctx* c, double dt, const double* alpha, int n_alpha, int A,
     if (st) { if (g) cudaGraphDestroy(g); return st; }
     if (e != cudaSuccess) return cuda_fail(c, e, "end graph capture");
     key.launches = c->launches - l0;
+    key.fresh_after = c->donor_fresh;
     c->launches = l0;
     e = cudaGraphInstantiate(&key.exec, g, 0);
     cudaGraphDestroy(g);
@@ -951,6 +1074,8 @@ int rk_step_graph(dn_ctx* c, double dt, const double* alpha, int n_alpha, int A,
   cudaError_t e = cudaGraphLaunch(hit->exec, c->stream);
   if (e != cudaSuccess) return cuda_fail(c, e, "graph launch");
   c->launches += hit->launches;
+  c->donor_fresh = hit->fresh_after;
+  c->donor_fresh_gen = c->generation;
   return DN_OK;
 }
 
@@ -1182,6 +1307,7 @@ int carry_patch(dn_ctx* c, DnPatch& p, int in_b, int out_b)
 int stage_all(dn_ctx* c, int in_b, int un_b, int out_b, double factor)
 {
   NvtxRange nvtx("dn stage");
+  donor_stale(c, out_b);
   int s;
   for (auto& p : c->patches) {
     if (p.owned && !p.patch_active && (s = carry_patch(c, p, in_b, out_b))) return s;
@@ -1366,6 +1492,7 @@ int upload_impl(dn_ctx* c, int id, int field, const H* host)
   if ((s = check_field(c, field))) return s;
   if (!host) return fail(c, DN_ERR_ARG, "host pointer is NULL");
   if (set_device(c) != DN_OK) return DN_ERR_CUDA;
+  donor_stale(c, c->fmap[field]);
   DnPatch& p = c->patches[id];
   if (p.compact) return upload_shadow(c, p, field, host);
   void* dst = p.buf[c->fmap[field]];
@@ -1379,9 +1506,9 @@ int upload_impl(dn_ctx* c, int id, int field, const H* host)
   if (c->precision == DN_FP32 && !p.base_set) {
     derive_base(p, host);
     c->plan_dirty = true;
-  c->ls_dirty = true;
-  c->batch_dirty = true;
-  c->generation++;
+    c->ls_dirty = true;
+    c->batch_dirty = true;
+    c->generation++;
   }
   if ((s = ensure_staging(c, n * sizeof(H)))) return s;
   e = cudaMemcpyAsync(c->staging, host, n * sizeof(H), cudaMemcpyHostToDevice, c->stream);
@@ -1473,6 +1600,7 @@ int upload_async_impl(dn_ctx* c, int id, int field, const H* host)
   if (!host) return fail(c, DN_ERR_ARG, "host pointer is NULL");
   if (set_device(c) != DN_OK) return DN_ERR_CUDA;
   if ((s = ensure_async(c))) return s;
+  donor_stale(c, c->fmap[field]);
   DnPatch& p = c->patches[id];
   if (c->precision == DN_FP32 && !p.base_set) {
     derive_base(p, host);
@@ -1784,6 +1912,7 @@ int dn_copy_field(dn_ctx* c, int i_src, int i_dst)
   if ((s = check_field(c, i_src)) || (s = check_field(c, i_dst))) return s;
   if (i_src == i_dst) return DN_OK;
   if (set_device(c) != DN_OK) return DN_ERR_CUDA;
+  donor_stale(c, c->fmap[i_dst]);
   for (auto& p : c->patches) {
     if (p.ncp == 0) continue;               // a compact shadow that holds no cell
     cudaError_t e = cudaMemcpyAsync(p.buf[c->fmap[i_dst]], p.buf[c->fmap[i_src]], 5 * p.ncp * elem_size(c),
@@ -1818,6 +1947,7 @@ int dn_compute_patches(dn_ctx* c, double factor, const int32_t* ids, int n)
   if (set_device(c) != DN_OK) return DN_ERR_CUDA;
   NvtxRange nvtx("dn stage (patch list)");
   const int in_b = c->fmap[0], un_b = c->fmap[1], out_b = c->fmap[2];
+  donor_stale(c, out_b);
   int s;
   for (size_t q = 0; q < c->patches.size(); ++q) {
     DnPatch& p = c->patches[q];
@@ -2520,6 +2650,7 @@ int exchange_move(dn_ctx* c, dn_exchange* e, int field, int peer, void* buf, boo
   const uint64_t* cell = static_cast<const uint64_t*>(x.dev[(size_t)peer * 4 + (pack ? 1 : 3)]);
   void* const* bufs = c->plan.bufs;
   const int phys = field == DN_FIELD_DONOR_COPY ? c->exch_phys : c->fmap[field];
+  if (!pack) donor_stale(c, phys);
   const int blocks = (int)std::min<int64_t>((n + 255) / 256, (int64_t)c->num_sms * 8);
   if (c->precision == DN_FP64) {
     if (pack) k_exchange_pack<double><<<blocks, 256, 0, c->stream>>>(bufs, c->plan.nc, phys, patch, cell, n, (double*)buf);
@@ -2703,6 +2834,7 @@ int dn_autotune(dn_ctx* c, const char* cache_path, double cost_out[DN_NUM_TILE_S
   if (!c) return DN_ERR_ARG;
   if (c->patches.empty()) return fail(c, DN_ERR_STATE, "no patches to tune for");
   if (set_device(c) != DN_OK) return DN_ERR_CUDA;
+  donor_stale(c, -1);
   const std::string dev = device_name(c->device);
   static_assert(DN_NUM_TILE_SHAPES == dn::kNumShapes, "tile shape count");
   double cost[dn::kNumShapes] = {};

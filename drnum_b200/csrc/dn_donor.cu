@@ -17,73 +17,40 @@ namespace {
 
 constexpr int kDonorThreads = 256;
 
-// table entries in the plan's width (NARROW: the 32-bit copies)
-template <bool NARROW> __device__ __forceinline__ int64_t rv_cell_at(const DonorPlan& p, int r)
-{ return NARROW ? (int64_t)p.rv_cell32[r] : p.rv_cell[r]; }
-template <bool NARROW> __device__ __forceinline__ int64_t gp_wi_at(const DonorPlan& p, int g)
-{ return NARROW ? (int64_t)p.gp_wi32[g] : p.gp_wi[g]; }
-template <bool NARROW> __device__ __forceinline__ int64_t idx_at(const DonorPlan& p, int64_t e)
-{ return NARROW ? (int64_t)p.idx32[e] : p.idx[e]; }
+// Donor value of variable v at device cell c: FP64 fields as stored, FP32
+// bulk offsets dequantised in FP64 (base + quantum * offset).
+template <bool FX> struct DonorField;
+template <> struct DonorField<false> {
+  const double* f;
+  using raw = double;
+  __device__ __forceinline__ DonorField(const DonorPlan& p, int pd, int buf)
+      : f(static_cast<const double*>(p.bufs[pd * 3 + buf])) {}
+  __device__ __forceinline__ raw load(int64_t i) const { return f[i]; }
+  __device__ __forceinline__ double value(const DonorPlan&, int, int, raw x) const { return x; }
+};
+template <> struct DonorField<true> {
+  const int32_t* f;
+  using raw = int32_t;
+  __device__ __forceinline__ DonorField(const DonorPlan& p, int pd, int buf)
+      : f(static_cast<const int32_t*>(p.bufs[pd * 3 + buf])) {}
+  __device__ __forceinline__ raw load(int64_t i) const { return f[i]; }
+  __device__ __forceinline__ double value(const DonorPlan& p, int pd, int v, raw x) const
+  { return p.base[pd * 5 + v] + p.quantum[pd * 5 + v] * (double)x; }
+};
 
-template <bool NARROW>
-__global__ void __launch_bounds__(kDonorThreads)
-k_donor_copy_f64(const DonorPlan p, int buf)
+// Writes the accumulated sums to receiving cell `cell` of patch pr.
+template <bool FX>
+__device__ __forceinline__ void store_recv(const DonorPlan& p, int buf, int pr, int64_t cell, const double acc[5],
+                                           int* err)
 {
-  const int r = blockIdx.x * blockDim.x + threadIdx.x;
-  if (r >= p.n_recv) return;
-  const int pr = p.rv_patch[r];
-  const int64_t cell = rv_cell_at<NARROW>(p, r);
-  double acc[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
-  for (int g = p.rv_grp[r]; g < p.rv_grp[r + 1]; ++g) {
-    const int pd = p.gp_donor[g];
-    const double* src = static_cast<const double*>(p.bufs[pd * 3 + buf]);
-    const int64_t ncd = p.nc[pd];
-    const int64_t w0 = gp_wi_at<NARROW>(p, g);
-    double inter[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
-    for (int s = 0; s < p.gp_stride[g]; ++s) {
-      const int64_t c = idx_at<NARROW>(p, w0 + s);
-      const double w = p.w[w0 + s];
-      #pragma unroll
-      for (int v = 0; v < 5; ++v) inter[v] += src[v * ncd + c] * w;
-    }
-    #pragma unroll
-    for (int v = 0; v < 5; ++v) acc[v] += inter[v];
-  }
-  double* dst = static_cast<double*>(p.bufs[pr * 3 + buf]);
   const int64_t ncr = p.nc[pr];
-  #pragma unroll
-  for (int v = 0; v < 5; ++v) dst[v * ncr + cell] = acc[v];
-}
-
-template <bool NARROW>
-__global__ void __launch_bounds__(kDonorThreads)
-k_donor_copy_fx32(const DonorPlan p, int buf, int* err)
-{
-  const int r = blockIdx.x * blockDim.x + threadIdx.x;
-  if (r >= p.n_recv) return;
-  const int pr = p.rv_patch[r];
-  const int64_t cell = rv_cell_at<NARROW>(p, r);
-  double acc[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
-  for (int g = p.rv_grp[r]; g < p.rv_grp[r + 1]; ++g) {
-    const int pd = p.gp_donor[g];
-    const int32_t* src = static_cast<const int32_t*>(p.bufs[pd * 3 + buf]);
-    const int64_t ncd = p.nc[pd];
-    const int64_t w0 = gp_wi_at<NARROW>(p, g);
-    double inter[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
-    for (int s = 0; s < p.gp_stride[g]; ++s) {
-      const int64_t c = idx_at<NARROW>(p, w0 + s);
-      const double w = p.w[w0 + s];
-      #pragma unroll
-      for (int v = 0; v < 5; ++v) {
-        const double u = p.base[pd * 5 + v] + p.quantum[pd * 5 + v] * (double)src[v * ncd + c];
-        inter[v] += u * w;
-      }
-    }
+  if (!FX) {
+    double* dst = static_cast<double*>(p.bufs[pr * 3 + buf]);
     #pragma unroll
-    for (int v = 0; v < 5; ++v) acc[v] += inter[v];
+    for (int v = 0; v < 5; ++v) dst[v * ncr + cell] = acc[v];
+    return;
   }
   int32_t* dst = static_cast<int32_t*>(p.bufs[pr * 3 + buf]);
-  const int64_t ncr = p.nc[pr];
   int bad = 0;
   #pragma unroll
   for (int v = 0; v < 5; ++v) {
@@ -97,6 +64,87 @@ k_donor_copy_fx32(const DonorPlan p, int buf, int* err)
   if (bad && err) atomicOr(err, bad);
 }
 
+// Pattern form.  Contributions are taken BLK at a time: the donor loads of
+// a block are all issued before the first product (loads past the
+// pattern's end re-read its first donor cell and are not summed), so a
+// receiving cell waits for about two memory round trips per block instead
+// of two per contribution.  The products and sums keep the table order.
+template <bool FX, int BLK>
+__global__ void __launch_bounds__(kDonorThreads)
+k_donor_copy_pat(const DonorPlan p, int buf, int* err)
+{
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= p.n_recv) return;
+  const int pr = p.rv_patch[r];
+  const int64_t cell = (int64_t)p.rv_cell32[r];
+  const int g1 = p.rv_grp[r + 1];
+  double acc[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+  for (int g = p.rv_grp[r]; g < g1; ++g) {
+    const uint2 bp = p.gp_bp[g];
+    const int pat = (int)bp.y;
+    const int pd = p.pt_donor[pat];
+    const int s0 = p.pt_start[pat], n = p.pt_start[pat + 1] - s0;
+    const int64_t ncd = p.nc[pd];
+    const int64_t c0 = (int64_t)bp.x;
+    const DonorField<FX> src(p, pd, buf);
+    double inter[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+    for (int b = 0; b < n; b += BLK) {
+      int64_t cc[BLK];
+      double w[BLK];
+      #pragma unroll
+      for (int s = 0; s < BLK; ++s) {
+        const bool on = b + s < n;
+        cc[s] = c0 + (on ? p.pt_off[s0 + b + s] : 0);
+        w[s] = on ? p.pt_w[s0 + b + s] : 0.0;
+      }
+      typename DonorField<FX>::raw x[BLK][5];
+      #pragma unroll
+      for (int s = 0; s < BLK; ++s) {
+        #pragma unroll
+        for (int v = 0; v < 5; ++v) x[s][v] = src.load(v * ncd + cc[s]);
+      }
+      #pragma unroll
+      for (int s = 0; s < BLK; ++s) {
+        if (b + s < n) {
+          #pragma unroll
+          for (int v = 0; v < 5; ++v) inter[v] += src.value(p, pd, v, x[s][v]) * w[s];
+        }
+      }
+    }
+    #pragma unroll
+    for (int v = 0; v < 5; ++v) acc[v] += inter[v];
+  }
+  store_recv<FX>(p, buf, pr, cell, acc, err);
+}
+
+// Wide form: 64-bit donor cells and contribution offsets.
+template <bool FX>
+__global__ void __launch_bounds__(kDonorThreads)
+k_donor_copy_wide(const DonorPlan p, int buf, int* err)
+{
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= p.n_recv) return;
+  const int pr = p.rv_patch[r];
+  const int64_t cell = p.rv_cell[r];
+  double acc[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+  for (int g = p.rv_grp[r]; g < p.rv_grp[r + 1]; ++g) {
+    const int pd = p.gp_donor[g];
+    const DonorField<FX> src(p, pd, buf);
+    const int64_t ncd = p.nc[pd];
+    const int64_t w0 = p.gp_wi[g];
+    double inter[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+    for (int s = 0; s < p.gp_stride[g]; ++s) {
+      const int64_t c = p.idx[w0 + s];
+      const double w = p.w[w0 + s];
+      #pragma unroll
+      for (int v = 0; v < 5; ++v) inter[v] += src.value(p, pd, v, src.load(v * ncd + c)) * w;
+    }
+    #pragma unroll
+    for (int v = 0; v < 5; ++v) acc[v] += inter[v];
+  }
+  store_recv<FX>(p, buf, pr, cell, acc, err);
+}
+
 int blocks_for(int n) { return (n + kDonorThreads - 1) / kDonorThreads; }
 
 } // namespace
@@ -104,16 +152,16 @@ int blocks_for(int n) { return (n + kDonorThreads - 1) / kDonorThreads; }
 cudaError_t launch_donor_copy_f64(const DonorPlan& p, int buf, cudaStream_t st)
 {
   if (p.n_recv <= 0) return cudaSuccess;
-  if (p.narrow) k_donor_copy_f64<true><<<blocks_for(p.n_recv), kDonorThreads, 0, st>>>(p, buf);
-  else k_donor_copy_f64<false><<<blocks_for(p.n_recv), kDonorThreads, 0, st>>>(p, buf);
+  if (p.patterned) k_donor_copy_pat<false, 4><<<blocks_for(p.n_recv), kDonorThreads, 0, st>>>(p, buf, nullptr);
+  else k_donor_copy_wide<false><<<blocks_for(p.n_recv), kDonorThreads, 0, st>>>(p, buf, nullptr);
   return cudaGetLastError();
 }
 
 cudaError_t launch_donor_copy_fx32(const DonorPlan& p, int buf, int* err, cudaStream_t st)
 {
   if (p.n_recv <= 0) return cudaSuccess;
-  if (p.narrow) k_donor_copy_fx32<true><<<blocks_for(p.n_recv), kDonorThreads, 0, st>>>(p, buf, err);
-  else k_donor_copy_fx32<false><<<blocks_for(p.n_recv), kDonorThreads, 0, st>>>(p, buf, err);
+  if (p.patterned) k_donor_copy_pat<true, 8><<<blocks_for(p.n_recv), kDonorThreads, 0, st>>>(p, buf, err);
+  else k_donor_copy_wide<true><<<blocks_for(p.n_recv), kDonorThreads, 0, st>>>(p, buf, err);
   return cudaGetLastError();
 }
 

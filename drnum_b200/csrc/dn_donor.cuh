@@ -9,21 +9,33 @@ namespace dn {
 
 // All receiving cells of all patches, each with its contributions grouped
 // by donor patch in table order (device pointers).
+//
+// Two forms.  The pattern form (patterned != 0; every device cell offset
+// below 2^32) stores a group as its first donor cell and the id of an
+// interpolation pattern: the donor patch, the other contributions' offsets
+// from the first donor cell and the weights.  Overlapping Cartesian patches
+// repeat a few thousand stencils over millions of receiving cells, so the
+// tables shrink from 12 B per contribution to 8 B per group, and the
+// pattern table stays in cache.  The wide form keeps every contribution's
+// 64-bit donor cell and weight.
 struct DonorPlan {
   int32_t n_recv;             // unique receiving cells over all patches
   const int32_t* rv_patch;    // receiving patch per receiving cell
-  const int64_t* rv_cell;     // cell index (device offset) in the receiving patch
   const int32_t* rv_grp;      // [n_recv + 1] CSR offsets into the groups
+  int patterned;
+  // pattern form
+  const uint32_t* rv_cell32;  // cell index (device offset) in the receiving patch
+  const uint2* gp_bp;         // per group: (first donor cell, pattern id)
+  const int32_t* pt_donor;    // donor patch per pattern
+  const int32_t* pt_start;    // [n_patterns + 1] CSR offsets into pt_off / pt_w
+  const int32_t* pt_off;      // donor cell of each contribution less the group's first
+  const double* pt_w;         // weight per contribution
+  // wide form
+  const int64_t* rv_cell;
   const int32_t* gp_donor;    // donor patch per group
   const int32_t* gp_stride;   // contributions per group
   const int64_t* gp_wi;       // first contribution of the group in idx/w
   const int64_t* idx;         // donor cell (device offset) per contribution
-  // the same three tables in 32 bits when every value fits (narrow != 0):
-  // a quarter less table traffic per contribution
-  int narrow;
-  const uint32_t* rv_cell32;
-  const uint32_t* gp_wi32;
-  const uint32_t* idx32;
   const double* w;            // weight per contribution
   void* const* bufs;          // [num_patches * 3] physical field buffers
   const int64_t* nc;          // [num_patches] cells per patch

@@ -227,3 +227,53 @@ def test_levelset_stagewise_post_operation_equals_fused_step(golden_dir):
     it.close()
     for p, cp in enumerate(objs):
         assert np.array_equal(cp.getField(0), z[f"p{p}_out"]), p
+
+
+@pytest.mark.parametrize("precision", [DN_FP64, DN_FP32])
+@pytest.mark.parametrize("graph", [0, 1])
+def test_step_start_donor_copy_left_out_only_while_current(precision, graph):
+    """A step starts with a donor copy (rungekutta.cpp:30) unless the step-
+    start buffer's receiving cells already hold it: the last step ended with
+    a donor copy into that buffer and nothing has written it since.  An
+    upload into field 0, or an upload into field 1 copied into field 0,
+    makes the next step copy again, bit for bit like a fresh context."""
+    name = "octants_8"
+    patches = cases_def.grid_case(name)[0]
+    garbage = [cases.random_state(*p["n"], seed=100 + q, amp=0.03) for q, p in enumerate(patches)]
+    alpha = np.ascontiguousarray(cases.RK3_ALPHA, dtype=np.float64)
+
+    def upload(it, field, states):
+        for q, U in enumerate(states):
+            a = np.ascontiguousarray(U, dtype=np.float64)
+            _lib.check(it.ctx, it.lib.dn_patch_upload(it.ctx, q, field, _lib.dptr(a)))
+
+    def fresh_step(states):
+        # (the first upload fixes the FP32-bulk base and quantum of every patch)
+        it, objs, _, dt, _ = make_grid(name, precision)
+        it.setOption(_lib.DN_OPT_GRAPH, graph)
+        upload(it, 0, states)
+        it.rkStep(dt, alpha)
+        out = [it.downloadField(q, 0) for q in range(len(objs))]
+        it.close()
+        return out
+
+    expect = fresh_step(garbage)
+    for route in ("upload", "copy"):
+        it, objs, _, dt, _ = make_grid(name, precision)
+        it.setOption(_lib.DN_OPT_GRAPH, graph)
+        n = [it.launchCount()]
+        for _ in range(3):
+            it.rkStep(dt, alpha)
+            n.append(it.launchCount())
+        per_step = np.diff(n)
+        assert per_step[1] == per_step[0] - 1 and per_step[2] == per_step[1], per_step
+        if route == "upload":
+            upload(it, 0, garbage)
+        else:
+            upload(it, 1, garbage)
+            it.copyField(1, 0)
+        it.rkStep(dt, alpha)
+        got = [it.downloadField(q, 0) for q in range(len(objs))]
+        it.close()
+        for q, (a, b) in enumerate(zip(got, expect)):
+            assert np.array_equal(a, b), (route, q)
