@@ -31,6 +31,7 @@ DN_OPT_BATCHED = 0
 DN_OPT_GRAPH = 1
 DN_OPT_BATCH_WAVES = 2
 DN_OPT_BATCH_MIN_PLANES = 3
+DN_OPT_DONOR_TABLES = 4
 DN_NUM_TILE_SHAPES = 3
 
 DN_BC_ZERO_FLUX = 0

@@ -129,6 +129,7 @@ struct dn_ctx {
   int donor_fresh = -1;
   int64_t donor_fresh_gen = -1;
   bool plan_chained = false;
+  bool donor_wide = false;                    // DN_OPT_DONOR_TABLES = 1
   // level-set layers per patch and their device form
   std::vector<dn::LevelSetLayers> ls;
   std::vector<char> ls_on;
@@ -690,50 +691,55 @@ int build_plan(dn_ctx* c)
     }
     c->plan_chained = chained;
   }
-  // pattern form: every group as (first donor cell, pattern id), the
-  // patterns (donor patch, offsets from the first donor cell, weights)
-  // listed once.  FP32-bulk plans leave zero weights out: a donor value is
+  // pattern form: every group as (first donor cell, first pattern entry,
+  // entries, donor patch); the pattern entries (offsets from the first
+  // donor cell, weights) listed once for all groups that share them.  A
+  // cell's first group sits at the cell's index, further groups after all
+  // first ones.  FP32-bulk plans leave zero weights out: a donor value is
   // always finite there, and adding +-0 to a sum that starts at +0 never
   // changes it.
   auto fits32 = [](const std::vector<int64_t>& v) {
     for (int64_t x : v) if (x < 0 || x > (int64_t)UINT32_MAX) return false;
     return true;
   };
-  bool patterned = fits32(rv_cell) && fits32(idx);
-  std::vector<uint2> gp_bp;
-  std::vector<int32_t> pt_donor, pt_start(1, 0), pt_off;
+  const size_t n_recv = rv_patch.size();
+  bool patterned = !c->donor_wide && fits32(rv_cell) && fits32(idx);
+  std::vector<uint4> gp_pat;
+  std::vector<int32_t> rv_more, pt_off;
   std::vector<double> pt_w;
   if (patterned) {
     const bool drop_zero = c->precision != DN_FP64;
-    std::unordered_map<std::string, int32_t> ids;
+    std::unordered_map<std::string, int32_t> starts;
     std::string key, last_key;
-    int32_t last_id = -1;
-    gp_bp.resize(gp_donor.size());
-    for (size_t g = 0; g < gp_donor.size() && patterned; ++g) {
+    int32_t last_start = 0;
+    bool any_more = false;
+    for (size_t r = 0; r < n_recv; ++r) any_more = any_more || rv_grp[r + 1] - rv_grp[r] > 1;
+    gp_pat.resize(n_recv, make_uint4(0u, 0u, 0u, 0u));
+    if (any_more) rv_more.assign(n_recv + 1, 0);
+    auto pattern_of = [&](size_t g, uint4* out) {
       const int64_t w0 = gp_wi[g], n = gp_stride[g];
       const int64_t c0 = n > 0 ? idx[(size_t)w0] : 0;
-      key.assign(reinterpret_cast<const char*>(&gp_donor[g]), sizeof(int32_t));
+      key.clear();
       for (int64_t q = 0; q < n; ++q) {
         const double ws = w[(size_t)(w0 + q)];
         if (drop_zero && ws == 0.0) continue;
         const int64_t d = idx[(size_t)(w0 + q)] - c0;
-        if (d < INT32_MIN || d > INT32_MAX) { patterned = false; break; }
+        if (d < INT32_MIN || d > INT32_MAX) return false;
         const int32_t d32 = (int32_t)d;
         key.append(reinterpret_cast<const char*>(&d32), sizeof(d32));
         key.append(reinterpret_cast<const char*>(&ws), sizeof(ws));
       }
-      if (!patterned) break;
-      int32_t id = last_id;
+      const size_t entries = key.size() / (sizeof(int32_t) + sizeof(double));
+      int32_t start = last_start;
       if (key != last_key) {
-        auto it = ids.find(key);
-        if (it != ids.end()) {
-          id = it->second;
+        auto it = starts.find(key);
+        if (it != starts.end()) {
+          start = it->second;
         } else {
-          if (pt_donor.size() >= (size_t)INT32_MAX - 1) { patterned = false; break; }
-          id = (int32_t)pt_donor.size();
-          ids.emplace(key, id);
-          pt_donor.push_back(gp_donor[g]);
-          for (size_t o = sizeof(int32_t); o < key.size(); o += sizeof(int32_t) + sizeof(double)) {
+          if (pt_off.size() + entries >= (size_t)INT32_MAX) return false;
+          start = (int32_t)pt_off.size();
+          starts.emplace(key, start);
+          for (size_t o = 0; o < key.size(); o += sizeof(int32_t) + sizeof(double)) {
             int32_t d32;
             double ws;
             std::memcpy(&d32, key.data() + o, sizeof(d32));
@@ -741,36 +747,47 @@ int build_plan(dn_ctx* c)
             pt_off.push_back(d32);
             pt_w.push_back(ws);
           }
-          if (pt_off.size() >= (size_t)INT32_MAX) { patterned = false; break; }
-          pt_start.push_back((int32_t)pt_off.size());
         }
         last_key = key;
-        last_id = id;
+        last_start = start;
       }
-      gp_bp[g] = make_uint2((unsigned)c0, (unsigned)id);
+      *out = make_uint4((unsigned)c0, (unsigned)start, (unsigned)entries, (unsigned)gp_donor[g]);
+      return true;
+    };
+    for (size_t r = 0; r < n_recv && patterned; ++r) {
+      const size_t g0 = (size_t)rv_grp[r], g1 = (size_t)rv_grp[r + 1];
+      if (g1 == g0) gp_pat[r] = make_uint4(0u, 0u, 0u, (unsigned)rv_patch[r]);   // no donor: sums to zero
+      else patterned = pattern_of(g0, &gp_pat[r]);
+      if (any_more) rv_more[r] = (int32_t)gp_pat.size();
+      for (size_t g = g0 + 1; g < g1 && patterned; ++g) {
+        uint4 e;
+        patterned = pattern_of(g, &e);
+        gp_pat.push_back(e);
+      }
     }
+    if (any_more) rv_more[n_recv] = (int32_t)gp_pat.size();
   }
   int s;
   dn::DonorPlan& P = c->plan;
   P.n_recv = (int32_t)rv_patch.size();
   P.patterned = patterned ? 1 : 0;
-  if ((s = plan_upload(c, rv_patch, &P.rv_patch)) || (s = plan_upload(c, rv_grp, &P.rv_grp)) ||
-      (s = plan_upload(c, nc, &P.nc)) || (s = plan_upload(c, base, &P.base)) ||
-      (s = plan_upload(c, quantum, &P.quantum))) {
+  if ((s = plan_upload(c, rv_patch, &P.rv_patch)) || (s = plan_upload(c, nc, &P.nc)) ||
+      (s = plan_upload(c, base, &P.base)) || (s = plan_upload(c, quantum, &P.quantum))) {
     free_plan(c);
     return s;
   }
   if (patterned) {
     const std::vector<uint32_t> rc(rv_cell.begin(), rv_cell.end());
-    if ((s = plan_upload(c, rc, &P.rv_cell32)) || (s = plan_upload(c, gp_bp, &P.gp_bp)) ||
-        (s = plan_upload(c, pt_donor, &P.pt_donor)) || (s = plan_upload(c, pt_start, &P.pt_start)) ||
-        (s = plan_upload(c, pt_off, &P.pt_off)) || (s = plan_upload(c, pt_w, &P.pt_w))) {
+    if ((s = plan_upload(c, rc, &P.rv_cell32)) || (s = plan_upload(c, gp_pat, &P.gp_pat)) ||
+        (s = plan_upload(c, rv_more, &P.rv_more)) || (s = plan_upload(c, pt_off, &P.pt_off)) ||
+        (s = plan_upload(c, pt_w, &P.pt_w))) {
       free_plan(c);
       return s;
     }
-  } else if ((s = plan_upload(c, rv_cell, &P.rv_cell)) || (s = plan_upload(c, gp_donor, &P.gp_donor)) ||
-             (s = plan_upload(c, gp_stride, &P.gp_stride)) || (s = plan_upload(c, gp_wi, &P.gp_wi)) ||
-             (s = plan_upload(c, idx, &P.idx)) || (s = plan_upload(c, w, &P.w))) {
+  } else if ((s = plan_upload(c, rv_grp, &P.rv_grp)) || (s = plan_upload(c, rv_cell, &P.rv_cell)) ||
+             (s = plan_upload(c, gp_donor, &P.gp_donor)) || (s = plan_upload(c, gp_stride, &P.gp_stride)) ||
+             (s = plan_upload(c, gp_wi, &P.gp_wi)) || (s = plan_upload(c, idx, &P.idx)) ||
+             (s = plan_upload(c, w, &P.w))) {
     free_plan(c);
     return s;
   }
@@ -2483,6 +2500,13 @@ int dn_set_option(dn_ctx* c, int option, int value)
       return fail(c, DN_ERR_ARG, "schedule option %d out of range: %d", option, value);
     (option == DN_OPT_BATCH_WAVES ? c->batch_waves : c->batch_min_planes) = value;
     c->batch_dirty = true;
+    c->generation++;
+    return DN_OK;
+  }
+  if (option == DN_OPT_DONOR_TABLES) {
+    if (value < 0 || value > 1) return fail(c, DN_ERR_ARG, "donor table option out of range: %d", value);
+    c->donor_wide = value == 1;
+    c->plan_dirty = true;
     c->generation++;
     return DN_OK;
   }

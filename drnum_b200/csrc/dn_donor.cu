@@ -64,55 +64,71 @@ __device__ __forceinline__ void store_recv(const DonorPlan& p, int buf, int pr, 
   if (bad && err) atomicOr(err, bad);
 }
 
-// Pattern form.  Contributions are taken BLK at a time: the donor loads of
-// a block are all issued before the first product (loads past the
-// pattern's end re-read its first donor cell and are not summed), so a
-// receiving cell waits for about two memory round trips per block instead
-// of two per contribution.  The products and sums keep the table order.
+// Adds the weighted donor sum of one pattern-form group to acc.
+// Contributions are taken BLK at a time: the donor loads of a block are all
+// issued before the first product, so a group waits for one memory round
+// trip per block instead of one per contribution.  Products and sums keep
+// the table order.
 template <bool FX, int BLK>
-__global__ void __launch_bounds__(kDonorThreads)
+__device__ __forceinline__ void add_group(const DonorPlan& p, int buf, uint4 gr, double acc[5])
+{
+  const int pd = (int)gr.w;
+  const int s0 = (int)gr.y, n = (int)gr.z;
+  const int64_t ncd = p.nc[pd];
+  const int64_t c0 = (int64_t)gr.x;
+  const DonorField<FX> src(p, pd, buf);
+  double inter[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+  for (int b = 0; b < n; b += BLK) {
+    int64_t cc[BLK];
+    double w[BLK];
+    typename DonorField<FX>::raw x[BLK][5];
+    #pragma unroll
+    for (int s = 0; s < BLK; ++s) {
+      if (b + s < n) {
+        cc[s] = c0 + p.pt_off[s0 + b + s];
+        w[s] = p.pt_w[s0 + b + s];
+      }
+    }
+    #pragma unroll
+    for (int s = 0; s < BLK; ++s) {
+      if (b + s < n) {
+        #pragma unroll
+        for (int v = 0; v < 5; ++v) x[s][v] = src.load(v * ncd + cc[s]);
+      }
+    }
+    #pragma unroll
+    for (int s = 0; s < BLK; ++s) {
+      if (b + s < n) {
+        #pragma unroll
+        for (int v = 0; v < 5; ++v) inter[v] += src.value(p, pd, v, x[s][v]) * w[s];
+      }
+    }
+  }
+  #pragma unroll
+  for (int v = 0; v < 5; ++v) acc[v] += inter[v];
+}
+
+// Pattern form: one thread per receiving cell, its first group next to its
+// own table entries, any further groups after it.
+template <bool FX, int BLK>
+__global__ void __launch_bounds__(kDonorThreads, FX ? 3 : 2)
 k_donor_copy_pat(const DonorPlan p, int buf, int* err)
 {
   const int r = blockIdx.x * blockDim.x + threadIdx.x;
   if (r >= p.n_recv) return;
   const int pr = p.rv_patch[r];
   const int64_t cell = (int64_t)p.rv_cell32[r];
-  const int g1 = p.rv_grp[r + 1];
+  int g = 0, g1 = 0;
+  if (p.rv_more) {
+    g = p.rv_more[r];
+    g1 = p.rv_more[r + 1];
+  }
   double acc[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
-  for (int g = p.rv_grp[r]; g < g1; ++g) {
-    const uint2 bp = p.gp_bp[g];
-    const int pat = (int)bp.y;
-    const int pd = p.pt_donor[pat];
-    const int s0 = p.pt_start[pat], n = p.pt_start[pat + 1] - s0;
-    const int64_t ncd = p.nc[pd];
-    const int64_t c0 = (int64_t)bp.x;
-    const DonorField<FX> src(p, pd, buf);
-    double inter[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
-    for (int b = 0; b < n; b += BLK) {
-      int64_t cc[BLK];
-      double w[BLK];
-      #pragma unroll
-      for (int s = 0; s < BLK; ++s) {
-        const bool on = b + s < n;
-        cc[s] = c0 + (on ? p.pt_off[s0 + b + s] : 0);
-        w[s] = on ? p.pt_w[s0 + b + s] : 0.0;
-      }
-      typename DonorField<FX>::raw x[BLK][5];
-      #pragma unroll
-      for (int s = 0; s < BLK; ++s) {
-        #pragma unroll
-        for (int v = 0; v < 5; ++v) x[s][v] = src.load(v * ncd + cc[s]);
-      }
-      #pragma unroll
-      for (int s = 0; s < BLK; ++s) {
-        if (b + s < n) {
-          #pragma unroll
-          for (int v = 0; v < 5; ++v) inter[v] += src.value(p, pd, v, x[s][v]) * w[s];
-        }
-      }
-    }
-    #pragma unroll
-    for (int v = 0; v < 5; ++v) acc[v] += inter[v];
+  uint4 gr = p.gp_pat[r];
+  for (;;) {
+    add_group<FX, BLK>(p, buf, gr, acc);
+    if (g >= g1) break;
+    gr = p.gp_pat[g++];
   }
   store_recv<FX>(p, buf, pr, cell, acc, err);
 }
@@ -160,7 +176,7 @@ cudaError_t launch_donor_copy_f64(const DonorPlan& p, int buf, cudaStream_t st)
 cudaError_t launch_donor_copy_fx32(const DonorPlan& p, int buf, int* err, cudaStream_t st)
 {
   if (p.n_recv <= 0) return cudaSuccess;
-  if (p.patterned) k_donor_copy_pat<true, 8><<<blocks_for(p.n_recv), kDonorThreads, 0, st>>>(p, buf, err);
+  if (p.patterned) k_donor_copy_pat<true, 4><<<blocks_for(p.n_recv), kDonorThreads, 0, st>>>(p, buf, err);
   else k_donor_copy_wide<true><<<blocks_for(p.n_recv), kDonorThreads, 0, st>>>(p, buf, err);
   return cudaGetLastError();
 }

@@ -11,26 +11,28 @@ namespace dn {
 // by donor patch in table order (device pointers).
 //
 // Two forms.  The pattern form (patterned != 0; every device cell offset
-// below 2^32) stores a group as its first donor cell and the id of an
-// interpolation pattern: the donor patch, the other contributions' offsets
-// from the first donor cell and the weights.  Overlapping Cartesian patches
-// repeat a few thousand stencils over millions of receiving cells, so the
-// tables shrink from 12 B per contribution to 8 B per group, and the
-// pattern table stays in cache.  The wide form keeps every contribution's
-// 64-bit donor cell and weight.
+// below 2^32) stores a group as its donor patch, its first donor cell and
+// the position of its contributions in a table of interpolation patterns
+// (the other contributions' offsets from the first donor cell, and the
+// weights).  Overlapping Cartesian patches repeat a few thousand stencils
+// over millions of receiving cells, so the pattern table stays in cache
+// and a receiving cell streams 24 B of tables.  A cell's first group is
+// group r of the cell's own index; the groups after it, where a cell has
+// donors in several patches, follow in table order at rv_more[r] ..
+// rv_more[r+1]-1 (rv_more NULL: no cell has more than one).  The wide form
+// keeps every contribution's 64-bit donor cell and weight.
 struct DonorPlan {
   int32_t n_recv;             // unique receiving cells over all patches
   const int32_t* rv_patch;    // receiving patch per receiving cell
-  const int32_t* rv_grp;      // [n_recv + 1] CSR offsets into the groups
   int patterned;
   // pattern form
   const uint32_t* rv_cell32;  // cell index (device offset) in the receiving patch
-  const uint2* gp_bp;         // per group: (first donor cell, pattern id)
-  const int32_t* pt_donor;    // donor patch per pattern
-  const int32_t* pt_start;    // [n_patterns + 1] CSR offsets into pt_off / pt_w
-  const int32_t* pt_off;      // donor cell of each contribution less the group's first
-  const double* pt_w;         // weight per contribution
+  const uint4* gp_pat;        // per group: (first donor cell, first pattern entry, entries, donor patch)
+  const int32_t* rv_more;     // [n_recv + 1] the groups after the first, or NULL
+  const int32_t* pt_off;      // pattern entries: donor cell less the group's first
+  const double* pt_w;         // pattern entries: weight
   // wide form
+  const int32_t* rv_grp;      // [n_recv + 1] CSR offsets into the groups
   const int64_t* rv_cell;
   const int32_t* gp_donor;    // donor patch per group
   const int32_t* gp_stride;   // contributions per group

@@ -359,13 +359,19 @@ int dn_lslayers_destroy(dn_lslayers* ls);
  *     0 launches one CTA per work item.  dn_autotune measures the choices.
  *   DN_OPT_BATCH_MIN_PLANES (default 8): shortest plane range of a work item
  *     when one CTA takes one item.
- *   The schedule options change no result.
+ *   DN_OPT_DONOR_TABLES (default 0): device form of the donor tables.  0 =
+ *     interpolation patterns (each group as donor patch, first donor cell and
+ *     a shared entry of offsets and weights) wherever every device cell
+ *     offset fits 32 bits, else per-contribution 64-bit tables; 1 = always
+ *     the per-contribution tables.
+ *   The schedule and table options change no result.
  * No reference counterpart (the reference launches 10 kernels per patch and
  * stage, each followed by a device synchronisation, gpu_cartesianiterator.h:218-304). */
 #define DN_OPT_BATCHED    0
 #define DN_OPT_GRAPH      1
 #define DN_OPT_BATCH_WAVES      2
 #define DN_OPT_BATCH_MIN_PLANES 3
+#define DN_OPT_DONOR_TABLES     4
 int dn_set_option(dn_ctx* ctx, int option, int value);
 
 /* Tile shape of a patch in the batched launch (j x k): 0 = 8 x 32 (FP64

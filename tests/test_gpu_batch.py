@@ -134,3 +134,34 @@ def test_schedule_options_are_checked():
     assert lib.dn_set_option(it.ctx, _lib.DN_OPT_BATCH_MIN_PLANES, 0) == _lib.DN_ERR_ARG
     assert lib.dn_set_option(it.ctx, _lib.DN_OPT_BATCH_WAVES, 3) == _lib.DN_OK
     it.close()
+
+
+@pytest.mark.parametrize("precision", [DN_FP64, DN_FP32])
+@pytest.mark.parametrize("name", ["jet", "tiled"])
+def test_donor_table_forms_give_the_same_result(name, precision):
+    # interpolation patterns (the default) and per-contribution tables on
+    # the dual-resolution jet (cells with donors in two or three patches)
+    # and the uneven grid (zero weights), reduced: the same bits
+    from drnum_b200 import workloads
+    case = workloads.build(name, 0.25)
+
+    def run(form):
+        _, objs = workloads.make_grid(case)
+        it = workloads.make_iterator(objs, precision, 0)
+        it.setOption(_lib.DN_OPT_DONOR_TABLES, form)
+        for _ in range(2):
+            it.rkStep(case["dt"], cases.RK3_ALPHA)
+        out = [it.downloadField(q, 0) for q in range(len(objs))]
+        it.close()
+        return out
+
+    a, b = run(0), run(1)
+    for q, (x, y) in enumerate(zip(a, b)):
+        assert np.array_equal(x, y), q
+
+
+def test_donor_table_option_is_checked():
+    it, _, _, _, _ = make_grid("octants_8", DN_FP32)
+    assert it.lib.dn_set_option(it.ctx, _lib.DN_OPT_DONOR_TABLES, 2) == _lib.DN_ERR_ARG
+    assert it.lib.dn_set_option(it.ctx, _lib.DN_OPT_DONOR_TABLES, 1) == _lib.DN_OK
+    it.close()
