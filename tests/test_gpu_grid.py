@@ -277,3 +277,39 @@ def test_step_start_donor_copy_left_out_only_while_current(precision, graph):
         it.close()
         for q, (a, b) in enumerate(zip(got, expect)):
             assert np.array_equal(a, b), (route, q)
+
+
+def test_step_start_donor_copy_kept_when_donors_include_receiving_cells(golden_dir):
+    # tables in which a donor cell of patch 1 is a receiving cell of patch 0:
+    # a repeated donor copy would read what the last one wrote, so every
+    # step keeps its step-start copy (with the reference's tables it is left
+    # out from the second step on)
+    z = _fixture(golden_dir, "pair_x")
+    patches = cases_def.grid_layout("pair_x")
+    alpha = np.ascontiguousarray(cases.RK3_ALPHA, dtype=np.float64)
+
+    def launches_per_step(chain):
+        it = B200CartesianIterator(AusmPlus(), 0, DN_FP64)
+        for p in patches:
+            cp = CartesianPatch(*p["n"], lengths=p["length"], origin=p["origin"],
+                                periodic=(False, False, False), seek=p["seek"])
+            cp.setField(0, cases.uniform_state([p], mach=0.3)[0])
+            it.addPatch(cp)
+        for q in range(2):
+            t = {k: z[f"p{q}_{k}"].copy() for k in TABLE_KEYS + ("counts",)}
+            if chain and q == 1:
+                assert int(t["donor_patch"][0]) == 0
+                t["donor_idx"][0] = z["p0_rec_unique"][0]
+            it.setDonorTablesOf(q, t)
+        it.updateDevice(fields=(0,))
+        n = [it.launchCount()]
+        for _ in range(3):
+            it.rkStep(1e-6, alpha)
+            n.append(it.launchCount())
+        it.close()
+        return np.diff(n)
+
+    plain = launches_per_step(False)
+    assert plain[1] == plain[0] - 1 and plain[2] == plain[1], plain
+    chained = launches_per_step(True)
+    assert chained[0] == chained[1] == chained[2] == plain[0], chained
