@@ -108,29 +108,55 @@ __device__ __forceinline__ void add_group(const DonorPlan& p, int buf, uint4 gr,
   for (int v = 0; v < 5; ++v) acc[v] += inter[v];
 }
 
-// Pattern form: one thread per receiving cell, its first group next to its
-// own table entries, any further groups after it.
+// Pattern form: a thread takes receiving cells r, r + stride, ... (stride
+// = all threads of the launch) and loads the next cell's table entries
+// before it gathers the current cell's donors, so the table loads of one
+// cell overlap the donor loads of the one before.
 template <bool FX, int BLK>
-__global__ void __launch_bounds__(kDonorThreads, FX ? 3 : 2)
+__global__ void __launch_bounds__(kDonorThreads, 2)
 k_donor_copy_pat(const DonorPlan p, int buf, int* err)
 {
-  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  const int stride = gridDim.x * blockDim.x;
+  int r = blockIdx.x * blockDim.x + threadIdx.x;
   if (r >= p.n_recv) return;
-  const int pr = p.rv_patch[r];
-  const int64_t cell = (int64_t)p.rv_cell32[r];
+  int pr = p.rv_patch[r];
+  uint32_t cell = p.rv_cell32[r];
+  uint4 gr = p.gp_pat[r];
   int g = 0, g1 = 0;
   if (p.rv_more) {
     g = p.rv_more[r];
     g1 = p.rv_more[r + 1];
   }
-  double acc[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
-  uint4 gr = p.gp_pat[r];
   for (;;) {
-    add_group<FX, BLK>(p, buf, gr, acc);
-    if (g >= g1) break;
-    gr = p.gp_pat[g++];
+    const int rn = r + stride;
+    const bool more = rn < p.n_recv;
+    int pr_n = 0, gn = 0, g1n = 0;
+    uint32_t cell_n = 0;
+    uint4 gr_n = make_uint4(0u, 0u, 0u, 0u);
+    if (more) {
+      pr_n = p.rv_patch[rn];
+      cell_n = p.rv_cell32[rn];
+      gr_n = p.gp_pat[rn];
+      if (p.rv_more) {
+        gn = p.rv_more[rn];
+        g1n = p.rv_more[rn + 1];
+      }
+    }
+    double acc[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+    for (;;) {
+      add_group<FX, BLK>(p, buf, gr, acc);
+      if (g >= g1) break;
+      gr = p.gp_pat[g++];
+    }
+    store_recv<FX>(p, buf, pr, (int64_t)cell, acc, err);
+    if (!more) break;
+    r = rn;
+    pr = pr_n;
+    cell = cell_n;
+    gr = gr_n;
+    g = gn;
+    g1 = g1n;
   }
-  store_recv<FX>(p, buf, pr, cell, acc, err);
 }
 
 // Wide form: 64-bit donor cells and contribution offsets.
@@ -163,12 +189,32 @@ k_donor_copy_wide(const DonorPlan p, int buf, int* err)
 
 int blocks_for(int n) { return (n + kDonorThreads - 1) / kDonorThreads; }
 
+// Grid of the pattern form: the CTAs that are resident at once (each
+// thread then walks several receiving cells), at most one per 256 cells.
+template <bool FX, int BLK>
+int pattern_blocks(int n)
+{
+  static int per_device[64] = {};
+  int dev = 0;
+  cudaGetDevice(&dev);
+  int& cap = per_device[dev & 63];
+  if (cap == 0) {
+    int sms = 0, per_sm = 0;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_donor_copy_pat<FX, BLK>, kDonorThreads, 0);
+    cap = sms * (per_sm > 0 ? per_sm : 1);
+    if (cap <= 0) cap = 1;
+  }
+  const int b = blocks_for(n);
+  return b < cap ? b : cap;
+}
+
 } // namespace
 
 cudaError_t launch_donor_copy_f64(const DonorPlan& p, int buf, cudaStream_t st)
 {
   if (p.n_recv <= 0) return cudaSuccess;
-  if (p.patterned) k_donor_copy_pat<false, 4><<<blocks_for(p.n_recv), kDonorThreads, 0, st>>>(p, buf, nullptr);
+  if (p.patterned) k_donor_copy_pat<false, 4><<<pattern_blocks<false, 4>(p.n_recv), kDonorThreads, 0, st>>>(p, buf, nullptr);
   else k_donor_copy_wide<false><<<blocks_for(p.n_recv), kDonorThreads, 0, st>>>(p, buf, nullptr);
   return cudaGetLastError();
 }
@@ -176,7 +222,7 @@ cudaError_t launch_donor_copy_f64(const DonorPlan& p, int buf, cudaStream_t st)
 cudaError_t launch_donor_copy_fx32(const DonorPlan& p, int buf, int* err, cudaStream_t st)
 {
   if (p.n_recv <= 0) return cudaSuccess;
-  if (p.patterned) k_donor_copy_pat<true, 4><<<blocks_for(p.n_recv), kDonorThreads, 0, st>>>(p, buf, err);
+  if (p.patterned) k_donor_copy_pat<true, 4><<<pattern_blocks<true, 4>(p.n_recv), kDonorThreads, 0, st>>>(p, buf, err);
   else k_donor_copy_wide<true><<<blocks_for(p.n_recv), kDonorThreads, 0, st>>>(p, buf, err);
   return cudaGetLastError();
 }
