@@ -129,6 +129,9 @@ struct dn_ctx {
   int donor_fresh = -1;
   int64_t donor_fresh_gen = -1;
   bool plan_chained = false;
+  // the level-set wall writes a donor or a receiving cell of the plan (its
+  // post-operation then makes the buffer's donor copy stale)
+  bool ls_touches_donors = true;
   bool donor_wide = false;                    // DN_OPT_DONOR_TABLES = 1
   // level-set layers per patch and their device form
   std::vector<dn::LevelSetLayers> ls;
@@ -591,6 +594,8 @@ bool has_donors(const dn_ctx* c)
 
 // Regroups the per-patch tables by receiving cell (groups in donor order)
 // and uploads them with the per-patch buffer table.
+bool levelset_touches_donors(const dn_ctx* c);
+
 int build_plan(dn_ctx* c)
 {
   free_plan(c);
@@ -691,6 +696,7 @@ int build_plan(dn_ctx* c)
     }
     c->plan_chained = chained;
   }
+  c->ls_touches_donors = levelset_touches_donors(c);
   // pattern form: every group as (first donor cell, first pattern entry,
   // entries, donor patch); the pattern entries (offsets from the first
   // donor cell, weights) listed once for all groups that share them.  A
@@ -823,9 +829,48 @@ int ls_upload(dn_ctx* c, const std::vector<T>& h, const T** out)
 // Flattens the inner layer cells of all patches with a level set (patch,
 // layer, cell order, as LevelSetObjectBC::transferCellLayerData,
 // levelsetobjectbc.cpp:38-134) and uploads them.
+// Whether a cell the level-set wall writes (inner layer cells, and the GPU
+// path's reset and inside cells) is a donor or a receiving cell of an owned
+// patch's donor tables (host cell indices).
+bool levelset_touches_donors(const dn_ctx* c)
+{
+  const size_t np = c->patches.size();
+  std::vector<std::vector<bool>> used(np);
+  auto mark = [&](size_t p, uint64_t cell) {
+    const DnPatch& P = c->patches[p];
+    if (used[p].empty()) used[p].assign((size_t)P.d.ni * P.d.nj * P.d.nk, false);
+    if (cell < used[p].size()) used[p][cell] = true;
+  };
+  for (size_t r = 0; r < np && r < c->tables.size(); ++r) {
+    if (!c->patches[r].owned) continue;
+    const dn::DonorTables& T = c->tables[r];
+    for (uint64_t u : T.rec_unique) mark(r, u);
+    size_t o = 0;
+    for (size_t q = 0; q < T.donor_patch.size(); ++q) {
+      const size_t m = (size_t)(T.num_receivers[q] * T.stride[q]);
+      for (size_t e = 0; e < m; ++e) mark((size_t)T.donor_patch[q], T.donor_idx[o + e]);
+      o += m;
+    }
+  }
+  auto hit = [&](size_t p, uint64_t cell) { return !used[p].empty() && cell < used[p].size() && used[p][cell]; };
+  for (size_t r = 0; r < np; ++r) {
+    if (!c->patches[r].owned) continue;
+    if (r < c->ls.size() && c->ls_on[r]) {
+      for (const auto& layer : c->ls[r].inner)
+        for (const dn::LayerCell& lc : layer) if (hit(r, lc.cell)) return true;
+    }
+    if (r < c->lsg.size() && c->lsg_on[r]) {
+      for (uint64_t cb : c->lsg[r].below) if (hit(r, cb)) return true;
+      for (const dn::LsInsideCell& ic : c->lsg[r].inside) if (hit(r, ic.cell)) return true;
+    }
+  }
+  return false;
+}
+
 int build_ls_plan(dn_ctx* c)
 {
   free_ls_plan(c);
+  c->ls_touches_donors = levelset_touches_donors(c);
   const size_t np = c->patches.size();
   std::vector<int32_t> patch;
   std::vector<int64_t> cell, donor, nc(np);
@@ -912,9 +957,9 @@ int levelset_bc(dn_ctx* c, int b, int step_b)
   for (char on : c->ls_on) any = any || on;
   for (char on : c->lsg_on) any_gpu = any_gpu || on;
   if (!any && !any_gpu) return DN_OK;
-  donor_stale(c, b);
   int s;
   if (c->ls_dirty && (s = build_ls_plan(c))) return s;
+  if (c->ls_touches_donors) donor_stale(c, b);
   const dn::LsPlan& L = c->ls_plan;
   cudaError_t e = cudaSuccess;
   if (any && L.n > 0) {
@@ -1030,7 +1075,7 @@ int rk_step_enqueue(dn_ctx* c, double dt, const double* alpha, int n_alpha, int 
   for (int s = 0; s < n_alpha; ++s) {
     const int out = (s & 1) ? Y : X;
     const double factor = alpha[s] * dt;   // (*i)*dt, rungekutta.cpp:37
-    if (s > 0 && post_op && (st = donor_copy(c, in))) return st;
+    if (s > 0 && post_op && !donor_current(c, in) && (st = donor_copy(c, in))) return st;
     if ((st = stage_all(c, in, A, out, factor))) return st;
     if ((st = donor_copy(c, out))) return st;   // copyDonorData(0) after the stage (:38)
     if ((st = levelset_bc(c, out, A))) return st;   // runPostOperations() (:39)

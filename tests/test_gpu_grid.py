@@ -313,3 +313,53 @@ def test_step_start_donor_copy_kept_when_donors_include_receiving_cells(golden_d
     assert plain[1] == plain[0] - 1 and plain[2] == plain[1], plain
     chained = launches_per_step(True)
     assert chained[0] == chained[1] == chained[2] == plain[0], chained
+
+
+@pytest.mark.parametrize("precision", [DN_FP64, DN_FP32])
+@pytest.mark.parametrize("graph", [0, 1])
+def test_donor_copies_after_a_wall_away_from_the_overlap_left_out(precision, graph):
+    # the reduced sphere workload: the level-set wall writes no donor and no
+    # receiving cell, so the donor copies that follow it (before the next
+    # stage and at the next step's start) would rewrite the same bits and are
+    # left out; the reference's stage-by-stage sequence with the wall as a
+    # post-operation (every copy made) gives the same result
+    from drnum_b200 import workloads
+    case = workloads.build("sphere", 0.25)
+    alpha = np.ascontiguousarray(cases.RK3_ALPHA, dtype=np.float64)
+
+    def fused():
+        _, objs = workloads.make_grid(case)
+        it = workloads.make_iterator(objs, precision, 0)
+        it.setOption(_lib.DN_OPT_GRAPH, graph)
+        n = [it.launchCount()]
+        for _ in range(3):
+            it.rkStep(case["dt"], alpha)
+            n.append(it.launchCount())
+        out = [it.downloadField(q, 0) for q in range(len(objs))]
+        it.close()
+        return out, np.diff(n)
+
+    def stagewise():
+        _, objs = workloads.make_grid(case)
+        it = workloads.make_iterator(objs, precision, 0)
+        rk = RungeKutta()
+        for a in cases.RK3_ALPHA:
+            rk.addAlpha(a)
+        rk.addIterator(it)
+        rk.addPostOperation(B200LevelSetObjectBC(it))
+        n = [it.launchCount()]
+        for _ in range(3):
+            rk(case["dt"])
+            n.append(it.launchCount())
+        out = [it.downloadField(q, 0) for q in range(len(objs))]
+        it.close()
+        return out, np.diff(n)
+
+    a, na = fused()
+    b, nb = stagewise()
+    for q, (x, y) in enumerate(zip(a, b)):
+        assert np.array_equal(x, y), q
+    # per step the stage-by-stage sequence makes 6 donor copies (one before
+    # and one after every stage); the fused step 4 in its first step (the
+    # step-start copy, one after every stage) and 3 from then on
+    assert na[0] == nb[0] - 2 and na[1] == na[2] == nb[1] - 3, (na, nb)
