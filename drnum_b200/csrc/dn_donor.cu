@@ -11,6 +11,8 @@
 #include "dn_donor.cuh"
 #include "fv_fx32.cuh"
 
+#include <atomic>
+
 namespace dn {
 
 namespace {
@@ -194,16 +196,19 @@ int blocks_for(int n) { return (n + kDonorThreads - 1) / kDonorThreads; }
 template <bool FX, int BLK>
 int pattern_blocks(int n)
 {
-  static int per_device[64] = {};
+  // per device, computed once (threads that race here store the same value)
+  static std::atomic<int> per_device[64];
   int dev = 0;
   cudaGetDevice(&dev);
-  int& cap = per_device[dev & 63];
-  if (cap == 0) {
+  std::atomic<int>& slot = per_device[dev & 63];
+  int cap = slot.load(std::memory_order_relaxed);
+  if (cap <= 0) {
     int sms = 0, per_sm = 0;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_donor_copy_pat<FX, BLK>, kDonorThreads, 0);
     cap = sms * (per_sm > 0 ? per_sm : 1);
     if (cap <= 0) cap = 1;
+    slot.store(cap, std::memory_order_relaxed);
   }
   const int b = blocks_for(n);
   return b < cap ? b : cap;
