@@ -194,7 +194,12 @@ int dn_patch_activate(dn_ctx* ctx, int patch, int active);
 /* One full low-storage RK time step with stage factors alpha[0..n-1]*dt,
  * without the field 0 -> 1 copy (field 1 holds the step-start state after
  * the call, as after the reference's step).  With donor tables it runs the
- * reference's sequence: donor copy, then per stage compute + donor copy.
+ * reference's sequence: donor copy, then per stage compute + donor copy
+ * (+ the level-set wall, and a donor copy before every later stage).  A
+ * donor copy into a buffer whose receiving cells already hold it (nothing
+ * but a donor copy has written the buffer since, under the same tables,
+ * and no donor cell is a receiving cell) is left out: it would write the
+ * same values.  Sharded contexts (an exchange hook) make every copy.
  * Replaces: RungeKutta::operator()(dt) (rungekutta.cpp:27-42). */
 int dn_rk_step(dn_ctx* ctx, double dt, const double* alpha, int n_alpha);
 
