@@ -165,3 +165,25 @@ def test_donor_table_option_is_checked():
     assert it.lib.dn_set_option(it.ctx, _lib.DN_OPT_DONOR_TABLES, 2) == _lib.DN_ERR_ARG
     assert it.lib.dn_set_option(it.ctx, _lib.DN_OPT_DONOR_TABLES, 1) == _lib.DN_OK
     it.close()
+
+
+@pytest.mark.parametrize("name", ["tiled", "jet"])
+def test_batched_workload_equals_per_patch(name):
+    # reduced workloads, FP32 bulk (ragged tiles, patch faces, overlaps):
+    # the batched launches give the bits of one launch per patch
+    from drnum_b200 import workloads
+    case = workloads.build(name, 0.25)
+
+    def run(batched):
+        _, objs = workloads.make_grid(case)
+        it = workloads.make_iterator(objs, DN_FP32, 0)
+        it.setOption(DN_OPT_BATCHED, batched)
+        for _ in range(2):
+            it.rkStep(case["dt"], cases.RK3_ALPHA)
+        out = [it.downloadField(q, 0) for q in range(len(objs))]
+        it.close()
+        return out
+
+    a, b = run(0), run(1)
+    for q, (x, y) in enumerate(zip(a, b)):
+        assert np.array_equal(x, y), q
