@@ -146,7 +146,7 @@ struct dn_ctx {
   std::vector<int> shape;
   bool batch_dirty = true;
   void* d_records = nullptr;
-  void* d_maps = nullptr;                     // FX32 batched: dn::BatchMaps per patch
+  void* d_maps = nullptr;                     // batched: dn::BatchMaps per tile shape and patch
   // work items per tile form (dn::kFxEdge, kFxInside, kFxFull; FP64: all in
   // [kFxEdge]) and tile shape
   void* d_items[3][dn::kNumShapes] = {};
@@ -1224,6 +1224,43 @@ void deal_runs(const std::vector<dn::WorkItem>& runs, int slots, std::vector<dn:
   }
 }
 
+// Column tiles (j0, k0, tile shape) of a patch whose batched tile shape is
+// `shape`.  An FP32-bulk patch with 16 x 32 tiles covers a remainder on a
+// closed axis with narrower tiles: a last column of at most 16 cells with
+// 16 x 16 tiles, a last band of at most 8 rows with 8 x 32 tiles (its corner
+// with a 16 x 16 tile).  They leave fewer idle lanes than 16 x 32 tiles
+// reaching beyond the patch; every cell is computed the same way in any
+// tile, so the bits do not change.
+struct TileRef {
+  int j0, k0, shape;
+};
+
+void patch_tiles(const dn_ctx* c, const DnPatch& P, int shape, std::vector<TileRef>& out)
+{
+  out.clear();
+  const bool fp64 = c->precision == DN_FP64;
+  int tj, tk;
+  dn::shape_tile(fp64, shape, &tj, &tk);
+  const int nj = P.d.nj, nk = P.d.nk;
+  int njm = nj, nkm = nk;          // the extents the main shape covers
+  bool kr = false, jr = false;
+  if (!fp64 && shape == 2) {
+    const int krem = nk % 32, jrem = nj % 16;
+    kr = P.d.face[2] != DN_FACE_PERIODIC && nk > 32 && krem > 0 && krem <= 16;
+    jr = P.d.face[1] != DN_FACE_PERIODIC && nj > 16 && jrem > 0 && jrem <= 8;
+    if (kr) nkm = nk - krem;
+    if (jr) njm = nj - jrem;
+  }
+  for (int j0 = 0; j0 < njm; j0 += tj)
+    for (int k0 = 0; k0 < nkm; k0 += tk) out.push_back(TileRef{j0, k0, shape});
+  if (kr)
+    for (int j0 = 0; j0 < njm; j0 += 16) out.push_back(TileRef{j0, nkm, 1});
+  if (jr) {
+    for (int k0 = 0; k0 < nkm; k0 += 32) out.push_back(TileRef{njm, k0, 0});
+    if (kr) out.push_back(TileRef{njm, nkm, 1});
+  }
+}
+
 // Patch records and work items (patch, column tile, plane range) of every
 // patch, grouped by tile form and shape.  FX32: each launch is one wave of
 // persistent CTAs over balanced groups of items (deal_runs).  FP64: plane
@@ -1235,7 +1272,9 @@ int build_batch(dn_ctx* c)
   if (np == 0) { c->batch_dirty = false; return DN_OK; }
   const bool fp64 = c->precision == DN_FP64;
   std::vector<dn::BatchPatch> rec(np);
-  std::vector<dn::BatchMaps> maps(np);
+  // tensor maps per tile shape and patch: maps[shape * np + patch]
+  std::vector<dn::BatchMaps> maps(np * dn::kNumShapes);
+  std::vector<std::vector<TileRef>> ptiles(np);
   long tiles = 0;
   for (size_t q = 0; q < np; ++q) {
     const DnPatch& P = c->patches[q];
@@ -1250,21 +1289,28 @@ int build_batch(dn_ctx* c)
     r.dx = P.d.dx; r.dy = P.d.dy; r.dz = P.d.dz;
     for (int v = 0; v < 5; ++v) { r.base[v] = P.base[v]; r.quantum[v] = P.quantum[v]; }
     r.wall = P.wall;
-    int tj, tk;
-    dn::shape_tile(fp64, c->shape[q], &tj, &tk);
-    if (P.owned && P.patch_active) tiles += (long)((P.d.nj + tj - 1) / tj) * ((P.d.nk + tk - 1) / tk);
+    patch_tiles(c, P, c->shape[q], ptiles[q]);
+    bool used[dn::kNumShapes] = {};
+    for (const TileRef& t : ptiles[q]) used[t.shape] = true;
+    if (P.owned && P.patch_active) tiles += (long)ptiles[q].size();
     // shadows are never staged: no tensor maps
     r.tma = P.owned ? 1 : 0;
-    if (!fp64) {
-      dn::FxGeom g{};
-      g.ni = P.d.ni; g.nj = P.d.nj; g.nk = P.d.nk; g.kp = P.kp;
-      for (int b = 0; b < 3 && r.tma; ++b)
-        r.tma = dn::encode_stage_maps(maps[q].in[b], &maps[q].un[b], (const int32_t*)P.buf[b],
-                                      (const int32_t*)P.buf[b], g, tj, tk) ? 1 : 0;
-    } else {
-      for (int b = 0; b < 3 && r.tma; ++b)
-        r.tma = dn::encode_stage_map_f64(&maps[q].in[b][0], (const double*)P.buf[b], P.d.ni, P.d.nj, P.d.nk, tj,
-                                         tk) ? 1 : 0;
+    for (int sh = 0; sh < dn::kNumShapes && r.tma; ++sh) {
+      if (!used[sh]) continue;
+      int tj, tk;
+      dn::shape_tile(fp64, sh, &tj, &tk);
+      dn::BatchMaps& M = maps[(size_t)sh * np + q];
+      if (!fp64) {
+        dn::FxGeom g{};
+        g.ni = P.d.ni; g.nj = P.d.nj; g.nk = P.d.nk; g.kp = P.kp;
+        for (int b = 0; b < 3 && r.tma; ++b)
+          r.tma = dn::encode_stage_maps(M.in[b], &M.un[b], (const int32_t*)P.buf[b], (const int32_t*)P.buf[b], g,
+                                        tj, tk) ? 1 : 0;
+      } else {
+        for (int b = 0; b < 3 && r.tma; ++b)
+          r.tma = dn::encode_stage_map_f64(&M.in[b][0], (const double*)P.buf[b], P.d.ni, P.d.nj, P.d.nk, tj, tk)
+                      ? 1 : 0;
+      }
     }
   }
   if (tiles == 0) {
@@ -1284,9 +1330,6 @@ int build_batch(dn_ctx* c)
   for (size_t q = 0; q < np; ++q) {
     const DnPatch& P = c->patches[q];
     if (!P.owned || !P.patch_active) continue;
-    const int sh = c->shape[q];
-    int tj, tk;
-    dn::shape_tile(fp64, sh, &tj, &tk);
     const bool per_y = P.d.face[1] == DN_FACE_PERIODIC, per_z = P.d.face[2] == DN_FACE_PERIODIC;
     // persistent CTAs: one run of all planes per column tile, cut by
     // deal_runs below
@@ -1295,14 +1338,16 @@ int build_batch(dn_ctx* c)
     if (ic < c->batch_min_planes) ic = c->batch_min_planes;   // amortise each item's 3-plane prologue
     if (ic > P.d.ni || persistent) ic = P.d.ni;
     for (int i0 = 0; i0 < P.d.ni; i0 += (int)ic)
-      for (int j0 = 0; j0 < P.d.nj; j0 += tj)
-        for (int k0 = 0; k0 < P.d.nk; k0 += tk) {
-          const bool fy = (j0 + tj <= P.d.nj) && (per_y || (j0 >= 2 && j0 + tj + 2 <= P.d.nj));
-          const bool fz = (k0 + tk <= P.d.nk) && (per_z || (k0 >= 2 && k0 + tk + 2 <= P.d.nk));
-          const bool inside = j0 + tj <= P.d.nj && k0 + tk <= P.d.nk;
-          const int form = fp64 ? dn::kFxEdge : (fy && fz) ? dn::kFxFull : inside ? dn::kFxInside : dn::kFxEdge;
-          items[form][sh].push_back(dn::WorkItem{(int)q, j0, k0, i0, std::min(P.d.ni, i0 + (int)ic)});
-        }
+      for (const TileRef& t : ptiles[q]) {
+        int tj, tk;
+        dn::shape_tile(fp64, t.shape, &tj, &tk);
+        const int j0 = t.j0, k0 = t.k0;
+        const bool fy = (j0 + tj <= P.d.nj) && (per_y || (j0 >= 2 && j0 + tj + 2 <= P.d.nj));
+        const bool fz = (k0 + tk <= P.d.nk) && (per_z || (k0 >= 2 && k0 + tk + 2 <= P.d.nk));
+        const bool inside = j0 + tj <= P.d.nj && k0 + tk <= P.d.nk;
+        const int form = fp64 ? dn::kFxEdge : (fy && fz) ? dn::kFxFull : inside ? dn::kFxInside : dn::kFxEdge;
+        items[form][t.shape].push_back(dn::WorkItem{(int)q, j0, k0, i0, std::min(P.d.ni, i0 + (int)ic)});
+      }
   }
   if (!fp64 && c->batch_waves > 0) {
     for (int f = 0; f < 3; ++f) {
@@ -1321,9 +1366,10 @@ int build_batch(dn_ctx* c)
   e = cudaMemcpyAsync(c->d_records, rec.data(), np * sizeof(dn::BatchPatch), cudaMemcpyHostToDevice, c->stream);
   if (e != cudaSuccess) return cuda_fail(c, e, "patch record upload");
   if (!maps.empty()) {
-    e = cudaMalloc(&c->d_maps, np * sizeof(dn::BatchMaps));
+    e = cudaMalloc(&c->d_maps, maps.size() * sizeof(dn::BatchMaps));
     if (e != cudaSuccess) return fail(c, DN_ERR_NOMEM, "cudaMalloc(tensor maps)");
-    e = cudaMemcpyAsync(c->d_maps, maps.data(), np * sizeof(dn::BatchMaps), cudaMemcpyHostToDevice, c->stream);
+    e = cudaMemcpyAsync(c->d_maps, maps.data(), maps.size() * sizeof(dn::BatchMaps), cudaMemcpyHostToDevice,
+                        c->stream);
     if (e != cudaSuccess) return cuda_fail(c, e, "tensor map upload");
   }
   for (int f = 0; f < 3; ++f) {
@@ -1415,7 +1461,7 @@ int stage_all(dn_ctx* c, int in_b, int un_b, int out_b, double factor)
       if (!c->n_items[f][q]) continue;
       dn::Batch b;
       b.patches = static_cast<const dn::BatchPatch*>(c->d_records);
-      b.maps = static_cast<const dn::BatchMaps*>(c->d_maps);
+      b.maps = c->d_maps ? static_cast<const dn::BatchMaps*>(c->d_maps) + (size_t)q * c->patches.size() : nullptr;
       b.items = static_cast<const dn::WorkItem*>(c->d_items[f][q]);
       b.n_items = c->n_items[f][q];
       b.groups = static_cast<const int*>(c->d_groups[f][q]);
@@ -2841,9 +2887,15 @@ namespace {
 // padded cells a patch occupies with tile shape `shape`
 double padded_cells(const dn_ctx* c, const DnPatch& p, int shape)
 {
-  int tj, tk;
-  dn::shape_tile(c->precision == DN_FP64, shape, &tj, &tk);
-  return (double)p.d.ni * (double)(((p.d.nj + tj - 1) / tj) * tj) * (double)(((p.d.nk + tk - 1) / tk) * tk);
+  std::vector<TileRef> t;
+  patch_tiles(c, p, shape, t);
+  double cells = 0;
+  for (const TileRef& r : t) {
+    int tj, tk;
+    dn::shape_tile(c->precision == DN_FP64, r.shape, &tj, &tk);
+    cells += (double)tj * (double)tk;
+  }
+  return (double)p.d.ni * cells;
 }
 
 std::string device_name(int dev)

@@ -174,16 +174,21 @@ def test_batched_workload_equals_per_patch(name):
     from drnum_b200 import workloads
     case = workloads.build(name, 0.25)
 
-    def run(batched):
+    def run(batched, shape=None):
         _, objs = workloads.make_grid(case)
         it = workloads.make_iterator(objs, DN_FP32, 0)
         it.setOption(DN_OPT_BATCHED, batched)
+        if shape is not None:
+            # 16 x 32 tiles: the batched launches cover short remainders of
+            # closed axes with 16 x 16 and 8 x 32 tiles
+            for q in range(len(objs)):
+                it.setTile(q, shape)
         for _ in range(2):
             it.rkStep(case["dt"], cases.RK3_ALPHA)
         out = [it.downloadField(q, 0) for q in range(len(objs))]
         it.close()
         return out
 
-    a, b = run(0), run(1)
-    for q, (x, y) in enumerate(zip(a, b)):
-        assert np.array_equal(x, y), q
+    a, b, c = run(0), run(1), run(1, 2)
+    for q, (x, y, z) in enumerate(zip(a, b, c)):
+        assert np.array_equal(x, y) and np.array_equal(x, z), q
