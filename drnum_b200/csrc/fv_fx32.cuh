@@ -260,6 +260,21 @@ __device__ __forceinline__ int fx_quant1(float x, FaceRange& r)
   return __float2int_rn(x);
 }
 
+// Patch-face flux of side `side` (axis AXIS) of a boundary cell with FP32
+// state U, in whole quanta (0 for a zero-flux side), recorded in r.  Placed
+// in the face arrays where the missing interior face would be, a min side's
+// flux counts as the face below the cell and a max side's as the face above
+// it, so the residual adds it with the reference's signs (+ min, - max).
+template <int AXIS>
+__device__ __forceinline__ void fx_wall_quanta(const WallBC& bc, int side, int face, const float U[5], float A,
+                                               const float2* face_scale, FaceRange& r, int q[5])
+{
+  float F[5];
+  const bool on = wall_flux<AXIS>(bc, side, face, U, A, F);
+  #pragma unroll
+  for (int v = 0; v < 5; ++v) q[v] = on ? fx_quant1(F[v] * face_scale[v].x, r) : 0;
+}
+
 // Cell whose state stands at index x of an axis: the wrapped cell on a
 // periodic axis, the nearest edge cell outside a closed one.  Copying the
 // edge cell outward makes the van Albada slope of an edge cell exactly zero
@@ -452,6 +467,16 @@ __device__ __forceinline__ bool fx_stage_tile_impl(const FxArgs& a, const CUtens
   const int tid = ty * TP + tp;
   const int kk = 2 * tp;                          // tile column of the pair's first cell
   const int j = j0 + ty, ka = k0 + kk, kb = ka + 1;
+  // inside tiles place the y and z patch-face fluxes of their boundary cells
+  // in the face arrays, in the slot of the missing face, during the slope
+  // phase (their state is in the ring then); the face phase leaves those
+  // slots alone and the residual sums them like interior faces.  The slots
+  // are written and read by the same thread.
+  const bool yz_walls = WALLS && MODE == kFxInside && a.wall.any;
+  const bool w_ymin = yz_walls && j == 0 && !g.per_y && g.nj > 2;
+  const bool w_ymax = yz_walls && j == g.nj - 1 && !g.per_y && g.nj > 2;
+  const bool w_zmin = yz_walls && ka == 0 && !g.per_z && g.nk > 2;
+  const bool w_zmax = yz_walls && kb == g.nk - 1 && !g.per_z && g.nk > 2;
   const bool own_a = PAIRS || ((j < g.nj) && (ka < g.nk));
   const bool own_b = PAIRS || ((j < g.nj) && (kb < g.nk));
   const int njk = g.nj * g.kp;                    // plane stride (rows of kp elements)
@@ -754,6 +779,35 @@ __device__ __forceinline__ bool fx_stage_tile_impl(const FxArgs& a, const CUtens
         }
       }
     }
+    FaceRange wmag_yz;   // y and z patch-face fluxes of the own cells
+    if (w_ymin || w_ymax || w_zmin || w_zmax) {
+      float Ua[5], Ub[5];
+      #pragma unroll
+      for (int v = 0; v < 5; ++v) {
+        const float2 u = RP(r0, v, 0, 0);
+        Ua[v] = u.x;
+        Ub[v] = u.y;
+      }
+      int qa[5], qb[5];
+      if (w_ymin || w_ymax) {
+        const int side = w_ymin ? 2 : 3;
+        fx_wall_quanta<1>(a.wall, side, i * g.nk + ka, Ua, P.A[1].x, P.face_scale, wmag_yz, qa);
+        fx_wall_quanta<1>(a.wall, side, i * g.nk + kb, Ub, P.A[1].x, P.face_scale, wmag_yz, qb);
+        #pragma unroll
+        for (int v = 0; v < 5; ++v)
+          *reinterpret_cast<int2*>(&sm.qy[v][w_ymin ? ty : ty + 1][kk]) = make_int2(qa[v], qb[v]);
+      }
+      if (w_zmin) {
+        fx_wall_quanta<2>(a.wall, 4, i * g.nj + j, Ua, P.A[2].x, P.face_scale, wmag_yz, qa);
+        #pragma unroll
+        for (int v = 0; v < 5; ++v) sm.qz[v][ty][tp].x = qa[v];
+      }
+      if (w_zmax) {
+        fx_wall_quanta<2>(a.wall, 5, i * g.nj + j, Ub, P.A[2].x, P.face_scale, wmag_yz, qb);
+        #pragma unroll
+        for (int v = 0; v < 5; ++v) sm.qz[v][ty][tp + 1].x = qb[v];
+      }
+    }
     __syncthreads();
 
     // every read of the staging plane (dequantised at the end of the last
@@ -769,6 +823,7 @@ __device__ __forceinline__ bool fx_stage_tile_impl(const FxArgs& a, const CUtens
     }
     if (tid == 0) sm.wide[par ^ 1] = 0;   // flag of the next plane (its last reader passed the barrier)
     fmag = xmag;                          // the x faces below the own cells count for this plane too
+    fmag.add(wmag_yz);
 
     // ---------------- B: faces
     // y faces below the own pair; the face below row j is needed even when
@@ -791,7 +846,7 @@ __device__ __forceinline__ bool fx_stage_tile_impl(const FxArgs& a, const CUtens
         int2 q = fx_quant2(mul2(F[v], P.face_scale[v]), fmag);
         if (!exa) q.x = 0;
         if (!exb) q.y = 0;
-        *reinterpret_cast<int2*>(&sm.qy[v][ty][kk]) = q;
+        if (!w_ymin) *reinterpret_cast<int2*>(&sm.qy[v][ty][kk]) = q;   // else: the patch face, placed before
       }
     }
     // z faces below the pair's two cells
@@ -812,7 +867,8 @@ __device__ __forceinline__ bool fx_stage_tile_impl(const FxArgs& a, const CUtens
         int2 q = fx_quant2(mul2(F[v], P.face_scale[v]), fmag);
         if (!exa) q.x = 0;
         if (!exb) q.y = 0;
-        sm.qz[v][ty][tp] = q;
+        if (w_zmin) sm.qz[v][ty][tp].y = q.y;   // .x: the patch face, placed before
+        else sm.qz[v][ty][tp] = q;
       }
     }
     // halo faces: below halo row TJ in column pairs (second-to-last warp)
@@ -836,12 +892,14 @@ __device__ __forceinline__ bool fx_stage_tile_impl(const FxArgs& a, const CUtens
           exa = ey && (PAIRS || k0 + c < g.nk);
           exb = ey && (PAIRS || k0 + c + 1 < g.nk);
         }
+        // (the last row's patch face, if any, is placed by its own cells)
+        const bool keep = yz_walls && j0 + TJ == g.nj && !g.per_y && g.nj > 2;
         #pragma unroll
         for (int v = 0; v < 5; ++v) {
           int2 q = fx_quant2(mul2(F[v], P.face_scale[v]), fmag);
           if (!exa) q.x = 0;
           if (!exb) q.y = 0;
-          *reinterpret_cast<int2*>(&sm.qy[v][TJ][c]) = q;
+          if (!keep) *reinterpret_cast<int2*>(&sm.qy[v][TJ][c]) = q;
         }
       } else if (h >= 32 && h < 32 + TJ / 2) {
         const int ja = h - 32, jb = ja + TJ / 2;
@@ -860,11 +918,15 @@ __device__ __forceinline__ bool fx_stage_tile_impl(const FxArgs& a, const CUtens
           exa = ez && (PAIRS || j0 + ja < g.nj);
           exb = ez && (PAIRS || j0 + jb < g.nj);
         }
+        // (the last column's patch face, if any, is placed by its own cells)
+        const bool keep = yz_walls && k0 + TK == g.nk && !g.per_z && g.nk > 2;
         #pragma unroll
         for (int v = 0; v < 5; ++v) {
           const int2 q = fx_quant2(mul2(F[v], P.face_scale[v]), fmag);
-          sm.qz[v][ja][TP].x = exa ? q.x : 0;
-          sm.qz[v][jb][TP].x = exb ? q.y : 0;
+          if (!keep) {
+            sm.qz[v][ja][TP].x = exa ? q.x : 0;
+            sm.qz[v][jb][TP].x = exb ? q.y : 0;
+          }
         }
       }
     }
@@ -924,10 +986,13 @@ __device__ __forceinline__ bool fx_stage_tile_impl(const FxArgs& a, const CUtens
       // patch-face fluxes of boundary cells: whole quanta like the interior
       // faces (a wall face replaces the cell's missing interior face, so a
       // cell still sums six faces)
+      // (inside tiles: the y and z sides are in the face arrays already)
       const bool any_wall = WALLS && a.wall.any;
-      const bool edge_ijk = any_wall && (i == 0 || i == g.ni - 1 || j == 0 || j == g.nj - 1);
-      const bool wall_a = any_wall && (edge_ijk || ka == 0 || ka == g.nk - 1);
-      const bool wall_b = own_b && any_wall && (edge_ijk || kb == g.nk - 1);
+      const bool x_only = MODE == kFxInside;
+      const bool edge_i = any_wall && (i == 0 || i == g.ni - 1);
+      const bool edge_ijk = edge_i || (any_wall && !x_only && (j == 0 || j == g.nj - 1));
+      const bool wall_a = x_only ? edge_i : any_wall && (edge_ijk || ka == 0 || ka == g.nk - 1);
+      const bool wall_b = own_b && (x_only ? edge_i : any_wall && (edge_ijk || kb == g.nk - 1));
       long long wa[5] = {0, 0, 0, 0, 0}, wb[5] = {0, 0, 0, 0, 0};
       FaceRange wmag;
       if (wall_a || wall_b) {
@@ -941,7 +1006,7 @@ __device__ __forceinline__ bool fx_stage_tile_impl(const FxArgs& a, const CUtens
           for (int v = 0; v < 5; ++v) uc[v] = fmaf(P.quantum[v].x, (float)a.in[v * nc + c + q], P.base[v].x);
           add_wall_fluxes(a.wall, g.ni, g.nj, g.nk, g.per_x, g.per_y, g.per_z, i, j, ka + q, uc, P.A[0].x, P.A[1].x,
                           P.A[2].x, q == 0 ? wa : wb,
-                          [&](int v, float F) { return fx_quant1(F * P.face_scale[v].x, wmag); });
+                          [&](int v, float F) { return fx_quant1(F * P.face_scale[v].x, wmag); }, !x_only);
         }
         fbad |= !(wmag.mag() < kFxFaceLimit);
       }

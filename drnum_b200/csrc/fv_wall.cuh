@@ -109,11 +109,13 @@ __device__ __forceinline__ bool wall_flux(const WallBC& bc, int side, int face, 
 }
 
 // Adds the wall fluxes of a boundary cell (i, j, k) to its residual r in the
-// reference's order; F_to_r converts a flux to the residual's type.
+// reference's order; F_to_r converts a flux to the residual's type.  yz =
+// false: the x sides only (a caller that has placed the y and z sides
+// elsewhere).
 template <typename T, typename R, typename Conv>
 __device__ __forceinline__ void add_wall_fluxes(const WallBC& bc, int ni, int nj, int nk, int per_x, int per_y,
                                                 int per_z, int i, int j, int k, const T U[5], T Ax, T Ay, T Az,
-                                                R r[5], Conv F_to_r)
+                                                R r[5], Conv F_to_r, bool yz = true)
 {
   T F[5];
   if (!per_x && ni > 2) {
@@ -126,6 +128,7 @@ __device__ __forceinline__ void add_wall_fluxes(const WallBC& bc, int ni, int nj
       for (int v = 0; v < 5; ++v) r[v] -= F_to_r(v, F[v]);
     }
   }
+  if (!yz) return;
   if (!per_y && nj > 2) {
     if (j == 0 && wall_flux<1>(bc, 2, i * nk + k, U, Ay, F)) {
       #pragma unroll
